@@ -1,0 +1,273 @@
+/*
+ * visloc_ba_cuda.h -- C ABI of the B200 bundle-adjustment solver.
+ *
+ * This is the drop-in boundary for the reference's bundle-adjustment
+ * accelerator plug-in:
+ *
+ *   trait BaAccelerator { fn optimize(&self, ba: &mut BundleAdjustment,
+ *                                     config: &BaConfig, scope: BaScope)
+ *                         -> Option<Result<BaResult, BaError>>; }
+ *   (pipelines/slam/src/ba_accel.rs:23-32, registered with
+ *    set_ba_accelerator, ba_accel.rs:38-40)
+ *
+ * The reference's own GPU implementation of that trait is GpuBundleAdjuster
+ * (crates/ba-gpu/src/solver.rs:80-85, impl at :729-742).  The entry points
+ * below follow the repository's native-library convention
+ * (native/descriptor_gemm/descriptor_gemm.cu:101-193: versioned ABI, opaque
+ * context, error string, int status with 0 = ok).
+ *
+ * Memory: the caller owns every array.  All calls are synchronous.  A context
+ * is not thread-safe; use one context per thread (or serialise calls).
+ *
+ * Identifiers: the reference keys poses and landmarks by u64 ids in BTreeMaps.
+ * This ABI takes dense indices; the host shim maps ids to indices in ascending
+ * id order, as GpuBundleAdjuster::upload does (solver.rs:256-314).
+ */
+#ifndef VISLOC_BA_CUDA_H
+#define VISLOC_BA_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VLBA_ABI_VERSION 1u
+
+/* ------------------------------------------------------------------ status */
+/* Return codes.  The Rust shim maps VLBA_DECLINED to `None` (the caller then
+ * runs the CPU solver) and the VLBA_ERR_* values that mirror BaError
+ * (pipelines/slam/src/bundle/mod.rs:1022-1056) to `Some(Err(..))`. */
+enum vlba_status {
+  VLBA_OK = 0,
+  VLBA_DECLINED = 1,                   /* outside what this solver implements */
+  VLBA_ERR_NO_POSES = 2,               /* BaError::NoPoses */
+  VLBA_ERR_NO_LANDMARKS = 3,           /* BaError::NoLandmarks */
+  VLBA_ERR_NO_OBSERVATIONS = 4,        /* BaError::NoObservations */
+  VLBA_ERR_ALL_POSES_FIXED = 5,        /* BaError::AllPosesFixed */
+  VLBA_ERR_MISSING_POSE = 6,           /* BaError::MissingPose(id) */
+  VLBA_ERR_MISSING_LANDMARK = 7,       /* BaError::MissingLandmark(id) */
+  VLBA_ERR_UNSUPPORTED_CAMERA_MODEL = 8, /* BaError::UnsupportedCameraModel */
+  VLBA_ERR_SINGULAR_SYSTEM = 9,        /* BaError::SingularSystem */
+  VLBA_ERR_INVALID_ARGUMENT = 10,      /* null pointer, bad size or config */
+  VLBA_ERR_CUDA = 11,                  /* a CUDA call failed */
+  VLBA_ERR_OUT_OF_MEMORY = 12,         /* device memory exhausted */
+  VLBA_ERR_TIMEOUT = 13,               /* a bounded device wait gave up */
+  VLBA_ERR_BUSY = 14                   /* server queue full / ticket pending */
+};
+
+/* ------------------------------------------------------------------ camera */
+/* The pinhole family whose Camera::project is the pinhole followed by radial
+ * 1 + k1 r^2 + k2 r^4 (core/types/camera.rs:15-41, project at :351-432,
+ * intrinsics at :243-260, radial_distortion at :213-227).  Parameter layouts
+ * are the reference's (COLMAP) layouts:
+ *   PINHOLE        [fx, fy, cx, cy (, k1 (, k2))]
+ *   SIMPLE_PINHOLE [f, cx, cy]
+ *   SIMPLE_RADIAL  [f, cx, cy, k1]
+ *   RADIAL         [f, cx, cy, k1 (, k2)]
+ *   OPENCV         [fx, fy, cx, cy, k1, k2, p1, p2] with p1 = p2 = 0
+ * Other models (fisheye, FOV, double sphere, tangential OpenCV) make
+ * visloc_ba_cuda_optimize return VLBA_DECLINED. */
+enum vlba_camera_model {
+  VLBA_CAMERA_PINHOLE = 0,
+  VLBA_CAMERA_SIMPLE_PINHOLE = 1,
+  VLBA_CAMERA_SIMPLE_RADIAL = 2,
+  VLBA_CAMERA_RADIAL = 3,
+  VLBA_CAMERA_OPENCV = 4,
+  VLBA_CAMERA_OTHER = 255
+};
+
+typedef struct vlba_camera {
+  uint32_t model;        /* enum vlba_camera_model */
+  uint32_t num_params;   /* <= 8 */
+  double params[8];
+  /* Fixed rig extrinsic T_sensor<-rig of a BaRigObservation
+   * (bundle/mod.rs:245-251).  Identity (1,0,0,0 / 0,0,0) for the monocular
+   * BaObservation, whose pose is the camera's own T_camera<-world. */
+  double sensor_from_rig_q[4]; /* w, i, j, k */
+  double sensor_from_rig_t[3];
+} vlba_camera;
+
+/* ----------------------------------------------------------------- problem */
+/* BundleAdjustment (bundle/mod.rs:530-622) restricted to the monocular and
+ * rig observations.  Poses are T_world->camera (Pose::world_to_camera,
+ * core/geometry/pose.rs:4-7): a unit quaternion (w, i, j, k) and a
+ * translation.  pose_q, pose_t and landmarks are overwritten with the
+ * optimised values on success, as the reference mutates `ba` in place. */
+typedef struct vlba_problem {
+  uint64_t num_poses;
+  uint64_t num_landmarks;
+  uint64_t num_observations;
+  double* pose_q;                 /* [4 * num_poses] */
+  double* pose_t;                 /* [3 * num_poses] */
+  const uint8_t* pose_fixed;      /* [num_poses], nonzero = fixed; NULL = none */
+  double* landmarks;              /* [3 * num_landmarks] */
+  const uint8_t* landmark_fixed;  /* [num_landmarks]; NULL = none fixed */
+  const uint32_t* obs_pose;       /* [num_observations] dense pose index */
+  const uint32_t* obs_landmark;   /* [num_observations] dense landmark index */
+  const double* obs_xy;           /* [2 * num_observations] pixel (u, v) */
+  /* Per-observation camera index into `cameras`.  NULL: every observation
+   * is a monocular BaObservation through cameras[0] (BundleAdjustment::camera).
+   * Non-NULL: each observation is a BaRigObservation with its own camera and
+   * sensor_from_rig. */
+  const uint32_t* obs_camera;
+  uint32_t num_cameras;
+  const vlba_camera* cameras;
+} vlba_problem;
+
+/* ------------------------------------------------------------------ config */
+enum vlba_robust_kernel {
+  VLBA_KERNEL_NONE = 0,   /* RobustKernel::None */
+  VLBA_KERNEL_HUBER = 1,  /* RobustKernel::Huber { delta } */
+  VLBA_KERNEL_CAUCHY = 2  /* RobustKernel::Cauchy { c } */
+};
+
+/* BaConfig (bundle/mod.rs:626-752) plus the PCG controls of GpuBaSettings
+ * (crates/ba-gpu/src/solver.rs:25-50).  visloc_ba_cuda_default_config fills
+ * the reference's defaults (mod.rs:729-752). */
+typedef struct vlba_config {
+  uint32_t max_iterations;
+  uint32_t has_initial_lambda;     /* 0 = None (pure Gauss-Newton) */
+  double initial_lambda;
+  double lambda_increase_factor;
+  double lambda_decrease_factor;
+  double max_lambda;
+  double min_lambda;
+  double step_tolerance;
+  double cost_tolerance;
+  uint32_t has_relative_cost_tolerance;
+  uint32_t robust_kernel;          /* enum vlba_robust_kernel */
+  double relative_cost_tolerance;
+  double robust_parameter;         /* Huber delta or Cauchy c */
+  uint32_t max_pcg_iterations;     /* per LM linear solve */
+  uint32_t flags;                  /* VLBA_FLAG_* */
+  double pcg_relative_tolerance;   /* stop once |r| <= tol |b| */
+  uint32_t reserved[8];
+} vlba_config;
+
+/* Record per-iteration device phase times in vlba_iteration (costs a device
+ * synchronisation per iteration; the analogue of VISLOC_BA_GPU_PROFILE,
+ * solver.rs:571,622-628). */
+#define VLBA_FLAG_PROFILE 1u
+
+/* ------------------------------------------------------------------ result */
+/* BaIterationStats (bundle/mod.rs:755-763) plus solver diagnostics. */
+typedef struct vlba_iteration {
+  uint64_t iteration;
+  double cost_before;
+  double cost_after;
+  double max_pose_step;
+  double max_landmark_step;
+  double lambda;
+  uint32_t step_accepted;
+  uint32_t pcg_iterations;
+  double pcg_relative_residual;    /* |r| / |b| at PCG exit */
+  double linearize_ms;             /* with VLBA_FLAG_PROFILE, else 0 */
+  double solve_ms;
+} vlba_iteration;
+
+/* BaResult (bundle/mod.rs:765-771) plus diagnostics. */
+typedef struct vlba_result {
+  double initial_cost;
+  double final_cost;
+  uint32_t converged;
+  uint32_t num_iterations;         /* total; entries beyond capacity dropped */
+  uint64_t initial_nonprojectable;
+  uint64_t final_nonprojectable;
+  uint64_t total_pcg_iterations;
+  uint64_t error_index;            /* id for MISSING_POSE / MISSING_LANDMARK */
+  double device_ms;                /* device time of the LM iterations */
+  double upload_ms;                /* host+device time of the upload */
+} vlba_result;
+
+/* Device layout of a problem, computed on the host without touching the GPU
+ * (the memory figure is what a solve allocates, for admission control). */
+typedef struct vlba_plan_info {
+  uint64_t variable_cameras;
+  uint64_t variable_landmarks;
+  uint64_t variable_observations;   /* observations of a variable landmark
+                                       by a variable camera */
+  uint64_t camera_pairs;            /* camera pairs sharing a variable
+                                       landmark: off-diagonal Schur blocks */
+  uint64_t schur_terms;             /* landmark terms summed into them */
+  uint32_t tile_size;               /* Schur tiles are tile_size^2 blocks */
+  uint32_t tile_rows;
+  uint32_t tiles;
+  uint32_t assembly_lanes;          /* lanes per off-diagonal block */
+  uint64_t device_bytes;
+  double bytes_per_iteration;       /* algorithmic bytes of one LM iteration
+                                       (linearisation + one trial) */
+  double bytes_per_pcg_iteration;
+} vlba_plan_info;
+
+/* ------------------------------------------------------------ entry points */
+
+/* ABI version of the loaded library (VLBA_ABI_VERSION). */
+uint32_t visloc_ba_cuda_abi_version(void);
+
+/* Reference defaults of BaConfig (mod.rs:729-752) and GpuBaSettings
+ * (solver.rs:36-50: 100 PCG iterations, tolerance 1e-4). */
+void visloc_ba_cuda_default_config(vlba_config* out);
+
+/* Create a solver context on CUDA device `device`; NULL on failure.
+ * Replaces GpuBundleAdjuster::new (solver.rs:130-190). */
+void* visloc_ba_cuda_create(int device);
+
+/* Release a context and all of its device memory. */
+void visloc_ba_cuda_destroy(void* ctx);
+
+/* Message of the last failure on `ctx` (valid until the next call on it). */
+const char* visloc_ba_cuda_last_error(void* ctx);
+
+/* Validation and eligibility only, no device work: the checks of
+ * BundleAdjustment::optimize_weighted_backend (bundle/lm.rs:168-229) and of
+ * GpuBundleAdjuster::check (solver.rs:212-251) that apply to this problem
+ * type.  `error_index` (may be NULL) receives the offending id. */
+int visloc_ba_cuda_check(const vlba_problem* problem, const vlba_config* config,
+                         uint64_t* error_index);
+
+/* Levenberg-Marquardt solve of `problem` in place.  Replaces
+ * GpuBundleAdjuster::optimize (solver.rs:552-690) and the reference CPU
+ * BundleAdjustment::optimize (bundle/optimize.rs:8-28 -> lm.rs:162-1017).
+ * `iterations` (capacity `iterations_capacity`, may be 0/NULL) receives the
+ * per-iteration trace of BaResult::iterations. */
+int visloc_ba_cuda_optimize(void* ctx, vlba_problem* problem,
+                            const vlba_config* config, vlba_result* result,
+                            vlba_iteration* iterations,
+                            uint32_t iterations_capacity);
+
+/* The three phases of visloc_ba_cuda_optimize, for callers that solve the
+ * same problem repeatedly or time the device solve alone:
+ *   upload:          validate, build the device structures, copy the state;
+ *   solve_uploaded:  LM from the uploaded initial state, device-resident;
+ *   download:        copy the last solve's poses and landmarks back.
+ * GpuBundleAdjuster::upload (solver.rs:253-385) is the reference's upload. */
+int visloc_ba_cuda_upload(void* ctx, const vlba_problem* problem,
+                          const vlba_config* config);
+int visloc_ba_cuda_solve_uploaded(void* ctx, const vlba_config* config,
+                                  vlba_result* result,
+                                  vlba_iteration* iterations,
+                                  uint32_t iterations_capacity);
+int visloc_ba_cuda_download(void* ctx, vlba_problem* problem);
+
+/* Host-only: validate `problem`, build its device layout and check every
+ * index of that layout against the arrays it addresses; `pcg_iterations`
+ * sets the PCG count of bytes_per_iteration.  No device is needed. */
+int visloc_ba_cuda_plan(const vlba_problem* problem, const vlba_config* config,
+                        double pcg_iterations, vlba_plan_info* info);
+
+/* Robust cost and non-projectable count of `problem` as given, in FP64 on the
+ * device: BundleAdjustment::robust_cost_weighted (bundle/problem.rs:497-560)
+ * and nonprojectable_observation_count (problem.rs:252-304), the pair the
+ * reference GPU path evaluates on the CPU (cost_and_nonprojectable,
+ * solver.rs:696-727). */
+int visloc_ba_cuda_cost(void* ctx, const vlba_problem* problem,
+                        const vlba_config* config, double* cost,
+                        uint64_t* nonprojectable);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VISLOC_BA_CUDA_H */

@@ -1,0 +1,1073 @@
+// ba_oracle.cpp -- TEST INFRASTRUCTURE ONLY.
+//
+// CPU FP64 restatement of the reference's bundle-adjustment
+// Levenberg-Marquardt solve (MarvinSt/visloc-rs), used as the checker for the
+// CUDA solver and as the timed CPU baseline.  Nothing in the product links or
+// calls this file; only tests/, __graft_entry__.smoke() and bench.py's CPU
+// baseline leg load the shared library built from it.
+//
+// The reference is Rust (no Rust toolchain exists here), so it cannot be
+// compiled or imported; this file restates its algorithm step by step:
+//   LM control and gates ........ pipelines/slam/src/bundle/lm.rs:162-1017
+//   validation .................. lm.rs:168-229
+//   variable slots .............. lm.rs:234-249
+//   normal equations (mono) ..... bundle/normal_equations.rs:421-493
+//   normal equations (rig) ...... normal_equations.rs:618-660,
+//                                 rig_residual_jacobians sqrt_qr.rs:960-1001
+//   projection + Jacobian ....... bundle/jacobians.rs:18-124
+//   Schur reduction (sparse) .... normal_equations.rs:1621-1733
+//   dense solve (Cholesky->LU) .. pipelines/slam/src/pose_graph.rs:2259-2270
+//   landmark-only step .......... normal_equations.rs:1332-1371
+//   robust kernels .............. pose_graph.rs:87-138
+//   cost / non-projectable ...... bundle/problem.rs:252-304, 497-560
+//   SE3 exp / compose ........... crates/core/src/geometry/se3.rs:32-121
+//   Camera::project ............. crates/core/src/types/camera.rs:351-432
+//   quaternion arithmetic ....... nalgebra 0.33.3 (UnitQuaternion *, transform,
+//                                 from_scaled_axis, to_rotation_matrix)
+//
+// Parallel loops (OpenMP) never change a result: every accumulator is owned by
+// one thread and visited in the serial order, as the reference's rayon paths
+// guarantee (bundle/mod.rs:22-70).  Compiled with -ffp-contract=off so no
+// multiply-add is fused, matching Rust's arithmetic.
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <vector>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#include "../include/visloc_ba_cuda.h"
+
+namespace {
+
+// ------------------------------------------------------------ small algebra
+struct Quat { double w, i, j, k; };
+struct V3 { double x, y, z; };
+
+inline V3 v3(double x, double y, double z) { return V3{x, y, z}; }
+inline V3 cross(const V3& a, const V3& b) {
+  return v3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+
+// nalgebra UnitQuaternion::to_rotation_matrix (row-major result).
+void quat_to_matrix(const Quat& q, double m[9]) {
+  const double i = q.i, j = q.j, k = q.k, w = q.w;
+  const double ww = w * w, ii = i * i, jj = j * j, kk = k * k;
+  const double ij = i * j * 2.0, wk = w * k * 2.0, wj = w * j * 2.0;
+  const double ik = i * k * 2.0, jk = j * k * 2.0, wi = w * i * 2.0;
+  m[0] = ww + ii - jj - kk; m[1] = ij - wk;           m[2] = wj + ik;
+  m[3] = wk + ij;           m[4] = ww - ii + jj - kk; m[5] = jk - wi;
+  m[6] = ik - wj;           m[7] = wi + jk;           m[8] = ww - ii - jj + kk;
+}
+
+// nalgebra UnitQuaternion * Vector3: t = 2 (v x p); p + w t + v x t.
+V3 quat_rotate(const Quat& q, const V3& p) {
+  const V3 v = v3(q.i, q.j, q.k);
+  V3 t = cross(v, p);
+  t = v3(t.x * 2.0, t.y * 2.0, t.z * 2.0);
+  const V3 c = cross(v, t);
+  return v3(t.x * q.w + c.x + p.x, t.y * q.w + c.y + p.y, t.z * q.w + c.z + p.z);
+}
+
+// Hamilton product a * b.
+Quat quat_mul(const Quat& a, const Quat& b) {
+  return Quat{a.w * b.w - a.i * b.i - a.j * b.j - a.k * b.k,
+              a.w * b.i + a.i * b.w + a.j * b.k - a.k * b.j,
+              a.w * b.j - a.i * b.k + a.j * b.w + a.k * b.i,
+              a.w * b.k + a.i * b.j - a.j * b.i + a.k * b.w};
+}
+
+// UnitQuaternion::from_scaled_axis = exp(Quaternion::from_imag(w / 2)).
+Quat quat_from_scaled_axis(const V3& w) {
+  const V3 h = v3(w.x / 2.0, w.y / 2.0, w.z / 2.0);
+  const double nn = h.x * h.x + h.y * h.y + h.z * h.z;
+  const double eps = std::numeric_limits<double>::epsilon();
+  if (nn <= eps * eps) return Quat{1.0, 0.0, 0.0, 0.0};
+  const double n = std::sqrt(nn);
+  const double s = std::sin(n) / n;
+  return Quat{std::cos(n), h.x * s, h.y * s, h.z * s};
+}
+
+void skew(const V3& v, double m[9]) {
+  m[0] = 0.0;  m[1] = -v.z; m[2] = v.y;
+  m[3] = v.z;  m[4] = 0.0;  m[5] = -v.x;
+  m[6] = -v.y; m[7] = v.x;  m[8] = 0.0;
+}
+
+void mat3_mul(const double a[9], const double b[9], double c[9]) {
+  for (int r = 0; r < 3; ++r)
+    for (int col = 0; col < 3; ++col) {
+      double s = 0.0;
+      for (int k = 0; k < 3; ++k) s += a[r * 3 + k] * b[k * 3 + col];
+      c[r * 3 + col] = s;
+    }
+}
+
+// so3_left_jacobian (se3.rs:109-121).
+void so3_left_jacobian(const V3& w, double v[9]) {
+  const double theta_sq = w.x * w.x + w.y * w.y + w.z * w.z;
+  double s[9], s2[9];
+  skew(w, s);
+  mat3_mul(s, s, s2);
+  double a, b;
+  if (theta_sq < 1e-10) {
+    a = 0.5;
+    b = 1.0 / 6.0;
+  } else {
+    const double theta = std::sqrt(theta_sq);
+    a = (1.0 - std::cos(theta)) / theta_sq;
+    b = (theta - std::sin(theta)) / (theta * theta_sq);
+  }
+  for (int e = 0; e < 9; ++e) v[e] = (e % 4 == 0 ? 1.0 : 0.0) + a * s[e] + b * s2[e];
+}
+
+struct Se3 { Quat q; V3 t; };
+
+// SE3::exp (se3.rs:72-82), tangent [rho; omega].
+Se3 se3_exp(const double xi[6]) {
+  const V3 rho = v3(xi[0], xi[1], xi[2]);
+  const V3 omega = v3(xi[3], xi[4], xi[5]);
+  Se3 out;
+  out.q = quat_from_scaled_axis(omega);
+  double v[9];
+  so3_left_jacobian(omega, v);
+  out.t = v3(v[0] * rho.x + v[1] * rho.y + v[2] * rho.z,
+             v[3] * rho.x + v[4] * rho.y + v[5] * rho.z,
+             v[6] * rho.x + v[7] * rho.y + v[8] * rho.z);
+  return out;
+}
+
+// SE3::compose (se3.rs:32-37): self * other.
+Se3 se3_compose(const Se3& a, const Se3& b) {
+  Se3 out;
+  out.q = quat_mul(a.q, b.q);
+  const V3 r = quat_rotate(a.q, b.t);
+  out.t = v3(r.x + a.t.x, r.y + a.t.y, r.z + a.t.z);
+  return out;
+}
+
+V3 se3_transform(const Se3& T, const V3& p) {
+  const V3 r = quat_rotate(T.q, p);
+  return v3(r.x + T.t.x, r.y + T.t.y, r.z + T.t.z);
+}
+
+// -------------------------------------------------------------- cameras
+struct Cam {
+  double fx, fy, cx, cy, k1, k2;
+  bool radial;        // MonoProjection::Radial (k1 or k2 nonzero)
+  bool rig;           // observation carries sensor_from_rig
+  Se3 sensor_from_rig;
+};
+
+// Camera::intrinsics / radial_distortion (camera.rs:213-260) restricted to
+// the radial pinhole family; false for any other model (the reference admits
+// them through Camera::project_with_point_jacobian, which this restatement,
+// like the CUDA solver, does not cover).
+bool resolve_camera(const vlba_camera& c, Cam* out) {
+  const double* p = c.params;
+  const uint32_t n = c.num_params;
+  double fx, fy, cx, cy, k1 = 0.0, k2 = 0.0;
+  bool has_radial = false;
+  switch (c.model) {
+    case VLBA_CAMERA_PINHOLE:
+      if (n < 4) return false;
+      fx = p[0]; fy = p[1]; cx = p[2]; cy = p[3];
+      if (n >= 5) { has_radial = true; k1 = p[4]; k2 = n >= 6 ? p[5] : 0.0; }
+      break;
+    case VLBA_CAMERA_OPENCV:
+      if (n < 4) return false;
+      fx = p[0]; fy = p[1]; cx = p[2]; cy = p[3];
+      if ((n >= 7 && p[6] != 0.0) || (n >= 8 && p[7] != 0.0)) return false;  // tangential
+      if (n >= 5) { has_radial = true; k1 = p[4]; k2 = n >= 6 ? p[5] : 0.0; }
+      break;
+    case VLBA_CAMERA_SIMPLE_PINHOLE:
+      if (n < 3) return false;
+      fx = fy = p[0]; cx = p[1]; cy = p[2];
+      break;
+    case VLBA_CAMERA_SIMPLE_RADIAL:
+      if (n < 3) return false;
+      fx = fy = p[0]; cx = p[1]; cy = p[2];
+      if (n >= 4) { has_radial = true; k1 = p[3]; k2 = 0.0; }
+      break;
+    case VLBA_CAMERA_RADIAL:
+      if (n < 3) return false;
+      fx = fy = p[0]; cx = p[1]; cy = p[2];
+      if (n >= 4) { has_radial = true; k1 = p[3]; k2 = n >= 5 ? p[4] : 0.0; }
+      break;
+    default:
+      return false;
+  }
+  out->fx = fx; out->fy = fy; out->cx = cx; out->cy = cy;
+  out->k1 = k1; out->k2 = k2;
+  out->radial = has_radial && (k1 != 0.0 || k2 != 0.0);
+  out->sensor_from_rig.q = Quat{c.sensor_from_rig_q[0], c.sensor_from_rig_q[1],
+                                c.sensor_from_rig_q[2], c.sensor_from_rig_q[3]};
+  out->sensor_from_rig.t = v3(c.sensor_from_rig_t[0], c.sensor_from_rig_t[1],
+                              c.sensor_from_rig_t[2]);
+  out->rig = false;
+  return true;
+}
+
+// Camera::project for the radial pinhole family (camera.rs:351-432).
+bool camera_project(const Cam& c, const V3& p, double out[2]) {
+  if (!(std::isfinite(p.x) && std::isfinite(p.y) && std::isfinite(p.z))) return false;
+  if (p.z <= 0.0) return false;
+  double x = p.x / p.z;
+  double y = p.y / p.z;
+  if (c.radial) {
+    const double r2 = x * x + y * y;
+    const double d = 1.0 + c.k1 * r2 + c.k2 * r2 * r2;
+    x *= d;
+    y *= d;
+  }
+  out[0] = c.fx * x + c.cx;
+  out[1] = c.fy * y + c.cy;
+  return true;
+}
+
+// mono_project_with_jacobian (jacobians.rs:63-113); j is row-major 2x3.
+bool mono_project_with_jacobian(const Cam& c, const V3& xc, double pred[2], double j[6]) {
+  if (xc.z <= 0.0) return false;
+  if (!c.radial) {
+    // project_pinhole (jacobians.rs:115-124) + the closed-form J_pi.
+    pred[0] = c.fx * xc.x / xc.z + c.cx;
+    pred[1] = c.fy * xc.y / xc.z + c.cy;
+    const double z_inv = 1.0 / xc.z;
+    j[0] = c.fx * z_inv;
+    j[1] = 0.0;
+    j[2] = -c.fx * xc.x * z_inv * z_inv;
+    j[3] = 0.0;
+    j[4] = c.fy * z_inv;
+    j[5] = -c.fy * xc.y * z_inv * z_inv;
+    return true;
+  }
+  const double x = xc.x / xc.z;
+  const double y = xc.y / xc.z;
+  const double r2 = x * x + y * y;
+  const double d = 1.0 + c.k1 * r2 + c.k2 * r2 * r2;
+  pred[0] = c.fx * (x * d) + c.cx;
+  pred[1] = c.fy * (y * d) + c.cy;
+  const double g = c.k1 + 2.0 * c.k2 * r2;
+  const double d11 = d + 2.0 * x * x * g;
+  const double d12 = 2.0 * x * y * g;
+  const double d22 = d + 2.0 * y * y * g;
+  const double z_inv = 1.0 / xc.z;
+  j[0] = c.fx * d11 * z_inv;
+  j[1] = c.fx * d12 * z_inv;
+  j[2] = -c.fx * (d11 * x + d12 * y) * z_inv;
+  j[3] = c.fy * d12 * z_inv;
+  j[4] = c.fy * d22 * z_inv;
+  j[5] = -c.fy * (d12 * x + d22 * y) * z_inv;
+  for (int e = 0; e < 2; ++e)
+    if (!std::isfinite(pred[e])) return false;
+  for (int e = 0; e < 6; ++e)
+    if (!std::isfinite(j[e])) return false;
+  return true;
+}
+
+// ---------------------------------------------------------- robust kernels
+struct Kernel {
+  uint32_t kind;
+  double p;
+  // RobustKernel::cost (pose_graph.rs:103-120).
+  double cost(double s) const {
+    if (kind == VLBA_KERNEL_HUBER) {
+      const double dsq = p * p;
+      return s <= dsq ? s : 2.0 * p * std::sqrt(s) - dsq;
+    }
+    if (kind == VLBA_KERNEL_CAUCHY) {
+      const double csq = p * p;
+      return csq * std::log(1.0 + s / csq);
+    }
+    return s;
+  }
+  // RobustKernel::weight (pose_graph.rs:122-138).
+  double weight(double s) const {
+    if (kind == VLBA_KERNEL_HUBER) {
+      const double dsq = p * p;
+      return s <= dsq ? 1.0 : p / std::sqrt(s);
+    }
+    if (kind == VLBA_KERNEL_CAUCHY) {
+      const double csq = p * p;
+      return 1.0 / (1.0 + s / csq);
+    }
+    return 1.0;
+  }
+};
+
+// ------------------------------------------------------------ the problem
+struct Problem {
+  const vlba_problem* p;
+  std::vector<Cam> cams;
+  bool per_obs_camera;
+  std::vector<Se3> poses;
+  std::vector<V3> points;
+  Kernel kernel;
+
+  const Cam& cam_of(size_t o) const {
+    return per_obs_camera ? cams[p->obs_camera[o]] : cams[0];
+  }
+};
+
+int threads_or_default(int threads) {
+#ifdef _OPENMP
+  return threads > 0 ? threads : omp_get_max_threads();
+#else
+  (void)threads;
+  return 1;
+#endif
+}
+
+// Per-observation residual and Jacobians.  Monocular: normal_equations.rs
+// :421-470; rig: rig_residual_jacobians (sqrt_qr.rs:960-1001).
+bool residual_jacobians(const Problem& P, size_t o, double r[2], double jp[12], double jl[6]) {
+  const uint32_t pi = P.p->obs_pose[o];
+  const uint32_t li = P.p->obs_landmark[o];
+  const Se3& T = P.poses[pi];
+  const V3& X = P.points[li];
+  const Cam& c = P.cam_of(o);
+  double R[9];
+  quat_to_matrix(T.q, R);
+  double xs[9];
+  skew(X, xs);
+  double rxs[9];  // R * [X]x
+  mat3_mul(R, xs, rxs);
+  double pred[2], jpi[6];
+  if (!P.per_obs_camera) {
+    const V3 xc = se3_transform(T, X);
+    if (xc.z <= 0.0) return false;
+    if (!mono_project_with_jacobian(c, xc, pred, jpi)) return false;
+    r[0] = pred[0] - P.p->obs_xy[2 * o];
+    r[1] = pred[1] - P.p->obs_xy[2 * o + 1];
+    // dx_dxi = [R | -R [X]x]; j_pose = j_pi * dx_dxi; j_lm = j_pi * R.
+    double dx[18];
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) {
+        dx[a * 6 + b] = R[a * 3 + b];
+        dx[a * 6 + 3 + b] = -rxs[a * 3 + b];
+      }
+    for (int a = 0; a < 2; ++a) {
+      for (int b = 0; b < 6; ++b) {
+        double s = 0.0;
+        for (int k = 0; k < 3; ++k) s += jpi[a * 3 + k] * dx[k * 6 + b];
+        jp[a * 6 + b] = s;
+      }
+      for (int b = 0; b < 3; ++b) {
+        double s = 0.0;
+        for (int k = 0; k < 3; ++k) s += jpi[a * 3 + k] * R[k * 3 + b];
+        jl[a * 3 + b] = s;
+      }
+    }
+    return true;
+  }
+  // Rig observation.
+  const V3 prig = se3_transform(T, X);
+  const V3 ps = se3_transform(c.sensor_from_rig, prig);
+  if (!c.radial) {
+    if (ps.z <= 0.0) return false;
+    pred[0] = c.fx * ps.x / ps.z + c.cx;
+    pred[1] = c.fy * ps.y / ps.z + c.cy;
+    const double z_inv = 1.0 / ps.z;  // pinhole_projection_jacobian (sqrt_qr.rs:445-463)
+    const double z_inv2 = z_inv * z_inv;
+    jpi[0] = c.fx * z_inv; jpi[1] = 0.0; jpi[2] = -c.fx * ps.x * z_inv2;
+    jpi[3] = 0.0; jpi[4] = c.fy * z_inv; jpi[5] = -c.fy * ps.y * z_inv2;
+  } else if (!mono_project_with_jacobian(c, ps, pred, jpi)) {
+    return false;
+  }
+  r[0] = pred[0] - P.p->obs_xy[2 * o];
+  r[1] = pred[1] - P.p->obs_xy[2 * o + 1];
+  double Rs[9];
+  quat_to_matrix(c.sensor_from_rig.q, Rs);
+  double drig[18];
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) {
+      drig[a * 6 + b] = R[a * 3 + b];
+      drig[a * 6 + 3 + b] = -rxs[a * 3 + b];
+    }
+  double pr[6];  // projection * R_sensor<-rig (2x3)
+  for (int a = 0; a < 2; ++a)
+    for (int b = 0; b < 3; ++b) {
+      double s = 0.0;
+      for (int k = 0; k < 3; ++k) s += jpi[a * 3 + k] * Rs[k * 3 + b];
+      pr[a * 3 + b] = s;
+    }
+  for (int a = 0; a < 2; ++a) {
+    for (int b = 0; b < 6; ++b) {
+      double s = 0.0;
+      for (int k = 0; k < 3; ++k) s += pr[a * 3 + k] * drig[k * 6 + b];
+      jp[a * 6 + b] = s;
+    }
+    for (int b = 0; b < 3; ++b) {
+      double s = 0.0;
+      for (int k = 0; k < 3; ++k) s += pr[a * 3 + k] * R[k * 3 + b];
+      jl[a * 3 + b] = s;
+    }
+  }
+  return true;
+}
+
+// robust_cost_weighted + nonprojectable_observation_count (problem.rs:252-304,
+// 497-560): cost over projectable observations, count of the others.
+void cost_and_nonprojectable(const Problem& P, int threads, double* cost, uint64_t* bad) {
+  const size_t n = P.p->num_observations;
+  const size_t chunk = 4096;
+  const size_t nchunks = (n + chunk - 1) / chunk;
+  std::vector<double> part(nchunks, 0.0);
+  std::vector<uint64_t> partbad(nchunks, 0);
+#pragma omp parallel for schedule(static) num_threads(threads)
+  for (long long ci = 0; ci < (long long)nchunks; ++ci) {
+    double s = 0.0;
+    uint64_t b = 0;
+    const size_t lo = (size_t)ci * chunk, hi = std::min(n, lo + chunk);
+    for (size_t o = lo; o < hi; ++o) {
+      const Se3& T = P.poses[P.p->obs_pose[o]];
+      const V3& X = P.points[P.p->obs_landmark[o]];
+      const Cam& c = P.cam_of(o);
+      V3 xc = se3_transform(T, X);
+      if (P.per_obs_camera) xc = se3_transform(c.sensor_from_rig, xc);
+      double pred[2];
+      if (xc.z <= 0.0 || !camera_project(c, xc, pred)) {
+        ++b;
+        continue;
+      }
+      const double rx = pred[0] - P.p->obs_xy[2 * o];
+      const double ry = pred[1] - P.p->obs_xy[2 * o + 1];
+      s += P.kernel.cost(rx * rx + ry * ry);
+    }
+    part[ci] = s;
+    partbad[ci] = b;
+  }
+  double total = 0.0;
+  uint64_t tb = 0;
+  for (size_t ci = 0; ci < nchunks; ++ci) {
+    total += part[ci];
+    tb += partbad[ci];
+  }
+  *cost = total;
+  *bad = tb;
+}
+
+// ------------------------------------------------------- dense factorisation
+// In-place Cholesky of the symmetric n x n row-major matrix `a` (lower
+// triangle used).  Blocked right-looking; trailing updates in parallel.
+bool cholesky(std::vector<double>& a, size_t n, int threads) {
+  const size_t nb = 48;
+  for (size_t k0 = 0; k0 < n; k0 += nb) {
+    const size_t k1 = std::min(n, k0 + nb);
+    // Factor the diagonal block.
+    for (size_t j = k0; j < k1; ++j) {
+      double s = a[j * n + j];
+      for (size_t q = k0; q < j; ++q) s -= a[j * n + q] * a[j * n + q];
+      if (!(s > 0.0) || !std::isfinite(s)) return false;
+      const double ljj = std::sqrt(s);
+      a[j * n + j] = ljj;
+      for (size_t i = j + 1; i < k1; ++i) {
+        double t = a[i * n + j];
+        for (size_t q = k0; q < j; ++q) t -= a[i * n + q] * a[j * n + q];
+        a[i * n + j] = t / ljj;
+      }
+    }
+    // Panel below the diagonal block.
+#pragma omp parallel for schedule(static) num_threads(threads)
+    for (long long ii = (long long)k1; ii < (long long)n; ++ii) {
+      const size_t i = (size_t)ii;
+      for (size_t j = k0; j < k1; ++j) {
+        double t = a[i * n + j];
+        for (size_t q = k0; q < j; ++q) t -= a[i * n + q] * a[j * n + q];
+        a[i * n + j] = t / a[j * n + j];
+      }
+    }
+    // Trailing update A22 -= L21 L21^T (lower triangle).
+#pragma omp parallel for schedule(dynamic, 16) num_threads(threads)
+    for (long long ii = (long long)k1; ii < (long long)n; ++ii) {
+      const size_t i = (size_t)ii;
+      const double* li = &a[i * n + k0];
+      for (size_t j = k1; j <= i; ++j) {
+        const double* lj = &a[j * n + k0];
+        double t = 0.0;
+        for (size_t q = 0; q < k1 - k0; ++q) t += li[q] * lj[q];
+        a[i * n + j] -= t;
+      }
+    }
+  }
+  return true;
+}
+
+void cholesky_solve(const std::vector<double>& l, size_t n, std::vector<double>& x) {
+  for (size_t i = 0; i < n; ++i) {
+    double s = x[i];
+    for (size_t q = 0; q < i; ++q) s -= l[i * n + q] * x[q];
+    x[i] = s / l[i * n + i];
+  }
+  for (size_t ii = n; ii-- > 0;) {
+    double s = x[ii];
+    for (size_t q = ii + 1; q < n; ++q) s -= l[q * n + ii] * x[q];
+    x[ii] = s / l[ii * n + ii];
+  }
+}
+
+// LU with partial pivoting (nalgebra's lu().solve fallback); false if singular.
+bool lu_solve(std::vector<double> a, size_t n, std::vector<double>& x) {
+  std::vector<size_t> piv(n);
+  for (size_t k = 0; k < n; ++k) {
+    size_t p = k;
+    double best = std::fabs(a[k * n + k]);
+    for (size_t i = k + 1; i < n; ++i)
+      if (std::fabs(a[i * n + k]) > best) { best = std::fabs(a[i * n + k]); p = i; }
+    if (best == 0.0) return false;
+    piv[k] = p;
+    if (p != k) {
+      for (size_t c = 0; c < n; ++c) std::swap(a[k * n + c], a[p * n + c]);
+      std::swap(x[k], x[p]);
+    }
+    const double inv = 1.0 / a[k * n + k];
+    for (size_t i = k + 1; i < n; ++i) {
+      const double f = a[i * n + k] * inv;
+      a[i * n + k] = f;
+      for (size_t c = k + 1; c < n; ++c) a[i * n + c] -= f * a[k * n + c];
+      x[i] -= f * x[k];
+    }
+  }
+  for (size_t ii = n; ii-- > 0;) {
+    double s = x[ii];
+    for (size_t c = ii + 1; c < n; ++c) s -= a[ii * n + c] * x[c];
+    x[ii] = s / a[ii * n + ii];
+  }
+  for (size_t i = 0; i < n; ++i)
+    if (!std::isfinite(x[i])) return false;
+  return true;
+}
+
+// nalgebra Matrix3::try_inverse: cofactor inverse, None when det == 0.
+bool try_inverse3(const double m[9], double inv[9]) {
+  const double m11 = m[0], m12 = m[1], m13 = m[2];
+  const double m21 = m[3], m22 = m[4], m23 = m[5];
+  const double m31 = m[6], m32 = m[7], m33 = m[8];
+  const double minor_m12_m23 = m22 * m33 - m32 * m23;
+  const double minor_m11_m23 = m21 * m33 - m31 * m23;
+  const double minor_m11_m22 = m21 * m32 - m31 * m22;
+  const double det = m11 * minor_m12_m23 - m12 * minor_m11_m23 + m13 * minor_m11_m22;
+  if (det == 0.0) return false;
+  inv[0] = minor_m12_m23 / det;
+  inv[1] = (m13 * m32 - m33 * m12) / det;
+  inv[2] = (m12 * m23 - m22 * m13) / det;
+  inv[3] = -minor_m11_m23 / det;
+  inv[4] = (m11 * m33 - m31 * m13) / det;
+  inv[5] = (m13 * m21 - m23 * m11) / det;
+  inv[6] = minor_m11_m22 / det;
+  inv[7] = (m12 * m31 - m32 * m11) / det;
+  inv[8] = (m11 * m22 - m21 * m12) / det;
+  return true;
+}
+
+// ------------------------------------------------------- normal equations
+struct Cross { uint32_t pose; double a[18]; };  // 6x3 row-major
+
+struct Normal {
+  std::vector<double> h_pp;   // 36 per variable pose
+  std::vector<double> b_p;    // 6 per variable pose
+  std::vector<double> h_ll;   // 9 per variable landmark
+  std::vector<double> b_l;    // 3 per variable landmark
+  std::vector<std::vector<Cross>> cross;  // per variable landmark
+};
+
+struct Slots {
+  std::vector<int64_t> pose_slot;  // -1: fixed
+  std::vector<int64_t> lm_slot;
+  std::vector<uint32_t> var_poses, var_lms;
+};
+
+void build_slots(const vlba_problem* p, Slots* s) {
+  s->pose_slot.assign(p->num_poses, -1);
+  s->lm_slot.assign(p->num_landmarks, -1);
+  for (uint64_t i = 0; i < p->num_poses; ++i)
+    if (!(p->pose_fixed && p->pose_fixed[i])) {
+      s->pose_slot[i] = (int64_t)s->var_poses.size();
+      s->var_poses.push_back((uint32_t)i);
+    }
+  for (uint64_t i = 0; i < p->num_landmarks; ++i)
+    if (!(p->landmark_fixed && p->landmark_fixed[i])) {
+      s->lm_slot[i] = (int64_t)s->var_lms.size();
+      s->var_lms.push_back((uint32_t)i);
+    }
+}
+
+// build_normal_equations (normal_equations.rs:352-493, 618-660): per-obs
+// contributions computed in parallel, accumulated by owner in obs order.
+void build_normal(const Problem& P, const Slots& S, int threads, Normal* N) {
+  const size_t np = S.var_poses.size(), nl = S.var_lms.size();
+  const size_t no = P.p->num_observations;
+  N->h_pp.assign(np * 36, 0.0);
+  N->b_p.assign(np * 6, 0.0);
+  N->h_ll.assign(nl * 9, 0.0);
+  N->b_l.assign(nl * 3, 0.0);
+  N->cross.assign(nl, {});
+  struct Contrib { double r[2], jp[12], jl[6], w; bool ok; };
+  std::vector<Contrib> c(no);
+#pragma omp parallel for schedule(static) num_threads(threads)
+  for (long long oo = 0; oo < (long long)no; ++oo) {
+    Contrib& k = c[oo];
+    k.ok = residual_jacobians(P, (size_t)oo, k.r, k.jp, k.jl);
+    if (k.ok) k.w = P.kernel.weight(k.r[0] * k.r[0] + k.r[1] * k.r[1]);
+  }
+  // Pose blocks: each thread owns poses p with p % nt == tid.
+#pragma omp parallel num_threads(threads)
+  {
+#ifdef _OPENMP
+    const int tid = omp_get_thread_num(), nt = omp_get_num_threads();
+#else
+    const int tid = 0, nt = 1;
+#endif
+    for (size_t o = 0; o < no; ++o) {
+      const Contrib& k = c[o];
+      if (!k.ok) continue;
+      const int64_t ps = S.pose_slot[P.p->obs_pose[o]];
+      if (ps >= 0 && (ps % nt) == tid) {
+        double* h = &N->h_pp[ps * 36];
+        double* b = &N->b_p[ps * 6];
+        for (int rr = 0; rr < 6; ++rr) {
+          for (int cc = 0; cc < 6; ++cc) {
+            const double v = k.jp[rr] * k.jp[cc] + k.jp[6 + rr] * k.jp[6 + cc];
+            h[rr * 6 + cc] += k.w * v;
+          }
+          b[rr] += k.w * (k.jp[rr] * k.r[0] + k.jp[6 + rr] * k.r[1]);
+        }
+      }
+      const int64_t ls = S.lm_slot[P.p->obs_landmark[o]];
+      if (ls >= 0 && (ls % nt) == tid) {
+        double* h = &N->h_ll[ls * 9];
+        double* b = &N->b_l[ls * 3];
+        for (int rr = 0; rr < 3; ++rr) {
+          for (int cc = 0; cc < 3; ++cc) {
+            const double v = k.jl[rr] * k.jl[cc] + k.jl[3 + rr] * k.jl[3 + cc];
+            h[rr * 3 + cc] += k.w * v;
+          }
+          b[rr] += k.w * (k.jl[rr] * k.r[0] + k.jl[3 + rr] * k.r[1]);
+        }
+        if (ps >= 0) {
+          Cross x;
+          x.pose = (uint32_t)ps;
+          for (int rr = 0; rr < 6; ++rr)
+            for (int cc = 0; cc < 3; ++cc)
+              x.a[rr * 3 + cc] = k.w * (k.jp[rr] * k.jl[cc] + k.jp[6 + rr] * k.jl[3 + cc]);
+          N->cross[ls].push_back(x);
+        }
+      }
+    }
+  }
+}
+
+// The reduced camera system S = D + lambda I - sum_l A H^-1 B^T (lower
+// blocks, mirrored), rhs = -b_p + sum_l A H^-1 b_l, as
+// solve_step_pose_blocks_with_debug (normal_equations.rs:1621-1700).
+void reduce(const Normal& N, size_t np, size_t nl, double lambda, int threads,
+            std::vector<double>& s, std::vector<double>& rhs,
+            std::vector<uint8_t>& inv_ok, std::vector<double>& hinv) {
+  const size_t dim = np * 6;
+  s.assign(dim * dim, 0.0);
+  rhs.assign(dim, 0.0);
+  for (size_t p = 0; p < np; ++p) {
+    for (int rr = 0; rr < 6; ++rr)
+      for (int cc = 0; cc < 6; ++cc) {
+        double v = N.h_pp[p * 36 + rr * 6 + cc];
+        if (rr == cc && lambda > 0.0) v += lambda;
+        s[(p * 6 + rr) * dim + p * 6 + cc] = v;
+      }
+    for (int k = 0; k < 6; ++k) rhs[p * 6 + k] = -N.b_p[p * 6 + k];
+  }
+  inv_ok.assign(nl, 0);
+  hinv.assign(nl * 9, 0.0);
+#pragma omp parallel for schedule(static) num_threads(threads)
+  for (long long ll = 0; ll < (long long)nl; ++ll) {
+    double h[9];
+    std::memcpy(h, &N.h_ll[ll * 9], sizeof h);
+    if (lambda > 0.0) { h[0] += lambda; h[4] += lambda; h[8] += lambda; }
+    inv_ok[ll] = try_inverse3(h, &hinv[ll * 9]) ? 1 : 0;
+  }
+#pragma omp parallel num_threads(threads)
+  {
+#ifdef _OPENMP
+    const int tid = omp_get_thread_num(), nt = omp_get_num_threads();
+#else
+    const int tid = 0, nt = 1;
+#endif
+    for (size_t l = 0; l < nl; ++l) {
+      if (!inv_ok[l]) continue;
+      const double* hi = &hinv[l * 9];
+      const std::vector<Cross>& cr = N.cross[l];
+      for (const Cross& a : cr) {
+        if ((int)(a.pose % nt) != tid) continue;
+        double ah[18];
+        for (int rr = 0; rr < 6; ++rr)
+          for (int cc = 0; cc < 3; ++cc) {
+            double t = 0.0;
+            for (int k = 0; k < 3; ++k) t += a.a[rr * 3 + k] * hi[k * 3 + cc];
+            ah[rr * 3 + cc] = t;
+          }
+        for (const Cross& b : cr) {
+          if (a.pose < b.pose) continue;
+          double* dst = &s[(size_t)a.pose * 6 * dim + (size_t)b.pose * 6];
+          for (int rr = 0; rr < 6; ++rr)
+            for (int cc = 0; cc < 6; ++cc) {
+              double t = 0.0;
+              for (int k = 0; k < 3; ++k) t += ah[rr * 3 + k] * b.a[cc * 3 + k];
+              dst[rr * dim + cc] -= t;
+            }
+        }
+        const double* bl = &N.b_l[l * 3];
+        for (int k = 0; k < 6; ++k) {
+          double t = 0.0;
+          for (int q = 0; q < 3; ++q) t += ah[k * 3 + q] * bl[q];
+          rhs[a.pose * 6 + k] += t;
+        }
+      }
+    }
+  }
+  // Mirror the lower block triangle.
+#pragma omp parallel for schedule(static) num_threads(threads)
+  for (long long ii = 0; ii < (long long)dim; ++ii)
+    for (size_t j = (size_t)ii + 1; j < dim; ++j) {
+      const size_t bi = (size_t)ii / 6, bj = j / 6;
+      if (bj > bi) s[(size_t)ii * dim + j] = s[j * dim + (size_t)ii];
+    }
+}
+
+// solve_step (normal_equations.rs:1314-1733).  Returns false on
+// BaError::SingularSystem.
+bool solve_step(const Normal& N, size_t np, size_t nl, double lambda, int solver,
+                int threads, std::vector<double>& dp, std::vector<double>& dl) {
+  dp.assign(np * 6, 0.0);
+  dl.assign(nl * 3, 0.0);
+  if (np == 0) {  // landmark-only (normal_equations.rs:1332-1371)
+    for (size_t l = 0; l < nl; ++l) {
+      double h[9], hi[9];
+      std::memcpy(h, &N.h_ll[l * 9], sizeof h);
+      if (lambda > 0.0) { h[0] += lambda; h[4] += lambda; h[8] += lambda; }
+      if (!try_inverse3(h, hi)) return false;
+      for (int k = 0; k < 3; ++k)
+        dl[l * 3 + k] = -(hi[k * 3] * N.b_l[l * 3] + hi[k * 3 + 1] * N.b_l[l * 3 + 1] +
+                          hi[k * 3 + 2] * N.b_l[l * 3 + 2]);
+    }
+    return true;
+  }
+  std::vector<double> s, rhs, hinv;
+  std::vector<uint8_t> ok;
+  reduce(N, np, nl, lambda, threads, s, rhs, ok, hinv);
+  const size_t dim = np * 6;
+  std::vector<double> x = rhs;
+  std::vector<double> a = s;
+  if (cholesky(a, dim, threads)) {
+    cholesky_solve(a, dim, x);
+  } else {
+    if (solver == 1) return false;  // LinearSolver::Sparse: block Cholesky only
+    x = rhs;
+    if (!lu_solve(s, dim, x)) return false;
+  }
+  dp = x;
+  // Back-substitution (normal_equations.rs:1717-1733).
+#pragma omp parallel for schedule(static) num_threads(threads)
+  for (long long ll = 0; ll < (long long)nl; ++ll) {
+    const size_t l = (size_t)ll;
+    if (!ok[l]) continue;
+    double acc[3] = {-N.b_l[l * 3], -N.b_l[l * 3 + 1], -N.b_l[l * 3 + 2]};
+    for (const Cross& c : N.cross[l]) {
+      for (int k = 0; k < 3; ++k) {
+        double t = 0.0;
+        for (int q = 0; q < 6; ++q) t += c.a[q * 3 + k] * dp[c.pose * 6 + q];
+        acc[k] -= t;
+      }
+    }
+    const double* hi = &hinv[l * 9];
+    for (int k = 0; k < 3; ++k)
+      dl[l * 3 + k] = hi[k * 3] * acc[0] + hi[k * 3 + 1] * acc[1] + hi[k * 3 + 2] * acc[2];
+  }
+  return true;
+}
+
+bool load_problem(const vlba_problem* p, const vlba_config* cfg, Problem* P, int* status,
+                  uint64_t* err_index) {
+  *status = VLBA_OK;
+  if (!p || !cfg) { *status = VLBA_ERR_INVALID_ARGUMENT; return false; }
+  if (p->num_cameras == 0 || !p->cameras) { *status = VLBA_ERR_UNSUPPORTED_CAMERA_MODEL; return false; }
+  P->p = p;
+  P->per_obs_camera = p->obs_camera != nullptr;
+  P->cams.resize(p->num_cameras);
+  for (uint32_t c = 0; c < p->num_cameras; ++c)
+    if (!resolve_camera(p->cameras[c], &P->cams[c])) {
+      *status = VLBA_ERR_UNSUPPORTED_CAMERA_MODEL;
+      return false;
+    }
+  // Order of the checks of lm.rs:168-229.
+  if (p->num_poses == 0) { *status = VLBA_ERR_NO_POSES; return false; }
+  if (p->num_observations == 0) { *status = VLBA_ERR_NO_OBSERVATIONS; return false; }
+  if (p->num_landmarks == 0) { *status = VLBA_ERR_NO_LANDMARKS; return false; }
+  for (uint64_t o = 0; o < p->num_observations; ++o) {
+    if (p->obs_pose[o] >= p->num_poses) {
+      *status = VLBA_ERR_MISSING_POSE;
+      if (err_index) *err_index = p->obs_pose[o];
+      return false;
+    }
+    if (p->obs_landmark[o] >= p->num_landmarks) {
+      *status = VLBA_ERR_MISSING_LANDMARK;
+      if (err_index) *err_index = p->obs_landmark[o];
+      return false;
+    }
+    if (P->per_obs_camera && p->obs_camera[o] >= p->num_cameras) {
+      *status = VLBA_ERR_INVALID_ARGUMENT;
+      if (err_index) *err_index = o;
+      return false;
+    }
+  }
+  P->poses.resize(p->num_poses);
+  for (uint64_t i = 0; i < p->num_poses; ++i) {
+    P->poses[i].q = Quat{p->pose_q[4 * i], p->pose_q[4 * i + 1], p->pose_q[4 * i + 2],
+                         p->pose_q[4 * i + 3]};
+    P->poses[i].t = v3(p->pose_t[3 * i], p->pose_t[3 * i + 1], p->pose_t[3 * i + 2]);
+  }
+  P->points.resize(p->num_landmarks);
+  for (uint64_t i = 0; i < p->num_landmarks; ++i)
+    P->points[i] = v3(p->landmarks[3 * i], p->landmarks[3 * i + 1], p->landmarks[3 * i + 2]);
+  P->kernel = Kernel{cfg->robust_kernel, cfg->robust_parameter};
+  return true;
+}
+
+void store_problem(const Problem& P, vlba_problem* p) {
+  for (uint64_t i = 0; i < p->num_poses; ++i) {
+    p->pose_q[4 * i] = P.poses[i].q.w;
+    p->pose_q[4 * i + 1] = P.poses[i].q.i;
+    p->pose_q[4 * i + 2] = P.poses[i].q.j;
+    p->pose_q[4 * i + 3] = P.poses[i].q.k;
+    p->pose_t[3 * i] = P.poses[i].t.x;
+    p->pose_t[3 * i + 1] = P.poses[i].t.y;
+    p->pose_t[3 * i + 2] = P.poses[i].t.z;
+  }
+  for (uint64_t i = 0; i < p->num_landmarks; ++i) {
+    p->landmarks[3 * i] = P.points[i].x;
+    p->landmarks[3 * i + 1] = P.points[i].y;
+    p->landmarks[3 * i + 2] = P.points[i].z;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int vlba_oracle_check(const vlba_problem* p, const vlba_config* cfg, uint64_t* err_index) {
+  Problem P;
+  int status;
+  if (!load_problem(p, cfg, &P, &status, err_index)) return status;
+  Slots S;
+  build_slots(p, &S);
+  if (S.var_poses.empty() && S.var_lms.empty()) return VLBA_ERR_ALL_POSES_FIXED;
+  return VLBA_OK;
+}
+
+int vlba_oracle_cost(const vlba_problem* p, const vlba_config* cfg, int threads, double* cost,
+                     uint64_t* nonprojectable) {
+  Problem P;
+  int status;
+  if (!load_problem(p, cfg, &P, &status, nullptr)) return status;
+  cost_and_nonprojectable(P, threads_or_default(threads), cost, nonprojectable);
+  return VLBA_OK;
+}
+
+// Camera::project of one camera-frame point; returns 0 when it does not project.
+int vlba_oracle_camera_project(const vlba_camera* cam, const double xc[3], double out[2]) {
+  Cam c;
+  if (!resolve_camera(*cam, &c)) return -1;
+  return camera_project(c, v3(xc[0], xc[1], xc[2]), out) ? 1 : 0;
+}
+
+// mono_project_with_jacobian; returns 0 when the point does not project.
+int vlba_oracle_mono_project(const vlba_camera* cam, const double xc[3], double pred[2],
+                             double jac[6]) {
+  Cam c;
+  if (!resolve_camera(*cam, &c)) return -1;
+  return mono_project_with_jacobian(c, v3(xc[0], xc[1], xc[2]), pred, jac) ? 1 : 0;
+}
+
+// T <- T * Exp(xi) for a pose given as quaternion (w,i,j,k) + translation.
+void vlba_oracle_pose_update(double q[4], double t[3], const double xi[6]) {
+  Se3 T{Quat{q[0], q[1], q[2], q[3]}, v3(t[0], t[1], t[2])};
+  const Se3 r = se3_compose(T, se3_exp(xi));
+  q[0] = r.q.w; q[1] = r.q.i; q[2] = r.q.j; q[3] = r.q.k;
+  t[0] = r.t.x; t[1] = r.t.y; t[2] = r.t.z;
+}
+
+// Normal equations at the current state: h_pp (36 per variable pose), b_p (6),
+// h_ll (9 per variable landmark), b_l (3).  Arrays sized by the caller.
+int vlba_oracle_normal_equations(const vlba_problem* p, const vlba_config* cfg, int threads,
+                                 double* h_pp, double* b_p, double* h_ll, double* b_l) {
+  Problem P;
+  int status;
+  if (!load_problem(p, cfg, &P, &status, nullptr)) return status;
+  Slots S;
+  build_slots(p, &S);
+  Normal N;
+  build_normal(P, S, threads_or_default(threads), &N);
+  std::copy(N.h_pp.begin(), N.h_pp.end(), h_pp);
+  std::copy(N.b_p.begin(), N.b_p.end(), b_p);
+  std::copy(N.h_ll.begin(), N.h_ll.end(), h_ll);
+  std::copy(N.b_l.begin(), N.b_l.end(), b_l);
+  return VLBA_OK;
+}
+
+// Reduced camera system (dense (6P)^2, both triangles) and its rhs at lambda,
+// plus the damped step (dp 6P, dl 3L) when dp/dl are non-NULL.
+int vlba_oracle_reduced_system(const vlba_problem* p, const vlba_config* cfg, double lambda,
+                               int threads, double* s_out, double* rhs_out, double* dp_out,
+                               double* dl_out) {
+  Problem P;
+  int status;
+  if (!load_problem(p, cfg, &P, &status, nullptr)) return status;
+  Slots S;
+  build_slots(p, &S);
+  const int nt = threads_or_default(threads);
+  Normal N;
+  build_normal(P, S, nt, &N);
+  const size_t np = S.var_poses.size(), nl = S.var_lms.size();
+  std::vector<double> s, rhs, hinv;
+  std::vector<uint8_t> ok;
+  if (np > 0) {
+    reduce(N, np, nl, lambda, nt, s, rhs, ok, hinv);
+    if (s_out) std::copy(s.begin(), s.end(), s_out);
+    if (rhs_out) std::copy(rhs.begin(), rhs.end(), rhs_out);
+  }
+  if (dp_out || dl_out) {
+    std::vector<double> dp, dl;
+    if (!solve_step(N, np, nl, lambda, 0, nt, dp, dl)) return VLBA_ERR_SINGULAR_SYSTEM;
+    if (dp_out) std::copy(dp.begin(), dp.end(), dp_out);
+    if (dl_out) std::copy(dl.begin(), dl.end(), dl_out);
+  }
+  return VLBA_OK;
+}
+
+// BundleAdjustment::optimize (lm.rs:162-1017, Legacy backend).
+// solver: 0 = LinearSolver::Dense (Cholesky, LU fallback), 1 = Sparse
+// (Cholesky only).  threads <= 0: all.
+int vlba_oracle_optimize(vlba_problem* p, const vlba_config* cfg, int solver, int threads,
+                         vlba_result* res, vlba_iteration* its, uint32_t cap) {
+  Problem P;
+  int status;
+  uint64_t err_index = 0;
+  if (res) std::memset(res, 0, sizeof *res);
+  if (!load_problem(p, cfg, &P, &status, &err_index)) {
+    if (res) res->error_index = err_index;
+    return status;
+  }
+  const int nt = threads_or_default(threads);
+  Slots S;
+  build_slots(p, &S);
+  if (S.var_poses.empty() && S.var_lms.empty()) return VLBA_ERR_ALL_POSES_FIXED;
+  const size_t np = S.var_poses.size(), nl = S.var_lms.size();
+
+  double initial_cost;
+  uint64_t current_nonproj;
+  cost_and_nonprojectable(P, nt, &initial_cost, &current_nonproj);
+  const uint64_t initial_nonproj = current_nonproj;
+  double current_cost = initial_cost;
+  double lambda = cfg->has_initial_lambda ? cfg->initial_lambda : 0.0;
+  bool converged = false;
+  uint32_t count = 0;
+  auto push = [&](uint64_t it, double cb, double ca, double mps, double mls, double lam,
+                  bool acc) {
+    if (its && count < cap) {
+      vlba_iteration& e = its[count];
+      std::memset(&e, 0, sizeof e);
+      e.iteration = it;
+      e.cost_before = cb;
+      e.cost_after = ca;
+      e.max_pose_step = mps;
+      e.max_landmark_step = mls;
+      e.lambda = lam;
+      e.step_accepted = acc ? 1u : 0u;
+    }
+    ++count;
+  };
+  uint64_t final_nonproj = current_nonproj;
+  for (uint32_t iteration = 0; iteration < cfg->max_iterations; ++iteration) {
+    Normal N;
+    build_normal(P, S, nt, &N);
+    const std::vector<Se3> saved_poses = P.poses;
+    const std::vector<V3> saved_points = P.points;
+    const double cost_before = current_cost;
+    std::vector<double> dp, dl;
+    if (!solve_step(N, np, nl, lambda, solver, nt, dp, dl)) {
+      lambda = std::min(lambda * cfg->lambda_increase_factor, cfg->max_lambda);
+      push(iteration, cost_before, cost_before, 0.0, 0.0, lambda, false);
+      if (lambda >= cfg->max_lambda) break;
+      continue;
+    }
+    double max_pose_step = 0.0;
+    for (size_t s = 0; s < np; ++s) {
+      const double* xi = &dp[s * 6];
+      double nn = 0.0;
+      for (int k = 0; k < 6; ++k) nn += xi[k] * xi[k];
+      max_pose_step = std::max(max_pose_step, std::sqrt(nn));
+      Se3& T = P.poses[S.var_poses[s]];
+      T = se3_compose(T, se3_exp(xi));
+    }
+    double max_lm_step = 0.0;
+    for (size_t s = 0; s < nl; ++s) {
+      const double* d = &dl[s * 3];
+      max_lm_step = std::max(max_lm_step, std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]));
+      V3& X = P.points[S.var_lms[s]];
+      X = v3(X.x + d[0], X.y + d[1], X.z + d[2]);
+    }
+    double cost_after;
+    uint64_t nonproj_after;
+    cost_and_nonprojectable(P, nt, &cost_after, &nonproj_after);
+    const bool cost_accepted = cfg->has_initial_lambda ? (cost_after < cost_before) : true;
+    const bool accepted = cost_accepted && nonproj_after <= current_nonproj;
+    if (!accepted) {
+      P.poses = saved_poses;
+      P.points = saved_points;
+      lambda = std::min(lambda * cfg->lambda_increase_factor, cfg->max_lambda);
+      push(iteration, cost_before, cost_after, max_pose_step, max_lm_step, lambda, false);
+      if (!cfg->has_initial_lambda) break;
+      if (lambda >= cfg->max_lambda) break;
+      continue;
+    }
+    push(iteration, cost_before, cost_after, max_pose_step, max_lm_step, lambda, true);
+    current_cost = cost_after;
+    current_nonproj = nonproj_after;
+    final_nonproj = nonproj_after;
+    if (cfg->has_initial_lambda)
+      lambda = std::max(lambda * cfg->lambda_decrease_factor, cfg->min_lambda);
+    if (max_pose_step < cfg->step_tolerance && max_lm_step < cfg->step_tolerance) {
+      converged = true;
+      break;
+    }
+    if (std::fabs(cost_before - cost_after) < cfg->cost_tolerance) {
+      converged = true;
+      break;
+    }
+    if (cfg->has_relative_cost_tolerance) {
+      const double tol = cfg->relative_cost_tolerance;
+      if (std::isfinite(tol) && tol >= 0.0 &&
+          (cost_before - cost_after) /
+                  std::max(std::fabs(cost_before), std::numeric_limits<double>::epsilon()) <
+              tol) {
+        converged = true;
+        break;
+      }
+    }
+  }
+  store_problem(P, p);
+  if (res) {
+    res->initial_cost = initial_cost;
+    res->final_cost = current_cost;
+    res->converged = converged ? 1u : 0u;
+    res->num_iterations = count;
+    res->initial_nonprojectable = initial_nonproj;
+    res->final_nonprojectable = final_nonproj;
+  }
+  return VLBA_OK;
+}
+
+}  // extern "C"

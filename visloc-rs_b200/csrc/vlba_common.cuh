@@ -1,0 +1,201 @@
+// vlba_common.cuh -- device data layout shared by the kernels and the host.
+//
+// Layout in HBM (one or more problems packed back to back):
+//   poses      f64 quaternion + translation, current and candidate copies, and
+//              a derived f64 (R, t) table per copy (96 B per pose);
+//   points     f64 xyz, current and candidate;
+//   obs        sorted point-major: pose, point, variable-camera slot, camera
+//              model, pixel (f64), and two linearisation records per obs:
+//              H_o = w J_l^T J_l (upper 3x3, f32, plus point index and slot)
+//              and e_o = w J_l^T r (f32);
+//   S          the reduced camera system in dense TB x TB tiles of 6x6 f32
+//              blocks (lower block triangle; diagonal tiles stored full);
+//   vectors    PCG x, r, z, p, q in f32, 6 per variable camera, tile padded.
+//
+// The pose Jacobian of every observation factors as J_p = J_l [I | -[X]x]
+// (right perturbation of T_world->rig, bundle/normal_equations.rs:447-456 and
+// sqrt_qr.rs:990-998), so H_o and e_o carry everything the Schur complement
+// needs: W_o = J_p^T J_l = B^T H_o with B = [I | -[X]x].
+
+#pragma once
+
+#include <vector_types.h>
+
+#include <cstdint>
+
+#include "../../include/visloc_ba_cuda.h"
+
+namespace vlba {
+
+constexpr uint32_t kNone = 0xFFFFFFFFu;
+constexpr int kBlock = 36;             // floats in a 6x6 block
+constexpr uint32_t kSpinLimit = 1u << 24;  // bounded device waits
+
+// Camera of an observation (f64).  R/t is sensor_from_rig (identity for
+// monocular observations).
+struct DevCamera {
+  double fx, fy, cx, cy, k1, k2;
+  double R[9];
+  double t[3];
+  int radial;  // MonoProjection::Radial
+  int rig;     // apply sensor_from_rig
+  int pad[2];
+};
+
+// Per-problem LM settings (BaConfig + PCG controls).
+struct LmParams {
+  double initial_lambda;
+  double lambda_increase_factor;
+  double lambda_decrease_factor;
+  double max_lambda;
+  double min_lambda;
+  double step_tolerance;
+  double cost_tolerance;
+  double relative_cost_tolerance;
+  double robust_parameter;
+  double pcg_relative_tolerance;
+  uint32_t has_initial_lambda;
+  uint32_t has_relative_cost_tolerance;
+  uint32_t robust_kernel;
+  uint32_t max_iterations;
+  uint32_t max_pcg_iterations;
+  uint32_t pad[3];
+};
+
+// Per-problem LM state, owned by the device (k_decide).
+struct Ctrl {
+  double lambda;
+  double current_cost;
+  double initial_cost;
+  double cost_after;
+  double max_pose_step;
+  double max_landmark_step;
+  double pcg_rel_res;
+  double pad_d;
+  unsigned long long current_nonproj;
+  unsigned long long initial_nonproj;
+  unsigned long long nonproj_after;
+  unsigned long long total_pcg;
+  uint32_t iteration;    // LM iterations (trials) performed
+  uint32_t done;
+  uint32_t converged;
+  uint32_t relinearize;  // linearise before the next trial
+  uint32_t cur;          // which state buffer (0/1) holds the current state
+  uint32_t pcg_iters;
+  uint32_t pcg_status;   // 0 converged, 1 iteration cap, 2 breakdown, 3 timeout
+  uint32_t nonfinite;    // the step had a non-finite entry (singular system)
+};
+
+// PCG control words of one problem (written by the PCG kernel).
+struct PcgState {
+  double rz;
+  double bnorm;
+  double rnorm;
+  uint32_t iters;
+  uint32_t status;  // 0 running/converged, 1 cap, 2 breakdown
+  uint32_t active;
+  uint32_t pad;
+};
+
+// Everything the kernels touch.  Passed by value.
+struct Dev {
+  // sizes
+  uint32_t num_problems;
+  uint32_t num_poses;
+  uint32_t num_points;
+  uint32_t num_obs;
+  uint32_t num_var_cams;       // padded slot count (multiple of TB per problem)
+  uint32_t num_tile_rows;
+  uint32_t num_tiles;
+  uint32_t num_offdiag_blocks;
+  uint32_t num_dup_pairs;
+  uint32_t num_point_chunks;
+  uint32_t tb;                  // tile size in blocks
+  uint32_t group;               // lanes per off-diagonal block in assembly
+
+  // problem ranges
+  const uint32_t* prob_pose_begin;   // [num_problems + 1]
+  const uint32_t* prob_point_begin;  // [num_problems + 1]
+  const uint32_t* prob_tr_begin;     // tile rows [num_problems + 1]
+  const uint32_t* prob_chunk_begin;  // point chunks [num_problems + 1]
+  const uint32_t* pose_prob;         // [num_poses]
+  const uint32_t* point_prob;        // [num_points]
+  const uint32_t* slot_prob;         // [num_var_cams]
+  const LmParams* params;            // [num_problems]
+  Ctrl* ctrl;                        // [num_problems]
+  PcgState* pcg;                     // [num_problems]
+  vlba_iteration* records;           // [num_problems * max_records]
+  uint32_t max_records;
+
+  // state: two buffers each; Ctrl::cur selects the current one, the other
+  // receives the candidate of a trial (an accepted step flips cur).
+  double* pose_q[2];    // [4 N] quaternion (w, i, j, k)
+  double* pose_t[2];    // [3 N]
+  double* pose_rt[2];   // [12 N] derived R (row-major) and t
+  double* points[2];    // [3 M]
+  const uint32_t* pose_slot;   // [N] variable slot or kNone
+  const uint8_t* point_var;    // [M] 1 = variable
+  double* pose_step;           // [N] |xi| of the last trial
+
+  // cameras
+  const DevCamera* cameras;
+
+  // observations, point-major
+  const uint32_t* pt_off;      // [M + 1]
+  const uint32_t* obs_pose;    // [K]
+  const uint32_t* obs_cam;     // [K] camera index
+  const uint32_t* obs_slot;    // [K] variable slot of the pose or kNone
+  const double2* obs_xy;       // [K]
+  float4* obs_h;               // [2 K]: {h00,h01,h02,h11} {h12,h22,point,slot}
+  float4* obs_e;               // [K]:   {e0,e1,e2,w}
+
+  // per-camera observation lists (indices into the point-major order)
+  const uint32_t* cam_off;     // [num_var_cams + 1]
+  const uint32_t* cam_obs;
+
+  // per point, per linearisation / per trial
+  float* pt_h;                 // [9 M] H_ll upper (6) + g_l (3)
+  float4* pt_s;                // [4 M] {hinv00,01,02,11} {hinv12,22,X.x,X.y} {X.z,v0,v1,v2} {g0,g1,g2,ok}
+
+  // per camera
+  double* cam_hpp;             // [27 C] H_pp upper 21 + g_p 6 (f64)
+
+  // reduced system
+  float* tiles;                // [num_tiles * tb*tb * 36]
+  const uint32_t* tile_ij;     // [num_tiles] (I << 16) | J
+  const uint32_t* blk_off;     // [num_offdiag_blocks + 1] pair ranges
+  const uint2* pairs;          // (k_i, k_j), sorted by block then point
+  const uint2* blk_dst;        // [num_offdiag_blocks] float offsets (block, mirror or kNone)
+  const uint32_t* diag_dst;    // [num_var_cams] float offset of the diagonal block
+  const uint32_t* dup_off;     // [num_var_cams + 1] same-camera pairs k != k'
+  const uint2* dup_pairs;
+  float* minv;                 // [36 C]
+  float* rhs;                  // [6 C]
+
+  // PCG
+  float* x;
+  float* r;
+  float* z;
+  float* p;
+  float* q;
+  float* partial;              // [num_tiles * 2 * tb * 6]
+  const uint32_t* tr_list_off; // [num_tile_rows + 1]
+  const uint32_t* tr_list;     // partial indices (tile * 2 + side)
+  const uint32_t* tr_prob;     // [num_tile_rows]
+  double* dots;                // [4 * num_tile_rows]
+  unsigned int* barrier;       // [4] grid barrier count, generation; active problems
+  unsigned int* error;         // [1] device error flags
+
+  // reductions
+  const uint32_t* chunk_point_begin;  // [num_point_chunks + 1]
+  double* chunk_cost;
+  unsigned long long* chunk_bad;
+  double* chunk_step;
+};
+
+enum ErrorBits : unsigned int {
+  kErrBarrierTimeout = 1u,
+  kErrTmaTimeout = 2u,
+};
+
+}  // namespace vlba

@@ -1,0 +1,1512 @@
+// vlba_kernels.cu -- the Levenberg-Marquardt step on sm_100a.
+//
+// One LM iteration (trial) of the reference (pipelines/slam/src/bundle/
+// lm.rs:356-1009, GPU twin crates/ba-gpu/src/solver.rs:552-690 with the
+// shaders of crates/ba-gpu/src/shaders/ba.wgsl) is the kernel sequence
+//
+//   k_linearize     per point, after an accepted step: residual, analytic
+//                   Jacobian, robust weight; per-obs H_o, e_o; per-point H_ll,
+//                   g_l                               (ba.wgsl:63-135, 185-204)
+//   k_point_prep    per point: damped 3x3 inverse in FP64, v = H^-1 g
+//                                                      (ba.wgsl:209-243)
+//   k_offdiag       per camera pair: S_ij = -sum W_i H^-1 W_j^T, a segmented
+//                   reduction over the pair's points (no atomics)
+//   k_cam_diag      per camera: S_ii = H_pp + lambda I - sum W H^-1 W^T, the
+//                   reduced rhs and the FP64 6x6 Cholesky block-Jacobi inverse
+//                                                      (ba.wgsl:141-183, 263-387)
+//   k_pcg           persistent: block-Jacobi PCG on S, tiles of S streamed
+//                   HBM -> shared memory by TMA bulk copies (ba.wgsl:420-562)
+//   k_pose_update   T <- T Exp(xi) in FP64             (solver.rs:599-607)
+//   k_cost<true>    back-substitution dl = -H^-1 (g + sum W^T dc), then the
+//                   FP64 robust cost and non-projectable count of the trial
+//                                                      (ba.wgsl:565-586,
+//                                                       solver.rs:696-727)
+//   k_decide        LM accept / reject, lambda schedule and convergence tests
+//                   in FP64 on the device              (solver.rs:629-682,
+//                                                       lm.rs:804-1008)
+//
+// Precision: Jacobians, H_o, Schur blocks and PCG vectors in FP32 (the Schur
+// off-diagonal blocks with compensated FP32 sums); FP64 for the residual, the
+// cost, the 3x3 and 6x6 inverses, the diagonal blocks and the PCG scalars.
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "vlba_kernels.cuh"
+
+namespace vlba {
+namespace {
+
+// ----------------------------------------------------------------- algebra
+// nalgebra UnitQuaternion::to_rotation_matrix (row-major).
+__device__ __forceinline__ void quat_to_matrix(const double* q, double* m) {
+  const double w = q[0], i = q[1], j = q[2], k = q[3];
+  const double ww = w * w, ii = i * i, jj = j * j, kk = k * k;
+  const double ij = i * j * 2.0, wk = w * k * 2.0, wj = w * j * 2.0;
+  const double ik = i * k * 2.0, jk = j * k * 2.0, wi = w * i * 2.0;
+  m[0] = ww + ii - jj - kk;
+  m[1] = ij - wk;
+  m[2] = wj + ik;
+  m[3] = wk + ij;
+  m[4] = ww - ii + jj - kk;
+  m[5] = jk - wi;
+  m[6] = ik - wj;
+  m[7] = wi + jk;
+  m[8] = ww - ii - jj + kk;
+}
+
+// nalgebra UnitQuaternion * Vector3.
+__device__ __forceinline__ void quat_rotate(const double* q, const double* p, double* out) {
+  const double tx = 2.0 * (q[2] * p[2] - q[3] * p[1]);
+  const double ty = 2.0 * (q[3] * p[0] - q[1] * p[2]);
+  const double tz = 2.0 * (q[1] * p[1] - q[2] * p[0]);
+  const double cx = q[2] * tz - q[3] * ty;
+  const double cy = q[3] * tx - q[1] * tz;
+  const double cz = q[1] * ty - q[2] * tx;
+  out[0] = tx * q[0] + cx + p[0];
+  out[1] = ty * q[0] + cy + p[1];
+  out[2] = tz * q[0] + cz + p[2];
+}
+
+__device__ __forceinline__ double robust_weight(uint32_t kind, double p, double s) {
+  if (kind == VLBA_KERNEL_HUBER) return s <= p * p ? 1.0 : p / sqrt(s);
+  if (kind == VLBA_KERNEL_CAUCHY) return 1.0 / (1.0 + s / (p * p));
+  return 1.0;
+}
+
+__device__ __forceinline__ double robust_cost(uint32_t kind, double p, double s) {
+  if (kind == VLBA_KERNEL_HUBER) return s <= p * p ? s : 2.0 * p * sqrt(s) - p * p;
+  if (kind == VLBA_KERNEL_CAUCHY) return p * p * log(1.0 + s / (p * p));
+  return s;
+}
+
+// World point -> sensor frame through pose (R, t) and the camera extrinsic.
+__device__ __forceinline__ void to_sensor(const double* rt, const DevCamera& cam,
+                                          const double* X, double* xs) {
+  double xc[3];
+  for (int a = 0; a < 3; ++a)
+    xc[a] = rt[a * 3] * X[0] + rt[a * 3 + 1] * X[1] + rt[a * 3 + 2] * X[2] + rt[9 + a];
+  if (cam.rig) {
+    for (int a = 0; a < 3; ++a)
+      xs[a] = cam.R[a * 3] * xc[0] + cam.R[a * 3 + 1] * xc[1] + cam.R[a * 3 + 2] * xc[2] +
+              cam.t[a];
+  } else {
+    xs[0] = xc[0];
+    xs[1] = xc[1];
+    xs[2] = xc[2];
+  }
+}
+
+// Camera::project for the radial pinhole family (camera.rs:351-432).
+__device__ __forceinline__ bool camera_project(const DevCamera& c, const double* p,
+                                               double* out) {
+  if (!(isfinite(p[0]) && isfinite(p[1]) && isfinite(p[2]))) return false;
+  if (p[2] <= 0.0) return false;
+  double x = p[0] / p[2];
+  double y = p[1] / p[2];
+  if (c.radial) {
+    const double r2 = x * x + y * y;
+    const double d = 1.0 + c.k1 * r2 + c.k2 * r2 * r2;
+    x *= d;
+    y *= d;
+  }
+  out[0] = c.fx * x + c.cx;
+  out[1] = c.fy * y + c.cy;
+  return true;
+}
+
+// mono_project_with_jacobian (jacobians.rs:63-113); j row-major 2x3.
+__device__ __forceinline__ bool project_jacobian(const DevCamera& c, const double* xc,
+                                                 double* pred, double* j) {
+  if (!(xc[2] > 0.0)) return false;
+  const double z_inv = 1.0 / xc[2];
+  if (!c.radial) {
+    pred[0] = c.fx * xc[0] / xc[2] + c.cx;
+    pred[1] = c.fy * xc[1] / xc[2] + c.cy;
+    j[0] = c.fx * z_inv;
+    j[1] = 0.0;
+    j[2] = -c.fx * xc[0] * z_inv * z_inv;
+    j[3] = 0.0;
+    j[4] = c.fy * z_inv;
+    j[5] = -c.fy * xc[1] * z_inv * z_inv;
+    return isfinite(pred[0]) && isfinite(pred[1]);
+  }
+  const double x = xc[0] / xc[2];
+  const double y = xc[1] / xc[2];
+  const double r2 = x * x + y * y;
+  const double d = 1.0 + c.k1 * r2 + c.k2 * r2 * r2;
+  pred[0] = c.fx * (x * d) + c.cx;
+  pred[1] = c.fy * (y * d) + c.cy;
+  const double g = c.k1 + 2.0 * c.k2 * r2;
+  const double d11 = d + 2.0 * x * x * g;
+  const double d12 = 2.0 * x * y * g;
+  const double d22 = d + 2.0 * y * y * g;
+  j[0] = c.fx * d11 * z_inv;
+  j[1] = c.fx * d12 * z_inv;
+  j[2] = -c.fx * (d11 * x + d12 * y) * z_inv;
+  j[3] = c.fy * d12 * z_inv;
+  j[4] = c.fy * d22 * z_inv;
+  j[5] = -c.fy * (d12 * x + d22 * y) * z_inv;
+  bool ok = isfinite(pred[0]) && isfinite(pred[1]);
+#pragma unroll
+  for (int e = 0; e < 6; ++e) ok = ok && isfinite(j[e]);
+  return ok;
+}
+
+// Upper-triangle index of (r, c), r <= c, in a symmetric 6x6.
+__host__ __device__ constexpr int ut6(int r, int c) { return r * 6 - (r * (r + 1)) / 2 + c; }
+
+// S += sign * B^T K B for symmetric or general 3x3 K and B = [I | -[X]x]:
+// B^T K B = [[K, -K[X]x], [[X]x K, -[X]x K [X]x]]; full 6x6 row-major.
+template <typename T>
+__device__ __forceinline__ void btkb(const T* K, T x, T y, T z, T* out) {
+  // C = K [X]x : row r of C is K_r x X.
+  T C[9];
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    const T k0 = K[r * 3], k1 = K[r * 3 + 1], k2 = K[r * 3 + 2];
+    C[r * 3 + 0] = k1 * z - k2 * y;
+    C[r * 3 + 1] = k2 * x - k0 * z;
+    C[r * 3 + 2] = k0 * y - k1 * x;
+  }
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      out[r * 6 + c] = K[r * 3 + c];
+      out[r * 6 + 3 + c] = -C[r * 3 + c];
+    }
+  // [X]x K (column c is X x K_c) and [X]x C.
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const T k0 = K[c], k1 = K[3 + c], k2 = K[6 + c];
+    out[18 + c] = y * k2 - z * k1;
+    out[24 + c] = z * k0 - x * k2;
+    out[30 + c] = x * k1 - y * k0;
+    const T c0 = C[c], c1 = C[3 + c], c2 = C[6 + c];
+    out[18 + 3 + c] = -(y * c2 - z * c1);
+    out[24 + 3 + c] = -(z * c0 - x * c2);
+    out[30 + 3 + c] = -(x * c1 - y * c0);
+  }
+}
+
+// Fixed-order block reductions (deterministic for a given block size).
+template <typename T, int N>
+__device__ __forceinline__ T block_sum(T v, T* red) {
+  red[threadIdx.x] = v;
+  __syncthreads();
+#pragma unroll
+  for (int s = N / 2; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+    __syncthreads();
+  }
+  const T out = red[0];
+  __syncthreads();
+  return out;
+}
+
+template <int N>
+__device__ __forceinline__ double block_max(double v, double* red) {
+  red[threadIdx.x] = v;
+  __syncthreads();
+#pragma unroll
+  for (int s = N / 2; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + s]);
+    __syncthreads();
+  }
+  const double out = red[0];
+  __syncthreads();
+  return out;
+}
+
+// 6x6 SPD inverse by Cholesky in FP64; false if not positive definite.
+__device__ bool chol_inverse6(const double* a, double* inv) {
+  double L[36];
+#pragma unroll
+  for (int e = 0; e < 36; ++e) L[e] = a[e];
+  for (int j = 0; j < 6; ++j) {
+    double s = L[j * 6 + j];
+    for (int q = 0; q < j; ++q) s -= L[j * 6 + q] * L[j * 6 + q];
+    if (!(s > 0.0) || !isfinite(s)) return false;
+    const double ljj = sqrt(s);
+    L[j * 6 + j] = ljj;
+    for (int i = j + 1; i < 6; ++i) {
+      double t = L[i * 6 + j];
+      for (int q = 0; q < j; ++q) t -= L[i * 6 + q] * L[j * 6 + q];
+      L[i * 6 + j] = t / ljj;
+    }
+  }
+  for (int c = 0; c < 6; ++c) {
+    double y[6];
+    for (int i = 0; i < 6; ++i) {
+      double s = (i == c) ? 1.0 : 0.0;
+      for (int q = 0; q < i; ++q) s -= L[i * 6 + q] * y[q];
+      y[i] = s / L[i * 6 + i];
+    }
+    for (int ii = 5; ii >= 0; --ii) {
+      double s = y[ii];
+      for (int q = ii + 1; q < 6; ++q) s -= L[q * 6 + ii] * inv[q * 6 + c];
+      inv[ii * 6 + c] = s / L[ii * 6 + ii];
+    }
+  }
+  return true;
+}
+
+// ------------------------------------------------------------ pose table
+__global__ void __launch_bounds__(256) k_pose_table(Dev d) {
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < d.num_poses;
+       p += gridDim.x * blockDim.x) {
+    const uint32_t cur = d.ctrl[d.pose_prob[p]].cur;
+    double q[4], m[9];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) q[a] = d.pose_q[cur][4 * p + a];
+    quat_to_matrix(q, m);
+    double* rt = d.pose_rt[cur] + 12 * (size_t)p;
+#pragma unroll
+    for (int a = 0; a < 9; ++a) rt[a] = m[a];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) rt[9 + a] = d.pose_t[cur][3 * p + a];
+  }
+}
+
+// ------------------------------------------------------------- linearize
+// One thread per point, its observations contiguous (point-major order).
+__global__ void __launch_bounds__(256) k_linearize(Dev d) {
+  for (uint32_t l = blockIdx.x * blockDim.x + threadIdx.x; l < d.num_points;
+       l += gridDim.x * blockDim.x) {
+    const uint32_t P = d.point_prob[l];
+    const Ctrl& c = d.ctrl[P];
+    if (c.done || !c.relinearize) continue;
+    const uint32_t cur = c.cur;
+    const LmParams& lp = d.params[P];
+    double X[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) X[a] = d.points[cur][3 * (size_t)l + a];
+    double hl[6] = {0, 0, 0, 0, 0, 0}, gl[3] = {0, 0, 0};
+    const uint32_t k0 = d.pt_off[l], k1 = d.pt_off[l + 1];
+    for (uint32_t k = k0; k < k1; ++k) {
+      const uint32_t pose = d.obs_pose[k];
+      const DevCamera& cam = d.cameras[d.obs_cam[k]];
+      const double* rt = d.pose_rt[cur] + 12 * (size_t)pose;
+      double xs[3], pred[2], jpi[6];
+      to_sensor(rt, cam, X, xs);
+      float h[6] = {0, 0, 0, 0, 0, 0}, e[3] = {0, 0, 0};
+      float wf = 0.0f;
+      if (project_jacobian(cam, xs, pred, jpi)) {
+        const double2 xy = d.obs_xy[k];
+        const double rx = pred[0] - xy.x, ry = pred[1] - xy.y;
+        const double w = robust_weight(lp.robust_kernel, lp.robust_parameter, rx * rx + ry * ry);
+        // Effective rotation world -> sensor.
+        double Re[9];
+        if (cam.rig) {
+          for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b)
+              Re[a * 3 + b] = cam.R[a * 3] * rt[b] + cam.R[a * 3 + 1] * rt[3 + b] +
+                              cam.R[a * 3 + 2] * rt[6 + b];
+        } else {
+#pragma unroll
+          for (int a = 0; a < 9; ++a) Re[a] = rt[a];
+        }
+        // J_l = J_pi R (2x3), FP32.
+        float jl[6];
+#pragma unroll
+        for (int a = 0; a < 2; ++a)
+#pragma unroll
+          for (int b = 0; b < 3; ++b)
+            jl[a * 3 + b] = (float)(jpi[a * 3] * Re[b] + jpi[a * 3 + 1] * Re[3 + b] +
+                                    jpi[a * 3 + 2] * Re[6 + b]);
+        wf = (float)w;
+        const float r0 = (float)rx, r1 = (float)ry;
+        h[0] = wf * (jl[0] * jl[0] + jl[3] * jl[3]);
+        h[1] = wf * (jl[0] * jl[1] + jl[3] * jl[4]);
+        h[2] = wf * (jl[0] * jl[2] + jl[3] * jl[5]);
+        h[3] = wf * (jl[1] * jl[1] + jl[4] * jl[4]);
+        h[4] = wf * (jl[1] * jl[2] + jl[4] * jl[5]);
+        h[5] = wf * (jl[2] * jl[2] + jl[5] * jl[5]);
+        e[0] = wf * (jl[0] * r0 + jl[3] * r1);
+        e[1] = wf * (jl[1] * r0 + jl[4] * r1);
+        e[2] = wf * (jl[2] * r0 + jl[5] * r1);
+      }
+      d.obs_h[2 * (size_t)k] = make_float4(h[0], h[1], h[2], h[3]);
+      d.obs_h[2 * (size_t)k + 1] =
+          make_float4(h[4], h[5], __uint_as_float(l), __uint_as_float(d.obs_slot[k]));
+      d.obs_e[k] = make_float4(e[0], e[1], e[2], wf);
+#pragma unroll
+      for (int a = 0; a < 6; ++a) hl[a] += h[a];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) gl[a] += e[a];
+    }
+    float* ph = d.pt_h + 9 * (size_t)l;
+#pragma unroll
+    for (int a = 0; a < 6; ++a) ph[a] = (float)hl[a];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) ph[6 + a] = (float)gl[a];
+  }
+}
+
+// ------------------------------------------------------------ point prep
+// Damped landmark inverse (FP64 cofactors, nalgebra Matrix3::try_inverse:
+// singular iff det == 0) and v = H^-1 g.  A singular or fixed point gets a
+// zero inverse, which drops it from the reduced system and back-substitution
+// exactly as the reference's `continue` does (normal_equations.rs:1662-1668).
+__global__ void __launch_bounds__(256) k_point_prep(Dev d) {
+  for (uint32_t l = blockIdx.x * blockDim.x + threadIdx.x; l < d.num_points;
+       l += gridDim.x * blockDim.x) {
+    const uint32_t P = d.point_prob[l];
+    const Ctrl& c = d.ctrl[P];
+    if (c.done) continue;
+    const uint32_t cur = c.cur;
+    const double lambda = c.lambda;
+    const float X0 = (float)d.points[cur][3 * (size_t)l];
+    const float X1 = (float)d.points[cur][3 * (size_t)l + 1];
+    const float X2 = (float)d.points[cur][3 * (size_t)l + 2];
+    double inv[6] = {0, 0, 0, 0, 0, 0}, v[3] = {0, 0, 0}, g[3] = {0, 0, 0};
+    float ok = 0.0f;
+    if (d.point_var[l]) {
+      const float* ph = d.pt_h + 9 * (size_t)l;
+      double a = ph[0], b = ph[1], cc = ph[2], dd = ph[3], e = ph[4], f = ph[5];
+      g[0] = ph[6];
+      g[1] = ph[7];
+      g[2] = ph[8];
+      if (lambda > 0.0) {
+        a += lambda;
+        dd += lambda;
+        f += lambda;
+      }
+      // Symmetric [[a b c] [b d e] [c e f]].
+      const double m22 = dd * f - e * e;   // minor (1,1)-(2,2)
+      const double m12 = b * f - e * cc;   // minor rows 1,2 cols 0,2
+      const double m11 = b * e - dd * cc;  // minor rows 1,2 cols 0,1
+      const double det = a * m22 - b * m12 + cc * m11;
+      if (det != 0.0 && isfinite(det)) {
+        inv[0] = m22 / det;
+        inv[1] = (cc * e - f * b) / det;
+        inv[2] = (b * e - dd * cc) / det;
+        inv[3] = (a * f - cc * cc) / det;
+        inv[4] = (cc * b - e * a) / det;
+        inv[5] = (a * dd - b * b) / det;
+        v[0] = inv[0] * g[0] + inv[1] * g[1] + inv[2] * g[2];
+        v[1] = inv[1] * g[0] + inv[3] * g[1] + inv[4] * g[2];
+        v[2] = inv[2] * g[0] + inv[4] * g[1] + inv[5] * g[2];
+        ok = 1.0f;
+      }
+    }
+    float4* ps = d.pt_s + 4 * (size_t)l;
+    ps[0] = make_float4((float)inv[0], (float)inv[1], (float)inv[2], (float)inv[3]);
+    ps[1] = make_float4((float)inv[4], (float)inv[5], X0, X1);
+    ps[2] = make_float4(X2, (float)v[0], (float)v[1], (float)v[2]);
+    ps[3] = make_float4((float)g[0], (float)g[1], (float)g[2], ok);
+  }
+}
+
+// ------------------------------------------------- off-diagonal Schur blocks
+// One group of G lanes per camera pair (i, j), i > j: lanes stride the pair's
+// points in order, each accumulating -B^T H_i H^-1 H_j B with compensated
+// (Kahan) FP32 sums, then a fixed butterfly over the group.  Deterministic,
+// no atomics; the destination is the block's slot in its dense tile (and the
+// mirrored slot inside a diagonal tile).
+template <int G>
+__global__ void __launch_bounds__(256) k_offdiag(Dev d) {
+  constexpr int kPerWarp = 32 / G;
+  const uint32_t lane = threadIdx.x % G;
+  const uint32_t warp_global = (blockIdx.x * blockDim.x + threadIdx.x) / 32;
+  const uint32_t warps_total = gridDim.x * blockDim.x / 32;
+  const uint32_t tile_floats = d.tb * d.tb * kBlock;
+  const uint32_t nwb = (d.num_offdiag_blocks + kPerWarp - 1) / kPerWarp;
+  for (uint32_t wb = warp_global; wb < nwb; wb += warps_total) {
+    const uint32_t b = wb * kPerWarp + (threadIdx.x % 32) / G;
+    bool valid = b < d.num_offdiag_blocks;
+    uint2 dst = make_uint2(kNone, kNone);
+    uint32_t c0 = 0, c1 = 0;
+    if (valid) {
+      dst = d.blk_dst[b];
+      const uint32_t tile = dst.x / tile_floats;
+      const uint32_t I = d.tile_ij[tile] >> 16;
+      valid = !d.ctrl[d.tr_prob[I]].done;
+      c0 = d.blk_off[b];
+      c1 = d.blk_off[b + 1];
+    }
+    float acc[36], cmp[36];
+#pragma unroll
+    for (int e = 0; e < 36; ++e) {
+      acc[e] = 0.0f;
+      cmp[e] = 0.0f;
+    }
+    if (valid) {
+      for (uint32_t cidx = c0 + lane; cidx < c1; cidx += G) {
+        const uint2 pr = d.pairs[cidx];
+        const float4 a0 = d.obs_h[2 * (size_t)pr.x], a1 = d.obs_h[2 * (size_t)pr.x + 1];
+        const float4 b0 = d.obs_h[2 * (size_t)pr.y], b1 = d.obs_h[2 * (size_t)pr.y + 1];
+        const uint32_t l = __float_as_uint(a1.z);
+        const float4 s0 = d.pt_s[4 * (size_t)l], s1 = d.pt_s[4 * (size_t)l + 1],
+                     s2 = d.pt_s[4 * (size_t)l + 2];
+        const float Hi[9] = {a0.x, a0.y, a0.z, a0.y, a0.w, a1.x, a0.z, a1.x, a1.y};
+        const float Hj[9] = {b0.x, b0.y, b0.z, b0.y, b0.w, b1.x, b0.z, b1.x, b1.y};
+        const float Mi[9] = {s0.x, s0.y, s0.z, s0.y, s0.w, s1.x, s0.z, s1.x, s1.y};
+        float M[9], K[9];
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+          for (int cc = 0; cc < 3; ++cc)
+            M[r * 3 + cc] = Mi[r * 3] * Hj[cc] + Mi[r * 3 + 1] * Hj[3 + cc] +
+                            Mi[r * 3 + 2] * Hj[6 + cc];
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+          for (int cc = 0; cc < 3; ++cc)
+            K[r * 3 + cc] = Hi[r * 3] * M[cc] + Hi[r * 3 + 1] * M[3 + cc] +
+                            Hi[r * 3 + 2] * M[6 + cc];
+        float blk[36];
+        btkb<float>(K, s1.z, s1.w, s2.x, blk);
+#pragma unroll
+        for (int e = 0; e < 36; ++e) {  // acc -= blk, Kahan compensated
+          const float y = -blk[e] - cmp[e];
+          const float t = acc[e] + y;
+          cmp[e] = (t - acc[e]) - y;
+          acc[e] = t;
+        }
+      }
+    }
+#pragma unroll
+    for (int off = G / 2; off > 0; off >>= 1)
+#pragma unroll
+      for (int e = 0; e < 36; ++e) acc[e] += __shfl_xor_sync(0xffffffffu, acc[e], off, G);
+    if (valid) {
+#pragma unroll
+      for (int e = 0; e < 36; ++e) {
+        if ((uint32_t)(e % G) == lane) {
+          d.tiles[dst.x + e] = acc[e];
+          if (dst.y != kNone) d.tiles[dst.y + (e % 6) * 6 + e / 6] = acc[e];
+        }
+      }
+    }
+  }
+}
+
+// acc[ut6(r,c)] += sign * (B^T K B)[r][c] for r <= c (K general 3x3).
+__device__ __forceinline__ void add_btkb_upper(const double* K, double x, double y, double z,
+                                               double* acc, double sign) {
+  double C[9];  // C = K [X]x, row r = K_r x X
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    const double k0 = K[r * 3], k1 = K[r * 3 + 1], k2 = K[r * 3 + 2];
+    C[r * 3 + 0] = k1 * z - k2 * y;
+    C[r * 3 + 1] = k2 * x - k0 * z;
+    C[r * 3 + 2] = k0 * y - k1 * x;
+  }
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+#pragma unroll
+    for (int c = r; c < 3; ++c) acc[ut6(r, c)] += sign * K[r * 3 + c];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) acc[ut6(r, 3 + c)] -= sign * C[r * 3 + c];
+  }
+  // Bottom-right -[X]x C: column c is -(X x C_c).
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const double c0 = C[c], c1 = C[3 + c], c2 = C[6 + c];
+    const double b0 = -(y * c2 - z * c1), b1 = -(z * c0 - x * c2), b2 = -(x * c1 - y * c0);
+    if (0 <= c) acc[ut6(3, 3 + c)] += sign * b0;
+    if (1 <= c) acc[ut6(4, 3 + c)] += sign * b1;
+    if (2 <= c) acc[ut6(5, 3 + c)] += sign * b2;
+  }
+}
+
+__device__ __forceinline__ double quad3(const double* H, double a, double b, double c) {
+  return a * (H[0] * a + H[1] * b + H[2] * c) + b * (H[3] * a + H[4] * b + H[5] * c) +
+         c * (H[6] * a + H[7] * b + H[8] * c);
+}
+
+// --------------------------------------------------- camera diagonal blocks
+// One block of 128 threads per variable camera: FP64 sums of
+//   S_ii = sum_o B^T (H_o - H_o H^-1 H_o) B + lambda I   (H_pp minus Schur)
+//   b_i  = sum_o B^T (H_o v - e_o)                        (-g_p + sum W v)
+// then the FP64 Cholesky inverse of S_ii as the block-Jacobi preconditioner
+// (ba.wgsl:263-387; fallback to the inverse damped diagonal, ba.wgsl:375-383).
+constexpr int kDiagThreads = 128;
+constexpr int kDiagAcc = 33;  // 21 upper S, 6 rhs, 6 diag(H_pp)
+
+__global__ void __launch_bounds__(kDiagThreads) k_cam_diag(Dev d) {
+  __shared__ double red[(kDiagThreads / 32) * kDiagAcc];
+  __shared__ double tot[kDiagAcc];
+  for (uint32_t s = blockIdx.x; s < d.num_var_cams; s += gridDim.x) {
+    const uint32_t P = d.slot_prob[s];
+    if (d.ctrl[P].done) continue;
+    const double lambda = d.ctrl[P].lambda;
+    double acc[kDiagAcc];
+#pragma unroll
+    for (int e = 0; e < kDiagAcc; ++e) acc[e] = 0.0;
+    const uint32_t o0 = d.cam_off[s], o1 = d.cam_off[s + 1];
+    for (uint32_t idx = o0 + threadIdx.x; idx < o1; idx += kDiagThreads) {
+      const uint32_t k = d.cam_obs[idx];
+      const float4 h0 = d.obs_h[2 * (size_t)k], h1 = d.obs_h[2 * (size_t)k + 1];
+      const float4 ev = d.obs_e[k];
+      const uint32_t l = __float_as_uint(h1.z);
+      const float4 s0 = d.pt_s[4 * (size_t)l], s1 = d.pt_s[4 * (size_t)l + 1],
+                   s2 = d.pt_s[4 * (size_t)l + 2], s3 = d.pt_s[4 * (size_t)l + 3];
+      const double H[9] = {h0.x, h0.y, h0.z, h0.y, h0.w, h1.x, h0.z, h1.x, h1.y};
+      const double X = s1.z, Y = s1.w, Z = s2.x;
+      double K[9], u[3];
+      const bool ok = s3.w != 0.0f;
+      if (ok) {
+        const double Mi[9] = {s0.x, s0.y, s0.z, s0.y, s0.w, s1.x, s0.z, s1.x, s1.y};
+        double M[9];
+        for (int r = 0; r < 3; ++r)
+          for (int cc = 0; cc < 3; ++cc)
+            M[r * 3 + cc] = Mi[r * 3] * H[cc] + Mi[r * 3 + 1] * H[3 + cc] + Mi[r * 3 + 2] * H[6 + cc];
+        for (int r = 0; r < 3; ++r)
+          for (int cc = 0; cc < 3; ++cc)
+            K[r * 3 + cc] = H[r * 3 + cc] - (H[r * 3] * M[cc] + H[r * 3 + 1] * M[3 + cc] +
+                                             H[r * 3 + 2] * M[6 + cc]);
+        const double v0 = s2.y, v1 = s2.z, v2 = s2.w;
+        u[0] = H[0] * v0 + H[1] * v1 + H[2] * v2 - ev.x;
+        u[1] = H[3] * v0 + H[4] * v1 + H[5] * v2 - ev.y;
+        u[2] = H[6] * v0 + H[7] * v1 + H[8] * v2 - ev.z;
+      } else {
+        for (int e = 0; e < 9; ++e) K[e] = H[e];
+        u[0] = -(double)ev.x;
+        u[1] = -(double)ev.y;
+        u[2] = -(double)ev.z;
+      }
+      add_btkb_upper(K, X, Y, Z, acc, 1.0);
+      acc[21] += u[0];
+      acc[22] += u[1];
+      acc[23] += u[2];
+      acc[24] += Y * u[2] - Z * u[1];
+      acc[25] += Z * u[0] - X * u[2];
+      acc[26] += X * u[1] - Y * u[0];
+      // diag(B^T H B) for the fallback preconditioner: H_aa, then the
+      // quadratic forms (X x e_a)^T H (X x e_a).
+      acc[27] += H[0];
+      acc[28] += H[4];
+      acc[29] += H[8];
+      acc[30] += quad3(H, 0.0, Z, -Y);
+      acc[31] += quad3(H, -Z, 0.0, X);
+      acc[32] += quad3(H, Y, -X, 0.0);
+    }
+    // Same-camera pairs k != k' of one point (a point observed twice by a
+    // camera): -B^T H_k H^-1 H_k' B, both orders listed.
+    for (uint32_t idx = d.dup_off[s] + threadIdx.x; idx < d.dup_off[s + 1];
+         idx += kDiagThreads) {
+      const uint2 pr = d.dup_pairs[idx];
+      const float4 a0 = d.obs_h[2 * (size_t)pr.x], a1 = d.obs_h[2 * (size_t)pr.x + 1];
+      const float4 b0 = d.obs_h[2 * (size_t)pr.y], b1 = d.obs_h[2 * (size_t)pr.y + 1];
+      const uint32_t l = __float_as_uint(a1.z);
+      const float4 s0 = d.pt_s[4 * (size_t)l], s1 = d.pt_s[4 * (size_t)l + 1],
+                   s2 = d.pt_s[4 * (size_t)l + 2];
+      const double Hi[9] = {a0.x, a0.y, a0.z, a0.y, a0.w, a1.x, a0.z, a1.x, a1.y};
+      const double Hj[9] = {b0.x, b0.y, b0.z, b0.y, b0.w, b1.x, b0.z, b1.x, b1.y};
+      const double Mi[9] = {s0.x, s0.y, s0.z, s0.y, s0.w, s1.x, s0.z, s1.x, s1.y};
+      double M[9], K[9];
+      for (int r = 0; r < 3; ++r)
+        for (int cc = 0; cc < 3; ++cc)
+          M[r * 3 + cc] = Mi[r * 3] * Hj[cc] + Mi[r * 3 + 1] * Hj[3 + cc] + Mi[r * 3 + 2] * Hj[6 + cc];
+      for (int r = 0; r < 3; ++r)
+        for (int cc = 0; cc < 3; ++cc)
+          K[r * 3 + cc] = Hi[r * 3] * M[cc] + Hi[r * 3 + 1] * M[3 + cc] + Hi[r * 3 + 2] * M[6 + cc];
+      add_btkb_upper(K, (double)s1.z, (double)s1.w, (double)s2.x, acc, -1.0);
+    }
+    // Fixed-order reduction: butterfly within each warp, then the warps'
+    // sums in warp order.
+#pragma unroll
+    for (int e = 0; e < kDiagAcc; ++e) {
+      double v = acc[e];
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+      acc[e] = v;
+    }
+    const int warp = threadIdx.x / 32;
+    if ((threadIdx.x % 32) == 0) {
+#pragma unroll
+      for (int e = 0; e < kDiagAcc; ++e) red[warp * kDiagAcc + e] = acc[e];
+    }
+    __syncthreads();
+    if (threadIdx.x < (unsigned)kDiagAcc) {
+      double t = 0.0;
+      for (int w = 0; w < kDiagThreads / 32; ++w) t += red[w * kDiagAcc + threadIdx.x];
+      tot[threadIdx.x] = t;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double S[36], inv[36];
+      for (int r = 0; r < 6; ++r)
+        for (int cc = 0; cc < 6; ++cc) {
+          double v = r <= cc ? tot[ut6(r, cc)] : tot[ut6(cc, r)];
+          if (r == cc && lambda > 0.0) v += lambda;
+          S[r * 6 + cc] = v;
+        }
+      float* blk = d.tiles + d.diag_dst[s];
+      for (int e = 0; e < 36; ++e) blk[e] = (float)S[e];
+      for (int a = 0; a < 6; ++a) d.rhs[6 * (size_t)s + a] = (float)tot[21 + a];
+      if (!chol_inverse6(S, inv)) {
+        for (int e = 0; e < 36; ++e) inv[e] = 0.0;
+        for (int a = 0; a < 6; ++a) inv[a * 7] = 1.0 / fmax(tot[27 + a] + lambda, 1e-20);
+      }
+      for (int e = 0; e < 36; ++e) d.minv[36 * (size_t)s + e] = (float)inv[e];
+    }
+    __syncthreads();
+  }
+}
+
+// ------------------------------------------------------------- pose update
+// T' = T * Exp(xi) in FP64 (SE3::exp + compose, se3.rs:32-37,72-82,109-121).
+__global__ void __launch_bounds__(256) k_pose_update(Dev d) {
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < d.num_poses;
+       p += gridDim.x * blockDim.x) {
+    const uint32_t P = d.pose_prob[p];
+    Ctrl& c = d.ctrl[P];
+    if (c.done) continue;
+    const uint32_t cur = c.cur, nxt = cur ^ 1u;
+    double q[4], t[3];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) q[a] = d.pose_q[cur][4 * (size_t)p + a];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) t[a] = d.pose_t[cur][3 * (size_t)p + a];
+    double step = 0.0;
+    const uint32_t slot = d.pose_slot[p];
+    if (slot != kNone) {
+      double xi[6];
+      double nn = 0.0;
+#pragma unroll
+      for (int a = 0; a < 6; ++a) {
+        xi[a] = (double)d.x[6 * (size_t)slot + a];
+        nn += xi[a] * xi[a];
+      }
+      step = sqrt(nn);
+      if (!isfinite(step)) c.nonfinite = 1u;
+      // Exp: rotation = exp(omega / 2) as a quaternion (nalgebra
+      // from_scaled_axis), translation = V(omega) rho.
+      const double hx = xi[3] / 2.0, hy = xi[4] / 2.0, hz = xi[5] / 2.0;
+      const double hn = hx * hx + hy * hy + hz * hz;
+      double qe[4] = {1.0, 0.0, 0.0, 0.0};
+      const double eps = 2.220446049250313e-16;
+      if (hn > eps * eps) {
+        const double n = sqrt(hn);
+        const double sn = sin(n) / n;
+        qe[0] = cos(n);
+        qe[1] = hx * sn;
+        qe[2] = hy * sn;
+        qe[3] = hz * sn;
+      }
+      const double wx = xi[3], wy = xi[4], wz = xi[5];
+      const double th2 = wx * wx + wy * wy + wz * wz;
+      double ca, cb;
+      if (th2 < 1e-10) {
+        ca = 0.5;
+        cb = 1.0 / 6.0;
+      } else {
+        const double th = sqrt(th2);
+        ca = (1.0 - cos(th)) / th2;
+        cb = (th - sin(th)) / (th * th2);
+      }
+      const double S[9] = {0.0, -wz, wy, wz, 0.0, -wx, -wy, wx, 0.0};
+      double te[3];
+      for (int a = 0; a < 3; ++a) {
+        double v = 0.0;
+        for (int b = 0; b < 3; ++b) {
+          double s2 = 0.0;
+          for (int k = 0; k < 3; ++k) s2 += S[a * 3 + k] * S[k * 3 + b];
+          const double vab = (a == b ? 1.0 : 0.0) + ca * S[a * 3 + b] + cb * s2;
+          v += vab * xi[b];
+        }
+        te[a] = v;
+      }
+      const double nq[4] = {q[0] * qe[0] - q[1] * qe[1] - q[2] * qe[2] - q[3] * qe[3],
+                            q[0] * qe[1] + q[1] * qe[0] + q[2] * qe[3] - q[3] * qe[2],
+                            q[0] * qe[2] - q[1] * qe[3] + q[2] * qe[0] + q[3] * qe[1],
+                            q[0] * qe[3] + q[1] * qe[2] - q[2] * qe[1] + q[3] * qe[0]};
+      double rte[3];
+      quat_rotate(q, te, rte);
+      for (int a = 0; a < 3; ++a) t[a] = rte[a] + t[a];
+      for (int a = 0; a < 4; ++a) q[a] = nq[a];
+    }
+    d.pose_step[p] = step;
+    double m[9];
+    quat_to_matrix(q, m);
+    double* rt = d.pose_rt[nxt] + 12 * (size_t)p;
+#pragma unroll
+    for (int a = 0; a < 9; ++a) rt[a] = m[a];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) d.pose_q[nxt][4 * (size_t)p + a] = q[a];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      d.pose_t[nxt][3 * (size_t)p + a] = t[a];
+      rt[9 + a] = t[a];
+    }
+  }
+}
+
+// ------------------------------------------------- back-substitution + cost
+// One block of 256 threads per chunk of points of one problem.  TRIAL: the
+// landmark step dl = -H^-1 (g + sum_o H_o (rho + omega x X)) of every
+// variable point (W_o^T dc = H_o B dc), the candidate point X + dl, and the
+// cost at the candidate poses/points.  !TRIAL: the cost of the current state.
+template <bool TRIAL>
+__global__ void __launch_bounds__(256) k_cost(Dev d) {
+  __shared__ double red[256];
+  __shared__ unsigned long long redu[256];
+  for (uint32_t ch = blockIdx.x; ch < d.num_point_chunks; ch += gridDim.x) {
+    const uint32_t lo = d.chunk_point_begin[ch], hi = d.chunk_point_begin[ch + 1];
+    const uint32_t P = d.point_prob[lo];
+    const Ctrl& c = d.ctrl[P];
+    if (c.done) continue;  // uniform: a chunk lies inside one problem
+    const uint32_t cur = c.cur;
+    const uint32_t pose_buf = TRIAL ? (cur ^ 1u) : cur;
+    const LmParams& lp = d.params[P];
+    double cost = 0.0, step = 0.0;
+    unsigned long long bad = 0;
+    for (uint32_t l = lo + threadIdx.x; l < hi; l += blockDim.x) {
+      double X[3];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) X[a] = d.points[cur][3 * (size_t)l + a];
+      const uint32_t k0 = d.pt_off[l], k1 = d.pt_off[l + 1];
+      if (TRIAL) {
+        const float4 s0 = d.pt_s[4 * (size_t)l], s1 = d.pt_s[4 * (size_t)l + 1],
+                     s2 = d.pt_s[4 * (size_t)l + 2], s3 = d.pt_s[4 * (size_t)l + 3];
+        if (d.point_var[l] && s3.w != 0.0f) {
+          const float x = s1.z, y = s1.w, z = s2.x;
+          float u0 = s3.x, u1 = s3.y, u2 = s3.z;
+          for (uint32_t k = k0; k < k1; ++k) {
+            const uint32_t slot = d.obs_slot[k];
+            if (slot == kNone) continue;
+            const float* dc = d.x + 6 * (size_t)slot;
+            const float w0 = dc[3], w1 = dc[4], w2 = dc[5];
+            const float b0 = dc[0] + (w1 * z - w2 * y);
+            const float b1 = dc[1] + (w2 * x - w0 * z);
+            const float b2 = dc[2] + (w0 * y - w1 * x);
+            const float4 h0 = d.obs_h[2 * (size_t)k], h1 = d.obs_h[2 * (size_t)k + 1];
+            u0 += h0.x * b0 + h0.y * b1 + h0.z * b2;
+            u1 += h0.y * b0 + h0.w * b1 + h1.x * b2;
+            u2 += h0.z * b0 + h1.x * b1 + h1.y * b2;
+          }
+          const float dl0 = -(s0.x * u0 + s0.y * u1 + s0.z * u2);
+          const float dl1 = -(s0.y * u0 + s0.w * u1 + s1.x * u2);
+          const float dl2 = -(s0.z * u0 + s1.x * u1 + s1.y * u2);
+          const double e0 = dl0, e1 = dl1, e2 = dl2;
+          step = fmax(step, sqrt(e0 * e0 + e1 * e1 + e2 * e2));
+          X[0] += e0;
+          X[1] += e1;
+          X[2] += e2;
+        }
+#pragma unroll
+        for (int a = 0; a < 3; ++a) d.points[cur ^ 1u][3 * (size_t)l + a] = X[a];
+      }
+      for (uint32_t k = k0; k < k1; ++k) {
+        const DevCamera& cam = d.cameras[d.obs_cam[k]];
+        const double* rt = d.pose_rt[pose_buf] + 12 * (size_t)d.obs_pose[k];
+        double xs[3], pred[2];
+        to_sensor(rt, cam, X, xs);
+        if (!(xs[2] > 0.0) || !camera_project(cam, xs, pred)) {
+          ++bad;
+          continue;
+        }
+        const double2 xy = d.obs_xy[k];
+        const double rx = pred[0] - xy.x, ry = pred[1] - xy.y;
+        cost += robust_cost(lp.robust_kernel, lp.robust_parameter, rx * rx + ry * ry);
+      }
+    }
+    const double tc = block_sum<double, 256>(cost, red);
+    const unsigned long long tb = block_sum<unsigned long long, 256>(bad, redu);
+    const double ts = block_max<256>(step, red);
+    if (threadIdx.x == 0) {
+      d.chunk_cost[ch] = tc;
+      d.chunk_bad[ch] = tb;
+      d.chunk_step[ch] = ts;
+    }
+  }
+}
+
+// ------------------------------------------------------------------ decide
+// The reference LM control per problem (solver.rs:629-682 / lm.rs:
+// 608-663, 804-1008): accept iff the cost decreased (or unconditionally
+// without initial_lambda) and the non-projectable count did not grow; lambda
+// x10 / x0.1 clamped; convergence on step, absolute and relative cost change.
+// A non-finite step is the reference's SingularSystem: lambda up, no step.
+template <bool INIT>
+__global__ void __launch_bounds__(256) k_decide(Dev d) {
+  __shared__ double red[256];
+  __shared__ unsigned long long redu[256];
+  const uint32_t P = blockIdx.x;
+  if (P >= d.num_problems) return;
+  Ctrl& c = d.ctrl[P];
+  if (c.done) return;
+  const LmParams& lp = d.params[P];
+  double cost = 0.0, lstep = 0.0, pstep = 0.0;
+  unsigned long long bad = 0;
+  for (uint32_t ch = d.prob_chunk_begin[P] + threadIdx.x; ch < d.prob_chunk_begin[P + 1];
+       ch += blockDim.x) {
+    cost += d.chunk_cost[ch];
+    bad += d.chunk_bad[ch];
+    lstep = fmax(lstep, d.chunk_step[ch]);
+  }
+  if (!INIT)
+    for (uint32_t p = d.prob_pose_begin[P] + threadIdx.x; p < d.prob_pose_begin[P + 1];
+         p += blockDim.x)
+      pstep = fmax(pstep, d.pose_step[p]);
+  cost = block_sum<double, 256>(cost, red);
+  bad = block_sum<unsigned long long, 256>(bad, redu);
+  lstep = block_max<256>(lstep, red);
+  pstep = block_max<256>(pstep, red);
+  if (threadIdx.x != 0) return;
+  if (INIT) {
+    c.initial_cost = cost;
+    c.current_cost = cost;
+    c.initial_nonproj = bad;
+    c.current_nonproj = bad;
+    c.lambda = lp.has_initial_lambda ? lp.initial_lambda : 0.0;
+    c.relinearize = 1u;
+    c.iteration = 0u;
+    c.converged = 0u;
+    c.nonfinite = 0u;
+    c.total_pcg = 0ull;
+    if (lp.max_iterations == 0) c.done = 1u;
+    return;
+  }
+  const uint32_t it = c.iteration;
+  const PcgState& pg = d.pcg[P];
+  vlba_iteration rec;
+  rec.iteration = it;
+  rec.cost_before = c.current_cost;
+  rec.pcg_iterations = pg.iters;
+  rec.pcg_relative_residual = pg.bnorm > 0.0 ? pg.rnorm / pg.bnorm : 0.0;
+  rec.linearize_ms = 0.0;
+  rec.solve_ms = 0.0;
+  c.total_pcg += pg.iters;
+  c.pcg_iters = pg.iters;
+  c.pcg_status = pg.status;
+  bool accepted = false;
+  bool stop = false;
+  if (c.nonfinite || !isfinite(pstep) || !isfinite(lstep)) {
+    // SingularSystem (lm.rs:608-663): lambda up, cost unchanged, no step.
+    c.lambda = fmin(c.lambda * lp.lambda_increase_factor, lp.max_lambda);
+    rec.cost_after = c.current_cost;
+    rec.max_pose_step = 0.0;
+    rec.max_landmark_step = 0.0;
+    rec.lambda = c.lambda;
+    rec.step_accepted = 0u;
+    if (c.lambda >= lp.max_lambda) stop = true;
+  } else {
+    const bool cost_ok = lp.has_initial_lambda ? (cost < c.current_cost) : true;
+    accepted = cost_ok && bad <= c.current_nonproj;
+    rec.cost_after = cost;
+    rec.max_pose_step = pstep;
+    rec.max_landmark_step = lstep;
+    if (!accepted) {
+      c.lambda = fmin(c.lambda * lp.lambda_increase_factor, lp.max_lambda);
+      rec.lambda = c.lambda;
+      rec.step_accepted = 0u;
+      if (!lp.has_initial_lambda || c.lambda >= lp.max_lambda) stop = true;
+    } else {
+      rec.lambda = c.lambda;
+      rec.step_accepted = 1u;
+      const double before = c.current_cost;
+      c.current_cost = cost;
+      c.current_nonproj = bad;
+      c.cur ^= 1u;
+      if (lp.has_initial_lambda)
+        c.lambda = fmax(c.lambda * lp.lambda_decrease_factor, lp.min_lambda);
+      if (pstep < lp.step_tolerance && lstep < lp.step_tolerance) {
+        c.converged = 1u;
+        stop = true;
+      } else if (fabs(before - cost) < lp.cost_tolerance) {
+        c.converged = 1u;
+        stop = true;
+      } else if (lp.has_relative_cost_tolerance) {
+        const double tol = lp.relative_cost_tolerance;
+        if (isfinite(tol) && tol >= 0.0 &&
+            (before - cost) / fmax(fabs(before), 2.220446049250313e-16) < tol) {
+          c.converged = 1u;
+          stop = true;
+        }
+      }
+    }
+  }
+  c.cost_after = rec.cost_after;
+  c.nonproj_after = bad;
+  c.max_pose_step = rec.max_pose_step;
+  c.max_landmark_step = rec.max_landmark_step;
+  if (it < d.max_records) d.records[(size_t)P * d.max_records + it] = rec;
+  c.iteration = it + 1;
+  c.relinearize = accepted ? 1u : 0u;
+  c.nonfinite = 0u;
+  if (stop || c.iteration >= lp.max_iterations) c.done = 1u;
+}
+
+// -------------------------------------------------------------------- PCG
+// Block-Jacobi PCG on the reduced camera system (the reference's pcg_init /
+// apply_lm / apply_pose / pcg_step, ba.wgsl:420-562, with the explicit S in
+// place of the implicit Schur operator): stop when |r| <= tol |b|, on
+// non-positive curvature, or at the iteration cap.
+//
+// One cooperative launch runs every iteration.  Per iteration:
+//   A  each block streams tiles of S (TB x TB blocks of 6x6, 36.9 KB at
+//      TB=16) HBM -> shared memory with cp.async.bulk (TMA) into a double
+//      buffer and writes, per tile (I,J), the row-side partial S_IJ p_J and
+//      the column-side partial S_IJ^T p_I (p = z + beta p formed on the fly);
+//   B  the owner of tile row I sums its partials in a fixed order into q_I,
+//      writes p_I and the partial dot p.q;
+//   C  x += alpha p, r -= alpha q, z = M^-1 r and the partial dots r.z, r.r.
+// All scalars are per problem and are summed over the problem's tile rows in
+// a fixed order, so every block computes bit-identical alphas and betas and a
+// problem's solve does not depend on what else is in the batch.  Blocks
+// synchronise through a grid barrier whose spin is bounded; a timeout sets
+// an error flag and every block leaves.
+template <int TB>
+struct Pcg {
+  static constexpr int kThreads = TB * TB;
+  static constexpr int kTileFloats = TB * TB * kBlock;
+  static constexpr uint32_t kTileBytes = kTileFloats * 4u;
+  static constexpr int kRow = TB * 6;
+  // Per tile row, stride kDots doubles: rz[3] (slot k mod 3), rr[3], pq[2]
+  // (slot k mod 2), b2.  Three rz/rr slots and two pq slots keep every value
+  // a block may still read in iteration k distinct from the ones written.
+  static constexpr size_t kSmem =
+      2 * (size_t)kTileBytes + 2 * kRow * 4 + kThreads * 6 * 4 + kThreads * 8 * 6 + 64;
+};
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
+}
+
+__device__ __forceinline__ void tma_load(void* dst, const void* src, uint32_t bytes,
+                                         uint64_t* bar) {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+               "r"(bytes)
+               : "memory");
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait; false (and the error flag) on timeout.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, unsigned int* err) {
+  uint32_t spins = 0;
+  while (!mbar_try_wait(bar, parity)) {
+    if (++spins > kSpinLimit) {
+      atomicOr(err, (unsigned int)kErrTmaTimeout);
+      return false;
+    }
+  }
+  return true;
+}
+
+// Sense-counting grid barrier with a bounded spin.  Returns false when any
+// block has flagged an error (every thread of the block sees the same value).
+__device__ bool grid_barrier(unsigned int* bar, unsigned int nblocks, unsigned int* err,
+                             unsigned int* s_flag) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned int* vgen = bar + 1;
+    const unsigned int gen = *vgen;
+    __threadfence();
+    const unsigned int arrived = atomicAdd(bar, 1u) + 1u;
+    if (arrived == nblocks) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      uint32_t spins = 0;
+      while (*vgen == gen) {
+        if (++spins > kSpinLimit) {
+          atomicOr(err, (unsigned int)kErrBarrierTimeout);
+          break;
+        }
+        __nanosleep(40);
+      }
+    }
+    __threadfence();
+    *s_flag = *(volatile unsigned int*)err;
+  }
+  __syncthreads();
+  return *s_flag == 0u;
+}
+
+// Per-problem PCG scalars, computed by the whole block from the tile-row
+// dots in a fixed order.
+struct ProbScal {
+  int active;
+  int status;   // when inactive: 0 converged, 1 cap, 2 breakdown
+  uint32_t iters;
+  double beta;
+  double rz;    // rz(k-1)
+  double rr;
+  double bnorm;
+};
+
+constexpr int kDotStride = 16;
+__device__ __forceinline__ int mod3(int k) { return ((k % 3) + 3) % 3; }
+constexpr int kDotRz = 0, kDotRr = 3, kDotPq = 6, kDotB2 = 8;
+
+template <int N>
+__device__ void prob_scalars(const Dev& d, uint32_t P, int k, double* red, ProbScal* out) {
+  const uint32_t t0 = d.prob_tr_begin[P], t1 = d.prob_tr_begin[P + 1];
+  const int sticky = *(volatile uint32_t*)&d.pcg[P].active;
+  double v[5] = {0, 0, 0, 0, 0};  // rz(k-1), rz(k-2), rr(k-1), pq(k-1), b2
+  const int s1 = mod3(k - 1), s2 = mod3(k - 2), sp = (k - 1) & 1;
+  for (uint32_t tr = t0 + threadIdx.x; tr < t1; tr += N) {
+    const double* dt = d.dots + kDotStride * (size_t)tr;
+    v[0] += __ldcg(dt + kDotRz + s1);
+    v[1] += __ldcg(dt + kDotRz + s2);
+    v[2] += __ldcg(dt + kDotRr + s1);
+    v[3] += __ldcg(dt + kDotPq + sp);
+    v[4] += __ldcg(dt + kDotB2);
+  }
+  for (int e = 0; e < 5; ++e) {
+    const double t = block_sum<double, N>(v[e], red);
+    if (threadIdx.x == 0) v[e] = t;
+  }
+  if (threadIdx.x == 0) {
+    const LmParams& lp = d.params[P];
+    ProbScal s;
+    s.active = sticky;
+    s.status = 0;
+    s.iters = (uint32_t)k;
+    s.beta = 0.0;
+    s.rz = v[0];
+    s.rr = v[2];
+    s.bnorm = sqrt(v[4]);
+    if (sticky) {
+      if (k == 0) {
+        // pcg_init (ba.wgsl:420-439): done when |b| = 0 or r.z <= 0.
+        if (!(v[4] > 0.0) || !(v[0] > 0.0) || lp.max_pcg_iterations == 0) s.active = 0;
+      } else if (!(v[3] > 0.0) || !isfinite(v[3])) {
+        s.active = 0;  // non-positive curvature in iteration k-1: x unchanged
+        s.status = 2;
+        s.iters = (uint32_t)(k - 1);
+      } else if (sqrt(v[2]) <= lp.pcg_relative_tolerance * s.bnorm || !(v[0] > 0.0)) {
+        s.active = 0;
+      } else if ((uint32_t)k >= lp.max_pcg_iterations) {
+        s.active = 0;
+        s.status = 1;
+      } else {
+        s.beta = v[0] / v[1];
+      }
+    }
+    *out = s;
+  }
+  __syncthreads();
+}
+
+template <int TB>
+__global__ void __launch_bounds__(Pcg<TB>::kThreads) k_pcg(Dev d) {
+  using C = Pcg<TB>;
+  constexpr int N = C::kThreads;
+  extern __shared__ __align__(128) unsigned char smem[];
+  float* const buf0 = reinterpret_cast<float*>(smem);  // buffer b at buf0 + b * kTileFloats
+  float* sPI = reinterpret_cast<float*>(smem + 2 * (size_t)C::kTileBytes);
+  float* sPJ = sPI + C::kRow;
+  float* colst = sPJ + C::kRow;                               // [N * 6]
+  double* red = reinterpret_cast<double*>(colst + N * 6);     // [N * 6]
+  __shared__ uint64_t mbar[2];
+  __shared__ ProbScal sc;
+  __shared__ uint32_t sc_prob;
+  __shared__ int sc_k;
+  __shared__ unsigned int s_flag;
+  __shared__ double s_alpha;
+
+  const uint32_t tid = threadIdx.x;
+  const uint32_t G = gridDim.x;
+  if (tid == 0) {
+    mbar_init(&mbar[0]);
+    mbar_init(&mbar[1]);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    sc_prob = kNone;
+    sc_k = -2;
+  }
+  __syncthreads();
+  uint32_t parity = 0;  // bit b: phase parity expected on buffer b
+  int nextbuf = 0;
+  bool ok = true;
+
+  auto scal = [&](uint32_t P, int k) {
+    if (sc_prob == P && sc_k == k) return;  // uniform: shared values
+    __syncthreads();
+    prob_scalars<N>(d, P, k, red, &sc);
+    if (tid == 0) {
+      sc_prob = P;
+      sc_k = k;
+    }
+    __syncthreads();
+  };
+
+  // ---- init: x = 0, r = b, z = M^-1 r, p = z; dots rz, b2 in slot k = -1.
+  for (uint32_t tr = blockIdx.x; tr < d.num_tile_rows; tr += G) {
+    const uint32_t P = d.tr_prob[tr];
+    if (!*(volatile uint32_t*)&d.pcg[P].active) continue;
+    const size_t base = (size_t)tr * C::kRow;
+    if (tid < (uint32_t)C::kRow) {
+      const float b = d.rhs[base + tid];
+      d.x[base + tid] = 0.0f;
+      d.r[base + tid] = b;
+      sPI[tid] = b;
+    }
+    __syncthreads();
+    double rz = 0.0, bb = 0.0;
+    if (tid < (uint32_t)C::kRow) {
+      const uint32_t cam = tid / 6, a = tid % 6;
+      const float* m = d.minv + 36 * (base / 6 + cam) + a * 6;
+      float z = 0.0f;
+#pragma unroll
+      for (int b = 0; b < 6; ++b) z += m[b] * sPI[cam * 6 + b];
+      d.z[base + tid] = z;
+      d.p[base + tid] = z;
+      rz = (double)sPI[tid] * (double)z;
+      bb = (double)sPI[tid] * (double)sPI[tid];
+    }
+    rz = block_sum<double, N>(rz, red);
+    bb = block_sum<double, N>(bb, red);
+    if (tid == 0) {
+      double* dt = d.dots + kDotStride * (size_t)tr;
+      dt[kDotRz + mod3(-1)] = rz;  // the values of "iteration -1"
+      dt[kDotRr + mod3(-1)] = bb;
+      dt[kDotPq + 1] = 1.0;
+      dt[kDotB2] = bb;
+    }
+  }
+  ok = grid_barrier(d.barrier, G, d.error, &s_flag);
+
+  for (int k = 0; ok; ++k) {
+    // ---- A: status of the problems this block owns, then the tiles.
+    for (uint32_t tr = blockIdx.x; tr < d.num_tile_rows; tr += G) {
+      const uint32_t P = d.tr_prob[tr];
+      if (d.prob_tr_begin[P] != tr) continue;  // owner = first tile row
+      if (!*(volatile uint32_t*)&d.pcg[P].active) continue;
+      scal(P, k);
+      if (!sc.active && tid == 0) {
+        PcgState& st = d.pcg[P];
+        st.iters = sc.iters;
+        st.status = (uint32_t)sc.status;
+        st.bnorm = sc.bnorm;
+        st.rnorm = sqrt(sc.rr);
+        st.rz = sc.rz;
+        __threadfence();
+        st.active = 0u;
+        atomicSub(d.barrier + 2, 1u);
+      }
+    }
+    {
+      uint32_t t = blockIdx.x;
+      int b = nextbuf;
+      if (t < d.num_tiles && tid == 0) tma_load(buf0 + b * C::kTileFloats, d.tiles + (size_t)t * C::kTileFloats,
+                                                C::kTileBytes, &mbar[b]);
+      while (t < d.num_tiles) {
+        const uint32_t tn = t + G;
+        const int bn = b ^ 1;
+        if (tn < d.num_tiles && tid == 0)
+          tma_load(buf0 + bn * C::kTileFloats, d.tiles + (size_t)tn * C::kTileFloats, C::kTileBytes, &mbar[bn]);
+        const uint32_t ij = d.tile_ij[t];
+        const uint32_t I = ij >> 16, J = ij & 0xFFFFu;
+        const uint32_t P = d.tr_prob[I];
+        scal(P, k);
+        const bool arrived = __syncthreads_and(mbar_wait(&mbar[b], (parity >> b) & 1u, d.error));
+        parity ^= 1u << b;
+        if (!arrived) ok = false;
+        if (sc.active && ok) {
+          if (tid < (uint32_t)C::kRow) {
+            const size_t bi = (size_t)I * C::kRow + tid, bj = (size_t)J * C::kRow + tid;
+            float pi = __ldcg(d.p + bi), pj = __ldcg(d.p + bj);
+            if (k > 0) {
+              const float beta = (float)sc.beta;
+              pi = __ldcg(d.z + bi) + beta * pi;
+              pj = __ldcg(d.z + bj) + beta * pj;
+            }
+            sPI[tid] = pi;
+            sPJ[tid] = pj;
+          }
+          __syncthreads();
+          const int li = tid / TB, lj = tid % TB;
+          const float4* blk = reinterpret_cast<const float4*>(buf0 + b * C::kTileFloats + tid * kBlock);
+          float s[36];
+#pragma unroll
+          for (int m = 0; m < 9; ++m) {
+            const float4 v = blk[m];
+            s[4 * m] = v.x;
+            s[4 * m + 1] = v.y;
+            s[4 * m + 2] = v.z;
+            s[4 * m + 3] = v.w;
+          }
+          float row[6], col[6];
+#pragma unroll
+          for (int a = 0; a < 6; ++a) {
+            float acc = 0.0f;
+#pragma unroll
+            for (int c = 0; c < 6; ++c) acc += s[a * 6 + c] * sPJ[lj * 6 + c];
+            row[a] = acc;
+          }
+#pragma unroll
+          for (int c = 0; c < 6; ++c) {
+            float acc = 0.0f;
+#pragma unroll
+            for (int a = 0; a < 6; ++a) acc += s[a * 6 + c] * sPI[li * 6 + a];
+            col[c] = acc;
+          }
+#pragma unroll
+          for (int off = TB / 2; off > 0; off >>= 1)
+#pragma unroll
+            for (int a = 0; a < 6; ++a) row[a] += __shfl_xor_sync(0xffffffffu, row[a], off, TB);
+          float* part = d.partial + (size_t)t * 2 * C::kRow;
+          if (lj == 0) {
+#pragma unroll
+            for (int a = 0; a < 6; ++a) part[li * 6 + a] = row[a];
+          }
+          if (I != J) {
+#pragma unroll
+            for (int c = 0; c < 6; ++c) colst[tid * 6 + c] = col[c];
+            __syncthreads();
+            if (tid < (uint32_t)C::kRow) {
+              const int cj = tid / 6, c = tid % 6;
+              float acc = 0.0f;
+#pragma unroll
+              for (int r2 = 0; r2 < TB; ++r2) acc += colst[(r2 * TB + cj) * 6 + c];
+              part[C::kRow + tid] = acc;
+            }
+          }
+        }
+        __syncthreads();  // buf[b] and the staging areas are free again
+        t = tn;
+        b = bn;
+      }
+      nextbuf = b;
+    }
+    ok = grid_barrier(d.barrier, G, d.error, &s_flag) && ok;
+    if (!ok) break;
+    if (*(volatile unsigned int*)(d.barrier + 2) == 0u) break;  // every problem done
+
+    // ---- B: q = S p for owned tile rows; p written; partial p.q.
+    for (uint32_t tr = blockIdx.x; tr < d.num_tile_rows; tr += G) {
+      const uint32_t P = d.tr_prob[tr];
+      scal(P, k);
+      if (!sc.active) continue;
+      const size_t base = (size_t)tr * C::kRow;
+      double pq = 0.0;
+      if (tid < (uint32_t)C::kRow) {
+        float pv = __ldcg(d.p + base + tid);
+        if (k > 0) pv = __ldcg(d.z + base + tid) + (float)sc.beta * pv;
+        d.p[base + tid] = pv;
+        float acc = 0.0f;
+        for (uint32_t m = d.tr_list_off[tr]; m < d.tr_list_off[tr + 1]; ++m)
+          acc += __ldcg(d.partial + (size_t)d.tr_list[m] * C::kRow + tid);
+        d.q[base + tid] = acc;
+        pq = (double)pv * (double)acc;
+      }
+      pq = block_sum<double, N>(pq, red);
+      if (tid == 0) d.dots[kDotStride * (size_t)tr + kDotPq + (k & 1)] = pq;
+    }
+    ok = grid_barrier(d.barrier, G, d.error, &s_flag);
+    if (!ok) break;
+
+    // ---- C: alpha = rz / p.q; x, r, z updates; partial r.z and r.r.
+    uint32_t cprob = kNone;
+    for (uint32_t tr = blockIdx.x; tr < d.num_tile_rows; tr += G) {
+      const uint32_t P = d.tr_prob[tr];
+      scal(P, k);
+      if (!sc.active) continue;
+      if (cprob != P) {
+        double pq = 0.0;
+        for (uint32_t t2 = d.prob_tr_begin[P] + tid; t2 < d.prob_tr_begin[P + 1]; t2 += N)
+          pq += __ldcg(d.dots + kDotStride * (size_t)t2 + kDotPq + (k & 1));
+        pq = block_sum<double, N>(pq, red);
+        if (tid == 0) s_alpha = (pq > 0.0 && isfinite(pq)) ? sc.rz / pq : 0.0;
+        __syncthreads();
+        cprob = P;
+      }
+      const double alpha = s_alpha;
+      if (alpha == 0.0) continue;  // breakdown: x frozen, flagged at A(k+1)
+      const size_t base = (size_t)tr * C::kRow;
+      const float af = (float)alpha;
+      if (tid < (uint32_t)C::kRow) {
+        const float pv = __ldcg(d.p + base + tid);
+        const float qv = __ldcg(d.q + base + tid);
+        d.x[base + tid] = __ldcg(d.x + base + tid) + af * pv;
+        const float rv = __ldcg(d.r + base + tid) - af * qv;
+        d.r[base + tid] = rv;
+        sPI[tid] = rv;
+      }
+      __syncthreads();
+      double rz = 0.0, rr = 0.0;
+      if (tid < (uint32_t)C::kRow) {
+        const uint32_t cam = tid / 6, a = tid % 6;
+        const float* m = d.minv + 36 * (base / 6 + cam) + a * 6;
+        float z = 0.0f;
+#pragma unroll
+        for (int b = 0; b < 6; ++b) z += m[b] * sPI[cam * 6 + b];
+        d.z[base + tid] = z;
+        rz = (double)sPI[tid] * (double)z;
+        rr = (double)sPI[tid] * (double)sPI[tid];
+      }
+      rz = block_sum<double, N>(rz, red);
+      rr = block_sum<double, N>(rr, red);
+      if (tid == 0) {
+        double* dt = d.dots + kDotStride * (size_t)tr;
+        dt[kDotRz + mod3(k)] = rz;
+        dt[kDotRr + mod3(k)] = rr;
+      }
+    }
+    ok = grid_barrier(d.barrier, G, d.error, &s_flag);
+  }
+  // Drain: nothing is in flight on the normal path (every issued copy was
+  // waited for); on the error path wait (bounded) for the last copies.
+  if (!ok && tid == 0) {
+    for (int b = 0; b < 2; ++b) {
+      uint32_t spins = 0;
+      while (!mbar_try_wait(&mbar[b], (parity >> b) & 1u) && ++spins < 1024u) {
+      }
+    }
+  }
+}
+
+__global__ void k_pcg_setup(Dev d) {
+  // Per-problem PCG state, grid-barrier words and the active count.
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    uint32_t active = 0;
+    for (uint32_t P = 0; P < d.num_problems; ++P) {
+      const bool on = !d.ctrl[P].done && d.prob_tr_begin[P + 1] > d.prob_tr_begin[P];
+      PcgState& s = d.pcg[P];
+      s.active = on ? 1u : 0u;
+      s.iters = 0u;
+      s.status = 0u;
+      s.rz = 0.0;
+      s.bnorm = 0.0;
+      s.rnorm = 0.0;
+      active += on ? 1u : 0u;
+    }
+    d.barrier[0] = 0u;
+    d.barrier[1] = 0u;
+    d.barrier[2] = active;
+  }
+}
+
+// Problems without variable cameras have no PCG; x has no entries for them.
+
+template <typename K>
+int grid_for(K kernel, int threads, size_t smem) {
+  (void)kernel;
+  (void)threads;
+  (void)smem;
+  return 0;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------- launchers
+static int grid1d(size_t n, int threads, int cap = 148 * 32) {
+  size_t g = (n + threads - 1) / threads;
+  if (g < 1) g = 1;
+  if (g > (size_t)cap) g = cap;
+  return (int)g;
+}
+
+cudaError_t launch_pose_table(const Dev& d, cudaStream_t s) {
+  k_pose_table<<<grid1d(d.num_poses, 256), 256, 0, s>>>(d);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_cost(const Dev& d, bool trial, cudaStream_t s) {
+  const int g = grid1d((size_t)d.num_point_chunks * 256, 256, 148 * 16);
+  if (trial)
+    k_cost<true><<<g, 256, 0, s>>>(d);
+  else
+    k_cost<false><<<g, 256, 0, s>>>(d);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_decide(const Dev& d, bool init, cudaStream_t s) {
+  if (init)
+    k_decide<true><<<d.num_problems, 256, 0, s>>>(d);
+  else
+    k_decide<false><<<d.num_problems, 256, 0, s>>>(d);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_linearize(const Dev& d, cudaStream_t s) {
+  k_linearize<<<grid1d(d.num_points, 256), 256, 0, s>>>(d);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_point_prep(const Dev& d, cudaStream_t s) {
+  k_point_prep<<<grid1d(d.num_points, 256), 256, 0, s>>>(d);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_offdiag(const Dev& d, cudaStream_t s) {
+  if (d.num_offdiag_blocks == 0) return cudaSuccess;
+  const size_t threads_needed = (size_t)d.num_offdiag_blocks * d.group;
+  const int g = grid1d(threads_needed, 256, 148 * 16);
+  switch (d.group) {
+    case 1: k_offdiag<1><<<g, 256, 0, s>>>(d); break;
+    case 2: k_offdiag<2><<<g, 256, 0, s>>>(d); break;
+    case 4: k_offdiag<4><<<g, 256, 0, s>>>(d); break;
+    case 8: k_offdiag<8><<<g, 256, 0, s>>>(d); break;
+    case 16: k_offdiag<16><<<g, 256, 0, s>>>(d); break;
+    default: k_offdiag<32><<<g, 256, 0, s>>>(d); break;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_cam_diag(const Dev& d, cudaStream_t s) {
+  if (d.num_var_cams == 0) return cudaSuccess;
+  const int g = d.num_var_cams < 148u * 16u ? (int)d.num_var_cams : 148 * 16;
+  k_cam_diag<<<g, kDiagThreads, 0, s>>>(d);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pose_update(const Dev& d, cudaStream_t s) {
+  k_pose_update<<<grid1d(d.num_poses, 256), 256, 0, s>>>(d);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pcg_setup(const Dev& d, cudaStream_t s) {
+  k_pcg_setup<<<1, 32, 0, s>>>(d);
+  return cudaGetLastError();
+}
+
+size_t pcg_smem_bytes(int tb) { return tb == 8 ? Pcg<8>::kSmem : Pcg<16>::kSmem; }
+
+int pcg_grid_size(int tb, int sm_count) {
+  int per_sm = 0;
+  cudaError_t e;
+  if (tb == 8) {
+    cudaFuncSetAttribute(k_pcg<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)Pcg<8>::kSmem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg<8>, Pcg<8>::kThreads,
+                                                      Pcg<8>::kSmem);
+  } else {
+    cudaFuncSetAttribute(k_pcg<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)Pcg<16>::kSmem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg<16>, Pcg<16>::kThreads,
+                                                      Pcg<16>::kSmem);
+  }
+  if (e != cudaSuccess || per_sm <= 0) return 0;
+  return per_sm * sm_count;
+}
+
+cudaError_t launch_pcg(const Dev& d, int grid, cudaStream_t s) {
+  if (d.num_tile_rows == 0) return cudaSuccess;
+  void* args[] = {const_cast<Dev*>(&d)};
+  if (d.tb == 8)
+    return cudaLaunchCooperativeKernel((const void*)k_pcg<8>, grid, Pcg<8>::kThreads, args,
+                                       Pcg<8>::kSmem, s);
+  return cudaLaunchCooperativeKernel((const void*)k_pcg<16>, grid, Pcg<16>::kThreads, args,
+                                     Pcg<16>::kSmem, s);
+}
+
+}  // namespace vlba

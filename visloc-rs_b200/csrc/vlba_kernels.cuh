@@ -1,0 +1,27 @@
+// vlba_kernels.cuh -- declarations of the LM-step kernels (vlba_kernels.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "vlba_common.cuh"
+
+namespace vlba {
+
+// Launch helpers; every kernel reads the per-problem Ctrl and skips problems
+// that are done (so a batch keeps running while some problems finish).
+cudaError_t launch_pose_table(const Dev& d, cudaStream_t s);
+cudaError_t launch_cost(const Dev& d, bool trial, cudaStream_t s);
+cudaError_t launch_decide(const Dev& d, bool init, cudaStream_t s);
+cudaError_t launch_linearize(const Dev& d, cudaStream_t s);
+cudaError_t launch_point_prep(const Dev& d, cudaStream_t s);
+cudaError_t launch_offdiag(const Dev& d, cudaStream_t s);
+cudaError_t launch_cam_diag(const Dev& d, cudaStream_t s);
+cudaError_t launch_pcg(const Dev& d, int sm_count, cudaStream_t s);
+cudaError_t launch_pose_update(const Dev& d, cudaStream_t s);
+cudaError_t launch_pcg_setup(const Dev& d, cudaStream_t s);
+
+// Occupancy-derived grid of the persistent PCG kernel (0 if it cannot run).
+int pcg_grid_size(int tb, int sm_count);
+size_t pcg_smem_bytes(int tb);
+
+}  // namespace vlba

@@ -1,0 +1,507 @@
+// vlba_plan.cpp -- see vlba_plan.h.
+#include "vlba_plan.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <stdexcept>
+#include <unordered_map>
+
+namespace vlba {
+
+namespace {
+
+void quat_to_matrix(const double* q, double* m) {
+  const double w = q[0], i = q[1], j = q[2], k = q[3];
+  const double ww = w * w, ii = i * i, jj = j * j, kk = k * k;
+  const double ij = i * j * 2.0, wk = w * k * 2.0, wj = w * j * 2.0;
+  const double ik = i * k * 2.0, jk = j * k * 2.0, wi = w * i * 2.0;
+  m[0] = ww + ii - jj - kk; m[1] = ij - wk;           m[2] = wj + ik;
+  m[3] = wk + ij;           m[4] = ww - ii + jj - kk; m[5] = jk - wi;
+  m[6] = ik - wj;           m[7] = wi + jk;           m[8] = ww - ii - jj + kk;
+}
+
+uint32_t round_up(uint32_t v, uint32_t m) { return (v + m - 1) / m * m; }
+
+}  // namespace
+
+bool resolve_camera(const vlba_camera& c, DevCamera* out) {
+  const double* p = c.params;
+  const uint32_t n = c.num_params;
+  double fx, fy, cx, cy, k1 = 0.0, k2 = 0.0;
+  bool has_radial = false;
+  switch (c.model) {
+    case VLBA_CAMERA_PINHOLE:
+      if (n < 4 || n > 8) return false;
+      fx = p[0]; fy = p[1]; cx = p[2]; cy = p[3];
+      if (n >= 5) { has_radial = true; k1 = p[4]; k2 = n >= 6 ? p[5] : 0.0; }
+      break;
+    case VLBA_CAMERA_OPENCV:
+      if (n < 4 || n > 8) return false;
+      fx = p[0]; fy = p[1]; cx = p[2]; cy = p[3];
+      if ((n >= 7 && p[6] != 0.0) || (n >= 8 && p[7] != 0.0)) return false;
+      if (n >= 5) { has_radial = true; k1 = p[4]; k2 = n >= 6 ? p[5] : 0.0; }
+      break;
+    case VLBA_CAMERA_SIMPLE_PINHOLE:
+      if (n < 3 || n > 8) return false;
+      fx = fy = p[0]; cx = p[1]; cy = p[2];
+      break;
+    case VLBA_CAMERA_SIMPLE_RADIAL:
+      if (n < 3 || n > 8) return false;
+      fx = fy = p[0]; cx = p[1]; cy = p[2];
+      if (n >= 4) { has_radial = true; k1 = p[3]; }
+      break;
+    case VLBA_CAMERA_RADIAL:
+      if (n < 3 || n > 8) return false;
+      fx = fy = p[0]; cx = p[1]; cy = p[2];
+      if (n >= 4) { has_radial = true; k1 = p[3]; k2 = n >= 5 ? p[4] : 0.0; }
+      break;
+    default:
+      return false;
+  }
+  std::memset(out, 0, sizeof *out);
+  out->fx = fx; out->fy = fy; out->cx = cx; out->cy = cy;
+  out->k1 = k1; out->k2 = k2;
+  out->radial = (has_radial && (k1 != 0.0 || k2 != 0.0)) ? 1 : 0;
+  quat_to_matrix(c.sensor_from_rig_q, out->R);
+  for (int a = 0; a < 3; ++a) out->t[a] = c.sensor_from_rig_t[a];
+  const bool identity = c.sensor_from_rig_q[0] == 1.0 && c.sensor_from_rig_q[1] == 0.0 &&
+                        c.sensor_from_rig_q[2] == 0.0 && c.sensor_from_rig_q[3] == 0.0 &&
+                        c.sensor_from_rig_t[0] == 0.0 && c.sensor_from_rig_t[1] == 0.0 &&
+                        c.sensor_from_rig_t[2] == 0.0;
+  out->rig = identity ? 0 : 1;
+  return true;
+}
+
+LmParams make_params(const vlba_config* cfg) {
+  LmParams lp;
+  std::memset(&lp, 0, sizeof lp);
+  lp.initial_lambda = cfg->initial_lambda;
+  lp.lambda_increase_factor = cfg->lambda_increase_factor;
+  lp.lambda_decrease_factor = cfg->lambda_decrease_factor;
+  lp.max_lambda = cfg->max_lambda;
+  lp.min_lambda = cfg->min_lambda;
+  lp.step_tolerance = cfg->step_tolerance;
+  lp.cost_tolerance = cfg->cost_tolerance;
+  lp.relative_cost_tolerance = cfg->relative_cost_tolerance;
+  lp.robust_parameter = cfg->robust_parameter;
+  lp.pcg_relative_tolerance = cfg->pcg_relative_tolerance;
+  lp.has_initial_lambda = cfg->has_initial_lambda ? 1u : 0u;
+  lp.has_relative_cost_tolerance = cfg->has_relative_cost_tolerance ? 1u : 0u;
+  lp.robust_kernel = cfg->robust_kernel;
+  lp.max_iterations = cfg->max_iterations;
+  lp.max_pcg_iterations = cfg->max_pcg_iterations;
+  return lp;
+}
+
+Validation validate_problem(const vlba_problem* p, const vlba_config* cfg) {
+  Validation v;
+  if (!p || !cfg) { v.status = VLBA_ERR_INVALID_ARGUMENT; return v; }
+  if (cfg->robust_kernel > VLBA_KERNEL_CAUCHY) { v.status = VLBA_ERR_INVALID_ARGUMENT; return v; }
+  if (p->num_poses >= kNone || p->num_landmarks >= kNone || p->num_observations >= kNone) {
+    v.status = VLBA_ERR_INVALID_ARGUMENT;
+    return v;
+  }
+  if ((p->num_poses && (!p->pose_q || !p->pose_t)) || (p->num_landmarks && !p->landmarks) ||
+      (p->num_observations && (!p->obs_pose || !p->obs_landmark || !p->obs_xy))) {
+    v.status = VLBA_ERR_INVALID_ARGUMENT;
+    return v;
+  }
+  // Camera model first (lm.rs:168 `intrinsics()?`); a model outside the
+  // radial pinhole family is declined, so the caller runs its CPU solver.
+  if (p->num_cameras == 0 || !p->cameras) { v.status = VLBA_ERR_UNSUPPORTED_CAMERA_MODEL; return v; }
+  for (uint32_t c = 0; c < p->num_cameras; ++c) {
+    DevCamera dc;
+    const uint32_t m = p->cameras[c].model;
+    if (m > VLBA_CAMERA_OPENCV) { v.status = VLBA_DECLINED; return v; }
+    if (!resolve_camera(p->cameras[c], &dc)) {
+      // Known model with a tangential term or malformed parameters.
+      v.status = (m == VLBA_CAMERA_OPENCV) ? VLBA_DECLINED : VLBA_ERR_UNSUPPORTED_CAMERA_MODEL;
+      return v;
+    }
+  }
+  if (p->num_poses == 0) { v.status = VLBA_ERR_NO_POSES; return v; }
+  if (p->num_observations == 0) { v.status = VLBA_ERR_NO_OBSERVATIONS; return v; }
+  if (p->num_landmarks == 0) { v.status = VLBA_ERR_NO_LANDMARKS; return v; }
+  for (uint64_t o = 0; o < p->num_observations; ++o) {
+    if (p->obs_pose[o] >= p->num_poses) {
+      v.status = VLBA_ERR_MISSING_POSE;
+      v.error_index = p->obs_pose[o];
+      return v;
+    }
+    if (p->obs_landmark[o] >= p->num_landmarks) {
+      v.status = VLBA_ERR_MISSING_LANDMARK;
+      v.error_index = p->obs_landmark[o];
+      return v;
+    }
+    if (p->obs_camera && p->obs_camera[o] >= p->num_cameras) {
+      v.status = VLBA_ERR_INVALID_ARGUMENT;
+      v.error_index = o;
+      return v;
+    }
+  }
+  bool any_var = false;
+  for (uint64_t i = 0; i < p->num_poses && !any_var; ++i)
+    any_var = !(p->pose_fixed && p->pose_fixed[i]);
+  for (uint64_t i = 0; i < p->num_landmarks && !any_var; ++i)
+    any_var = !(p->landmark_fixed && p->landmark_fixed[i]);
+  if (!any_var) { v.status = VLBA_ERR_ALL_POSES_FIXED; return v; }
+  return v;
+}
+
+void build_plan(const vlba_problem* const* problems, const vlba_config* const* configs,
+                uint32_t n, uint32_t tb, Plan* plan) {
+  Plan& P = *plan;
+  P = Plan();
+  P.tb = tb;
+  P.num_problems = n;
+  uint64_t tot_poses = 0, tot_points = 0, tot_obs = 0, tot_cams = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    tot_poses += problems[i]->num_poses;
+    tot_points += problems[i]->num_landmarks;
+    tot_obs += problems[i]->num_observations;
+    tot_cams += problems[i]->num_cameras;
+  }
+  if (tot_poses >= kNone || tot_points >= kNone || tot_obs >= kNone)
+    throw std::runtime_error("batch exceeds 2^32 poses, points or observations");
+  P.pose_q.resize(4 * tot_poses);
+  P.pose_t.resize(3 * tot_poses);
+  P.points.resize(3 * tot_points);
+  P.pose_slot.assign(tot_poses, kNone);
+  P.point_var.assign(tot_points, 0);
+  P.pose_prob.resize(tot_poses);
+  P.point_prob.resize(tot_points);
+  P.pt_off.assign(tot_points + 1, 0);
+  P.obs_pose.resize(tot_obs);
+  P.obs_cam.resize(tot_obs);
+  P.obs_slot.resize(tot_obs);
+  P.obs_xy.resize(2 * tot_obs);
+  P.cameras.reserve(tot_cams);
+  P.prob_pose_begin.push_back(0);
+  P.prob_point_begin.push_back(0);
+  P.prob_obs_begin.push_back(0);
+  P.prob_tr_begin.push_back(0);
+  P.prob_chunk_begin.push_back(0);
+  P.prob_camera_begin.push_back(0);
+  P.chunk_point_begin.push_back(0);
+  P.cam_off.push_back(0);
+  P.dup_off.push_back(0);
+  P.blk_off.push_back(0);
+  P.tr_list_off.push_back(0);
+
+  const uint32_t tile_floats = tb * tb * kBlock;
+  uint32_t pose_base = 0, point_base = 0, obs_base = 0, slot_base = 0, tr_base = 0;
+  uint32_t tile_count = 0;
+
+  for (uint32_t pi = 0; pi < n; ++pi) {
+    const vlba_problem* p = problems[pi];
+    P.params.push_back(make_params(configs[pi]));
+    const uint32_t np = (uint32_t)p->num_poses, nl = (uint32_t)p->num_landmarks,
+                   no = (uint32_t)p->num_observations;
+    const uint32_t cam_base = (uint32_t)P.cameras.size();
+    for (uint32_t c = 0; c < p->num_cameras; ++c) {
+      DevCamera dc;
+      if (!resolve_camera(p->cameras[c], &dc)) throw std::runtime_error("camera model");
+      if (!p->obs_camera) dc.rig = 0;  // monocular: the pose is the camera
+      P.cameras.push_back(dc);
+    }
+    // Poses and variable slots, in index (= ascending id) order (lm.rs:234-249).
+    uint32_t nvar = 0;
+    for (uint32_t i = 0; i < np; ++i) {
+      const uint32_t g = pose_base + i;
+      for (int a = 0; a < 4; ++a) P.pose_q[4 * (size_t)g + a] = p->pose_q[4 * (size_t)i + a];
+      for (int a = 0; a < 3; ++a) P.pose_t[3 * (size_t)g + a] = p->pose_t[3 * (size_t)i + a];
+      P.pose_prob[g] = pi;
+      if (!(p->pose_fixed && p->pose_fixed[i])) P.pose_slot[g] = slot_base + nvar++;
+    }
+    P.real_var_cams += nvar;
+    const uint32_t nslots = round_up(nvar, tb);
+    for (uint32_t s = 0; s < nslots; ++s) P.slot_prob.push_back(pi);
+    for (uint32_t j = 0; j < nl; ++j) {
+      const uint32_t g = point_base + j;
+      for (int a = 0; a < 3; ++a) P.points[3 * (size_t)g + a] = p->landmarks[3 * (size_t)j + a];
+      P.point_prob[g] = pi;
+      const bool var = !(p->landmark_fixed && p->landmark_fixed[j]);
+      P.point_var[g] = var ? 1 : 0;
+      if (var) ++P.var_points;
+    }
+    // Point-major observation order: stable counting sort by landmark.
+    std::vector<uint32_t> cnt(nl + 1, 0);
+    for (uint32_t o = 0; o < no; ++o) ++cnt[p->obs_landmark[o] + 1];
+    for (uint32_t j = 0; j < nl; ++j) cnt[j + 1] += cnt[j];
+    std::vector<uint32_t> order(no);
+    {
+      std::vector<uint32_t> fill(cnt.begin(), cnt.end() - 1);
+      for (uint32_t o = 0; o < no; ++o) order[fill[p->obs_landmark[o]]++] = o;
+    }
+    for (uint32_t j = 0; j < nl; ++j) P.pt_off[point_base + j + 1] = obs_base + cnt[j + 1];
+    for (uint32_t k = 0; k < no; ++k) {
+      const uint32_t o = order[k];
+      const uint32_t g = obs_base + k;
+      const uint32_t pose = pose_base + p->obs_pose[o];
+      P.obs_pose[g] = pose;
+      P.obs_cam[g] = cam_base + (p->obs_camera ? p->obs_camera[o] : 0u);
+      P.obs_slot[g] = P.pose_slot[pose];
+      P.obs_xy[2 * (size_t)g] = p->obs_xy[2 * (size_t)o];
+      P.obs_xy[2 * (size_t)g + 1] = p->obs_xy[2 * (size_t)o + 1];
+    }
+    // Per-slot observation lists (ascending point-major index).
+    {
+      std::vector<uint32_t> c2(nslots + 1, 0);
+      for (uint32_t k = 0; k < no; ++k) {
+        const uint32_t s = P.obs_slot[obs_base + k];
+        if (s != kNone) ++c2[s - slot_base + 1];
+      }
+      for (uint32_t s = 0; s < nslots; ++s) c2[s + 1] += c2[s];
+      const uint32_t list_base = (uint32_t)P.cam_obs.size();
+      P.cam_obs.resize(list_base + c2[nslots]);
+      std::vector<uint32_t> fill(c2.begin(), c2.end() - 1);
+      for (uint32_t k = 0; k < no; ++k) {
+        const uint32_t s = P.obs_slot[obs_base + k];
+        if (s != kNone) P.cam_obs[list_base + fill[s - slot_base]++] = obs_base + k;
+      }
+      for (uint32_t s = 0; s < nslots; ++s) P.cam_off.push_back(list_base + c2[s + 1]);
+    }
+    // Camera pairs sharing a variable point: block (i, j), i > j (local
+    // slots).  Counted in a dense nvar x nvar table (sparse map beyond).
+    const uint64_t nv64 = nvar;
+    const bool dense_table = nv64 * nv64 <= (64ull << 20);
+    std::vector<uint32_t> table;
+    std::unordered_map<uint64_t, uint32_t> map;
+    if (dense_table) table.assign(nv64 * nv64, 0);
+    auto key_count = [&](uint32_t i, uint32_t j) -> uint32_t& {
+      if (dense_table) return table[(uint64_t)i * nv64 + j];
+      return map[(uint64_t)i * nv64 + j];
+    };
+    std::vector<uint32_t> dup_cnt(nslots + 1, 0);
+    for (uint32_t j = 0; j < nl; ++j) {
+      if (!P.point_var[point_base + j]) continue;
+      const uint32_t k0 = cnt[j], k1 = cnt[j + 1];
+      for (uint32_t a = k0; a < k1; ++a) {
+        const uint32_t sa = P.obs_slot[obs_base + a];
+        if (sa == kNone) continue;
+        ++P.var_obs;
+        for (uint32_t b = k0; b < k1; ++b) {
+          if (b == a) continue;
+          const uint32_t sb = P.obs_slot[obs_base + b];
+          if (sb == kNone) continue;
+          if (sa > sb) ++key_count(sa - slot_base, sb - slot_base);
+          else if (sa == sb) ++dup_cnt[sa - slot_base + 1];
+        }
+      }
+    }
+    // Blocks in row-major order; per-tile existence.
+    const uint32_t ntr = nslots / tb;
+    std::vector<uint8_t> tile_has((size_t)ntr * ntr, 0);
+    std::vector<uint64_t> keys;
+    if (dense_table) {
+      for (uint64_t i = 0; i < nv64; ++i)
+        for (uint64_t jj = 0; jj < i; ++jj)
+          if (table[i * nv64 + jj]) keys.push_back(i * nv64 + jj);
+    } else {
+      keys.reserve(map.size());
+      for (const auto& kv : map) keys.push_back(kv.first);
+      std::sort(keys.begin(), keys.end());
+    }
+    const uint32_t blk_base = (uint32_t)P.blk_dst.size();
+    const uint32_t pair_base = (uint32_t)P.pairs.size();
+    std::vector<uint32_t> blk_fill(keys.size());
+    {
+      uint32_t run = pair_base;
+      for (size_t b = 0; b < keys.size(); ++b) {
+        const uint32_t i = (uint32_t)(keys[b] / nv64), jj = (uint32_t)(keys[b] % nv64);
+        tile_has[(size_t)(i / tb) * ntr + jj / tb] = 1;
+        uint32_t& c = key_count(i, jj);
+        const uint32_t count = c;
+        c = (uint32_t)b;  // table now maps key -> local block id
+        blk_fill[b] = run;
+        run += count;
+        P.blk_off.push_back(run);
+      }
+      P.pairs.resize(run);
+    }
+    P.camera_pairs += keys.size();
+    for (uint32_t t = 0; t < ntr; ++t) tile_has[(size_t)t * ntr + t] = 1;
+    // Compact tile ids, row-major.
+    std::vector<uint32_t> tile_id((size_t)ntr * ntr, kNone);
+    for (uint32_t I = 0; I < ntr; ++I)
+      for (uint32_t J = 0; J <= I; ++J)
+        if (tile_has[(size_t)I * ntr + J]) {
+          tile_id[(size_t)I * ntr + J] = tile_count++;
+          if (tr_base + I > 0xFFFFu || tr_base + J > 0xFFFFu)
+            throw std::runtime_error("more than 65535 tile rows");
+          P.tile_ij.push_back(((tr_base + I) << 16) | (tr_base + J));
+        }
+    // Block destinations.
+    P.blk_dst.resize(blk_base + keys.size());
+    for (size_t b = 0; b < keys.size(); ++b) {
+      const uint32_t i = (uint32_t)(keys[b] / nv64), jj = (uint32_t)(keys[b] % nv64);
+      const uint32_t I = i / tb, J = jj / tb, li = i % tb, lj = jj % tb;
+      const uint32_t t = tile_id[(size_t)I * ntr + J];
+      PairIdx dst;
+      dst.a = t * tile_floats + (li * tb + lj) * kBlock;
+      dst.b = (I == J) ? t * tile_floats + (lj * tb + li) * kBlock : kNone;
+      P.blk_dst[blk_base + b] = dst;
+    }
+    for (uint32_t s = 0; s < nslots; ++s) {
+      const uint32_t I = s / tb, li = s % tb;
+      P.diag_dst.push_back(tile_id[(size_t)I * ntr + I] * tile_floats + (li * tb + li) * kBlock);
+    }
+    // Scatter the pairs, point by point (so each block's list is in point
+    // order), and the same-camera duplicates.
+    for (uint32_t s = 0; s < nslots; ++s) dup_cnt[s + 1] += dup_cnt[s];
+    const uint32_t dup_base = (uint32_t)P.dup_pairs.size();
+    P.dup_pairs.resize(dup_base + dup_cnt[nslots]);
+    std::vector<uint32_t> dup_fill(dup_cnt.begin(), dup_cnt.end() - 1);
+    for (uint32_t j = 0; j < nl; ++j) {
+      if (!P.point_var[point_base + j]) continue;
+      const uint32_t k0 = cnt[j], k1 = cnt[j + 1];
+      for (uint32_t a = k0; a < k1; ++a) {
+        const uint32_t sa = P.obs_slot[obs_base + a];
+        if (sa == kNone) continue;
+        for (uint32_t b = k0; b < k1; ++b) {
+          if (b == a) continue;
+          const uint32_t sb = P.obs_slot[obs_base + b];
+          if (sb == kNone) continue;
+          if (sa > sb) {
+            const uint32_t blk = key_count(sa - slot_base, sb - slot_base);
+            P.pairs[blk_fill[blk]++] = PairIdx{obs_base + a, obs_base + b};
+          } else if (sa == sb) {
+            P.dup_pairs[dup_base + dup_fill[sa - slot_base]++] = PairIdx{obs_base + a, obs_base + b};
+          }
+        }
+      }
+    }
+    for (uint32_t s = 0; s < nslots; ++s) P.dup_off.push_back(dup_base + dup_cnt[s + 1]);
+    // Tile-row partial lists: row sides (I, J <= I), then column sides (K > I, I).
+    for (uint32_t I = 0; I < ntr; ++I) {
+      for (uint32_t J = 0; J <= I; ++J) {
+        const uint32_t t = tile_id[(size_t)I * ntr + J];
+        if (t != kNone) P.tr_list.push_back(2 * t);
+      }
+      for (uint32_t K = I + 1; K < ntr; ++K) {
+        const uint32_t t = tile_id[(size_t)K * ntr + I];
+        if (t != kNone) P.tr_list.push_back(2 * t + 1);
+      }
+      P.tr_list_off.push_back((uint32_t)P.tr_list.size());
+      P.tr_prob.push_back(pi);
+    }
+    // Point chunks of at most 256 points.
+    for (uint32_t j0 = 0; j0 < nl; j0 += 256)
+      P.chunk_point_begin.push_back(point_base + std::min(nl, j0 + 256));
+    pose_base += np;
+    point_base += nl;
+    obs_base += no;
+    slot_base += nslots;
+    tr_base += ntr;
+    P.prob_pose_begin.push_back(pose_base);
+    P.prob_point_begin.push_back(point_base);
+    P.prob_obs_begin.push_back(obs_base);
+    P.prob_tr_begin.push_back(tr_base);
+    P.prob_chunk_begin.push_back((uint32_t)P.chunk_point_begin.size() - 1);
+    P.prob_camera_begin.push_back((uint32_t)P.cameras.size());
+  }
+  P.num_var_cams = slot_base;
+  P.num_tile_rows = tr_base;
+  P.num_pairs = P.pairs.size();
+  // Lanes per block in the off-diagonal assembly: about three points per
+  // lane (the mean pair count per block sets the shape).
+  const double mean = P.camera_pairs ? (double)P.num_pairs / (double)P.camera_pairs : 1.0;
+  uint32_t g = 1;
+  while (g < 32 && (double)(2 * g) * 3.0 <= mean + 1e-9) g *= 2;
+  P.group = g;
+}
+
+std::string check_plan(const Plan& P) {
+  const uint64_t nposes = P.pose_prob.size(), npts = P.point_prob.size(),
+                 nobs = P.obs_pose.size(), ncam = P.cameras.size(), nslots = P.num_var_cams;
+  const uint64_t ntiles = P.tile_ij.size();
+  const uint64_t tile_floats = (uint64_t)P.tb * P.tb * kBlock;
+  auto bad = [](const char* what) { return std::string("plan check failed: ") + what; };
+  if (P.pt_off.size() != npts + 1 || P.pt_off.back() != nobs) return bad("pt_off");
+  for (uint64_t j = 0; j < npts; ++j)
+    if (P.pt_off[j] > P.pt_off[j + 1]) return bad("pt_off order");
+  if (P.obs_cam.size() != nobs || P.obs_slot.size() != nobs || P.obs_xy.size() != 2 * nobs)
+    return bad("obs sizes");
+  for (uint64_t k = 0; k < nobs; ++k) {
+    if (P.obs_pose[k] >= nposes) return bad("obs_pose");
+    if (P.obs_cam[k] >= ncam) return bad("obs_cam");
+    if (P.obs_slot[k] != kNone && P.obs_slot[k] >= nslots) return bad("obs_slot");
+  }
+  for (uint64_t i = 0; i < nposes; ++i)
+    if (P.pose_slot[i] != kNone && P.pose_slot[i] >= nslots) return bad("pose_slot");
+  if (P.cam_off.size() != nslots + 1 || P.cam_off.back() != P.cam_obs.size()) return bad("cam_off");
+  for (uint64_t s = 0; s < nslots; ++s)
+    if (P.cam_off[s] > P.cam_off[s + 1]) return bad("cam_off order");
+  for (uint32_t k : P.cam_obs)
+    if (k >= nobs) return bad("cam_obs");
+  if (P.slot_prob.size() != nslots || nslots != (uint64_t)P.num_tile_rows * P.tb)
+    return bad("slots");
+  if (P.blk_off.size() != P.blk_dst.size() + 1 || P.blk_off.back() != P.pairs.size())
+    return bad("blk_off");
+  for (size_t b = 0; b + 1 < P.blk_off.size(); ++b)
+    if (P.blk_off[b] > P.blk_off[b + 1]) return bad("blk_off order");
+  for (const PairIdx& pr : P.pairs)
+    if (pr.a >= nobs || pr.b >= nobs) return bad("pairs");
+  for (const PairIdx& d : P.blk_dst) {
+    if ((uint64_t)d.a + kBlock > ntiles * tile_floats) return bad("blk_dst");
+    if (d.b != kNone && (uint64_t)d.b + kBlock > ntiles * tile_floats) return bad("blk_dst mirror");
+  }
+  if (P.diag_dst.size() != nslots) return bad("diag_dst size");
+  for (uint32_t d : P.diag_dst)
+    if ((uint64_t)d + kBlock > ntiles * tile_floats) return bad("diag_dst");
+  if (P.dup_off.size() != nslots + 1 || P.dup_off.back() != P.dup_pairs.size()) return bad("dup_off");
+  for (const PairIdx& pr : P.dup_pairs)
+    if (pr.a >= nobs || pr.b >= nobs) return bad("dup_pairs");
+  for (uint32_t ij : P.tile_ij)
+    if ((ij >> 16) >= P.num_tile_rows || (ij & 0xFFFFu) > (ij >> 16)) return bad("tile_ij");
+  if (P.tr_list_off.size() != (uint64_t)P.num_tile_rows + 1 || P.tr_list_off.back() != P.tr_list.size())
+    return bad("tr_list_off");
+  for (uint32_t e : P.tr_list)
+    if (e >= 2 * ntiles) return bad("tr_list");
+  if (P.tr_prob.size() != P.num_tile_rows) return bad("tr_prob");
+  for (uint32_t pr : P.tr_prob)
+    if (pr >= P.num_problems) return bad("tr_prob value");
+  if (P.chunk_point_begin.back() != npts) return bad("chunks");
+  for (size_t c = 0; c + 1 < P.chunk_point_begin.size(); ++c) {
+    const uint32_t lo = P.chunk_point_begin[c], hi = P.chunk_point_begin[c + 1];
+    if (lo >= hi || hi - lo > 256) return bad("chunk size");
+    if (P.point_prob[lo] != P.point_prob[hi - 1]) return bad("chunk spans problems");
+  }
+  if (P.prob_chunk_begin.size() != P.num_problems + 1u || P.prob_pose_begin.size() != P.num_problems + 1u ||
+      P.prob_tr_begin.size() != P.num_problems + 1u)
+    return bad("problem ranges");
+  return std::string();
+}
+
+size_t Plan::device_bytes() const {
+  const size_t npose = pose_prob.size(), npt = point_prob.size(), nobs = obs_pose.size();
+  size_t b = 0;
+  b += npose * (8 * (4 + 3 + 12) * 2 + 8 + 4 + 4);  // state x2, step, slot, prob
+  b += npt * (8 * 3 * 2 + 4 + 1 + 4 + 36 + 64);     // points x2, off, var, prob, pt_h, pt_s
+  b += nobs * (4 * 3 + 16 + 32 + 16);                // pose, cam, slot, xy, obs_h, obs_e
+  b += cam_obs.size() * 4 + pairs.size() * 8 + dup_pairs.size() * 8;
+  b += blk_dst.size() * (8 + 4);
+  b += tile_ij.size() * ((size_t)tb * tb * kBlock * 4 + 4 + 2 * (size_t)tb * 6 * 4);
+  b += (size_t)num_var_cams * (4 + 4 + 4 + 4 + 36 * 4 + 6 * 4 * 6);
+  b += tr_list.size() * 4 + (size_t)num_tile_rows * (4 + 4 + 16 * 8);
+  b += chunk_point_begin.size() * (4 + 8 + 8 + 8);
+  b += cameras.size() * sizeof(DevCamera);
+  return b;
+}
+
+double algorithmic_bytes(const Plan& P, double k, double* b_pcg_out) {
+  // Counts of the byte model: N_o variable observations, N_p variable
+  // points, N_c variable cameras, N_e camera pairs sharing a variable point.
+  const double No = (double)P.var_obs, Np = (double)P.var_points,
+               Nc = (double)P.real_var_cams, Ne = (double)P.camera_pairs;
+  const double b_lin = 88.0 * No + 48.0 * Np + 156.0 * Nc;
+  const double b_asm = 72.0 * No + 84.0 * Np + 144.0 * Ne + 168.0 * Nc;
+  const double b_pcg = 148.0 * Ne + 288.0 * Nc;
+  const double b_bs = 76.0 * No + 60.0 * Np;
+  const double b_cost = 16.0 * No + 36.0 * Np + 96.0 * Nc;
+  if (b_pcg_out) *b_pcg_out = b_pcg;
+  return b_lin + b_asm + k * b_pcg + b_bs + b_cost;
+}
+
+}  // namespace vlba

@@ -1,0 +1,89 @@
+// vlba_plan.h -- host-side construction of the device layout of one or more
+// bundle-adjustment problems (the analogue of GpuBundleAdjuster::upload,
+// crates/ba-gpu/src/solver.rs:253-385, extended to the explicit reduced
+// camera system and to batches).  Pure C++; no CUDA calls.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "vlba_common.cuh"
+
+namespace vlba {
+
+struct PairIdx {
+  uint32_t a, b;
+};
+
+struct Plan {
+  uint32_t tb = 16;
+  uint32_t group = 8;
+  uint32_t num_problems = 0;
+
+  std::vector<uint32_t> prob_pose_begin, prob_point_begin, prob_obs_begin, prob_tr_begin,
+      prob_chunk_begin, prob_camera_begin;
+  std::vector<uint32_t> pose_prob, point_prob, slot_prob;
+  std::vector<LmParams> params;
+
+  std::vector<double> pose_q, pose_t, points;
+  std::vector<uint32_t> pose_slot;
+  std::vector<uint8_t> point_var;
+  std::vector<DevCamera> cameras;
+
+  std::vector<uint32_t> pt_off, obs_pose, obs_cam, obs_slot;
+  std::vector<double> obs_xy;  // 2 per obs
+  std::vector<uint32_t> cam_off, cam_obs;
+
+  uint32_t num_var_cams = 0;  // padded slots
+  uint32_t num_tile_rows = 0;
+  std::vector<uint32_t> tile_ij;
+  std::vector<uint32_t> blk_off;
+  std::vector<PairIdx> pairs;
+  std::vector<PairIdx> blk_dst;
+  std::vector<uint32_t> diag_dst;
+  std::vector<uint32_t> dup_off;
+  std::vector<PairIdx> dup_pairs;
+  std::vector<uint32_t> tr_list_off, tr_list, tr_prob;
+  std::vector<uint32_t> chunk_point_begin;
+
+  // statistics (per plan)
+  uint64_t real_var_cams = 0;
+  uint64_t var_points = 0;
+  uint64_t var_obs = 0;          // observations with a variable point
+  uint64_t camera_pairs = 0;     // nonzero off-diagonal blocks (N_e)
+  uint64_t num_pairs = 0;        // point contributions to those blocks
+
+  size_t device_bytes() const;
+};
+
+// Per-problem outcome of validation (BaError order of lm.rs:168-229).
+struct Validation {
+  int status = VLBA_OK;
+  uint64_t error_index = 0;
+};
+
+// Resolve a vlba_camera into DevCamera; false if the model is outside the
+// radial pinhole family (the caller declines).
+bool resolve_camera(const vlba_camera& c, DevCamera* out);
+
+// Validate one problem and its config without building anything.
+Validation validate_problem(const vlba_problem* p, const vlba_config* cfg);
+
+LmParams make_params(const vlba_config* cfg);
+
+// Build the plan for `n` problems (all must have validated OK).  `tb` is the
+// tile size (8 or 16).  Throws std::runtime_error on internal inconsistency.
+void build_plan(const vlba_problem* const* problems, const vlba_config* const* configs,
+                uint32_t n, uint32_t tb, Plan* plan);
+
+// Bounds-check every index array of the plan against the arrays it indexes.
+// Returns an empty string when the plan is consistent.
+std::string check_plan(const Plan& plan);
+
+// Algorithmic bytes of one LM iteration (linearisation + one trial with
+// `pcg_iterations` PCG iterations) under the byte model of the headline
+// roofline: B_lin + B_asm + k B_pcg + B_bs + B_cost.
+double algorithmic_bytes(const Plan& plan, double pcg_iterations, double* b_pcg_out);
+
+}  // namespace vlba

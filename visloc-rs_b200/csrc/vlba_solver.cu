@@ -1,0 +1,576 @@
+// vlba_solver.cu -- solver context, device upload, the LM driver and the C ABI
+// of include/visloc_ba_cuda.h.
+//
+// The LM loop runs on the device (k_decide owns accept/reject and lambda);
+// the host only issues the per-iteration kernel sequence and polls a 4-byte
+// "all done" word per iteration.  The reference's host loop instead reads
+// back the step and evaluates the cost on the CPU every iteration
+// (crates/ba-gpu/src/solver.rs:514-548, 696-727).
+
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "vlba_kernels.cuh"
+#include "vlba_plan.h"
+
+namespace vlba {
+
+struct CudaError : std::runtime_error {
+  cudaError_t code;
+  CudaError(cudaError_t c, const char* what)
+      : std::runtime_error(std::string(what) + ": " + cudaGetErrorString(c)), code(c) {}
+};
+
+#define VLBA_CUDA(expr)                                   \
+  do {                                                    \
+    cudaError_t e_ = (expr);                              \
+    if (e_ != cudaSuccess) throw ::vlba::CudaError(e_, #expr);    \
+  } while (0)
+
+struct Status : std::runtime_error {
+  int code;
+  uint64_t index;
+  Status(int c, const std::string& m, uint64_t i = 0) : std::runtime_error(m), code(c), index(i) {}
+};
+
+// Device memory owned by a context.
+class Arena {
+ public:
+  ~Arena() { release(); }
+  template <typename T>
+  T* alloc(size_t count) {
+    if (count == 0) count = 1;
+    void* p = nullptr;
+    const cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      throw CudaError(e, "cudaMalloc");
+    }
+    ptrs_.push_back(p);
+    bytes_ += count * sizeof(T);
+    return static_cast<T*>(p);
+  }
+  template <typename T>
+  T* upload(const std::vector<T>& v, cudaStream_t s) {
+    T* p = alloc<T>(v.size());
+    if (!v.empty()) VLBA_CUDA(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+    return p;
+  }
+  void release() {
+    for (void* p : ptrs_) cudaFree(p);
+    ptrs_.clear();
+    bytes_ = 0;
+  }
+  size_t bytes() const { return bytes_; }
+
+ private:
+  std::vector<void*> ptrs_;
+  size_t bytes_ = 0;
+};
+
+struct Context {
+  int device = 0;
+  int sm_count = 148;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev[6] = {};
+  std::string error;
+  Arena arena;
+  Plan plan;
+  Dev dev;
+  bool uploaded = false;
+  int pcg_grid = 0;
+  uint32_t* h_done = nullptr;  // pinned poll word
+  // the uploaded problem's sizes (for download)
+  std::vector<uint64_t> num_poses, num_points;
+};
+
+namespace {
+
+void set_device(Context* c) { VLBA_CUDA(cudaSetDevice(c->device)); }
+
+// Upload a built plan: allocate and fill every device array of Dev.
+void upload_plan(Context* c, uint32_t max_records) {
+  Plan& P = c->plan;
+  cudaStream_t s = c->stream;
+  c->arena.release();
+  c->uploaded = false;
+  Dev d;
+  std::memset(&d, 0, sizeof d);
+  const size_t npose = P.pose_prob.size(), npt = P.point_prob.size(), nobs = P.obs_pose.size();
+  d.num_problems = P.num_problems;
+  d.num_poses = (uint32_t)npose;
+  d.num_points = (uint32_t)npt;
+  d.num_obs = (uint32_t)nobs;
+  d.num_var_cams = P.num_var_cams;
+  d.num_tile_rows = P.num_tile_rows;
+  d.num_tiles = (uint32_t)P.tile_ij.size();
+  d.num_offdiag_blocks = (uint32_t)P.blk_dst.size();
+  d.num_dup_pairs = (uint32_t)P.dup_pairs.size();
+  d.num_point_chunks = (uint32_t)P.chunk_point_begin.size() - 1;
+  d.tb = P.tb;
+  d.group = P.group;
+  Arena& A = c->arena;
+  d.prob_pose_begin = A.upload(P.prob_pose_begin, s);
+  d.prob_point_begin = A.upload(P.prob_point_begin, s);
+  d.prob_tr_begin = A.upload(P.prob_tr_begin, s);
+  d.prob_chunk_begin = A.upload(P.prob_chunk_begin, s);
+  d.pose_prob = A.upload(P.pose_prob, s);
+  d.point_prob = A.upload(P.point_prob, s);
+  d.slot_prob = A.upload(P.slot_prob, s);
+  d.params = A.upload(P.params, s);
+  d.ctrl = A.alloc<Ctrl>(P.num_problems);
+  d.pcg = A.alloc<PcgState>(P.num_problems);
+  d.max_records = max_records;
+  d.records = A.alloc<vlba_iteration>((size_t)P.num_problems * (max_records ? max_records : 1));
+  for (int b = 0; b < 2; ++b) {
+    d.pose_q[b] = A.alloc<double>(4 * npose);
+    d.pose_t[b] = A.alloc<double>(3 * npose);
+    d.pose_rt[b] = A.alloc<double>(12 * npose);
+    d.points[b] = A.alloc<double>(3 * npt);
+  }
+  VLBA_CUDA(cudaMemcpyAsync(d.pose_q[0], P.pose_q.data(), P.pose_q.size() * 8, cudaMemcpyHostToDevice, s));
+  VLBA_CUDA(cudaMemcpyAsync(d.pose_t[0], P.pose_t.data(), P.pose_t.size() * 8, cudaMemcpyHostToDevice, s));
+  VLBA_CUDA(cudaMemcpyAsync(d.points[0], P.points.data(), P.points.size() * 8, cudaMemcpyHostToDevice, s));
+  d.pose_slot = A.upload(P.pose_slot, s);
+  d.point_var = A.upload(P.point_var, s);
+  d.pose_step = A.alloc<double>(npose);
+  d.cameras = A.upload(P.cameras, s);
+  d.pt_off = A.upload(P.pt_off, s);
+  d.obs_pose = A.upload(P.obs_pose, s);
+  d.obs_cam = A.upload(P.obs_cam, s);
+  d.obs_slot = A.upload(P.obs_slot, s);
+  {
+    double2* xy = A.alloc<double2>(nobs);
+    if (nobs) VLBA_CUDA(cudaMemcpyAsync(xy, P.obs_xy.data(), nobs * 16, cudaMemcpyHostToDevice, s));
+    d.obs_xy = xy;
+  }
+  d.obs_h = A.alloc<float4>(2 * nobs);
+  d.obs_e = A.alloc<float4>(nobs);
+  d.cam_off = A.upload(P.cam_off, s);
+  d.cam_obs = A.upload(P.cam_obs, s);
+  d.pt_h = A.alloc<float>(9 * npt);
+  d.pt_s = A.alloc<float4>(4 * npt);
+  d.cam_hpp = nullptr;
+  const size_t tile_floats = (size_t)P.tb * P.tb * kBlock;
+  d.tiles = A.alloc<float>(P.tile_ij.size() * tile_floats);
+  VLBA_CUDA(cudaMemsetAsync(d.tiles, 0, P.tile_ij.size() * tile_floats * 4, s));
+  d.tile_ij = A.upload(P.tile_ij, s);
+  d.blk_off = A.upload(P.blk_off, s);
+  d.pairs = reinterpret_cast<const uint2*>(A.upload(P.pairs, s));
+  d.blk_dst = reinterpret_cast<const uint2*>(A.upload(P.blk_dst, s));
+  d.diag_dst = A.upload(P.diag_dst, s);
+  d.dup_off = A.upload(P.dup_off, s);
+  d.dup_pairs = reinterpret_cast<const uint2*>(A.upload(P.dup_pairs, s));
+  const size_t nvec = (size_t)P.num_var_cams * 6;
+  d.minv = A.alloc<float>(36 * (size_t)P.num_var_cams);
+  d.rhs = A.alloc<float>(nvec);
+  d.x = A.alloc<float>(nvec);
+  d.r = A.alloc<float>(nvec);
+  d.z = A.alloc<float>(nvec);
+  d.p = A.alloc<float>(nvec);
+  d.q = A.alloc<float>(nvec);
+  VLBA_CUDA(cudaMemsetAsync(d.x, 0, nvec * 4 + 4, s));
+  d.partial = A.alloc<float>(P.tile_ij.size() * 2 * (size_t)P.tb * 6);
+  d.tr_list_off = A.upload(P.tr_list_off, s);
+  d.tr_list = A.upload(P.tr_list, s);
+  d.tr_prob = A.upload(P.tr_prob, s);
+  d.dots = A.alloc<double>(16 * (size_t)(P.num_tile_rows ? P.num_tile_rows : 1));
+  d.barrier = A.alloc<unsigned int>(4);
+  d.error = A.alloc<unsigned int>(1);
+  VLBA_CUDA(cudaMemsetAsync(d.barrier, 0, 16, s));
+  VLBA_CUDA(cudaMemsetAsync(d.error, 0, 4, s));
+  d.chunk_point_begin = A.upload(P.chunk_point_begin, s);
+  const size_t nch = P.chunk_point_begin.size() - 1;
+  d.chunk_cost = A.alloc<double>(nch);
+  d.chunk_bad = A.alloc<unsigned long long>(nch);
+  d.chunk_step = A.alloc<double>(nch);
+  c->dev = d;
+  c->pcg_grid = P.num_tile_rows ? pcg_grid_size((int)P.tb, c->sm_count) : 0;
+  if (P.num_tile_rows && c->pcg_grid <= 0)
+    throw Status(VLBA_ERR_CUDA, "the PCG kernel cannot be made co-resident on this device");
+  VLBA_CUDA(cudaStreamSynchronize(s));
+  c->uploaded = true;
+}
+
+// Reset the state to the uploaded initial values and the LM control words.
+void reset_state(Context* c) {
+  Dev& d = c->dev;
+  const Plan& P = c->plan;
+  cudaStream_t s = c->stream;
+  VLBA_CUDA(cudaMemcpyAsync(d.pose_q[0], P.pose_q.data(), P.pose_q.size() * 8, cudaMemcpyHostToDevice, s));
+  VLBA_CUDA(cudaMemcpyAsync(d.pose_t[0], P.pose_t.data(), P.pose_t.size() * 8, cudaMemcpyHostToDevice, s));
+  VLBA_CUDA(cudaMemcpyAsync(d.points[0], P.points.data(), P.points.size() * 8, cudaMemcpyHostToDevice, s));
+  VLBA_CUDA(cudaMemsetAsync(d.ctrl, 0, sizeof(Ctrl) * P.num_problems, s));
+  VLBA_CUDA(cudaMemsetAsync(d.error, 0, 4, s));
+}
+
+void check_launch(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) throw CudaError(e, what);
+}
+
+struct RunStats {
+  double device_ms = 0.0;
+};
+
+// The device LM loop over all uploaded problems.
+RunStats run_lm(Context* c, bool profile, std::vector<double>* lin_ms, std::vector<double>* solve_ms) {
+  Dev& d = c->dev;
+  cudaStream_t s = c->stream;
+  uint32_t max_iters = 0;
+  for (const LmParams& lp : c->plan.params) max_iters = std::max(max_iters, lp.max_iterations);
+  RunStats st;
+  VLBA_CUDA(cudaEventRecord(c->ev[0], s));
+  check_launch(launch_pose_table(d, s), "pose table");
+  check_launch(launch_cost(d, false, s), "initial cost");
+  check_launch(launch_decide(d, true, s), "init");
+  for (uint32_t it = 0; it < max_iters; ++it) {
+    if (profile) VLBA_CUDA(cudaEventRecord(c->ev[2], s));
+    check_launch(launch_linearize(d, s), "linearize");
+    if (profile) VLBA_CUDA(cudaEventRecord(c->ev[3], s));
+    check_launch(launch_point_prep(d, s), "point prep");
+    check_launch(launch_offdiag(d, s), "off-diagonal blocks");
+    check_launch(launch_cam_diag(d, s), "camera blocks");
+    check_launch(launch_pcg_setup(d, s), "pcg setup");
+    check_launch(launch_pcg(d, c->pcg_grid, s), "pcg");
+    check_launch(launch_pose_update(d, s), "pose update");
+    check_launch(launch_cost(d, true, s), "trial cost");
+    check_launch(launch_decide(d, false, s), "decide");
+    if (profile) VLBA_CUDA(cudaEventRecord(c->ev[4], s));
+    // Poll the per-problem control words (one small copy per iteration).
+    std::vector<Ctrl> ctrl(c->plan.num_problems);
+    VLBA_CUDA(cudaMemcpyAsync(ctrl.data(), d.ctrl, sizeof(Ctrl) * ctrl.size(), cudaMemcpyDeviceToHost, s));
+    unsigned int err = 0;
+    VLBA_CUDA(cudaMemcpyAsync(&err, d.error, 4, cudaMemcpyDeviceToHost, s));
+    VLBA_CUDA(cudaStreamSynchronize(s));
+    if (profile) {
+      float a = 0.f, b = 0.f;
+      VLBA_CUDA(cudaEventElapsedTime(&a, c->ev[2], c->ev[3]));
+      VLBA_CUDA(cudaEventElapsedTime(&b, c->ev[3], c->ev[4]));
+      lin_ms->push_back(a);
+      solve_ms->push_back(b);
+    }
+    if (err) throw Status(VLBA_ERR_TIMEOUT, "a bounded device wait gave up (error bits " + std::to_string(err) + ")");
+    bool all_done = true;
+    for (const Ctrl& x : ctrl) all_done = all_done && x.done;
+    if (all_done) break;
+  }
+  VLBA_CUDA(cudaEventRecord(c->ev[1], s));
+  VLBA_CUDA(cudaEventSynchronize(c->ev[1]));
+  float ms = 0.f;
+  VLBA_CUDA(cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]));
+  st.device_ms = ms;
+  return st;
+}
+
+void fill_result(Context* c, uint32_t prob, vlba_result* res, vlba_iteration* its, uint32_t cap,
+                 const std::vector<double>* lin_ms, const std::vector<double>* solve_ms) {
+  Ctrl ctrl;
+  VLBA_CUDA(cudaMemcpy(&ctrl, c->dev.ctrl + prob, sizeof ctrl, cudaMemcpyDeviceToHost));
+  if (res) {
+    res->initial_cost = ctrl.initial_cost;
+    res->final_cost = ctrl.current_cost;
+    res->converged = ctrl.converged;
+    res->num_iterations = ctrl.iteration;
+    res->initial_nonprojectable = ctrl.initial_nonproj;
+    res->final_nonprojectable = ctrl.current_nonproj;
+    res->total_pcg_iterations = ctrl.total_pcg;
+  }
+  const uint32_t n = std::min(std::min(ctrl.iteration, cap), c->dev.max_records);
+  if (its && n) {
+    VLBA_CUDA(cudaMemcpy(its, c->dev.records + (size_t)prob * c->dev.max_records,
+                         n * sizeof(vlba_iteration), cudaMemcpyDeviceToHost));
+    if (lin_ms)
+      for (uint32_t i = 0; i < n && i < lin_ms->size(); ++i) its[i].linearize_ms = (*lin_ms)[i];
+    if (solve_ms)
+      for (uint32_t i = 0; i < n && i < solve_ms->size(); ++i) its[i].solve_ms = (*solve_ms)[i];
+  }
+}
+
+void download_problem(Context* c, uint32_t prob, vlba_problem* p) {
+  Ctrl ctrl;
+  VLBA_CUDA(cudaMemcpy(&ctrl, c->dev.ctrl + prob, sizeof ctrl, cudaMemcpyDeviceToHost));
+  const uint32_t b = ctrl.cur;
+  const uint32_t pose0 = c->plan.prob_pose_begin[prob], pt0 = c->plan.prob_point_begin[prob];
+  const size_t np = c->plan.prob_pose_begin[prob + 1] - pose0;
+  const size_t nl = c->plan.prob_point_begin[prob + 1] - pt0;
+  if (np != p->num_poses || nl != p->num_landmarks)
+    throw Status(VLBA_ERR_INVALID_ARGUMENT, "download: problem sizes differ from the upload");
+  VLBA_CUDA(cudaMemcpy(p->pose_q, c->dev.pose_q[b] + 4 * (size_t)pose0, np * 32, cudaMemcpyDeviceToHost));
+  VLBA_CUDA(cudaMemcpy(p->pose_t, c->dev.pose_t[b] + 3 * (size_t)pose0, np * 24, cudaMemcpyDeviceToHost));
+  VLBA_CUDA(cudaMemcpy(p->landmarks, c->dev.points[b] + 3 * (size_t)pt0, nl * 24, cudaMemcpyDeviceToHost));
+}
+
+int pick_tb(const vlba_problem* const* probs, uint32_t n) {
+  // Tile size: 16 blocks for cameras counts that fill 16-wide tile rows,
+  // 8 for small windows (less zero fill in their dense tiles).
+  uint64_t vars = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    const vlba_problem* p = probs[i];
+    uint64_t v = 0;
+    for (uint64_t k = 0; k < p->num_poses; ++k) v += !(p->pose_fixed && p->pose_fixed[k]);
+    vars += v;
+  }
+  const double mean = n ? (double)vars / n : 0.0;
+  return mean >= 48.0 ? 16 : 8;
+}
+
+template <typename F>
+int guarded(Context* c, F&& f) {
+  try {
+    if (c) c->error.clear();
+    f();
+    return VLBA_OK;
+  } catch (const Status& s) {
+    if (c) c->error = s.what();
+    return s.code;
+  } catch (const CudaError& e) {
+    if (c) c->error = e.what();
+    return e.code == cudaErrorMemoryAllocation ? VLBA_ERR_OUT_OF_MEMORY : VLBA_ERR_CUDA;
+  } catch (const std::bad_alloc&) {
+    if (c) c->error = "host allocation failed";
+    return VLBA_ERR_OUT_OF_MEMORY;
+  } catch (const std::exception& e) {
+    if (c) c->error = e.what();
+    return VLBA_ERR_INVALID_ARGUMENT;
+  }
+}
+
+void do_upload(Context* c, const vlba_problem* const* probs, const vlba_config* const* cfgs,
+               uint32_t n, uint32_t max_records, double* upload_ms) {
+  const auto t0 = std::chrono::steady_clock::now();
+  for (uint32_t i = 0; i < n; ++i) {
+    const Validation v = validate_problem(probs[i], cfgs[i]);
+    if (v.status != VLBA_OK)
+      throw Status(v.status, "problem " + std::to_string(i) + " failed validation", v.error_index);
+  }
+  set_device(c);
+  build_plan(probs, cfgs, n, (uint32_t)pick_tb(probs, n), &c->plan);
+  const std::string bad = check_plan(c->plan);
+  if (!bad.empty()) throw Status(VLBA_ERR_INVALID_ARGUMENT, bad);
+  upload_plan(c, max_records);
+  c->num_poses.clear();
+  c->num_points.clear();
+  for (uint32_t i = 0; i < n; ++i) {
+    c->num_poses.push_back(probs[i]->num_poses);
+    c->num_points.push_back(probs[i]->num_landmarks);
+  }
+  const auto t1 = std::chrono::steady_clock::now();
+  if (upload_ms) *upload_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+}
+
+}  // namespace
+}  // namespace vlba
+
+using vlba::Context;
+
+extern "C" {
+
+uint32_t visloc_ba_cuda_abi_version(void) { return VLBA_ABI_VERSION; }
+
+void visloc_ba_cuda_default_config(vlba_config* out) {
+  if (!out) return;
+  std::memset(out, 0, sizeof *out);
+  out->max_iterations = 20;
+  out->has_initial_lambda = 1;
+  out->initial_lambda = 1e-4;
+  out->lambda_increase_factor = 10.0;
+  out->lambda_decrease_factor = 0.1;
+  out->max_lambda = 1e12;
+  out->min_lambda = 1e-9;
+  out->step_tolerance = 1e-7;
+  out->cost_tolerance = 1e-9;
+  out->has_relative_cost_tolerance = 0;
+  out->relative_cost_tolerance = 0.0;
+  out->robust_kernel = VLBA_KERNEL_NONE;
+  out->robust_parameter = 0.0;
+  out->max_pcg_iterations = 100;
+  out->pcg_relative_tolerance = 1e-4;
+  out->flags = 0;
+}
+
+void* visloc_ba_cuda_create(int device) {
+  auto* c = new (std::nothrow) Context();
+  if (!c) return nullptr;
+  c->device = device;
+  try {
+    int count = 0;
+    VLBA_CUDA(cudaGetDeviceCount(&count));
+    if (device < 0 || device >= count) throw std::runtime_error("no such device");
+    VLBA_CUDA(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    VLBA_CUDA(cudaGetDeviceProperties(&prop, device));
+    if (prop.major < 10) throw std::runtime_error("requires an sm_100 (Blackwell) device");
+    c->sm_count = prop.multiProcessorCount;
+    VLBA_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    for (auto& e : c->ev) VLBA_CUDA(cudaEventCreate(&e));
+  } catch (...) {
+    delete c;
+    return nullptr;
+  }
+  return c;
+}
+
+void visloc_ba_cuda_destroy(void* ctx) {
+  auto* c = static_cast<Context*>(ctx);
+  if (!c) return;
+  cudaSetDevice(c->device);
+  c->arena.release();
+  for (auto& e : c->ev)
+    if (e) cudaEventDestroy(e);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+const char* visloc_ba_cuda_last_error(void* ctx) {
+  auto* c = static_cast<Context*>(ctx);
+  return c ? c->error.c_str() : "null context";
+}
+
+int visloc_ba_cuda_check(const vlba_problem* problem, const vlba_config* config,
+                         uint64_t* error_index) {
+  const vlba::Validation v = vlba::validate_problem(problem, config);
+  if (error_index) *error_index = v.error_index;
+  return v.status;
+}
+
+int visloc_ba_cuda_upload(void* ctx, const vlba_problem* problem, const vlba_config* config) {
+  auto* c = static_cast<Context*>(ctx);
+  if (!c) return VLBA_ERR_INVALID_ARGUMENT;
+  return vlba::guarded(c, [&] {
+    const vlba_problem* probs[1] = {problem};
+    const vlba_config* cfgs[1] = {config};
+    vlba::do_upload(c, probs, cfgs, 1, config ? config->max_iterations : 0, nullptr);
+  });
+}
+
+int visloc_ba_cuda_solve_uploaded(void* ctx, const vlba_config* config, vlba_result* result,
+                                  vlba_iteration* iterations, uint32_t iterations_capacity) {
+  auto* c = static_cast<Context*>(ctx);
+  if (!c) return VLBA_ERR_INVALID_ARGUMENT;
+  return vlba::guarded(c, [&] {
+    if (!c->uploaded) throw vlba::Status(VLBA_ERR_INVALID_ARGUMENT, "nothing uploaded");
+    vlba::set_device(c);
+    if (config) {
+      vlba::LmParams lp = vlba::make_params(config);
+      if (lp.max_iterations > c->dev.max_records)
+        throw vlba::Status(VLBA_ERR_INVALID_ARGUMENT, "max_iterations exceeds the uploaded capacity");
+      VLBA_CUDA(cudaMemcpyAsync(const_cast<vlba::LmParams*>(c->dev.params), &lp, sizeof lp,
+                                cudaMemcpyHostToDevice, c->stream));
+      c->plan.params[0] = lp;
+    }
+    vlba::reset_state(c);
+    const bool profile = config && (config->flags & VLBA_FLAG_PROFILE);
+    std::vector<double> lin, sol;
+    const vlba::RunStats st = vlba::run_lm(c, profile, &lin, &sol);
+    if (result) std::memset(result, 0, sizeof *result);
+    vlba::fill_result(c, 0, result, iterations, iterations_capacity, profile ? &lin : nullptr,
+                      profile ? &sol : nullptr);
+    if (result) result->device_ms = st.device_ms;
+  });
+}
+
+int visloc_ba_cuda_download(void* ctx, vlba_problem* problem) {
+  auto* c = static_cast<Context*>(ctx);
+  if (!c || !problem) return VLBA_ERR_INVALID_ARGUMENT;
+  return vlba::guarded(c, [&] {
+    if (!c->uploaded) throw vlba::Status(VLBA_ERR_INVALID_ARGUMENT, "nothing uploaded");
+    vlba::set_device(c);
+    vlba::download_problem(c, 0, problem);
+  });
+}
+
+int visloc_ba_cuda_optimize(void* ctx, vlba_problem* problem, const vlba_config* config,
+                            vlba_result* result, vlba_iteration* iterations,
+                            uint32_t iterations_capacity) {
+  auto* c = static_cast<Context*>(ctx);
+  if (!c) return VLBA_ERR_INVALID_ARGUMENT;
+  if (result) std::memset(result, 0, sizeof *result);
+  double upload_ms = 0.0;
+  int st = vlba::guarded(c, [&] {
+    const vlba_problem* probs[1] = {problem};
+    const vlba_config* cfgs[1] = {config};
+    vlba::do_upload(c, probs, cfgs, 1, config ? config->max_iterations : 0, &upload_ms);
+  });
+  if (st != VLBA_OK) {
+    if (result && (st == VLBA_ERR_MISSING_POSE || st == VLBA_ERR_MISSING_LANDMARK)) {
+      uint64_t idx = 0;
+      vlba::validate_problem(problem, config);
+      visloc_ba_cuda_check(problem, config, &idx);
+      result->error_index = idx;
+    }
+    return st;
+  }
+  st = visloc_ba_cuda_solve_uploaded(ctx, nullptr, result, iterations, iterations_capacity);
+  if (st != VLBA_OK) return st;
+  if (result) result->upload_ms = upload_ms;
+  return visloc_ba_cuda_download(ctx, problem);
+}
+
+int visloc_ba_cuda_plan(const vlba_problem* problem, const vlba_config* config,
+                        double pcg_iterations, vlba_plan_info* info) {
+  return vlba::guarded(nullptr, [&] {
+    const vlba::Validation v = vlba::validate_problem(problem, config);
+    if (v.status != VLBA_OK) throw vlba::Status(v.status, "validation", v.error_index);
+    const vlba_problem* probs[1] = {problem};
+    const vlba_config* cfgs[1] = {config};
+    vlba::Plan plan;
+    vlba::build_plan(probs, cfgs, 1, (uint32_t)vlba::pick_tb(probs, 1), &plan);
+    const std::string bad = vlba::check_plan(plan);
+    if (!bad.empty()) throw vlba::Status(VLBA_ERR_INVALID_ARGUMENT, bad);
+    if (info) {
+      std::memset(info, 0, sizeof *info);
+      info->variable_cameras = plan.real_var_cams;
+      info->variable_landmarks = plan.var_points;
+      info->variable_observations = plan.var_obs;
+      info->camera_pairs = plan.camera_pairs;
+      info->schur_terms = plan.num_pairs;
+      info->tile_size = plan.tb;
+      info->tile_rows = plan.num_tile_rows;
+      info->tiles = (uint32_t)plan.tile_ij.size();
+      info->assembly_lanes = plan.group;
+      info->device_bytes = plan.device_bytes();
+      double b_pcg = 0.0;
+      info->bytes_per_iteration = vlba::algorithmic_bytes(plan, pcg_iterations, &b_pcg);
+      info->bytes_per_pcg_iteration = b_pcg;
+    }
+  });
+}
+
+int visloc_ba_cuda_cost(void* ctx, const vlba_problem* problem, const vlba_config* config,
+                        double* cost, uint64_t* nonprojectable) {
+  auto* c = static_cast<Context*>(ctx);
+  if (!c) return VLBA_ERR_INVALID_ARGUMENT;
+  return vlba::guarded(c, [&] {
+    vlba_config cfg = *config;
+    cfg.max_iterations = 0;
+    const vlba_problem* probs[1] = {problem};
+    const vlba_config* cfgs[1] = {&cfg};
+    const vlba::Validation v = vlba::validate_problem(problem, &cfg);
+    if (v.status != VLBA_OK && v.status != VLBA_ERR_ALL_POSES_FIXED)
+      throw vlba::Status(v.status, "validation", v.error_index);
+    vlba::set_device(c);
+    vlba::build_plan(probs, cfgs, 1, 8, &c->plan);
+    const std::string bad = vlba::check_plan(c->plan);
+    if (!bad.empty()) throw vlba::Status(VLBA_ERR_INVALID_ARGUMENT, bad);
+    vlba::upload_plan(c, 1);
+    vlba::reset_state(c);
+    vlba::Dev& d = c->dev;
+    vlba::check_launch(vlba::launch_pose_table(d, c->stream), "pose table");
+    vlba::check_launch(vlba::launch_cost(d, false, c->stream), "cost");
+    vlba::check_launch(vlba::launch_decide(d, true, c->stream), "cost reduce");
+    vlba::Ctrl ctrl;
+    VLBA_CUDA(cudaMemcpyAsync(&ctrl, d.ctrl, sizeof ctrl, cudaMemcpyDeviceToHost, c->stream));
+    VLBA_CUDA(cudaStreamSynchronize(c->stream));
+    if (cost) *cost = ctrl.initial_cost;
+    if (nonprojectable) *nonprojectable = ctrl.initial_nonproj;
+  });
+}
+
+}  // extern "C"

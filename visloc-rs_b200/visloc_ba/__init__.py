@@ -1,0 +1,24 @@
+"""visloc_ba: B200 bundle-adjustment solver (host side).
+
+The solver itself is the CUDA library libvisloc_ba_cuda.so built from
+../csrc; this package mirrors the reference's BA API (problem.py) and binds
+the library's C ABI (_abi.py, solver.py).
+"""
+
+from .problem import (  # noqa: F401
+    SE3,
+    BaConfig,
+    BaError,
+    BaIterationStats,
+    BaObservation,
+    BaResult,
+    BaRigObservation,
+    BaScope,
+    BundleAdjustment,
+    Camera,
+    CameraModel,
+    PackedProblem,
+    Pose,
+    RobustKernel,
+    quat_from_axis_angle,
+)

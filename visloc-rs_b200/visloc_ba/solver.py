@@ -1,0 +1,201 @@
+"""Binding of the CUDA solver's C ABI and the accelerator plug-in.
+
+`GpuBundleAdjuster` mirrors the reference's plug-in
+(crates/ba-gpu/src/solver.rs:80-85 and its `impl BaAccelerator`, :729-742):
+`optimize(ba, config, scope)` returns None when it declines (the caller then
+runs its CPU solver) and raises BaError for the reference's error variants.
+"""
+
+from __future__ import annotations
+
+import copy
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+from . import _abi
+from .problem import (
+    BaConfig,
+    BaError,
+    BaResult,
+    BaScope,
+    BundleAdjustment,
+    PackedProblem,
+    result_from_abi,
+)
+
+_ERROR_KIND = {
+    _abi.ERR_NO_POSES: "NoPoses",
+    _abi.ERR_NO_LANDMARKS: "NoLandmarks",
+    _abi.ERR_NO_OBSERVATIONS: "NoObservations",
+    _abi.ERR_ALL_POSES_FIXED: "AllPosesFixed",
+    _abi.ERR_MISSING_POSE: "MissingPose",
+    _abi.ERR_MISSING_LANDMARK: "MissingLandmark",
+    _abi.ERR_UNSUPPORTED_CAMERA_MODEL: "UnsupportedCameraModel",
+    _abi.ERR_SINGULAR_SYSTEM: "SingularSystem",
+}
+
+
+class SolverError(RuntimeError):
+    """A non-BaError failure of the CUDA library (CUDA error, timeout...)."""
+
+    def __init__(self, status: int, message: str):
+        self.status = status
+        super().__init__(f"{_abi.STATUS_NAMES.get(status, status)}: {message}")
+
+
+class CudaSolver:
+    """One solver context (device memory, stream) of libvisloc_ba_cuda.so."""
+
+    def __init__(self, device: int = 0, library: str | None = None):
+        self.lib = _abi.load_solver_library(library)
+        self.ctx = self.lib.visloc_ba_cuda_create(int(device))
+        if not self.ctx:
+            raise RuntimeError(
+                "visloc_ba_cuda_create failed: no CUDA device of compute capability 10.x"
+            )
+
+    def close(self):
+        if getattr(self, "ctx", None):
+            self.lib.visloc_ba_cuda_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def last_error(self) -> str:
+        return self.lib.visloc_ba_cuda_last_error(self.ctx).decode()
+
+    def _iters(self, config: BaConfig):
+        cap = max(1, int(config.max_iterations))
+        return (_abi.Iteration * cap)(), cap
+
+    def optimize(self, packed: PackedProblem, config: BaConfig):
+        """LM solve in place on `packed`.  Returns (status, BaResult|None)."""
+        prob = packed.abi()
+        cfg = config.to_abi()
+        res = _abi.Result()
+        iters, cap = self._iters(config)
+        st = self.lib.visloc_ba_cuda_optimize(self.ctx, C.byref(prob), C.byref(cfg),
+                                              C.byref(res), iters, cap)
+        if st != _abi.OK:
+            return st, res
+        return st, result_from_abi(res, iters, res.num_iterations)
+
+    def upload(self, packed: PackedProblem, config: BaConfig) -> int:
+        return self.lib.visloc_ba_cuda_upload(self.ctx, C.byref(packed.abi()),
+                                              C.byref(config.to_abi()))
+
+    def solve_uploaded(self, config: BaConfig | None = None):
+        res = _abi.Result()
+        cfg = config or BaConfig()
+        iters, cap = self._iters(cfg)
+        cfg_ptr = C.byref(config.to_abi()) if config is not None else None
+        st = self.lib.visloc_ba_cuda_solve_uploaded(self.ctx, cfg_ptr, C.byref(res), iters, cap)
+        if st != _abi.OK:
+            return st, res
+        return st, result_from_abi(res, iters, res.num_iterations)
+
+    def download(self, packed: PackedProblem) -> int:
+        return self.lib.visloc_ba_cuda_download(self.ctx, C.byref(packed.abi()))
+
+    def cost(self, packed: PackedProblem, config: BaConfig | None = None):
+        config = config or BaConfig()
+        c = C.c_double()
+        n = C.c_uint64()
+        st = self.lib.visloc_ba_cuda_cost(self.ctx, C.byref(packed.abi()),
+                                          C.byref(config.to_abi()), C.byref(c), C.byref(n))
+        if st != _abi.OK:
+            raise SolverError(st, self.last_error())
+        return c.value, n.value
+
+
+def check(packed: PackedProblem, config: BaConfig | None = None):
+    """Validation only (no device needed): (status, error_index)."""
+    lib = _abi.load_solver_library()
+    idx = C.c_uint64()
+    st = lib.visloc_ba_cuda_check(C.byref(packed.abi()), C.byref((config or BaConfig()).to_abi()),
+                                  C.byref(idx))
+    return st, idx.value
+
+
+def plan(packed: PackedProblem, config: BaConfig | None = None, pcg_iterations: float = 40.0):
+    """Host-only device layout of a problem (no device needed): (status, PlanInfo)."""
+    lib = _abi.load_solver_library()
+    info = _abi.PlanInfo()
+    st = lib.visloc_ba_cuda_plan(C.byref(packed.abi()), C.byref((config or BaConfig()).to_abi()),
+                                 float(pcg_iterations), C.byref(info))
+    return st, info
+
+
+def _env_num(name, cast, default):
+    try:
+        return cast(os.environ[name])
+    except (KeyError, ValueError):
+        return default
+
+
+@dataclass
+class GpuBaSettings:
+    """PCG controls of each LM linear solve (solver.rs:25-50)."""
+
+    max_pcg_iterations: int = 100
+    pcg_relative_tolerance: float = 1e-4
+    local_windows: bool = False
+
+    @staticmethod
+    def from_env() -> "GpuBaSettings":
+        return GpuBaSettings(
+            _env_num("VISLOC_BA_GPU_PCG_ITERS", int, 100),
+            _env_num("VISLOC_BA_GPU_PCG_TOL", float, 1e-4),
+            "VISLOC_BA_GPU_LOCAL" in os.environ,
+        )
+
+
+class GpuBundleAdjuster:
+    """The BaAccelerator of this solver (drop-in for crates/ba-gpu)."""
+
+    def __init__(self, device: int = 0, settings: GpuBaSettings | None = None):
+        self.solver = CudaSolver(device)
+        self.settings = settings or GpuBaSettings.from_env()
+
+    def _config(self, config: BaConfig) -> BaConfig:
+        cfg = copy.copy(config)
+        cfg.max_pcg_iterations = self.settings.max_pcg_iterations
+        cfg.pcg_relative_tolerance = self.settings.pcg_relative_tolerance
+        return cfg
+
+    def solve(self, ba: BundleAdjustment, config: BaConfig) -> BaResult:
+        """BundleAdjustment::optimize semantics: mutate `ba`, return BaResult,
+        raise BaError.  Raises SolverError when the library declines."""
+        packed, pose_ids, lm_ids, missing = ba.pack()
+        cfg = self._config(config)
+        st, res = self.solver.optimize(packed, cfg)
+        if st in (_abi.ERR_MISSING_POSE, _abi.ERR_MISSING_LANDMARK) and missing is not None:
+            raise missing
+        if st in _ERROR_KIND:
+            raise BaError(_ERROR_KIND[st])
+        if st != _abi.OK:
+            raise SolverError(st, self.solver.last_error())
+        ba.unpack(packed, pose_ids, lm_ids)
+        return res
+
+    def optimize(self, ba: BundleAdjustment, config: BaConfig, scope: BaScope = BaScope.GLOBAL):
+        """BaAccelerator::optimize: None = declined (run the CPU solver)."""
+        if scope == BaScope.LOCAL and not self.settings.local_windows:
+            return None
+        try:
+            return self.solve(ba, config)
+        except SolverError as e:
+            if e.status == _abi.DECLINED:
+                return None
+            raise
