@@ -1,0 +1,370 @@
+#!/usr/bin/env python
+"""Benchmark: LM iterations/s and observations/s of the 4M-observation bundle
+adjustment on B200, with the HBM roofline fraction of the dominant kernel.
+
+Workload (default `ring-4m`): 1,200 cameras on a ring with shared pinhole
+intrinsics (6000x4000), 500,000 points in a 10 m cube, track lengths geometric
+(mean 8, clipped to [2, 60]) -> ~4.06M observations; pixel noise N(0,1),
+2% outliers within +-50 px, poses perturbed 0.01 rad / 0.05 m, Huber 1 px,
+30 LM iterations, PCG tolerance 1e-6.  Inputs are seeded synthetic data
+(no data set is needed or used).
+
+One step = one LM solve (all its iterations) from the same initial state.
+`value` times steps on the device with the problem resident in HBM (events
+on the solver's stream inside the library); `e2e` times the C-ABI call
+`visloc_ba_cuda_optimize` with host buffers (host-side planning, H2D, LM,
+D2H).  With --gpus N every rank solves its own problem (replicas, weak
+scaling); the reported time is the max over ranks.
+
+--impl reference times the CPU restatement of the reference solver (the FP64
+oracle, OpenMP over all host cores): one LM iteration of the same workload
+per step.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "visloc-rs_b200"))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+FALLBACK_HBM_GBS = 6650.0
+PCG_KERNEL = "k_pcg"
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="ring-4m", choices=["ring-4m", "ring-50"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------- workloads
+def make_workload(name: str, rank: int):
+    from visloc_ba import BaConfig, RobustKernel, synth
+
+    if name == "ring-4m":
+        problem = synth.large_ring_problem(seed=2000 + rank)
+        cfg = BaConfig(max_iterations=30, robust_kernel=RobustKernel.huber(1.0),
+                       max_pcg_iterations=200, pcg_relative_tolerance=1e-6)
+        desc = {"workload": "ring-4m", "cameras": 1200, "points": 500_000,
+                "observations": int(problem.num_observations), "image": "6000x4000",
+                "lm_iterations": 30, "pcg_tolerance": 1e-6, "robust": "huber(1px)",
+                "track_length": "geometric mean 8, [2,60]"}
+    else:
+        problem = synth.ring_problem(50, 5000, seed=1001 + rank)
+        cfg = BaConfig(max_iterations=20, robust_kernel=RobustKernel.huber(1.0),
+                       max_pcg_iterations=200, pcg_relative_tolerance=1e-6)
+        desc = {"workload": "ring-50", "cameras": 50, "points": 5000,
+                "observations": int(problem.num_observations), "image": "640x480",
+                "lm_iterations": 20, "robust": "huber(1px)"}
+    return problem, cfg, desc
+
+
+# ------------------------------------------------------------- distributed
+class Dist:
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+
+            torch.cuda.set_device(self.local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                    device_id=torch.device("cuda", self.local))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, v: float) -> float:
+        if not self.pg:
+            return v
+        import torch
+
+        t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{self.local}")
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, v: float) -> float:
+        if not self.pg:
+            return v
+        import torch
+
+        t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{self.local}")
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.SUM)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# ------------------------------------------------------------------ clocks
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons while running."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        out, _ = self.proc.communicate(timeout=10)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def hbm_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def traffic_per_pcg_iteration():
+    """DRAM bytes per PCG iteration of k_pcg from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "k_pcg_ring4m_traffic.txt")
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith("dram_bytes_per_pcg_iteration"):
+                    return float(line.split("=")[1])
+    except (OSError, ValueError):
+        pass
+    return None
+
+
+# -------------------------------------------------------------- CPU side
+def cpu_sample(problem, cfg, threads=0):
+    """One LM iteration of the FP64 oracle on all host cores: seconds."""
+    from oracle import oracle
+
+    c = problem.copy()
+    one = type(cfg)(**{**cfg.__dict__, "max_iterations": 1})
+    t0 = time.perf_counter()
+    st, _ = oracle.optimize(c, one, solver=oracle.SPARSE, threads=threads)
+    dt = time.perf_counter() - t0
+    if st != 0:
+        raise RuntimeError(f"oracle failed: {st}")
+    return dt
+
+
+def run_reference(args, dist: Dist):
+    if dist.rank != 0:
+        return
+    problem, cfg, desc = make_workload(args.workload, 0)
+    from oracle import oracle
+
+    oracle.lib()
+    cores = os.cpu_count() or 1
+    for _ in range(args.warmup):  # a cost pass per warm-up step (page-in, threads)
+        oracle.cost(problem, cfg)
+    times = [cpu_sample(problem, cfg) for _ in range(args.steps)]
+    total = sum(times)
+    value = args.steps / total
+    line = {
+        "impl": "reference", "metric": "lm_iterations_per_s", "value": value,
+        "unit": "LM iterations/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": desc,
+        "observations_per_s": value * desc["observations"],
+        "cpu_baseline": {"value": value, "unit": "LM iterations/s", "cores": cores,
+                         "kind": "port",
+                         "sample": "1 LM iteration (Schur + Cholesky, FP64) of the same "
+                                   "workload per step, all host cores"},
+        "e2e": {"value": value, "unit": "LM iterations/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# -------------------------------------------------------------- GPU side
+def run_ours(args, dist: Dist):
+    import torch
+
+    from visloc_ba.solver import CudaSolver, plan
+
+    torch.cuda.set_device(dist.local)
+    problem, cfg, desc = make_workload(args.workload, dist.rank)
+    cfg.profile = True
+    st, info = plan(problem, cfg, 1.0)
+    if st != 0:
+        raise RuntimeError(f"plan failed: {st}")
+    solver = CudaSolver(dist.local)
+    st = solver.upload(problem, cfg)
+    if st != 0:
+        raise RuntimeError(f"upload failed: {solver.last_error()}")
+    for _ in range(args.warmup):
+        st, res = solver.solve_uploaded(cfg)
+        if st != 0:
+            raise RuntimeError(f"solve failed: {solver.last_error()}")
+
+    clocks = Clocks(dist.local)
+    dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    wall0 = time.perf_counter()
+    results = []
+    for _ in range(args.steps):
+        st, res = solver.solve_uploaded(cfg)
+        if st != 0:
+            raise RuntimeError(f"solve failed: {solver.last_error()}")
+        results.append(res)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - wall0
+    dist.barrier()
+    clk = clocks.stop()
+
+    dev_ms = sum(r.device_ms for r in results)
+    lm_iters = sum(len(r.iterations) for r in results)
+    pcg_iters = sum(it.pcg_iterations for r in results for it in r.iterations)
+    pcg_ms = sum(it.pcg_ms for r in results for it in r.iterations)
+    launches = sum(r.kernel_launches for r in results)
+    t_max = dist.max(dev_ms / 1e3)
+    lm_total = dist.sum(lm_iters)
+    value = lm_total / t_max
+    nobs = desc["observations"]
+
+    # Roofline of the dominant kernel (k_pcg): algorithmic bytes per PCG
+    # iteration x iterations of a launch / launch time, averaged over launches.
+    b_pcg = info.bytes_per_pcg_iteration
+    peak, peak_kind = hbm_peak()
+    achieved = (pcg_iters * b_pcg) / (pcg_ms / 1e3) / 1e9 if pcg_ms > 0 else 0.0
+    traffic = traffic_per_pcg_iteration()
+    n_pcg_launches = sum(1 for r in results for it in r.iterations)
+    mean_k = pcg_iters / max(1, n_pcg_launches)
+    # Whole LM step: algorithmic bytes of linearisation + trial at the mean k.
+    st2, info_k = plan(problem, cfg, mean_k)
+    step_bytes = info_k.bytes_per_iteration
+    step_gbs = step_bytes * lm_iters / (dev_ms / 1e3) / 1e9
+
+    e2e = None
+    if not args.no_e2e:
+        e2e_cfg = type(cfg)(**{**cfg.__dict__, "profile": False})
+        copies = [problem.copy() for _ in range(args.steps)]
+        e2e_iters = 0
+        dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for c in copies:
+            st, r = solver.optimize(c, e2e_cfg)
+            if st != 0:
+                raise RuntimeError(f"optimize failed: {solver.last_error()}")
+            e2e_iters += len(r.iterations)
+        torch.cuda.synchronize()
+        t_e2e = dist.max(time.perf_counter() - t0)
+        e2e = {"value": dist.sum(e2e_iters) / t_e2e, "unit": "LM iterations/s",
+               "h2d_bytes_per_step": int(info.upload_bytes),
+               "d2h_bytes_per_step": int(problem.num_poses * 56 + problem.num_landmarks * 24
+                                         + 64 * 30 + 128),
+               "ms_per_step": 1e3 * t_e2e / args.steps}
+
+    cpu = None
+    if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
+        dt = cpu_sample(problem, cfg)
+        cpu = {"value": 1.0 / dt, "unit": "LM iterations/s", "cores": os.cpu_count(),
+               "kind": "port",
+               "sample": "1 LM iteration (FP64 Schur + Cholesky) of the same workload, "
+                         f"{os.cpu_count()} threads, {dt:.1f} s"}
+
+    if dist.rank == 0:
+        line = {
+            "metric": "lm_iterations_per_s", "value": value, "unit": "LM iterations/s",
+            "n_gpus": dist.world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+            "data": "synthetic", "config": {**desc, "parallelism": f"replicas x{dist.world}",
+                                            "l2": "inputs larger than L2 (problem > 0.8 GB)"},
+            "observations_per_s": value * nobs,
+            "lm_iterations_per_step": lm_iters / args.steps,
+            "pcg_iterations_per_lm_iteration": mean_k,
+            "roofline": {"kernel": PCG_KERNEL, "bound": "hbm", "achieved": achieved,
+                         "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_kind": peak_kind,
+                         "traffic": traffic, "traffic_unit": "bytes per PCG iteration",
+                         "algorithmic_bytes_per_pcg_iteration": b_pcg},
+            "lm_step_roofline": {"achieved": step_gbs, "peak": peak, "unit": "GB/s",
+                                 "frac": step_gbs / peak,
+                                 "algorithmic_bytes_per_lm_iteration": step_bytes},
+            "phase_ms_per_lm_iteration": {
+                k: sum(getattr(it, f) for r in results for it in r.iterations) / max(1, lm_iters)
+                for k, f in [("linearize", "linearize_ms"), ("assemble", "assemble_ms"),
+                             ("pcg", "pcg_ms"), ("update_cost_decide", "update_ms")]},
+            "final_cost": results[-1].final_cost,
+            "initial_cost": results[-1].initial_cost,
+            "wall_s": wall,
+            "clocks": clk,
+            "gpu_launches": int(launches),
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    solver.close()
+
+
+def main():
+    args = parse_args()
+    dist = Dist()
+    try:
+        if args.impl == "reference":
+            run_reference(args, dist)
+        else:
+            run_ours(args, dist)
+    finally:
+        dist.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -163,8 +163,12 @@ typedef struct vlba_iteration {
   uint32_t step_accepted;
   uint32_t pcg_iterations;
   double pcg_relative_residual;    /* |r| / |b| at PCG exit */
-  double linearize_ms;             /* with VLBA_FLAG_PROFILE, else 0 */
-  double solve_ms;
+  /* Device time of the iteration's phases with VLBA_FLAG_PROFILE (else 0):
+   * linearisation, reduced-system assembly, PCG, update + cost + decision. */
+  double linearize_ms;
+  double assemble_ms;
+  double pcg_ms;
+  double update_ms;
 } vlba_iteration;
 
 /* BaResult (bundle/mod.rs:765-771) plus diagnostics. */
@@ -179,6 +183,7 @@ typedef struct vlba_result {
   uint64_t error_index;            /* id for MISSING_POSE / MISSING_LANDMARK */
   double device_ms;                /* device time of the LM iterations */
   double upload_ms;                /* host+device time of the upload */
+  uint64_t kernel_launches;        /* kernels launched by the LM iterations */
 } vlba_result;
 
 /* Device layout of a problem, computed on the host without touching the GPU
@@ -196,6 +201,7 @@ typedef struct vlba_plan_info {
   uint32_t tiles;
   uint32_t assembly_lanes;          /* lanes per off-diagonal block */
   uint64_t device_bytes;
+  uint64_t upload_bytes;            /* host -> device bytes of an upload */
   double bytes_per_iteration;       /* algorithmic bytes of one LM iteration
                                        (linearisation + one trial) */
   double bytes_per_pcg_iteration;

@@ -133,6 +133,9 @@ struct Dev {
   double* pose_t[2];    // [3 N]
   double* pose_rt[2];   // [12 N] derived R (row-major) and t
   double* points[2];    // [3 M]
+  const double* init_pose_q;   // uploaded initial state (reset by copy on device)
+  const double* init_pose_t;
+  const double* init_points;
   const uint32_t* pose_slot;   // [N] variable slot or kNone
   const uint8_t* point_var;    // [M] 1 = variable
   double* pose_step;           // [N] |xi| of the last trial

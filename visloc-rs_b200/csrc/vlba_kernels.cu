@@ -871,7 +871,9 @@ __global__ void __launch_bounds__(256) k_decide(Dev d) {
   rec.pcg_iterations = pg.iters;
   rec.pcg_relative_residual = pg.bnorm > 0.0 ? pg.rnorm / pg.bnorm : 0.0;
   rec.linearize_ms = 0.0;
-  rec.solve_ms = 0.0;
+  rec.assemble_ms = 0.0;
+  rec.pcg_ms = 0.0;
+  rec.update_ms = 0.0;
   c.total_pcg += pg.iters;
   c.pcg_iters = pg.iters;
   c.pcg_status = pg.status;

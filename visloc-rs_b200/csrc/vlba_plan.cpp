@@ -490,6 +490,16 @@ size_t Plan::device_bytes() const {
   return b;
 }
 
+size_t Plan::upload_bytes() const {
+  auto b = [](const auto& v) { return v.size() * sizeof(v[0]); };
+  return b(prob_pose_begin) + b(prob_point_begin) + b(prob_tr_begin) + b(prob_chunk_begin) +
+         b(pose_prob) + b(point_prob) + b(slot_prob) + b(params) + b(pose_q) + b(pose_t) +
+         b(points) + b(pose_slot) + b(point_var) + b(cameras) + b(pt_off) + b(obs_pose) +
+         b(obs_cam) + b(obs_slot) + b(obs_xy) + b(cam_off) + b(cam_obs) + b(tile_ij) +
+         b(blk_off) + b(pairs) + b(blk_dst) + b(diag_dst) + b(dup_off) + b(dup_pairs) +
+         b(tr_list_off) + b(tr_list) + b(tr_prob) + b(chunk_point_begin);
+}
+
 double algorithmic_bytes(const Plan& P, double k, double* b_pcg_out) {
   // Counts of the byte model: N_o variable observations, N_p variable
   // points, N_c variable cameras, N_e camera pairs sharing a variable point.

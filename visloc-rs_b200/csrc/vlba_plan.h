@@ -55,6 +55,7 @@ struct Plan {
   uint64_t num_pairs = 0;        // point contributions to those blocks
 
   size_t device_bytes() const;
+  size_t upload_bytes() const;  // bytes copied host -> device by an upload
 };
 
 // Per-problem outcome of validation (BaError order of lm.rs:168-229).

@@ -86,7 +86,7 @@ struct Context {
   Dev dev;
   bool uploaded = false;
   int pcg_grid = 0;
-  uint32_t* h_done = nullptr;  // pinned poll word
+  uint32_t flags = 0;  // flags of the uploaded config
   // the uploaded problem's sizes (for download)
   std::vector<uint64_t> num_poses, num_points;
 };
@@ -135,9 +135,9 @@ void upload_plan(Context* c, uint32_t max_records) {
     d.pose_rt[b] = A.alloc<double>(12 * npose);
     d.points[b] = A.alloc<double>(3 * npt);
   }
-  VLBA_CUDA(cudaMemcpyAsync(d.pose_q[0], P.pose_q.data(), P.pose_q.size() * 8, cudaMemcpyHostToDevice, s));
-  VLBA_CUDA(cudaMemcpyAsync(d.pose_t[0], P.pose_t.data(), P.pose_t.size() * 8, cudaMemcpyHostToDevice, s));
-  VLBA_CUDA(cudaMemcpyAsync(d.points[0], P.points.data(), P.points.size() * 8, cudaMemcpyHostToDevice, s));
+  d.init_pose_q = A.upload(P.pose_q, s);
+  d.init_pose_t = A.upload(P.pose_t, s);
+  d.init_points = A.upload(P.points, s);
   d.pose_slot = A.upload(P.pose_slot, s);
   d.point_var = A.upload(P.point_var, s);
   d.pose_step = A.alloc<double>(npose);
@@ -176,7 +176,7 @@ void upload_plan(Context* c, uint32_t max_records) {
   d.z = A.alloc<float>(nvec);
   d.p = A.alloc<float>(nvec);
   d.q = A.alloc<float>(nvec);
-  VLBA_CUDA(cudaMemsetAsync(d.x, 0, nvec * 4 + 4, s));
+  VLBA_CUDA(cudaMemsetAsync(d.x, 0, nvec * 4, s));
   d.partial = A.alloc<float>(P.tile_ij.size() * 2 * (size_t)P.tb * 6);
   d.tr_list_off = A.upload(P.tr_list_off, s);
   d.tr_list = A.upload(P.tr_list, s);
@@ -204,9 +204,9 @@ void reset_state(Context* c) {
   Dev& d = c->dev;
   const Plan& P = c->plan;
   cudaStream_t s = c->stream;
-  VLBA_CUDA(cudaMemcpyAsync(d.pose_q[0], P.pose_q.data(), P.pose_q.size() * 8, cudaMemcpyHostToDevice, s));
-  VLBA_CUDA(cudaMemcpyAsync(d.pose_t[0], P.pose_t.data(), P.pose_t.size() * 8, cudaMemcpyHostToDevice, s));
-  VLBA_CUDA(cudaMemcpyAsync(d.points[0], P.points.data(), P.points.size() * 8, cudaMemcpyHostToDevice, s));
+  VLBA_CUDA(cudaMemcpyAsync(d.pose_q[0], d.init_pose_q, P.pose_q.size() * 8, cudaMemcpyDeviceToDevice, s));
+  VLBA_CUDA(cudaMemcpyAsync(d.pose_t[0], d.init_pose_t, P.pose_t.size() * 8, cudaMemcpyDeviceToDevice, s));
+  VLBA_CUDA(cudaMemcpyAsync(d.points[0], d.init_points, P.points.size() * 8, cudaMemcpyDeviceToDevice, s));
   VLBA_CUDA(cudaMemsetAsync(d.ctrl, 0, sizeof(Ctrl) * P.num_problems, s));
   VLBA_CUDA(cudaMemsetAsync(d.error, 0, 4, s));
 }
@@ -217,60 +217,76 @@ void check_launch(cudaError_t e, const char* what) {
 
 struct RunStats {
   double device_ms = 0.0;
+  uint64_t launches = 0;
+};
+
+struct PhaseTimes {
+  std::vector<double> lin, assemble, pcg, update;
 };
 
 // The device LM loop over all uploaded problems.
-RunStats run_lm(Context* c, bool profile, std::vector<double>* lin_ms, std::vector<double>* solve_ms) {
+RunStats run_lm(Context* c, bool profile, PhaseTimes* pt) {
   Dev& d = c->dev;
   cudaStream_t s = c->stream;
   uint32_t max_iters = 0;
   for (const LmParams& lp : c->plan.params) max_iters = std::max(max_iters, lp.max_iterations);
   RunStats st;
+  std::vector<Ctrl> ctrl(c->plan.num_problems);
   VLBA_CUDA(cudaEventRecord(c->ev[0], s));
   check_launch(launch_pose_table(d, s), "pose table");
   check_launch(launch_cost(d, false, s), "initial cost");
   check_launch(launch_decide(d, true, s), "init");
+  st.launches += 3;
   for (uint32_t it = 0; it < max_iters; ++it) {
-    if (profile) VLBA_CUDA(cudaEventRecord(c->ev[2], s));
+    if (profile) VLBA_CUDA(cudaEventRecord(c->ev[1], s));
     check_launch(launch_linearize(d, s), "linearize");
-    if (profile) VLBA_CUDA(cudaEventRecord(c->ev[3], s));
+    if (profile) VLBA_CUDA(cudaEventRecord(c->ev[2], s));
     check_launch(launch_point_prep(d, s), "point prep");
     check_launch(launch_offdiag(d, s), "off-diagonal blocks");
     check_launch(launch_cam_diag(d, s), "camera blocks");
     check_launch(launch_pcg_setup(d, s), "pcg setup");
+    if (profile) VLBA_CUDA(cudaEventRecord(c->ev[3], s));
     check_launch(launch_pcg(d, c->pcg_grid, s), "pcg");
+    if (profile) VLBA_CUDA(cudaEventRecord(c->ev[4], s));
     check_launch(launch_pose_update(d, s), "pose update");
     check_launch(launch_cost(d, true, s), "trial cost");
     check_launch(launch_decide(d, false, s), "decide");
-    if (profile) VLBA_CUDA(cudaEventRecord(c->ev[4], s));
+    if (profile) VLBA_CUDA(cudaEventRecord(c->ev[5], s));
+    // linearize, point prep, pcg setup, pose update, cost, decide always;
+    // off-diagonal, camera-diagonal and PCG kernels when the system has them.
+    st.launches += 6 + (d.num_offdiag_blocks ? 1 : 0) + (d.num_var_cams ? 1 : 0) +
+                   (d.num_tile_rows ? 1 : 0);
     // Poll the per-problem control words (one small copy per iteration).
-    std::vector<Ctrl> ctrl(c->plan.num_problems);
     VLBA_CUDA(cudaMemcpyAsync(ctrl.data(), d.ctrl, sizeof(Ctrl) * ctrl.size(), cudaMemcpyDeviceToHost, s));
     unsigned int err = 0;
     VLBA_CUDA(cudaMemcpyAsync(&err, d.error, 4, cudaMemcpyDeviceToHost, s));
     VLBA_CUDA(cudaStreamSynchronize(s));
     if (profile) {
-      float a = 0.f, b = 0.f;
-      VLBA_CUDA(cudaEventElapsedTime(&a, c->ev[2], c->ev[3]));
-      VLBA_CUDA(cudaEventElapsedTime(&b, c->ev[3], c->ev[4]));
-      lin_ms->push_back(a);
-      solve_ms->push_back(b);
+      float a = 0.f, b = 0.f, e = 0.f, f = 0.f;
+      VLBA_CUDA(cudaEventElapsedTime(&a, c->ev[1], c->ev[2]));
+      VLBA_CUDA(cudaEventElapsedTime(&b, c->ev[2], c->ev[3]));
+      VLBA_CUDA(cudaEventElapsedTime(&e, c->ev[3], c->ev[4]));
+      VLBA_CUDA(cudaEventElapsedTime(&f, c->ev[4], c->ev[5]));
+      pt->lin.push_back(a);
+      pt->assemble.push_back(b);
+      pt->pcg.push_back(e);
+      pt->update.push_back(f);
     }
     if (err) throw Status(VLBA_ERR_TIMEOUT, "a bounded device wait gave up (error bits " + std::to_string(err) + ")");
     bool all_done = true;
     for (const Ctrl& x : ctrl) all_done = all_done && x.done;
     if (all_done) break;
   }
-  VLBA_CUDA(cudaEventRecord(c->ev[1], s));
-  VLBA_CUDA(cudaEventSynchronize(c->ev[1]));
+  VLBA_CUDA(cudaEventRecord(c->ev[5], s));
+  VLBA_CUDA(cudaEventSynchronize(c->ev[5]));
   float ms = 0.f;
-  VLBA_CUDA(cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]));
+  VLBA_CUDA(cudaEventElapsedTime(&ms, c->ev[0], c->ev[5]));
   st.device_ms = ms;
   return st;
 }
 
 void fill_result(Context* c, uint32_t prob, vlba_result* res, vlba_iteration* its, uint32_t cap,
-                 const std::vector<double>* lin_ms, const std::vector<double>* solve_ms) {
+                 const PhaseTimes* pt) {
   Ctrl ctrl;
   VLBA_CUDA(cudaMemcpy(&ctrl, c->dev.ctrl + prob, sizeof ctrl, cudaMemcpyDeviceToHost));
   if (res) {
@@ -286,10 +302,13 @@ void fill_result(Context* c, uint32_t prob, vlba_result* res, vlba_iteration* it
   if (its && n) {
     VLBA_CUDA(cudaMemcpy(its, c->dev.records + (size_t)prob * c->dev.max_records,
                          n * sizeof(vlba_iteration), cudaMemcpyDeviceToHost));
-    if (lin_ms)
-      for (uint32_t i = 0; i < n && i < lin_ms->size(); ++i) its[i].linearize_ms = (*lin_ms)[i];
-    if (solve_ms)
-      for (uint32_t i = 0; i < n && i < solve_ms->size(); ++i) its[i].solve_ms = (*solve_ms)[i];
+    if (pt)
+      for (uint32_t i = 0; i < n && i < pt->lin.size(); ++i) {
+        its[i].linearize_ms = pt->lin[i];
+        its[i].assemble_ms = pt->assemble[i];
+        its[i].pcg_ms = pt->pcg[i];
+        its[i].update_ms = pt->update[i];
+      }
   }
 }
 
@@ -447,6 +466,7 @@ int visloc_ba_cuda_upload(void* ctx, const vlba_problem* problem, const vlba_con
     const vlba_problem* probs[1] = {problem};
     const vlba_config* cfgs[1] = {config};
     vlba::do_upload(c, probs, cfgs, 1, config ? config->max_iterations : 0, nullptr);
+    c->flags = config ? config->flags : 0;
   });
 }
 
@@ -466,13 +486,15 @@ int visloc_ba_cuda_solve_uploaded(void* ctx, const vlba_config* config, vlba_res
       c->plan.params[0] = lp;
     }
     vlba::reset_state(c);
-    const bool profile = config && (config->flags & VLBA_FLAG_PROFILE);
-    std::vector<double> lin, sol;
-    const vlba::RunStats st = vlba::run_lm(c, profile, &lin, &sol);
+    const bool profile = (config ? config->flags : c->flags) & VLBA_FLAG_PROFILE;
+    vlba::PhaseTimes pt;
+    const vlba::RunStats st = vlba::run_lm(c, profile, &pt);
     if (result) std::memset(result, 0, sizeof *result);
-    vlba::fill_result(c, 0, result, iterations, iterations_capacity, profile ? &lin : nullptr,
-                      profile ? &sol : nullptr);
-    if (result) result->device_ms = st.device_ms;
+    vlba::fill_result(c, 0, result, iterations, iterations_capacity, profile ? &pt : nullptr);
+    if (result) {
+      result->device_ms = st.device_ms;
+      result->kernel_launches = st.launches;
+    }
   });
 }
 
@@ -497,6 +519,7 @@ int visloc_ba_cuda_optimize(void* ctx, vlba_problem* problem, const vlba_config*
     const vlba_problem* probs[1] = {problem};
     const vlba_config* cfgs[1] = {config};
     vlba::do_upload(c, probs, cfgs, 1, config ? config->max_iterations : 0, &upload_ms);
+    c->flags = config ? config->flags : 0;
   });
   if (st != VLBA_OK) {
     if (result && (st == VLBA_ERR_MISSING_POSE || st == VLBA_ERR_MISSING_LANDMARK)) {
@@ -536,6 +559,7 @@ int visloc_ba_cuda_plan(const vlba_problem* problem, const vlba_config* config,
       info->tiles = (uint32_t)plan.tile_ij.size();
       info->assembly_lanes = plan.group;
       info->device_bytes = plan.device_bytes();
+      info->upload_bytes = plan.upload_bytes();
       double b_pcg = 0.0;
       info->bytes_per_iteration = vlba::algorithmic_bytes(plan, pcg_iterations, &b_pcg);
       info->bytes_per_pcg_iteration = b_pcg;

@@ -126,7 +126,9 @@ class Iteration(C.Structure):
         ("pcg_iterations", C.c_uint32),
         ("pcg_relative_residual", C.c_double),
         ("linearize_ms", C.c_double),
-        ("solve_ms", C.c_double),
+        ("assemble_ms", C.c_double),
+        ("pcg_ms", C.c_double),
+        ("update_ms", C.c_double),
     ]
 
 
@@ -142,6 +144,7 @@ class Result(C.Structure):
         ("error_index", C.c_uint64),
         ("device_ms", C.c_double),
         ("upload_ms", C.c_double),
+        ("kernel_launches", C.c_uint64),
     ]
 
 
@@ -157,6 +160,7 @@ class PlanInfo(C.Structure):
         ("tiles", C.c_uint32),
         ("assembly_lanes", C.c_uint32),
         ("device_bytes", C.c_uint64),
+        ("upload_bytes", C.c_uint64),
         ("bytes_per_iteration", C.c_double),
         ("bytes_per_pcg_iteration", C.c_double),
     ]

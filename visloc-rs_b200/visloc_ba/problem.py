@@ -275,6 +275,10 @@ class BaIterationStats:
     step_accepted: bool
     pcg_iterations: int = 0
     pcg_relative_residual: float = 0.0
+    linearize_ms: float = 0.0
+    assemble_ms: float = 0.0
+    pcg_ms: float = 0.0
+    update_ms: float = 0.0
 
 
 @dataclass
@@ -288,6 +292,7 @@ class BaResult:
     total_pcg_iterations: int = 0
     device_ms: float = 0.0
     upload_ms: float = 0.0
+    kernel_launches: int = 0
 
 
 class BaError(Exception):
@@ -326,6 +331,10 @@ def result_from_abi(res: _abi.Result, iters, count: int) -> BaResult:
                 bool(it.step_accepted),
                 int(it.pcg_iterations),
                 it.pcg_relative_residual,
+                it.linearize_ms,
+                it.assemble_ms,
+                it.pcg_ms,
+                it.update_ms,
             )
         )
     return BaResult(
@@ -338,6 +347,7 @@ def result_from_abi(res: _abi.Result, iters, count: int) -> BaResult:
         int(res.total_pcg_iterations),
         res.device_ms,
         res.upload_ms,
+        int(res.kernel_launches),
     )
 
 
