@@ -272,6 +272,25 @@ int visloc_ba_cuda_cost(void* ctx, const vlba_problem* problem,
                         const vlba_config* config, double* cost,
                         uint64_t* nonprojectable);
 
+/* ------------------------------------------------------------- diagnostics */
+/* One damped linear step at the given state, without updating it: the step
+ * of solve_step (bundle/normal_equations.rs:1621-1733) as this solver forms
+ * it (linearisation, reduced system, PCG, back-substitution).  dp holds 6
+ * values ([rho; omega]) per variable pose and dl 3 per variable landmark, in
+ * index order; both may be NULL.  pcg_iterations / pcg_relative_residual may
+ * be NULL. */
+int visloc_ba_cuda_linear_step(void* ctx, const vlba_problem* problem,
+                               const vlba_config* config, double lambda,
+                               double* dp, double* dl, uint32_t* pcg_iterations,
+                               double* pcg_relative_residual);
+
+/* The damped reduced camera system S (dense, (6 Nc)^2 row-major, both
+ * triangles, Nc = variable poses) and its right-hand side at `lambda`, as
+ * assembled on the device. */
+int visloc_ba_cuda_reduced_system(void* ctx, const vlba_problem* problem,
+                                  const vlba_config* config, double lambda,
+                                  double* s_dense, double* rhs);
+
 #ifdef __cplusplus
 }
 #endif

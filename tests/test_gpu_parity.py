@@ -122,7 +122,8 @@ def test_landmark_only_matches_the_oracle(solver):
 
 def test_pure_gauss_newton_matches_the_oracle(solver):
     """initial_lambda = None: every solved step is accepted (lm.rs:804-808)."""
-    p = synth.ring_problem(12, 600, seed=12, outlier_fraction=0.0)
+    # Every point seen by >= 3 cameras: the undamped system is well posed.
+    p = synth.ring_problem(12, 600, seed=12, outlier_fraction=0.0, track=("uniform", 3, 6))
     cfg = tight(BaConfig(max_iterations=6, initial_lambda=None))
     res, res_ref, _, _ = compare(solver, p, cfg)
     assert [i.step_accepted for i in res.iterations] == [i.step_accepted for i in res_ref.iterations]
@@ -184,3 +185,34 @@ def test_unsupported_lens_is_declined():
     acc = GpuBundleAdjuster(0)
     assert acc.optimize(ba, BaConfig(), BaScope.GLOBAL) is None
     assert acc.optimize(drifted_bundle(), BaConfig(), BaScope.LOCAL) is None  # local off
+
+
+@pytest.mark.parametrize("ncams", [30, 70])  # 8-wide and 16-wide Schur tiles
+def test_reduced_system_matches_the_oracle(solver, ncams):
+    """The assembled damped reduced camera system S and its rhs against the
+    oracle's FP64 Schur complement (normal_equations.rs:1621-1700)."""
+    p = synth.ring_problem(ncams, 3000, seed=50 + ncams)
+    cfg = BaConfig(robust_kernel=RobustKernel.huber(1.0))
+    lam = 1e-3
+    s, rhs = solver.reduced_system(p, cfg, lam)
+    st, s_ref, rhs_ref, _, _ = oracle.reduced_system(p, lam, cfg, step=False)
+    assert st == 0
+    scale = np.abs(s_ref).max()
+    assert np.abs(s - s_ref).max() <= 2e-5 * scale
+    assert np.abs(rhs - rhs_ref).max() <= 2e-5 * np.abs(rhs_ref).max()
+
+
+@pytest.mark.parametrize("ncams", [30, 70])
+def test_linear_step_matches_the_exact_solve(solver, ncams):
+    """One damped step (PCG on S + back-substitution) against the oracle's
+    Cholesky solve of the same system."""
+    p = synth.ring_problem(ncams, 3000, seed=60 + ncams)
+    cfg = BaConfig(robust_kernel=RobustKernel.huber(1.0), max_pcg_iterations=500,
+                   pcg_relative_tolerance=1e-7)
+    lam = 1e-2
+    dp, dl, iters, rr = solver.linear_step(p, cfg, lam)
+    st, _, _, dp_ref, dl_ref = oracle.reduced_system(p, lam, cfg)
+    assert st == 0
+    assert rr <= 1e-7 and iters < 500
+    assert np.abs(dp - dp_ref).max() <= 1e-3 * np.abs(dp_ref).max()
+    assert np.abs(dl - dl_ref).max() <= 1e-3 * np.abs(dl_ref).max()

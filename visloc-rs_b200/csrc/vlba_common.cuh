@@ -181,13 +181,21 @@ struct Dev {
   float* z;
   float* p;
   float* q;
-  float* partial;              // [num_tiles * 2 * tb * 6]
+  float* partial;              // [list slots * tb * 6]: row-contiguous partials
+  const uint2* tile_slot;      // [num_tiles] slot of the row side, column side
+  const uint4* tile_meta;      // [num_tiles] {ij, row slot, column slot, problem}
   const uint32_t* tr_list_off; // [num_tile_rows + 1]
   const uint32_t* tr_list;     // partial indices (tile * 2 + side)
   const uint32_t* tr_prob;     // [num_tile_rows]
-  double* dots;                // [4 * num_tile_rows]
-  unsigned int* barrier;       // [4] grid barrier count, generation; active problems
+  double* dots;                // [16 * num_tile_rows]
+  unsigned int* row_cnt;       // [num_tile_rows] tile arrivals per row (PCG)
+  uint32_t l2_resident_tiles;  // tiles [0, n) are streamed with L2 evict_last
+  unsigned int* barrier;       // [kBarrierWords]: top count, generation, active
+                               // problems, -, group counts
   unsigned int* error;         // [1] device error flags
+  // Optional PCG phase trace (globaltimer ns): [iteration][block][kTracePhases]
+  // for iterations < kTraceIters; null unless VLBA_TRACE_PCG is set.
+  unsigned long long* trace;
 
   // reductions
   const uint32_t* chunk_point_begin;  // [num_point_chunks + 1]
@@ -195,6 +203,10 @@ struct Dev {
   unsigned long long* chunk_bad;
   double* chunk_step;
 };
+
+constexpr int kBarrierWords = 4 + 256;  // grid barrier state (up to 4096 blocks)
+constexpr int kTracePhases = 6;
+constexpr int kTraceIters = 64;
 
 enum ErrorBits : unsigned int {
   kErrBarrierTimeout = 1u,

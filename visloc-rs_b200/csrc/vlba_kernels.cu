@@ -31,6 +31,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 
 #include "vlba_kernels.cuh"
@@ -941,30 +942,38 @@ __global__ void __launch_bounds__(256) k_decide(Dev d) {
 // place of the implicit Schur operator): stop when |r| <= tol |b|, on
 // non-positive curvature, or at the iteration cap.
 //
-// One cooperative launch runs every iteration.  Per iteration:
-//   A  each block streams tiles of S (TB x TB blocks of 6x6, 36.9 KB at
-//      TB=16) HBM -> shared memory with cp.async.bulk (TMA) into a double
-//      buffer and writes, per tile (I,J), the row-side partial S_IJ p_J and
-//      the column-side partial S_IJ^T p_I (p = z + beta p formed on the fly);
-//   B  the owner of tile row I sums its partials in a fixed order into q_I,
-//      writes p_I and the partial dot p.q;
-//   C  x += alpha p, r -= alpha q, z = M^-1 r and the partial dots r.z, r.r.
-// All scalars are per problem and are summed over the problem's tile rows in
-// a fixed order, so every block computes bit-identical alphas and betas and a
-// problem's solve does not depend on what else is in the batch.  Blocks
-// synchronise through a grid barrier whose spin is bounded; a timeout sets
-// an error flag and every block leaves.
-template <int TB>
+// One cooperative launch runs every iteration; two grid barriers each.
+//   A  every warp streams its own tiles of S (8 x 8 blocks of 6x6, 9.2 KB)
+//      HBM/L2 -> shared memory with cp.async.bulk (TMA) through a private
+//      three-stage ring, and writes per tile (I,J) the row-side partial
+//      S_IJ p_J and the column-side partial S_IJ^T p_I, with p = z + beta p
+//      formed on the fly; no block-wide synchronisation per tile.  Partials
+//      of a tile row are contiguous; each tile posts a release increment on
+//      the row's arrival counter.  The owner block of a row (row mod grid)
+//      then waits (bounded) for the row's count and reduces it in a fixed
+//      order into q, the new p and the partial p.q.
+//   C  the owner of a tile row: x += alpha p, r -= alpha q, z = M^-1 r and
+//      the partial dots r.z and r.r.
+// The first tiles of the next iteration are prefetched before the barriers.
+// The leading tiles (a byte budget set from the L2 size) are loaded with an
+// L2 evict_last policy and the rest with evict_first; at exit the resident
+// lines are returned to the normal eviction priority.
+// All scalars are per problem, summed over the problem's tile rows in a fixed
+// order, so every block derives bit-identical alphas and betas and a
+// problem's solve does not depend on what else is in the batch.  The grid
+// barrier and every mbarrier wait are bounded; a timeout sets an error flag
+// and every block leaves.
 struct Pcg {
-  static constexpr int kThreads = TB * TB;
-  static constexpr int kTileFloats = TB * TB * kBlock;
+  static constexpr int kTB = 8;              // tile edge in 6x6 blocks
+  static constexpr int kWarps = 8;           // one block per SM (shared memory)
+  static constexpr int kThreads = 32 * kWarps;
+  static constexpr int kStages = 3;          // per-warp TMA ring
+  static constexpr int kTileFloats = kTB * kTB * kBlock;
   static constexpr uint32_t kTileBytes = kTileFloats * 4u;
-  static constexpr int kRow = TB * 6;
-  // Per tile row, stride kDots doubles: rz[3] (slot k mod 3), rr[3], pq[2]
-  // (slot k mod 2), b2.  Three rz/rr slots and two pq slots keep every value
-  // a block may still read in iteration k distinct from the ones written.
-  static constexpr size_t kSmem =
-      2 * (size_t)kTileBytes + 2 * kRow * 4 + kThreads * 6 * 4 + kThreads * 8 * 6 + 64;
+  static constexpr int kRow = kTB * 6;       // floats of a tile-row vector segment
+  static constexpr size_t kWarpBytes = (size_t)kStages * kTileBytes + 2 * kRow * 4;
+  static constexpr size_t kSmem = kWarps * kWarpBytes + (size_t)kWarps * kRow * 4 +
+                                  (size_t)kThreads * 8 + 64;
 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
@@ -975,16 +984,28 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
 }
 
+__device__ __forceinline__ uint64_t l2_policy(bool keep) {
+  uint64_t p;
+  if (keep)
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  else
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+
+// One bulk copy global -> shared completing on `bar`, with an L2 policy.
+// The destination stage is reused only after every thread's reads of it have
+// completed (their values consumed, then a warp or block barrier), so the
+// copy needs no proxy fence -- the reuse rule of TMA pipelines.
 __device__ __forceinline__ void tma_load(void* dst, const void* src, uint32_t bytes,
-                                         uint64_t* bar) {
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                                         uint64_t* bar, uint64_t policy) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
                "r"(bytes)
                : "memory");
   asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
-          "r"(smem_addr(dst)),
-      "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint"
+      " [%0], [%1], %2, [%3], %4;" ::"r"(smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar)), "l"(policy)
       : "memory");
 }
 
@@ -1011,146 +1032,332 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, unsign
   return true;
 }
 
-// Sense-counting grid barrier with a bounded spin.  Returns false when any
-// block has flagged an error (every thread of the block sees the same value).
+__device__ __forceinline__ unsigned int atom_add_acq_rel(unsigned int* a, unsigned int v) {
+  unsigned int old;
+  asm volatile("atom.add.acq_rel.gpu.u32 %0, [%1], %2;" : "=r"(old) : "l"(a), "r"(v) : "memory");
+  return old;
+}
+
+__device__ __forceinline__ void red_add_release(unsigned int* a, unsigned int v) {
+  asm volatile("red.add.release.gpu.u32 [%0], %1;" ::"l"(a), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ unsigned int ld_acquire(const unsigned int* a) {
+  unsigned int v;
+  asm volatile("ld.acquire.gpu.u32 %0, [%1];" : "=r"(v) : "l"(a) : "memory");
+  return v;
+}
+
+// Two-level counting grid barrier with a bounded spin: blocks arrive on one
+// of the group counters (kBarGroup blocks each) with acquire-release
+// atomics; the last arrival of a group arrives on the top counter, whose last
+// arrival publishes the next generation.  Every block tracks the generation
+// it waits for (`gen`, starting from the value at launch), so the wait needs
+// no read before the arrival.  Returns false when any block has flagged an
+// error (every thread of the block sees the same value).  Layout of `bar`:
+// [0] top count, [1] generation, [4 + g] group counts.
+constexpr unsigned int kBarGroup = 16u;
+
 __device__ bool grid_barrier(unsigned int* bar, unsigned int nblocks, unsigned int* err,
-                             unsigned int* s_flag) {
+                             unsigned int* s_flag, unsigned int& gen) {
   __syncthreads();
+  ++gen;
   if (threadIdx.x == 0) {
-    volatile unsigned int* vgen = bar + 1;
-    const unsigned int gen = *vgen;
-    __threadfence();
-    const unsigned int arrived = atomicAdd(bar, 1u) + 1u;
-    if (arrived == nblocks) {
-      atomicExch(bar, 0u);
-      __threadfence();
-      atomicAdd(bar + 1, 1u);
+    const unsigned int g = blockIdx.x / kBarGroup;
+    const unsigned int ngroups = (nblocks + kBarGroup - 1) / kBarGroup;
+    const unsigned int in_group = min(kBarGroup, nblocks - g * kBarGroup);
+    bool top = false;
+    if (atom_add_acq_rel(bar + 4 + g, 1u) + 1u == in_group) {
+      bar[4 + g] = 0u;  // nobody touches it again before the release
+      top = atom_add_acq_rel(bar, 1u) + 1u == ngroups;
+    }
+    if (top) {
+      bar[0] = 0u;
+      asm volatile("st.release.gpu.u32 [%0], %1;" ::"l"(bar + 1), "r"(gen) : "memory");
     } else {
       uint32_t spins = 0;
-      while (*vgen == gen) {
+      while (ld_acquire(bar + 1) != gen) {
         if (++spins > kSpinLimit) {
           atomicOr(err, (unsigned int)kErrBarrierTimeout);
           break;
         }
-        __nanosleep(40);
+        __nanosleep(8);
       }
     }
-    __threadfence();
     *s_flag = *(volatile unsigned int*)err;
   }
   __syncthreads();
   return *s_flag == 0u;
 }
 
-// Per-problem PCG scalars, computed by the whole block from the tile-row
-// dots in a fixed order.
+__device__ __forceinline__ unsigned long long globaltimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Per-tile marks (first kTraceTiles tiles of each warp): [iteration][warp][tile][4].
+constexpr int kTraceTiles = 8;
+__device__ __forceinline__ void trace_tile(const Dev& d, int k, uint32_t gw, uint32_t tw, uint32_t m,
+                                           int which) {
+  if (d.trace && (threadIdx.x & 31u) == 0 && k < kTraceIters && m < (uint32_t)kTraceTiles) {
+    unsigned long long* w = d.trace + (size_t)kTraceIters * gridDim.x * kTracePhases +
+                            (size_t)kTraceIters * tw * 2;
+    w[(((size_t)k * tw + gw) * kTraceTiles + m) * 4 + which] = globaltimer();
+  }
+}
+
+// Per-warp marks after the block marks: [iteration][warp of grid][2].
+__device__ __forceinline__ void trace_warp(const Dev& d, int k, uint32_t gw, uint32_t tw, int which) {
+  if (d.trace && (threadIdx.x & 31u) == 0 && k < kTraceIters) {
+    unsigned long long* w = d.trace + (size_t)kTraceIters * gridDim.x * kTracePhases;
+    w[((size_t)k * tw + gw) * 2 + which] = globaltimer();
+  }
+}
+
+__device__ __forceinline__ void trace_mark(const Dev& d, int k, int phase) {
+  if (d.trace && threadIdx.x == 0 && k < kTraceIters) {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    d.trace[((size_t)k * gridDim.x + blockIdx.x) * kTracePhases + phase] = t;
+  }
+}
+
+// Per-problem PCG scalars from the tile-row dots, summed by warp 0 in a
+// fixed order (lane-strided partial sums, then a butterfly).
 struct ProbScal {
   int active;
   int status;   // when inactive: 0 converged, 1 cap, 2 breakdown
   uint32_t iters;
+  uint32_t pad;
   double beta;
   double rz;    // rz(k-1)
   double rr;
   double bnorm;
 };
 
-constexpr int kDotStride = 16;
+// Tile-row dots, one contiguous array per quantity (coalesced per-problem
+// sums): slot q of tile row tr at dots[q * num_tile_rows + tr].  rz and rr
+// rotate over three slots (iteration k mod 3), p.q over two.
 __device__ __forceinline__ int mod3(int k) { return ((k % 3) + 3) % 3; }
 constexpr int kDotRz = 0, kDotRr = 3, kDotPq = 6, kDotB2 = 8;
-
-template <int N>
-__device__ void prob_scalars(const Dev& d, uint32_t P, int k, double* red, ProbScal* out) {
-  const uint32_t t0 = d.prob_tr_begin[P], t1 = d.prob_tr_begin[P + 1];
-  const int sticky = *(volatile uint32_t*)&d.pcg[P].active;
-  double v[5] = {0, 0, 0, 0, 0};  // rz(k-1), rz(k-2), rr(k-1), pq(k-1), b2
-  const int s1 = mod3(k - 1), s2 = mod3(k - 2), sp = (k - 1) & 1;
-  for (uint32_t tr = t0 + threadIdx.x; tr < t1; tr += N) {
-    const double* dt = d.dots + kDotStride * (size_t)tr;
-    v[0] += __ldcg(dt + kDotRz + s1);
-    v[1] += __ldcg(dt + kDotRz + s2);
-    v[2] += __ldcg(dt + kDotRr + s1);
-    v[3] += __ldcg(dt + kDotPq + sp);
-    v[4] += __ldcg(dt + kDotB2);
-  }
-  for (int e = 0; e < 5; ++e) {
-    const double t = block_sum<double, N>(v[e], red);
-    if (threadIdx.x == 0) v[e] = t;
-  }
-  if (threadIdx.x == 0) {
-    const LmParams& lp = d.params[P];
-    ProbScal s;
-    s.active = sticky;
-    s.status = 0;
-    s.iters = (uint32_t)k;
-    s.beta = 0.0;
-    s.rz = v[0];
-    s.rr = v[2];
-    s.bnorm = sqrt(v[4]);
-    if (sticky) {
-      if (k == 0) {
-        // pcg_init (ba.wgsl:420-439): done when |b| = 0 or r.z <= 0.
-        if (!(v[4] > 0.0) || !(v[0] > 0.0) || lp.max_pcg_iterations == 0) s.active = 0;
-      } else if (!(v[3] > 0.0) || !isfinite(v[3])) {
-        s.active = 0;  // non-positive curvature in iteration k-1: x unchanged
-        s.status = 2;
-        s.iters = (uint32_t)(k - 1);
-      } else if (sqrt(v[2]) <= lp.pcg_relative_tolerance * s.bnorm || !(v[0] > 0.0)) {
-        s.active = 0;
-      } else if ((uint32_t)k >= lp.max_pcg_iterations) {
-        s.active = 0;
-        s.status = 1;
-      } else {
-        s.beta = v[0] / v[1];
-      }
-    }
-    *out = s;
-  }
-  __syncthreads();
+__device__ __forceinline__ double* dot_at(const Dev& d, int slot, uint32_t tr) {
+  return d.dots + (size_t)slot * d.num_tile_rows + tr;
 }
 
-template <int TB>
-__global__ void __launch_bounds__(Pcg<TB>::kThreads) k_pcg(Dev d) {
-  using C = Pcg<TB>;
-  constexpr int N = C::kThreads;
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  return v;
+}
+
+// Per-problem scalars computed by one warp (every lane returns the same
+// values): the sums over the problem's tile rows in lane-strided order and a
+// butterfly; the sticky flag is read once and broadcast.
+__device__ ProbScal prob_scalars_warp(const Dev& d, uint32_t P, int k) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t t0 = d.prob_tr_begin[P], t1 = d.prob_tr_begin[P + 1];
+  double v[5] = {0, 0, 0, 0, 0};  // rz(k-1), rz(k-2), rr(k-1), pq(k-1), b2
+  const int s1 = mod3(k - 1), s2 = mod3(k - 2), sp = (k - 1) & 1;
+  for (uint32_t tr = t0 + lane; tr < t1; tr += 32) {
+    v[0] += __ldcg(dot_at(d, kDotRz + s1, tr));
+    v[1] += __ldcg(dot_at(d, kDotRz + s2, tr));
+    v[2] += __ldcg(dot_at(d, kDotRr + s1, tr));
+    v[3] += __ldcg(dot_at(d, kDotPq + sp, tr));
+    v[4] += __ldcg(dot_at(d, kDotB2, tr));
+  }
+#pragma unroll
+  for (int e = 0; e < 5; ++e) v[e] = warp_sum(v[e]);
+  int sticky = 0;
+  if (lane == 0) sticky = (int)*(volatile uint32_t*)&d.pcg[P].active;
+  sticky = __shfl_sync(0xffffffffu, sticky, 0);
+  const LmParams& lp = d.params[P];
+  ProbScal s;
+  s.active = sticky;
+  s.status = 0;
+  s.iters = (uint32_t)k;
+  s.pad = 0;
+  s.beta = 0.0;
+  s.rz = v[0];
+  s.rr = v[2];
+  s.bnorm = sqrt(v[4]);
+  if (sticky) {
+    if (k == 0) {
+      // pcg_init (ba.wgsl:420-439): done when |b| = 0 or r.z <= 0.
+      if (!(v[4] > 0.0) || !(v[0] > 0.0) || lp.max_pcg_iterations == 0) s.active = 0;
+    } else if (!(v[3] > 0.0) || !isfinite(v[3])) {
+      s.active = 0;  // non-positive curvature in iteration k-1: x unchanged
+      s.status = 2;
+      s.iters = (uint32_t)(k - 1);
+    } else if (sqrt(v[2]) <= lp.pcg_relative_tolerance * s.bnorm || !(v[0] > 0.0)) {
+      s.active = 0;
+    } else if ((uint32_t)k >= lp.max_pcg_iterations) {
+      s.active = 0;
+      s.status = 1;
+    } else {
+      s.beta = v[0] / v[1];
+    }
+  }
+  return s;
+}
+
+// Fixed-order sum of a double over the block: butterfly per warp, then the
+// warps in order (result valid in every thread).
+template <int NW>
+__device__ __forceinline__ double block_sum_fast(double v, double* red) {
+  v = warp_sum(v);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double t = 0.0;
+#pragma unroll
+  for (int w = 0; w < NW; ++w) t += red[w];
+  __syncthreads();
+  return t;
+}
+
+__global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
+  using C = Pcg;
+  constexpr int NW = C::kWarps;
+  constexpr uint32_t TBC = C::kTB;
   extern __shared__ __align__(128) unsigned char smem[];
-  float* const buf0 = reinterpret_cast<float*>(smem);  // buffer b at buf0 + b * kTileFloats
-  float* sPI = reinterpret_cast<float*>(smem + 2 * (size_t)C::kTileBytes);
-  float* sPJ = sPI + C::kRow;
-  float* colst = sPJ + C::kRow;                               // [N * 6]
-  double* red = reinterpret_cast<double*>(colst + N * 6);     // [N * 6]
-  __shared__ uint64_t mbar[2];
+  const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+  // Per-warp region: kStages tile buffers, then the warp's p segments.
+  unsigned char* wbase = smem + (size_t)warp * C::kWarpBytes;
+  float* const ring = reinterpret_cast<float*>(wbase);
+  float* const wPI = reinterpret_cast<float*>(wbase + (size_t)C::kStages * C::kTileBytes);
+  float* const wPJ = wPI + C::kRow;
+  float* const colw = reinterpret_cast<float*>(smem + (size_t)NW * C::kWarpBytes);  // [NW kRow]
+  double* const red = reinterpret_cast<double*>(colw + NW * C::kRow);             // [N]
+  __shared__ uint64_t mbar[NW][C::kStages];
   __shared__ ProbScal sc;
   __shared__ uint32_t sc_prob;
   __shared__ int sc_k;
   __shared__ unsigned int s_flag;
   __shared__ double s_alpha;
 
-  const uint32_t tid = threadIdx.x;
   const uint32_t G = gridDim.x;
-  if (tid == 0) {
-    mbar_init(&mbar[0]);
-    mbar_init(&mbar[1]);
+  const uint32_t TW = G * NW;  // warps in the grid
+  const uint32_t gw = blockIdx.x * NW + warp;
+  const uint32_t ntiles = d.num_tiles;
+  // This warp's tiles: gw + m TW, m < Mw, in the same order each iteration.
+  const uint32_t Mw = gw < ntiles ? (ntiles - 1 - gw) / TW + 1 : 0u;
+  const uint64_t keep = l2_policy(true), stream = l2_policy(false);
+  if (lane == 0) {
+    for (int st = 0; st < C::kStages; ++st) mbar_init(&mbar[warp][st]);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (tid == 0) {
     sc_prob = kNone;
     sc_k = -2;
   }
   __syncthreads();
-  uint32_t parity = 0;  // bit b: phase parity expected on buffer b
-  int nextbuf = 0;
+  // Warp tile sequence s = k Mw + m: stage s % kStages, phase (s / kStages) & 1.
+  uint64_t issued = 0, consumed = 0;
+  auto tile_of = [&](uint64_t s) -> uint32_t { return gw + (uint32_t)(s % Mw) * TW; };
+  auto issue = [&](uint64_t s) {  // lane 0 only
+    const uint32_t t = tile_of(s);
+    const int st = (int)(s % C::kStages);
+    tma_load(ring + (size_t)st * C::kTileFloats, d.tiles + (size_t)t * C::kTileFloats,
+             C::kTileBytes, &mbar[warp][st], t < d.l2_resident_tiles ? keep : stream);
+  };
   bool ok = true;
 
+  // Block-level per-problem scalars (cached per problem and iteration).
   auto scal = [&](uint32_t P, int k) {
     if (sc_prob == P && sc_k == k) return;  // uniform: shared values
     __syncthreads();
-    prob_scalars<N>(d, P, k, red, &sc);
-    if (tid == 0) {
-      sc_prob = P;
-      sc_k = k;
+    if (warp == 0) {
+      const ProbScal s = prob_scalars_warp(d, P, k);
+      if (lane == 0) {
+        sc = s;
+        sc_prob = P;
+        sc_k = k;
+      }
     }
     __syncthreads();
   };
 
-  // ---- init: x = 0, r = b, z = M^-1 r, p = z; dots rz, b2 in slot k = -1.
+  // Rows this block owns (row R belongs to block R mod G), kOwn at most
+  // (a larger grid than rows x kOwn is never launched): list bounds and
+  // problem, constant for the launch.
+  constexpr int kOwn = 4;
+  __shared__ uint32_t own_m0[kOwn], own_m1[kOwn], own_prob[kOwn];
+  const uint32_t nown = blockIdx.x < d.num_tile_rows
+                            ? min((uint32_t)kOwn, (d.num_tile_rows - 1 - blockIdx.x) / G + 1)
+                            : 0u;
+  if (tid < nown) {
+    const uint32_t R = blockIdx.x + tid * G;
+    own_m0[tid] = d.tr_list_off[R];
+    own_m1[tid] = d.tr_list_off[R + 1];
+    own_prob[tid] = d.tr_prob[R];
+  }
+  unsigned int bar_gen = *(volatile unsigned int*)(d.barrier + 1);
+  // Per owned row, threads [0, kRow): p, z (prefetched before the tiles), then
+  // q and the new p (reduction), x, r and the M^-1 row (prefetched for C).
+  float own_p[kOwn] = {}, own_z[kOwn] = {}, own_q[kOwn] = {}, own_x[kOwn] = {}, own_r[kOwn] = {};
+  float own_m[kOwn][6] = {};
+
+  // Fixed-order reduction of tile row R: warp w sums slots m0 + w + j NW
+  // (contiguous kRow floats, coalesced, kBatch in flight), in slot order;
+  // then the warps' sums in warp order.  Gives q_R, the new p_R and the
+  // partial p.q of iteration k.
+  auto reduce_row = [&](int j, int k, double beta) {
+    const uint32_t R = blockIdx.x + (uint32_t)j * G;
+    const uint32_t m0 = own_m0[j], m1 = own_m1[j];
+    constexpr int kPer = (C::kRow + 31) / 32;
+    constexpr int kBatch = 24;  // 24 slots per warp in flight: one round for 192 slots
+    float acc[kPer];
+#pragma unroll
+    for (int e = 0; e < kPer; ++e) acc[e] = 0.0f;
+    for (uint32_t m = m0 + warp; m < m1; m += kBatch * NW) {
+      float v[kBatch][kPer];
+#pragma unroll
+      for (int u = 0; u < kBatch; ++u) {
+        const uint32_t slot = m + u * NW;
+        const float* src = d.partial + (size_t)slot * C::kRow;
+#pragma unroll
+        for (int e = 0; e < kPer; ++e)
+          v[u][e] = (slot < m1 && lane + 32 * e < (uint32_t)C::kRow) ? __ldcg(src + lane + 32 * e)
+                                                                    : 0.0f;
+      }
+#pragma unroll
+      for (int u = 0; u < kBatch; ++u)
+#pragma unroll
+        for (int e = 0; e < kPer; ++e) acc[e] += v[u][e];
+    }
+#pragma unroll
+    for (int e = 0; e < kPer; ++e)
+      if (lane + 32 * e < (uint32_t)C::kRow) colw[warp * C::kRow + lane + 32 * e] = acc[e];
+    __syncthreads();
+    double pq = 0.0;
+    if (tid < (uint32_t)C::kRow) {
+      const size_t at = (size_t)R * C::kRow + tid;
+      float q = 0.0f;
+#pragma unroll
+      for (int w2 = 0; w2 < NW; ++w2) q += colw[w2 * C::kRow + tid];
+      float pv = own_p[j];
+      if (k > 0) pv = __fmaf_rn((float)beta, pv, own_z[j]);
+      own_p[j] = pv;
+      own_q[j] = q;
+      d.p[at] = pv;
+      d.q[at] = q;
+      pq = (double)pv * (double)q;
+      // Operands of this row's update in C, fetched now.
+      own_x[j] = __ldcg(d.x + at);
+      own_r[j] = __ldcg(d.r + at);
+      const float* mm = d.minv + 36 * (size_t)(R * TBC + tid / 6) + (tid % 6) * 6;
+#pragma unroll
+      for (int b2 = 0; b2 < 6; ++b2) own_m[j][b2] = mm[b2];
+    }
+    pq = block_sum_fast<NW>(pq, red);
+    if (tid == 0) {
+      *dot_at(d, kDotPq + (k & 1), R) = pq;
+      d.row_cnt[R] = 0u;  // every tile of row R has arrived this iteration
+    }
+  };
+
+  // ---- init: x = 0, r = b, z = M^-1 r, p = z; dots rz, b2 of "iteration -1".
+  float* const sPI = colw;  // block scratch of kRow floats for init / C
   for (uint32_t tr = blockIdx.x; tr < d.num_tile_rows; tr += G) {
     const uint32_t P = d.tr_prob[tr];
     if (!*(volatile uint32_t*)&d.pcg[P].active) continue;
@@ -1174,20 +1381,28 @@ __global__ void __launch_bounds__(Pcg<TB>::kThreads) k_pcg(Dev d) {
       rz = (double)sPI[tid] * (double)z;
       bb = (double)sPI[tid] * (double)sPI[tid];
     }
-    rz = block_sum<double, N>(rz, red);
-    bb = block_sum<double, N>(bb, red);
+    rz = block_sum_fast<NW>(rz, red);
+    bb = block_sum_fast<NW>(bb, red);
     if (tid == 0) {
-      double* dt = d.dots + kDotStride * (size_t)tr;
-      dt[kDotRz + mod3(-1)] = rz;  // the values of "iteration -1"
-      dt[kDotRr + mod3(-1)] = bb;
-      dt[kDotPq + 1] = 1.0;
-      dt[kDotB2] = bb;
+      *dot_at(d, kDotRz + mod3(-1), tr) = rz;
+      *dot_at(d, kDotRr + mod3(-1), tr) = bb;
+      *dot_at(d, kDotPq + 1, tr) = 1.0;
+      *dot_at(d, kDotB2, tr) = bb;
+      d.row_cnt[tr] = 0u;
     }
   }
-  ok = grid_barrier(d.barrier, G, d.error, &s_flag);
+  // The metadata of the warp's first two tiles (the same every iteration).
+  const uint4 meta0 = Mw > 0 ? d.tile_meta[gw] : make_uint4(0u, 0u, 0u, 0u);
+  const uint4 meta1 = Mw > 1 ? d.tile_meta[gw + TW] : make_uint4(0u, 0u, 0u, 0u);
+  // The first tiles of every warp go out before the barrier.
+  if (lane == 0)
+    for (; issued < (uint64_t)C::kStages && issued < Mw; ++issued) issue(issued);
+  issued = __shfl_sync(0xffffffffu, issued, 0);
+  ok = grid_barrier(d.barrier, G, d.error, &s_flag, bar_gen);
 
   for (int k = 0; ok; ++k) {
-    // ---- A: status of the problems this block owns, then the tiles.
+    trace_mark(d, k, 0);
+    // ---- A: status of the problems this block owns, then the warps' tiles.
     for (uint32_t tr = blockIdx.x; tr < d.num_tile_rows; tr += G) {
       const uint32_t P = d.tr_prob[tr];
       if (d.prob_tr_begin[P] != tr) continue;  // owner = first tile row
@@ -1205,129 +1420,227 @@ __global__ void __launch_bounds__(Pcg<TB>::kThreads) k_pcg(Dev d) {
         atomicSub(d.barrier + 2, 1u);
       }
     }
+    // The owned rows' p and z (read again only by their owner this iteration).
+    if (tid < (uint32_t)C::kRow)
+      for (uint32_t j = 0; j < nown; ++j) {
+        const size_t at = (size_t)(blockIdx.x + j * G) * C::kRow + tid;
+        own_p[j] = __ldcg(d.p + at);
+        own_z[j] = __ldcg(d.z + at);
+      }
+    // The block computes the scalars of its first tile's problem once; warps
+    // whose tile is of that problem read them from shared memory.
+    if (NW > 0) {
+      const uint32_t b0 = blockIdx.x * NW;
+      if (b0 < ntiles) scal(d.tile_meta[b0].w, k);
+    }
+    trace_mark(d, k, 1);
     {
-      uint32_t t = blockIdx.x;
-      int b = nextbuf;
-      if (t < d.num_tiles && tid == 0) tma_load(buf0 + b * C::kTileFloats, d.tiles + (size_t)t * C::kTileFloats,
-                                                C::kTileBytes, &mbar[b]);
-      while (t < d.num_tiles) {
-        const uint32_t tn = t + G;
-        const int bn = b ^ 1;
-        if (tn < d.num_tiles && tid == 0)
-          tma_load(buf0 + bn * C::kTileFloats, d.tiles + (size_t)tn * C::kTileFloats, C::kTileBytes, &mbar[bn]);
-        const uint32_t ij = d.tile_ij[t];
-        const uint32_t I = ij >> 16, J = ij & 0xFFFFu;
-        const uint32_t P = d.tr_prob[I];
-        scal(P, k);
-        const bool arrived = __syncthreads_and(mbar_wait(&mbar[b], (parity >> b) & 1u, d.error));
-        parity ^= 1u << b;
-        if (!arrived) ok = false;
-        if (sc.active && ok) {
-          if (tid < (uint32_t)C::kRow) {
-            const size_t bi = (size_t)I * C::kRow + tid, bj = (size_t)J * C::kRow + tid;
-            float pi = __ldcg(d.p + bi), pj = __ldcg(d.p + bj);
-            if (k > 0) {
-              const float beta = (float)sc.beta;
-              pi = __ldcg(d.z + bi) + beta * pi;
-              pj = __ldcg(d.z + bj) + beta * pj;
-            }
-            sPI[tid] = pi;
-            sPJ[tid] = pj;
+      // Software pipeline per warp: tile metadata two tiles ahead, the p/z
+      // segments (entries e = lane + 32 j of [0, 2 kRow): row I's, then row
+      // J's) one tile ahead, the tile itself kStages ahead (TMA ring).
+      constexpr int kPre = (2 * C::kRow + 31) / 32;
+      float pre_p[kPre], pre_z[kPre];
+      auto prefetch_seg = [&](uint32_t ij) {
+#pragma unroll
+        for (int j = 0; j < kPre; ++j) {
+          const uint32_t e = lane + 32u * j;
+          if (e < 2u * C::kRow) {
+            const uint32_t row = e < (uint32_t)C::kRow ? (ij >> 16) : (ij & 0xFFFFu);
+            const size_t at = (size_t)row * C::kRow + (e % C::kRow);
+            pre_p[j] = __ldcg(d.p + at);
+            pre_z[j] = __ldcg(d.z + at);
           }
-          __syncthreads();
-          const int li = tid / TB, lj = tid % TB;
-          const float4* blk = reinterpret_cast<const float4*>(buf0 + b * C::kTileFloats + tid * kBlock);
-          float s[36];
+        }
+      };
+      uint32_t wprob = kNone;
+      ProbScal ws;
+      ws.active = 0;
+      ws.beta = 0.0;
+      uint4 meta_cur = meta0, meta_nxt = meta1;
+      uint64_t done_mask = 0;  // tiles m < 64 processed this iteration
+      if (Mw > 0) prefetch_seg(meta_cur.x);
+      trace_warp(d, k, gw, TW, 0);
+      for (uint32_t m = 0; m < Mw; ++m) {
+        const uint64_t s = (uint64_t)k * Mw + m;
+        trace_tile(d, k, gw, TW, m, 0);
+        const uint4 meta = meta_cur;
+        uint4 meta_nn = make_uint4(0u, 0u, 0u, 0u);
+        if (m + 2 < Mw) meta_nn = d.tile_meta[tile_of(s + 2)];
+        const uint32_t I = meta.x >> 16, J = meta.x & 0xFFFFu;
+        const uint32_t P = meta.w;
+        if (P != wprob) {
+          if (sc_prob == P && sc_k == k) ws = sc;  // the block's scalars
+          else ws = prob_scalars_warp(d, P, k);
+          wprob = P;
+        }
+        const bool active = ws.active != 0;
+        if (active) {
 #pragma unroll
-          for (int m = 0; m < 9; ++m) {
-            const float4 v = blk[m];
-            s[4 * m] = v.x;
-            s[4 * m + 1] = v.y;
-            s[4 * m + 2] = v.z;
-            s[4 * m + 3] = v.w;
-          }
-          float row[6], col[6];
-#pragma unroll
-          for (int a = 0; a < 6; ++a) {
-            float acc = 0.0f;
-#pragma unroll
-            for (int c = 0; c < 6; ++c) acc += s[a * 6 + c] * sPJ[lj * 6 + c];
-            row[a] = acc;
-          }
-#pragma unroll
-          for (int c = 0; c < 6; ++c) {
-            float acc = 0.0f;
-#pragma unroll
-            for (int a = 0; a < 6; ++a) acc += s[a * 6 + c] * sPI[li * 6 + a];
-            col[c] = acc;
-          }
-#pragma unroll
-          for (int off = TB / 2; off > 0; off >>= 1)
-#pragma unroll
-            for (int a = 0; a < 6; ++a) row[a] += __shfl_xor_sync(0xffffffffu, row[a], off, TB);
-          float* part = d.partial + (size_t)t * 2 * C::kRow;
-          if (lj == 0) {
-#pragma unroll
-            for (int a = 0; a < 6; ++a) part[li * 6 + a] = row[a];
-          }
-          if (I != J) {
-#pragma unroll
-            for (int c = 0; c < 6; ++c) colst[tid * 6 + c] = col[c];
-            __syncthreads();
-            if (tid < (uint32_t)C::kRow) {
-              const int cj = tid / 6, c = tid % 6;
-              float acc = 0.0f;
-#pragma unroll
-              for (int r2 = 0; r2 < TB; ++r2) acc += colst[(r2 * TB + cj) * 6 + c];
-              part[C::kRow + tid] = acc;
+          for (int j = 0; j < kPre; ++j) {
+            const uint32_t e = lane + 32u * j;
+            if (e < 2u * C::kRow) {
+              const float v = k > 0 ? __fmaf_rn((float)ws.beta, pre_p[j], pre_z[j]) : pre_p[j];
+              if (e < (uint32_t)C::kRow) wPI[e] = v;
+              else wPJ[e - C::kRow] = v;
             }
           }
         }
-        __syncthreads();  // buf[b] and the staging areas are free again
-        t = tn;
-        b = bn;
+        if (m + 1 < Mw) prefetch_seg(meta_nxt.x);
+        const int st = (int)(s % C::kStages);
+        trace_tile(d, k, gw, TW, m, 1);
+        const bool arrived =
+            __all_sync(0xffffffffu, mbar_wait(&mbar[warp][st], (uint32_t)((s / C::kStages) & 1),
+                                              d.error));
+        consumed = s + 1;
+        __syncwarp();  // the segments are visible to the whole warp
+        trace_tile(d, k, gw, TW, m, 2);
+        if (!arrived) ok = false;
+        if (active && arrived) {
+          // Lane l takes blocks l and l + 32: (li, lj) = (l / 8, l % 8) and
+          // (l / 8 + 4, l % 8); 16-byte reads at a 144-byte stride are free
+          // of bank conflicts within each quarter warp.
+          const float* tile = ring + (size_t)st * C::kTileFloats;
+          const int li = (int)(lane >> 3), lj = (int)(lane & 7);
+          float row[2][6], col[6];
+#pragma unroll
+          for (int c = 0; c < 6; ++c) col[c] = 0.0f;
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const float4* blk = reinterpret_cast<const float4*>(tile + (lane + 32 * h) * kBlock);
+            float sv[36];
+#pragma unroll
+            for (int q = 0; q < 9; ++q) {
+              const float4 v = blk[q];
+              sv[4 * q] = v.x;
+              sv[4 * q + 1] = v.y;
+              sv[4 * q + 2] = v.z;
+              sv[4 * q + 3] = v.w;
+            }
+            const float* pj = wPJ + lj * 6;
+            const float* pi = wPI + (li + 4 * h) * 6;
+#pragma unroll
+            for (int a = 0; a < 6; ++a) {
+              float acc = 0.0f;
+#pragma unroll
+              for (int c = 0; c < 6; ++c) acc += sv[a * 6 + c] * pj[c];
+              row[h][a] = acc;
+            }
+#pragma unroll
+            for (int c = 0; c < 6; ++c) {
+              float acc = 0.0f;
+#pragma unroll
+              for (int a = 0; a < 6; ++a) acc += sv[a * 6 + c] * pi[a];
+              col[c] += acc;
+            }
+          }
+          // Row sides: over lj (the 8 lanes of a row group) by butterfly.
+#pragma unroll
+          for (int off = 4; off > 0; off >>= 1)
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+#pragma unroll
+              for (int a = 0; a < 6; ++a)
+                row[h][a] += __shfl_xor_sync(0xffffffffu, row[h][a], off, 8);
+          float* part = d.partial + (size_t)meta.y * C::kRow;
+          if (lj == 0) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+#pragma unroll
+              for (int a = 0; a < 6; ++a) part[(li + 4 * h) * 6 + a] = row[h][a];
+          }
+          if (I != J) {
+            // Column side: over li -- the lanes of equal lj, by butterfly.
+#pragma unroll
+            for (int off = 8; off < 32; off <<= 1)
+#pragma unroll
+              for (int c = 0; c < 6; ++c) col[c] += __shfl_xor_sync(0xffffffffu, col[c], off);
+            if (li == 0) {
+              float* partc = d.partial + (size_t)meta.z * C::kRow;
+#pragma unroll
+              for (int c = 0; c < 6; ++c) partc[lj * 6 + c] = col[c];
+            }
+          }
+          if (m < 64u) {
+            done_mask |= 1ull << m;
+          } else {
+            __syncwarp();
+            if (lane == 0) {
+              red_add_release(d.row_cnt + I, 1u);
+              if (I != J) red_add_release(d.row_cnt + J, 1u);
+            }
+          }
+        }
+        __syncwarp();  // the stage and the segments are free again
+        trace_tile(d, k, gw, TW, m, 3);
+        // Refill the stage with the tile kStages ahead (possibly the next
+        // iteration's; S does not change during the solve).
+        if (lane == 0 && issued < s + 1 + C::kStages) {
+          issue(issued);
+          ++issued;
+        }
+        issued = __shfl_sync(0xffffffffu, issued, 0);
+        meta_cur = meta_nxt;
+        meta_nxt = meta_nn;
       }
-      nextbuf = b;
+      trace_warp(d, k, gw, TW, 1);
+      // Arrivals for the warp's first 64 tiles of this iteration (the rest
+      // arrived one by one above): after all of the warp's partial stores, a
+      // release fence in every lane, then relaxed increments on the rows each
+      // processed tile feeds, spread over the lanes.
+      __syncwarp();
+      if (done_mask) {
+        asm volatile("fence.acq_rel.gpu;" ::: "memory");
+        for (uint32_t m = lane; m < Mw && m < 64u; m += 32) {
+          if (!((done_mask >> m) & 1ull)) continue;
+          const uint4 meta = d.tile_meta[gw + m * TW];
+          const uint32_t I = meta.x >> 16, J = meta.x & 0xFFFFu;
+          atomicAdd(d.row_cnt + I, 1u);
+          if (I != J) atomicAdd(d.row_cnt + J, 1u);
+        }
+      }
     }
-    ok = grid_barrier(d.barrier, G, d.error, &s_flag) && ok;
+    // Row reductions by their owners: wait, bounded, for every tile of the
+    // row to arrive, then reduce.
+    for (uint32_t j = 0; j < nown; ++j) {
+      const uint32_t R = blockIdx.x + j * G;
+      scal(own_prob[j], k);
+      if (!sc.active) continue;
+      if (tid == 0) {
+        const uint32_t need = own_m1[j] - own_m0[j];
+        uint32_t spins = 0;
+        while (ld_acquire(d.row_cnt + R) < need) {
+          if (++spins > kSpinLimit) {
+            atomicOr(d.error, (unsigned int)kErrBarrierTimeout);
+            break;
+          }
+          __nanosleep(8);
+        }
+      }
+      __syncthreads();
+      reduce_row((int)j, k, sc.beta);
+    }
+    trace_mark(d, k, 2);
+    ok = grid_barrier(d.barrier, G, d.error, &s_flag, bar_gen) && ok;
+    trace_mark(d, k, 3);
     if (!ok) break;
     if (*(volatile unsigned int*)(d.barrier + 2) == 0u) break;  // every problem done
 
-    // ---- B: q = S p for owned tile rows; p written; partial p.q.
-    for (uint32_t tr = blockIdx.x; tr < d.num_tile_rows; tr += G) {
-      const uint32_t P = d.tr_prob[tr];
-      scal(P, k);
-      if (!sc.active) continue;
-      const size_t base = (size_t)tr * C::kRow;
-      double pq = 0.0;
-      if (tid < (uint32_t)C::kRow) {
-        float pv = __ldcg(d.p + base + tid);
-        if (k > 0) pv = __ldcg(d.z + base + tid) + (float)sc.beta * pv;
-        d.p[base + tid] = pv;
-        float acc = 0.0f;
-        for (uint32_t m = d.tr_list_off[tr]; m < d.tr_list_off[tr + 1]; ++m)
-          acc += __ldcg(d.partial + (size_t)d.tr_list[m] * C::kRow + tid);
-        d.q[base + tid] = acc;
-        pq = (double)pv * (double)acc;
-      }
-      pq = block_sum<double, N>(pq, red);
-      if (tid == 0) d.dots[kDotStride * (size_t)tr + kDotPq + (k & 1)] = pq;
-    }
-    ok = grid_barrier(d.barrier, G, d.error, &s_flag);
-    if (!ok) break;
-
-    // ---- C: alpha = rz / p.q; x, r, z updates; partial r.z and r.r.
+    // ---- C: alpha = rz / p.q; x, r, z updates; partial r.z and r.r, from
+    // the operands the owner holds in registers.
     uint32_t cprob = kNone;
-    for (uint32_t tr = blockIdx.x; tr < d.num_tile_rows; tr += G) {
-      const uint32_t P = d.tr_prob[tr];
+    for (uint32_t j = 0; j < nown; ++j) {
+      const uint32_t tr = blockIdx.x + j * G;
+      const uint32_t P = own_prob[j];
       scal(P, k);
       if (!sc.active) continue;
       if (cprob != P) {
-        double pq = 0.0;
-        for (uint32_t t2 = d.prob_tr_begin[P] + tid; t2 < d.prob_tr_begin[P + 1]; t2 += N)
-          pq += __ldcg(d.dots + kDotStride * (size_t)t2 + kDotPq + (k & 1));
-        pq = block_sum<double, N>(pq, red);
-        if (tid == 0) s_alpha = (pq > 0.0 && isfinite(pq)) ? sc.rz / pq : 0.0;
+        if (tid < 32) {
+          double pq = 0.0;
+          for (uint32_t t2 = d.prob_tr_begin[P] + tid; t2 < d.prob_tr_begin[P + 1]; t2 += 32)
+            pq += __ldcg(dot_at(d, kDotPq + (k & 1), t2));
+          pq = warp_sum(pq);
+          if (tid == 0) s_alpha = (pq > 0.0 && isfinite(pq)) ? sc.rz / pq : 0.0;
+        }
         __syncthreads();
         cprob = P;
       }
@@ -1336,43 +1649,49 @@ __global__ void __launch_bounds__(Pcg<TB>::kThreads) k_pcg(Dev d) {
       const size_t base = (size_t)tr * C::kRow;
       const float af = (float)alpha;
       if (tid < (uint32_t)C::kRow) {
-        const float pv = __ldcg(d.p + base + tid);
-        const float qv = __ldcg(d.q + base + tid);
-        d.x[base + tid] = __ldcg(d.x + base + tid) + af * pv;
-        const float rv = __ldcg(d.r + base + tid) - af * qv;
+        d.x[base + tid] = own_x[j] + af * own_p[j];
+        const float rv = own_r[j] - af * own_q[j];
         d.r[base + tid] = rv;
         sPI[tid] = rv;
       }
       __syncthreads();
       double rz = 0.0, rr = 0.0;
       if (tid < (uint32_t)C::kRow) {
-        const uint32_t cam = tid / 6, a = tid % 6;
-        const float* m = d.minv + 36 * (base / 6 + cam) + a * 6;
+        const uint32_t cam = tid / 6;
         float z = 0.0f;
 #pragma unroll
-        for (int b = 0; b < 6; ++b) z += m[b] * sPI[cam * 6 + b];
+        for (int b = 0; b < 6; ++b) z += own_m[j][b] * sPI[cam * 6 + b];
         d.z[base + tid] = z;
         rz = (double)sPI[tid] * (double)z;
         rr = (double)sPI[tid] * (double)sPI[tid];
       }
-      rz = block_sum<double, N>(rz, red);
-      rr = block_sum<double, N>(rr, red);
+      rz = block_sum_fast<NW>(rz, red);
+      rr = block_sum_fast<NW>(rr, red);
       if (tid == 0) {
-        double* dt = d.dots + kDotStride * (size_t)tr;
-        dt[kDotRz + mod3(k)] = rz;
-        dt[kDotRr + mod3(k)] = rr;
+        *dot_at(d, kDotRz + mod3(k), tr) = rz;
+        *dot_at(d, kDotRr + mod3(k), tr) = rr;
       }
     }
-    ok = grid_barrier(d.barrier, G, d.error, &s_flag);
+    trace_mark(d, k, 4);
+    ok = grid_barrier(d.barrier, G, d.error, &s_flag, bar_gen);
+    trace_mark(d, k, 5);
   }
-  // Drain: nothing is in flight on the normal path (every issued copy was
-  // waited for); on the error path wait (bounded) for the last copies.
-  if (!ok && tid == 0) {
-    for (int b = 0; b < 2; ++b) {
+  // Drain the copies still in flight (prefetched tiles), bounded.
+  if (lane == 0) {
+    for (uint64_t s = consumed; s < issued; ++s) {
       uint32_t spins = 0;
-      while (!mbar_try_wait(&mbar[b], (parity >> b) & 1u) && ++spins < 1024u) {
+      while (!mbar_try_wait(&mbar[warp][s % C::kStages], (uint32_t)((s / C::kStages) & 1)) &&
+             ++spins < kSpinLimit) {
       }
     }
+  }
+  // Return this warp's L2-resident tiles to the normal eviction priority.
+  for (uint32_t m = 0; m < Mw; ++m) {
+    const uint32_t t = gw + m * TW;
+    if (t >= d.l2_resident_tiles) break;
+    const char* base = reinterpret_cast<const char*>(d.tiles + (size_t)t * C::kTileFloats);
+    for (uint32_t off = lane * 128u; off < C::kTileBytes; off += 32u * 128u)
+      asm volatile("applypriority.global.L2::evict_normal [%0], 128;" ::"l"(base + off) : "memory");
   }
 }
 
@@ -1391,21 +1710,12 @@ __global__ void k_pcg_setup(Dev d) {
       s.rnorm = 0.0;
       active += on ? 1u : 0u;
     }
-    d.barrier[0] = 0u;
-    d.barrier[1] = 0u;
+    for (int w = 0; w < kBarrierWords; ++w) d.barrier[w] = 0u;
     d.barrier[2] = active;
+    for (uint32_t tr = 0; tr < d.num_tile_rows; ++tr) d.row_cnt[tr] = 0u;
   }
 }
 
-// Problems without variable cameras have no PCG; x has no entries for them.
-
-template <typename K>
-int grid_for(K kernel, int threads, size_t smem) {
-  (void)kernel;
-  (void)threads;
-  (void)smem;
-  return 0;
-}
 
 }  // namespace
 
@@ -1481,34 +1791,21 @@ cudaError_t launch_pcg_setup(const Dev& d, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-size_t pcg_smem_bytes(int tb) { return tb == 8 ? Pcg<8>::kSmem : Pcg<16>::kSmem; }
+size_t pcg_smem_bytes(int) { return Pcg::kSmem; }
 
-int pcg_grid_size(int tb, int sm_count) {
+int pcg_grid_size(int, int sm_count) {
   int per_sm = 0;
-  cudaError_t e;
-  if (tb == 8) {
-    cudaFuncSetAttribute(k_pcg<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)Pcg<8>::kSmem);
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg<8>, Pcg<8>::kThreads,
-                                                      Pcg<8>::kSmem);
-  } else {
-    cudaFuncSetAttribute(k_pcg<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)Pcg<16>::kSmem);
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg<16>, Pcg<16>::kThreads,
-                                                      Pcg<16>::kSmem);
-  }
+  cudaFuncSetAttribute(k_pcg, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Pcg::kSmem);
+  const cudaError_t e =
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg, Pcg::kThreads, Pcg::kSmem);
   if (e != cudaSuccess || per_sm <= 0) return 0;
-  return per_sm * sm_count;
+  return std::min(per_sm * sm_count, (kBarrierWords - 4) * (int)kBarGroup);
 }
 
 cudaError_t launch_pcg(const Dev& d, int grid, cudaStream_t s) {
   if (d.num_tile_rows == 0) return cudaSuccess;
   void* args[] = {const_cast<Dev*>(&d)};
-  if (d.tb == 8)
-    return cudaLaunchCooperativeKernel((const void*)k_pcg<8>, grid, Pcg<8>::kThreads, args,
-                                       Pcg<8>::kSmem, s);
-  return cudaLaunchCooperativeKernel((const void*)k_pcg<16>, grid, Pcg<16>::kThreads, args,
-                                     Pcg<16>::kSmem, s);
+  return cudaLaunchCooperativeKernel((const void*)k_pcg, grid, Pcg::kThreads, args, Pcg::kSmem, s);
 }
 
 }  // namespace vlba

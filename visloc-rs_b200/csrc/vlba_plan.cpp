@@ -403,6 +403,21 @@ void build_plan(const vlba_problem* const* problems, const vlba_config* const* c
   }
   P.num_var_cams = slot_base;
   P.num_tile_rows = tr_base;
+  // Partial slots: position of (tile, side) in the tile-row lists, so a row's
+  // partials are contiguous.
+  P.tile_slot.assign(P.tile_ij.size(), PairIdx{kNone, kNone});
+  for (uint32_t m = 0; m < (uint32_t)P.tr_list.size(); ++m) {
+    const uint32_t t = P.tr_list[m] / 2, side = P.tr_list[m] % 2;
+    if (side == 0) P.tile_slot[t].a = m;
+    else P.tile_slot[t].b = m;
+  }
+  P.tile_meta.resize(4 * P.tile_ij.size());
+  for (size_t t = 0; t < P.tile_ij.size(); ++t) {
+    P.tile_meta[4 * t] = P.tile_ij[t];
+    P.tile_meta[4 * t + 1] = P.tile_slot[t].a;
+    P.tile_meta[4 * t + 2] = P.tile_slot[t].b;
+    P.tile_meta[4 * t + 3] = P.tr_prob[P.tile_ij[t] >> 16];
+  }
   P.num_pairs = P.pairs.size();
   // Lanes per block in the off-diagonal assembly: about three points per
   // lane (the mean pair count per block sets the shape).
@@ -459,6 +474,13 @@ std::string check_plan(const Plan& P) {
     return bad("tr_list_off");
   for (uint32_t e : P.tr_list)
     if (e >= 2 * ntiles) return bad("tr_list");
+  if (P.tile_slot.size() != ntiles) return bad("tile_slot size");
+  for (uint64_t t = 0; t < ntiles; ++t) {
+    const uint32_t I = P.tile_ij[t] >> 16, J = P.tile_ij[t] & 0xFFFFu;
+    if (P.tile_slot[t].a >= P.tr_list.size()) return bad("tile_slot row");
+    if ((I != J) != (P.tile_slot[t].b != kNone)) return bad("tile_slot column presence");
+    if (I != J && P.tile_slot[t].b >= P.tr_list.size()) return bad("tile_slot column");
+  }
   if (P.tr_prob.size() != P.num_tile_rows) return bad("tr_prob");
   for (uint32_t pr : P.tr_prob)
     if (pr >= P.num_problems) return bad("tr_prob value");
@@ -497,7 +519,7 @@ size_t Plan::upload_bytes() const {
          b(points) + b(pose_slot) + b(point_var) + b(cameras) + b(pt_off) + b(obs_pose) +
          b(obs_cam) + b(obs_slot) + b(obs_xy) + b(cam_off) + b(cam_obs) + b(tile_ij) +
          b(blk_off) + b(pairs) + b(blk_dst) + b(diag_dst) + b(dup_off) + b(dup_pairs) +
-         b(tr_list_off) + b(tr_list) + b(tr_prob) + b(chunk_point_begin);
+         b(tr_list_off) + b(tr_list) + b(tr_prob) + b(chunk_point_begin) + b(tile_slot) + b(tile_meta);
 }
 
 double algorithmic_bytes(const Plan& P, double k, double* b_pcg_out) {

@@ -45,6 +45,8 @@ struct Plan {
   std::vector<uint32_t> dup_off;
   std::vector<PairIdx> dup_pairs;
   std::vector<uint32_t> tr_list_off, tr_list, tr_prob;
+  std::vector<PairIdx> tile_slot;  // per tile: partial slot of its row side, column side
+  std::vector<uint32_t> tile_meta;  // per tile: ij, row slot, column slot (or kNone), problem
   std::vector<uint32_t> chunk_point_begin;
 
   // statistics (per plan)

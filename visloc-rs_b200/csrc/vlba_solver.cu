@@ -9,8 +9,10 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <chrono>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <stdexcept>
@@ -87,6 +89,9 @@ struct Context {
   bool uploaded = false;
   int pcg_grid = 0;
   uint32_t flags = 0;  // flags of the uploaded config
+  size_t l2_bytes = 0;
+  double l2_fraction = 0.5;  // share of the L2 that keeps S resident in PCG
+  int pcg_grid_hint = 0;     // blocks of the PCG launch (trace sizing)
   // the uploaded problem's sizes (for download)
   std::vector<uint64_t> num_poses, num_points;
 };
@@ -177,14 +182,29 @@ void upload_plan(Context* c, uint32_t max_records) {
   d.p = A.alloc<float>(nvec);
   d.q = A.alloc<float>(nvec);
   VLBA_CUDA(cudaMemsetAsync(d.x, 0, nvec * 4, s));
-  d.partial = A.alloc<float>(P.tile_ij.size() * 2 * (size_t)P.tb * 6);
+  d.partial = A.alloc<float>(P.tr_list.size() * (size_t)P.tb * 6);
+  d.tile_slot = reinterpret_cast<const uint2*>(A.upload(P.tile_slot, s));
+  d.tile_meta = reinterpret_cast<const uint4*>(A.upload(P.tile_meta, s));
   d.tr_list_off = A.upload(P.tr_list_off, s);
   d.tr_list = A.upload(P.tr_list, s);
   d.tr_prob = A.upload(P.tr_prob, s);
-  d.dots = A.alloc<double>(16 * (size_t)(P.num_tile_rows ? P.num_tile_rows : 1));
-  d.barrier = A.alloc<unsigned int>(4);
+  d.dots = A.alloc<double>(9 * (size_t)(P.num_tile_rows ? P.num_tile_rows : 1));
+  d.row_cnt = A.alloc<unsigned int>(P.num_tile_rows ? P.num_tile_rows : 1);
+  VLBA_CUDA(cudaMemsetAsync(d.row_cnt, 0, 4 * (size_t)(P.num_tile_rows ? P.num_tile_rows : 1), s));
+  {
+    // L2-resident share of S: the leading tiles up to a fraction of the L2.
+    const double frac = c->l2_fraction;
+    const double budget = frac * (double)c->l2_bytes;
+    const double tile_bytes = (double)tile_floats * 4.0;
+    d.l2_resident_tiles = (uint32_t)std::min<double>((double)P.tile_ij.size(), budget / tile_bytes);
+  }
+  d.trace = nullptr;
+  if (std::getenv("VLBA_TRACE_PCG") && c->pcg_grid_hint > 0)
+    d.trace = A.alloc<unsigned long long>((size_t)kTraceIters * c->pcg_grid_hint *
+                                          (kTracePhases + 2 * 32 + 32 * 8 * 4));
+  d.barrier = A.alloc<unsigned int>(kBarrierWords);
   d.error = A.alloc<unsigned int>(1);
-  VLBA_CUDA(cudaMemsetAsync(d.barrier, 0, 16, s));
+  VLBA_CUDA(cudaMemsetAsync(d.barrier, 0, 4 * kBarrierWords, s));
   VLBA_CUDA(cudaMemsetAsync(d.error, 0, 4, s));
   d.chunk_point_begin = A.upload(P.chunk_point_begin, s);
   const size_t nch = P.chunk_point_begin.size() - 1;
@@ -192,7 +212,15 @@ void upload_plan(Context* c, uint32_t max_records) {
   d.chunk_bad = A.alloc<unsigned long long>(nch);
   d.chunk_step = A.alloc<double>(nch);
   c->dev = d;
+  // Co-resident grid, but no more blocks than tiles or tile rows to work on
+  // (fewer blocks make the grid barriers cheaper on small systems).
   c->pcg_grid = P.num_tile_rows ? pcg_grid_size((int)P.tb, c->sm_count) : 0;
+  c->pcg_grid = std::min<int>(c->pcg_grid,
+                              (int)std::max<size_t>(P.tile_ij.size(), P.num_tile_rows));
+  if (c->pcg_grid > 0 && (size_t)c->pcg_grid * 4 < P.num_tile_rows)
+    throw Status(VLBA_ERR_INVALID_ARGUMENT,
+                 "reduced system too large: more than 4 tile rows per PCG block");
+  if (d.trace && c->pcg_grid > c->pcg_grid_hint) d.trace = nullptr;  // sized for fewer blocks
   if (P.num_tile_rows && c->pcg_grid <= 0)
     throw Status(VLBA_ERR_CUDA, "the PCG kernel cannot be made co-resident on this device");
   VLBA_CUDA(cudaStreamSynchronize(s));
@@ -224,6 +252,57 @@ struct PhaseTimes {
   std::vector<double> lin, assemble, pcg, update;
 };
 
+// VLBA_TRACE_PCG: per-phase device time of the PCG iterations (mean over
+// blocks of each phase's span, and the iteration's wall span), to stderr.
+void dump_trace(Context* c) {
+  const Dev& d = c->dev;
+  const int G = c->pcg_grid;
+  std::vector<unsigned long long> t((size_t)kTraceIters * G * kTracePhases);
+  VLBA_CUDA(cudaMemcpyAsync(t.data(), d.trace, t.size() * 8, cudaMemcpyDeviceToHost, c->stream));
+  PcgState pg;
+  VLBA_CUDA(cudaMemcpyAsync(&pg, d.pcg, sizeof pg, cudaMemcpyDeviceToHost, c->stream));
+  VLBA_CUDA(cudaStreamSynchronize(c->stream));
+  const int iters = std::min<int>((int)pg.iters, kTraceIters - 1);
+  double acc[kTracePhases] = {0};
+  double wall = 0.0;
+  for (int k = 0; k < iters; ++k) {
+    unsigned long long lo = ~0ull, hi = 0;
+    for (int b = 0; b < G; ++b) {
+      const unsigned long long* r = &t[((size_t)k * G + b) * kTracePhases];
+      for (int ph = 1; ph < kTracePhases; ++ph) acc[ph] += (double)(r[ph] - r[ph - 1]) / G;
+      lo = std::min(lo, r[0]);
+      hi = std::max(hi, r[kTracePhases - 1]);
+    }
+    wall += (double)(hi - lo);
+  }
+  const char* path = std::getenv("VLBA_TRACE_PCG");
+  if (path && path[0] == '/') {  // raw dump: G, iterations, then the stamps
+    if (FILE* f = std::fopen(path, "ab")) {
+      const int32_t hdr[3] = {G, iters, kTracePhases};
+      std::fwrite(hdr, sizeof hdr, 1, f);
+      std::fwrite(t.data(), 8, (size_t)iters * G * kTracePhases, f);
+      // Per-warp marks (warps per block from the kernel's configuration).
+      const size_t tw = (size_t)G * 8;
+      std::vector<unsigned long long> w((size_t)kTraceIters * tw * 2);
+      VLBA_CUDA(cudaMemcpy(w.data(), d.trace + (size_t)kTraceIters * G * kTracePhases,
+                           w.size() * 8, cudaMemcpyDeviceToHost));
+      std::fwrite(w.data(), 8, (size_t)iters * tw * 2, f);
+      std::vector<unsigned long long> tt((size_t)kTraceIters * tw * 8 * 4);
+      VLBA_CUDA(cudaMemcpy(tt.data(), d.trace + (size_t)kTraceIters * G * kTracePhases +
+                                          (size_t)kTraceIters * tw * 2,
+                           tt.size() * 8, cudaMemcpyDeviceToHost));
+      std::fwrite(tt.data(), 8, (size_t)iters * tw * 8 * 4, f);
+      std::fclose(f);
+    }
+  }
+  if (iters > 0)
+    std::fprintf(stderr,
+                 "vlba pcg trace: %u iterations, per iteration (us): status %.2f tiles %.2f "
+                 "arrive+reduce %.2f barrier1 %.2f update %.2f barrier2 %.2f | span %.2f\n",
+                 pg.iters, acc[1] / iters / 1e3, acc[2] / iters / 1e3, 0.0, acc[3] / iters / 1e3,
+                 acc[4] / iters / 1e3, acc[5] / iters / 1e3, wall / iters / 1e3);
+}
+
 // The device LM loop over all uploaded problems.
 RunStats run_lm(Context* c, bool profile, PhaseTimes* pt) {
   Dev& d = c->dev;
@@ -247,6 +326,7 @@ RunStats run_lm(Context* c, bool profile, PhaseTimes* pt) {
     check_launch(launch_pcg_setup(d, s), "pcg setup");
     if (profile) VLBA_CUDA(cudaEventRecord(c->ev[3], s));
     check_launch(launch_pcg(d, c->pcg_grid, s), "pcg");
+    if (d.trace) dump_trace(c);
     if (profile) VLBA_CUDA(cudaEventRecord(c->ev[4], s));
     check_launch(launch_pose_update(d, s), "pose update");
     check_launch(launch_cost(d, true, s), "trial cost");
@@ -337,7 +417,8 @@ int pick_tb(const vlba_problem* const* probs, uint32_t n) {
     vars += v;
   }
   const double mean = n ? (double)vars / n : 0.0;
-  return mean >= 48.0 ? 16 : 8;
+  (void)mean;
+  return 8;  // the PCG streams 8 x 8-block tiles, one warp per tile
 }
 
 template <typename F>
@@ -427,6 +508,9 @@ void* visloc_ba_cuda_create(int device) {
     VLBA_CUDA(cudaGetDeviceProperties(&prop, device));
     if (prop.major < 10) throw std::runtime_error("requires an sm_100 (Blackwell) device");
     c->sm_count = prop.multiProcessorCount;
+    c->l2_bytes = (size_t)prop.l2CacheSize;
+    c->pcg_grid_hint = 4 * prop.multiProcessorCount;
+    if (const char* f = std::getenv("VLBA_L2_RESIDENT_FRACTION")) c->l2_fraction = std::atof(f);
     VLBA_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     for (auto& e : c->ev) VLBA_CUDA(cudaEventCreate(&e));
   } catch (...) {
@@ -564,6 +648,119 @@ int visloc_ba_cuda_plan(const vlba_problem* problem, const vlba_config* config,
       info->bytes_per_iteration = vlba::algorithmic_bytes(plan, pcg_iterations, &b_pcg);
       info->bytes_per_pcg_iteration = b_pcg;
     }
+  });
+}
+
+namespace vlba {
+namespace {
+// Upload one problem and linearise it at its state with damping `lambda`
+// (init + linearize + point prep + assembly).
+void prepare_system(Context* c, const vlba_problem* problem, const vlba_config* config,
+                    double lambda) {
+  vlba_config cfg = *config;
+  cfg.max_iterations = 1;
+  const vlba_problem* probs[1] = {problem};
+  const vlba_config* cfgs[1] = {&cfg};
+  do_upload(c, probs, cfgs, 1, 1, nullptr);
+  reset_state(c);
+  Dev& d = c->dev;
+  cudaStream_t s = c->stream;
+  check_launch(launch_pose_table(d, s), "pose table");
+  check_launch(launch_cost(d, false, s), "cost");
+  check_launch(launch_decide(d, true, s), "init");
+  VLBA_CUDA(cudaMemcpyAsync(&d.ctrl[0].lambda, &lambda, sizeof lambda, cudaMemcpyHostToDevice, s));
+  check_launch(launch_linearize(d, s), "linearize");
+  check_launch(launch_point_prep(d, s), "point prep");
+  check_launch(launch_offdiag(d, s), "off-diagonal blocks");
+  check_launch(launch_cam_diag(d, s), "camera blocks");
+}
+}  // namespace
+}  // namespace vlba
+
+int visloc_ba_cuda_linear_step(void* ctx, const vlba_problem* problem, const vlba_config* config,
+                               double lambda, double* dp, double* dl, uint32_t* pcg_iterations,
+                               double* pcg_relative_residual) {
+  auto* c = static_cast<Context*>(ctx);
+  if (!c || !problem || !config) return VLBA_ERR_INVALID_ARGUMENT;
+  return vlba::guarded(c, [&] {
+    vlba::prepare_system(c, problem, config, lambda);
+    vlba::Dev& d = c->dev;
+    cudaStream_t s = c->stream;
+    vlba::check_launch(vlba::launch_pcg_setup(d, s), "pcg setup");
+    vlba::check_launch(vlba::launch_pcg(d, c->pcg_grid, s), "pcg");
+    if (d.trace) vlba::dump_trace(c);
+    vlba::check_launch(vlba::launch_pose_update(d, s), "pose update");
+    vlba::check_launch(vlba::launch_cost(d, true, s), "back-substitution");
+    const vlba::Plan& P = c->plan;
+    std::vector<float> x((size_t)P.num_var_cams * 6);
+    if (!x.empty())
+      VLBA_CUDA(cudaMemcpyAsync(x.data(), d.x, x.size() * 4, cudaMemcpyDeviceToHost, s));
+    std::vector<double> pts0(P.points.size()), pts1(P.points.size());
+    VLBA_CUDA(cudaMemcpyAsync(pts0.data(), d.points[0], pts0.size() * 8, cudaMemcpyDeviceToHost, s));
+    VLBA_CUDA(cudaMemcpyAsync(pts1.data(), d.points[1], pts1.size() * 8, cudaMemcpyDeviceToHost, s));
+    vlba::PcgState pg;
+    VLBA_CUDA(cudaMemcpyAsync(&pg, d.pcg, sizeof pg, cudaMemcpyDeviceToHost, s));
+    unsigned int err = 0;
+    VLBA_CUDA(cudaMemcpyAsync(&err, d.error, 4, cudaMemcpyDeviceToHost, s));
+    VLBA_CUDA(cudaStreamSynchronize(s));
+    if (err) throw vlba::Status(VLBA_ERR_TIMEOUT, "a bounded device wait gave up");
+    if (dp) {
+      size_t n = 0;
+      for (size_t i = 0; i < P.pose_slot.size(); ++i)
+        if (P.pose_slot[i] != vlba::kNone) {
+          for (int a = 0; a < 6; ++a) dp[6 * n + a] = x[6 * (size_t)P.pose_slot[i] + a];
+          ++n;
+        }
+    }
+    if (dl) {
+      size_t n = 0;
+      for (size_t j = 0; j < P.point_var.size(); ++j)
+        if (P.point_var[j]) {
+          for (int a = 0; a < 3; ++a) dl[3 * n + a] = pts1[3 * j + a] - pts0[3 * j + a];
+          ++n;
+        }
+    }
+    if (pcg_iterations) *pcg_iterations = pg.iters;
+    if (pcg_relative_residual) *pcg_relative_residual = pg.bnorm > 0 ? pg.rnorm / pg.bnorm : 0.0;
+  });
+}
+
+int visloc_ba_cuda_reduced_system(void* ctx, const vlba_problem* problem,
+                                  const vlba_config* config, double lambda, double* s_dense,
+                                  double* rhs) {
+  auto* c = static_cast<Context*>(ctx);
+  if (!c || !problem || !config) return VLBA_ERR_INVALID_ARGUMENT;
+  return vlba::guarded(c, [&] {
+    vlba::prepare_system(c, problem, config, lambda);
+    vlba::Dev& d = c->dev;
+    const vlba::Plan& P = c->plan;
+    const size_t tile_floats = (size_t)P.tb * P.tb * vlba::kBlock;
+    std::vector<float> tiles(P.tile_ij.size() * tile_floats), r((size_t)P.num_var_cams * 6);
+    VLBA_CUDA(cudaMemcpyAsync(tiles.data(), d.tiles, tiles.size() * 4, cudaMemcpyDeviceToHost, c->stream));
+    if (!r.empty())
+      VLBA_CUDA(cudaMemcpyAsync(r.data(), d.rhs, r.size() * 4, cudaMemcpyDeviceToHost, c->stream));
+    VLBA_CUDA(cudaStreamSynchronize(c->stream));
+    // Variable slot -> dense index (slots are the variable poses in order).
+    const size_t nc = P.real_var_cams, dim = 6 * nc;
+    if (s_dense) {
+      std::fill(s_dense, s_dense + dim * dim, 0.0);
+      for (size_t t = 0; t < P.tile_ij.size(); ++t) {
+        const uint32_t I = P.tile_ij[t] >> 16, J = P.tile_ij[t] & 0xFFFFu;
+        for (uint32_t li = 0; li < P.tb; ++li)
+          for (uint32_t lj = 0; lj < P.tb; ++lj) {
+            const size_t i = (size_t)I * P.tb + li, j = (size_t)J * P.tb + lj;
+            if (i >= nc || j >= nc) continue;
+            const float* blk = &tiles[t * tile_floats + (li * P.tb + lj) * vlba::kBlock];
+            for (int a = 0; a < 6; ++a)
+              for (int b = 0; b < 6; ++b) {
+                s_dense[(6 * i + a) * dim + 6 * j + b] = blk[a * 6 + b];
+                if (I != J) s_dense[(6 * j + b) * dim + 6 * i + a] = blk[a * 6 + b];
+              }
+          }
+      }
+    }
+    if (rhs)
+      for (size_t e = 0; e < dim; ++e) rhs[e] = r[e];
   });
 }
 

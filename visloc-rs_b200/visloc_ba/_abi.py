@@ -186,6 +186,15 @@ SOLVER_EXPORTS = {
     ),
     "visloc_ba_cuda_download": (C.c_int, [C.c_void_p, P(Problem)]),
     "visloc_ba_cuda_plan": (C.c_int, [P(Problem), P(Config), C.c_double, P(PlanInfo)]),
+    "visloc_ba_cuda_linear_step": (
+        C.c_int,
+        [C.c_void_p, P(Problem), P(Config), C.c_double, P(C.c_double), P(C.c_double),
+         P(C.c_uint32), P(C.c_double)],
+    ),
+    "visloc_ba_cuda_reduced_system": (
+        C.c_int,
+        [C.c_void_p, P(Problem), P(Config), C.c_double, P(C.c_double), P(C.c_double)],
+    ),
     "visloc_ba_cuda_cost": (
         C.c_int,
         [C.c_void_p, P(Problem), P(Config), P(C.c_double), P(C.c_uint64)],

@@ -108,6 +108,40 @@ class CudaSolver:
     def download(self, packed: PackedProblem) -> int:
         return self.lib.visloc_ba_cuda_download(self.ctx, C.byref(packed.abi()))
 
+    def linear_step(self, packed: PackedProblem, config: BaConfig, lam: float):
+        """One damped step at the current state: (dp (6 per variable pose),
+        dl (3 per variable landmark), PCG iterations, PCG relative residual)."""
+        import numpy as np
+
+        npv = int(packed.num_poses - (0 if packed.pose_fixed is None else packed.pose_fixed.sum()))
+        nlv = int(packed.num_landmarks
+                  - (0 if packed.landmark_fixed is None else packed.landmark_fixed.sum()))
+        dp = np.zeros(6 * npv)
+        dl = np.zeros(3 * nlv)
+        it = C.c_uint32()
+        rr = C.c_double()
+        st = self.lib.visloc_ba_cuda_linear_step(
+            self.ctx, C.byref(packed.abi()), C.byref(config.to_abi()), float(lam),
+            dp.ctypes.data_as(C.POINTER(C.c_double)), dl.ctypes.data_as(C.POINTER(C.c_double)),
+            C.byref(it), C.byref(rr))
+        if st != _abi.OK:
+            raise SolverError(st, self.last_error())
+        return dp, dl, it.value, rr.value
+
+    def reduced_system(self, packed: PackedProblem, config: BaConfig, lam: float):
+        """The assembled damped reduced system (S dense, rhs) at the state."""
+        import numpy as np
+
+        npv = int(packed.num_poses - (0 if packed.pose_fixed is None else packed.pose_fixed.sum()))
+        s = np.zeros((6 * npv, 6 * npv))
+        rhs = np.zeros(6 * npv)
+        st = self.lib.visloc_ba_cuda_reduced_system(
+            self.ctx, C.byref(packed.abi()), C.byref(config.to_abi()), float(lam),
+            s.ctypes.data_as(C.POINTER(C.c_double)), rhs.ctypes.data_as(C.POINTER(C.c_double)))
+        if st != _abi.OK:
+            raise SolverError(st, self.last_error())
+        return s, rhs
+
     def cost(self, packed: PackedProblem, config: BaConfig | None = None):
         config = config or BaConfig()
         c = C.c_double()
