@@ -291,6 +291,39 @@ int visloc_ba_cuda_reduced_system(void* ctx, const vlba_problem* problem,
                                   const vlba_config* config, double lambda,
                                   double* s_dense, double* rhs);
 
+/* ----------------------------------------------------- allocation-free cost */
+/* No counterpart in the reference: an addition for callers that cannot
+ * allocate device memory when they need a cost -- a tracking thread with a
+ * frame deadline, where cudaMalloc/cudaFree may synchronise the device and
+ * stall it, or a process whose device memory belongs to another allocator.
+ *
+ * The same robust cost and non-projectable count as visloc_ba_cuda_cost, for
+ * a problem whose arrays are already in DEVICE memory: pose_q, pose_t,
+ * landmarks, obs_pose, obs_landmark, obs_xy and obs_camera are device
+ * pointers; `cameras` (at most VLBA_NOALLOC_MAX_CAMERAS) is read on the host
+ * during the call; pose_fixed and landmark_fixed are ignored.  `cost` (one
+ * double) and `counts` (two words: non-projectable observations, and
+ * observations skipped for a pose, landmark or camera index out of range)
+ * are device pointers, written by a kernel enqueued on `stream` (a
+ * cudaStream_t of the current device; NULL = default stream); the call
+ * returns without waiting for it.
+ *
+ * Nothing is allocated: the kernel's scratch is a fixed 1 MiB array in the
+ * library's device code, held by every GPU that loads the library, which
+ * limits a call to VLBA_NOALLOC_MAX_OBSERVATIONS observations (larger
+ * problems return VLBA_ERR_INVALID_ARGUMENT).  All calls on a device share
+ * that array: calls whose kernels may overlap on the GPU race and must be
+ * serialised by the caller.  The first call on each device looks the
+ * array's address up (set-up); make it before any stream capture.
+ * `error` (capacity `error_capacity`, may be NULL) receives a message when
+ * the status is not VLBA_OK. */
+#define VLBA_NOALLOC_MAX_OBSERVATIONS 16777216ull
+#define VLBA_NOALLOC_MAX_CAMERAS 16u
+int visloc_ba_cuda_cost_noalloc(const vlba_problem* problem,
+                                const vlba_config* config, void* stream,
+                                double* cost, uint64_t* counts, char* error,
+                                size_t error_capacity);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,145 @@
+"""visloc_ba_cuda_cost_noalloc: the robust cost without any device allocation.
+
+The entry point serves callers that cannot allocate device memory when they
+need a cost -- a tracking thread with a frame deadline, where cudaMalloc and
+cudaFree may synchronise the device and stall it, or a process whose device
+memory belongs to another allocator.  Their problem arrays are already on the
+device; the library evaluates the cost there with a fixed scratch array of its
+own.  These tests hold it to visloc_ba_cuda_cost (which builds its own device
+copy of the problem) within that entry point's tolerance against the oracle,
+on calls made back to back so that each call meets the scratch contents the
+previous one left.
+
+The file name puts it last in collection order: a run that stops at the first
+failure has run every other test before this one.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from visloc_ba import BaConfig, PackedProblem, RobustKernel, synth
+from visloc_ba import _abi
+
+COST_RTOL = 1e-12  # the cost tolerance of the GPU-vs-oracle cost test
+MAX_OBS = 16777216  # VLBA_NOALLOC_MAX_OBSERVATIONS
+
+
+class DeviceProblem:
+    """A PackedProblem's arrays copied into device memory (by torch, on the
+    test's side: the entry point under test allocates nothing itself)."""
+
+    def __init__(self, packed: PackedProblem):
+        import torch
+
+        self.packed = packed
+        self.keep = []
+
+        def dev(a, ctype):
+            if a is None:
+                return None
+            t = torch.from_numpy(np.ascontiguousarray(a)).cuda()
+            self.keep.append(t)
+            return C.cast(C.c_void_p(t.data_ptr()), C.POINTER(ctype))
+
+        p = packed.abi()  # host cameras; array fields replaced below
+        p.pose_q = dev(packed.pose_q, C.c_double)
+        p.pose_t = dev(packed.pose_t, C.c_double)
+        p.landmarks = dev(packed.landmarks, C.c_double)
+        p.obs_pose = dev(packed.obs_pose, C.c_uint32)
+        p.obs_landmark = dev(packed.obs_landmark, C.c_uint32)
+        p.obs_xy = dev(packed.obs_xy, C.c_double)
+        if packed.obs_camera is not None:
+            p.obs_camera = dev(packed.obs_camera, C.c_uint32)
+        self.abi = p
+        self.cost = torch.empty(1, dtype=torch.float64, device="cuda")
+        self.counts = torch.empty(2, dtype=torch.int64, device="cuda")
+
+
+def noalloc_cost(lib, dp: DeviceProblem, cfg: BaConfig):
+    import torch
+
+    dp.cost.fill_(float("nan"))
+    dp.counts.fill_(-1)
+    err = C.create_string_buffer(256)
+    stream = torch.cuda.current_stream().cuda_stream
+    st = lib.visloc_ba_cuda_cost_noalloc(
+        C.byref(dp.abi), C.byref(cfg.to_abi()), C.c_void_p(stream),
+        C.c_void_p(dp.cost.data_ptr()), C.c_void_p(dp.counts.data_ptr()), err, len(err))
+    assert st == _abi.OK, err.value.decode()
+    torch.cuda.current_stream().synchronize()
+    counts = dp.counts.cpu().numpy()
+    return float(dp.cost.cpu().item()), int(counts[0]), int(counts[1])
+
+
+def problems():
+    shared = synth.ring_problem(40, 4000, seed=2, width=2000, height=1500, focal=(1500, 1500),
+                                k1=(0.0, 0.0), per_camera_intrinsics=False,
+                                track=("geometric", 8.0, 2, 40))
+    return [
+        ("ring-12-per-camera-radial", synth.ring_problem(12, 1500, seed=71)),
+        ("ring-40-shared-pinhole", shared),
+        ("stereo-window", synth.stereo_window(20, 1500, seed=6)),
+        ("pose-only", synth.pose_only(800, seed=4)),
+    ]
+
+
+KERNELS = [RobustKernel.none(), RobustKernel.huber(1.0), RobustKernel.cauchy(2.0)]
+
+
+@pytest.mark.gpu
+def test_matches_the_allocating_cost_on_calls_in_a_row(solver):
+    lib = solver.lib
+    cases = [(name, DeviceProblem(p)) for name, p in problems()]
+    # Back to back: each problem twice, then the next one (a smaller problem
+    # after a larger one meets the larger one's partials in the scratch).
+    for kernel in KERNELS:
+        cfg = BaConfig(robust_kernel=kernel)
+        for name, dp in cases:
+            want, want_bad = solver.cost(dp.packed, cfg)
+            for _ in range(2):
+                got, bad, invalid = noalloc_cost(lib, dp, cfg)
+                assert invalid == 0, name
+                assert bad == want_bad, name
+                assert got == pytest.approx(want, rel=COST_RTOL), (name, got, want)
+
+
+@pytest.mark.gpu
+def test_out_of_range_indices_are_counted_and_skipped(solver):
+    lib = solver.lib
+    p = synth.ring_problem(12, 800, seed=72)
+    cfg = BaConfig(robust_kernel=RobustKernel.huber(1.0))
+    broken = PackedProblem(p.pose_q, p.pose_t, p.landmarks, p.obs_pose.copy(),
+                           p.obs_landmark.copy(), p.obs_xy, p.cameras, p.pose_fixed,
+                           p.landmark_fixed, p.obs_camera)
+    broken.obs_pose[5] = p.num_poses
+    broken.obs_landmark[17] = p.num_landmarks + 3
+    keep = np.ones(p.num_observations, bool)
+    keep[[5, 17]] = False
+    trimmed = PackedProblem(p.pose_q, p.pose_t, p.landmarks, p.obs_pose[keep],
+                            p.obs_landmark[keep], p.obs_xy[keep], p.cameras, p.pose_fixed,
+                            p.landmark_fixed, p.obs_camera[keep])
+    want, want_bad = solver.cost(trimmed, cfg)
+    dp = DeviceProblem(broken)
+    for _ in range(2):
+        got, bad, invalid = noalloc_cost(lib, dp, cfg)
+        assert invalid == 2 and bad == want_bad
+        assert got == pytest.approx(want, rel=COST_RTOL)
+
+
+def test_rejects_more_observations_than_the_scratch_holds():
+    """Rejected on the host before any device work (no GPU needed)."""
+    lib = _abi.load_solver_library()
+    p = synth.ring_problem(6, 50, seed=3).abi()
+    p.num_observations = MAX_OBS + 1
+    cost = C.c_double()
+    counts = (C.c_uint64 * 2)()
+    err = C.create_string_buffer(256)
+    st = lib.visloc_ba_cuda_cost_noalloc(C.byref(p), C.byref(BaConfig().to_abi()), None,
+                                         C.cast(C.byref(cost), C.c_void_p),
+                                         C.cast(counts, C.c_void_p), err, len(err))
+    assert st == _abi.ERR_INVALID_ARGUMENT
+    assert b"at most 16777216" in err.value

@@ -199,6 +199,11 @@ SOLVER_EXPORTS = {
         C.c_int,
         [C.c_void_p, P(Problem), P(Config), P(C.c_double), P(C.c_uint64)],
     ),
+    # Device pointers for the problem arrays and both outputs; see the header.
+    "visloc_ba_cuda_cost_noalloc": (
+        C.c_int,
+        [P(Problem), P(Config), C.c_void_p, C.c_void_p, C.c_void_p, C.c_char_p, C.c_size_t],
+    ),
 }
 
 PACKAGE_DIR = os.path.dirname(os.path.abspath(__file__))
