@@ -6,8 +6,10 @@
 //   points     f64 xyz, current and candidate;
 //   obs        sorted point-major: pose, point, variable-camera slot, camera
 //              model, pixel (f64), and two linearisation records per obs:
-//              H_o = w J_l^T J_l (upper 3x3, f32, plus point index and slot)
-//              and e_o = w J_l^T r (f32);
+//              H_o = w J_l^T J_l (upper 3x3, f32, plus point index and the
+//              point's z) and e_o = w J_l^T r (f32); per trial, a copy of the
+//              point's damped inverse and x, y next to each observation, so
+//              that a Schur term reads three 32-byte records;
 //   S          the reduced camera system in dense TB x TB tiles of 6x6 f32
 //              blocks (lower block triangle; diagonal tiles stored full);
 //   vectors    PCG x, r, z, p, q in f32, 6 per variable camera, tile padded.
@@ -149,8 +151,10 @@ struct Dev {
   const uint32_t* obs_cam;     // [K] camera index
   const uint32_t* obs_slot;    // [K] variable slot of the pose or kNone
   const double2* obs_xy;       // [K]
-  float4* obs_h;               // [2 K]: {h00,h01,h02,h11} {h12,h22,point,slot}
+  float4* obs_h;               // [2 K]: {h00,h01,h02,h11} {h12,h22,point,X.z}
   float4* obs_e;               // [K]:   {e0,e1,e2,w}
+  float4* obs_p;               // [2 K]: the observation's point, per trial:
+                               //        {hinv00,01,02,11} {hinv12,22,X.x,X.y}
 
   // per-camera observation lists (indices into the point-major order)
   const uint32_t* cam_off;     // [num_var_cams + 1]

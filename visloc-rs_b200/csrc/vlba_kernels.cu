@@ -139,6 +139,19 @@ __device__ bool chol_inverse6(const double* a, double* inv) {
   return true;
 }
 
+// 32-byte vector load (read-only path) and store: one request per 32-byte
+// sector on sm_100.  The address must be 32-byte aligned.
+__device__ __forceinline__ void ld8(const float4* p, float4& a, float4& b) {
+  asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+      : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
+      : "l"(p));
+}
+__device__ __forceinline__ void st8(float4* p, float4 a, float4 b) {
+  asm volatile("st.global.v8.f32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(p), "f"(a.x), "f"(a.y),
+               "f"(a.z), "f"(a.w), "f"(b.x), "f"(b.y), "f"(b.z), "f"(b.w)
+               : "memory");
+}
+
 // ------------------------------------------------------------ pose table
 __global__ void __launch_bounds__(256) k_pose_table(Dev d) {
   for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < d.num_poses;
@@ -215,8 +228,7 @@ __global__ void __launch_bounds__(256) k_linearize(Dev d) {
         e[2] = wf * (jl[2] * r0 + jl[5] * r1);
       }
       d.obs_h[2 * (size_t)k] = make_float4(h[0], h[1], h[2], h[3]);
-      d.obs_h[2 * (size_t)k + 1] =
-          make_float4(h[4], h[5], __uint_as_float(l), __uint_as_float(d.obs_slot[k]));
+      d.obs_h[2 * (size_t)k + 1] = make_float4(h[4], h[5], __uint_as_float(l), (float)X[2]);
       d.obs_e[k] = make_float4(e[0], e[1], e[2], wf);
 #pragma unroll
       for (int a = 0; a < 6; ++a) hl[a] += h[a];
@@ -279,8 +291,14 @@ __global__ void __launch_bounds__(256) k_point_prep(Dev d) {
       }
     }
     float4* ps = d.pt_s + 4 * (size_t)l;
-    ps[0] = make_float4((float)inv[0], (float)inv[1], (float)inv[2], (float)inv[3]);
-    ps[1] = make_float4((float)inv[4], (float)inv[5], X0, X1);
+    const float4 p0 = make_float4((float)inv[0], (float)inv[1], (float)inv[2], (float)inv[3]);
+    const float4 p1 = make_float4((float)inv[4], (float)inv[5], X0, X1);
+    ps[0] = p0;
+    ps[1] = p1;
+    // The same 32 bytes beside each observation of a variable point (read by
+    // the off-diagonal assembly next to the observation's own record).
+    if (d.point_var[l])
+      for (uint32_t k = d.pt_off[l]; k < d.pt_off[l + 1]; ++k) st8(d.obs_p + 2 * (size_t)k, p0, p1);
     ps[2] = make_float4(X2, (float)v[0], (float)v[1], (float)v[2]);
     ps[3] = make_float4((float)g[0], (float)g[1], (float)g[2], ok);
   }
@@ -292,8 +310,13 @@ __global__ void __launch_bounds__(256) k_point_prep(Dev d) {
 // (Kahan) FP32 sums, then a fixed butterfly over the group.  Deterministic,
 // no atomics; the destination is the block's slot in its dense tile (and the
 // mirrored slot inside a diagonal tile).
+//
+// A term reads three 32-byte records with one request each -- H_i (with the
+// point's z), the point's damped inverse and x, y stored beside observation
+// i, and H_j -- all addressed by the pair entry, whose successor is fetched
+// while the current term is computed.
 template <int G>
-__global__ void __launch_bounds__(256) k_offdiag(Dev d) {
+__global__ void __launch_bounds__(256, 2) k_offdiag(Dev d) {
   constexpr int kPerWarp = 32 / G;
   const uint32_t lane = threadIdx.x % G;
   const uint32_t warp_global = (blockIdx.x * blockDim.x + threadIdx.x) / 32;
@@ -319,17 +342,17 @@ __global__ void __launch_bounds__(256) k_offdiag(Dev d) {
       acc[e] = 0.0f;
       cmp[e] = 0.0f;
     }
-    if (valid) {
+    if (valid && c0 + lane < c1) {
+      uint2 pr = d.pairs[c0 + lane];
       for (uint32_t cidx = c0 + lane; cidx < c1; cidx += G) {
-        const uint2 pr = d.pairs[cidx];
-        const float4 a0 = d.obs_h[2 * (size_t)pr.x], a1 = d.obs_h[2 * (size_t)pr.x + 1];
-        const float4 b0 = d.obs_h[2 * (size_t)pr.y], b1 = d.obs_h[2 * (size_t)pr.y + 1];
-        const uint32_t l = __float_as_uint(a1.z);
-        const float4 s0 = d.pt_s[4 * (size_t)l], s1 = d.pt_s[4 * (size_t)l + 1],
-                     s2 = d.pt_s[4 * (size_t)l + 2];
+        float4 a0, a1, p0, p1, b0, b1;
+        ld8(d.obs_h + 2 * (size_t)pr.x, a0, a1);
+        ld8(d.obs_p + 2 * (size_t)pr.x, p0, p1);
+        ld8(d.obs_h + 2 * (size_t)pr.y, b0, b1);
+        if (cidx + G < c1) pr = d.pairs[cidx + G];
         const float Hi[9] = {a0.x, a0.y, a0.z, a0.y, a0.w, a1.x, a0.z, a1.x, a1.y};
         const float Hj[9] = {b0.x, b0.y, b0.z, b0.y, b0.w, b1.x, b0.z, b1.x, b1.y};
-        const float Mi[9] = {s0.x, s0.y, s0.z, s0.y, s0.w, s1.x, s0.z, s1.x, s1.y};
+        const float Mi[9] = {p0.x, p0.y, p0.z, p0.y, p0.w, p1.x, p0.z, p1.x, p1.y};
         float M[9], K[9];
 #pragma unroll
         for (int r = 0; r < 3; ++r)
@@ -344,7 +367,7 @@ __global__ void __launch_bounds__(256) k_offdiag(Dev d) {
             K[r * 3 + cc] = Hi[r * 3] * M[cc] + Hi[r * 3 + 1] * M[3 + cc] +
                             Hi[r * 3 + 2] * M[6 + cc];
         float blk[36];
-        btkb<float>(K, s1.z, s1.w, s2.x, blk);
+        btkb<float>(K, p1.z, p1.w, a1.w, blk);
 #pragma unroll
         for (int e = 0; e < 36; ++e) {  // acc -= blk, Kahan compensated
           const float y = -blk[e] - cmp[e];
@@ -1137,13 +1160,17 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
   }
   __syncthreads();
   // Warp tile sequence s = k Mw + m: stage s % kStages, phase (s / kStages) & 1.
+  // `issued` (sequence number of the next copy) and `iss_m` (its tile index
+  // m, kept modulo Mw by increments) are tracked by lane 0 alone.
   uint64_t issued = 0, consumed = 0;
-  auto tile_of = [&](uint64_t s) -> uint32_t { return gw + (uint32_t)(s % Mw) * TW; };
-  auto issue = [&](uint64_t s) {  // lane 0 only
-    const uint32_t t = tile_of(s);
-    const int st = (int)(s % C::kStages);
+  uint32_t iss_m = 0;
+  auto issue = [&]() {  // lane 0 only
+    const uint32_t t = gw + iss_m * TW;
+    const int st = (int)(issued % C::kStages);
     tma_load(ring + (size_t)st * C::kTileFloats, d.tiles + (size_t)t * C::kTileFloats,
              C::kTileBytes, &mbar[warp][st], t < d.l2_resident_tiles ? keep : stream);
+    ++issued;
+    iss_m = (iss_m + 1u == Mw) ? 0u : iss_m + 1u;
   };
   bool ok = true;
 
@@ -1281,8 +1308,7 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
   const uint4 meta1 = Mw > 1 ? d.tile_meta[gw + TW] : make_uint4(0u, 0u, 0u, 0u);
   // The first tiles of every warp go out before the barrier.
   if (lane == 0)
-    for (; issued < (uint64_t)C::kStages && issued < Mw; ++issued) issue(issued);
-  issued = __shfl_sync(0xffffffffu, issued, 0);
+    while (issued < (uint64_t)C::kStages && issued < Mw) issue();
   ok = grid_barrier(d.barrier, G, d.error, &s_flag, bar_gen);
 
   for (int k = 0; ok; ++k) {
@@ -1350,7 +1376,7 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
         trace_tile(d, k, gw, TW, m, 0);
         const uint4 meta = meta_cur;
         uint4 meta_nn = make_uint4(0u, 0u, 0u, 0u);
-        if (m + 2 < Mw) meta_nn = d.tile_meta[tile_of(s + 2)];
+        if (m + 2 < Mw) meta_nn = d.tile_meta[gw + (m + 2) * TW];
         const uint32_t I = meta.x >> 16, J = meta.x & 0xFFFFu;
         const uint32_t P = meta.w;
         if (P != wprob) {
@@ -1459,11 +1485,7 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
         trace_tile(d, k, gw, TW, m, 3);
         // Refill the stage with the tile kStages ahead (possibly the next
         // iteration's; S does not change during the solve).
-        if (lane == 0 && issued < s + 1 + C::kStages) {
-          issue(issued);
-          ++issued;
-        }
-        issued = __shfl_sync(0xffffffffu, issued, 0);
+        if (lane == 0 && issued < s + 1 + C::kStages) issue();
         meta_cur = meta_nxt;
         meta_nxt = meta_nn;
       }

@@ -501,7 +501,7 @@ size_t Plan::device_bytes() const {
   size_t b = 0;
   b += npose * (8 * (4 + 3 + 12) * 2 + 8 + 4 + 4);  // state x2, step, slot, prob
   b += npt * (8 * 3 * 2 + 4 + 1 + 4 + 36 + 64);     // points x2, off, var, prob, pt_h, pt_s
-  b += nobs * (4 * 3 + 16 + 32 + 16);                // pose, cam, slot, xy, obs_h, obs_e
+  b += nobs * (4 * 3 + 16 + 32 + 16 + 32);           // pose, cam, slot, xy, obs_h, obs_e, obs_p
   b += cam_obs.size() * 4 + pairs.size() * 8 + dup_pairs.size() * 8;
   b += blk_dst.size() * (8 + 4);
   b += tile_ij.size() * ((size_t)tb * tb * kBlock * 4 + 4 + 2 * (size_t)tb * 6 * 4);

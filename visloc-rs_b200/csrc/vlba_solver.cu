@@ -158,6 +158,7 @@ void upload_plan(Context* c, uint32_t max_records) {
   }
   d.obs_h = A.alloc<float4>(2 * nobs);
   d.obs_e = A.alloc<float4>(nobs);
+  d.obs_p = A.alloc<float4>(2 * nobs);
   d.cam_off = A.upload(P.cam_off, s);
   d.cam_obs = A.upload(P.cam_obs, s);
   d.pt_h = A.alloc<float>(9 * npt);
