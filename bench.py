@@ -19,6 +19,12 @@ scaling); the reported time is the max over ranks.
 --impl reference times the CPU restatement of the reference solver (the FP64
 oracle, OpenMP over all host cores): one LM iteration of the same workload
 per step.
+
+Workload `windows-512`: 512 uneven local BA windows (5-40 stereo keyframes,
+baseline 0.11 m, 752x480 pinhole, 200-5,000 points, 3-12 observations per
+point, 10% of the poses fixed), ~9.3M observations, solved as one batch with
+the 10-iteration LM loop captured as a CUDA graph; one step = one batched
+solve.  `value` counts the LM iterations of all windows.
 """
 
 from __future__ import annotations
@@ -47,7 +53,7 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="ring-4m", choices=["ring-4m", "ring-50"])
+    ap.add_argument("--workload", default="ring-4m", choices=["ring-4m", "ring-50", "windows-512"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
@@ -65,6 +71,16 @@ def make_workload(name: str, rank: int):
                 "observations": int(problem.num_observations), "image": "6000x4000",
                 "lm_iterations": 30, "pcg_tolerance": 1e-6, "robust": "huber(1px)",
                 "track_length": "geometric mean 8, [2,60]"}
+    elif name == "windows-512":
+        problem = synth.window_batch(512, seed=4000 + 1000 * rank)
+        cfg = BaConfig(max_iterations=10, robust_kernel=RobustKernel.huber(1.0),
+                       max_pcg_iterations=200, pcg_relative_tolerance=1e-6, graph=True)
+        desc = {"workload": "windows-512", "windows": 512,
+                "keyframes": "U{5..40} stereo (baseline 0.11 m)", "image": "752x480",
+                "points": int(sum(p.num_landmarks for p in problem)),
+                "observations": int(sum(p.num_observations for p in problem)),
+                "lm_iterations": 10, "pcg_tolerance": 1e-6, "robust": "huber(1px)",
+                "fixed_poses": "10%", "cuda_graph": True}
     else:
         problem = synth.ring_problem(50, 5000, seed=1001 + rank)
         cfg = BaConfig(max_iterations=20, robust_kernel=RobustKernel.huber(1.0),
@@ -200,6 +216,21 @@ def cpu_sample(problem, cfg, threads=0):
     return dt
 
 
+def batch_cpu_sample(problems, cfg, windows=8):
+    """The oracle's full solve (all threads) of the first `windows` windows:
+    (LM iterations, seconds)."""
+    from oracle import oracle
+
+    one = type(cfg)(**{**cfg.__dict__, "graph": False})
+    iters, t0 = 0, time.perf_counter()
+    for p in problems[:windows]:
+        st, res = oracle.optimize(p.copy(), one, solver=oracle.SPARSE)
+        if st != 0:
+            raise RuntimeError(f"oracle failed: {st}")
+        iters += len(res.iterations)
+    return iters, time.perf_counter() - t0
+
+
 def run_reference(args, dist: Dist):
     if dist.rank != 0:
         return
@@ -208,6 +239,29 @@ def run_reference(args, dist: Dist):
 
     oracle.lib()
     cores = os.cpu_count() or 1
+    if args.workload == "windows-512":
+        times, iters = [], []
+        for k in range(args.warmup + args.steps):
+            n, dt = batch_cpu_sample(problem[8 * k:], cfg)
+            if k >= args.warmup:
+                times.append(dt)
+                iters.append(n)
+        value = sum(iters) / sum(times)
+        line = {
+            "impl": "reference", "metric": "lm_iterations_per_s", "value": value,
+            "unit": "LM iterations/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": desc,
+            "cpu_baseline": {"value": value, "unit": "LM iterations/s", "cores": cores,
+                             "kind": "port",
+                             "sample": "full LM solves of 8 windows of the batch per step "
+                                       "(FP64 Schur + Cholesky), all host cores"},
+            "e2e": {"value": value, "unit": "LM iterations/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line), flush=True)
+        return
     for _ in range(args.warmup):  # a cost pass per warm-up step (page-in, threads)
         oracle.cost(problem, cfg)
     times = [cpu_sample(problem, cfg) for _ in range(args.steps)]
@@ -354,12 +408,127 @@ def run_ours(args, dist: Dist):
     solver.close()
 
 
+def run_batch(args, dist: Dist):
+    """Batched windows: every window of the batch in one launch sequence."""
+    import torch
+
+    from visloc_ba.solver import CudaSolver
+
+    torch.cuda.set_device(dist.local)
+    problems, cfg, desc = make_workload(args.workload, dist.rank)
+    solver = CudaSolver(dist.local)
+    solver.batch_upload(problems, cfg)
+    for _ in range(args.warmup):
+        solver.batch_solve_uploaded()
+    clocks = Clocks(dist.local)
+    dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    wall0 = time.perf_counter()
+    runs = [solver.batch_solve_uploaded() for _ in range(args.steps)]
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - wall0
+    dist.barrier()
+    clk = clocks.stop()
+    dev_ms = sum(r[0].device_ms for r in runs)
+    lm_iters = sum(len(x.iterations) for r in runs for x in r)
+    obs_iters = sum(len(x.iterations) * p.num_observations for r in runs
+                    for x, p in zip(r, problems))
+    launches = sum(r[0].kernel_launches for r in runs)
+    t_max = dist.max(dev_ms / 1e3)
+    value = dist.sum(lm_iters) / t_max
+
+    # Phase times and the PCG roofline from one profiled (host-driven) solve
+    # outside the timed region.
+    from visloc_ba.solver import plan
+
+    prof_cfg = type(cfg)(**{**cfg.__dict__, "graph": False, "profile": True})
+    solver.batch_upload(problems, prof_cfg)
+    prof = solver.batch_solve_uploaded()
+    # Iteration records carry the phase times of the batch (same on every window).
+    its = max(prof, key=lambda x: len(x.iterations)).iterations
+    pcg_ms = sum(i.pcg_ms for i in its)
+    pcg_bytes = 0.0
+    for p, x in zip(problems, prof):
+        st, info = plan(p, cfg, 1.0)
+        pcg_bytes += info.bytes_per_pcg_iteration * sum(i.pcg_iterations for i in x.iterations)
+    peak, peak_kind = hbm_peak()
+    achieved = pcg_bytes / (pcg_ms / 1e3) / 1e9 if pcg_ms > 0 else 0.0
+
+    e2e = None
+    if not args.no_e2e:
+        copies = [[p.copy() for p in problems] for _ in range(min(args.steps, 2))]
+        e2e_cfg = type(cfg)(**{**cfg.__dict__})
+        dist.barrier()
+        t0 = time.perf_counter()
+        e2e_iters = 0
+        for batch in copies:
+            _, rs = solver.batch_optimize(batch, e2e_cfg)
+            e2e_iters += sum(len(x.iterations) for x in rs)
+        t_e2e = dist.max(time.perf_counter() - t0)
+        h2d = sum(p.num_poses * 57 + p.num_landmarks * 25 + p.num_observations * 20
+                  for p in problems)
+        e2e = {"value": dist.sum(e2e_iters) / t_e2e, "unit": "LM iterations/s",
+               "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(sum(p.num_poses * 56 + p.num_landmarks * 24
+                                             for p in problems)),
+               "ms_per_step": 1e3 * t_e2e / len(copies)}
+
+    # The plain per-problem GPU solve of the same windows (a sample of 32).
+    sample = problems[:32]
+    plain_cfg = type(cfg)(**{**cfg.__dict__, "graph": False})
+    t0 = time.perf_counter()
+    plain_iters = 0
+    for p in sample:
+        st, r = solver.optimize(p.copy(), plain_cfg)
+        plain_iters += len(r.iterations)
+    plain = plain_iters / (time.perf_counter() - t0)
+
+    cpu = None
+    if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
+        n, dt = batch_cpu_sample(problems, cfg)
+        cpu = {"value": n / dt, "unit": "LM iterations/s", "cores": os.cpu_count(),
+               "kind": "port",
+               "sample": f"full LM solves of 8 windows, {os.cpu_count()} threads, {dt:.1f} s"}
+
+    if dist.rank == 0:
+        line = {
+            "metric": "lm_iterations_per_s", "value": value, "unit": "LM iterations/s",
+            "n_gpus": dist.world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+            "config": {**desc, "parallelism": f"replicas x{dist.world}",
+                       "l2": "inputs larger than L2 (batch > 2 GB)"},
+            "observations_per_s": dist.sum(obs_iters) / t_max,
+            "windows_per_s": dist.sum(512 * args.steps) / t_max,
+            "lm_iterations_per_step": lm_iters / args.steps,
+            "plain_per_problem_lm_iterations_per_s": plain,
+            "roofline": {"kernel": PCG_KERNEL, "bound": "hbm", "achieved": achieved,
+                         "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_kind": peak_kind, "traffic": None,
+                         "traffic_unit": "bytes per PCG iteration"},
+            "phase_ms_per_lm_iteration": {
+                k: sum(getattr(i, f) for i in its) / max(1, len(its))
+                for k, f in [("linearize", "linearize_ms"), ("assemble", "assemble_ms"),
+                             ("pcg", "pcg_ms"), ("update_cost_decide", "update_ms")]},
+            "wall_s": wall,
+            "clocks": clk,
+            "gpu_launches": int(launches),
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    solver.close()
+
+
 def main():
     args = parse_args()
     dist = Dist()
     try:
         if args.impl == "reference":
             run_reference(args, dist)
+        elif args.workload == "windows-512":
+            run_batch(args, dist)
         else:
             run_ours(args, dist)
     finally:

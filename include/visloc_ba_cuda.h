@@ -151,6 +151,12 @@ typedef struct vlba_config {
  * solver.rs:571,622-628). */
 #define VLBA_FLAG_PROFILE 1u
 
+/* Run the initial cost and all max_iterations LM iterations as one CUDA graph,
+ * captured at the first solve of an upload and replayed by later solves:
+ * no host synchronisation between iterations (iterations after every problem
+ * has finished cost only their launches).  Ignored with VLBA_FLAG_PROFILE. */
+#define VLBA_FLAG_GRAPH 2u
+
 /* ------------------------------------------------------------------ result */
 /* BaIterationStats (bundle/mod.rs:755-763) plus solver diagnostics. */
 typedef struct vlba_iteration {
@@ -271,6 +277,32 @@ int visloc_ba_cuda_plan(const vlba_problem* problem, const vlba_config* config,
 int visloc_ba_cuda_cost(void* ctx, const vlba_problem* problem,
                         const vlba_config* config, double* cost,
                         uint64_t* nonprojectable);
+
+/* ----------------------------------------------------------------- batches */
+/* Many independent problems (local BA windows, pose-only refinements, whole
+ * models) packed into one device layout and solved together: every kernel
+ * launch covers all of them, each problem keeps its own LM state (lambda,
+ * accept/reject, convergence) and stops on its own, and every sum is taken
+ * per problem in a fixed order, so a problem's result is identical solved
+ * alone or in any batch.  The reference solves such windows one call at a
+ * time through BaAccelerator::optimize (ba_accel.rs:23-32); this is its
+ * batched form.
+ *
+ * statuses[i] (may be NULL) receives problem i's validation status; problems
+ * that fail validation are left out of the batch (the call still succeeds if
+ * any problem remains).  results has n entries and iterations n x
+ * iterations_capacity (row i for problem i); entries of problems left out are
+ * zeroed.  The configs' VLBA_FLAG_* bits are combined. */
+int visloc_ba_cuda_batch_optimize(void* ctx, uint32_t n, vlba_problem* const* problems,
+                                  const vlba_config* const* configs, int* statuses,
+                                  vlba_result* results, vlba_iteration* iterations,
+                                  uint32_t iterations_capacity);
+int visloc_ba_cuda_batch_upload(void* ctx, uint32_t n, const vlba_problem* const* problems,
+                                const vlba_config* const* configs, int* statuses);
+int visloc_ba_cuda_batch_solve_uploaded(void* ctx, vlba_result* results,
+                                        vlba_iteration* iterations,
+                                        uint32_t iterations_capacity);
+int visloc_ba_cuda_batch_download(void* ctx, uint32_t n, vlba_problem* const* problems);
 
 /* ------------------------------------------------------------- diagnostics */
 /* One damped linear step at the given state, without updating it: the step

@@ -875,13 +875,17 @@ struct Pcg {
   static constexpr int kTB = 8;              // tile edge in 6x6 blocks
   static constexpr int kWarps = 8;           // one block per SM (shared memory)
   static constexpr int kThreads = 32 * kWarps;
-  static constexpr int kStages = 3;          // per-warp TMA ring
+  static constexpr int kStages = 2;          // per-warp TMA ring
   static constexpr int kTileFloats = kTB * kTB * kBlock;
   static constexpr uint32_t kTileBytes = kTileFloats * 4u;
   static constexpr int kRow = kTB * 6;       // floats of a tile-row vector segment
   static constexpr size_t kWarpBytes = (size_t)kStages * kTileBytes + 2 * kRow * 4;
+  // Owned tile rows per block and their state in shared memory: p, z, q, x,
+  // r (kRow floats each) and the kRow x 6 rows of M^-1, kept for the launch.
+  static constexpr int kOwnMax = 32;
+  static constexpr int kOwnFloats = 5 * kRow + 6 * kRow;
   static constexpr size_t kSmem = kWarps * kWarpBytes + (size_t)kWarps * kRow * 4 +
-                                  (size_t)kThreads * 8 + 64;
+                                  (size_t)kThreads * 8 + (size_t)kOwnMax * kOwnFloats * 4 + 64;
 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
@@ -1126,7 +1130,6 @@ __device__ __forceinline__ double block_sum_fast(double v, double* red) {
 __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
   using C = Pcg;
   constexpr int NW = C::kWarps;
-  constexpr uint32_t TBC = C::kTB;
   extern __shared__ __align__(128) unsigned char smem[];
   const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
   // Per-warp region: kStages tile buffers, then the warp's p segments.
@@ -1136,6 +1139,7 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
   float* const wPJ = wPI + C::kRow;
   float* const colw = reinterpret_cast<float*>(smem + (size_t)NW * C::kWarpBytes);  // [NW kRow]
   double* const red = reinterpret_cast<double*>(colw + NW * C::kRow);             // [N]
+  float* const own = reinterpret_cast<float*>(red + C::kThreads);  // [kOwnMax][kOwnFloats]
   __shared__ uint64_t mbar[NW][C::kStages];
   __shared__ ProbScal sc;
   __shared__ uint32_t sc_prob;
@@ -1189,10 +1193,13 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
     __syncthreads();
   };
 
-  // Rows this block owns (row R belongs to block R mod G), kOwn at most
-  // (a larger grid than rows x kOwn is never launched): list bounds and
-  // problem, constant for the launch.
-  constexpr int kOwn = 4;
+  // Rows this block owns (row R belongs to block R mod G), kOwnMax at most
+  // (the host never launches a grid with rows > G kOwnMax): list bounds and
+  // problem, constant for the launch.  The owner alone writes its rows' p, z,
+  // x and r, so their shared-memory copies stay current for the whole solve.
+  constexpr int kOwn = C::kOwnMax;
+  constexpr int kOP = 0, kOZ = C::kRow, kOQ = 2 * C::kRow, kOX = 3 * C::kRow, kOR = 4 * C::kRow,
+                kOM = 5 * C::kRow;
   __shared__ uint32_t own_m0[kOwn], own_m1[kOwn], own_prob[kOwn];
   const uint32_t nown = blockIdx.x < d.num_tile_rows
                             ? min((uint32_t)kOwn, (d.num_tile_rows - 1 - blockIdx.x) / G + 1)
@@ -1203,11 +1210,8 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
     own_m1[tid] = d.tr_list_off[R + 1];
     own_prob[tid] = d.tr_prob[R];
   }
+  auto ownrow = [&](uint32_t j) -> float* { return own + (size_t)j * C::kOwnFloats; };
   unsigned int bar_gen = *(volatile unsigned int*)(d.barrier + 1);
-  // Per owned row, threads [0, kRow): p, z (prefetched before the tiles), then
-  // q and the new p (reduction), x, r and the M^-1 row (prefetched for C).
-  float own_p[kOwn] = {}, own_z[kOwn] = {}, own_q[kOwn] = {}, own_x[kOwn] = {}, own_r[kOwn] = {};
-  float own_m[kOwn][6] = {};
 
   // Fixed-order reduction of tile row R: warp w sums slots m0 + w + j NW
   // (contiguous kRow floats, coalesced, kBatch in flight), in slot order;
@@ -1247,19 +1251,14 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
       float q = 0.0f;
 #pragma unroll
       for (int w2 = 0; w2 < NW; ++w2) q += colw[w2 * C::kRow + tid];
-      float pv = own_p[j];
-      if (k > 0) pv = __fmaf_rn((float)beta, pv, own_z[j]);
-      own_p[j] = pv;
-      own_q[j] = q;
+      float* o = ownrow((uint32_t)j);
+      float pv = o[kOP + tid];
+      if (k > 0) pv = __fmaf_rn((float)beta, pv, o[kOZ + tid]);
+      o[kOP + tid] = pv;
+      o[kOQ + tid] = q;
       d.p[at] = pv;
       d.q[at] = q;
       pq = (double)pv * (double)q;
-      // Operands of this row's update in C, fetched now.
-      own_x[j] = __ldcg(d.x + at);
-      own_r[j] = __ldcg(d.r + at);
-      const float* mm = d.minv + 36 * (size_t)(R * TBC + tid / 6) + (tid % 6) * 6;
-#pragma unroll
-      for (int b2 = 0; b2 < 6; ++b2) own_m[j][b2] = mm[b2];
     }
     pq = block_sum_fast<NW>(pq, red);
     if (tid == 0) {
@@ -1270,14 +1269,18 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
 
   // ---- init: x = 0, r = b, z = M^-1 r, p = z; dots rz, b2 of "iteration -1".
   float* const sPI = colw;  // block scratch of kRow floats for init / C
-  for (uint32_t tr = blockIdx.x; tr < d.num_tile_rows; tr += G) {
+  for (uint32_t j = 0; j < nown; ++j) {
+    const uint32_t tr = blockIdx.x + j * G;
     const uint32_t P = d.tr_prob[tr];
     if (!*(volatile uint32_t*)&d.pcg[P].active) continue;
     const size_t base = (size_t)tr * C::kRow;
+    float* o = ownrow(j);
     if (tid < (uint32_t)C::kRow) {
       const float b = d.rhs[base + tid];
       d.x[base + tid] = 0.0f;
       d.r[base + tid] = b;
+      o[kOX + tid] = 0.0f;
+      o[kOR + tid] = b;
       sPI[tid] = b;
     }
     __syncthreads();
@@ -1287,9 +1290,15 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
       const float* m = d.minv + 36 * (base / 6 + cam) + a * 6;
       float z = 0.0f;
 #pragma unroll
-      for (int b = 0; b < 6; ++b) z += m[b] * sPI[cam * 6 + b];
+      for (int b = 0; b < 6; ++b) {
+        const float mb = m[b];
+        o[kOM + tid * 6 + b] = mb;
+        z += mb * sPI[cam * 6 + b];
+      }
       d.z[base + tid] = z;
       d.p[base + tid] = z;
+      o[kOZ + tid] = z;
+      o[kOP + tid] = z;
       rz = (double)sPI[tid] * (double)z;
       bb = (double)sPI[tid] * (double)sPI[tid];
     }
@@ -1331,13 +1340,6 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
         atomicSub(d.barrier + 2, 1u);
       }
     }
-    // The owned rows' p and z (read again only by their owner this iteration).
-    if (tid < (uint32_t)C::kRow)
-      for (uint32_t j = 0; j < nown; ++j) {
-        const size_t at = (size_t)(blockIdx.x + j * G) * C::kRow + tid;
-        own_p[j] = __ldcg(d.p + at);
-        own_z[j] = __ldcg(d.z + at);
-      }
     // The block computes the scalars of its first tile's problem once; warps
     // whose tile is of that problem read them from shared memory.
     if (NW > 0) {
@@ -1555,9 +1557,13 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
       if (alpha == 0.0) continue;  // breakdown: x frozen, flagged at A(k+1)
       const size_t base = (size_t)tr * C::kRow;
       const float af = (float)alpha;
+      float* o = ownrow(j);
       if (tid < (uint32_t)C::kRow) {
-        d.x[base + tid] = own_x[j] + af * own_p[j];
-        const float rv = own_r[j] - af * own_q[j];
+        const float xv = o[kOX + tid] + af * o[kOP + tid];
+        o[kOX + tid] = xv;
+        d.x[base + tid] = xv;
+        const float rv = o[kOR + tid] - af * o[kOQ + tid];
+        o[kOR + tid] = rv;
         d.r[base + tid] = rv;
         sPI[tid] = rv;
       }
@@ -1567,7 +1573,8 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
         const uint32_t cam = tid / 6;
         float z = 0.0f;
 #pragma unroll
-        for (int b = 0; b < 6; ++b) z += own_m[j][b] * sPI[cam * 6 + b];
+        for (int b = 0; b < 6; ++b) z += o[kOM + tid * 6 + b] * sPI[cam * 6 + b];
+        o[kOZ + tid] = z;
         d.z[base + tid] = z;
         rz = (double)sPI[tid] * (double)z;
         rr = (double)sPI[tid] * (double)sPI[tid];
@@ -1599,6 +1606,23 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
     const char* base = reinterpret_cast<const char*>(d.tiles + (size_t)t * C::kTileFloats);
     for (uint32_t off = lane * 128u; off < C::kTileBytes; off += 32u * 128u)
       asm volatile("applypriority.global.L2::evict_normal [%0], 128;" ::"l"(base + off) : "memory");
+  }
+}
+
+// Current state (buffer Ctrl::cur) of every problem into buffer 0.
+__global__ void __launch_bounds__(256) k_state_to_front(Dev d) {
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < d.num_poses; p += stride) {
+    if (d.ctrl[d.pose_prob[p]].cur == 0u) continue;
+#pragma unroll
+    for (int a = 0; a < 4; ++a) d.pose_q[0][4 * (size_t)p + a] = d.pose_q[1][4 * (size_t)p + a];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) d.pose_t[0][3 * (size_t)p + a] = d.pose_t[1][3 * (size_t)p + a];
+  }
+  for (uint32_t l = blockIdx.x * blockDim.x + threadIdx.x; l < d.num_points; l += stride) {
+    if (d.ctrl[d.point_prob[l]].cur == 0u) continue;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) d.points[0][3 * (size_t)l + a] = d.points[1][3 * (size_t)l + a];
   }
 }
 
@@ -1699,6 +1723,13 @@ cudaError_t launch_pcg_setup(const Dev& d, cudaStream_t s) {
 }
 
 size_t pcg_smem_bytes(int) { return Pcg::kSmem; }
+int pcg_rows_per_block() { return Pcg::kOwnMax; }
+
+cudaError_t launch_state_to_front(const Dev& d, cudaStream_t s) {
+  const size_t n = std::max<size_t>(d.num_poses, d.num_points);
+  k_state_to_front<<<grid1d(n, 256), 256, 0, s>>>(d);
+  return cudaGetLastError();
+}
 
 int pcg_grid_size(int, int sm_count) {
   int per_sm = 0;

@@ -19,9 +19,13 @@ cudaError_t launch_cam_diag(const Dev& d, cudaStream_t s);
 cudaError_t launch_pcg(const Dev& d, int sm_count, cudaStream_t s);
 cudaError_t launch_pose_update(const Dev& d, cudaStream_t s);
 cudaError_t launch_pcg_setup(const Dev& d, cudaStream_t s);
+// Copy each problem's current state into state buffer 0 (for a bulk download).
+cudaError_t launch_state_to_front(const Dev& d, cudaStream_t s);
 
 // Occupancy-derived grid of the persistent PCG kernel (0 if it cannot run).
 int pcg_grid_size(int tb, int sm_count);
 size_t pcg_smem_bytes(int tb);
+// Tile rows one PCG block can own (a launch covers grid x this many rows).
+int pcg_rows_per_block();
 
 }  // namespace vlba

@@ -419,12 +419,10 @@ void build_plan(const vlba_problem* const* problems, const vlba_config* const* c
     P.tile_meta[4 * t + 3] = P.tr_prob[P.tile_ij[t] >> 16];
   }
   P.num_pairs = P.pairs.size();
-  // Lanes per block in the off-diagonal assembly: about three points per
-  // lane (the mean pair count per block sets the shape).
-  const double mean = P.camera_pairs ? (double)P.num_pairs / (double)P.camera_pairs : 1.0;
-  uint32_t g = 1;
-  while (g < 32 && (double)(2 * g) * 3.0 <= mean + 1e-9) g *= 2;
-  P.group = g;
+  // Lanes per block in the off-diagonal assembly.  The lane count sets the
+  // order of each block's sum, so it is the same for every problem and batch
+  // (a result must not depend on what it is batched with).
+  P.group = 8;
 }
 
 std::string check_plan(const Plan& P) {

@@ -92,18 +92,30 @@ struct Context {
   size_t l2_bytes = 0;
   double l2_fraction = 0.5;  // share of the L2 that keeps S resident in PCG
   int pcg_grid_hint = 0;     // blocks of the PCG launch (trace sizing)
-  // the uploaded problem's sizes (for download)
+  // the uploaded problems' sizes (for download)
   std::vector<uint64_t> num_poses, num_points;
+  // batch upload: input index -> problem of the plan (-1: failed validation)
+  std::vector<int> batch_slot;
+  // the LM loop of the current upload captured as one graph (VLBA_FLAG_GRAPH)
+  cudaGraphExec_t graph = nullptr;
+  uint32_t graph_iters = 0;
 };
 
 namespace {
 
 void set_device(Context* c) { VLBA_CUDA(cudaSetDevice(c->device)); }
 
+void drop_graph(Context* c) {
+  if (c->graph) cudaGraphExecDestroy(c->graph);
+  c->graph = nullptr;
+  c->graph_iters = 0;
+}
+
 // Upload a built plan: allocate and fill every device array of Dev.
 void upload_plan(Context* c, uint32_t max_records) {
   Plan& P = c->plan;
   cudaStream_t s = c->stream;
+  drop_graph(c);  // its kernels hold the old device pointers
   c->arena.release();
   c->uploaded = false;
   Dev d;
@@ -218,9 +230,10 @@ void upload_plan(Context* c, uint32_t max_records) {
   c->pcg_grid = P.num_tile_rows ? pcg_grid_size((int)P.tb, c->sm_count) : 0;
   c->pcg_grid = std::min<int>(c->pcg_grid,
                               (int)std::max<size_t>(P.tile_ij.size(), P.num_tile_rows));
-  if (c->pcg_grid > 0 && (size_t)c->pcg_grid * 4 < P.num_tile_rows)
+  if (c->pcg_grid > 0 && (size_t)c->pcg_grid * pcg_rows_per_block() < P.num_tile_rows)
     throw Status(VLBA_ERR_INVALID_ARGUMENT,
-                 "reduced system too large: more than 4 tile rows per PCG block");
+                 "reduced system too large: more than " + std::to_string(pcg_rows_per_block()) +
+                     " tile rows per PCG block");
   if (d.trace && c->pcg_grid > c->pcg_grid_hint) d.trace = nullptr;  // sized for fewer blocks
   if (P.num_tile_rows && c->pcg_grid <= 0)
     throw Status(VLBA_ERR_CUDA, "the PCG kernel cannot be made co-resident on this device");
@@ -305,38 +318,109 @@ void dump_trace(Context* c) {
 }
 
 // The device LM loop over all uploaded problems.
+// The kernels of one LM iteration (trial), in order; `ev` (4 events or null)
+// brackets the phases for profiling.  Returns the number of launches.
+uint64_t enqueue_iteration(Context* c, cudaEvent_t* ev) {
+  Dev& d = c->dev;
+  cudaStream_t s = c->stream;
+  if (ev) VLBA_CUDA(cudaEventRecord(ev[0], s));
+  check_launch(launch_linearize(d, s), "linearize");
+  if (ev) VLBA_CUDA(cudaEventRecord(ev[1], s));
+  check_launch(launch_point_prep(d, s), "point prep");
+  check_launch(launch_offdiag(d, s), "off-diagonal blocks");
+  check_launch(launch_cam_diag(d, s), "camera blocks");
+  check_launch(launch_pcg_setup(d, s), "pcg setup");
+  if (ev) VLBA_CUDA(cudaEventRecord(ev[2], s));
+  check_launch(launch_pcg(d, c->pcg_grid, s), "pcg");
+  if (d.trace) dump_trace(c);
+  if (ev) VLBA_CUDA(cudaEventRecord(ev[3], s));
+  check_launch(launch_pose_update(d, s), "pose update");
+  check_launch(launch_cost(d, true, s), "trial cost");
+  check_launch(launch_decide(d, false, s), "decide");
+  if (ev) VLBA_CUDA(cudaEventRecord(ev[4], s));
+  // linearize, point prep, pcg setup, pose update, cost, decide always;
+  // off-diagonal, camera-diagonal and PCG kernels when the system has them.
+  return 6 + (d.num_offdiag_blocks ? 1 : 0) + (d.num_var_cams ? 1 : 0) + (d.num_tile_rows ? 1 : 0);
+}
+
+uint64_t enqueue_initial(Context* c) {
+  Dev& d = c->dev;
+  cudaStream_t s = c->stream;
+  check_launch(launch_pose_table(d, s), "pose table");
+  check_launch(launch_cost(d, false, s), "initial cost");
+  check_launch(launch_decide(d, true, s), "init");
+  return 3;
+}
+
+void check_device_error(Context* c) {
+  unsigned int err = 0;
+  VLBA_CUDA(cudaMemcpyAsync(&err, c->dev.error, 4, cudaMemcpyDeviceToHost, c->stream));
+  VLBA_CUDA(cudaStreamSynchronize(c->stream));
+  if (err)
+    throw Status(VLBA_ERR_TIMEOUT,
+                 "a bounded device wait gave up (error bits " + std::to_string(err) + ")");
+}
+
+// The LM loop with VLBA_FLAG_GRAPH: the initial cost and max_iters
+// iterations captured once per upload as one CUDA graph and replayed; no
+// host synchronisation between iterations (the kernels of a problem that has
+// finished return at once).
+RunStats run_lm_graph(Context* c, uint32_t max_iters) {
+  cudaStream_t s = c->stream;
+  RunStats st;
+  uint64_t launches = 0;
+  if (!c->graph || c->graph_iters != max_iters) {
+    drop_graph(c);
+    cudaGraph_t g = nullptr;
+    VLBA_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    try {
+      launches += enqueue_initial(c);
+      for (uint32_t it = 0; it < max_iters; ++it) launches += enqueue_iteration(c, nullptr);
+    } catch (...) {
+      cudaStreamEndCapture(s, &g);
+      if (g) cudaGraphDestroy(g);
+      cudaGetLastError();
+      throw;
+    }
+    VLBA_CUDA(cudaStreamEndCapture(s, &g));
+    const cudaError_t e = cudaGraphInstantiate(&c->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+      c->graph = nullptr;
+      throw CudaError(e, "cudaGraphInstantiate");
+    }
+    c->graph_iters = max_iters;
+  } else {
+    launches = 3;
+    for (uint32_t it = 0; it < max_iters; ++it) {
+      const Dev& d = c->dev;
+      launches += 6 + (d.num_offdiag_blocks ? 1 : 0) + (d.num_var_cams ? 1 : 0) +
+                  (d.num_tile_rows ? 1 : 0);
+    }
+  }
+  VLBA_CUDA(cudaEventRecord(c->ev[0], s));
+  VLBA_CUDA(cudaGraphLaunch(c->graph, s));
+  VLBA_CUDA(cudaEventRecord(c->ev[5], s));
+  check_device_error(c);
+  float ms = 0.f;
+  VLBA_CUDA(cudaEventElapsedTime(&ms, c->ev[0], c->ev[5]));
+  st.device_ms = ms;
+  st.launches = launches;
+  return st;
+}
+
 RunStats run_lm(Context* c, bool profile, PhaseTimes* pt) {
   Dev& d = c->dev;
   cudaStream_t s = c->stream;
   uint32_t max_iters = 0;
   for (const LmParams& lp : c->plan.params) max_iters = std::max(max_iters, lp.max_iterations);
+  if ((c->flags & VLBA_FLAG_GRAPH) && !profile && !d.trace) return run_lm_graph(c, max_iters);
   RunStats st;
   std::vector<Ctrl> ctrl(c->plan.num_problems);
   VLBA_CUDA(cudaEventRecord(c->ev[0], s));
-  check_launch(launch_pose_table(d, s), "pose table");
-  check_launch(launch_cost(d, false, s), "initial cost");
-  check_launch(launch_decide(d, true, s), "init");
-  st.launches += 3;
+  st.launches += enqueue_initial(c);
   for (uint32_t it = 0; it < max_iters; ++it) {
-    if (profile) VLBA_CUDA(cudaEventRecord(c->ev[1], s));
-    check_launch(launch_linearize(d, s), "linearize");
-    if (profile) VLBA_CUDA(cudaEventRecord(c->ev[2], s));
-    check_launch(launch_point_prep(d, s), "point prep");
-    check_launch(launch_offdiag(d, s), "off-diagonal blocks");
-    check_launch(launch_cam_diag(d, s), "camera blocks");
-    check_launch(launch_pcg_setup(d, s), "pcg setup");
-    if (profile) VLBA_CUDA(cudaEventRecord(c->ev[3], s));
-    check_launch(launch_pcg(d, c->pcg_grid, s), "pcg");
-    if (d.trace) dump_trace(c);
-    if (profile) VLBA_CUDA(cudaEventRecord(c->ev[4], s));
-    check_launch(launch_pose_update(d, s), "pose update");
-    check_launch(launch_cost(d, true, s), "trial cost");
-    check_launch(launch_decide(d, false, s), "decide");
-    if (profile) VLBA_CUDA(cudaEventRecord(c->ev[5], s));
-    // linearize, point prep, pcg setup, pose update, cost, decide always;
-    // off-diagonal, camera-diagonal and PCG kernels when the system has them.
-    st.launches += 6 + (d.num_offdiag_blocks ? 1 : 0) + (d.num_var_cams ? 1 : 0) +
-                   (d.num_tile_rows ? 1 : 0);
+    st.launches += enqueue_iteration(c, profile ? c->ev + 1 : nullptr);
     // Poll the per-problem control words (one small copy per iteration).
     VLBA_CUDA(cudaMemcpyAsync(ctrl.data(), d.ctrl, sizeof(Ctrl) * ctrl.size(), cudaMemcpyDeviceToHost, s));
     unsigned int err = 0;
@@ -407,18 +491,55 @@ void download_problem(Context* c, uint32_t prob, vlba_problem* p) {
   VLBA_CUDA(cudaMemcpy(p->landmarks, c->dev.points[b] + 3 * (size_t)pt0, nl * 24, cudaMemcpyDeviceToHost));
 }
 
-int pick_tb(const vlba_problem* const* probs, uint32_t n) {
-  // Tile size: 16 blocks for cameras counts that fill 16-wide tile rows,
-  // 8 for small windows (less zero fill in their dense tiles).
-  uint64_t vars = 0;
-  for (uint32_t i = 0; i < n; ++i) {
-    const vlba_problem* p = probs[i];
-    uint64_t v = 0;
-    for (uint64_t k = 0; k < p->num_poses; ++k) v += !(p->pose_fixed && p->pose_fixed[k]);
-    vars += v;
+// Results of every problem of the plan with two bulk copies; `slot[i]` maps
+// output i to a problem of the plan (-1: zeroed entry).
+void fill_results_bulk(Context* c, const std::vector<int>& slot, vlba_result* res,
+                       vlba_iteration* its, uint32_t cap, const RunStats& st,
+                       const PhaseTimes* pt) {
+  const Dev& d = c->dev;
+  const uint32_t np = c->plan.num_problems;
+  std::vector<Ctrl> ctrl(np);
+  VLBA_CUDA(cudaMemcpy(ctrl.data(), d.ctrl, sizeof(Ctrl) * np, cudaMemcpyDeviceToHost));
+  std::vector<vlba_iteration> rec;
+  if (its && cap) {
+    rec.resize((size_t)np * d.max_records);
+    VLBA_CUDA(cudaMemcpy(rec.data(), d.records, rec.size() * sizeof(vlba_iteration),
+                         cudaMemcpyDeviceToHost));
   }
-  const double mean = n ? (double)vars / n : 0.0;
-  (void)mean;
+  for (size_t i = 0; i < slot.size(); ++i) {
+    if (res) std::memset(res + i, 0, sizeof *res);
+    if (its && cap) std::memset(its + i * cap, 0, sizeof(vlba_iteration) * cap);
+    if (slot[i] < 0) continue;
+    const Ctrl& x = ctrl[slot[i]];
+    if (res) {
+      res[i].initial_cost = x.initial_cost;
+      res[i].final_cost = x.current_cost;
+      res[i].converged = x.converged;
+      res[i].num_iterations = x.iteration;
+      res[i].initial_nonprojectable = x.initial_nonproj;
+      res[i].final_nonprojectable = x.current_nonproj;
+      res[i].total_pcg_iterations = x.total_pcg;
+      res[i].device_ms = st.device_ms;
+      res[i].kernel_launches = st.launches;
+    }
+    const uint32_t m = std::min(std::min(x.iteration, cap), d.max_records);
+    if (its && m) {
+      std::memcpy(its + i * cap, rec.data() + (size_t)slot[i] * d.max_records,
+                  m * sizeof(vlba_iteration));
+      // Iteration k of every problem ran in the batch's iteration k.
+      if (pt)
+        for (uint32_t k = 0; k < m && k < pt->lin.size(); ++k) {
+          vlba_iteration& r = its[i * cap + k];
+          r.linearize_ms = pt->lin[k];
+          r.assemble_ms = pt->assemble[k];
+          r.pcg_ms = pt->pcg[k];
+          r.update_ms = pt->update[k];
+        }
+    }
+  }
+}
+
+int pick_tb(const vlba_problem* const*, uint32_t) {
   return 8;  // the PCG streams 8 x 8-block tiles, one warp per tile
 }
 
@@ -446,6 +567,7 @@ int guarded(Context* c, F&& f) {
 void do_upload(Context* c, const vlba_problem* const* probs, const vlba_config* const* cfgs,
                uint32_t n, uint32_t max_records, double* upload_ms) {
   const auto t0 = std::chrono::steady_clock::now();
+  c->batch_slot.clear();
   for (uint32_t i = 0; i < n; ++i) {
     const Validation v = validate_problem(probs[i], cfgs[i]);
     if (v.status != VLBA_OK)
@@ -525,6 +647,7 @@ void visloc_ba_cuda_destroy(void* ctx) {
   auto* c = static_cast<Context*>(ctx);
   if (!c) return;
   cudaSetDevice(c->device);
+  vlba::drop_graph(c);
   c->arena.release();
   for (auto& e : c->ev)
     if (e) cudaEventDestroy(e);
@@ -619,6 +742,95 @@ int visloc_ba_cuda_optimize(void* ctx, vlba_problem* problem, const vlba_config*
   if (st != VLBA_OK) return st;
   if (result) result->upload_ms = upload_ms;
   return visloc_ba_cuda_download(ctx, problem);
+}
+
+int visloc_ba_cuda_batch_upload(void* ctx, uint32_t n, const vlba_problem* const* problems,
+                                const vlba_config* const* configs, int* statuses) {
+  auto* c = static_cast<Context*>(ctx);
+  if (!c || (n && (!problems || !configs))) return VLBA_ERR_INVALID_ARGUMENT;
+  return vlba::guarded(c, [&] {
+    std::vector<const vlba_problem*> ps;
+    std::vector<const vlba_config*> cs;
+    std::vector<int> slot(n, -1);
+    uint32_t max_rec = 0, flags = 0;
+    int first_bad = VLBA_ERR_INVALID_ARGUMENT;
+    for (uint32_t i = 0; i < n; ++i) {
+      const vlba::Validation v = vlba::validate_problem(problems[i], configs[i]);
+      if (statuses) statuses[i] = v.status;
+      if (v.status != VLBA_OK) {
+        if (ps.empty() && first_bad == VLBA_ERR_INVALID_ARGUMENT) first_bad = v.status;
+        continue;
+      }
+      slot[i] = (int)ps.size();
+      ps.push_back(problems[i]);
+      cs.push_back(configs[i]);
+      max_rec = std::max(max_rec, configs[i]->max_iterations);
+      flags |= configs[i]->flags;
+    }
+    if (ps.empty()) throw vlba::Status(first_bad, "no problem of the batch passed validation");
+    vlba::do_upload(c, ps.data(), cs.data(), (uint32_t)ps.size(), max_rec, nullptr);
+    c->flags = flags;
+    c->batch_slot = std::move(slot);
+  });
+}
+
+int visloc_ba_cuda_batch_solve_uploaded(void* ctx, vlba_result* results,
+                                        vlba_iteration* iterations,
+                                        uint32_t iterations_capacity) {
+  auto* c = static_cast<Context*>(ctx);
+  if (!c) return VLBA_ERR_INVALID_ARGUMENT;
+  return vlba::guarded(c, [&] {
+    if (!c->uploaded || c->batch_slot.empty())
+      throw vlba::Status(VLBA_ERR_INVALID_ARGUMENT, "no batch uploaded");
+    vlba::set_device(c);
+    vlba::reset_state(c);
+    const bool profile = c->flags & VLBA_FLAG_PROFILE;
+    vlba::PhaseTimes pt;
+    const vlba::RunStats st = vlba::run_lm(c, profile, &pt);
+    vlba::fill_results_bulk(c, c->batch_slot, results, iterations, iterations_capacity, st,
+                            profile ? &pt : nullptr);
+  });
+}
+
+int visloc_ba_cuda_batch_download(void* ctx, uint32_t n, vlba_problem* const* problems) {
+  auto* c = static_cast<Context*>(ctx);
+  if (!c || (n && !problems)) return VLBA_ERR_INVALID_ARGUMENT;
+  return vlba::guarded(c, [&] {
+    if (!c->uploaded || c->batch_slot.size() != n)
+      throw vlba::Status(VLBA_ERR_INVALID_ARGUMENT, "download: not the uploaded batch");
+    vlba::set_device(c);
+    const vlba::Dev& d = c->dev;
+    const vlba::Plan& P = c->plan;
+    vlba::check_launch(vlba::launch_state_to_front(d, c->stream), "state gather");
+    std::vector<double> q(P.pose_q.size()), t(P.pose_t.size()), x(P.points.size());
+    VLBA_CUDA(cudaMemcpyAsync(q.data(), d.pose_q[0], q.size() * 8, cudaMemcpyDeviceToHost, c->stream));
+    VLBA_CUDA(cudaMemcpyAsync(t.data(), d.pose_t[0], t.size() * 8, cudaMemcpyDeviceToHost, c->stream));
+    VLBA_CUDA(cudaMemcpyAsync(x.data(), d.points[0], x.size() * 8, cudaMemcpyDeviceToHost, c->stream));
+    VLBA_CUDA(cudaStreamSynchronize(c->stream));
+    for (uint32_t i = 0; i < n; ++i) {
+      const int k = c->batch_slot[i];
+      if (k < 0 || !problems[i]) continue;
+      vlba_problem* p = problems[i];
+      const uint32_t pose0 = P.prob_pose_begin[k], pt0 = P.prob_point_begin[k];
+      const size_t np = P.prob_pose_begin[k + 1] - pose0, nl = P.prob_point_begin[k + 1] - pt0;
+      if (np != p->num_poses || nl != p->num_landmarks)
+        throw vlba::Status(VLBA_ERR_INVALID_ARGUMENT, "download: problem sizes differ from the upload");
+      std::memcpy(p->pose_q, q.data() + 4 * (size_t)pose0, np * 32);
+      std::memcpy(p->pose_t, t.data() + 3 * (size_t)pose0, np * 24);
+      std::memcpy(p->landmarks, x.data() + 3 * (size_t)pt0, nl * 24);
+    }
+  });
+}
+
+int visloc_ba_cuda_batch_optimize(void* ctx, uint32_t n, vlba_problem* const* problems,
+                                  const vlba_config* const* configs, int* statuses,
+                                  vlba_result* results, vlba_iteration* iterations,
+                                  uint32_t iterations_capacity) {
+  int st = visloc_ba_cuda_batch_upload(ctx, n, problems, configs, statuses);
+  if (st != VLBA_OK) return st;
+  st = visloc_ba_cuda_batch_solve_uploaded(ctx, results, iterations, iterations_capacity);
+  if (st != VLBA_OK) return st;
+  return visloc_ba_cuda_batch_download(ctx, n, problems);
 }
 
 int visloc_ba_cuda_plan(const vlba_problem* problem, const vlba_config* config,

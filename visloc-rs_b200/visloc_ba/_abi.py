@@ -61,6 +61,7 @@ KERNEL_HUBER = 1
 KERNEL_CAUCHY = 2
 
 FLAG_PROFILE = 1
+FLAG_GRAPH = 2
 
 
 class Camera(C.Structure):
@@ -199,6 +200,18 @@ SOLVER_EXPORTS = {
         C.c_int,
         [C.c_void_p, P(Problem), P(Config), P(C.c_double), P(C.c_uint64)],
     ),
+    "visloc_ba_cuda_batch_optimize": (
+        C.c_int,
+        [C.c_void_p, C.c_uint32, P(P(Problem)), P(P(Config)), P(C.c_int), P(Result),
+         P(Iteration), C.c_uint32],
+    ),
+    "visloc_ba_cuda_batch_upload": (
+        C.c_int, [C.c_void_p, C.c_uint32, P(P(Problem)), P(P(Config)), P(C.c_int)],
+    ),
+    "visloc_ba_cuda_batch_solve_uploaded": (
+        C.c_int, [C.c_void_p, P(Result), P(Iteration), C.c_uint32],
+    ),
+    "visloc_ba_cuda_batch_download": (C.c_int, [C.c_void_p, C.c_uint32, P(P(Problem))]),
     # Device pointers for the problem arrays and both outputs; see the header.
     "visloc_ba_cuda_cost_noalloc": (
         C.c_int,

@@ -240,6 +240,8 @@ class BaConfig:
     max_pcg_iterations: int = 100
     pcg_relative_tolerance: float = 1e-4
     profile: bool = False
+    # Run the LM loop as one captured CUDA graph (VLBA_FLAG_GRAPH).
+    graph: bool = False
 
     def to_abi(self) -> _abi.Config:
         c = _abi.Config()
@@ -260,7 +262,7 @@ class BaConfig:
         c.robust_parameter = float(self.robust_kernel.parameter)
         c.max_pcg_iterations = int(self.max_pcg_iterations)
         c.pcg_relative_tolerance = float(self.pcg_relative_tolerance)
-        c.flags = _abi.FLAG_PROFILE if self.profile else 0
+        c.flags = (_abi.FLAG_PROFILE if self.profile else 0) | (_abi.FLAG_GRAPH if self.graph else 0)
         return c
 
 

@@ -108,6 +108,72 @@ class CudaSolver:
     def download(self, packed: PackedProblem) -> int:
         return self.lib.visloc_ba_cuda_download(self.ctx, C.byref(packed.abi()))
 
+    # ------------------------------------------------------------ batches
+    def _batch_arrays(self, problems, configs):
+        n = len(problems)
+        if isinstance(configs, BaConfig):
+            configs = [configs] * n
+        probs = [p.abi() for p in problems]
+        cfgs = [c.to_abi() for c in configs]
+        pp = (C.POINTER(_abi.Problem) * n)(*[C.pointer(x) for x in probs])
+        cp = (C.POINTER(_abi.Config) * n)(*[C.pointer(x) for x in cfgs])
+        cap = max(1, max(int(c.max_iterations) for c in configs)) if n else 1
+        self._batch_keep = (probs, cfgs, pp, cp)
+        self._batch_n, self._batch_cap = n, cap
+        return n, pp, cp, cap
+
+    def _batch_results(self, res, iters, statuses, n, cap):
+        out = []
+        for i in range(n):
+            if statuses is not None and statuses[i] != _abi.OK:
+                out.append(None)
+                continue
+            row = (_abi.Iteration * cap).from_buffer(iters, i * cap * C.sizeof(_abi.Iteration))
+            out.append(result_from_abi(res[i], row, res[i].num_iterations))
+        return out
+
+    def batch_upload(self, problems, configs):
+        """Upload a batch (configs: one BaConfig or one per problem).  Returns
+        the per-problem validation statuses; raises SolverError if none is
+        left."""
+        n, pp, cp, _ = self._batch_arrays(problems, configs)
+        statuses = (C.c_int * n)()
+        st = self.lib.visloc_ba_cuda_batch_upload(self.ctx, n, pp, cp, statuses)
+        if st != _abi.OK:
+            raise SolverError(st, self.last_error())
+        self._batch_statuses = list(statuses)
+        return list(statuses)
+
+    def batch_solve_uploaded(self):
+        """Solve the uploaded batch from its initial state: list of BaResult
+        (None for problems left out)."""
+        n, cap = self._batch_n, self._batch_cap
+        res = (_abi.Result * n)()
+        iters = (_abi.Iteration * (n * cap))()
+        st = self.lib.visloc_ba_cuda_batch_solve_uploaded(self.ctx, res, iters, cap)
+        if st != _abi.OK:
+            raise SolverError(st, self.last_error())
+        return self._batch_results(res, iters, self._batch_statuses, n, cap)
+
+    def batch_download(self, problems) -> None:
+        n = len(problems)
+        probs = [p.abi() for p in problems]
+        pp = (C.POINTER(_abi.Problem) * n)(*[C.pointer(x) for x in probs])
+        st = self.lib.visloc_ba_cuda_batch_download(self.ctx, n, pp)
+        if st != _abi.OK:
+            raise SolverError(st, self.last_error())
+
+    def batch_optimize(self, problems, configs):
+        """Solve a batch in place: (statuses, [BaResult | None])."""
+        n, pp, cp, cap = self._batch_arrays(problems, configs)
+        statuses = (C.c_int * n)()
+        res = (_abi.Result * n)()
+        iters = (_abi.Iteration * (n * cap))()
+        st = self.lib.visloc_ba_cuda_batch_optimize(self.ctx, n, pp, cp, statuses, res, iters, cap)
+        if st != _abi.OK:
+            raise SolverError(st, self.last_error())
+        return list(statuses), self._batch_results(res, iters, list(statuses), n, cap)
+
     def linear_step(self, packed: PackedProblem, config: BaConfig, lam: float):
         """One damped step at the current state: (dp (6 per variable pose),
         dl (3 per variable landmark), PCG iterations, PCG relative residual)."""

@@ -249,27 +249,27 @@ def stereo_window(num_keyframes=20, num_points=2000, seed=0, *, baseline=0.11,
     X = np.stack([rng.uniform(-6, 6, num_points), rng.uniform(-3, 3, num_points),
                   rng.uniform(3, 25, num_points) + s.max() * rng.random(num_points)], 1)
     ext_t = np.array([-baseline, 0.0, 0.0])
-    # Candidate sensors: 2n (kf, side).
+    # Candidate sensors: 2n (kf, side); each point takes U{lo..hi} of the
+    # sensors that see it, in random order (points seen by fewer than two
+    # sensors stay unobserved).
     kf = np.repeat(np.arange(n), 2)
     side = np.tile([0, 1], n)
-    obs_pose, obs_pt, obs_side = [], [], []
     lo, hi = obs_per_point
     want = rng.integers(lo, hi + 1, num_points)
-    for j in range(num_points):
-        xc = r_true[kf] @ X[j] + t_true[kf] + np.where(side[:, None] == 1, ext_t, 0.0)
-        z = xc[:, 2]
-        u = f * xc[:, 0] / np.maximum(z, 1e-9) + cx
-        v = f * xc[:, 1] / np.maximum(z, 1e-9) + cy
-        vis = np.nonzero((z > 0.5) & (u >= 0) & (u < width) & (v >= 0) & (v < height))[0]
-        if vis.size < 2:
-            continue
-        pick = rng.choice(vis, size=min(int(want[j]), vis.size), replace=False)
-        obs_pose.append(kf[pick])
-        obs_side.append(side[pick])
-        obs_pt.append(np.full(pick.size, j))
-    obs_pose = np.concatenate(obs_pose).astype(np.uint32)
-    obs_side = np.concatenate(obs_side).astype(np.uint32)
-    obs_pt = np.concatenate(obs_pt).astype(np.uint32)
+    ts = t_true[kf] + np.where(side[:, None] == 1, ext_t, 0.0)
+    xc = np.einsum("sij,mj->msi", r_true[kf], X) + ts[None]
+    z = xc[..., 2]
+    u = f * xc[..., 0] / np.maximum(z, 1e-9) + cx
+    v = f * xc[..., 1] / np.maximum(z, 1e-9) + cy
+    vis = (z > 0.5) & (u >= 0) & (u < width) & (v >= 0) & (v < height)
+    nvis = vis.sum(1)
+    take = np.where(nvis >= 2, np.minimum(want, nvis), 0)
+    order = np.argsort(rng.random(vis.shape) + np.where(vis, 0.0, 2.0), axis=1)
+    rows, cols = np.nonzero(np.arange(2 * n)[None, :] < take[:, None])
+    sensor = order[rows, cols]
+    obs_pose = kf[sensor].astype(np.uint32)
+    obs_side = side[sensor].astype(np.uint32)
+    obs_pt = rows.astype(np.uint32)
     xc = np.einsum("nij,nj->ni", r_true[obs_pose], X[obs_pt]) + t_true[obs_pose]
     xc = xc + np.where(obs_side[:, None] == 1, ext_t, 0.0)
     uv = np.stack([f * xc[:, 0] / xc[:, 2] + cx, f * xc[:, 1] / xc[:, 2] + cy], 1)
@@ -286,6 +286,16 @@ def stereo_window(num_keyframes=20, num_points=2000, seed=0, *, baseline=0.11,
                            np.zeros(num_points, np.uint8), obs_side)
     packed.truth = dict(pose_q=q_true, pose_t=t_true, points=X, centers=centers)
     return packed
+
+
+def window_batch(num_windows=512, seed=4000, *, keyframes=(5, 40), points=(200, 5000)):
+    """Uneven local BA windows: each a stereo window of U{5..40} keyframes
+    and U{200..5000} points (3-12 observations per point, 10% of the poses
+    fixed as anchors), seeded per window."""
+    rng = np.random.default_rng(seed)
+    nk = rng.integers(keyframes[0], keyframes[1] + 1, num_windows)
+    npt = rng.integers(points[0], points[1] + 1, num_windows)
+    return [stereo_window(int(nk[w]), int(npt[w]), seed=seed + 1 + w) for w in range(num_windows)]
 
 
 def pose_only(num_matches=500, seed=0, *, width=752, height=480, f=458.0,
