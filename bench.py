@@ -25,6 +25,15 @@ baseline 0.11 m, 752x480 pinhole, 200-5,000 points, 3-12 observations per
 point, 10% of the poses fixed), ~9.3M observations, solved as one batch with
 the 10-iteration LM loop captured as a CUDA graph; one step = one batched
 solve.  `value` counts the LM iterations of all windows.
+
+Workload `served`: a Poisson stream of requests, 70% local windows (10-40
+stereo keyframes, 1k-5k points), 25% pose-only refinements (100-2,000
+matches, 30% outliers), 5% global BAs (300 cameras, 60k points, ~400k
+observations), through the serving loop (visloc_ba_cuda_server_*) at an
+offered rate of five times the plain per-problem solve rate; `value` is the
+served solves/s (wall clock), with p50/p99 latency, beside the plain rate
+(the same requests solved one by one through visloc_ba_cuda_optimize) and the
+saturated rate (every request submitted at once).
 """
 
 from __future__ import annotations
@@ -53,7 +62,9 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="ring-4m", choices=["ring-4m", "ring-50", "windows-512"])
+    ap.add_argument("--workload", default="ring-4m",
+                    choices=["ring-4m", "ring-50", "windows-512", "served"])
+    ap.add_argument("--requests", type=int, default=300, help="served: stream length")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
@@ -521,6 +532,139 @@ def run_batch(args, dist: Dist):
     solver.close()
 
 
+def served_requests(n, seed):
+    from visloc_ba import synth
+
+    rng = np.random.default_rng(seed)
+    reqs = []
+    for i in range(n):
+        u = rng.random()
+        if u < 0.70:
+            reqs.append(("window", synth.stereo_window(int(rng.integers(10, 41)),
+                                                       int(rng.integers(1000, 5001)),
+                                                       seed=seed + 1 + i)))
+        elif u < 0.95:
+            reqs.append(("pose-only", synth.pose_only(int(rng.integers(100, 2001)),
+                                                      seed=seed + 1 + i)))
+        else:
+            reqs.append(("global", synth.ring_problem(
+                300, 60000, seed=seed + 1 + i, width=1920, height=1080, focal=(1500.0, 1500.0),
+                k1=(0.0, 0.0), per_camera_intrinsics=False, track=("geometric", 6.7, 2, 40))))
+    return reqs
+
+
+def serve_stream(server, reqs, cfg, rate, seed):
+    """Submit `reqs` at Poisson arrival times (rate per second; 0 = all at
+    once) and wait for all: (wall seconds, latencies ms, kinds)."""
+    import threading
+
+    rng = np.random.default_rng(seed)
+    gaps = rng.exponential(1.0 / rate, len(reqs)) if rate > 0 else np.zeros(len(reqs))
+    copies = [p.copy() for _, p in reqs]
+    tickets = [None] * len(reqs)
+    lat = [None] * len(reqs)
+    ready = threading.Semaphore(0)
+
+    def waiter():
+        for i in range(len(reqs)):
+            ready.acquire()
+            st, _, info = server.wait(tickets[i])
+            if st != 0:
+                raise RuntimeError(f"request {i} failed: {st} {server.last_error()}")
+            lat[i] = info["latency_ms"]
+
+    th = threading.Thread(target=waiter)
+    th.start()
+    t0 = time.perf_counter()
+    due = t0
+    for i, c in enumerate(copies):
+        due += gaps[i]
+        delay = due - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        tickets[i] = server.submit(c, cfg)
+        ready.release()
+    th.join()
+    wall = time.perf_counter() - t0
+    return wall, lat, [k for k, _ in reqs]
+
+
+def run_served(args, dist: Dist):
+    """The served mixed stream through the serving loop, against the plain
+    per-problem solve of the same requests."""
+    import torch
+
+    from visloc_ba import BaConfig, RobustKernel
+    from visloc_ba.solver import BaServer, CudaSolver
+
+    torch.cuda.set_device(dist.local)
+    reqs = served_requests(args.requests, 5000 + 1000 * dist.rank)
+    cfg = BaConfig(max_iterations=10, robust_kernel=RobustKernel.huber(1.0),
+                   max_pcg_iterations=100, pcg_relative_tolerance=1e-4)
+    solver = CudaSolver(dist.local)
+    for _, p in reqs[: args.warmup]:
+        solver.optimize(p.copy(), cfg)
+    dist.barrier()
+    t0 = time.perf_counter()
+    for _, p in reqs:
+        st, _ = solver.optimize(p.copy(), cfg)
+        if st != 0:
+            raise RuntimeError(solver.last_error())
+    plain = len(reqs) / (time.perf_counter() - t0)
+    solver.close()
+
+    server = BaServer(dist.local, slots=3, memory_bytes=12 << 30, max_batch=64)
+    serve_stream(server, reqs[: max(8, args.warmup)], cfg, 0.0, 1)  # warm-up
+    clocks = Clocks(dist.local)
+    dist.barrier()
+    clocks.start()
+    wall, lat, kinds = serve_stream(server, reqs, cfg, 5.0 * plain, 2)
+    clk = clocks.stop()
+    sat_wall, sat_lat, _ = serve_stream(server, reqs, cfg, 0.0, 3)
+    server.close()
+    value = dist.sum(len(reqs) / dist.max(wall))
+    lat = np.array(lat)
+    by_kind = {}
+    for k in sorted(set(kinds)):
+        v = np.array([x for x, kk in zip(lat, kinds) if kk == k])
+        by_kind[k] = {"count": int(v.size), "p50_ms": float(np.percentile(v, 50)),
+                      "p99_ms": float(np.percentile(v, 99))}
+    if dist.rank == 0:
+        nobs = sum(p.num_observations for _, p in reqs)
+        line = {
+            "metric": "served_solves_per_s", "value": value, "unit": "solves/s",
+            "n_gpus": dist.world, "steps": 1, "warmup": args.warmup,
+            "ms_per_step": 1e3 * wall, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+            "config": {"workload": "served", "requests": len(reqs),
+                       "mix": "70% windows (10-40 kf, 1k-5k pts), 25% pose-only "
+                              "(100-2000 matches, 30% outliers), 5% global "
+                              "(300 cams, 60k pts, ~400k obs)",
+                       "observations": int(nobs), "lm_iterations": 10,
+                       "pcg": "tol 1e-4, max 100", "robust": "huber(1px)",
+                       "arrivals": "Poisson at 5x the plain solve rate",
+                       "server": "3 slots x 4 GiB, batches <= 64",
+                       "parallelism": f"replicas x{dist.world}"},
+            "latency_ms": {"p50": float(np.percentile(lat, 50)),
+                           "p99": float(np.percentile(lat, 99)),
+                           "max": float(lat.max())},
+            "latency_by_kind": by_kind,
+            "offered_rate": 5.0 * plain,
+            "plain_per_problem_solves_per_s": plain,
+            "saturated_solves_per_s": len(reqs) / sat_wall,
+            "saturated_latency_ms": {"p50": float(np.percentile(sat_lat, 50)),
+                                     "p99": float(np.percentile(sat_lat, 99))},
+            "clocks": clk,
+            "e2e": {"value": value, "unit": "solves/s",
+                    "h2d_bytes_per_step": int(sum(p.num_poses * 57 + p.num_landmarks * 25 +
+                                                  p.num_observations * 20 for _, p in reqs)),
+                    "d2h_bytes_per_step": int(sum(p.num_poses * 56 + p.num_landmarks * 24
+                                                  for _, p in reqs))},
+            "cpu_baseline": None,
+        }
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse_args()
     dist = Dist()
@@ -529,6 +673,8 @@ def main():
             run_reference(args, dist)
         elif args.workload == "windows-512":
             run_batch(args, dist)
+        elif args.workload == "served":
+            run_served(args, dist)
         else:
             run_ours(args, dist)
     finally:

@@ -304,6 +304,43 @@ int visloc_ba_cuda_batch_solve_uploaded(void* ctx, vlba_result* results,
                                         uint32_t iterations_capacity);
 int visloc_ba_cuda_batch_download(void* ctx, uint32_t n, vlba_problem* const* problems);
 
+/* ----------------------------------------------------------------- serving */
+/* A request loop on one GPU for streams of independent solves (localisation
+ * refinements, local windows, occasional global BAs).  A submitted ticket is
+ * validated and planned on a host thread, then admitted into a batch by one
+ * of `slots` worker slots as soon as a slot and device memory are free; the
+ * batches of different slots overlap on the device.  A request of many
+ * observations runs as a batch of its own.  Each slot owns
+ * memory_bytes / slots of device memory, allocated once at creation
+ * (memory_bytes 0: half of the free memory); a request that does not fit a
+ * slot completes with VLBA_ERR_OUT_OF_MEMORY.  Results are the same as solving
+ * the problem alone.  The problem's arrays are read while the ticket is
+ * planned and written (the optimised state) when it completes: keep them
+ * alive and untouched until visloc_ba_cuda_server_wait has returned for the
+ * ticket.  The reference has no serving loop; its callers solve one problem
+ * per BaAccelerator::optimize call (ba_accel.rs:23-32). */
+typedef struct vlba_ticket_info {
+  double latency_ms;   /* submit -> done */
+  double queue_ms;     /* submit -> its batch started (planning included) */
+  double solve_ms;     /* its batch's upload, LM and download */
+  uint32_t batch_size; /* problems in its batch */
+  uint32_t slot;
+} vlba_ticket_info;
+
+void* visloc_ba_cuda_server_create(int device, uint32_t slots, uint64_t memory_bytes,
+                                   uint32_t max_batch);
+/* Finishes the tickets already submitted, then stops. */
+void visloc_ba_cuda_server_destroy(void* server);
+int visloc_ba_cuda_server_submit(void* server, vlba_problem* problem,
+                                 const vlba_config* config, uint64_t* ticket);
+/* Wait up to timeout_ms (negative: no limit, 0: poll) for a ticket: its
+ * status (VLBA_ERR_BUSY if still pending), result, iterations and timing.
+ * A ticket whose status has been returned is released. */
+int visloc_ba_cuda_server_wait(void* server, uint64_t ticket, double timeout_ms,
+                               vlba_result* result, vlba_iteration* iterations,
+                               uint32_t iterations_capacity, vlba_ticket_info* info);
+const char* visloc_ba_cuda_server_last_error(void* server);
+
 /* ------------------------------------------------------------- diagnostics */
 /* One damped linear step at the given state, without updating it: the step
  * of solve_step (bundle/normal_equations.rs:1621-1733) as this solver forms

@@ -4,7 +4,10 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <atomic>
+#include <exception>
 #include <stdexcept>
+#include <thread>
 #include <unordered_map>
 
 namespace vlba {
@@ -149,8 +152,12 @@ Validation validate_problem(const vlba_problem* p, const vlba_config* cfg) {
   return v;
 }
 
-void build_plan(const vlba_problem* const* problems, const vlba_config* const* configs,
-                uint32_t n, uint32_t tb, Plan* plan) {
+namespace {
+
+void finish_tiles(Plan& P);
+
+void build_plan_serial(const vlba_problem* const* problems, const vlba_config* const* configs,
+                       uint32_t n, uint32_t tb, Plan* plan) {
   Plan& P = *plan;
   P = Plan();
   P.tb = tb;
@@ -277,16 +284,17 @@ void build_plan(const vlba_problem* const* problems, const vlba_config* const* c
     for (uint32_t j = 0; j < nl; ++j) {
       if (!P.point_var[point_base + j]) continue;
       const uint32_t k0 = cnt[j], k1 = cnt[j + 1];
+      // Each unordered pair once; the observation of the larger slot first.
       for (uint32_t a = k0; a < k1; ++a) {
         const uint32_t sa = P.obs_slot[obs_base + a];
         if (sa == kNone) continue;
         ++P.var_obs;
-        for (uint32_t b = k0; b < k1; ++b) {
-          if (b == a) continue;
+        for (uint32_t b = k0; b < a; ++b) {
           const uint32_t sb = P.obs_slot[obs_base + b];
           if (sb == kNone) continue;
           if (sa > sb) ++key_count(sa - slot_base, sb - slot_base);
-          else if (sa == sb) ++dup_cnt[sa - slot_base + 1];
+          else if (sb > sa) ++key_count(sb - slot_base, sa - slot_base);
+          else dup_cnt[sa - slot_base + 1] += 2;  // both orders
         }
       }
     }
@@ -359,15 +367,19 @@ void build_plan(const vlba_problem* const* problems, const vlba_config* const* c
       for (uint32_t a = k0; a < k1; ++a) {
         const uint32_t sa = P.obs_slot[obs_base + a];
         if (sa == kNone) continue;
-        for (uint32_t b = k0; b < k1; ++b) {
-          if (b == a) continue;
+        for (uint32_t b = k0; b < a; ++b) {
           const uint32_t sb = P.obs_slot[obs_base + b];
           if (sb == kNone) continue;
           if (sa > sb) {
             const uint32_t blk = key_count(sa - slot_base, sb - slot_base);
             P.pairs[blk_fill[blk]++] = PairIdx{obs_base + a, obs_base + b};
-          } else if (sa == sb) {
-            P.dup_pairs[dup_base + dup_fill[sa - slot_base]++] = PairIdx{obs_base + a, obs_base + b};
+          } else if (sb > sa) {
+            const uint32_t blk = key_count(sb - slot_base, sa - slot_base);
+            P.pairs[blk_fill[blk]++] = PairIdx{obs_base + b, obs_base + a};
+          } else {
+            uint32_t& f = dup_fill[sa - slot_base];
+            P.dup_pairs[dup_base + f++] = PairIdx{obs_base + a, obs_base + b};
+            P.dup_pairs[dup_base + f++] = PairIdx{obs_base + b, obs_base + a};
           }
         }
       }
@@ -405,6 +417,17 @@ void build_plan(const vlba_problem* const* problems, const vlba_config* const* c
   P.num_tile_rows = tr_base;
   // Partial slots: position of (tile, side) in the tile-row lists, so a row's
   // partials are contiguous.
+  finish_tiles(P);
+  P.num_pairs = P.pairs.size();
+  // Lanes per block in the off-diagonal assembly.  The lane count sets the
+  // order of each block's sum, so it is the same for every problem and batch
+  // (a result must not depend on what it is batched with).
+  P.group = 8;
+}
+
+// Partial slots (positions of each tile's row and column side in the
+// tile-row lists) and the per-tile metadata the PCG reads.
+void finish_tiles(Plan& P) {
   P.tile_slot.assign(P.tile_ij.size(), PairIdx{kNone, kNone});
   for (uint32_t m = 0; m < (uint32_t)P.tr_list.size(); ++m) {
     const uint32_t t = P.tr_list[m] / 2, side = P.tr_list[m] % 2;
@@ -418,11 +441,146 @@ void build_plan(const vlba_problem* const* problems, const vlba_config* const* c
     P.tile_meta[4 * t + 2] = P.tile_slot[t].b;
     P.tile_meta[4 * t + 3] = P.tr_prob[P.tile_ij[t] >> 16];
   }
+}
+
+}  // namespace
+
+void merge_plans(const std::vector<const Plan*>& parts, Plan* out) {
+  Plan& P = *out;
+  P = Plan();
+  if (parts.empty()) throw std::runtime_error("merge of no plans");
+  P.tb = parts[0]->tb;
+  P.group = parts[0]->group;
+  size_t tp = 0, tl = 0, to = 0;
+  for (const Plan* q : parts) {
+    if (q->tb != P.tb || q->group != P.group) throw std::runtime_error("plans of different shapes");
+    tp += q->pose_prob.size();
+    tl += q->point_prob.size();
+    to += q->obs_pose.size();
+  }
+  if (tp >= kNone || tl >= kNone || to >= kNone)
+    throw std::runtime_error("batch exceeds 2^32 poses, points or observations");
+  auto cat = [](auto& dst, const auto& src) { dst.insert(dst.end(), src.begin(), src.end()); };
+  const uint32_t tf = P.tb * P.tb * kBlock;
+  uint32_t pose_b = 0, point_b = 0, obs_b = 0, slot_b = 0, tr_b = 0, tile_b = 0, cam_b = 0;
+  uint32_t pair_b = 0, dup_b = 0, camobs_b = 0, trl_b = 0, chunk_b = 0;
+  P.num_problems = 0;
+  P.prob_pose_begin = {0};
+  P.prob_point_begin = {0};
+  P.prob_obs_begin = {0};
+  P.prob_tr_begin = {0};
+  P.prob_chunk_begin = {0};
+  P.prob_camera_begin = {0};
+  P.pt_off = {0};
+  P.cam_off = {0};
+  P.blk_off = {0};
+  P.dup_off = {0};
+  P.tr_list_off = {0};
+  P.chunk_point_begin = {0};
+  for (const Plan* qp : parts) {
+    const Plan& Q = *qp;
+    for (uint32_t qi = 0; qi < Q.num_problems; ++qi) {
+      const uint32_t pi = P.num_problems + qi;
+      P.prob_pose_begin.push_back(pose_b + Q.prob_pose_begin[qi + 1]);
+      P.prob_point_begin.push_back(point_b + Q.prob_point_begin[qi + 1]);
+      P.prob_obs_begin.push_back(obs_b + Q.prob_obs_begin[qi + 1]);
+      P.prob_tr_begin.push_back(tr_b + Q.prob_tr_begin[qi + 1]);
+      P.prob_chunk_begin.push_back(chunk_b + Q.prob_chunk_begin[qi + 1]);
+      P.prob_camera_begin.push_back(cam_b + Q.prob_camera_begin[qi + 1]);
+      (void)pi;
+    }
+    const uint32_t pb = P.num_problems;
+    for (uint32_t v : Q.pose_prob) P.pose_prob.push_back(pb + v);
+    for (uint32_t v : Q.point_prob) P.point_prob.push_back(pb + v);
+    for (uint32_t v : Q.slot_prob) P.slot_prob.push_back(pb + v);
+    for (uint32_t v : Q.tr_prob) P.tr_prob.push_back(pb + v);
+    cat(P.params, Q.params);
+    cat(P.pose_q, Q.pose_q);
+    cat(P.pose_t, Q.pose_t);
+    cat(P.points, Q.points);
+    for (uint32_t v : Q.pose_slot) P.pose_slot.push_back(v == kNone ? kNone : slot_b + v);
+    cat(P.point_var, Q.point_var);
+    cat(P.cameras, Q.cameras);
+    for (size_t j = 1; j < Q.pt_off.size(); ++j) P.pt_off.push_back(obs_b + Q.pt_off[j]);
+    for (uint32_t v : Q.obs_pose) P.obs_pose.push_back(pose_b + v);
+    for (uint32_t v : Q.obs_cam) P.obs_cam.push_back(cam_b + v);
+    for (uint32_t v : Q.obs_slot) P.obs_slot.push_back(v == kNone ? kNone : slot_b + v);
+    cat(P.obs_xy, Q.obs_xy);
+    for (size_t j = 1; j < Q.cam_off.size(); ++j) P.cam_off.push_back(camobs_b + Q.cam_off[j]);
+    for (uint32_t v : Q.cam_obs) P.cam_obs.push_back(obs_b + v);
+    for (uint32_t v : Q.tile_ij) {
+      const uint32_t I = (v >> 16) + tr_b, J = (v & 0xFFFFu) + tr_b;
+      if (I > 0xFFFFu || J > 0xFFFFu) throw std::runtime_error("more than 65535 tile rows");
+      P.tile_ij.push_back((I << 16) | J);
+    }
+    for (size_t j = 1; j < Q.blk_off.size(); ++j) P.blk_off.push_back(pair_b + Q.blk_off[j]);
+    for (const PairIdx& v : Q.pairs) P.pairs.push_back(PairIdx{obs_b + v.a, obs_b + v.b});
+    const uint64_t fo = (uint64_t)tile_b * tf;
+    if (fo + (uint64_t)Q.tile_ij.size() * tf >= kNone)
+      throw std::runtime_error("reduced systems exceed 2^32 floats");
+    for (const PairIdx& v : Q.blk_dst)
+      P.blk_dst.push_back(PairIdx{(uint32_t)(v.a + fo), v.b == kNone ? kNone : (uint32_t)(v.b + fo)});
+    for (uint32_t v : Q.diag_dst) P.diag_dst.push_back((uint32_t)(v + fo));
+    for (size_t j = 1; j < Q.dup_off.size(); ++j) P.dup_off.push_back(dup_b + Q.dup_off[j]);
+    for (const PairIdx& v : Q.dup_pairs) P.dup_pairs.push_back(PairIdx{obs_b + v.a, obs_b + v.b});
+    for (size_t j = 1; j < Q.tr_list_off.size(); ++j) P.tr_list_off.push_back(trl_b + Q.tr_list_off[j]);
+    for (uint32_t v : Q.tr_list) P.tr_list.push_back(v + 2 * tile_b);
+    for (size_t j = 1; j < Q.chunk_point_begin.size(); ++j)
+      P.chunk_point_begin.push_back(point_b + Q.chunk_point_begin[j]);
+    P.real_var_cams += Q.real_var_cams;
+    P.var_points += Q.var_points;
+    P.var_obs += Q.var_obs;
+    P.camera_pairs += Q.camera_pairs;
+    P.num_problems += Q.num_problems;
+    pose_b += (uint32_t)Q.pose_prob.size();
+    point_b += (uint32_t)Q.point_prob.size();
+    obs_b += (uint32_t)Q.obs_pose.size();
+    slot_b += Q.num_var_cams;
+    tr_b += Q.num_tile_rows;
+    tile_b += (uint32_t)Q.tile_ij.size();
+    cam_b += (uint32_t)Q.cameras.size();
+    pair_b += (uint32_t)Q.pairs.size();
+    dup_b += (uint32_t)Q.dup_pairs.size();
+    camobs_b += (uint32_t)Q.cam_obs.size();
+    trl_b += (uint32_t)Q.tr_list.size();
+    chunk_b += (uint32_t)Q.chunk_point_begin.size() - 1;
+  }
+  P.num_var_cams = slot_b;
+  P.num_tile_rows = tr_b;
   P.num_pairs = P.pairs.size();
-  // Lanes per block in the off-diagonal assembly.  The lane count sets the
-  // order of each block's sum, so it is the same for every problem and batch
-  // (a result must not depend on what it is batched with).
-  P.group = 8;
+  finish_tiles(P);
+}
+
+void build_plan(const vlba_problem* const* problems, const vlba_config* const* configs,
+                uint32_t n, uint32_t tb, Plan* plan) {
+  if (n <= 1) {
+    build_plan_serial(problems, configs, n, tb, plan);
+    return;
+  }
+  // One plan per problem on the host's threads, then one merge: the same
+  // per-problem layout as a single build, so results do not depend on it.
+  std::vector<Plan> parts(n);
+  std::atomic<uint32_t> next{0};
+  std::exception_ptr err;
+  std::atomic<bool> failed{false};
+  auto work = [&] {
+    for (uint32_t i; (i = next.fetch_add(1)) < n && !failed.load();) {
+      try {
+        build_plan_serial(problems + i, configs + i, 1, tb, &parts[i]);
+      } catch (...) {
+        if (!failed.exchange(true)) err = std::current_exception();
+      }
+    }
+  };
+  const uint32_t nt = std::max(1u, std::min<uint32_t>(n, std::thread::hardware_concurrency()));
+  std::vector<std::thread> pool;
+  for (uint32_t t = 1; t < nt; ++t) pool.emplace_back(work);
+  work();
+  for (auto& t : pool) t.join();
+  if (err) std::rethrow_exception(err);
+  std::vector<const Plan*> ptrs;
+  for (const Plan& q : parts) ptrs.push_back(&q);
+  merge_plans(ptrs, plan);
 }
 
 std::string check_plan(const Plan& P) {

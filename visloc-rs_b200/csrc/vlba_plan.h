@@ -75,10 +75,17 @@ Validation validate_problem(const vlba_problem* p, const vlba_config* cfg);
 
 LmParams make_params(const vlba_config* cfg);
 
-// Build the plan for `n` problems (all must have validated OK).  `tb` is the
-// tile size (8 or 16).  Throws std::runtime_error on internal inconsistency.
+// Build the plan for `n` problems (all must have validated OK); with n > 1
+// each problem is built on its own host thread and the parts are merged.
+// `tb` is the tile size in blocks.  Throws std::runtime_error on internal
+// inconsistency.
 void build_plan(const vlba_problem* const* problems, const vlba_config* const* configs,
                 uint32_t n, uint32_t tb, Plan* plan);
+
+// Concatenate plans (built by build_plan) into one batch plan: indices are
+// offset, each problem's layout and order are kept, so a problem solves the
+// same in the merged plan as in its own.
+void merge_plans(const std::vector<const Plan*>& parts, Plan* out);
 
 // Bounds-check every index array of the plan against the arrays it indexes.
 // Returns an empty string when the plan is consistent.

@@ -14,8 +14,13 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <condition_variable>
+#include <deque>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
+#include <thread>
+#include <unordered_map>
 #include <string>
 #include <vector>
 
@@ -42,21 +47,46 @@ struct Status : std::runtime_error {
   Status(int c, const std::string& m, uint64_t i = 0) : std::runtime_error(m), code(c), index(i) {}
 };
 
-// Device memory owned by a context.
+// Device memory owned by a context: one cudaMalloc per array, or, after
+// use_slab(), bump allocation inside one slab allocated once (a serving slot
+// reuses its memory for every batch without further cudaMalloc/cudaFree).
 class Arena {
  public:
-  ~Arena() { release(); }
+  ~Arena() {
+    release();
+    if (slab_) cudaFree(slab_);
+  }
+  void use_slab(size_t bytes) {
+    release();
+    if (slab_) cudaFree(slab_);
+    slab_ = nullptr;
+    const cudaError_t e = cudaMalloc(&slab_, bytes);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      slab_ = nullptr;
+      throw CudaError(e, "cudaMalloc (slab)");
+    }
+    slab_size_ = bytes;
+  }
   template <typename T>
   T* alloc(size_t count) {
     if (count == 0) count = 1;
+    const size_t need = count * sizeof(T);
+    if (slab_) {
+      const size_t off = (slab_used_ + 255) / 256 * 256;
+      if (off + need > slab_size_) throw CudaError(cudaErrorMemoryAllocation, "slab exhausted");
+      slab_used_ = off + need;
+      bytes_ += need;
+      return reinterpret_cast<T*>(static_cast<char*>(slab_) + off);
+    }
     void* p = nullptr;
-    const cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+    const cudaError_t e = cudaMalloc(&p, need);
     if (e != cudaSuccess) {
       cudaGetLastError();
       throw CudaError(e, "cudaMalloc");
     }
     ptrs_.push_back(p);
-    bytes_ += count * sizeof(T);
+    bytes_ += need;
     return static_cast<T*>(p);
   }
   template <typename T>
@@ -69,12 +99,23 @@ class Arena {
     for (void* p : ptrs_) cudaFree(p);
     ptrs_.clear();
     bytes_ = 0;
+    slab_used_ = 0;
   }
   size_t bytes() const { return bytes_; }
 
  private:
   std::vector<void*> ptrs_;
   size_t bytes_ = 0;
+  void* slab_ = nullptr;
+  size_t slab_size_ = 0, slab_used_ = 0;
+};
+
+// Serialises the persistent PCG kernels of several contexts sharing a GPU
+// (each launch waits for the previous one of any context): two cooperative
+// grids never wait on each other's resources.
+struct PcgGate {
+  std::mutex mu;
+  cudaEvent_t last = nullptr;
 };
 
 struct Context {
@@ -99,6 +140,7 @@ struct Context {
   // the LM loop of the current upload captured as one graph (VLBA_FLAG_GRAPH)
   cudaGraphExec_t graph = nullptr;
   uint32_t graph_iters = 0;
+  PcgGate* gate = nullptr;  // set for the slots of a server
 };
 
 namespace {
@@ -331,7 +373,14 @@ uint64_t enqueue_iteration(Context* c, cudaEvent_t* ev) {
   check_launch(launch_cam_diag(d, s), "camera blocks");
   check_launch(launch_pcg_setup(d, s), "pcg setup");
   if (ev) VLBA_CUDA(cudaEventRecord(ev[2], s));
-  check_launch(launch_pcg(d, c->pcg_grid, s), "pcg");
+  if (c->gate && d.num_tile_rows) {
+    std::lock_guard<std::mutex> lock(c->gate->mu);
+    VLBA_CUDA(cudaStreamWaitEvent(s, c->gate->last, 0));
+    check_launch(launch_pcg(d, c->pcg_grid, s), "pcg");
+    VLBA_CUDA(cudaEventRecord(c->gate->last, s));
+  } else {
+    check_launch(launch_pcg(d, c->pcg_grid, s), "pcg");
+  }
   if (d.trace) dump_trace(c);
   if (ev) VLBA_CUDA(cudaEventRecord(ev[3], s));
   check_launch(launch_pose_update(d, s), "pose update");
@@ -588,7 +637,63 @@ void do_upload(Context* c, const vlba_problem* const* probs, const vlba_config* 
   if (upload_ms) *upload_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
 }
 
+// Write the current state of every uploaded problem back into `problems`
+// (slot[i]: problem of the plan for output i, -1 skips it).
+void download_all(Context* c, const std::vector<int>& slot, vlba_problem* const* problems) {
+  const Dev& d = c->dev;
+  const Plan& P = c->plan;
+  check_launch(launch_state_to_front(d, c->stream), "state gather");
+  std::vector<double> q(P.pose_q.size()), t(P.pose_t.size()), x(P.points.size());
+  VLBA_CUDA(cudaMemcpyAsync(q.data(), d.pose_q[0], q.size() * 8, cudaMemcpyDeviceToHost, c->stream));
+  VLBA_CUDA(cudaMemcpyAsync(t.data(), d.pose_t[0], t.size() * 8, cudaMemcpyDeviceToHost, c->stream));
+  VLBA_CUDA(cudaMemcpyAsync(x.data(), d.points[0], x.size() * 8, cudaMemcpyDeviceToHost, c->stream));
+  VLBA_CUDA(cudaStreamSynchronize(c->stream));
+  for (size_t i = 0; i < slot.size(); ++i) {
+    const int k = slot[i];
+    if (k < 0 || !problems[i]) continue;
+    vlba_problem* p = problems[i];
+    const uint32_t pose0 = P.prob_pose_begin[k], pt0 = P.prob_point_begin[k];
+    const size_t np = P.prob_pose_begin[k + 1] - pose0, nl = P.prob_point_begin[k + 1] - pt0;
+    if (np != p->num_poses || nl != p->num_landmarks)
+      throw Status(VLBA_ERR_INVALID_ARGUMENT, "download: problem sizes differ from the upload");
+    std::memcpy(p->pose_q, q.data() + 4 * (size_t)pose0, np * 32);
+    std::memcpy(p->pose_t, t.data() + 3 * (size_t)pose0, np * 24);
+    std::memcpy(p->landmarks, x.data() + 3 * (size_t)pt0, nl * 24);
+  }
+}
+
 }  // namespace
+
+Context* make_context(int device) {
+  std::unique_ptr<Context> c(new Context());
+  c->device = device;
+  int count = 0;
+  VLBA_CUDA(cudaGetDeviceCount(&count));
+  if (device < 0 || device >= count) throw std::runtime_error("no such device");
+  VLBA_CUDA(cudaSetDevice(device));
+  cudaDeviceProp prop;
+  VLBA_CUDA(cudaGetDeviceProperties(&prop, device));
+  if (prop.major < 10) throw std::runtime_error("requires an sm_100 (Blackwell) device");
+  c->sm_count = prop.multiProcessorCount;
+  c->l2_bytes = (size_t)prop.l2CacheSize;
+  c->pcg_grid_hint = 4 * prop.multiProcessorCount;
+  if (const char* f = std::getenv("VLBA_L2_RESIDENT_FRACTION")) c->l2_fraction = std::atof(f);
+  VLBA_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  for (auto& e : c->ev) VLBA_CUDA(cudaEventCreate(&e));
+  return c.release();
+}
+
+void free_context(Context* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  drop_graph(c);
+  c->arena.release();
+  for (auto& e : c->ev)
+    if (e) cudaEventDestroy(e);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
 }  // namespace vlba
 
 using vlba::Context;
@@ -619,41 +724,14 @@ void visloc_ba_cuda_default_config(vlba_config* out) {
 }
 
 void* visloc_ba_cuda_create(int device) {
-  auto* c = new (std::nothrow) Context();
-  if (!c) return nullptr;
-  c->device = device;
   try {
-    int count = 0;
-    VLBA_CUDA(cudaGetDeviceCount(&count));
-    if (device < 0 || device >= count) throw std::runtime_error("no such device");
-    VLBA_CUDA(cudaSetDevice(device));
-    cudaDeviceProp prop;
-    VLBA_CUDA(cudaGetDeviceProperties(&prop, device));
-    if (prop.major < 10) throw std::runtime_error("requires an sm_100 (Blackwell) device");
-    c->sm_count = prop.multiProcessorCount;
-    c->l2_bytes = (size_t)prop.l2CacheSize;
-    c->pcg_grid_hint = 4 * prop.multiProcessorCount;
-    if (const char* f = std::getenv("VLBA_L2_RESIDENT_FRACTION")) c->l2_fraction = std::atof(f);
-    VLBA_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
-    for (auto& e : c->ev) VLBA_CUDA(cudaEventCreate(&e));
+    return vlba::make_context(device);
   } catch (...) {
-    delete c;
     return nullptr;
   }
-  return c;
 }
 
-void visloc_ba_cuda_destroy(void* ctx) {
-  auto* c = static_cast<Context*>(ctx);
-  if (!c) return;
-  cudaSetDevice(c->device);
-  vlba::drop_graph(c);
-  c->arena.release();
-  for (auto& e : c->ev)
-    if (e) cudaEventDestroy(e);
-  if (c->stream) cudaStreamDestroy(c->stream);
-  delete c;
-}
+void visloc_ba_cuda_destroy(void* ctx) { vlba::free_context(static_cast<Context*>(ctx)); }
 
 const char* visloc_ba_cuda_last_error(void* ctx) {
   auto* c = static_cast<Context*>(ctx);
@@ -799,26 +877,7 @@ int visloc_ba_cuda_batch_download(void* ctx, uint32_t n, vlba_problem* const* pr
     if (!c->uploaded || c->batch_slot.size() != n)
       throw vlba::Status(VLBA_ERR_INVALID_ARGUMENT, "download: not the uploaded batch");
     vlba::set_device(c);
-    const vlba::Dev& d = c->dev;
-    const vlba::Plan& P = c->plan;
-    vlba::check_launch(vlba::launch_state_to_front(d, c->stream), "state gather");
-    std::vector<double> q(P.pose_q.size()), t(P.pose_t.size()), x(P.points.size());
-    VLBA_CUDA(cudaMemcpyAsync(q.data(), d.pose_q[0], q.size() * 8, cudaMemcpyDeviceToHost, c->stream));
-    VLBA_CUDA(cudaMemcpyAsync(t.data(), d.pose_t[0], t.size() * 8, cudaMemcpyDeviceToHost, c->stream));
-    VLBA_CUDA(cudaMemcpyAsync(x.data(), d.points[0], x.size() * 8, cudaMemcpyDeviceToHost, c->stream));
-    VLBA_CUDA(cudaStreamSynchronize(c->stream));
-    for (uint32_t i = 0; i < n; ++i) {
-      const int k = c->batch_slot[i];
-      if (k < 0 || !problems[i]) continue;
-      vlba_problem* p = problems[i];
-      const uint32_t pose0 = P.prob_pose_begin[k], pt0 = P.prob_point_begin[k];
-      const size_t np = P.prob_pose_begin[k + 1] - pose0, nl = P.prob_point_begin[k + 1] - pt0;
-      if (np != p->num_poses || nl != p->num_landmarks)
-        throw vlba::Status(VLBA_ERR_INVALID_ARGUMENT, "download: problem sizes differ from the upload");
-      std::memcpy(p->pose_q, q.data() + 4 * (size_t)pose0, np * 32);
-      std::memcpy(p->pose_t, t.data() + 3 * (size_t)pose0, np * 24);
-      std::memcpy(p->landmarks, x.data() + 3 * (size_t)pt0, nl * 24);
-    }
+    vlba::download_all(c, c->batch_slot, problems);
   });
 }
 
@@ -1005,6 +1064,345 @@ int visloc_ba_cuda_cost(void* ctx, const vlba_problem* problem, const vlba_confi
     if (cost) *cost = ctrl.initial_cost;
     if (nonprojectable) *nonprojectable = ctrl.initial_nonproj;
   });
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ server
+// A request loop on one GPU: tickets are planned on host threads as they
+// arrive, then admitted into batches by worker slots as slots and device
+// memory free up.  Each slot owns a context (its own stream and a slab of
+// device memory sized at start), so the batches of different slots overlap
+// on the device; the persistent PCG kernels of the slots take turns (PcgGate).
+// A large request (many observations) runs as a batch of its own, so small
+// requests are not held behind it.  Every problem keeps its own LM state and
+// fixed-order sums, so its result is the same in any batch.
+namespace vlba {
+namespace {
+
+double now_ms() {
+  return std::chrono::duration<double, std::milli>(
+             std::chrono::steady_clock::now().time_since_epoch())
+      .count();
+}
+
+struct Ticket {
+  uint64_t id = 0;
+  vlba_problem* problem = nullptr;
+  vlba_config config{};
+  Plan plan;
+  size_t bytes = 0;
+  uint64_t obs = 0;
+  int status = VLBA_ERR_BUSY;
+  uint64_t error_index = 0;
+  std::string error;
+  vlba_result result{};
+  std::vector<vlba_iteration> iters;
+  double t_submit = 0.0, t_start = 0.0, t_done = 0.0;
+  uint32_t batch = 0, slot = 0;
+  bool done = false;
+};
+
+struct Server {
+  int device = 0;
+  uint32_t max_batch = 64;
+  size_t slot_bytes = 0;
+  uint64_t large_obs = 100000;
+  std::vector<Context*> slots;
+  PcgGate gate;
+  std::mutex mu;
+  std::condition_variable cv;
+  std::deque<Ticket*> to_plan, ready;
+  std::unordered_map<uint64_t, std::unique_ptr<Ticket>> tickets;
+  uint64_t next_id = 1;
+  uint32_t planning = 0;  // tickets taken by a planner, not yet ready or done
+  bool stop = false;
+  std::vector<std::thread> threads;
+  std::string error;
+};
+
+// Device bytes a ticket's upload takes from a slot's slab (the plan's arrays
+// plus its iteration records and the slab's alignment padding).
+size_t ticket_bytes(const Plan& P, uint32_t records) {
+  return P.device_bytes() + (size_t)records * sizeof(vlba_iteration) + 64 * 256 + (1u << 20);
+}
+
+void plan_ticket(Server* S, Ticket* t) {
+  const Validation v = validate_problem(t->problem, &t->config);
+  if (v.status != VLBA_OK) {
+    t->status = v.status;
+    t->error_index = v.error_index;
+    t->error = "validation";
+    return;
+  }
+  try {
+    const vlba_problem* ps[1] = {t->problem};
+    const vlba_config* cs[1] = {&t->config};
+    build_plan(ps, cs, 1, (uint32_t)pick_tb(ps, 1), &t->plan);
+    const std::string bad = check_plan(t->plan);
+    if (!bad.empty()) throw Status(VLBA_ERR_INVALID_ARGUMENT, bad);
+    t->bytes = ticket_bytes(t->plan, t->config.max_iterations);
+    t->obs = t->problem->num_observations;
+    if (t->bytes > S->slot_bytes)
+      throw Status(VLBA_ERR_OUT_OF_MEMORY, "request larger than a serving slot's memory");
+    t->status = VLBA_ERR_BUSY;
+  } catch (const Status& e) {
+    t->status = e.code;
+    t->error = e.what();
+  } catch (const std::exception& e) {
+    t->status = VLBA_ERR_INVALID_ARGUMENT;
+    t->error = e.what();
+  }
+}
+
+void planner_loop(Server* S) {
+  for (;;) {
+    Ticket* t = nullptr;
+    {
+      std::unique_lock<std::mutex> lock(S->mu);
+      S->cv.wait(lock, [&] { return S->stop || !S->to_plan.empty(); });
+      if (S->to_plan.empty()) return;  // stopping
+      t = S->to_plan.front();
+      S->to_plan.pop_front();
+      ++S->planning;
+    }
+    plan_ticket(S, t);
+    std::lock_guard<std::mutex> lock(S->mu);
+    --S->planning;
+    if (t->status == VLBA_ERR_BUSY) {
+      S->ready.push_back(t);
+    } else {
+      t->done = true;
+      t->t_done = now_ms();
+    }
+    S->cv.notify_all();
+  }
+}
+
+// Takes the next batch from the ready queue (caller holds the lock): a large
+// request alone when it is first in line, else small requests in arrival
+// order up to the slot's memory and the batch cap (large ones wait for the
+// next slot).
+std::vector<Ticket*> take_batch(Server* S) {
+  std::vector<Ticket*> batch;
+  size_t bytes = 0;
+  for (auto it = S->ready.begin(); it != S->ready.end() && batch.size() < S->max_batch;) {
+    Ticket* t = *it;
+    if (t->obs >= S->large_obs) {
+      if (batch.empty()) {
+        batch.push_back(t);
+        S->ready.erase(it);
+        break;
+      }
+      ++it;
+      continue;
+    }
+    if (bytes + t->bytes > S->slot_bytes) break;
+    bytes += t->bytes;
+    batch.push_back(t);
+    it = S->ready.erase(it);
+  }
+  return batch;
+}
+
+void run_batch(Server* S, uint32_t k, const std::vector<Ticket*>& batch) {
+  Context* c = S->slots[k];
+  const double t0 = now_ms();
+  for (Ticket* t : batch) {
+    t->t_start = t0;
+    t->batch = (uint32_t)batch.size();
+    t->slot = k;
+  }
+  try {
+    set_device(c);
+    std::vector<const Plan*> parts;
+    uint32_t records = 1, flags = 0;
+    for (Ticket* t : batch) {
+      parts.push_back(&t->plan);
+      records = std::max(records, t->config.max_iterations);
+      flags |= t->config.flags;
+    }
+    if (parts.size() == 1) c->plan = std::move(batch[0]->plan);
+    else merge_plans(parts, &c->plan);
+    upload_plan(c, records);
+    c->flags = flags & ~(uint32_t)(VLBA_FLAG_GRAPH | VLBA_FLAG_PROFILE);
+    reset_state(c);
+    PhaseTimes pt;
+    const RunStats st = run_lm(c, false, &pt);
+    std::vector<int> slot(batch.size());
+    std::vector<vlba_result> res(batch.size());
+    std::vector<vlba_iteration> its(batch.size() * (size_t)records);
+    for (size_t i = 0; i < batch.size(); ++i) slot[i] = (int)i;
+    fill_results_bulk(c, slot, res.data(), its.data(), records, st, nullptr);
+    std::vector<vlba_problem*> probs;
+    for (Ticket* t : batch) probs.push_back(t->problem);
+    download_all(c, slot, probs.data());
+    for (size_t i = 0; i < batch.size(); ++i) {
+      Ticket* t = batch[i];
+      t->result = res[i];
+      const uint32_t m = std::min(res[i].num_iterations, records);
+      t->iters.assign(its.begin() + i * records, its.begin() + i * records + m);
+      t->status = VLBA_OK;
+    }
+  } catch (const Status& e) {
+    for (Ticket* t : batch) {
+      t->status = e.code;
+      t->error = e.what();
+    }
+  } catch (const CudaError& e) {
+    for (Ticket* t : batch) {
+      t->status = e.code == cudaErrorMemoryAllocation ? VLBA_ERR_OUT_OF_MEMORY : VLBA_ERR_CUDA;
+      t->error = e.what();
+    }
+  } catch (const std::exception& e) {
+    for (Ticket* t : batch) {
+      t->status = VLBA_ERR_INVALID_ARGUMENT;
+      t->error = e.what();
+    }
+  }
+  for (Ticket* t : batch) t->plan = Plan();  // the host plan is no longer needed
+  std::lock_guard<std::mutex> lock(S->mu);
+  const double t1 = now_ms();
+  for (Ticket* t : batch) {
+    t->done = true;
+    t->t_done = t1;
+  }
+  S->cv.notify_all();
+}
+
+void worker_loop(Server* S, uint32_t k) {
+  cudaSetDevice(S->device);
+  for (;;) {
+    std::vector<Ticket*> batch;
+    {
+      std::unique_lock<std::mutex> lock(S->mu);
+      // Stop only once every submitted ticket has been planned and taken.
+      S->cv.wait(lock, [&] {
+        return !S->ready.empty() || (S->stop && S->to_plan.empty() && S->planning == 0);
+      });
+      if (S->ready.empty()) return;
+      batch = take_batch(S);
+    }
+    if (!batch.empty()) run_batch(S, k, batch);
+  }
+}
+
+void stop_server(Server* S) {
+  {
+    std::lock_guard<std::mutex> lock(S->mu);
+    S->stop = true;
+  }
+  S->cv.notify_all();
+  for (auto& t : S->threads)
+    if (t.joinable()) t.join();
+  for (Context* c : S->slots) free_context(c);
+  S->slots.clear();
+  if (S->gate.last) cudaEventDestroy(S->gate.last);
+  S->gate.last = nullptr;
+}
+
+}  // namespace
+}  // namespace vlba
+
+extern "C" {
+
+void* visloc_ba_cuda_server_create(int device, uint32_t slots, uint64_t memory_bytes,
+                                   uint32_t max_batch) {
+  auto* S = new (std::nothrow) vlba::Server();
+  if (!S) return nullptr;
+  try {
+    S->device = device;
+    if (slots == 0) slots = 3;
+    if (max_batch) S->max_batch = max_batch;
+    VLBA_CUDA(cudaSetDevice(device));
+    if (memory_bytes == 0) {
+      size_t free_b = 0, total_b = 0;
+      VLBA_CUDA(cudaMemGetInfo(&free_b, &total_b));
+      memory_bytes = free_b / 2;
+    }
+    S->slot_bytes = (size_t)(memory_bytes / slots);
+    VLBA_CUDA(cudaEventCreateWithFlags(&S->gate.last, cudaEventDisableTiming));
+    for (uint32_t k = 0; k < slots; ++k) {
+      vlba::Context* c = vlba::make_context(device);
+      S->slots.push_back(c);
+      c->arena.use_slab(S->slot_bytes);
+      c->gate = &S->gate;
+    }
+    const uint32_t planners =
+        std::max(1u, std::min(8u, std::thread::hardware_concurrency() / 2));
+    for (uint32_t i = 0; i < planners; ++i) S->threads.emplace_back(vlba::planner_loop, S);
+    for (uint32_t k = 0; k < slots; ++k) S->threads.emplace_back(vlba::worker_loop, S, k);
+  } catch (...) {
+    vlba::stop_server(S);
+    delete S;
+    return nullptr;
+  }
+  return S;
+}
+
+void visloc_ba_cuda_server_destroy(void* server) {
+  auto* S = static_cast<vlba::Server*>(server);
+  if (!S) return;
+  vlba::stop_server(S);
+  delete S;
+}
+
+int visloc_ba_cuda_server_submit(void* server, vlba_problem* problem, const vlba_config* config,
+                                 uint64_t* ticket) {
+  auto* S = static_cast<vlba::Server*>(server);
+  if (!S || !problem || !config || !ticket) return VLBA_ERR_INVALID_ARGUMENT;
+  auto t = std::make_unique<vlba::Ticket>();
+  t->problem = problem;
+  t->config = *config;
+  t->t_submit = vlba::now_ms();
+  std::lock_guard<std::mutex> lock(S->mu);
+  if (S->stop) return VLBA_ERR_INVALID_ARGUMENT;
+  t->id = S->next_id++;
+  *ticket = t->id;
+  S->to_plan.push_back(t.get());
+  S->tickets.emplace(t->id, std::move(t));
+  S->cv.notify_all();
+  return VLBA_OK;
+}
+
+int visloc_ba_cuda_server_wait(void* server, uint64_t ticket, double timeout_ms,
+                               vlba_result* result, vlba_iteration* iterations,
+                               uint32_t iterations_capacity, vlba_ticket_info* info) {
+  auto* S = static_cast<vlba::Server*>(server);
+  if (!S) return VLBA_ERR_INVALID_ARGUMENT;
+  std::unique_lock<std::mutex> lock(S->mu);
+  auto it = S->tickets.find(ticket);
+  if (it == S->tickets.end()) return VLBA_ERR_INVALID_ARGUMENT;
+  vlba::Ticket* t = it->second.get();
+  auto ready = [&] { return t->done; };
+  if (timeout_ms < 0) S->cv.wait(lock, ready);
+  else if (!S->cv.wait_for(lock, std::chrono::duration<double, std::milli>(timeout_ms), ready))
+    return VLBA_ERR_BUSY;
+  if (result) {
+    *result = t->result;
+    result->error_index = t->error_index;
+  }
+  if (iterations && iterations_capacity) {
+    const size_t m = std::min<size_t>(iterations_capacity, t->iters.size());
+    std::memcpy(iterations, t->iters.data(), m * sizeof(vlba_iteration));
+  }
+  if (info) {
+    std::memset(info, 0, sizeof *info);
+    info->latency_ms = t->t_done - t->t_submit;
+    info->queue_ms = (t->t_start > 0.0 ? t->t_start : t->t_done) - t->t_submit;
+    info->solve_ms = t->t_start > 0.0 ? t->t_done - t->t_start : 0.0;
+    info->batch_size = t->batch;
+    info->slot = t->slot;
+  }
+  const int st = t->status;
+  if (st != VLBA_OK) S->error = t->error;
+  S->tickets.erase(it);
+  return st;
+}
+
+const char* visloc_ba_cuda_server_last_error(void* server) {
+  auto* S = static_cast<vlba::Server*>(server);
+  return S ? S->error.c_str() : "null server";
 }
 
 }  // extern "C"

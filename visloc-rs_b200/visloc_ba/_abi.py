@@ -169,6 +169,16 @@ class PlanInfo(C.Structure):
 
 P = C.POINTER
 # name -> (restype, argtypes): every symbol include/visloc_ba_cuda.h declares.
+class TicketInfo(C.Structure):
+    _fields_ = [
+        ("latency_ms", C.c_double),
+        ("queue_ms", C.c_double),
+        ("solve_ms", C.c_double),
+        ("batch_size", C.c_uint32),
+        ("slot", C.c_uint32),
+    ]
+
+
 SOLVER_EXPORTS = {
     "visloc_ba_cuda_abi_version": (C.c_uint32, []),
     "visloc_ba_cuda_default_config": (None, [P(Config)]),
@@ -212,6 +222,17 @@ SOLVER_EXPORTS = {
         C.c_int, [C.c_void_p, P(Result), P(Iteration), C.c_uint32],
     ),
     "visloc_ba_cuda_batch_download": (C.c_int, [C.c_void_p, C.c_uint32, P(P(Problem))]),
+    "visloc_ba_cuda_server_create": (C.c_void_p, [C.c_int, C.c_uint32, C.c_uint64, C.c_uint32]),
+    "visloc_ba_cuda_server_destroy": (None, [C.c_void_p]),
+    "visloc_ba_cuda_server_submit": (
+        C.c_int, [C.c_void_p, P(Problem), P(Config), P(C.c_uint64)],
+    ),
+    "visloc_ba_cuda_server_wait": (
+        C.c_int,
+        [C.c_void_p, C.c_uint64, C.c_double, P(Result), P(Iteration), C.c_uint32,
+         P(TicketInfo)],
+    ),
+    "visloc_ba_cuda_server_last_error": (C.c_char_p, [C.c_void_p]),
     # Device pointers for the problem arrays and both outputs; see the header.
     "visloc_ba_cuda_cost_noalloc": (
         C.c_int,

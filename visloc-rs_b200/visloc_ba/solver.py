@@ -299,3 +299,67 @@ class GpuBundleAdjuster:
             if e.status == _abi.DECLINED:
                 return None
             raise
+
+
+class BaServer:
+    """The request loop of libvisloc_ba_cuda.so (visloc_ba_cuda_server_*):
+    submit problems from any thread, wait for their results.  A submitted
+    problem's arrays are written in place when its ticket completes; the
+    server keeps the problem (and its config) alive until then."""
+
+    def __init__(self, device: int = 0, slots: int = 3, memory_bytes: int = 0,
+                 max_batch: int = 64, library: str | None = None):
+        self.lib = _abi.load_solver_library(library)
+        self.srv = self.lib.visloc_ba_cuda_server_create(int(device), int(slots),
+                                                          int(memory_bytes), int(max_batch))
+        if not self.srv:
+            raise RuntimeError("visloc_ba_cuda_server_create failed")
+        self._live = {}
+
+    def submit(self, packed: PackedProblem, config: BaConfig) -> int:
+        prob = packed.abi()
+        cfg = config.to_abi()
+        ticket = C.c_uint64()
+        st = self.lib.visloc_ba_cuda_server_submit(self.srv, C.byref(prob), C.byref(cfg),
+                                                   C.byref(ticket))
+        if st != _abi.OK:
+            raise SolverError(st, "submit")
+        self._live[ticket.value] = (packed, prob, cfg, max(1, int(config.max_iterations)))
+        return ticket.value
+
+    def wait(self, ticket: int, timeout_ms: float = -1.0):
+        """(status, BaResult | None, info dict); status BUSY if not done."""
+        packed, prob, cfg, cap = self._live[ticket]
+        res = _abi.Result()
+        iters = (_abi.Iteration * cap)()
+        info = _abi.TicketInfo()
+        st = self.lib.visloc_ba_cuda_server_wait(self.srv, ticket, float(timeout_ms),
+                                                 C.byref(res), iters, cap, C.byref(info))
+        if st == _abi.ERR_BUSY:
+            return st, None, None
+        del self._live[ticket]
+        meta = {"latency_ms": info.latency_ms, "queue_ms": info.queue_ms,
+                "solve_ms": info.solve_ms, "batch_size": info.batch_size, "slot": info.slot}
+        if st != _abi.OK:
+            return st, None, meta
+        return st, result_from_abi(res, iters, res.num_iterations), meta
+
+    def last_error(self) -> str:
+        return self.lib.visloc_ba_cuda_server_last_error(self.srv).decode()
+
+    def close(self):
+        if getattr(self, "srv", None):
+            self.lib.visloc_ba_cuda_server_destroy(self.srv)
+            self.srv = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
