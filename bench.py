@@ -605,12 +605,14 @@ def run_served(args, dist: Dist):
     for _, p in reqs[: args.warmup]:
         solver.optimize(p.copy(), cfg)
     dist.barrier()
-    t0 = time.perf_counter()
-    for _, p in reqs:
-        st, _ = solver.optimize(p.copy(), cfg)
-        if st != 0:
-            raise RuntimeError(solver.last_error())
-    plain = len(reqs) / (time.perf_counter() - t0)
+    plain = 0.0
+    for _ in range(2):  # the faster of two passes (host noise only lowers a pass)
+        t0 = time.perf_counter()
+        for _, p in reqs:
+            st, _ = solver.optimize(p.copy(), cfg)
+            if st != 0:
+                raise RuntimeError(solver.last_error())
+        plain = max(plain, len(reqs) / (time.perf_counter() - t0))
     solver.close()
 
     server = BaServer(dist.local, slots=3, memory_bytes=12 << 30, max_batch=64)

@@ -156,8 +156,28 @@ namespace {
 
 void finish_tiles(Plan& P);
 
+// Runs f(t) for t in [0, n) on n threads (t = 0 on the caller's thread),
+// rethrowing the first exception.
+template <typename F>
+void run_threads(uint32_t n, F&& f) {
+  std::exception_ptr err;
+  std::atomic<bool> failed{false};
+  auto body = [&](uint32_t t) {
+    try {
+      f(t);
+    } catch (...) {
+      if (!failed.exchange(true)) err = std::current_exception();
+    }
+  };
+  std::vector<std::thread> pool;
+  for (uint32_t t = 1; t < n; ++t) pool.emplace_back(body, t);
+  body(0);
+  for (auto& th : pool) th.join();
+  if (err) std::rethrow_exception(err);
+}
+
 void build_plan_serial(const vlba_problem* const* problems, const vlba_config* const* configs,
-                       uint32_t n, uint32_t tb, Plan* plan) {
+                       uint32_t n, uint32_t tb, Plan* plan, uint32_t max_threads) {
   Plan& P = *plan;
   P = Plan();
   P.tb = tb;
@@ -281,23 +301,78 @@ void build_plan_serial(const vlba_problem* const* problems, const vlba_config* c
       return map[(uint64_t)i * nv64 + j];
     };
     std::vector<uint32_t> dup_cnt(nslots + 1, 0);
-    for (uint32_t j = 0; j < nl; ++j) {
-      if (!P.point_var[point_base + j]) continue;
-      const uint32_t k0 = cnt[j], k1 = cnt[j + 1];
-      // Each unordered pair once; the observation of the larger slot first.
-      for (uint32_t a = k0; a < k1; ++a) {
-        const uint32_t sa = P.obs_slot[obs_base + a];
-        if (sa == kNone) continue;
-        ++P.var_obs;
-        for (uint32_t b = k0; b < a; ++b) {
-          const uint32_t sb = P.obs_slot[obs_base + b];
-          if (sb == kNone) continue;
-          if (sa > sb) ++key_count(sa - slot_base, sb - slot_base);
-          else if (sb > sa) ++key_count(sb - slot_base, sa - slot_base);
-          else dup_cnt[sa - slot_base + 1] += 2;  // both orders
-        }
+    // With a dense table and enough pairs, the points are split into T
+    // contiguous ranges counted (and later scattered) on T threads, each into
+    // its own table; per-thread offsets keep every block's list in point
+    // order, as the one-thread build has it.
+    uint32_t T = 1;
+    std::vector<uint32_t> range{0, nl};
+    if (dense_table && max_threads > 1) {
+      std::vector<double> work(nl + 1, 0.0);
+      for (uint32_t j = 0; j < nl; ++j) {
+        const double t = (double)(cnt[j + 1] - cnt[j]);
+        work[j + 1] = work[j] + t * t;
+      }
+      const double table_bytes = (double)(nv64 * nv64) * 4.0;
+      if (work[nl] > 2e6) {
+        T = std::min<uint32_t>(max_threads, (uint32_t)std::max(1.0, (256.0 * (1 << 20)) / table_bytes));
+        T = std::max(1u, std::min<uint32_t>(T, (uint32_t)(work[nl] / 2e5)));
+      }
+      range.assign(T + 1, nl);
+      range[0] = 0;
+      for (uint32_t t = 1, j = 0; t < T; ++t) {
+        const double goal = work[nl] * t / T;
+        while (j < nl && work[j + 1] < goal) ++j;
+        range[t] = j;
       }
     }
+    std::vector<std::vector<uint32_t>> ttab(T > 1 ? T : 0), tdup(T > 1 ? T : 0);
+    std::vector<uint64_t> tvar(T, 0);
+    auto count_points = [&](uint32_t t, uint32_t* tab, uint32_t* dup) {
+      for (uint32_t j = range[t]; j < range[t + 1]; ++j) {
+        if (!P.point_var[point_base + j]) continue;
+        const uint32_t k0 = cnt[j], k1 = cnt[j + 1];
+        // Each unordered pair once; the observation of the larger slot first.
+        for (uint32_t a = k0; a < k1; ++a) {
+          const uint32_t sa = P.obs_slot[obs_base + a];
+          if (sa == kNone) continue;
+          ++tvar[t];
+          for (uint32_t b = k0; b < a; ++b) {
+            const uint32_t sb = P.obs_slot[obs_base + b];
+            if (sb == kNone) continue;
+            if (sa > sb) {
+              if (tab) ++tab[(uint64_t)(sa - slot_base) * nv64 + (sb - slot_base)];
+              else ++key_count(sa - slot_base, sb - slot_base);
+            } else if (sb > sa) {
+              if (tab) ++tab[(uint64_t)(sb - slot_base) * nv64 + (sa - slot_base)];
+              else ++key_count(sb - slot_base, sa - slot_base);
+            } else {
+              dup[sa - slot_base + 1] += 2;  // both orders
+            }
+          }
+        }
+      }
+    };
+    if (T > 1) {
+      run_threads(T, [&](uint32_t t) {
+        ttab[t].assign(nv64 * nv64, 0);
+        tdup[t].assign(nslots + 1, 0);
+        count_points(t, ttab[t].data(), tdup[t].data());
+      });
+      run_threads(T, [&](uint32_t t) {  // merged counts, rows split over threads
+        for (uint64_t i = t; i < nv64; i += T)
+          for (uint64_t jj = 0; jj < i; ++jj) {
+            uint32_t sum = 0;
+            for (uint32_t u = 0; u < T; ++u) sum += ttab[u][i * nv64 + jj];
+            table[i * nv64 + jj] = sum;
+          }
+      });
+      for (uint32_t u = 0; u < T; ++u)
+        for (uint32_t q = 0; q <= nslots; ++q) dup_cnt[q] += tdup[u][q];
+    } else {
+      count_points(0, nullptr, dup_cnt.data());
+    }
+    for (uint32_t t = 0; t < T; ++t) P.var_obs += tvar[t];
     // Blocks in row-major order; per-tile existence.
     const uint32_t ntr = nslots / tb;
     std::vector<uint8_t> tile_has((size_t)ntr * ntr, 0);
@@ -361,28 +436,63 @@ void build_plan_serial(const vlba_problem* const* problems, const vlba_config* c
     const uint32_t dup_base = (uint32_t)P.dup_pairs.size();
     P.dup_pairs.resize(dup_base + dup_cnt[nslots]);
     std::vector<uint32_t> dup_fill(dup_cnt.begin(), dup_cnt.end() - 1);
-    for (uint32_t j = 0; j < nl; ++j) {
-      if (!P.point_var[point_base + j]) continue;
-      const uint32_t k0 = cnt[j], k1 = cnt[j + 1];
-      for (uint32_t a = k0; a < k1; ++a) {
-        const uint32_t sa = P.obs_slot[obs_base + a];
-        if (sa == kNone) continue;
-        for (uint32_t b = k0; b < a; ++b) {
-          const uint32_t sb = P.obs_slot[obs_base + b];
-          if (sb == kNone) continue;
-          if (sa > sb) {
-            const uint32_t blk = key_count(sa - slot_base, sb - slot_base);
-            P.pairs[blk_fill[blk]++] = PairIdx{obs_base + a, obs_base + b};
-          } else if (sb > sa) {
-            const uint32_t blk = key_count(sb - slot_base, sa - slot_base);
-            P.pairs[blk_fill[blk]++] = PairIdx{obs_base + b, obs_base + a};
-          } else {
-            uint32_t& f = dup_fill[sa - slot_base];
-            P.dup_pairs[dup_base + f++] = PairIdx{obs_base + a, obs_base + b};
-            P.dup_pairs[dup_base + f++] = PairIdx{obs_base + b, obs_base + a};
+    // fill(t, i, j): the next pair position of block (i, j) for range t.
+    auto scatter_points = [&](uint32_t t, uint32_t* fill_tab, uint32_t* dfill) {
+      auto next = [&](uint32_t i, uint32_t jj) -> uint32_t& {
+        if (fill_tab) return fill_tab[(uint64_t)i * nv64 + jj];
+        return blk_fill[key_count(i, jj)];
+      };
+      for (uint32_t j = range[t]; j < range[t + 1]; ++j) {
+        if (!P.point_var[point_base + j]) continue;
+        const uint32_t k0 = cnt[j], k1 = cnt[j + 1];
+        for (uint32_t a = k0; a < k1; ++a) {
+          const uint32_t sa = P.obs_slot[obs_base + a];
+          if (sa == kNone) continue;
+          for (uint32_t b = k0; b < a; ++b) {
+            const uint32_t sb = P.obs_slot[obs_base + b];
+            if (sb == kNone) continue;
+            if (sa > sb) {
+              P.pairs[next(sa - slot_base, sb - slot_base)++] = PairIdx{obs_base + a, obs_base + b};
+            } else if (sb > sa) {
+              P.pairs[next(sb - slot_base, sa - slot_base)++] = PairIdx{obs_base + b, obs_base + a};
+            } else {
+              uint32_t& f = dfill[sa - slot_base];
+              P.dup_pairs[dup_base + f++] = PairIdx{obs_base + a, obs_base + b};
+              P.dup_pairs[dup_base + f++] = PairIdx{obs_base + b, obs_base + a};
+            }
           }
         }
       }
+    };
+    if (T > 1) {
+      // Per-range start positions: block b's ranges in order, from blk_fill[b].
+      run_threads(T, [&](uint32_t t) {
+        for (uint64_t i = t; i < nv64; i += T)
+          for (uint64_t jj = 0; jj < i; ++jj) {
+            if (!table[i * nv64 + jj] && !ttab[0][i * nv64 + jj]) {
+              bool any = false;
+              for (uint32_t u = 1; u < T && !any; ++u) any = ttab[u][i * nv64 + jj] != 0;
+              if (!any) continue;
+            }
+            uint32_t at = blk_fill[table[i * nv64 + jj]];
+            for (uint32_t u = 0; u < T; ++u) {
+              const uint32_t c = ttab[u][i * nv64 + jj];
+              ttab[u][i * nv64 + jj] = at;
+              at += c;
+            }
+          }
+      });
+      for (uint32_t s = 0, q = 0; s < nslots; ++s) {
+        uint32_t at = dup_fill[s];
+        for (uint32_t u = 0; u < T; ++u) {
+          q = tdup[u][s + 1];
+          tdup[u][s + 1] = at;
+          at += q;
+        }
+      }
+      run_threads(T, [&](uint32_t t) { scatter_points(t, ttab[t].data(), tdup[t].data() + 1); });
+    } else {
+      scatter_points(0, nullptr, dup_fill.data());
     }
     for (uint32_t s = 0; s < nslots; ++s) P.dup_off.push_back(dup_base + dup_cnt[s + 1]);
     // Tile-row partial lists: row sides (I, J <= I), then column sides (K > I, I).
@@ -552,9 +662,10 @@ void merge_plans(const std::vector<const Plan*>& parts, Plan* out) {
 }
 
 void build_plan(const vlba_problem* const* problems, const vlba_config* const* configs,
-                uint32_t n, uint32_t tb, Plan* plan) {
+                uint32_t n, uint32_t tb, Plan* plan, uint32_t max_threads) {
+  if (max_threads == 0) max_threads = std::max(1u, std::thread::hardware_concurrency());
   if (n <= 1) {
-    build_plan_serial(problems, configs, n, tb, plan);
+    build_plan_serial(problems, configs, n, tb, plan, max_threads);
     return;
   }
   // One plan per problem on the host's threads, then one merge: the same
@@ -566,7 +677,7 @@ void build_plan(const vlba_problem* const* problems, const vlba_config* const* c
   auto work = [&] {
     for (uint32_t i; (i = next.fetch_add(1)) < n && !failed.load();) {
       try {
-        build_plan_serial(problems + i, configs + i, 1, tb, &parts[i]);
+        build_plan_serial(problems + i, configs + i, 1, tb, &parts[i], 1);
       } catch (...) {
         if (!failed.exchange(true)) err = std::current_exception();
       }

@@ -76,11 +76,12 @@ Validation validate_problem(const vlba_problem* p, const vlba_config* cfg);
 LmParams make_params(const vlba_config* cfg);
 
 // Build the plan for `n` problems (all must have validated OK); with n > 1
-// each problem is built on its own host thread and the parts are merged.
-// `tb` is the tile size in blocks.  Throws std::runtime_error on internal
+// each problem is built on its own host thread and the parts are merged;
+// one large problem splits its pair counting over up to `max_threads` threads
+// (0: all the host's).  `tb` is the tile size in blocks.  Throws std::runtime_error on internal
 // inconsistency.
 void build_plan(const vlba_problem* const* problems, const vlba_config* const* configs,
-                uint32_t n, uint32_t tb, Plan* plan);
+                uint32_t n, uint32_t tb, Plan* plan, uint32_t max_threads = 0);
 
 // Concatenate plans (built by build_plan) into one batch plan: indices are
 // offset, each problem's layout and order are kept, so a problem solves the

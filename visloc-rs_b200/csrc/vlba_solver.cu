@@ -47,9 +47,16 @@ struct Status : std::runtime_error {
   Status(int c, const std::string& m, uint64_t i = 0) : std::runtime_error(m), code(c), index(i) {}
 };
 
-// Device memory owned by a context: one cudaMalloc per array, or, after
-// use_slab(), bump allocation inside one slab allocated once (a serving slot
-// reuses its memory for every batch without further cudaMalloc/cudaFree).
+// A slab allocation that does not fit (the upload is redone on a larger slab).
+struct SlabFull : std::runtime_error {
+  size_t need;
+  explicit SlabFull(size_t n) : std::runtime_error("slab exhausted"), need(n) {}
+};
+
+// Device memory owned by a context: bump allocation inside one slab.  A
+// context's slab grows to the largest upload it has seen (capacity-grown, so
+// repeated solves of similar sizes allocate nothing); a serving slot's slab
+// is fixed at creation (use_slab) and never grows.
 class Arena {
  public:
   ~Arena() {
@@ -57,24 +64,28 @@ class Arena {
     if (slab_) cudaFree(slab_);
   }
   void use_slab(size_t bytes) {
-    release();
-    if (slab_) cudaFree(slab_);
-    slab_ = nullptr;
-    const cudaError_t e = cudaMalloc(&slab_, bytes);
-    if (e != cudaSuccess) {
-      cudaGetLastError();
-      slab_ = nullptr;
-      throw CudaError(e, "cudaMalloc (slab)");
-    }
-    slab_size_ = bytes;
+    set_slab(bytes);
+    growable_ = false;
   }
+  // Make room for an upload of about `bytes` and reset the bump pointer.
+  void reserve(size_t bytes) {
+    release();
+    if (slab_ && slab_size_ >= bytes) return;
+    if (!growable_) throw CudaError(cudaErrorMemoryAllocation, "request exceeds the slot's memory");
+    set_slab(bytes);
+  }
+  bool growable() const { return growable_; }
+  size_t capacity() const { return slab_size_; }
   template <typename T>
   T* alloc(size_t count) {
     if (count == 0) count = 1;
     const size_t need = count * sizeof(T);
     if (slab_) {
       const size_t off = (slab_used_ + 255) / 256 * 256;
-      if (off + need > slab_size_) throw CudaError(cudaErrorMemoryAllocation, "slab exhausted");
+      if (off + need > slab_size_) {
+        if (growable_) throw SlabFull(off + need);
+        throw CudaError(cudaErrorMemoryAllocation, "slab exhausted");
+      }
       slab_used_ = off + need;
       bytes_ += need;
       return reinterpret_cast<T*>(static_cast<char*>(slab_) + off);
@@ -104,10 +115,24 @@ class Arena {
   size_t bytes() const { return bytes_; }
 
  private:
+  void set_slab(size_t bytes) {
+    release();
+    if (slab_) cudaFree(slab_);
+    slab_ = nullptr;
+    slab_size_ = 0;
+    const cudaError_t e = cudaMalloc(&slab_, bytes);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      slab_ = nullptr;
+      throw CudaError(e, "cudaMalloc (slab)");
+    }
+    slab_size_ = bytes;
+  }
   std::vector<void*> ptrs_;
   size_t bytes_ = 0;
   void* slab_ = nullptr;
   size_t slab_size_ = 0, slab_used_ = 0;
+  bool growable_ = true;
 };
 
 // Serialises the persistent PCG kernels of several contexts sharing a GPU
@@ -154,7 +179,7 @@ void drop_graph(Context* c) {
 }
 
 // Upload a built plan: allocate and fill every device array of Dev.
-void upload_plan(Context* c, uint32_t max_records) {
+void upload_plan_once(Context* c, uint32_t max_records) {
   Plan& P = c->plan;
   cudaStream_t s = c->stream;
   drop_graph(c);  // its kernels hold the old device pointers
@@ -281,6 +306,19 @@ void upload_plan(Context* c, uint32_t max_records) {
     throw Status(VLBA_ERR_CUDA, "the PCG kernel cannot be made co-resident on this device");
   VLBA_CUDA(cudaStreamSynchronize(s));
   c->uploaded = true;
+}
+
+void upload_plan(Context* c, uint32_t max_records) {
+  const size_t est = c->plan.device_bytes() + (size_t)max_records * sizeof(vlba_iteration) *
+                                                   c->plan.num_problems + (4u << 20);
+  if (c->arena.growable()) c->arena.reserve(std::max(est, c->arena.capacity()));
+  try {
+    upload_plan_once(c, max_records);
+  } catch (const SlabFull& f) {
+    // The estimate was short: one retry on a slab with room to spare.
+    c->arena.reserve(std::max(2 * c->arena.capacity(), f.need + f.need / 2));
+    upload_plan_once(c, max_records);
+  }
 }
 
 // Reset the state to the uploaded initial values and the LM control words.
@@ -1108,6 +1146,7 @@ struct Server {
   uint32_t max_batch = 64;
   size_t slot_bytes = 0;
   uint64_t large_obs = 100000;
+  uint32_t plan_threads = 1;  // host threads per planner for one large plan
   std::vector<Context*> slots;
   PcgGate gate;
   std::mutex mu;
@@ -1138,7 +1177,7 @@ void plan_ticket(Server* S, Ticket* t) {
   try {
     const vlba_problem* ps[1] = {t->problem};
     const vlba_config* cs[1] = {&t->config};
-    build_plan(ps, cs, 1, (uint32_t)pick_tb(ps, 1), &t->plan);
+    build_plan(ps, cs, 1, (uint32_t)pick_tb(ps, 1), &t->plan, S->plan_threads);
     const std::string bad = check_plan(t->plan);
     if (!bad.empty()) throw Status(VLBA_ERR_INVALID_ARGUMENT, bad);
     t->bytes = ticket_bytes(t->plan, t->config.max_iterations);
@@ -1330,6 +1369,7 @@ void* visloc_ba_cuda_server_create(int device, uint32_t slots, uint64_t memory_b
     }
     const uint32_t planners =
         std::max(1u, std::min(8u, std::thread::hardware_concurrency() / 2));
+    S->plan_threads = std::max(1u, std::thread::hardware_concurrency() / planners);
     for (uint32_t i = 0; i < planners; ++i) S->threads.emplace_back(vlba::planner_loop, S);
     for (uint32_t k = 0; k < slots; ++k) S->threads.emplace_back(vlba::worker_loop, S, k);
   } catch (...) {
