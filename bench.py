@@ -104,10 +104,15 @@ def make_workload(name: str, rank: int):
 
 # ------------------------------------------------------------- distributed
 class Dist:
-    def __init__(self):
+    """Replicas: one process per GPU, each solving its own problem; the
+    process group carries only the barrier and the max/sum of the timings
+    (NCCL on GPUs, gloo for the CPU tests)."""
+
+    def __init__(self, backend: str = "nccl"):
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.backend = backend
         self.pg = None
         if self.world > 1:
             import datetime
@@ -115,10 +120,16 @@ class Dist:
             import torch
             import torch.distributed as dist
 
-            torch.cuda.set_device(self.local)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                    device_id=torch.device("cuda", self.local))
+            if backend == "nccl":
+                torch.cuda.set_device(self.local)
+                dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                        device_id=torch.device("cuda", self.local))
+            else:
+                dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
             self.pg = dist
+
+    def _device(self):
+        return f"cuda:{self.local}" if self.backend == "nccl" else "cpu"
 
     def barrier(self):
         if self.pg:
@@ -129,7 +140,7 @@ class Dist:
             return v
         import torch
 
-        t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{self.local}")
+        t = torch.tensor([v], dtype=torch.float64, device=self._device())
         self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
         return float(t.item())
 
@@ -138,13 +149,20 @@ class Dist:
             return v
         import torch
 
-        t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{self.local}")
+        t = torch.tensor([v], dtype=torch.float64, device=self._device())
         self.pg.all_reduce(t, op=self.pg.ReduceOp.SUM)
         return float(t.item())
 
     def close(self):
         if self.pg:
             self.pg.destroy_process_group()
+
+
+def replica_rate(dist: Dist, units: float, seconds: float):
+    """Whole-job rate of replicas: the units of all ranks over the slowest
+    rank's time (weak scaling).  Returns (rate, max seconds)."""
+    t_max = dist.max(seconds)
+    return dist.sum(units) / t_max, t_max
 
 
 # ------------------------------------------------------------------ clocks
@@ -337,9 +355,7 @@ def run_ours(args, dist: Dist):
     pcg_iters = sum(it.pcg_iterations for r in results for it in r.iterations)
     pcg_ms = sum(it.pcg_ms for r in results for it in r.iterations)
     launches = sum(r.kernel_launches for r in results)
-    t_max = dist.max(dev_ms / 1e3)
-    lm_total = dist.sum(lm_iters)
-    value = lm_total / t_max
+    value, t_max = replica_rate(dist, lm_iters, dev_ms / 1e3)
     nobs = desc["observations"]
 
     # Roofline of the dominant kernel (k_pcg): algorithmic bytes per PCG

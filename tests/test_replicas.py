@@ -1,0 +1,61 @@
+"""The multi-GPU form of the bench is replicas only: every rank solves its
+own problem and the process group carries the barrier and the max/sum of the
+timings.  This runs that host logic on two CPU ranks over gloo, each rank
+solving a different problem with the FP64 oracle."""
+
+from __future__ import annotations
+
+import os
+import socket
+import sys
+
+import pytest
+import torch.multiprocessing as mp
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _free_port() -> int:
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank(rank: int, world: int, port: int, out):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank),
+                      WORLD_SIZE=str(world), LOCAL_RANK=str(rank))
+    sys.path[:0] = [ROOT, os.path.join(ROOT, "visloc-rs_b200")]
+    import time
+
+    import bench
+    from oracle import oracle
+    from visloc_ba import BaConfig, RobustKernel, synth
+
+    dist = bench.Dist(backend="gloo")
+    p = synth.ring_problem(8, 200, seed=70 + rank)  # each replica its own problem
+    cfg = BaConfig(max_iterations=3 + rank, robust_kernel=RobustKernel.huber(1.0))
+    dist.barrier()
+    t0 = time.perf_counter()
+    st, res = oracle.optimize(p, cfg, threads=1)
+    dt = time.perf_counter() - t0 + 0.05 * rank  # ranks of different speed
+    dist.barrier()
+    rate, t_max = bench.replica_rate(dist, len(res.iterations), dt)
+    out.put((rank, st, len(res.iterations), dt, rate, t_max))
+    dist.close()
+
+
+def test_two_replicas_aggregate_over_gloo():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    rows = sorted(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    (_, st0, it0, dt0, rate0, tmax0), (_, st1, it1, dt1, rate1, tmax1) = rows
+    assert st0 == 0 and st1 == 0
+    assert tmax0 == tmax1 == pytest.approx(max(dt0, dt1))
+    assert rate0 == rate1 == pytest.approx((it0 + it1) / max(dt0, dt1))
