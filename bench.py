@@ -77,7 +77,7 @@ def make_workload(name: str, rank: int):
     if name == "ring-4m":
         problem = synth.large_ring_problem(seed=2000 + rank)
         cfg = BaConfig(max_iterations=30, robust_kernel=RobustKernel.huber(1.0),
-                       max_pcg_iterations=200, pcg_relative_tolerance=1e-6)
+                       max_pcg_iterations=200, pcg_relative_tolerance=1e-6, autotune=True)
         desc = {"workload": "ring-4m", "cameras": 1200, "points": 500_000,
                 "observations": int(problem.num_observations), "image": "6000x4000",
                 "lm_iterations": 30, "pcg_tolerance": 1e-6, "robust": "huber(1px)",
@@ -85,13 +85,14 @@ def make_workload(name: str, rank: int):
     elif name == "windows-512":
         problem = synth.window_batch(512, seed=4000 + 1000 * rank)
         cfg = BaConfig(max_iterations=10, robust_kernel=RobustKernel.huber(1.0),
-                       max_pcg_iterations=200, pcg_relative_tolerance=1e-6, graph=True)
+                       max_pcg_iterations=200, pcg_relative_tolerance=1e-6, graph=True,
+                       autotune=True)
         desc = {"workload": "windows-512", "windows": 512,
                 "keyframes": "U{5..40} stereo (baseline 0.11 m)", "image": "752x480",
                 "points": int(sum(p.num_landmarks for p in problem)),
                 "observations": int(sum(p.num_observations for p in problem)),
                 "lm_iterations": 10, "pcg_tolerance": 1e-6, "robust": "huber(1px)",
-                "fixed_poses": "10%", "cuda_graph": True}
+                "fixed_poses": "10%", "cuda_graph": True, "autotuned_launch_shape": True}
     else:
         problem = synth.ring_problem(50, 5000, seed=1001 + rank)
         cfg = BaConfig(max_iterations=20, robust_kernel=RobustKernel.huber(1.0),

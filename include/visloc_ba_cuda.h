@@ -157,6 +157,11 @@ typedef struct vlba_config {
  * has finished cost only their launches).  Ignored with VLBA_FLAG_PROFILE. */
 #define VLBA_FLAG_GRAPH 2u
 
+/* Before the first solve of an upload, choose the launch shape (see
+ * visloc_ba_cuda_autotune) unless one was tuned for a system of this shape
+ * earlier in the process. */
+#define VLBA_FLAG_AUTOTUNE 4u
+
 /* ------------------------------------------------------------------ result */
 /* BaIterationStats (bundle/mod.rs:755-763) plus solver diagnostics. */
 typedef struct vlba_iteration {
@@ -303,6 +308,27 @@ int visloc_ba_cuda_batch_solve_uploaded(void* ctx, vlba_result* results,
                                         vlba_iteration* iterations,
                                         uint32_t iterations_capacity);
 int visloc_ba_cuda_batch_download(void* ctx, uint32_t n, vlba_problem* const* problems);
+
+/* --------------------------------------------------------------- autotuner */
+/* Launch shape of the uploaded system: the blocks of the persistent PCG
+ * kernel and the share of the L2 that keeps tiles of S resident across PCG
+ * iterations.  Neither changes any result (every sum's order is fixed by the
+ * problem's layout), only the time.  visloc_ba_cuda_autotune times a fixed
+ * number of PCG iterations for candidate shapes on the system assembled at the
+ * uploaded state, applies the fastest and caches it for systems of the same
+ * shape (tiles, tile rows and problems, by powers of two) for the process;
+ * visloc_ba_cuda_set_launch_shape forces one (pcg_blocks 0: the largest
+ * co-resident grid).  No counterpart in the reference (its shader workgroup
+ * sizes are fixed). */
+typedef struct vlba_launch_shape {
+  int32_t pcg_blocks;
+  int32_t reserved;
+  double l2_resident_fraction;
+  double pcg_iteration_us;   /* measured by the autotuner (0 when forced) */
+} vlba_launch_shape;
+
+int visloc_ba_cuda_autotune(void* ctx, vlba_launch_shape* chosen);
+int visloc_ba_cuda_set_launch_shape(void* ctx, const vlba_launch_shape* shape);
 
 /* ----------------------------------------------------------------- serving */
 /* A request loop on one GPU for streams of independent solves (localisation

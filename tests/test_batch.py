@@ -144,3 +144,29 @@ def test_single_problem_graph_mode(solver):
     assert ra.final_cost == rb.final_cost
     assert same_state(a, b)
     assert rb.kernel_launches >= ra.kernel_launches  # finished iterations still launch
+
+
+def test_launch_shapes_do_not_change_results(solver):
+    """The autotuner's choices (PCG blocks, L2-resident share of S) leave
+    every bit of the result as it is."""
+    probs = mixed_problems()
+    c = cfg()
+    outs = []
+    for blocks, l2 in ((0, 0.5), (3, 0.0), (17, 0.9)):
+        solver.batch_upload([p.copy() for p in probs], c)
+        solver.set_launch_shape(blocks, l2)
+        res = solver.batch_solve_uploaded()
+        out = [p.copy() for p in probs]
+        solver.batch_download(out)
+        outs.append((res, out))
+    (r0, o0) = outs[0]
+    for r, o in outs[1:]:
+        for a, b, pa, pb in zip(r0, r, o0, o):
+            assert a.final_cost == b.final_cost
+            assert same_state(pa, pb)
+    solver.batch_upload([p.copy() for p in probs], c)
+    shape = solver.autotune()
+    assert shape["pcg_blocks"] >= 1 and shape["pcg_iteration_us"] > 0.0
+    res = solver.batch_solve_uploaded()
+    for a, b in zip(r0, res):
+        assert a.final_cost == b.final_cost

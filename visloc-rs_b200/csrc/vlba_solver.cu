@@ -16,6 +16,8 @@
 #include <cstring>
 #include <condition_variable>
 #include <deque>
+#include <map>
+#include <tuple>
 #include <memory>
 #include <mutex>
 #include <stdexcept>
@@ -166,6 +168,7 @@ struct Context {
   cudaGraphExec_t graph = nullptr;
   uint32_t graph_iters = 0;
   PcgGate* gate = nullptr;  // set for the slots of a server
+  bool tuned = false;       // the launch shape of this upload has been chosen
 };
 
 namespace {
@@ -176,6 +179,66 @@ void drop_graph(Context* c) {
   if (c->graph) cudaGraphExecDestroy(c->graph);
   c->graph = nullptr;
   c->graph_iters = 0;
+}
+
+// L2-resident share of S: the leading tiles up to a fraction of the L2.
+uint32_t l2_tiles(const Context* c, double frac) {
+  const double tile_bytes = (double)c->plan.tb * c->plan.tb * kBlock * 4.0;
+  return (uint32_t)std::min<double>((double)c->plan.tile_ij.size(),
+                                    frac * (double)c->l2_bytes / tile_bytes);
+}
+
+// ---------------------------------------------------------------- autotuner
+// Launch shapes that leave every result bit for bit the same (the PCG's
+// blocks and the L2-resident share of S: every sum's order is fixed by the
+// plan, not by which block or warp computes it), chosen by timing a fixed
+// number of PCG iterations on the uploaded system and cached per system
+// shape for the process.  The tile size and the assembly's lane count set
+// summation orders, so they are not tuned: a problem must solve the same
+// alone and in any batch.
+struct ShapeKey {
+  uint32_t tiles, rows, problems;
+  bool operator<(const ShapeKey& o) const {
+    return std::tie(tiles, rows, problems) < std::tie(o.tiles, o.rows, o.problems);
+  }
+};
+struct LaunchShape {
+  int pcg_grid = 0;
+  double l2_fraction = 0.5;
+  double pcg_iteration_us = 0.0;
+};
+std::mutex g_tune_mu;
+std::map<ShapeKey, LaunchShape> g_tune_cache;
+
+uint32_t log2_bucket(uint64_t v) {
+  uint32_t b = 0;
+  while (v > 1) {
+    v >>= 1;
+    ++b;
+  }
+  return b;
+}
+
+ShapeKey shape_key(const Plan& P) {
+  return ShapeKey{log2_bucket(P.tile_ij.size()), log2_bucket(P.num_tile_rows),
+                  log2_bucket(P.num_problems)};
+}
+
+int pcg_grid_max(const Context* c) {
+  const Plan& P = c->plan;
+  const int g = P.num_tile_rows ? pcg_grid_size((int)P.tb, c->sm_count) : 0;
+  return std::min<int>(g, (int)std::max<size_t>(P.tile_ij.size(), P.num_tile_rows));
+}
+
+int pcg_grid_min(const Context* c) {
+  const int per = pcg_rows_per_block();
+  return (int)((c->plan.num_tile_rows + per - 1) / per);
+}
+
+void apply_shape(Context* c, const LaunchShape& sh) {
+  const int gmax = pcg_grid_max(c), gmin = std::max(1, pcg_grid_min(c));
+  if (gmax > 0) c->pcg_grid = std::max(gmin, std::min(gmax, sh.pcg_grid > 0 ? sh.pcg_grid : gmax));
+  c->dev.l2_resident_tiles = l2_tiles(c, std::max(0.0, std::min(1.0, sh.l2_fraction)));
 }
 
 // Upload a built plan: allocate and fill every device array of Dev.
@@ -271,13 +334,7 @@ void upload_plan_once(Context* c, uint32_t max_records) {
   d.dots = A.alloc<double>(9 * (size_t)(P.num_tile_rows ? P.num_tile_rows : 1));
   d.row_cnt = A.alloc<unsigned int>(P.num_tile_rows ? P.num_tile_rows : 1);
   VLBA_CUDA(cudaMemsetAsync(d.row_cnt, 0, 4 * (size_t)(P.num_tile_rows ? P.num_tile_rows : 1), s));
-  {
-    // L2-resident share of S: the leading tiles up to a fraction of the L2.
-    const double frac = c->l2_fraction;
-    const double budget = frac * (double)c->l2_bytes;
-    const double tile_bytes = (double)tile_floats * 4.0;
-    d.l2_resident_tiles = (uint32_t)std::min<double>((double)P.tile_ij.size(), budget / tile_bytes);
-  }
+  d.l2_resident_tiles = l2_tiles(c, c->l2_fraction);
   d.trace = nullptr;
   if (std::getenv("VLBA_TRACE_PCG") && c->pcg_grid_hint > 0)
     d.trace = A.alloc<unsigned long long>((size_t)kTraceIters * c->pcg_grid_hint *
@@ -301,9 +358,19 @@ void upload_plan_once(Context* c, uint32_t max_records) {
     throw Status(VLBA_ERR_INVALID_ARGUMENT,
                  "reduced system too large: more than " + std::to_string(pcg_rows_per_block()) +
                      " tile rows per PCG block");
-  if (d.trace && c->pcg_grid > c->pcg_grid_hint) d.trace = nullptr;  // sized for fewer blocks
   if (P.num_tile_rows && c->pcg_grid <= 0)
     throw Status(VLBA_ERR_CUDA, "the PCG kernel cannot be made co-resident on this device");
+  // A launch shape tuned earlier for a system of this shape.
+  c->tuned = false;
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    auto it = g_tune_cache.find(shape_key(P));
+    if (it != g_tune_cache.end()) {
+      apply_shape(c, it->second);
+      c->tuned = true;
+    }
+  }
+  if (c->dev.trace && c->pcg_grid > c->pcg_grid_hint) c->dev.trace = nullptr;  // sized for fewer blocks
   VLBA_CUDA(cudaStreamSynchronize(s));
   c->uploaded = true;
 }
@@ -496,7 +563,13 @@ RunStats run_lm_graph(Context* c, uint32_t max_iters) {
   return st;
 }
 
+LaunchShape autotune(Context* c);
+
 RunStats run_lm(Context* c, bool profile, PhaseTimes* pt) {
+  if ((c->flags & VLBA_FLAG_AUTOTUNE) && !c->tuned) {
+    autotune(c);
+    reset_state(c);
+  }
   Dev& d = c->dev;
   cudaStream_t s = c->stream;
   uint32_t max_iters = 0;
@@ -535,6 +608,76 @@ RunStats run_lm(Context* c, bool profile, PhaseTimes* pt) {
   VLBA_CUDA(cudaEventElapsedTime(&ms, c->ev[0], c->ev[5]));
   st.device_ms = ms;
   return st;
+}
+
+// Times kIters PCG iterations (tolerance 0) on the system assembled at the
+// uploaded initial state for each candidate shape; keeps the fastest.
+LaunchShape autotune(Context* c) {
+  constexpr uint32_t kIters = 16;
+  Dev& d = c->dev;
+  Plan& P = c->plan;
+  cudaStream_t s = c->stream;
+  LaunchShape best;
+  best.pcg_grid = c->pcg_grid;
+  best.l2_fraction = c->l2_fraction;
+  if (!d.num_tile_rows) {
+    c->tuned = true;
+    return best;
+  }
+  std::vector<LmParams> tmp = P.params;
+  for (LmParams& lp : tmp) {
+    lp.pcg_relative_tolerance = 0.0;
+    lp.max_pcg_iterations = kIters;
+  }
+  VLBA_CUDA(cudaMemcpyAsync(const_cast<LmParams*>(d.params), tmp.data(), tmp.size() * sizeof(LmParams),
+                            cudaMemcpyHostToDevice, s));
+  reset_state(c);
+  enqueue_initial(c);
+  check_launch(launch_linearize(d, s), "linearize");
+  check_launch(launch_point_prep(d, s), "point prep");
+  check_launch(launch_offdiag(d, s), "off-diagonal blocks");
+  check_launch(launch_cam_diag(d, s), "camera blocks");
+  const int gmax = pcg_grid_max(c), gmin = std::max(1, pcg_grid_min(c));
+  std::vector<int> grids;
+  for (double f : {1.0, 0.75, 0.5, 0.375, 0.25, 0.125}) {
+    const int g = std::max(gmin, (int)(f * gmax));
+    if (std::find(grids.begin(), grids.end(), g) == grids.end()) grids.push_back(g);
+  }
+  double best_ms = 1e30;
+  for (int g : grids)
+    for (double frac : {0.5, 0.0, 0.9}) {
+      LaunchShape sh;
+      sh.pcg_grid = g;
+      sh.l2_fraction = frac;
+      apply_shape(c, sh);
+      float ms = 1e30f;
+      for (int rep = 0; rep < 3; ++rep) {
+        VLBA_CUDA(cudaEventRecord(c->ev[0], s));
+        check_launch(launch_pcg_setup(d, s), "pcg setup");
+        check_launch(launch_pcg(d, c->pcg_grid, s), "pcg");
+        VLBA_CUDA(cudaEventRecord(c->ev[1], s));
+        VLBA_CUDA(cudaEventSynchronize(c->ev[1]));
+        float t = 0.f;
+        VLBA_CUDA(cudaEventElapsedTime(&t, c->ev[0], c->ev[1]));
+        if (rep > 0) ms = std::min(ms, t);  // the first run warms the caches
+      }
+      if (ms < best_ms) {
+        best_ms = ms;
+        best = sh;
+      }
+    }
+  check_device_error(c);
+  VLBA_CUDA(cudaMemcpyAsync(const_cast<LmParams*>(d.params), P.params.data(),
+                            P.params.size() * sizeof(LmParams), cudaMemcpyHostToDevice, s));
+  VLBA_CUDA(cudaStreamSynchronize(s));
+  best.pcg_iteration_us = 1e3 * best_ms / kIters;
+  apply_shape(c, best);
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tune_cache[shape_key(P)] = best;
+  }
+  c->tuned = true;
+  return best;
 }
 
 void fill_result(Context* c, uint32_t prob, vlba_result* res, vlba_iteration* its, uint32_t cap,
@@ -1438,6 +1581,39 @@ int visloc_ba_cuda_server_wait(void* server, uint64_t ticket, double timeout_ms,
   if (st != VLBA_OK) S->error = t->error;
   S->tickets.erase(it);
   return st;
+}
+
+int visloc_ba_cuda_autotune(void* ctx, vlba_launch_shape* chosen) {
+  auto* c = static_cast<Context*>(ctx);
+  if (!c) return VLBA_ERR_INVALID_ARGUMENT;
+  return vlba::guarded(c, [&] {
+    if (!c->uploaded) throw vlba::Status(VLBA_ERR_INVALID_ARGUMENT, "nothing uploaded");
+    vlba::set_device(c);
+    {  // a new measurement, not the cached shape
+      std::lock_guard<std::mutex> lock(vlba::g_tune_mu);
+      vlba::g_tune_cache.erase(vlba::shape_key(c->plan));
+    }
+    const vlba::LaunchShape sh = vlba::autotune(c);
+    if (chosen) {
+      std::memset(chosen, 0, sizeof *chosen);
+      chosen->pcg_blocks = c->pcg_grid;
+      chosen->l2_resident_fraction = sh.l2_fraction;
+      chosen->pcg_iteration_us = sh.pcg_iteration_us;
+    }
+  });
+}
+
+int visloc_ba_cuda_set_launch_shape(void* ctx, const vlba_launch_shape* shape) {
+  auto* c = static_cast<Context*>(ctx);
+  if (!c || !shape) return VLBA_ERR_INVALID_ARGUMENT;
+  return vlba::guarded(c, [&] {
+    if (!c->uploaded) throw vlba::Status(VLBA_ERR_INVALID_ARGUMENT, "nothing uploaded");
+    vlba::LaunchShape sh;
+    sh.pcg_grid = shape->pcg_blocks;
+    sh.l2_fraction = shape->l2_resident_fraction;
+    vlba::apply_shape(c, sh);
+    c->tuned = true;
+  });
 }
 
 const char* visloc_ba_cuda_server_last_error(void* server) {

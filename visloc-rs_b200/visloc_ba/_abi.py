@@ -62,6 +62,7 @@ KERNEL_CAUCHY = 2
 
 FLAG_PROFILE = 1
 FLAG_GRAPH = 2
+FLAG_AUTOTUNE = 4
 
 
 class Camera(C.Structure):
@@ -169,6 +170,15 @@ class PlanInfo(C.Structure):
 
 P = C.POINTER
 # name -> (restype, argtypes): every symbol include/visloc_ba_cuda.h declares.
+class LaunchShape(C.Structure):
+    _fields_ = [
+        ("pcg_blocks", C.c_int32),
+        ("reserved", C.c_int32),
+        ("l2_resident_fraction", C.c_double),
+        ("pcg_iteration_us", C.c_double),
+    ]
+
+
 class TicketInfo(C.Structure):
     _fields_ = [
         ("latency_ms", C.c_double),
@@ -222,6 +232,8 @@ SOLVER_EXPORTS = {
         C.c_int, [C.c_void_p, P(Result), P(Iteration), C.c_uint32],
     ),
     "visloc_ba_cuda_batch_download": (C.c_int, [C.c_void_p, C.c_uint32, P(P(Problem))]),
+    "visloc_ba_cuda_autotune": (C.c_int, [C.c_void_p, P(LaunchShape)]),
+    "visloc_ba_cuda_set_launch_shape": (C.c_int, [C.c_void_p, P(LaunchShape)]),
     "visloc_ba_cuda_server_create": (C.c_void_p, [C.c_int, C.c_uint32, C.c_uint64, C.c_uint32]),
     "visloc_ba_cuda_server_destroy": (None, [C.c_void_p]),
     "visloc_ba_cuda_server_submit": (

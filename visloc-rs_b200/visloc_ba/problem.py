@@ -242,6 +242,8 @@ class BaConfig:
     profile: bool = False
     # Run the LM loop as one captured CUDA graph (VLBA_FLAG_GRAPH).
     graph: bool = False
+    # Choose the launch shape before the first solve of an upload.
+    autotune: bool = False
 
     def to_abi(self) -> _abi.Config:
         c = _abi.Config()
@@ -262,7 +264,8 @@ class BaConfig:
         c.robust_parameter = float(self.robust_kernel.parameter)
         c.max_pcg_iterations = int(self.max_pcg_iterations)
         c.pcg_relative_tolerance = float(self.pcg_relative_tolerance)
-        c.flags = (_abi.FLAG_PROFILE if self.profile else 0) | (_abi.FLAG_GRAPH if self.graph else 0)
+        c.flags = ((_abi.FLAG_PROFILE if self.profile else 0) | (_abi.FLAG_GRAPH if self.graph else 0)
+                   | (_abi.FLAG_AUTOTUNE if self.autotune else 0))
         return c
 
 

@@ -108,6 +108,23 @@ class CudaSolver:
     def download(self, packed: PackedProblem) -> int:
         return self.lib.visloc_ba_cuda_download(self.ctx, C.byref(packed.abi()))
 
+    # ---------------------------------------------------------- autotuner
+    def autotune(self) -> dict:
+        """Time candidate launch shapes on the uploaded system; apply and
+        return the fastest."""
+        sh = _abi.LaunchShape()
+        st = self.lib.visloc_ba_cuda_autotune(self.ctx, C.byref(sh))
+        if st != _abi.OK:
+            raise SolverError(st, self.last_error())
+        return {"pcg_blocks": sh.pcg_blocks, "l2_resident_fraction": sh.l2_resident_fraction,
+                "pcg_iteration_us": sh.pcg_iteration_us}
+
+    def set_launch_shape(self, pcg_blocks: int, l2_resident_fraction: float) -> None:
+        sh = _abi.LaunchShape(int(pcg_blocks), 0, float(l2_resident_fraction), 0.0)
+        st = self.lib.visloc_ba_cuda_set_launch_shape(self.ctx, C.byref(sh))
+        if st != _abi.OK:
+            raise SolverError(st, self.last_error())
+
     # ------------------------------------------------------------ batches
     def _batch_arrays(self, problems, configs):
         n = len(problems)
