@@ -1145,7 +1145,6 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
   __shared__ uint32_t sc_prob;
   __shared__ int sc_k;
   __shared__ unsigned int s_flag;
-  __shared__ double s_alpha;
 
   const uint32_t G = gridDim.x;
   const uint32_t TW = G * NW;  // warps in the grid
@@ -1198,6 +1197,7 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
   // problem, constant for the launch.  The owner alone writes its rows' p, z,
   // x and r, so their shared-memory copies stay current for the whole solve.
   constexpr int kOwn = C::kOwnMax;
+  constexpr uint32_t kBigRow = 32;  // rows of this many tiles reduce over the whole block
   constexpr int kOP = 0, kOZ = C::kRow, kOQ = 2 * C::kRow, kOX = 3 * C::kRow, kOR = 4 * C::kRow,
                 kOM = 5 * C::kRow;
   __shared__ uint32_t own_m0[kOwn], own_m1[kOwn], own_prob[kOwn];
@@ -1267,50 +1267,57 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
     }
   };
 
+  // Row-local steps run one warp per owned row (row j on warp j mod NW),
+  // entries e = lane and lane + 32 of the row's kRow, with the warp's segment
+  // buffer as scratch; their dots are butterflies over the warp.
+  static_assert(C::kRow > 32 && C::kRow <= 64, "two entries per lane");
+  const bool e1 = lane + 32u < (uint32_t)C::kRow;  // this lane has a second entry
+  float* const sPI = wPI;  // warp scratch of kRow floats (init / C)
+
   // ---- init: x = 0, r = b, z = M^-1 r, p = z; dots rz, b2 of "iteration -1".
-  float* const sPI = colw;  // block scratch of kRow floats for init / C
-  for (uint32_t j = 0; j < nown; ++j) {
+  for (uint32_t j = warp; j < nown; j += NW) {
     const uint32_t tr = blockIdx.x + j * G;
     const uint32_t P = d.tr_prob[tr];
     if (!*(volatile uint32_t*)&d.pcg[P].active) continue;
     const size_t base = (size_t)tr * C::kRow;
     float* o = ownrow(j);
-    if (tid < (uint32_t)C::kRow) {
-      const float b = d.rhs[base + tid];
-      d.x[base + tid] = 0.0f;
-      d.r[base + tid] = b;
-      o[kOX + tid] = 0.0f;
-      o[kOR + tid] = b;
-      sPI[tid] = b;
+    for (uint32_t e = lane; e < (uint32_t)C::kRow; e += 32) {
+      const float b = d.rhs[base + e];
+      d.x[base + e] = 0.0f;
+      d.r[base + e] = b;
+      o[kOX + e] = 0.0f;
+      o[kOR + e] = b;
+      sPI[e] = b;
     }
-    __syncthreads();
+    __syncwarp();
     double rz = 0.0, bb = 0.0;
-    if (tid < (uint32_t)C::kRow) {
-      const uint32_t cam = tid / 6, a = tid % 6;
+    for (uint32_t e = lane; e < (uint32_t)C::kRow; e += 32) {
+      const uint32_t cam = e / 6, a = e % 6;
       const float* m = d.minv + 36 * (base / 6 + cam) + a * 6;
       float z = 0.0f;
 #pragma unroll
       for (int b = 0; b < 6; ++b) {
         const float mb = m[b];
-        o[kOM + tid * 6 + b] = mb;
+        o[kOM + e * 6 + b] = mb;
         z += mb * sPI[cam * 6 + b];
       }
-      d.z[base + tid] = z;
-      d.p[base + tid] = z;
-      o[kOZ + tid] = z;
-      o[kOP + tid] = z;
-      rz = (double)sPI[tid] * (double)z;
-      bb = (double)sPI[tid] * (double)sPI[tid];
+      d.z[base + e] = z;
+      d.p[base + e] = z;
+      o[kOZ + e] = z;
+      o[kOP + e] = z;
+      rz += (double)sPI[e] * (double)z;
+      bb += (double)sPI[e] * (double)sPI[e];
     }
-    rz = block_sum_fast<NW>(rz, red);
-    bb = block_sum_fast<NW>(bb, red);
-    if (tid == 0) {
+    rz = warp_sum(rz);
+    bb = warp_sum(bb);
+    if (lane == 0) {
       *dot_at(d, kDotRz + mod3(-1), tr) = rz;
       *dot_at(d, kDotRr + mod3(-1), tr) = bb;
       *dot_at(d, kDotPq + 1, tr) = 1.0;
       *dot_at(d, kDotB2, tr) = bb;
       d.row_cnt[tr] = 0u;
     }
+    __syncwarp();
   }
   // The metadata of the warp's first two tiles (the same every iteration).
   const uint4 meta0 = Mw > 0 ? d.tile_meta[gw] : make_uint4(0u, 0u, 0u, 0u);
@@ -1322,23 +1329,26 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
 
   for (int k = 0; ok; ++k) {
     trace_mark(d, k, 0);
-    // ---- A: status of the problems this block owns, then the warps' tiles.
-    for (uint32_t tr = blockIdx.x; tr < d.num_tile_rows; tr += G) {
-      const uint32_t P = d.tr_prob[tr];
+    // ---- A: status of the problems whose first tile row this block owns
+    // (by that row's warp), then the warps' tiles.
+    for (uint32_t j = warp; j < nown; j += NW) {
+      const uint32_t tr = blockIdx.x + j * G;
+      const uint32_t P = own_prob[j];
       if (d.prob_tr_begin[P] != tr) continue;  // owner = first tile row
       if (!*(volatile uint32_t*)&d.pcg[P].active) continue;
-      scal(P, k);
-      if (!sc.active && tid == 0) {
+      const ProbScal ps = prob_scalars_warp(d, P, k);
+      if (!ps.active && lane == 0) {
         PcgState& st = d.pcg[P];
-        st.iters = sc.iters;
-        st.status = (uint32_t)sc.status;
-        st.bnorm = sc.bnorm;
-        st.rnorm = sqrt(sc.rr);
-        st.rz = sc.rz;
+        st.iters = ps.iters;
+        st.status = (uint32_t)ps.status;
+        st.bnorm = ps.bnorm;
+        st.rnorm = sqrt(ps.rr);
+        st.rz = ps.rz;
         __threadfence();
         st.active = 0u;
         atomicSub(d.barrier + 2, 1u);
       }
+      __syncwarp();
     }
     // The block computes the scalars of its first tile's problem once; warps
     // whose tile is of that problem read them from shared memory.
@@ -1509,24 +1519,89 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
       }
     }
     // Row reductions by their owners: wait, bounded, for every tile of the
-    // row to arrive, then reduce.
-    for (uint32_t j = 0; j < nown; ++j) {
+    // row to arrive, then reduce -- a row of many tiles by the whole block
+    // (its slots spread over the warps), the others one warp per row.
+    auto wait_row = [&](uint32_t j) {  // one thread
+      const uint32_t need = own_m1[j] - own_m0[j];
       const uint32_t R = blockIdx.x + j * G;
+      uint32_t spins = 0;
+      while (ld_acquire(d.row_cnt + R) < need) {
+        if (++spins > kSpinLimit) {
+          atomicOr(d.error, (unsigned int)kErrBarrierTimeout);
+          break;
+        }
+        __nanosleep(8);
+      }
+    };
+    for (uint32_t j = 0; j < nown; ++j) {
+      if (own_m1[j] - own_m0[j] < kBigRow) continue;
       scal(own_prob[j], k);
       if (!sc.active) continue;
-      if (tid == 0) {
-        const uint32_t need = own_m1[j] - own_m0[j];
-        uint32_t spins = 0;
-        while (ld_acquire(d.row_cnt + R) < need) {
-          if (++spins > kSpinLimit) {
-            atomicOr(d.error, (unsigned int)kErrBarrierTimeout);
-            break;
-          }
-          __nanosleep(8);
-        }
-      }
+      if (tid == 0) wait_row(j);
       __syncthreads();
       reduce_row((int)j, k, sc.beta);
+    }
+    uint32_t oprob = kNone;
+    ProbScal os;
+    os.active = 0;
+    os.beta = 0.0;
+    for (uint32_t j = warp; j < nown; j += NW) {
+      if (own_m1[j] - own_m0[j] >= kBigRow) continue;
+      const uint32_t P = own_prob[j];
+      if (P != oprob) {
+        os = prob_scalars_warp(d, P, k);
+        oprob = P;
+      }
+      if (!os.active) continue;
+      if (lane == 0) wait_row(j);
+      __syncwarp();
+      // Slots in order, eight loads in flight per lane.
+      const uint32_t R = blockIdx.x + j * G;
+      const uint32_t m0 = own_m0[j], m1 = own_m1[j];
+      float q0 = 0.0f, q1 = 0.0f;
+      for (uint32_t m = m0; m < m1; m += 8) {
+        float v0[8], v1[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          const uint32_t slot = m + u;
+          const float* src = d.partial + (size_t)slot * C::kRow;
+          v0[u] = slot < m1 ? __ldcg(src + lane) : 0.0f;
+          v1[u] = (slot < m1 && e1) ? __ldcg(src + 32 + lane) : 0.0f;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          q0 += v0[u];
+          q1 += v1[u];
+        }
+      }
+      float* o = ownrow(j);
+      const size_t at = (size_t)R * C::kRow;
+      double pq = 0.0;
+      {
+        float pv = o[kOP + lane];
+        if (k > 0) pv = __fmaf_rn((float)os.beta, pv, o[kOZ + lane]);
+        o[kOP + lane] = pv;
+        o[kOQ + lane] = q0;
+        d.p[at + lane] = pv;
+        d.q[at + lane] = q0;
+        pq = (double)pv * (double)q0;
+      }
+      if (e1) {
+        const uint32_t e = 32 + lane;
+        float pv = o[kOP + e];
+        if (k > 0) pv = __fmaf_rn((float)os.beta, pv, o[kOZ + e]);
+        o[kOP + e] = pv;
+        o[kOQ + e] = q1;
+        d.p[at + e] = pv;
+        d.q[at + e] = q1;
+        pq += (double)pv * (double)q1;
+      }
+      pq = warp_sum(pq);
+      if (lane == 0) {
+        *dot_at(d, kDotPq + (k & 1), R) = pq;
+        d.row_cnt[R] = 0u;  // every tile of row R has arrived this iteration
+      }
+      __syncwarp();
     }
     trace_mark(d, k, 2);
     ok = grid_barrier(d.barrier, G, d.error, &s_flag, bar_gen) && ok;
@@ -1534,57 +1609,54 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
     if (!ok) break;
     if (*(volatile unsigned int*)(d.barrier + 2) == 0u) break;  // every problem done
 
-    // ---- C: alpha = rz / p.q; x, r, z updates; partial r.z and r.r, from
-    // the operands the owner holds in registers.
+    // ---- C, one warp per owned row: alpha = rz / p.q of the row's
+    // problem; x, r, z updates; the row's r.z and r.r.
     uint32_t cprob = kNone;
-    for (uint32_t j = 0; j < nown; ++j) {
+    double alpha = 0.0;
+    for (uint32_t j = warp; j < nown; j += NW) {
       const uint32_t tr = blockIdx.x + j * G;
       const uint32_t P = own_prob[j];
-      scal(P, k);
-      if (!sc.active) continue;
-      if (cprob != P) {
-        if (tid < 32) {
-          double pq = 0.0;
-          for (uint32_t t2 = d.prob_tr_begin[P] + tid; t2 < d.prob_tr_begin[P + 1]; t2 += 32)
-            pq += __ldcg(dot_at(d, kDotPq + (k & 1), t2));
-          pq = warp_sum(pq);
-          if (tid == 0) s_alpha = (pq > 0.0 && isfinite(pq)) ? sc.rz / pq : 0.0;
-        }
-        __syncthreads();
+      if (P != cprob) {
+        const ProbScal ps = prob_scalars_warp(d, P, k);
+        double pq = 0.0;
+        for (uint32_t t2 = d.prob_tr_begin[P] + lane; t2 < d.prob_tr_begin[P + 1]; t2 += 32)
+          pq += __ldcg(dot_at(d, kDotPq + (k & 1), t2));
+        pq = warp_sum(pq);
+        alpha = (ps.active && pq > 0.0 && isfinite(pq)) ? ps.rz / pq : 0.0;
         cprob = P;
       }
-      const double alpha = s_alpha;
-      if (alpha == 0.0) continue;  // breakdown: x frozen, flagged at A(k+1)
+      if (alpha == 0.0) continue;  // inactive, or breakdown: x frozen, flagged at A(k+1)
       const size_t base = (size_t)tr * C::kRow;
       const float af = (float)alpha;
       float* o = ownrow(j);
-      if (tid < (uint32_t)C::kRow) {
-        const float xv = o[kOX + tid] + af * o[kOP + tid];
-        o[kOX + tid] = xv;
-        d.x[base + tid] = xv;
-        const float rv = o[kOR + tid] - af * o[kOQ + tid];
-        o[kOR + tid] = rv;
-        d.r[base + tid] = rv;
-        sPI[tid] = rv;
+      for (uint32_t e = lane; e < (uint32_t)C::kRow; e += 32) {
+        const float xv = o[kOX + e] + af * o[kOP + e];
+        o[kOX + e] = xv;
+        d.x[base + e] = xv;
+        const float rv = o[kOR + e] - af * o[kOQ + e];
+        o[kOR + e] = rv;
+        d.r[base + e] = rv;
+        sPI[e] = rv;
       }
-      __syncthreads();
+      __syncwarp();
       double rz = 0.0, rr = 0.0;
-      if (tid < (uint32_t)C::kRow) {
-        const uint32_t cam = tid / 6;
+      for (uint32_t e = lane; e < (uint32_t)C::kRow; e += 32) {
+        const uint32_t cam = e / 6;
         float z = 0.0f;
 #pragma unroll
-        for (int b = 0; b < 6; ++b) z += o[kOM + tid * 6 + b] * sPI[cam * 6 + b];
-        o[kOZ + tid] = z;
-        d.z[base + tid] = z;
-        rz = (double)sPI[tid] * (double)z;
-        rr = (double)sPI[tid] * (double)sPI[tid];
+        for (int b = 0; b < 6; ++b) z += o[kOM + e * 6 + b] * sPI[cam * 6 + b];
+        o[kOZ + e] = z;
+        d.z[base + e] = z;
+        rz += (double)sPI[e] * (double)z;
+        rr += (double)sPI[e] * (double)sPI[e];
       }
-      rz = block_sum_fast<NW>(rz, red);
-      rr = block_sum_fast<NW>(rr, red);
-      if (tid == 0) {
+      rz = warp_sum(rz);
+      rr = warp_sum(rr);
+      if (lane == 0) {
         *dot_at(d, kDotRz + mod3(k), tr) = rz;
         *dot_at(d, kDotRr + mod3(k), tr) = rr;
       }
+      __syncwarp();
     }
     trace_mark(d, k, 4);
     ok = grid_barrier(d.barrier, G, d.error, &s_flag, bar_gen);
@@ -1626,27 +1698,29 @@ __global__ void __launch_bounds__(256) k_state_to_front(Dev d) {
   }
 }
 
-__global__ void k_pcg_setup(Dev d) {
-  // Per-problem PCG state, grid-barrier words and the active count.
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    uint32_t active = 0;
-    for (uint32_t P = 0; P < d.num_problems; ++P) {
-      const bool on = !d.ctrl[P].done && d.prob_tr_begin[P + 1] > d.prob_tr_begin[P];
-      PcgState& s = d.pcg[P];
-      s.active = on ? 1u : 0u;
-      s.iters = 0u;
-      s.status = 0u;
-      s.rz = 0.0;
-      s.bnorm = 0.0;
-      s.rnorm = 0.0;
-      active += on ? 1u : 0u;
-    }
-    for (int w = 0; w < kBarrierWords; ++w) d.barrier[w] = 0u;
-    d.barrier[2] = active;
-    for (uint32_t tr = 0; tr < d.num_tile_rows; ++tr) d.row_cnt[tr] = 0u;
+__global__ void __launch_bounds__(1024) k_pcg_setup(Dev d) {
+  // Per-problem PCG state, grid-barrier words and the active count (one
+  // block; problems and rows strided over its threads).
+  __shared__ unsigned int active;
+  if (threadIdx.x == 0) active = 0u;
+  __syncthreads();
+  unsigned int mine = 0;
+  for (uint32_t P = threadIdx.x; P < d.num_problems; P += blockDim.x) {
+    const bool on = !d.ctrl[P].done && d.prob_tr_begin[P + 1] > d.prob_tr_begin[P];
+    PcgState& s = d.pcg[P];
+    s.active = on ? 1u : 0u;
+    s.iters = 0u;
+    s.status = 0u;
+    s.rz = 0.0;
+    s.bnorm = 0.0;
+    s.rnorm = 0.0;
+    mine += on ? 1u : 0u;
   }
+  if (mine) atomicAdd(&active, mine);
+  for (uint32_t tr = threadIdx.x; tr < d.num_tile_rows; tr += blockDim.x) d.row_cnt[tr] = 0u;
+  __syncthreads();
+  for (int w = threadIdx.x; w < kBarrierWords; w += blockDim.x) d.barrier[w] = w == 2 ? active : 0u;
 }
-
 
 }  // namespace
 
@@ -1718,7 +1792,7 @@ cudaError_t launch_pose_update(const Dev& d, cudaStream_t s) {
 }
 
 cudaError_t launch_pcg_setup(const Dev& d, cudaStream_t s) {
-  k_pcg_setup<<<1, 32, 0, s>>>(d);
+  k_pcg_setup<<<1, 1024, 0, s>>>(d);
   return cudaGetLastError();
 }
 
