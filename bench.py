@@ -63,7 +63,7 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="ring-4m",
-                    choices=["ring-4m", "ring-50", "windows-512", "served"])
+                    choices=["ring-4m", "ring-50", "street-20m", "windows-512", "served"])
     ap.add_argument("--requests", type=int, default=300, help="served: stream length")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -82,6 +82,15 @@ def make_workload(name: str, rank: int):
                 "observations": int(problem.num_observations), "image": "6000x4000",
                 "lm_iterations": 30, "pcg_tolerance": 1e-6, "robust": "huber(1px)",
                 "track_length": "geometric mean 8, [2,60]"}
+    elif name == "street-20m":
+        problem = synth.street_loop(seed=3000 + rank)
+        cfg = BaConfig(max_iterations=15, robust_kernel=RobustKernel.huber(1.0),
+                       max_pcg_iterations=200, pcg_relative_tolerance=1e-6, autotune=True)
+        desc = {"workload": "street-20m", "cameras": 5600, "points": int(problem.num_landmarks),
+                "observations": int(problem.num_observations), "image": "1920x1080",
+                "scene": "closed street loop, facade planes +-0.2 m",
+                "lm_iterations": 15, "pcg_tolerance": 1e-6, "robust": "huber(1px)",
+                "track_length": "consecutive views, geometric mean 6.7, [2,40]"}
     elif name == "windows-512":
         problem = synth.window_batch(512, seed=4000 + 1000 * rank)
         cfg = BaConfig(max_iterations=10, robust_kernel=RobustKernel.huber(1.0),
@@ -233,9 +242,18 @@ def traffic_per_pcg_iteration():
 
 # -------------------------------------------------------------- CPU side
 def cpu_sample(problem, cfg, threads=0):
-    """One LM iteration of the FP64 oracle on all host cores: seconds."""
+    """One LM iteration of the FP64 oracle on all host cores: (seconds,
+    fraction of the workload's observations it covered).  A problem too large
+    for the oracle's dense reduced solve (more than 2,000 poses) is sampled
+    as the sub-problem of a contiguous stretch of 700 of its poses."""
     from oracle import oracle
+    from visloc_ba import synth
 
+    frac = 1.0
+    if problem.num_poses > 2000:
+        sub = synth.sub_problem(problem, range(700))
+        frac = sub.num_observations / problem.num_observations
+        problem = sub
     c = problem.copy()
     one = type(cfg)(**{**cfg.__dict__, "max_iterations": 1})
     t0 = time.perf_counter()
@@ -243,7 +261,7 @@ def cpu_sample(problem, cfg, threads=0):
     dt = time.perf_counter() - t0
     if st != 0:
         raise RuntimeError(f"oracle failed: {st}")
-    return dt
+    return dt, frac
 
 
 def batch_cpu_sample(problems, cfg, windows=8):
@@ -294,9 +312,10 @@ def run_reference(args, dist: Dist):
         return
     for _ in range(args.warmup):  # a cost pass per warm-up step (page-in, threads)
         oracle.cost(problem, cfg)
-    times = [cpu_sample(problem, cfg) for _ in range(args.steps)]
-    total = sum(times)
-    value = args.steps / total
+    samples = [cpu_sample(problem, cfg) for _ in range(args.steps)]
+    frac = samples[0][1]
+    total = sum(t for t, _ in samples)
+    value = args.steps * frac / total  # LM iterations of the whole workload per second
     line = {
         "impl": "reference", "metric": "lm_iterations_per_s", "value": value,
         "unit": "LM iterations/s", "n_gpus": args.gpus, "steps": args.steps,
@@ -306,8 +325,11 @@ def run_reference(args, dist: Dist):
         "observations_per_s": value * desc["observations"],
         "cpu_baseline": {"value": value, "unit": "LM iterations/s", "cores": cores,
                          "kind": "port",
-                         "sample": "1 LM iteration (Schur + Cholesky, FP64) of the same "
-                                   "workload per step, all host cores"},
+                         "sample": "1 LM iteration (Schur + Cholesky, FP64) per step of the "
+                                   + ("same workload" if frac == 1.0 else
+                                      f"sub-problem of 700 consecutive poses ({frac:.3f} of the "
+                                      "observations; rate scaled by that share)")
+                                   + ", all host cores"},
         "e2e": {"value": value, "unit": "LM iterations/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -395,10 +417,13 @@ def run_ours(args, dist: Dist):
 
     cpu = None
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
-        dt = cpu_sample(problem, cfg)
-        cpu = {"value": 1.0 / dt, "unit": "LM iterations/s", "cores": os.cpu_count(),
+        dt, frac = cpu_sample(problem, cfg)
+        what = ("the same workload" if frac == 1.0 else
+                f"the sub-problem of 700 consecutive poses ({frac:.3f} of the observations; "
+                "rate scaled by that share)")
+        cpu = {"value": frac / dt, "unit": "LM iterations/s", "cores": os.cpu_count(),
                "kind": "port",
-               "sample": "1 LM iteration (FP64 Schur + Cholesky) of the same workload, "
+               "sample": f"1 LM iteration (FP64 Schur + Cholesky) of {what}, "
                          f"{os.cpu_count()} threads, {dt:.1f} s"}
 
     if dist.rank == 0:

@@ -111,9 +111,15 @@ def project_v(r, t, X, cam):
 
 
 def _perturb(rng, q, t, rot_noise, trans_noise):
+    """Pose noise about each camera's own centre: a rotation of N(0,
+    rot_noise) per axis and a centre offset of N(0, trans_noise) per axis
+    (perturbing t directly would swing far-off cameras about the origin)."""
     n = q.shape[0]
     dq = axis_angle_quat_v(rng.normal(0.0, rot_noise, (n, 3)))
-    return quat_mul_v(q, dq), t + rng.normal(0.0, trans_noise, (n, 3))
+    q1 = quat_mul_v(q, dq)
+    c = -np.einsum("nji,nj->ni", quat_to_matrix_v(q), t)
+    c1 = c + rng.normal(0.0, trans_noise, (n, 3))
+    return q1, -np.einsum("nij,nj->ni", quat_to_matrix_v(q1), c1)
 
 
 def _measure(rng, uv, sigma, outlier_fraction):
@@ -286,6 +292,106 @@ def stereo_window(num_keyframes=20, num_points=2000, seed=0, *, baseline=0.11,
                            np.zeros(num_points, np.uint8), obs_side)
     packed.truth = dict(pose_q=q_true, pose_t=t_true, points=X, centers=centers)
     return packed
+
+
+def street_loop(num_cameras=5600, num_points=3_000_000, seed=3000, *, spacing=1.0,
+                width=1920, height=1080, f=1000.0, street_half_width=8.0, facade_jitter=0.2,
+                facade_height=(0.5, 12.0), track=(6.7, 2, 40), sigma=1.0, outlier_fraction=0.02,
+                rotation_noise=0.01, translation_noise=0.05, point_noise=0.05, fixed=(0, 1)):
+    """Forward-facing cameras along a closed circular street loop, points on
+    the facade planes on both sides (normal jitter +-facade_jitter).  Each
+    point is seen by a run of consecutive cameras (track length geometric,
+    mean track[0], clipped to [track[1], track[2]]) drawn among the cameras
+    that have it in view ahead of them."""
+    rng = np.random.default_rng(seed)
+    n = num_cameras
+    perim = n * spacing
+    radius = perim / (2.0 * np.pi)
+    ang = 2.0 * np.pi * np.arange(n) / n
+    centers = np.stack([radius * np.cos(ang), np.full(n, 1.6), radius * np.sin(ang)], 1)
+    fwd = np.stack([-np.sin(ang), np.zeros(n), np.cos(ang)], 1)  # tangent (direction of travel)
+    r_true = look_at(centers, centers + fwd)
+    t_true = -np.einsum("nij,nj->ni", r_true, centers)
+    q_true = matrix_to_quat_v(r_true)
+    cx, cy = width / 2.0, height / 2.0
+    # Points: arc position, side, height; radial offset = facade +- jitter.
+    s_arc = rng.uniform(0.0, perim, num_points)
+    side = np.where(rng.random(num_points) < 0.5, -1.0, 1.0)
+    h = rng.uniform(facade_height[0], facade_height[1], num_points)
+    rad = radius + side * (street_half_width + rng.normal(0.0, facade_jitter, num_points))
+    pa = s_arc / radius
+    X = np.stack([rad * np.cos(pa), h, rad * np.sin(pa)], 1)
+    # Cameras with the point in view lie behind it along the loop, from about
+    # d_min (facade at the image edge) to d_max metres.
+    half_fov = np.arctan(cx / f)
+    d_min = (street_half_width + 1.0) / np.tan(half_fov)
+    d_max = 45.0
+    lo_cam = np.floor((s_arc - d_max) / spacing).astype(np.int64)
+    hi_cam = np.floor((s_arc - d_min) / spacing).astype(np.int64)
+    avail = hi_cam - lo_cam + 1
+    mean, tlo, thi = track
+    T = np.clip(rng.geometric(1.0 / mean, num_points), tlo, thi)
+    T = np.minimum(T, avail)
+    start = lo_cam + (rng.random(num_points) * (avail - T + 1)).astype(np.int64)
+    obs_pt = np.repeat(np.arange(num_points, dtype=np.int64), T)
+    first = np.repeat(np.cumsum(T) - T, T)
+    obs_cam = (np.repeat(start, T) + (np.arange(obs_pt.size) - first)) % n
+    # Keep the observations that project inside the image in front.
+    keep = np.zeros(obs_pt.size, bool)
+    uv = np.zeros((obs_pt.size, 2))
+    chunk = 1 << 22
+    for a in range(0, obs_pt.size, chunk):
+        b = min(obs_pt.size, a + chunk)
+        ci, pi = obs_cam[a:b], obs_pt[a:b]
+        xc = np.einsum("nij,nj->ni", r_true[ci], X[pi]) + t_true[ci]
+        z = xc[:, 2]
+        u = f * xc[:, 0] / np.maximum(z, 1e-9) + cx
+        v = f * xc[:, 1] / np.maximum(z, 1e-9) + cy
+        keep[a:b] = (z > 0.5) & (u >= 0) & (u < width) & (v >= 0) & (v < height)
+        uv[a:b, 0], uv[a:b, 1] = u, v
+    # Points left with fewer than two observations drop out of the problem.
+    cnt = np.bincount(obs_pt[keep], minlength=num_points)
+    keep &= cnt[obs_pt] >= 2
+    obs_pt, obs_cam, uv = obs_pt[keep], obs_cam[keep], uv[keep]
+    used = np.zeros(num_points, bool)
+    used[obs_pt] = True
+    remap = np.cumsum(used) - 1
+    X = X[used]
+    obs_pt = remap[obs_pt]
+    uv = _measure(rng, uv, sigma, outlier_fraction)
+    q0, t0 = _perturb(rng, q_true, t_true, rotation_noise, translation_noise)
+    pose_fixed = np.zeros(n, np.uint8)
+    for i in fixed:
+        pose_fixed[i] = 1
+        q0[i], t0[i] = q_true[i], t_true[i]
+    X0 = X + rng.normal(0.0, point_noise, X.shape)
+    cam = Camera.pinhole(width, height, f, f, cx, cy)
+    packed = PackedProblem(q0, t0, X0, obs_cam.astype(np.uint32), obs_pt.astype(np.uint32), uv,
+                           [cam], pose_fixed, np.zeros(X.shape[0], np.uint8), None)
+    packed.truth = dict(pose_q=q_true, pose_t=t_true, points=X, centers=centers)
+    return packed
+
+
+def sub_problem(packed: PackedProblem, cameras) -> PackedProblem:
+    """The part of a problem seen by a set of poses: those poses, their
+    observations, and the landmarks they observe at least twice (the first
+    selected pose fixed, as in the whole problem's gauge)."""
+    cams = np.asarray(sorted(set(int(c) for c in cameras)), dtype=np.int64)
+    pose_map = np.full(packed.num_poses, -1, np.int64)
+    pose_map[cams] = np.arange(cams.size)
+    sel = pose_map[packed.obs_pose] >= 0
+    cnt = np.bincount(packed.obs_landmark[sel], minlength=packed.num_landmarks)
+    sel &= cnt[packed.obs_landmark] >= 2
+    used = np.zeros(packed.num_landmarks, bool)
+    used[packed.obs_landmark[sel]] = True
+    lm_map = np.cumsum(used) - 1
+    fixed = np.zeros(cams.size, np.uint8)
+    fixed[0] = 1
+    lf = None if packed.landmark_fixed is None else packed.landmark_fixed[used]
+    oc = None if packed.obs_camera is None else packed.obs_camera[sel]
+    return PackedProblem(packed.pose_q[cams], packed.pose_t[cams], packed.landmarks[used],
+                         pose_map[packed.obs_pose[sel]], lm_map[packed.obs_landmark[sel]],
+                         packed.obs_xy[sel], packed.cameras, fixed, lf, oc)
 
 
 def window_batch(num_windows=512, seed=4000, *, keyframes=(5, 40), points=(200, 5000)):
