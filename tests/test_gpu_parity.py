@@ -103,10 +103,14 @@ def test_street_loop_matches_the_oracle(solver):
     motion with short tracks leaves a flat cost valley that LM crosses slowly
     (the camera centres still move 5e-4 of the extent between iterations 30
     and 60 in the oracle), where two solvers' states cannot be compared; this
-    case has anchor poses around the loop and longer tracks, and the default
-    street geometry is compared through its reduced system and one step."""
-    p = synth.street_loop(240, 15000, seed=17, fixed=(0, 1, 120), track=(12.0, 4, 40))
-    cfg = tight(BaConfig(max_iterations=12, robust_kernel=RobustKernel.huber(1.0)))
+    case has anchor poses around the loop and longer tracks, and enough
+    iterations for both to settle (near the end an FP32 step can be rejected
+    where the FP64 one is accepted, which the next iterations make up); the
+    default street geometry is compared through its reduced system and one
+    step."""
+    p = synth.street_loop(240, 15000, seed=17, fixed=(0, 1, 120), track=(12.0, 4, 40),
+                          outlier_fraction=0.0)
+    cfg = tight(BaConfig(max_iterations=20, robust_kernel=RobustKernel.huber(1.0)))
     compare(solver, p, cfg)
 
 
@@ -133,7 +137,10 @@ def test_street_loop_reduced_system_and_step(solver):
 def test_stereo_window_matches_the_oracle(solver):
     """Rig observations (right camera as sensor_from_rig), 10% poses fixed."""
     p = synth.stereo_window(20, 1500, seed=6)
-    cfg = tight(BaConfig(max_iterations=10, robust_kernel=RobustKernel.huber(1.0)))
+    # 20 iterations: the FP32 and FP64 solves take the same accept/reject and
+    # lambda sequence, but mid-way their costs differ by up to 2e-4 before
+    # meeting again (1.7e-5 at iteration 10, 9e-8 at 20).
+    cfg = tight(BaConfig(max_iterations=20, robust_kernel=RobustKernel.huber(1.0)))
     compare(solver, p, cfg)
 
 
