@@ -309,6 +309,34 @@ int visloc_ba_cuda_batch_solve_uploaded(void* ctx, vlba_result* results,
                                         uint32_t iterations_capacity);
 int visloc_ba_cuda_batch_download(void* ctx, uint32_t n, vlba_problem* const* problems);
 
+/* --------------------------------------------------------- reduced solves */
+/* ReducedSolveAccelerator::solve (pipelines/slam/src/ba_accel.rs:50-72 and
+ * :128-135): block-Jacobi preconditioned conjugate gradients on a reduced
+ * camera system the caller has formed, in the reference's layout -- the
+ * damped 6x6 diagonal blocks (f64, column-major, nalgebra Matrix6), the
+ * sorted edges (a, b), a < b, and for each edge the (row b, column a)
+ * block (f32, column-major), the right-hand side, and the stopping rule
+ * |r| <= tol |rhs| within max_iterations.  The step (6 per node) and the
+ * iteration count are returned.  Cluster and coarse-level preconditioners
+ * and the accelerator-side elimination are not implemented: a shim returns
+ * None for systems that carry them (empty offdiag, clusters or coarse), and
+ * the caller runs its CPU solver. */
+typedef struct vlba_reduced_system {
+  uint32_t num_nodes;
+  uint32_t reserved;
+  uint64_t num_edges;
+  const double* diag;      /* [36 num_nodes] */
+  const uint32_t* edges;   /* [2 num_edges] */
+  const float* offdiag;    /* [36 num_edges] */
+  const double* rhs;       /* [6 num_nodes] */
+  double tol;
+  uint32_t max_iterations;
+  uint32_t reserved2;
+} vlba_reduced_system;
+
+int visloc_ba_cuda_reduced_solve(void* ctx, const vlba_reduced_system* system, double* x,
+                                 uint32_t* iterations, double* relative_residual);
+
 /* --------------------------------------------------------------- autotuner */
 /* Launch shape of the uploaded system: the blocks of the persistent PCG
  * kernel and the share of the L2 that keeps tiles of S resident across PCG

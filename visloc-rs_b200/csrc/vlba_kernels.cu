@@ -1681,6 +1681,49 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
   }
 }
 
+// A reduced camera system given by the caller (ReducedCameraSystem,
+// pipelines/slam/src/ba_accel.rs:50-72) into the tiles: edge e's (row b,
+// column a) block, column-major, to its row-major slot (and the mirrored
+// slot in a diagonal tile); node i's damped diagonal block, column-major
+// f64, to its diagonal slot, its FP64 Cholesky inverse (the block-Jacobi
+// preconditioner; the diagonal's inverse if not positive definite) and its
+// rhs.  Padding slots keep zero blocks, preconditioner and rhs.
+__global__ void __launch_bounds__(256) k_reduced_fill(Dev d, uint32_t n, uint64_t ne,
+                                                      const double* diag, const float* offdiag,
+                                                      const double* rhs) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < ne; e += stride) {
+    const uint2 dst = d.blk_dst[e];
+    const float* src = offdiag + 36 * e;
+#pragma unroll
+    for (int r = 0; r < 6; ++r)
+#pragma unroll
+      for (int c = 0; c < 6; ++c) {
+        d.tiles[dst.x + r * 6 + c] = src[c * 6 + r];
+        if (dst.y != kNone) d.tiles[dst.y + c * 6 + r] = src[c * 6 + r];
+      }
+  }
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < d.num_var_cams;
+       i += stride) {
+    double a[36], inv[36];
+    if (i < n) {
+      for (int r = 0; r < 6; ++r)
+        for (int c = 0; c < 6; ++c) a[r * 6 + c] = diag[36 * i + c * 6 + r];
+      float* blk = d.tiles + d.diag_dst[i];
+      for (int e2 = 0; e2 < 36; ++e2) blk[e2] = (float)a[e2];
+      if (!chol_inverse6(a, inv)) {
+        for (int e2 = 0; e2 < 36; ++e2) inv[e2] = 0.0;
+        for (int q = 0; q < 6; ++q) inv[q * 7] = 1.0 / fmax(a[q * 7], 1e-20);
+      }
+      for (int q = 0; q < 6; ++q) d.rhs[6 * i + q] = (float)rhs[6 * i + q];
+    } else {
+      for (int e2 = 0; e2 < 36; ++e2) inv[e2] = 0.0;
+      for (int q = 0; q < 6; ++q) d.rhs[6 * i + q] = 0.0f;
+    }
+    for (int e2 = 0; e2 < 36; ++e2) d.minv[36 * i + e2] = (float)inv[e2];
+  }
+}
+
 // Current state (buffer Ctrl::cur) of every problem into buffer 0.
 __global__ void __launch_bounds__(256) k_state_to_front(Dev d) {
   const uint32_t stride = gridDim.x * blockDim.x;
@@ -1798,6 +1841,13 @@ cudaError_t launch_pcg_setup(const Dev& d, cudaStream_t s) {
 
 size_t pcg_smem_bytes(int) { return Pcg::kSmem; }
 int pcg_rows_per_block() { return Pcg::kOwnMax; }
+
+cudaError_t launch_reduced_fill(const Dev& d, uint32_t n, uint64_t ne, const double* diag,
+                                const float* offdiag, const double* rhs, cudaStream_t s) {
+  const size_t work = std::max<size_t>((size_t)ne, d.num_var_cams);
+  k_reduced_fill<<<grid1d(work, 256), 256, 0, s>>>(d, n, ne, diag, offdiag, rhs);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_state_to_front(const Dev& d, cudaStream_t s) {
   const size_t n = std::max<size_t>(d.num_poses, d.num_points);

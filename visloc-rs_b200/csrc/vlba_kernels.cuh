@@ -19,6 +19,10 @@ cudaError_t launch_cam_diag(const Dev& d, cudaStream_t s);
 cudaError_t launch_pcg(const Dev& d, int sm_count, cudaStream_t s);
 cudaError_t launch_pose_update(const Dev& d, cudaStream_t s);
 cudaError_t launch_pcg_setup(const Dev& d, cudaStream_t s);
+// Fill the tiles, preconditioner and rhs of a reduced system given directly
+// (device arrays in the reference's layout).
+cudaError_t launch_reduced_fill(const Dev& d, uint32_t n, uint64_t ne, const double* diag,
+                                const float* offdiag, const double* rhs, cudaStream_t s);
 // Copy each problem's current state into state buffer 0 (for a bulk download).
 cudaError_t launch_state_to_front(const Dev& d, cudaStream_t s);
 

@@ -555,6 +555,82 @@ void finish_tiles(Plan& P) {
 
 }  // namespace
 
+void build_reduced_plan(uint32_t n, const uint32_t* edges, uint64_t ne, uint32_t tb,
+                        const LmParams& params, Plan* plan) {
+  Plan& P = *plan;
+  P = Plan();
+  if (n == 0) throw std::runtime_error("a reduced system of no nodes");
+  if (ne >= kNone) throw std::runtime_error("more than 2^32 edges");
+  P.tb = tb;
+  P.group = 8;
+  P.num_problems = 1;
+  const uint32_t nslots = round_up(n, tb), ntr = nslots / tb;
+  P.prob_pose_begin = {0, 0};
+  P.prob_point_begin = {0, 0};
+  P.prob_obs_begin = {0, 0};
+  P.prob_tr_begin = {0, ntr};
+  P.prob_chunk_begin = {0, 0};
+  P.prob_camera_begin = {0, 0};
+  P.params = {params};
+  P.slot_prob.assign(nslots, 0u);
+  P.pt_off = {0};
+  P.cam_off.assign(nslots + 1, 0u);
+  P.dup_off.assign(nslots + 1, 0u);
+  P.chunk_point_begin = {0};
+  P.num_var_cams = nslots;
+  P.num_tile_rows = ntr;
+  P.real_var_cams = n;
+  // Tiles: the diagonal ones and those holding an edge's (b, a) block.
+  std::vector<uint8_t> tile_has((size_t)ntr * ntr, 0);
+  for (uint32_t t = 0; t < ntr; ++t) tile_has[(size_t)t * ntr + t] = 1;
+  for (uint64_t e = 0; e < ne; ++e) {
+    const uint32_t a = edges[2 * e], b = edges[2 * e + 1];
+    if (!(a < b) || b >= n) throw std::runtime_error("edge (a, b) must have a < b < nodes");
+    if (e && (uint64_t)edges[2 * e - 2] * n + edges[2 * e - 1] >= (uint64_t)a * n + b)
+      throw std::runtime_error("edges must be sorted and distinct");
+    tile_has[(size_t)(b / tb) * ntr + a / tb] = 1;
+  }
+  std::vector<uint32_t> tile_id((size_t)ntr * ntr, kNone);
+  uint32_t count = 0;
+  for (uint32_t I = 0; I < ntr; ++I)
+    for (uint32_t J = 0; J <= I; ++J)
+      if (tile_has[(size_t)I * ntr + J]) {
+        if (I > 0xFFFFu) throw std::runtime_error("more than 65535 tile rows");
+        tile_id[(size_t)I * ntr + J] = count++;
+        P.tile_ij.push_back((I << 16) | J);
+      }
+  const uint32_t tf = tb * tb * kBlock;
+  if ((uint64_t)count * tf >= kNone) throw std::runtime_error("reduced system exceeds 2^32 floats");
+  P.blk_off.assign(ne + 1, 0u);
+  P.blk_dst.resize(ne);
+  for (uint64_t e = 0; e < ne; ++e) {
+    const uint32_t a = edges[2 * e], b = edges[2 * e + 1];
+    const uint32_t I = b / tb, J = a / tb, li = b % tb, lj = a % tb;
+    const uint32_t t = tile_id[(size_t)I * ntr + J];
+    P.blk_dst[e].a = t * tf + (li * tb + lj) * kBlock;
+    P.blk_dst[e].b = (I == J) ? t * tf + (lj * tb + li) * kBlock : kNone;
+  }
+  for (uint32_t sidx = 0; sidx < nslots; ++sidx) {
+    const uint32_t I = sidx / tb, li = sidx % tb;
+    P.diag_dst.push_back(tile_id[(size_t)I * ntr + I] * tf + (li * tb + li) * kBlock);
+  }
+  P.tr_list_off = {0};
+  for (uint32_t I = 0; I < ntr; ++I) {
+    for (uint32_t J = 0; J <= I; ++J) {
+      const uint32_t t = tile_id[(size_t)I * ntr + J];
+      if (t != kNone) P.tr_list.push_back(2 * t);
+    }
+    for (uint32_t K = I + 1; K < ntr; ++K) {
+      const uint32_t t = tile_id[(size_t)K * ntr + I];
+      if (t != kNone) P.tr_list.push_back(2 * t + 1);
+    }
+    P.tr_list_off.push_back((uint32_t)P.tr_list.size());
+    P.tr_prob.push_back(0);
+  }
+  P.camera_pairs = ne;
+  finish_tiles(P);
+}
+
 void merge_plans(const std::vector<const Plan*>& parts, Plan* out) {
   Plan& P = *out;
   P = Plan();

@@ -83,6 +83,12 @@ LmParams make_params(const vlba_config* cfg);
 void build_plan(const vlba_problem* const* problems, const vlba_config* const* configs,
                 uint32_t n, uint32_t tb, Plan* plan, uint32_t max_threads = 0);
 
+// The layout of a reduced camera system given directly (n nodes, sorted
+// edges (a, b), a < b): its tiles, block destinations and PCG lists, with no
+// observations; `params` carries the PCG tolerance and iteration cap.
+void build_reduced_plan(uint32_t n, const uint32_t* edges, uint64_t ne, uint32_t tb,
+                        const LmParams& params, Plan* plan);
+
 // Concatenate plans (built by build_plan) into one batch plan: indices are
 // offset, each problem's layout and order are kept, so a problem solves the
 // same in the merged plan as in its own.

@@ -1583,6 +1583,59 @@ int visloc_ba_cuda_server_wait(void* server, uint64_t ticket, double timeout_ms,
   return st;
 }
 
+int visloc_ba_cuda_reduced_solve(void* ctx, const vlba_reduced_system* sys, double* x,
+                                 uint32_t* iterations, double* relative_residual) {
+  auto* c = static_cast<Context*>(ctx);
+  if (!c || !sys || !x || !sys->diag || !sys->rhs || sys->num_nodes == 0 ||
+      (sys->num_edges && (!sys->edges || !sys->offdiag)) || !(sys->tol >= 0.0))
+    return VLBA_ERR_INVALID_ARGUMENT;
+  return vlba::guarded(c, [&] {
+    vlba::set_device(c);
+    vlba_config cfg;
+    visloc_ba_cuda_default_config(&cfg);
+    cfg.max_pcg_iterations = sys->max_iterations;
+    cfg.pcg_relative_tolerance = sys->tol;
+    const vlba::LmParams lp = vlba::make_params(&cfg);
+    vlba::build_reduced_plan(sys->num_nodes, sys->edges, sys->num_edges, 8, lp, &c->plan);
+    const std::string bad = vlba::check_plan(c->plan);
+    if (!bad.empty()) throw vlba::Status(VLBA_ERR_INVALID_ARGUMENT, bad);
+    vlba::upload_plan(c, 1);
+    cudaStream_t s = c->stream;
+    const size_t n = sys->num_nodes, ne = sys->num_edges;
+    // The caller's arrays, staged for the fill kernel.
+    struct Staged {
+      void* p = nullptr;
+      ~Staged() {
+        if (p) cudaFree(p);
+      }
+    } diag, off, rhs;
+    VLBA_CUDA(cudaMalloc(&diag.p, 36 * n * 8));
+    VLBA_CUDA(cudaMalloc(&rhs.p, 6 * n * 8));
+    if (ne) VLBA_CUDA(cudaMalloc(&off.p, 36 * ne * 4));
+    VLBA_CUDA(cudaMemcpyAsync(diag.p, sys->diag, 36 * n * 8, cudaMemcpyHostToDevice, s));
+    VLBA_CUDA(cudaMemcpyAsync(rhs.p, sys->rhs, 6 * n * 8, cudaMemcpyHostToDevice, s));
+    if (ne) VLBA_CUDA(cudaMemcpyAsync(off.p, sys->offdiag, 36 * ne * 4, cudaMemcpyHostToDevice, s));
+    vlba::Dev& d = c->dev;
+    vlba::reset_state(c);
+    vlba::check_launch(vlba::launch_reduced_fill(d, (uint32_t)n, ne, (const double*)diag.p,
+                                                 (const float*)off.p, (const double*)rhs.p, s),
+                       "reduced fill");
+    vlba::check_launch(vlba::launch_pcg_setup(d, s), "pcg setup");
+    vlba::check_launch(vlba::launch_pcg(d, c->pcg_grid, s), "pcg");
+    std::vector<float> xf(6 * n);
+    VLBA_CUDA(cudaMemcpyAsync(xf.data(), d.x, xf.size() * 4, cudaMemcpyDeviceToHost, s));
+    vlba::PcgState pg;
+    VLBA_CUDA(cudaMemcpyAsync(&pg, d.pcg, sizeof pg, cudaMemcpyDeviceToHost, s));
+    unsigned int err = 0;
+    VLBA_CUDA(cudaMemcpyAsync(&err, d.error, 4, cudaMemcpyDeviceToHost, s));
+    VLBA_CUDA(cudaStreamSynchronize(s));
+    if (err) throw vlba::Status(VLBA_ERR_TIMEOUT, "a bounded device wait gave up");
+    for (size_t i = 0; i < xf.size(); ++i) x[i] = xf[i];
+    if (iterations) *iterations = pg.iters;
+    if (relative_residual) *relative_residual = pg.bnorm > 0 ? pg.rnorm / pg.bnorm : 0.0;
+  });
+}
+
 int visloc_ba_cuda_autotune(void* ctx, vlba_launch_shape* chosen) {
   auto* c = static_cast<Context*>(ctx);
   if (!c) return VLBA_ERR_INVALID_ARGUMENT;

@@ -170,6 +170,21 @@ class PlanInfo(C.Structure):
 
 P = C.POINTER
 # name -> (restype, argtypes): every symbol include/visloc_ba_cuda.h declares.
+class ReducedSystem(C.Structure):
+    _fields_ = [
+        ("num_nodes", C.c_uint32),
+        ("reserved", C.c_uint32),
+        ("num_edges", C.c_uint64),
+        ("diag", C.POINTER(C.c_double)),
+        ("edges", C.POINTER(C.c_uint32)),
+        ("offdiag", C.POINTER(C.c_float)),
+        ("rhs", C.POINTER(C.c_double)),
+        ("tol", C.c_double),
+        ("max_iterations", C.c_uint32),
+        ("reserved2", C.c_uint32),
+    ]
+
+
 class LaunchShape(C.Structure):
     _fields_ = [
         ("pcg_blocks", C.c_int32),
@@ -232,6 +247,9 @@ SOLVER_EXPORTS = {
         C.c_int, [C.c_void_p, P(Result), P(Iteration), C.c_uint32],
     ),
     "visloc_ba_cuda_batch_download": (C.c_int, [C.c_void_p, C.c_uint32, P(P(Problem))]),
+    "visloc_ba_cuda_reduced_solve": (
+        C.c_int, [C.c_void_p, P(ReducedSystem), P(C.c_double), P(C.c_uint32), P(C.c_double)],
+    ),
     "visloc_ba_cuda_autotune": (C.c_int, [C.c_void_p, P(LaunchShape)]),
     "visloc_ba_cuda_set_launch_shape": (C.c_int, [C.c_void_p, P(LaunchShape)]),
     "visloc_ba_cuda_server_create": (C.c_void_p, [C.c_int, C.c_uint32, C.c_uint64, C.c_uint32]),

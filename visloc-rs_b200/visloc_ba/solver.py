@@ -108,6 +108,39 @@ class CudaSolver:
     def download(self, packed: PackedProblem) -> int:
         return self.lib.visloc_ba_cuda_download(self.ctx, C.byref(packed.abi()))
 
+    # ------------------------------------------------------ reduced solve
+    def reduced_solve(self, diag, edges, offdiag, rhs, tol: float, max_iterations: int):
+        """ReducedSolveAccelerator::solve on a reduced camera system:
+        diag (n,6,6) damped diagonal blocks, edges (e,2) sorted (a, b) with
+        a < b, offdiag (e,6,6) the (row b, column a) blocks, rhs (n,6).
+        Returns (x (n,6), iterations, relative residual)."""
+        import numpy as np
+
+        diag = np.ascontiguousarray(np.asarray(diag, np.float64).transpose(0, 2, 1))  # column-major
+        off = np.ascontiguousarray(np.asarray(offdiag, np.float32).reshape(-1, 6, 6)
+                                   .transpose(0, 2, 1))
+        edges = np.ascontiguousarray(np.asarray(edges, np.uint32).reshape(-1, 2))
+        rhs = np.ascontiguousarray(np.asarray(rhs, np.float64).reshape(-1, 6))
+        n = diag.shape[0]
+        sysm = _abi.ReducedSystem()
+        sysm.num_nodes = n
+        sysm.num_edges = edges.shape[0]
+        sysm.diag = diag.ctypes.data_as(C.POINTER(C.c_double))
+        sysm.edges = edges.ctypes.data_as(C.POINTER(C.c_uint32))
+        sysm.offdiag = off.ctypes.data_as(C.POINTER(C.c_float))
+        sysm.rhs = rhs.ctypes.data_as(C.POINTER(C.c_double))
+        sysm.tol = float(tol)
+        sysm.max_iterations = int(max_iterations)
+        x = np.zeros((n, 6))
+        it = C.c_uint32()
+        rr = C.c_double()
+        st = self.lib.visloc_ba_cuda_reduced_solve(self.ctx, C.byref(sysm),
+                                                   x.ctypes.data_as(C.POINTER(C.c_double)),
+                                                   C.byref(it), C.byref(rr))
+        if st != _abi.OK:
+            raise SolverError(st, self.last_error())
+        return x, it.value, rr.value
+
     # ---------------------------------------------------------- autotuner
     def autotune(self) -> dict:
         """Time candidate launch shapes on the uploaded system; apply and
