@@ -396,6 +396,14 @@ int visloc_ba_cuda_server_wait(void* server, uint64_t ticket, double timeout_ms,
 const char* visloc_ba_cuda_server_last_error(void* server);
 
 /* ------------------------------------------------------------- diagnostics */
+/* Self-test of the bounded device waits every kernel uses (mbarrier waits,
+ * row counters, the grid barrier give up after 2 s, set an error bit and let
+ * the kernel return, so a lost arrival becomes VLBA_ERR_TIMEOUT instead of a
+ * hung GPU): waits on a device flag that nothing sets for limit_ms and
+ * returns VLBA_ERR_TIMEOUT with the time it waited.  The context stays usable
+ * afterwards.  No reference counterpart. */
+int visloc_ba_cuda_wait_probe(void* ctx, double limit_ms, double* waited_ms);
+
 /* One damped linear step at the given state, without updating it: the step
  * of solve_step (bundle/normal_equations.rs:1621-1733) as this solver forms
  * it (linearisation, reduced system, PCG, back-substitution).  dp holds 6

@@ -31,7 +31,10 @@ namespace vlba {
 
 constexpr uint32_t kNone = 0xFFFFFFFFu;
 constexpr int kBlock = 36;             // floats in a 6x6 block
-constexpr uint32_t kSpinLimit = 1u << 24;  // bounded device waits
+// Every device wait (on an mbarrier, a counter or a flag that another block
+// writes) gives up after this long, sets an error bit and lets its kernel
+// return: a lost arrival turns into VLBA_ERR_TIMEOUT, never a hung GPU.
+constexpr unsigned long long kWaitLimitNs = 2000000000ull;  // 2 s
 
 // Camera of an observation (f64).  R/t is sensor_from_rig (identity for
 // monocular observations).
@@ -216,5 +219,14 @@ enum ErrorBits : unsigned int {
   kErrBarrierTimeout = 1u,
   kErrTmaTimeout = 2u,
 };
+
+#ifdef __CUDACC__
+// Nanoseconds of the GPU's global timer (deadlines of the bounded waits).
+__device__ __forceinline__ unsigned long long now_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+#endif
 
 }  // namespace vlba

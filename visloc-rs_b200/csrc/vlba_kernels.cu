@@ -932,11 +932,12 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Bounded wait; false (and the error flag) on timeout.
+// Bounded wait; false (and the error flag) once kWaitLimitNs have passed.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, unsigned int* err) {
-  uint32_t spins = 0;
+  if (mbar_try_wait(bar, parity)) return true;
+  const unsigned long long t_end = now_ns() + kWaitLimitNs;
   while (!mbar_try_wait(bar, parity)) {
-    if (++spins > kSpinLimit) {
+    if (now_ns() > t_end) {
       atomicOr(err, (unsigned int)kErrTmaTimeout);
       return false;
     }
@@ -987,9 +988,9 @@ __device__ bool grid_barrier(unsigned int* bar, unsigned int nblocks, unsigned i
       bar[0] = 0u;
       asm volatile("st.release.gpu.u32 [%0], %1;" ::"l"(bar + 1), "r"(gen) : "memory");
     } else {
-      uint32_t spins = 0;
+      const unsigned long long t_end = now_ns() + kWaitLimitNs;
       while (ld_acquire(bar + 1) != gen) {
-        if (++spins > kSpinLimit) {
+        if (now_ns() > t_end) {
           atomicOr(err, (unsigned int)kErrBarrierTimeout);
           break;
         }
@@ -1524,9 +1525,9 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
     auto wait_row = [&](uint32_t j) {  // one thread
       const uint32_t need = own_m1[j] - own_m0[j];
       const uint32_t R = blockIdx.x + j * G;
-      uint32_t spins = 0;
+      const unsigned long long t_end = now_ns() + kWaitLimitNs;
       while (ld_acquire(d.row_cnt + R) < need) {
-        if (++spins > kSpinLimit) {
+        if (now_ns() > t_end) {
           atomicOr(d.error, (unsigned int)kErrBarrierTimeout);
           break;
         }
@@ -1665,9 +1666,9 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
   // Drain the copies still in flight (prefetched tiles), bounded.
   if (lane == 0) {
     for (uint64_t s = consumed; s < issued; ++s) {
-      uint32_t spins = 0;
+      const unsigned long long t_end = now_ns() + kWaitLimitNs;
       while (!mbar_try_wait(&mbar[warp][s % C::kStages], (uint32_t)((s / C::kStages) & 1)) &&
-             ++spins < kSpinLimit) {
+             now_ns() <= t_end) {
       }
     }
   }
@@ -1722,6 +1723,24 @@ __global__ void __launch_bounds__(256) k_reduced_fill(Dev d, uint32_t n, uint64_
     }
     for (int e2 = 0; e2 < 36; ++e2) d.minv[36 * i + e2] = (float)inv[e2];
   }
+}
+
+// Self-test of the bounded waits: thread 0 waits on a flag that nothing
+// sets, with the wait primitive the kernels use, until `limit_ns` has
+// passed; it then sets the timeout bit and returns, recording how long it
+// waited.
+__global__ void k_wait_probe(const unsigned int* flag, unsigned long long limit_ns,
+                             unsigned int* err, unsigned long long* waited) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  const unsigned long long t0 = now_ns(), t_end = t0 + limit_ns;
+  while (ld_acquire(flag) == 0u) {
+    if (now_ns() > t_end) {
+      atomicOr(err, (unsigned int)kErrBarrierTimeout);
+      break;
+    }
+    __nanosleep(1000);
+  }
+  *waited = now_ns() - t0;
 }
 
 // Current state (buffer Ctrl::cur) of every problem into buffer 0.
@@ -1846,6 +1865,12 @@ cudaError_t launch_reduced_fill(const Dev& d, uint32_t n, uint64_t ne, const dou
                                 const float* offdiag, const double* rhs, cudaStream_t s) {
   const size_t work = std::max<size_t>((size_t)ne, d.num_var_cams);
   k_reduced_fill<<<grid1d(work, 256), 256, 0, s>>>(d, n, ne, diag, offdiag, rhs);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_wait_probe(const unsigned int* flag, unsigned long long limit_ns,
+                              unsigned int* err, unsigned long long* waited, cudaStream_t s) {
+  k_wait_probe<<<1, 32, 0, s>>>(flag, limit_ns, err, waited);
   return cudaGetLastError();
 }
 

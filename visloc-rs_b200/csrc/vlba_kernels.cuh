@@ -23,6 +23,9 @@ cudaError_t launch_pcg_setup(const Dev& d, cudaStream_t s);
 // (device arrays in the reference's layout).
 cudaError_t launch_reduced_fill(const Dev& d, uint32_t n, uint64_t ne, const double* diag,
                                 const float* offdiag, const double* rhs, cudaStream_t s);
+// Bounded-wait self-test: waits on `flag` (which nothing sets) for limit_ns.
+cudaError_t launch_wait_probe(const unsigned int* flag, unsigned long long limit_ns,
+                              unsigned int* err, unsigned long long* waited, cudaStream_t s);
 // Copy each problem's current state into state buffer 0 (for a bulk download).
 cudaError_t launch_state_to_front(const Dev& d, cudaStream_t s);
 

@@ -1636,6 +1636,39 @@ int visloc_ba_cuda_reduced_solve(void* ctx, const vlba_reduced_system* sys, doub
   });
 }
 
+int visloc_ba_cuda_wait_probe(void* ctx, double limit_ms, double* waited_ms) {
+  auto* c = static_cast<Context*>(ctx);
+  if (!c || !(limit_ms >= 0.0) || limit_ms > 10000.0) return VLBA_ERR_INVALID_ARGUMENT;
+  unsigned int err = 0;
+  const int st = vlba::guarded(c, [&] {
+    vlba::set_device(c);
+    struct Words {
+      void* p = nullptr;
+      ~Words() {
+        if (p) cudaFree(p);
+      }
+    } w;
+    VLBA_CUDA(cudaMalloc(&w.p, 16));
+    VLBA_CUDA(cudaMemsetAsync(w.p, 0, 16, c->stream));
+    auto* flag = static_cast<unsigned int*>(w.p);
+    auto* waited = reinterpret_cast<unsigned long long*>(static_cast<char*>(w.p) + 8);
+    vlba::check_launch(vlba::launch_wait_probe(flag, (unsigned long long)(limit_ms * 1e6),
+                                               flag + 1, waited, c->stream),
+                       "wait probe");
+    unsigned long long ns = 0;
+    VLBA_CUDA(cudaMemcpyAsync(&err, flag + 1, 4, cudaMemcpyDeviceToHost, c->stream));
+    VLBA_CUDA(cudaMemcpyAsync(&ns, waited, 8, cudaMemcpyDeviceToHost, c->stream));
+    VLBA_CUDA(cudaStreamSynchronize(c->stream));
+    if (waited_ms) *waited_ms = ns / 1e6;
+  });
+  if (st != VLBA_OK) return st;
+  if (err) {
+    c->error = "the wait gave up as bounded (a flag that nothing sets)";
+    return VLBA_ERR_TIMEOUT;
+  }
+  return VLBA_OK;
+}
+
 int visloc_ba_cuda_autotune(void* ctx, vlba_launch_shape* chosen) {
   auto* c = static_cast<Context*>(ctx);
   if (!c) return VLBA_ERR_INVALID_ARGUMENT;

@@ -251,6 +251,7 @@ SOLVER_EXPORTS = {
         C.c_int, [C.c_void_p, P(ReducedSystem), P(C.c_double), P(C.c_uint32), P(C.c_double)],
     ),
     "visloc_ba_cuda_autotune": (C.c_int, [C.c_void_p, P(LaunchShape)]),
+    "visloc_ba_cuda_wait_probe": (C.c_int, [C.c_void_p, C.c_double, P(C.c_double)]),
     "visloc_ba_cuda_set_launch_shape": (C.c_int, [C.c_void_p, P(LaunchShape)]),
     "visloc_ba_cuda_server_create": (C.c_void_p, [C.c_int, C.c_uint32, C.c_uint64, C.c_uint32]),
     "visloc_ba_cuda_server_destroy": (None, [C.c_void_p]),

@@ -141,6 +141,12 @@ class CudaSolver:
             raise SolverError(st, self.last_error())
         return x, it.value, rr.value
 
+    def wait_probe(self, limit_ms: float):
+        """(status, waited ms) of the bounded-wait self-test."""
+        waited = C.c_double()
+        st = self.lib.visloc_ba_cuda_wait_probe(self.ctx, float(limit_ms), C.byref(waited))
+        return st, waited.value
+
     # ---------------------------------------------------------- autotuner
     def autotune(self) -> dict:
         """Time candidate launch shapes on the uploaded system; apply and
