@@ -150,6 +150,7 @@ struct Dev {
 
   // observations, point-major
   const uint32_t* pt_off;      // [M + 1]
+  const uint32_t* obs_point;   // [K] point of each observation
   const uint32_t* obs_pose;    // [K]
   const uint32_t* obs_cam;     // [K] camera index
   const uint32_t* obs_slot;    // [K] variable slot of the pose or kNone

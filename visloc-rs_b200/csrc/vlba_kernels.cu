@@ -170,10 +170,13 @@ __global__ void __launch_bounds__(256) k_pose_table(Dev d) {
 }
 
 // ------------------------------------------------------------- linearize
-// One thread per point, its observations contiguous (point-major order).
+// One thread per observation (point-major order): the residual and analytic
+// Jacobian in FP64, the IRLS weight, and the observation's H_o and e_o.  The
+// point sums H_ll and g_l are formed by k_point_prep from these records.
 __global__ void __launch_bounds__(256) k_linearize(Dev d) {
-  for (uint32_t l = blockIdx.x * blockDim.x + threadIdx.x; l < d.num_points;
-       l += gridDim.x * blockDim.x) {
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < d.num_obs;
+       k += gridDim.x * blockDim.x) {
+    const uint32_t l = d.obs_point[k];
     const uint32_t P = d.point_prob[l];
     const Ctrl& c = d.ctrl[P];
     if (c.done || !c.relinearize) continue;
@@ -182,9 +185,7 @@ __global__ void __launch_bounds__(256) k_linearize(Dev d) {
     double X[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) X[a] = d.points[cur][3 * (size_t)l + a];
-    double hl[6] = {0, 0, 0, 0, 0, 0}, gl[3] = {0, 0, 0};
-    const uint32_t k0 = d.pt_off[l], k1 = d.pt_off[l + 1];
-    for (uint32_t k = k0; k < k1; ++k) {
+    {
       const uint32_t pose = d.obs_pose[k];
       const DevCamera& cam = d.cameras[d.obs_cam[k]];
       const double* rt = d.pose_rt[cur] + 12 * (size_t)pose;
@@ -230,16 +231,7 @@ __global__ void __launch_bounds__(256) k_linearize(Dev d) {
       d.obs_h[2 * (size_t)k] = make_float4(h[0], h[1], h[2], h[3]);
       d.obs_h[2 * (size_t)k + 1] = make_float4(h[4], h[5], __uint_as_float(l), (float)X[2]);
       d.obs_e[k] = make_float4(e[0], e[1], e[2], wf);
-#pragma unroll
-      for (int a = 0; a < 6; ++a) hl[a] += h[a];
-#pragma unroll
-      for (int a = 0; a < 3; ++a) gl[a] += e[a];
     }
-    float* ph = d.pt_h + 9 * (size_t)l;
-#pragma unroll
-    for (int a = 0; a < 6; ++a) ph[a] = (float)hl[a];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) ph[6 + a] = (float)gl[a];
   }
 }
 
@@ -261,6 +253,29 @@ __global__ void __launch_bounds__(256) k_point_prep(Dev d) {
     const float X2 = (float)d.points[cur][3 * (size_t)l + 2];
     double inv[6] = {0, 0, 0, 0, 0, 0}, v[3] = {0, 0, 0}, g[3] = {0, 0, 0};
     float ok = 0.0f;
+    if (d.point_var[l] && c.relinearize) {
+      // H_ll and g_l of the new linearisation: the observations' records
+      // summed in observation order (FP64 sums, stored FP32).
+      double hl[6] = {0, 0, 0, 0, 0, 0}, gl[3] = {0, 0, 0};
+      for (uint32_t k = d.pt_off[l]; k < d.pt_off[l + 1]; ++k) {
+        const float4 h0 = d.obs_h[2 * (size_t)k], h1 = d.obs_h[2 * (size_t)k + 1];
+        const float4 e = d.obs_e[k];
+        hl[0] += h0.x;
+        hl[1] += h0.y;
+        hl[2] += h0.z;
+        hl[3] += h0.w;
+        hl[4] += h1.x;
+        hl[5] += h1.y;
+        gl[0] += e.x;
+        gl[1] += e.y;
+        gl[2] += e.z;
+      }
+      float* ph = d.pt_h + 9 * (size_t)l;
+#pragma unroll
+      for (int a = 0; a < 6; ++a) ph[a] = (float)hl[a];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) ph[6 + a] = (float)gl[a];
+    }
     if (d.point_var[l]) {
       const float* ph = d.pt_h + 9 * (size_t)l;
       double a = ph[0], b = ph[1], cc = ph[2], dd = ph[3], e = ph[4], f = ph[5];
@@ -647,14 +662,17 @@ __global__ void __launch_bounds__(256) k_pose_update(Dev d) {
 }
 
 // ------------------------------------------------- back-substitution + cost
-// One block of 256 threads per chunk of points of one problem.  TRIAL: the
-// landmark step dl = -H^-1 (g + sum_o H_o (rho + omega x X)) of every
-// variable point (W_o^T dc = H_o B dc), the candidate point X + dl, and the
-// cost at the candidate poses/points.  !TRIAL: the cost of the current state.
+// One block of 256 threads per chunk of (at most 256) points of one problem,
+// in two steps: one thread per point -- with TRIAL, the landmark step
+// dl = -H^-1 (g + sum_o H_o (rho + omega x X)) of every variable point
+// (W_o^T dc = H_o B dc) and the candidate point X + dl -- then one thread per
+// observation of the chunk for the cost at the candidate poses/points (the
+// current state without TRIAL).  Sums in a fixed order per chunk.
 template <bool TRIAL>
 __global__ void __launch_bounds__(256) k_cost(Dev d) {
   __shared__ double red[256];
   __shared__ unsigned long long redu[256];
+  __shared__ double sX[3 * 256];  // the chunk's (candidate) points
   for (uint32_t ch = blockIdx.x; ch < d.num_point_chunks; ch += gridDim.x) {
     const uint32_t lo = d.chunk_point_begin[ch], hi = d.chunk_point_begin[ch + 1];
     const uint32_t P = d.point_prob[lo];
@@ -701,19 +719,26 @@ __global__ void __launch_bounds__(256) k_cost(Dev d) {
 #pragma unroll
         for (int a = 0; a < 3; ++a) d.points[cur ^ 1u][3 * (size_t)l + a] = X[a];
       }
-      for (uint32_t k = k0; k < k1; ++k) {
-        const DevCamera& cam = d.cameras[d.obs_cam[k]];
-        const double* rt = d.pose_rt[pose_buf] + 12 * (size_t)d.obs_pose[k];
-        double xs[3], pred[2];
-        to_sensor(rt, cam, X, xs);
-        if (!(xs[2] > 0.0) || !camera_project(cam, xs, pred)) {
-          ++bad;
-          continue;
-        }
-        const double2 xy = d.obs_xy[k];
-        const double rx = pred[0] - xy.x, ry = pred[1] - xy.y;
-        cost += robust_cost(lp.robust_kernel, lp.robust_parameter, rx * rx + ry * ry);
+#pragma unroll
+      for (int a = 0; a < 3; ++a) sX[3 * (l - lo) + a] = X[a];
+    }
+    __syncthreads();
+    // The chunk's observations, one thread each (stride 256), at the points
+    // just placed in shared memory.
+    const uint32_t o0 = d.pt_off[lo], o1 = d.pt_off[hi];
+    for (uint32_t k = o0 + threadIdx.x; k < o1; k += blockDim.x) {
+      const double* Xk = sX + 3 * (d.obs_point[k] - lo);
+      const DevCamera& cam = d.cameras[d.obs_cam[k]];
+      const double* rt = d.pose_rt[pose_buf] + 12 * (size_t)d.obs_pose[k];
+      double xs[3], pred[2];
+      to_sensor(rt, cam, Xk, xs);
+      if (!(xs[2] > 0.0) || !camera_project(cam, xs, pred)) {
+        ++bad;
+        continue;
       }
+      const double2 xy = d.obs_xy[k];
+      const double rx = pred[0] - xy.x, ry = pred[1] - xy.y;
+      cost += robust_cost(lp.robust_kernel, lp.robust_parameter, rx * rx + ry * ry);
     }
     const double tc = block_sum<double, 256>(cost, red);
     const unsigned long long tb = block_sum<unsigned long long, 256>(bad, redu);
@@ -1817,7 +1842,7 @@ cudaError_t launch_decide(const Dev& d, bool init, cudaStream_t s) {
 }
 
 cudaError_t launch_linearize(const Dev& d, cudaStream_t s) {
-  k_linearize<<<grid1d(d.num_points, 256), 256, 0, s>>>(d);
+  k_linearize<<<grid1d(d.num_obs, 256), 256, 0, s>>>(d);
   return cudaGetLastError();
 }
 

@@ -203,6 +203,7 @@ void build_plan_serial(const vlba_problem* const* problems, const vlba_config* c
   P.obs_cam.resize(tot_obs);
   P.obs_slot.resize(tot_obs);
   P.obs_xy.resize(2 * tot_obs);
+  P.obs_point.resize(tot_obs);
   P.cameras.reserve(tot_cams);
   P.prob_pose_begin.push_back(0);
   P.prob_point_begin.push_back(0);
@@ -261,7 +262,10 @@ void build_plan_serial(const vlba_problem* const* problems, const vlba_config* c
       std::vector<uint32_t> fill(cnt.begin(), cnt.end() - 1);
       for (uint32_t o = 0; o < no; ++o) order[fill[p->obs_landmark[o]]++] = o;
     }
-    for (uint32_t j = 0; j < nl; ++j) P.pt_off[point_base + j + 1] = obs_base + cnt[j + 1];
+    for (uint32_t j = 0; j < nl; ++j) {
+      P.pt_off[point_base + j + 1] = obs_base + cnt[j + 1];
+      for (uint32_t k = cnt[j]; k < cnt[j + 1]; ++k) P.obs_point[obs_base + k] = point_base + j;
+    }
     for (uint32_t k = 0; k < no; ++k) {
       const uint32_t o = order[k];
       const uint32_t g = obs_base + k;
@@ -688,6 +692,7 @@ void merge_plans(const std::vector<const Plan*>& parts, Plan* out) {
     cat(P.point_var, Q.point_var);
     cat(P.cameras, Q.cameras);
     for (size_t j = 1; j < Q.pt_off.size(); ++j) P.pt_off.push_back(obs_b + Q.pt_off[j]);
+    for (uint32_t v : Q.obs_point) P.obs_point.push_back(point_b + v);
     for (uint32_t v : Q.obs_pose) P.obs_pose.push_back(pose_b + v);
     for (uint32_t v : Q.obs_cam) P.obs_cam.push_back(cam_b + v);
     for (uint32_t v : Q.obs_slot) P.obs_slot.push_back(v == kNone ? kNone : slot_b + v);
@@ -779,9 +784,12 @@ std::string check_plan(const Plan& P) {
   if (P.pt_off.size() != npts + 1 || P.pt_off.back() != nobs) return bad("pt_off");
   for (uint64_t j = 0; j < npts; ++j)
     if (P.pt_off[j] > P.pt_off[j + 1]) return bad("pt_off order");
-  if (P.obs_cam.size() != nobs || P.obs_slot.size() != nobs || P.obs_xy.size() != 2 * nobs)
+  if (P.obs_cam.size() != nobs || P.obs_slot.size() != nobs || P.obs_xy.size() != 2 * nobs ||
+      P.obs_point.size() != nobs)
     return bad("obs sizes");
   for (uint64_t k = 0; k < nobs; ++k) {
+    const uint32_t l = P.obs_point[k];
+    if (l >= npts || P.pt_off[l] > k || P.pt_off[l + 1] <= k) return bad("obs_point");
     if (P.obs_pose[k] >= nposes) return bad("obs_pose");
     if (P.obs_cam[k] >= ncam) return bad("obs_cam");
     if (P.obs_slot[k] != kNone && P.obs_slot[k] >= nslots) return bad("obs_slot");
@@ -844,7 +852,7 @@ size_t Plan::device_bytes() const {
   size_t b = 0;
   b += npose * (8 * (4 + 3 + 12) * 2 + 8 + 4 + 4);  // state x2, step, slot, prob
   b += npt * (8 * 3 * 2 + 4 + 1 + 4 + 36 + 64);     // points x2, off, var, prob, pt_h, pt_s
-  b += nobs * (4 * 3 + 16 + 32 + 16 + 32);           // pose, cam, slot, xy, obs_h, obs_e, obs_p
+  b += nobs * (4 * 4 + 16 + 32 + 16 + 32);           // point, pose, cam, slot, xy, obs_h, obs_e, obs_p
   b += cam_obs.size() * 4 + pairs.size() * 8 + dup_pairs.size() * 8;
   b += blk_dst.size() * (8 + 4);
   b += tile_ij.size() * ((size_t)tb * tb * kBlock * 4 + 4 + 2 * (size_t)tb * 6 * 4);
@@ -859,7 +867,7 @@ size_t Plan::upload_bytes() const {
   auto b = [](const auto& v) { return v.size() * sizeof(v[0]); };
   return b(prob_pose_begin) + b(prob_point_begin) + b(prob_tr_begin) + b(prob_chunk_begin) +
          b(pose_prob) + b(point_prob) + b(slot_prob) + b(params) + b(pose_q) + b(pose_t) +
-         b(points) + b(pose_slot) + b(point_var) + b(cameras) + b(pt_off) + b(obs_pose) +
+         b(points) + b(pose_slot) + b(point_var) + b(cameras) + b(pt_off) + b(obs_point) + b(obs_pose) +
          b(obs_cam) + b(obs_slot) + b(obs_xy) + b(cam_off) + b(cam_obs) + b(tile_ij) +
          b(blk_off) + b(pairs) + b(blk_dst) + b(diag_dst) + b(dup_off) + b(dup_pairs) +
          b(tr_list_off) + b(tr_list) + b(tr_prob) + b(chunk_point_begin) + b(tile_slot) + b(tile_meta);

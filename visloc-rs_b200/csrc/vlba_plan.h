@@ -31,7 +31,7 @@ struct Plan {
   std::vector<uint8_t> point_var;
   std::vector<DevCamera> cameras;
 
-  std::vector<uint32_t> pt_off, obs_pose, obs_cam, obs_slot;
+  std::vector<uint32_t> pt_off, obs_point, obs_pose, obs_cam, obs_slot;
   std::vector<double> obs_xy;  // 2 per obs
   std::vector<uint32_t> cam_off, cam_obs;
 

@@ -290,6 +290,7 @@ void upload_plan_once(Context* c, uint32_t max_records) {
   d.pose_step = A.alloc<double>(npose);
   d.cameras = A.upload(P.cameras, s);
   d.pt_off = A.upload(P.pt_off, s);
+  d.obs_point = A.upload(P.obs_point, s);
   d.obs_pose = A.upload(P.obs_pose, s);
   d.obs_cam = A.upload(P.obs_cam, s);
   d.obs_slot = A.upload(P.obs_slot, s);
