@@ -1575,7 +1575,7 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
       if (own_m1[j] - own_m0[j] >= kBigRow) continue;
       const uint32_t P = own_prob[j];
       if (P != oprob) {
-        os = prob_scalars_warp(d, P, k);
+        os = (sc_prob == P && sc_k == k) ? sc : prob_scalars_warp(d, P, k);
         oprob = P;
       }
       if (!os.active) continue;
@@ -1643,7 +1643,9 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
       const uint32_t tr = blockIdx.x + j * G;
       const uint32_t P = own_prob[j];
       if (P != cprob) {
-        const ProbScal ps = prob_scalars_warp(d, P, k);
+        // The block's scalars of this iteration when they are this problem's
+        // (the single-problem case), else this warp's own.
+        const ProbScal ps = (sc_prob == P && sc_k == k) ? sc : prob_scalars_warp(d, P, k);
         double pq = 0.0;
         for (uint32_t t2 = d.prob_tr_begin[P] + lane; t2 < d.prob_tr_begin[P + 1]; t2 += 32)
           pq += __ldcg(dot_at(d, kDotPq + (k & 1), t2));
