@@ -8,7 +8,6 @@
 #include <exception>
 #include <stdexcept>
 #include <thread>
-#include <unordered_map>
 
 namespace vlba {
 
@@ -176,10 +175,76 @@ void run_threads(uint32_t n, F&& f) {
   if (err) std::rethrow_exception(err);
 }
 
+// Stable counting sort of the indices i in [0, n) by key(i) < m (kNone:
+// left out) on T threads over contiguous index ranges: order[] receives
+// value_base + i bucket after bucket, off[b] .. off[b + 1] bucket b's range.
+// The output does not depend on T.
+template <typename Key>
+void counting_sort(uint32_t n, uint32_t m, uint32_t T, Key key, uint32_t value_base,
+                   uint32_t* order, uint32_t* off) {
+  std::vector<std::vector<uint32_t>> tc(T, std::vector<uint32_t>(m, 0));
+  auto ilo = [&](uint32_t t) { return (uint32_t)((uint64_t)n * t / T); };
+  auto blo = [&](uint32_t t) { return (uint32_t)((uint64_t)m * t / T); };
+  run_threads(T, [&](uint32_t t) {
+    uint32_t* c = tc[t].data();
+    for (uint32_t i = ilo(t); i < ilo(t + 1); ++i) {
+      const uint32_t b = key(i);
+      if (b != kNone) ++c[b];
+    }
+  });
+  // Bucket totals per chunk of buckets, then each (bucket, range) start.
+  std::vector<uint64_t> csum(T + 1, 0);
+  run_threads(T, [&](uint32_t t) {
+    uint64_t s = 0;
+    for (uint32_t b = blo(t); b < blo(t + 1); ++b)
+      for (uint32_t u = 0; u < T; ++u) s += tc[u][b];
+    csum[t + 1] = s;
+  });
+  for (uint32_t t = 0; t < T; ++t) csum[t + 1] += csum[t];
+  run_threads(T, [&](uint32_t t) {
+    uint32_t run = (uint32_t)csum[t];
+    for (uint32_t b = blo(t); b < blo(t + 1); ++b) {
+      off[b] = run;
+      for (uint32_t u = 0; u < T; ++u) {
+        const uint32_t c = tc[u][b];
+        tc[u][b] = run;
+        run += c;
+      }
+    }
+  });
+  off[m] = (uint32_t)csum[T];
+  run_threads(T, [&](uint32_t t) {
+    uint32_t* c = tc[t].data();
+    for (uint32_t i = ilo(t); i < ilo(t + 1); ++i) {
+      const uint32_t b = key(i);
+      if (b != kNone) order[c[b]++] = value_base + i;
+    }
+  });
+}
+
 void build_plan_serial(const vlba_problem* const* problems, const vlba_config* const* configs,
                        uint32_t n, uint32_t tb, Plan* plan, uint32_t max_threads) {
   Plan& P = *plan;
-  P = Plan();
+  {
+    // A plan rebuilt in place keeps the memory of its largest arrays (their
+    // pages stay mapped, so the rebuild takes no page faults on them); their
+    // contents go.
+    Plan old = std::move(P);
+    P = Plan();
+    auto keep = [](auto& dst, auto& src) {
+      dst.swap(src);
+      dst.clear();
+    };
+    keep(P.pairs, old.pairs);
+    keep(P.dup_pairs, old.dup_pairs);
+    keep(P.scratch, old.scratch);
+    keep(P.obs_point, old.obs_point);
+    keep(P.obs_pose, old.obs_pose);
+    keep(P.obs_cam, old.obs_cam);
+    keep(P.obs_slot, old.obs_slot);
+    keep(P.obs_xy, old.obs_xy);
+    keep(P.cam_obs, old.cam_obs);
+  }
   P.tb = tb;
   P.num_problems = n;
   uint64_t tot_poses = 0, tot_points = 0, tot_obs = 0, tot_cams = 0;
@@ -254,74 +319,60 @@ void build_plan_serial(const vlba_problem* const* problems, const vlba_config* c
       if (var) ++P.var_points;
     }
     // Point-major observation order: stable counting sort by landmark.
+    // Observation-level passes run on up to max_threads threads (the
+    // per-thread landmark counts bound to 2^25 words).
+    const uint32_t To = std::max(1u, std::min<uint32_t>(max_threads, no / 200000));
+    const uint32_t Ts = std::max(1u, std::min<uint32_t>(To, (uint32_t)((32u << 20) / (nl + 1u))));
     std::vector<uint32_t> cnt(nl + 1, 0);
-    for (uint32_t o = 0; o < no; ++o) ++cnt[p->obs_landmark[o] + 1];
-    for (uint32_t j = 0; j < nl; ++j) cnt[j + 1] += cnt[j];
     std::vector<uint32_t> order(no);
-    {
-      std::vector<uint32_t> fill(cnt.begin(), cnt.end() - 1);
-      for (uint32_t o = 0; o < no; ++o) order[fill[p->obs_landmark[o]]++] = o;
-    }
-    for (uint32_t j = 0; j < nl; ++j) {
-      P.pt_off[point_base + j + 1] = obs_base + cnt[j + 1];
-      for (uint32_t k = cnt[j]; k < cnt[j + 1]; ++k) P.obs_point[obs_base + k] = point_base + j;
-    }
-    for (uint32_t k = 0; k < no; ++k) {
-      const uint32_t o = order[k];
-      const uint32_t g = obs_base + k;
-      const uint32_t pose = pose_base + p->obs_pose[o];
-      P.obs_pose[g] = pose;
-      P.obs_cam[g] = cam_base + (p->obs_camera ? p->obs_camera[o] : 0u);
-      P.obs_slot[g] = P.pose_slot[pose];
-      P.obs_xy[2 * (size_t)g] = p->obs_xy[2 * (size_t)o];
-      P.obs_xy[2 * (size_t)g + 1] = p->obs_xy[2 * (size_t)o + 1];
-    }
+    counting_sort(no, nl, Ts, [p](uint32_t o) { return p->obs_landmark[o]; }, 0u, order.data(),
+                  cnt.data());
+    run_threads(To, [&](uint32_t t) {
+      for (uint32_t j = (uint32_t)((uint64_t)nl * t / To); j < (uint32_t)((uint64_t)nl * (t + 1) / To); ++j) {
+        P.pt_off[point_base + j + 1] = obs_base + cnt[j + 1];
+        for (uint32_t k = cnt[j]; k < cnt[j + 1]; ++k) P.obs_point[obs_base + k] = point_base + j;
+      }
+      for (uint32_t k = (uint32_t)((uint64_t)no * t / To); k < (uint32_t)((uint64_t)no * (t + 1) / To); ++k) {
+        const uint32_t o = order[k];
+        const uint32_t g = obs_base + k;
+        const uint32_t pose = pose_base + p->obs_pose[o];
+        P.obs_pose[g] = pose;
+        P.obs_cam[g] = cam_base + (p->obs_camera ? p->obs_camera[o] : 0u);
+        P.obs_slot[g] = P.pose_slot[pose];
+        P.obs_xy[2 * (size_t)g] = p->obs_xy[2 * (size_t)o];
+        P.obs_xy[2 * (size_t)g + 1] = p->obs_xy[2 * (size_t)o + 1];
+      }
+    });
     // Per-slot observation lists (ascending point-major index).
-    {
-      std::vector<uint32_t> c2(nslots + 1, 0);
-      for (uint32_t k = 0; k < no; ++k) {
-        const uint32_t s = P.obs_slot[obs_base + k];
-        if (s != kNone) ++c2[s - slot_base + 1];
-      }
-      for (uint32_t s = 0; s < nslots; ++s) c2[s + 1] += c2[s];
-      const uint32_t list_base = (uint32_t)P.cam_obs.size();
-      P.cam_obs.resize(list_base + c2[nslots]);
-      std::vector<uint32_t> fill(c2.begin(), c2.end() - 1);
-      for (uint32_t k = 0; k < no; ++k) {
-        const uint32_t s = P.obs_slot[obs_base + k];
-        if (s != kNone) P.cam_obs[list_base + fill[s - slot_base]++] = obs_base + k;
-      }
-      for (uint32_t s = 0; s < nslots; ++s) P.cam_off.push_back(list_base + c2[s + 1]);
-    }
-    // Camera pairs sharing a variable point: block (i, j), i > j (local
-    // slots).  Counted in a dense nvar x nvar table (sparse map beyond).
-    const uint64_t nv64 = nvar;
-    const bool dense_table = nv64 * nv64 <= (64ull << 20);
-    std::vector<uint32_t> table;
-    std::unordered_map<uint64_t, uint32_t> map;
-    if (dense_table) table.assign(nv64 * nv64, 0);
-    auto key_count = [&](uint32_t i, uint32_t j) -> uint32_t& {
-      if (dense_table) return table[(uint64_t)i * nv64 + j];
-      return map[(uint64_t)i * nv64 + j];
-    };
-    std::vector<uint32_t> dup_cnt(nslots + 1, 0);
-    // With a dense table and enough pairs, the points are split into T
-    // contiguous ranges counted (and later scattered) on T threads, each into
-    // its own table; per-thread offsets keep every block's list in point
-    // order, as the one-thread build has it.
+    std::vector<uint32_t> c2(nslots + 1, 0);
+    const uint32_t list_base = (uint32_t)P.cam_obs.size();
+    P.cam_obs.resize(list_base + (size_t)no);
+    counting_sort(no, nslots, To, [&](uint32_t k) {
+      const uint32_t s = P.obs_slot[obs_base + k];
+      return s == kNone ? kNone : s - slot_base;
+    }, obs_base, P.cam_obs.data() + list_base, c2.data());
+    P.cam_obs.resize(list_base + (size_t)c2[nslots]);
+    for (uint32_t s = 0; s < nslots; ++s) P.cam_off.push_back(list_base + c2[s + 1]);
+    // Camera pairs sharing a variable point: blocks (i, j), j < i (local
+    // slots), each holding its terms (x, y) -- x the observation in slot i,
+    // y the one in slot j -- in point order and, within a point, in the order
+    // of the loop "for a, for b < a" over the point's observations.  Points
+    // with enough work are split into T contiguous ranges, one per thread,
+    // in three passes that keep that order whatever T is: (A) count each
+    // row's terms per range; (B) scatter them row-major, ranges in order,
+    // with each term's column beside it; (C) per row, a stable counting sort
+    // by column.  A point's observations in one slot give that slot's
+    // same-camera terms, both orders.
     uint32_t T = 1;
     std::vector<uint32_t> range{0, nl};
-    if (dense_table && max_threads > 1) {
+    if (max_threads > 1) {
       std::vector<double> work(nl + 1, 0.0);
       for (uint32_t j = 0; j < nl; ++j) {
         const double t = (double)(cnt[j + 1] - cnt[j]);
         work[j + 1] = work[j] + t * t;
       }
-      const double table_bytes = (double)(nv64 * nv64) * 4.0;
-      if (work[nl] > 2e6) {
-        T = std::min<uint32_t>(max_threads, (uint32_t)std::max(1.0, (256.0 * (1 << 20)) / table_bytes));
-        T = std::max(1u, std::min<uint32_t>(T, (uint32_t)(work[nl] / 2e5)));
-      }
+      if (work[nl] > 2e6)
+        T = std::max(1u, std::min<uint32_t>({max_threads, nvar, (uint32_t)(work[nl] / 2e5)}));
       range.assign(T + 1, nl);
       range[0] = 0;
       for (uint32_t t = 1, j = 0; t < T; ++t) {
@@ -330,84 +381,124 @@ void build_plan_serial(const vlba_problem* const* problems, const vlba_config* c
         range[t] = j;
       }
     }
-    std::vector<std::vector<uint32_t>> ttab(T > 1 ? T : 0), tdup(T > 1 ? T : 0);
-    std::vector<uint64_t> tvar(T, 0);
-    auto count_points = [&](uint32_t t, uint32_t* tab, uint32_t* dup) {
+    // f(la, lb, a, b) for every pair a > b of variable-slot observations of a
+    // variable point in range t (local slots, local observation indices).
+    auto each_pair = [&](uint32_t t, auto&& f, uint64_t* var) {
       for (uint32_t j = range[t]; j < range[t + 1]; ++j) {
         if (!P.point_var[point_base + j]) continue;
         const uint32_t k0 = cnt[j], k1 = cnt[j + 1];
-        // Each unordered pair once; the observation of the larger slot first.
         for (uint32_t a = k0; a < k1; ++a) {
           const uint32_t sa = P.obs_slot[obs_base + a];
           if (sa == kNone) continue;
-          ++tvar[t];
+          if (var) ++*var;
           for (uint32_t b = k0; b < a; ++b) {
             const uint32_t sb = P.obs_slot[obs_base + b];
-            if (sb == kNone) continue;
-            if (sa > sb) {
-              if (tab) ++tab[(uint64_t)(sa - slot_base) * nv64 + (sb - slot_base)];
-              else ++key_count(sa - slot_base, sb - slot_base);
-            } else if (sb > sa) {
-              if (tab) ++tab[(uint64_t)(sb - slot_base) * nv64 + (sa - slot_base)];
-              else ++key_count(sb - slot_base, sa - slot_base);
-            } else {
-              dup[sa - slot_base + 1] += 2;  // both orders
-            }
+            if (sb != kNone) f(sa - slot_base, sb - slot_base, a, b);
           }
         }
       }
     };
-    if (T > 1) {
-      run_threads(T, [&](uint32_t t) {
-        ttab[t].assign(nv64 * nv64, 0);
-        tdup[t].assign(nslots + 1, 0);
-        count_points(t, ttab[t].data(), tdup[t].data());
-      });
-      run_threads(T, [&](uint32_t t) {  // merged counts, rows split over threads
-        for (uint64_t i = t; i < nv64; i += T)
-          for (uint64_t jj = 0; jj < i; ++jj) {
-            uint32_t sum = 0;
-            for (uint32_t u = 0; u < T; ++u) sum += ttab[u][i * nv64 + jj];
-            table[i * nv64 + jj] = sum;
-          }
-      });
-      for (uint32_t u = 0; u < T; ++u)
-        for (uint32_t q = 0; q <= nslots; ++q) dup_cnt[q] += tdup[u][q];
-    } else {
-      count_points(0, nullptr, dup_cnt.data());
-    }
+    // (A) per range: terms of each row, same-camera terms of each slot.
+    std::vector<std::vector<uint64_t>> tcnt(T, std::vector<uint64_t>(2 * (size_t)nvar, 0));
+    std::vector<uint64_t> tvar(T, 0);
+    run_threads(T, [&](uint32_t t) {
+      uint64_t* c = tcnt[t].data();
+      each_pair(t, [c, nvar](uint32_t la, uint32_t lb, uint32_t, uint32_t) {
+        if (la != lb) ++c[std::max(la, lb)];
+        else c[nvar + la] += 2;
+      }, &tvar[t]);
+    });
     for (uint32_t t = 0; t < T; ++t) P.var_obs += tvar[t];
+    // Row and slot ranges; per range, its start inside each (the counts
+    // become positions).
+    const uint64_t pair_base = P.pairs.size(), dup_base = P.dup_pairs.size();
+    std::vector<uint64_t> row_at(nvar + 1, pair_base), dup_at(nslots + 1, dup_base);
+    for (uint32_t i = 0; i < nvar; ++i) {
+      uint64_t at = row_at[i], d = dup_at[i];
+      for (uint32_t t = 0; t < T; ++t) {
+        const uint64_t c = tcnt[t][i], e = tcnt[t][nvar + i];
+        tcnt[t][i] = at;
+        tcnt[t][nvar + i] = d;
+        at += c;
+        d += e;
+      }
+      row_at[i + 1] = at;
+      dup_at[i + 1] = d;
+    }
+    for (uint32_t s = nvar; s < nslots; ++s) dup_at[s + 1] = dup_at[s];
+    if (row_at[nvar] >= kNone) throw std::runtime_error("more than 2^32 Schur terms");
+    if (dup_at[nslots] >= kNone) throw std::runtime_error("more than 2^32 same-camera terms");
+    P.pairs.resize(row_at[nvar]);
+    P.dup_pairs.resize(dup_at[nslots]);
+    for (uint32_t s = 0; s < nslots; ++s) P.dup_off.push_back((uint32_t)dup_at[s + 1]);
+    // (B) scatter, each term's column beside it.
+    auto& term_col = P.scratch;
+    term_col.resize(row_at[nvar] - pair_base);
+    run_threads(T, [&](uint32_t t) {
+      uint64_t* pos = tcnt[t].data();
+      uint64_t* dpos = pos + nvar;
+      each_pair(t, [&](uint32_t la, uint32_t lb, uint32_t a, uint32_t b) {
+        const uint32_t ga = obs_base + a, gb = obs_base + b;
+        if (la > lb) {
+          term_col[pos[la] - pair_base] = lb;
+          P.pairs[pos[la]++] = PairIdx{ga, gb};
+        } else if (lb > la) {
+          term_col[pos[lb] - pair_base] = la;
+          P.pairs[pos[lb]++] = PairIdx{gb, ga};
+        } else {
+          P.dup_pairs[dpos[la]++] = PairIdx{ga, gb};
+          P.dup_pairs[dpos[la]++] = PairIdx{gb, ga};
+        }
+      }, nullptr);
+    });
+    // (C) per row, a stable counting sort of its terms by column; the row's
+    // blocks are its distinct columns, ascending.
+    std::vector<std::vector<uint32_t>> row_col(nvar), row_count(nvar);
+    {
+      std::atomic<uint32_t> next{0};
+      run_threads(T, [&](uint32_t) {
+        std::vector<uint32_t> mark(nvar, 0), touched;
+        std::vector<uint64_t> at(nvar, 0);
+        std::vector<PairIdx> buf;
+        for (uint32_t i; (i = next.fetch_add(1)) < nvar;) {
+          const uint64_t lo = row_at[i], hi = row_at[i + 1];
+          touched.clear();
+          for (uint64_t k = lo; k < hi; ++k)
+            if (mark[term_col[k - pair_base]]++ == 0) touched.push_back(term_col[k - pair_base]);
+          std::sort(touched.begin(), touched.end());
+          row_col[i] = touched;
+          row_count[i].resize(touched.size());
+          uint64_t run = lo;
+          for (size_t b = 0; b < touched.size(); ++b) {
+            row_count[i][b] = mark[touched[b]];
+            at[touched[b]] = run;
+            run += mark[touched[b]];
+            mark[touched[b]] = 0;
+          }
+          if (touched.size() > 1) {
+            buf.assign(P.pairs.begin() + lo, P.pairs.begin() + hi);
+            for (uint64_t k = lo; k < hi; ++k) P.pairs[at[term_col[k - pair_base]]++] = buf[k - lo];
+          }
+        }
+      });
+    }
+    term_col.clear();
     // Blocks in row-major order; per-tile existence.
     const uint32_t ntr = nslots / tb;
     std::vector<uint8_t> tile_has((size_t)ntr * ntr, 0);
-    std::vector<uint64_t> keys;
-    if (dense_table) {
-      for (uint64_t i = 0; i < nv64; ++i)
-        for (uint64_t jj = 0; jj < i; ++jj)
-          if (table[i * nv64 + jj]) keys.push_back(i * nv64 + jj);
-    } else {
-      keys.reserve(map.size());
-      for (const auto& kv : map) keys.push_back(kv.first);
-      std::sort(keys.begin(), keys.end());
-    }
     const uint32_t blk_base = (uint32_t)P.blk_dst.size();
-    const uint32_t pair_base = (uint32_t)P.pairs.size();
-    std::vector<uint32_t> blk_fill(keys.size());
-    {
-      uint32_t run = pair_base;
-      for (size_t b = 0; b < keys.size(); ++b) {
-        const uint32_t i = (uint32_t)(keys[b] / nv64), jj = (uint32_t)(keys[b] % nv64);
-        tile_has[(size_t)(i / tb) * ntr + jj / tb] = 1;
-        uint32_t& c = key_count(i, jj);
-        const uint32_t count = c;
-        c = (uint32_t)b;  // table now maps key -> local block id
-        blk_fill[b] = run;
-        run += count;
-        P.blk_off.push_back(run);
+    std::vector<uint32_t> row_blk(nvar + 1, 0);  // first local block of each row
+    for (uint32_t i = 0; i < nvar; ++i) {
+      row_blk[i + 1] = row_blk[i] + (uint32_t)row_col[i].size();
+      uint64_t run = row_at[i];
+      for (size_t b = 0; b < row_col[i].size(); ++b) {
+        tile_has[(size_t)(i / tb) * ntr + row_col[i][b] / tb] = 1;
+        run += row_count[i][b];
+        P.blk_off.push_back((uint32_t)run);
       }
-      P.pairs.resize(run);
     }
-    P.camera_pairs += keys.size();
+    const uint32_t nblk = row_blk[nvar];
+    P.camera_pairs += nblk;
     for (uint32_t t = 0; t < ntr; ++t) tile_has[(size_t)t * ntr + t] = 1;
     // Compact tile ids, row-major.
     std::vector<uint32_t> tile_id((size_t)ntr * ntr, kNone);
@@ -420,85 +511,21 @@ void build_plan_serial(const vlba_problem* const* problems, const vlba_config* c
           P.tile_ij.push_back(((tr_base + I) << 16) | (tr_base + J));
         }
     // Block destinations.
-    P.blk_dst.resize(blk_base + keys.size());
-    for (size_t b = 0; b < keys.size(); ++b) {
-      const uint32_t i = (uint32_t)(keys[b] / nv64), jj = (uint32_t)(keys[b] % nv64);
-      const uint32_t I = i / tb, J = jj / tb, li = i % tb, lj = jj % tb;
-      const uint32_t t = tile_id[(size_t)I * ntr + J];
-      PairIdx dst;
-      dst.a = t * tile_floats + (li * tb + lj) * kBlock;
-      dst.b = (I == J) ? t * tile_floats + (lj * tb + li) * kBlock : kNone;
-      P.blk_dst[blk_base + b] = dst;
-    }
+    P.blk_dst.resize(blk_base + nblk);
+    for (uint32_t i = 0; i < nvar; ++i)
+      for (uint32_t b = row_blk[i]; b < row_blk[i + 1]; ++b) {
+        const uint32_t jj = row_col[i][b - row_blk[i]];
+        const uint32_t I = i / tb, J = jj / tb, li = i % tb, lj = jj % tb;
+        const uint32_t t = tile_id[(size_t)I * ntr + J];
+        PairIdx dst;
+        dst.a = t * tile_floats + (li * tb + lj) * kBlock;
+        dst.b = (I == J) ? t * tile_floats + (lj * tb + li) * kBlock : kNone;
+        P.blk_dst[blk_base + b] = dst;
+      }
     for (uint32_t s = 0; s < nslots; ++s) {
       const uint32_t I = s / tb, li = s % tb;
       P.diag_dst.push_back(tile_id[(size_t)I * ntr + I] * tile_floats + (li * tb + li) * kBlock);
     }
-    // Scatter the pairs, point by point (so each block's list is in point
-    // order), and the same-camera duplicates.
-    for (uint32_t s = 0; s < nslots; ++s) dup_cnt[s + 1] += dup_cnt[s];
-    const uint32_t dup_base = (uint32_t)P.dup_pairs.size();
-    P.dup_pairs.resize(dup_base + dup_cnt[nslots]);
-    std::vector<uint32_t> dup_fill(dup_cnt.begin(), dup_cnt.end() - 1);
-    // fill(t, i, j): the next pair position of block (i, j) for range t.
-    auto scatter_points = [&](uint32_t t, uint32_t* fill_tab, uint32_t* dfill) {
-      auto next = [&](uint32_t i, uint32_t jj) -> uint32_t& {
-        if (fill_tab) return fill_tab[(uint64_t)i * nv64 + jj];
-        return blk_fill[key_count(i, jj)];
-      };
-      for (uint32_t j = range[t]; j < range[t + 1]; ++j) {
-        if (!P.point_var[point_base + j]) continue;
-        const uint32_t k0 = cnt[j], k1 = cnt[j + 1];
-        for (uint32_t a = k0; a < k1; ++a) {
-          const uint32_t sa = P.obs_slot[obs_base + a];
-          if (sa == kNone) continue;
-          for (uint32_t b = k0; b < a; ++b) {
-            const uint32_t sb = P.obs_slot[obs_base + b];
-            if (sb == kNone) continue;
-            if (sa > sb) {
-              P.pairs[next(sa - slot_base, sb - slot_base)++] = PairIdx{obs_base + a, obs_base + b};
-            } else if (sb > sa) {
-              P.pairs[next(sb - slot_base, sa - slot_base)++] = PairIdx{obs_base + b, obs_base + a};
-            } else {
-              uint32_t& f = dfill[sa - slot_base];
-              P.dup_pairs[dup_base + f++] = PairIdx{obs_base + a, obs_base + b};
-              P.dup_pairs[dup_base + f++] = PairIdx{obs_base + b, obs_base + a};
-            }
-          }
-        }
-      }
-    };
-    if (T > 1) {
-      // Per-range start positions: block b's ranges in order, from blk_fill[b].
-      run_threads(T, [&](uint32_t t) {
-        for (uint64_t i = t; i < nv64; i += T)
-          for (uint64_t jj = 0; jj < i; ++jj) {
-            if (!table[i * nv64 + jj] && !ttab[0][i * nv64 + jj]) {
-              bool any = false;
-              for (uint32_t u = 1; u < T && !any; ++u) any = ttab[u][i * nv64 + jj] != 0;
-              if (!any) continue;
-            }
-            uint32_t at = blk_fill[table[i * nv64 + jj]];
-            for (uint32_t u = 0; u < T; ++u) {
-              const uint32_t c = ttab[u][i * nv64 + jj];
-              ttab[u][i * nv64 + jj] = at;
-              at += c;
-            }
-          }
-      });
-      for (uint32_t s = 0, q = 0; s < nslots; ++s) {
-        uint32_t at = dup_fill[s];
-        for (uint32_t u = 0; u < T; ++u) {
-          q = tdup[u][s + 1];
-          tdup[u][s + 1] = at;
-          at += q;
-        }
-      }
-      run_threads(T, [&](uint32_t t) { scatter_points(t, ttab[t].data(), tdup[t].data() + 1); });
-    } else {
-      scatter_points(0, nullptr, dup_fill.data());
-    }
-    for (uint32_t s = 0; s < nslots; ++s) P.dup_off.push_back(dup_base + dup_cnt[s + 1]);
     // Tile-row partial lists: row sides (I, J <= I), then column sides (K > I, I).
     for (uint32_t I = 0; I < ntr; ++I) {
       for (uint32_t J = 0; J <= I; ++J) {
@@ -775,6 +802,23 @@ void build_plan(const vlba_problem* const* problems, const vlba_config* const* c
   merge_plans(ptrs, plan);
 }
 
+// True when pred(i) holds for every i in [0, n); long ranges are checked on
+// the host's threads.
+template <typename F>
+bool all_of_range(uint64_t n, F&& pred) {
+  const uint64_t hw = std::max(1u, std::thread::hardware_concurrency());
+  const uint32_t T = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(hw, n >> 20));
+  std::atomic<bool> ok{true};
+  run_threads(T, [&](uint32_t t) {
+    for (uint64_t i = n * t / T, e = n * (t + 1) / T; i < e; ++i)
+      if (!pred(i)) {
+        ok = false;
+        return;
+      }
+  });
+  return ok;
+}
+
 std::string check_plan(const Plan& P) {
   const uint64_t nposes = P.pose_prob.size(), npts = P.point_prob.size(),
                  nobs = P.obs_pose.size(), ncam = P.cameras.size(), nslots = P.num_var_cams;
@@ -782,33 +826,32 @@ std::string check_plan(const Plan& P) {
   const uint64_t tile_floats = (uint64_t)P.tb * P.tb * kBlock;
   auto bad = [](const char* what) { return std::string("plan check failed: ") + what; };
   if (P.pt_off.size() != npts + 1 || P.pt_off.back() != nobs) return bad("pt_off");
-  for (uint64_t j = 0; j < npts; ++j)
-    if (P.pt_off[j] > P.pt_off[j + 1]) return bad("pt_off order");
+  if (!all_of_range(npts, [&](uint64_t j) { return P.pt_off[j] <= P.pt_off[j + 1]; }))
+    return bad("pt_off order");
   if (P.obs_cam.size() != nobs || P.obs_slot.size() != nobs || P.obs_xy.size() != 2 * nobs ||
       P.obs_point.size() != nobs)
     return bad("obs sizes");
-  for (uint64_t k = 0; k < nobs; ++k) {
-    const uint32_t l = P.obs_point[k];
-    if (l >= npts || P.pt_off[l] > k || P.pt_off[l + 1] <= k) return bad("obs_point");
-    if (P.obs_pose[k] >= nposes) return bad("obs_pose");
-    if (P.obs_cam[k] >= ncam) return bad("obs_cam");
-    if (P.obs_slot[k] != kNone && P.obs_slot[k] >= nslots) return bad("obs_slot");
-  }
+  if (!all_of_range(nobs, [&](uint64_t k) {
+        const uint32_t l = P.obs_point[k];
+        return l < npts && P.pt_off[l] <= k && P.pt_off[l + 1] > k && P.obs_pose[k] < nposes &&
+               P.obs_cam[k] < ncam && (P.obs_slot[k] == kNone || P.obs_slot[k] < nslots);
+      }))
+    return bad("observation arrays");
   for (uint64_t i = 0; i < nposes; ++i)
     if (P.pose_slot[i] != kNone && P.pose_slot[i] >= nslots) return bad("pose_slot");
   if (P.cam_off.size() != nslots + 1 || P.cam_off.back() != P.cam_obs.size()) return bad("cam_off");
   for (uint64_t s = 0; s < nslots; ++s)
     if (P.cam_off[s] > P.cam_off[s + 1]) return bad("cam_off order");
-  for (uint32_t k : P.cam_obs)
-    if (k >= nobs) return bad("cam_obs");
+  if (!all_of_range(P.cam_obs.size(), [&](uint64_t q) { return P.cam_obs[q] < nobs; }))
+    return bad("cam_obs");
   if (P.slot_prob.size() != nslots || nslots != (uint64_t)P.num_tile_rows * P.tb)
     return bad("slots");
   if (P.blk_off.size() != P.blk_dst.size() + 1 || P.blk_off.back() != P.pairs.size())
     return bad("blk_off");
   for (size_t b = 0; b + 1 < P.blk_off.size(); ++b)
     if (P.blk_off[b] > P.blk_off[b + 1]) return bad("blk_off order");
-  for (const PairIdx& pr : P.pairs)
-    if (pr.a >= nobs || pr.b >= nobs) return bad("pairs");
+  if (!all_of_range(P.pairs.size(), [&](uint64_t q) { return P.pairs[q].a < nobs && P.pairs[q].b < nobs; }))
+    return bad("pairs");
   for (const PairIdx& d : P.blk_dst) {
     if ((uint64_t)d.a + kBlock > ntiles * tile_floats) return bad("blk_dst");
     if (d.b != kNone && (uint64_t)d.b + kBlock > ntiles * tile_floats) return bad("blk_dst mirror");
@@ -817,8 +860,9 @@ std::string check_plan(const Plan& P) {
   for (uint32_t d : P.diag_dst)
     if ((uint64_t)d + kBlock > ntiles * tile_floats) return bad("diag_dst");
   if (P.dup_off.size() != nslots + 1 || P.dup_off.back() != P.dup_pairs.size()) return bad("dup_off");
-  for (const PairIdx& pr : P.dup_pairs)
-    if (pr.a >= nobs || pr.b >= nobs) return bad("dup_pairs");
+  if (!all_of_range(P.dup_pairs.size(),
+                    [&](uint64_t q) { return P.dup_pairs[q].a < nobs && P.dup_pairs[q].b < nobs; }))
+    return bad("dup_pairs");
   for (uint32_t ij : P.tile_ij)
     if ((ij >> 16) >= P.num_tile_rows || (ij & 0xFFFFu) > (ij >> 16)) return bad("tile_ij");
   if (P.tr_list_off.size() != (uint64_t)P.num_tile_rows + 1 || P.tr_list_off.back() != P.tr_list.size())

@@ -5,7 +5,10 @@
 #pragma once
 
 #include <cstdint>
+#include <memory>
+#include <new>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "vlba_common.cuh"
@@ -15,6 +18,29 @@ namespace vlba {
 struct PairIdx {
   uint32_t a, b;
 };
+
+// Allocator whose resize() leaves new elements uninitialised, for the large
+// pair arrays that the builder sizes first and then writes in full (from
+// several threads, which then also take the page faults).
+template <typename T>
+struct NoInit : std::allocator<T> {
+  template <typename U>
+  struct rebind {
+    using other = NoInit<U>;
+  };
+  NoInit() noexcept = default;
+  template <typename U>
+  NoInit(const NoInit<U>&) noexcept {}
+  template <typename U>
+  void construct(U* p) noexcept {
+    ::new (static_cast<void*>(p)) U;
+  }
+  template <typename U, typename... A>
+  void construct(U* p, A&&... a) {
+    ::new (static_cast<void*>(p)) U(std::forward<A>(a)...);
+  }
+};
+using PairList = std::vector<PairIdx, NoInit<PairIdx>>;
 
 struct Plan {
   uint32_t tb = 16;
@@ -39,15 +65,19 @@ struct Plan {
   uint32_t num_tile_rows = 0;
   std::vector<uint32_t> tile_ij;
   std::vector<uint32_t> blk_off;
-  std::vector<PairIdx> pairs;
+  PairList pairs;  // per block, its (row-slot observation, column-slot observation) terms
   std::vector<PairIdx> blk_dst;
   std::vector<uint32_t> diag_dst;
   std::vector<uint32_t> dup_off;
-  std::vector<PairIdx> dup_pairs;
+  PairList dup_pairs;
   std::vector<uint32_t> tr_list_off, tr_list, tr_prob;
   std::vector<PairIdx> tile_slot;  // per tile: partial slot of its row side, column side
   std::vector<uint32_t> tile_meta;  // per tile: ij, row slot, column slot (or kNone), problem
   std::vector<uint32_t> chunk_point_begin;
+
+  // Builder working memory (each term's column), kept with the plan so that
+  // a rebuild in place reuses its pages; never uploaded.
+  std::vector<uint32_t, NoInit<uint32_t>> scratch;
 
   // statistics (per plan)
   uint64_t real_var_cams = 0;

@@ -102,8 +102,8 @@ class Arena {
     bytes_ += need;
     return static_cast<T*>(p);
   }
-  template <typename T>
-  T* upload(const std::vector<T>& v, cudaStream_t s) {
+  template <typename T, typename A>
+  T* upload(const std::vector<T, A>& v, cudaStream_t s) {
     T* p = alloc<T>(v.size());
     if (!v.empty()) VLBA_CUDA(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s));
     return p;
