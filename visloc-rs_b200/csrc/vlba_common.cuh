@@ -196,9 +196,8 @@ struct Dev {
   const uint32_t* tr_list;     // partial indices (tile * 2 + side)
   const uint32_t* tr_prob;     // [num_tile_rows]
   double* dots;                // [16 * num_tile_rows]
-  unsigned int* row_cnt;       // [num_tile_rows] tile arrivals per row (PCG)
   uint32_t l2_resident_tiles;  // tiles [0, n) are streamed with L2 evict_last
-  unsigned int* barrier;       // [kBarrierWords]: top count, generation, active
+  unsigned int* barrier;       // [kBarrierWords]: [0] grid-barrier arrivals, [2] active problems
                                // problems, -, group counts
   unsigned int* error;         // [1] device error flags
   // Optional PCG phase trace (globaltimer ns): [iteration][block][kTracePhases]
@@ -212,7 +211,7 @@ struct Dev {
   double* chunk_step;
 };
 
-constexpr int kBarrierWords = 4 + 256;  // grid barrier state (up to 4096 blocks)
+constexpr int kBarrierWords = 4;  // PCG grid-barrier and active-count words
 constexpr int kTracePhases = 6;
 constexpr int kTraceIters = 64;
 

@@ -970,12 +970,6 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, unsign
   return true;
 }
 
-__device__ __forceinline__ unsigned int atom_add_acq_rel(unsigned int* a, unsigned int v) {
-  unsigned int old;
-  asm volatile("atom.add.acq_rel.gpu.u32 %0, [%1], %2;" : "=r"(old) : "l"(a), "r"(v) : "memory");
-  return old;
-}
-
 __device__ __forceinline__ void red_add_release(unsigned int* a, unsigned int v) {
   asm volatile("red.add.release.gpu.u32 [%0], %1;" ::"l"(a), "r"(v) : "memory");
 }
@@ -986,40 +980,26 @@ __device__ __forceinline__ unsigned int ld_acquire(const unsigned int* a) {
   return v;
 }
 
-// Two-level counting grid barrier with a bounded spin: blocks arrive on one
-// of the group counters (kBarGroup blocks each) with acquire-release
-// atomics; the last arrival of a group arrives on the top counter, whose last
-// arrival publishes the next generation.  Every block tracks the generation
-// it waits for (`gen`, starting from the value at launch), so the wait needs
-// no read before the arrival.  Returns false when any block has flagged an
-// error (every thread of the block sees the same value).  Layout of `bar`:
-// [0] top count, [1] generation, [4 + g] group counts.
-constexpr unsigned int kBarGroup = 16u;
-
+// Grid barrier on one arrival counter, bar[0], zeroed by k_pcg_setup before
+// every launch: each block's arrival is a release reduction (no round trip),
+// then its thread 0 polls with acquire loads, bounded in time, until the
+// count reaches nblocks times the block's generation `gen` (the barriers it
+// has passed, counted from the launch).  Returns false when any block has
+// flagged an error (every thread of the block sees the same value).
 __device__ bool grid_barrier(unsigned int* bar, unsigned int nblocks, unsigned int* err,
                              unsigned int* s_flag, unsigned int& gen) {
   __syncthreads();
   ++gen;
   if (threadIdx.x == 0) {
-    const unsigned int g = blockIdx.x / kBarGroup;
-    const unsigned int ngroups = (nblocks + kBarGroup - 1) / kBarGroup;
-    const unsigned int in_group = min(kBarGroup, nblocks - g * kBarGroup);
-    bool top = false;
-    if (atom_add_acq_rel(bar + 4 + g, 1u) + 1u == in_group) {
-      bar[4 + g] = 0u;  // nobody touches it again before the release
-      top = atom_add_acq_rel(bar, 1u) + 1u == ngroups;
-    }
-    if (top) {
-      bar[0] = 0u;
-      asm volatile("st.release.gpu.u32 [%0], %1;" ::"l"(bar + 1), "r"(gen) : "memory");
-    } else {
+    red_add_release(bar, 1u);
+    const unsigned int target = gen * nblocks;
+    if ((int)(ld_acquire(bar) - target) < 0) {
       const unsigned long long t_end = now_ns() + kWaitLimitNs;
-      while (ld_acquire(bar + 1) != gen) {
+      while ((int)(ld_acquire(bar) - target) < 0) {
         if (now_ns() > t_end) {
           atomicOr(err, (unsigned int)kErrBarrierTimeout);
           break;
         }
-        __nanosleep(8);
       }
     }
     *s_flag = *(volatile unsigned int*)err;
@@ -1153,6 +1133,50 @@ __device__ __forceinline__ double block_sum_fast(double v, double* red) {
   return t;
 }
 
+// A partial slot holds kSlotEmpty -- a NaN bit pattern that FP32 arithmetic
+// never produces (it returns the canonical NaN) -- in every entry until the
+// warp of its tile stores the partial.  The owner of the slot's tile row
+// reads it once no entry is empty and empties it again for the next
+// iteration; the grid barriers between that store and the next iteration's
+// partial stores order the two.
+constexpr uint32_t kSlotEmpty = 0xFFC0DEADu;
+
+// Wait (bounded) until the U x 2 entries v[u][e] -- loaded from src(u) + 32 e
+// where valid(u, e) -- are all filled, reloading the empty ones; then empty
+// the slots' entries.  Warp-collective.
+template <int U, typename Src, typename Valid>
+__device__ __forceinline__ void take_slots(float (&v)[U][2], Src src, Valid valid,
+                                           unsigned int* err) {
+  auto missing = [&]() {
+    bool miss = false;
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+#pragma unroll
+      for (int e = 0; e < 2; ++e)
+        if (valid(u, e) && __float_as_uint(v[u][e]) == kSlotEmpty) miss = true;
+    return miss;
+  };
+  if (__any_sync(0xffffffffu, missing())) {
+    const unsigned long long t_end = now_ns() + kWaitLimitNs;
+    do {
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+#pragma unroll
+        for (int e = 0; e < 2; ++e)
+          if (valid(u, e) && __float_as_uint(v[u][e]) == kSlotEmpty) v[u][e] = __ldcg(src(u) + 32 * e);
+      if (__any_sync(0xffffffffu, now_ns() > t_end)) {
+        if ((threadIdx.x & 31u) == 0) atomicOr(err, (unsigned int)kErrBarrierTimeout);
+        break;
+      }
+    } while (__any_sync(0xffffffffu, missing()));
+  }
+#pragma unroll
+  for (int u = 0; u < U; ++u)
+#pragma unroll
+    for (int e = 0; e < 2; ++e)
+      if (valid(u, e)) __stcg(src(u) + 32 * e, __uint_as_float(kSlotEmpty));
+}
+
 __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
   using C = Pcg;
   constexpr int NW = C::kWarps;
@@ -1174,7 +1198,11 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
 
   const uint32_t G = gridDim.x;
   const uint32_t TW = G * NW;  // warps in the grid
-  const uint32_t gw = blockIdx.x * NW + warp;
+  // Warps are numbered from the last block down, so the blocks that own one
+  // tile row more than others (the first ones) get the warps with one tile
+  // fewer.
+  const uint32_t gw0 = (G - 1u - blockIdx.x) * NW;
+  const uint32_t gw = gw0 + warp;
   const uint32_t ntiles = d.num_tiles;
   // This warp's tiles: gw + m TW, m < Mw, in the same order each iteration.
   const uint32_t Mw = gw < ntiles ? (ntiles - 1 - gw) / TW + 1 : 0u;
@@ -1237,7 +1265,7 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
     own_prob[tid] = d.tr_prob[R];
   }
   auto ownrow = [&](uint32_t j) -> float* { return own + (size_t)j * C::kOwnFloats; };
-  unsigned int bar_gen = *(volatile unsigned int*)(d.barrier + 1);
+  unsigned int bar_gen = 0u;  // barriers passed in this launch (the counter starts at 0)
 
   // Fixed-order reduction of tile row R: warp w sums slots m0 + w + j NW
   // (contiguous kRow floats, coalesced, kBatch in flight), in slot order;
@@ -1247,21 +1275,25 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
     const uint32_t R = blockIdx.x + (uint32_t)j * G;
     const uint32_t m0 = own_m0[j], m1 = own_m1[j];
     constexpr int kPer = (C::kRow + 31) / 32;
-    constexpr int kBatch = 24;  // 24 slots per warp in flight: one round for 192 slots
+    constexpr int kBatch = 20;  // 20 slots per warp in flight: one round for 160 slots
     float acc[kPer];
 #pragma unroll
     for (int e = 0; e < kPer; ++e) acc[e] = 0.0f;
+    static_assert(kPer == 2, "two entries per lane");
     for (uint32_t m = m0 + warp; m < m1; m += kBatch * NW) {
       float v[kBatch][kPer];
+      float* const base = d.partial + (size_t)m * C::kRow + lane;
+      auto src = [&](int u) { return base + (size_t)u * NW * C::kRow; };
 #pragma unroll
       for (int u = 0; u < kBatch; ++u) {
         const uint32_t slot = m + u * NW;
-        const float* src = d.partial + (size_t)slot * C::kRow;
 #pragma unroll
         for (int e = 0; e < kPer; ++e)
-          v[u][e] = (slot < m1 && lane + 32 * e < (uint32_t)C::kRow) ? __ldcg(src + lane + 32 * e)
-                                                                    : 0.0f;
+          v[u][e] = (slot < m1 && lane + 32 * e < (uint32_t)C::kRow) ? __ldcg(src(u) + 32 * e) : 0.0f;
       }
+      take_slots<kBatch>(v, src, [&](int u, int e) {
+        return m + u * NW < m1 && lane + 32 * e < (uint32_t)C::kRow;
+      }, d.error);
 #pragma unroll
       for (int u = 0; u < kBatch; ++u)
 #pragma unroll
@@ -1287,10 +1319,7 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
       pq = (double)pv * (double)q;
     }
     pq = block_sum_fast<NW>(pq, red);
-    if (tid == 0) {
-      *dot_at(d, kDotPq + (k & 1), R) = pq;
-      d.row_cnt[R] = 0u;  // every tile of row R has arrived this iteration
-    }
+    if (tid == 0) *dot_at(d, kDotPq + (k & 1), R) = pq;
   };
 
   // Row-local steps run one warp per owned row (row j on warp j mod NW),
@@ -1341,9 +1370,14 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
       *dot_at(d, kDotRr + mod3(-1), tr) = bb;
       *dot_at(d, kDotPq + 1, tr) = 1.0;
       *dot_at(d, kDotB2, tr) = bb;
-      d.row_cnt[tr] = 0u;
     }
     __syncwarp();
+  }
+  // Every partial slot starts empty.
+  {
+    const size_t n = (size_t)d.tr_list_off[d.num_tile_rows] * C::kRow;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + tid; i < n; i += (size_t)G * blockDim.x)
+      __stcg(d.partial + i, __uint_as_float(kSlotEmpty));
   }
   // The metadata of the warp's first two tiles (the same every iteration).
   const uint4 meta0 = Mw > 0 ? d.tile_meta[gw] : make_uint4(0u, 0u, 0u, 0u);
@@ -1379,8 +1413,7 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
     // The block computes the scalars of its first tile's problem once; warps
     // whose tile is of that problem read them from shared memory.
     if (NW > 0) {
-      const uint32_t b0 = blockIdx.x * NW;
-      if (b0 < ntiles) scal(d.tile_meta[b0].w, k);
+      if (gw0 < ntiles) scal(d.tile_meta[gw0].w, k);
     }
     trace_mark(d, k, 1);
     {
@@ -1406,7 +1439,6 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
       ws.active = 0;
       ws.beta = 0.0;
       uint4 meta_cur = meta0, meta_nxt = meta1;
-      uint64_t done_mask = 0;  // tiles m < 64 processed this iteration
       if (Mw > 0) prefetch_seg(meta_cur.x);
       trace_warp(d, k, gw, TW, 0);
       for (uint32_t m = 0; m < Mw; ++m) {
@@ -1465,8 +1497,17 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
               sv[4 * q + 2] = v.z;
               sv[4 * q + 3] = v.w;
             }
-            const float* pj = wPJ + lj * 6;
-            const float* pi = wPI + (li + 4 * h) * 6;
+            // The segments' six entries as three 8-byte shared loads.
+            float pj[6], pi[6];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+              const float2 vj = reinterpret_cast<const float2*>(wPJ + lj * 6)[c];
+              const float2 vi = reinterpret_cast<const float2*>(wPI + (li + 4 * h) * 6)[c];
+              pj[2 * c] = vj.x;
+              pj[2 * c + 1] = vj.y;
+              pi[2 * c] = vi.x;
+              pi[2 * c + 1] = vi.y;
+            }
 #pragma unroll
             for (int a = 0; a < 6; ++a) {
               float acc = 0.0f;
@@ -1482,40 +1523,61 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
               col[c] += acc;
             }
           }
-          // Row sides: over lj (the 8 lanes of a row group) by butterfly.
+          // Row sides: sums over lj (lane bits 0-2) by a reduce-scatter
+          // butterfly -- offsets 4, 2, 1, each lane keeping the half its bit
+          // selects -- so every lane ends with one or two finished entries
+          // (the sums of an all-reduce butterfly, in the same order).
+          // Lane bit 2 picks h, bit 1 the entries a = 0-2 or 3-5, bit 0 the
+          // first two of those or the third.
+          const bool b2 = (lane >> 2) & 1u, b1 = (lane >> 1) & 1u, b0 = lane & 1u;
+          float rs[6];
 #pragma unroll
-          for (int off = 4; off > 0; off >>= 1)
-#pragma unroll
-            for (int h = 0; h < 2; ++h)
-#pragma unroll
-              for (int a = 0; a < 6; ++a)
-                row[h][a] += __shfl_xor_sync(0xffffffffu, row[h][a], off, 8);
-          float* part = d.partial + (size_t)meta.y * C::kRow;
-          if (lj == 0) {
-#pragma unroll
-            for (int h = 0; h < 2; ++h)
-#pragma unroll
-              for (int a = 0; a < 6; ++a) part[(li + 4 * h) * 6 + a] = row[h][a];
+          for (int a = 0; a < 6; ++a) {
+            const float keep = b2 ? row[1][a] : row[0][a];
+            const float send = b2 ? row[0][a] : row[1][a];
+            rs[a] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
           }
-          if (I != J) {
-            // Column side: over li -- the lanes of equal lj, by butterfly.
+          float r3[3];
 #pragma unroll
-            for (int off = 8; off < 32; off <<= 1)
-#pragma unroll
-              for (int c = 0; c < 6; ++c) col[c] += __shfl_xor_sync(0xffffffffu, col[c], off);
-            if (li == 0) {
-              float* partc = d.partial + (size_t)meta.z * C::kRow;
-#pragma unroll
-              for (int c = 0; c < 6; ++c) partc[lj * 6 + c] = col[c];
+          for (int a = 0; a < 3; ++a) {
+            const float keep = b1 ? rs[a + 3] : rs[a];
+            const float send = b1 ? rs[a] : rs[a + 3];
+            r3[a] = keep + __shfl_xor_sync(0xffffffffu, send, 2);
+          }
+          // Bit 0: the even lane keeps entries 0 and 1 of the three, the odd
+          // lane entry 2.
+          const float x0 = __shfl_xor_sync(0xffffffffu, b0 ? r3[0] : r3[2], 1);
+          const float x1 = __shfl_xor_sync(0xffffffffu, r3[1], 1);
+          float* part = d.partial + (size_t)meta.y * C::kRow;
+          {
+            const int base = (li + 4 * (int)b2) * 6 + 3 * (int)b1;
+            if (b0) {
+              part[base + 2] = r3[2] + x0;
+            } else {
+              part[base] = r3[0] + x0;
+              part[base + 1] = r3[1] + x1;
             }
           }
-          if (m < 64u) {
-            done_mask |= 1ull << m;
-          } else {
-            __syncwarp();
-            if (lane == 0) {
-              red_add_release(d.row_cnt + I, 1u);
-              if (I != J) red_add_release(d.row_cnt + J, 1u);
+          if (I != J) {
+            // Column side: sums over li (lane bits 3-4), offsets 8 then 16:
+            // bit 3 picks the entries c = 0-2 or 3-5, bit 4 the first two
+            // of those or the third.
+            const bool b3 = (lane >> 3) & 1u, b4 = (lane >> 4) & 1u;
+            float c3[3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+              const float keep = b3 ? col[c + 3] : col[c];
+              const float send = b3 ? col[c] : col[c + 3];
+              c3[c] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+            }
+            const float y0 = __shfl_xor_sync(0xffffffffu, b4 ? c3[0] : c3[2], 16);
+            const float y1 = __shfl_xor_sync(0xffffffffu, c3[1], 16);
+            float* partc = d.partial + (size_t)meta.z * C::kRow + lj * 6 + 3 * (int)b3;
+            if (b4) {
+              partc[2] = c3[2] + y0;
+            } else {
+              partc[0] = c3[0] + y0;
+              partc[1] = c3[1] + y1;
             }
           }
         }
@@ -1528,43 +1590,14 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
         meta_nxt = meta_nn;
       }
       trace_warp(d, k, gw, TW, 1);
-      // Arrivals for the warp's first 64 tiles of this iteration (the rest
-      // arrived one by one above): after all of the warp's partial stores, a
-      // release fence in every lane, then relaxed increments on the rows each
-      // processed tile feeds, spread over the lanes.
-      __syncwarp();
-      if (done_mask) {
-        asm volatile("fence.acq_rel.gpu;" ::: "memory");
-        for (uint32_t m = lane; m < Mw && m < 64u; m += 32) {
-          if (!((done_mask >> m) & 1ull)) continue;
-          const uint4 meta = d.tile_meta[gw + m * TW];
-          const uint32_t I = meta.x >> 16, J = meta.x & 0xFFFFu;
-          atomicAdd(d.row_cnt + I, 1u);
-          if (I != J) atomicAdd(d.row_cnt + J, 1u);
-        }
-      }
     }
-    // Row reductions by their owners: wait, bounded, for every tile of the
-    // row to arrive, then reduce -- a row of many tiles by the whole block
-    // (its slots spread over the warps), the others one warp per row.
-    auto wait_row = [&](uint32_t j) {  // one thread
-      const uint32_t need = own_m1[j] - own_m0[j];
-      const uint32_t R = blockIdx.x + j * G;
-      const unsigned long long t_end = now_ns() + kWaitLimitNs;
-      while (ld_acquire(d.row_cnt + R) < need) {
-        if (now_ns() > t_end) {
-          atomicOr(d.error, (unsigned int)kErrBarrierTimeout);
-          break;
-        }
-        __nanosleep(8);
-      }
-    };
+    // Row reductions by their owners, each slot read as soon as it is
+    // filled: a row of many tiles by the whole block (its slots spread over
+    // the warps), the others one warp per row.
     for (uint32_t j = 0; j < nown; ++j) {
       if (own_m1[j] - own_m0[j] < kBigRow) continue;
       scal(own_prob[j], k);
       if (!sc.active) continue;
-      if (tid == 0) wait_row(j);
-      __syncthreads();
       reduce_row((int)j, k, sc.beta);
     }
     uint32_t oprob = kNone;
@@ -1579,25 +1612,24 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
         oprob = P;
       }
       if (!os.active) continue;
-      if (lane == 0) wait_row(j);
-      __syncwarp();
       // Slots in order, eight loads in flight per lane.
       const uint32_t R = blockIdx.x + j * G;
       const uint32_t m0 = own_m0[j], m1 = own_m1[j];
       float q0 = 0.0f, q1 = 0.0f;
       for (uint32_t m = m0; m < m1; m += 8) {
-        float v0[8], v1[8];
+        float v[8][2];
+        float* const base = d.partial + (size_t)m * C::kRow + lane;
+        auto src = [&](int u) { return base + u * C::kRow; };
 #pragma unroll
         for (int u = 0; u < 8; ++u) {
-          const uint32_t slot = m + u;
-          const float* src = d.partial + (size_t)slot * C::kRow;
-          v0[u] = slot < m1 ? __ldcg(src + lane) : 0.0f;
-          v1[u] = (slot < m1 && e1) ? __ldcg(src + 32 + lane) : 0.0f;
+          v[u][0] = m + u < m1 ? __ldcg(src(u)) : 0.0f;
+          v[u][1] = (m + u < m1 && e1) ? __ldcg(src(u) + 32) : 0.0f;
         }
+        take_slots<8>(v, src, [&](int u, int e) { return m + u < m1 && (e == 0 || e1); }, d.error);
 #pragma unroll
         for (int u = 0; u < 8; ++u) {
-          q0 += v0[u];
-          q1 += v1[u];
+          q0 += v[u][0];
+          q1 += v[u][1];
         }
       }
       float* o = ownrow(j);
@@ -1623,10 +1655,7 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
         pq += (double)pv * (double)q1;
       }
       pq = warp_sum(pq);
-      if (lane == 0) {
-        *dot_at(d, kDotPq + (k & 1), R) = pq;
-        d.row_cnt[R] = 0u;  // every tile of row R has arrived this iteration
-      }
+      if (lane == 0) *dot_at(d, kDotPq + (k & 1), R) = pq;
       __syncwarp();
     }
     trace_mark(d, k, 2);
@@ -1806,7 +1835,6 @@ __global__ void __launch_bounds__(1024) k_pcg_setup(Dev d) {
     mine += on ? 1u : 0u;
   }
   if (mine) atomicAdd(&active, mine);
-  for (uint32_t tr = threadIdx.x; tr < d.num_tile_rows; tr += blockDim.x) d.row_cnt[tr] = 0u;
   __syncthreads();
   for (int w = threadIdx.x; w < kBarrierWords; w += blockDim.x) d.barrier[w] = w == 2 ? active : 0u;
 }
@@ -1913,7 +1941,7 @@ int pcg_grid_size(int, int sm_count) {
   const cudaError_t e =
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg, Pcg::kThreads, Pcg::kSmem);
   if (e != cudaSuccess || per_sm <= 0) return 0;
-  return std::min(per_sm * sm_count, (kBarrierWords - 4) * (int)kBarGroup);
+  return per_sm * sm_count;
 }
 
 cudaError_t launch_pcg(const Dev& d, int grid, cudaStream_t s) {

@@ -333,8 +333,6 @@ void upload_plan_once(Context* c, uint32_t max_records) {
   d.tr_list = A.upload(P.tr_list, s);
   d.tr_prob = A.upload(P.tr_prob, s);
   d.dots = A.alloc<double>(9 * (size_t)(P.num_tile_rows ? P.num_tile_rows : 1));
-  d.row_cnt = A.alloc<unsigned int>(P.num_tile_rows ? P.num_tile_rows : 1);
-  VLBA_CUDA(cudaMemsetAsync(d.row_cnt, 0, 4 * (size_t)(P.num_tile_rows ? P.num_tile_rows : 1), s));
   d.l2_resident_tiles = l2_tiles(c, c->l2_fraction);
   d.trace = nullptr;
   if (std::getenv("VLBA_TRACE_PCG") && c->pcg_grid_hint > 0)
