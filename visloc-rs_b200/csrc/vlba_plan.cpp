@@ -664,107 +664,176 @@ void build_reduced_plan(uint32_t n, const uint32_t* edges, uint64_t ne, uint32_t
 
 void merge_plans(const std::vector<const Plan*>& parts, Plan* out) {
   Plan& P = *out;
-  P = Plan();
+  {
+    // As in a rebuild in place: the large arrays keep their memory.
+    Plan old = std::move(P);
+    P = Plan();
+    auto keep = [](auto& dst, auto& src) {
+      dst.swap(src);
+      dst.clear();
+    };
+    keep(P.pairs, old.pairs);
+    keep(P.dup_pairs, old.dup_pairs);
+    keep(P.obs_point, old.obs_point);
+    keep(P.obs_pose, old.obs_pose);
+    keep(P.obs_cam, old.obs_cam);
+    keep(P.obs_slot, old.obs_slot);
+    keep(P.obs_xy, old.obs_xy);
+    keep(P.cam_obs, old.cam_obs);
+  }
   if (parts.empty()) throw std::runtime_error("merge of no plans");
   P.tb = parts[0]->tb;
   P.group = parts[0]->group;
-  size_t tp = 0, tl = 0, to = 0;
-  for (const Plan* q : parts) {
-    if (q->tb != P.tb || q->group != P.group) throw std::runtime_error("plans of different shapes");
-    tp += q->pose_prob.size();
-    tl += q->point_prob.size();
-    to += q->obs_pose.size();
-  }
-  if (tp >= kNone || tl >= kNone || to >= kNone)
-    throw std::runtime_error("batch exceeds 2^32 poses, points or observations");
-  auto cat = [](auto& dst, const auto& src) { dst.insert(dst.end(), src.begin(), src.end()); };
   const uint32_t tf = P.tb * P.tb * kBlock;
-  uint32_t pose_b = 0, point_b = 0, obs_b = 0, slot_b = 0, tr_b = 0, tile_b = 0, cam_b = 0;
-  uint32_t pair_b = 0, dup_b = 0, camobs_b = 0, trl_b = 0, chunk_b = 0;
-  P.num_problems = 0;
-  P.prob_pose_begin = {0};
-  P.prob_point_begin = {0};
-  P.prob_obs_begin = {0};
-  P.prob_tr_begin = {0};
-  P.prob_chunk_begin = {0};
-  P.prob_camera_begin = {0};
-  P.pt_off = {0};
-  P.cam_off = {0};
-  P.blk_off = {0};
-  P.dup_off = {0};
-  P.tr_list_off = {0};
-  P.chunk_point_begin = {0};
-  for (const Plan* qp : parts) {
-    const Plan& Q = *qp;
-    for (uint32_t qi = 0; qi < Q.num_problems; ++qi) {
-      const uint32_t pi = P.num_problems + qi;
-      P.prob_pose_begin.push_back(pose_b + Q.prob_pose_begin[qi + 1]);
-      P.prob_point_begin.push_back(point_b + Q.prob_point_begin[qi + 1]);
-      P.prob_obs_begin.push_back(obs_b + Q.prob_obs_begin[qi + 1]);
-      P.prob_tr_begin.push_back(tr_b + Q.prob_tr_begin[qi + 1]);
-      P.prob_chunk_begin.push_back(chunk_b + Q.prob_chunk_begin[qi + 1]);
-      P.prob_camera_begin.push_back(cam_b + Q.prob_camera_begin[qi + 1]);
-      (void)pi;
-    }
-    const uint32_t pb = P.num_problems;
-    for (uint32_t v : Q.pose_prob) P.pose_prob.push_back(pb + v);
-    for (uint32_t v : Q.point_prob) P.point_prob.push_back(pb + v);
-    for (uint32_t v : Q.slot_prob) P.slot_prob.push_back(pb + v);
-    for (uint32_t v : Q.tr_prob) P.tr_prob.push_back(pb + v);
-    cat(P.params, Q.params);
-    cat(P.pose_q, Q.pose_q);
-    cat(P.pose_t, Q.pose_t);
-    cat(P.points, Q.points);
-    for (uint32_t v : Q.pose_slot) P.pose_slot.push_back(v == kNone ? kNone : slot_b + v);
-    cat(P.point_var, Q.point_var);
-    cat(P.cameras, Q.cameras);
-    for (size_t j = 1; j < Q.pt_off.size(); ++j) P.pt_off.push_back(obs_b + Q.pt_off[j]);
-    for (uint32_t v : Q.obs_point) P.obs_point.push_back(point_b + v);
-    for (uint32_t v : Q.obs_pose) P.obs_pose.push_back(pose_b + v);
-    for (uint32_t v : Q.obs_cam) P.obs_cam.push_back(cam_b + v);
-    for (uint32_t v : Q.obs_slot) P.obs_slot.push_back(v == kNone ? kNone : slot_b + v);
-    cat(P.obs_xy, Q.obs_xy);
-    for (size_t j = 1; j < Q.cam_off.size(); ++j) P.cam_off.push_back(camobs_b + Q.cam_off[j]);
-    for (uint32_t v : Q.cam_obs) P.cam_obs.push_back(obs_b + v);
-    for (uint32_t v : Q.tile_ij) {
-      const uint32_t I = (v >> 16) + tr_b, J = (v & 0xFFFFu) + tr_b;
-      if (I > 0xFFFFu || J > 0xFFFFu) throw std::runtime_error("more than 65535 tile rows");
-      P.tile_ij.push_back((I << 16) | J);
-    }
-    for (size_t j = 1; j < Q.blk_off.size(); ++j) P.blk_off.push_back(pair_b + Q.blk_off[j]);
-    for (const PairIdx& v : Q.pairs) P.pairs.push_back(PairIdx{obs_b + v.a, obs_b + v.b});
-    const uint64_t fo = (uint64_t)tile_b * tf;
-    if (fo + (uint64_t)Q.tile_ij.size() * tf >= kNone)
-      throw std::runtime_error("reduced systems exceed 2^32 floats");
-    for (const PairIdx& v : Q.blk_dst)
-      P.blk_dst.push_back(PairIdx{(uint32_t)(v.a + fo), v.b == kNone ? kNone : (uint32_t)(v.b + fo)});
-    for (uint32_t v : Q.diag_dst) P.diag_dst.push_back((uint32_t)(v + fo));
-    for (size_t j = 1; j < Q.dup_off.size(); ++j) P.dup_off.push_back(dup_b + Q.dup_off[j]);
-    for (const PairIdx& v : Q.dup_pairs) P.dup_pairs.push_back(PairIdx{obs_b + v.a, obs_b + v.b});
-    for (size_t j = 1; j < Q.tr_list_off.size(); ++j) P.tr_list_off.push_back(trl_b + Q.tr_list_off[j]);
-    for (uint32_t v : Q.tr_list) P.tr_list.push_back(v + 2 * tile_b);
-    for (size_t j = 1; j < Q.chunk_point_begin.size(); ++j)
-      P.chunk_point_begin.push_back(point_b + Q.chunk_point_begin[j]);
+  // Where each part starts in every concatenated array (prefix sums).
+  struct Base {
+    uint64_t prob, pose, point, obs, slot, tr, tile, cam, pair, dup, camobs, trl, chunk, blk;
+  };
+  const size_t np = parts.size();
+  std::vector<Base> at(np + 1);
+  at[0] = Base{};
+  for (size_t i = 0; i < np; ++i) {
+    const Plan& Q = *parts[i];
+    if (Q.tb != P.tb || Q.group != P.group) throw std::runtime_error("plans of different shapes");
+    Base b = at[i];
+    b.prob += Q.num_problems;
+    b.pose += Q.pose_prob.size();
+    b.point += Q.point_prob.size();
+    b.obs += Q.obs_pose.size();
+    b.slot += Q.num_var_cams;
+    b.tr += Q.num_tile_rows;
+    b.tile += Q.tile_ij.size();
+    b.cam += Q.cameras.size();
+    b.pair += Q.pairs.size();
+    b.dup += Q.dup_pairs.size();
+    b.camobs += Q.cam_obs.size();
+    b.trl += Q.tr_list.size();
+    b.chunk += Q.chunk_point_begin.size() - 1;
+    b.blk += Q.blk_dst.size();
+    at[i + 1] = b;
     P.real_var_cams += Q.real_var_cams;
     P.var_points += Q.var_points;
     P.var_obs += Q.var_obs;
     P.camera_pairs += Q.camera_pairs;
-    P.num_problems += Q.num_problems;
-    pose_b += (uint32_t)Q.pose_prob.size();
-    point_b += (uint32_t)Q.point_prob.size();
-    obs_b += (uint32_t)Q.obs_pose.size();
-    slot_b += Q.num_var_cams;
-    tr_b += Q.num_tile_rows;
-    tile_b += (uint32_t)Q.tile_ij.size();
-    cam_b += (uint32_t)Q.cameras.size();
-    pair_b += (uint32_t)Q.pairs.size();
-    dup_b += (uint32_t)Q.dup_pairs.size();
-    camobs_b += (uint32_t)Q.cam_obs.size();
-    trl_b += (uint32_t)Q.tr_list.size();
-    chunk_b += (uint32_t)Q.chunk_point_begin.size() - 1;
   }
-  P.num_var_cams = slot_b;
-  P.num_tile_rows = tr_b;
+  const Base& T = at[np];
+  if (T.pose >= kNone || T.point >= kNone || T.obs >= kNone)
+    throw std::runtime_error("batch exceeds 2^32 poses, points or observations");
+  if (T.pair >= kNone || T.dup >= kNone || T.camobs >= kNone)
+    throw std::runtime_error("batch exceeds 2^32 Schur terms");
+  if (T.tr > 0x10000u) throw std::runtime_error("more than 65535 tile rows");
+  if (T.tile * tf >= kNone) throw std::runtime_error("reduced systems exceed 2^32 floats");
+  P.num_problems = (uint32_t)T.prob;
+  P.num_var_cams = (uint32_t)T.slot;
+  P.num_tile_rows = (uint32_t)T.tr;
+  // Sized once; every part then writes its own ranges.
+  for (auto* v : {&P.prob_pose_begin, &P.prob_point_begin, &P.prob_obs_begin, &P.prob_tr_begin,
+                  &P.prob_chunk_begin, &P.prob_camera_begin})
+    v->assign(T.prob + 1, 0u);
+  P.pose_prob.resize(T.pose);
+  P.point_prob.resize(T.point);
+  P.slot_prob.resize(T.slot);
+  P.tr_prob.resize(T.tr);
+  P.params.resize(T.prob);
+  P.pose_q.resize(4 * T.pose);
+  P.pose_t.resize(3 * T.pose);
+  P.points.resize(3 * T.point);
+  P.pose_slot.resize(T.pose);
+  P.point_var.resize(T.point);
+  P.cameras.resize(T.cam);
+  P.pt_off.assign(T.point + 1, 0u);
+  P.obs_point.resize(T.obs);
+  P.obs_pose.resize(T.obs);
+  P.obs_cam.resize(T.obs);
+  P.obs_slot.resize(T.obs);
+  P.obs_xy.resize(2 * T.obs);
+  P.cam_off.assign(T.slot + 1, 0u);
+  P.cam_obs.resize(T.camobs);
+  P.tile_ij.resize(T.tile);
+  P.blk_off.assign(T.blk + 1, 0u);
+  P.pairs.resize(T.pair);
+  P.blk_dst.resize(T.blk);
+  P.diag_dst.resize(T.slot);
+  P.dup_off.assign(T.slot + 1, 0u);
+  P.dup_pairs.resize(T.dup);
+  P.tr_list_off.assign(T.tr + 1, 0u);
+  P.tr_list.resize(T.trl);
+  P.chunk_point_begin.assign(T.chunk + 1, 0u);
+  auto fill = [&](size_t i) {
+    const Plan& Q = *parts[i];
+    const Base& b = at[i];
+    const uint32_t prob_b = (uint32_t)b.prob, pose_b = (uint32_t)b.pose, point_b = (uint32_t)b.point,
+                   obs_b = (uint32_t)b.obs, slot_b = (uint32_t)b.slot, tr_b = (uint32_t)b.tr,
+                   tile_b = (uint32_t)b.tile, cam_b = (uint32_t)b.cam, pair_b = (uint32_t)b.pair,
+                   dup_b = (uint32_t)b.dup, camobs_b = (uint32_t)b.camobs, trl_b = (uint32_t)b.trl,
+                   chunk_b = (uint32_t)b.chunk, blk_b = (uint32_t)b.blk;
+    for (uint32_t qi = 0; qi < Q.num_problems; ++qi) {
+      const size_t o = (size_t)prob_b + qi + 1;
+      P.prob_pose_begin[o] = pose_b + Q.prob_pose_begin[qi + 1];
+      P.prob_point_begin[o] = point_b + Q.prob_point_begin[qi + 1];
+      P.prob_obs_begin[o] = obs_b + Q.prob_obs_begin[qi + 1];
+      P.prob_tr_begin[o] = tr_b + Q.prob_tr_begin[qi + 1];
+      P.prob_chunk_begin[o] = chunk_b + Q.prob_chunk_begin[qi + 1];
+      P.prob_camera_begin[o] = cam_b + Q.prob_camera_begin[qi + 1];
+      P.params[prob_b + qi] = Q.params[qi];
+    }
+    auto shift = [](auto& dst, size_t d0, const auto& src, uint32_t add) {
+      for (size_t k = 0; k < src.size(); ++k) dst[d0 + k] = src[k] + add;
+    };
+    auto shift_none = [](auto& dst, size_t d0, const auto& src, uint32_t add) {
+      for (size_t k = 0; k < src.size(); ++k) dst[d0 + k] = src[k] == kNone ? kNone : src[k] + add;
+    };
+    auto copy = [](auto& dst, size_t d0, const auto& src) {
+      if (!src.empty()) std::memcpy(&dst[d0], src.data(), src.size() * sizeof(src[0]));
+    };
+    // Offset arrays: entries 1.. of the part after the previous parts' entries.
+    auto shift_off = [](auto& dst, size_t d0, const auto& src, uint32_t add) {
+      for (size_t k = 1; k < src.size(); ++k) dst[d0 + k] = src[k] + add;
+    };
+    shift(P.pose_prob, pose_b, Q.pose_prob, prob_b);
+    shift(P.point_prob, point_b, Q.point_prob, prob_b);
+    shift(P.slot_prob, slot_b, Q.slot_prob, prob_b);
+    shift(P.tr_prob, tr_b, Q.tr_prob, prob_b);
+    copy(P.pose_q, 4 * (size_t)pose_b, Q.pose_q);
+    copy(P.pose_t, 3 * (size_t)pose_b, Q.pose_t);
+    copy(P.points, 3 * (size_t)point_b, Q.points);
+    shift_none(P.pose_slot, pose_b, Q.pose_slot, slot_b);
+    copy(P.point_var, point_b, Q.point_var);
+    copy(P.cameras, cam_b, Q.cameras);
+    shift_off(P.pt_off, point_b, Q.pt_off, obs_b);
+    shift(P.obs_point, obs_b, Q.obs_point, point_b);
+    shift(P.obs_pose, obs_b, Q.obs_pose, pose_b);
+    shift(P.obs_cam, obs_b, Q.obs_cam, cam_b);
+    shift_none(P.obs_slot, obs_b, Q.obs_slot, slot_b);
+    copy(P.obs_xy, 2 * (size_t)obs_b, Q.obs_xy);
+    shift_off(P.cam_off, slot_b, Q.cam_off, camobs_b);
+    shift(P.cam_obs, camobs_b, Q.cam_obs, obs_b);
+    for (size_t k = 0; k < Q.tile_ij.size(); ++k) {
+      const uint32_t v = Q.tile_ij[k];
+      P.tile_ij[tile_b + k] = (((v >> 16) + tr_b) << 16) | ((v & 0xFFFFu) + tr_b);
+    }
+    shift_off(P.blk_off, blk_b, Q.blk_off, pair_b);
+    for (size_t k = 0; k < Q.pairs.size(); ++k)
+      P.pairs[pair_b + k] = PairIdx{obs_b + Q.pairs[k].a, obs_b + Q.pairs[k].b};
+    const uint32_t fo = tile_b * tf;
+    for (size_t k = 0; k < Q.blk_dst.size(); ++k) {
+      const PairIdx& v = Q.blk_dst[k];
+      P.blk_dst[blk_b + k] = PairIdx{v.a + fo, v.b == kNone ? kNone : v.b + fo};
+    }
+    shift(P.diag_dst, slot_b, Q.diag_dst, fo);
+    shift_off(P.dup_off, slot_b, Q.dup_off, dup_b);
+    for (size_t k = 0; k < Q.dup_pairs.size(); ++k)
+      P.dup_pairs[dup_b + k] = PairIdx{obs_b + Q.dup_pairs[k].a, obs_b + Q.dup_pairs[k].b};
+    shift_off(P.tr_list_off, tr_b, Q.tr_list_off, trl_b);
+    shift(P.tr_list, trl_b, Q.tr_list, 2 * tile_b);
+    shift_off(P.chunk_point_begin, chunk_b, Q.chunk_point_begin, point_b);
+  };
+  const uint32_t nt = (uint32_t)std::max<size_t>(
+      1, std::min<size_t>({np, std::max(1u, std::thread::hardware_concurrency()), T.obs / 65536 + 1}));
+  std::atomic<size_t> next{0};
+  run_threads(nt, [&](uint32_t) {
+    for (size_t i; (i = next.fetch_add(1)) < np;) fill(i);
+  });
   P.num_pairs = P.pairs.size();
   finish_tiles(P);
 }

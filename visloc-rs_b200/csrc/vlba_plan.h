@@ -57,9 +57,15 @@ struct Plan {
   std::vector<uint8_t> point_var;
   std::vector<DevCamera> cameras;
 
-  std::vector<uint32_t> pt_off, obs_point, obs_pose, obs_cam, obs_slot;
-  std::vector<double> obs_xy;  // 2 per obs
-  std::vector<uint32_t> cam_off, cam_obs;
+  // Observation-scale arrays are sized first and then written in full, so
+  // their resize leaves them uninitialised.
+  template <typename T>
+  using ObsArray = std::vector<T, NoInit<T>>;
+  std::vector<uint32_t> pt_off;
+  ObsArray<uint32_t> obs_point, obs_pose, obs_cam, obs_slot;
+  ObsArray<double> obs_xy;  // 2 per obs
+  std::vector<uint32_t> cam_off;
+  ObsArray<uint32_t> cam_obs;
 
   uint32_t num_var_cams = 0;  // padded slots
   uint32_t num_tile_rows = 0;
