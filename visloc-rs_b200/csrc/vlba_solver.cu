@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -102,12 +103,6 @@ class Arena {
     bytes_ += need;
     return static_cast<T*>(p);
   }
-  template <typename T, typename A>
-  T* upload(const std::vector<T, A>& v, cudaStream_t s) {
-    T* p = alloc<T>(v.size());
-    if (!v.empty()) VLBA_CUDA(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s));
-    return p;
-  }
   void release() {
     for (void* p : ptrs_) cudaFree(p);
     ptrs_.clear();
@@ -169,6 +164,11 @@ struct Context {
   uint32_t graph_iters = 0;
   PcgGate* gate = nullptr;  // set for the slots of a server
   bool tuned = false;       // the launch shape of this upload has been chosen
+  // Pinned staging for uploads and downloads: two buffers of stage_cap bytes,
+  // each refilled once the device copy out of it (its event) has completed.
+  char* stage[2] = {nullptr, nullptr};
+  size_t stage_cap = 0;
+  cudaEvent_t stage_ev[2] = {};
 };
 
 namespace {
@@ -241,6 +241,126 @@ void apply_shape(Context* c, const LaunchShape& sh) {
   c->dev.l2_resident_tiles = l2_tiles(c, std::max(0.0, std::min(1.0, sh.l2_fraction)));
 }
 
+// memcpy, split over host threads from 8 MB up.
+void par_memcpy(void* dst, const void* src, size_t n) {
+  const size_t kPart = 4u << 20;
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const unsigned T = (unsigned)std::min<size_t>(std::min(hw, 16u), n / kPart);
+  char* d = static_cast<char*>(dst);
+  const char* s = static_cast<const char*>(src);
+  if (T <= 1) {
+    std::memcpy(d, s, n);
+    return;
+  }
+  std::vector<std::thread> pool;
+  for (unsigned t = 1; t < T; ++t)
+    pool.emplace_back([=] {
+      const size_t a = n * t / T, e = n * (t + 1) / T;
+      std::memcpy(d + a, s + a, e - a);
+    });
+  std::memcpy(d, s, n / T);
+  for (auto& th : pool) th.join();
+}
+
+// The context's two pinned staging buffers with at least `want` bytes each
+// (at most 64 MB); false when no pinned memory can be had.
+bool reserve_stage(Context* c, size_t want) {
+  constexpr size_t kMax = 64u << 20, kGrain = 1u << 20;
+  want = std::min(kMax, (want + kGrain - 1) / kGrain * kGrain);
+  if (c->stage_cap >= want) return true;
+  for (int i = 0; i < 2; ++i) {
+    if (c->stage_ev[i]) VLBA_CUDA(cudaEventSynchronize(c->stage_ev[i]));
+    else VLBA_CUDA(cudaEventCreateWithFlags(&c->stage_ev[i], cudaEventDisableTiming));
+    if (c->stage[i]) cudaFreeHost(c->stage[i]);
+    c->stage[i] = nullptr;
+  }
+  c->stage_cap = 0;
+  for (int i = 0; i < 2; ++i) {
+    void* p = nullptr;
+    if (cudaHostAlloc(&p, want, cudaHostAllocPortable) != cudaSuccess) {
+      cudaGetLastError();
+      if (c->stage[0]) cudaFreeHost(c->stage[0]);
+      c->stage[0] = nullptr;
+      return false;
+    }
+    c->stage[i] = static_cast<char*>(p);
+  }
+  c->stage_cap = want;
+  return true;
+}
+
+// Host -> device copies of an upload through the context's pinned staging
+// buffers: the host copies the next piece into one buffer (on several
+// threads when it is large) while the device copies the previous piece out
+// of the other.  Copies from pageable memory directly when no pinned memory
+// can be had.
+class Stager {
+ public:
+  explicit Stager(Context* c) : c_(c) {}
+  template <typename T, typename A>
+  T* up(Arena& arena, const std::vector<T, A>& v) {
+    T* p = arena.alloc<T>(v.size());
+    add(p, v.data(), v.size() * sizeof(T));
+    return p;
+  }
+  void add(void* dst, const void* src, size_t bytes) {
+    if (bytes) items_.push_back(Item{static_cast<char*>(dst), static_cast<const char*>(src), bytes});
+  }
+  void flush(cudaStream_t s) {
+    size_t total = 0;
+    for (const Item& it : items_) total += it.bytes;
+    if (total == 0) return;
+    if (!reserve_stage(c_, total)) {
+      for (const Item& it : items_)
+        VLBA_CUDA(cudaMemcpyAsync(it.dst, it.src, it.bytes, cudaMemcpyHostToDevice, s));
+      items_.clear();
+      return;
+    }
+    const size_t cap = c_->stage_cap;
+    int b = 0;
+    size_t fill = 0;
+    struct Piece {
+      char* dst;
+      size_t off, bytes;
+    };
+    std::vector<Piece> pending;
+    VLBA_CUDA(cudaEventSynchronize(c_->stage_ev[0]));
+    auto issue = [&]() {
+      for (const Piece& q : pending)
+        VLBA_CUDA(cudaMemcpyAsync(q.dst, c_->stage[b] + q.off, q.bytes, cudaMemcpyHostToDevice, s));
+      VLBA_CUDA(cudaEventRecord(c_->stage_ev[b], s));
+      pending.clear();
+      b ^= 1;
+      fill = 0;
+      VLBA_CUDA(cudaEventSynchronize(c_->stage_ev[b]));
+    };
+    for (const Item& it : items_) {
+      for (size_t off = 0; off < it.bytes;) {
+        const size_t n = std::min(it.bytes - off, cap - fill);
+        if (n == 0) {
+          issue();
+          continue;
+        }
+        par_memcpy(c_->stage[b] + fill, it.src + off, n);
+        pending.push_back(Piece{it.dst + off, fill, n});
+        fill = std::min(cap, (fill + n + 255) / 256 * 256);
+        off += n;
+      }
+    }
+    if (!pending.empty()) issue();
+    items_.clear();
+  }
+
+ private:
+  struct Item {
+    char* dst;
+    const char* src;
+    size_t bytes;
+  };
+  Context* c_;
+  std::vector<Item> items_;
+};
+
 // Upload a built plan: allocate and fill every device array of Dev.
 void upload_plan_once(Context* c, uint32_t max_records) {
   Plan& P = c->plan;
@@ -264,14 +384,15 @@ void upload_plan_once(Context* c, uint32_t max_records) {
   d.tb = P.tb;
   d.group = P.group;
   Arena& A = c->arena;
-  d.prob_pose_begin = A.upload(P.prob_pose_begin, s);
-  d.prob_point_begin = A.upload(P.prob_point_begin, s);
-  d.prob_tr_begin = A.upload(P.prob_tr_begin, s);
-  d.prob_chunk_begin = A.upload(P.prob_chunk_begin, s);
-  d.pose_prob = A.upload(P.pose_prob, s);
-  d.point_prob = A.upload(P.point_prob, s);
-  d.slot_prob = A.upload(P.slot_prob, s);
-  d.params = A.upload(P.params, s);
+  Stager st(c);
+  d.prob_pose_begin = st.up(A, P.prob_pose_begin);
+  d.prob_point_begin = st.up(A, P.prob_point_begin);
+  d.prob_tr_begin = st.up(A, P.prob_tr_begin);
+  d.prob_chunk_begin = st.up(A, P.prob_chunk_begin);
+  d.pose_prob = st.up(A, P.pose_prob);
+  d.point_prob = st.up(A, P.point_prob);
+  d.slot_prob = st.up(A, P.slot_prob);
+  d.params = st.up(A, P.params);
   d.ctrl = A.alloc<Ctrl>(P.num_problems);
   d.pcg = A.alloc<PcgState>(P.num_problems);
   d.max_records = max_records;
@@ -282,41 +403,41 @@ void upload_plan_once(Context* c, uint32_t max_records) {
     d.pose_rt[b] = A.alloc<double>(12 * npose);
     d.points[b] = A.alloc<double>(3 * npt);
   }
-  d.init_pose_q = A.upload(P.pose_q, s);
-  d.init_pose_t = A.upload(P.pose_t, s);
-  d.init_points = A.upload(P.points, s);
-  d.pose_slot = A.upload(P.pose_slot, s);
-  d.point_var = A.upload(P.point_var, s);
+  d.init_pose_q = st.up(A, P.pose_q);
+  d.init_pose_t = st.up(A, P.pose_t);
+  d.init_points = st.up(A, P.points);
+  d.pose_slot = st.up(A, P.pose_slot);
+  d.point_var = st.up(A, P.point_var);
   d.pose_step = A.alloc<double>(npose);
-  d.cameras = A.upload(P.cameras, s);
-  d.pt_off = A.upload(P.pt_off, s);
-  d.obs_point = A.upload(P.obs_point, s);
-  d.obs_pose = A.upload(P.obs_pose, s);
-  d.obs_cam = A.upload(P.obs_cam, s);
-  d.obs_slot = A.upload(P.obs_slot, s);
+  d.cameras = st.up(A, P.cameras);
+  d.pt_off = st.up(A, P.pt_off);
+  d.obs_point = st.up(A, P.obs_point);
+  d.obs_pose = st.up(A, P.obs_pose);
+  d.obs_cam = st.up(A, P.obs_cam);
+  d.obs_slot = st.up(A, P.obs_slot);
   {
     double2* xy = A.alloc<double2>(nobs);
-    if (nobs) VLBA_CUDA(cudaMemcpyAsync(xy, P.obs_xy.data(), nobs * 16, cudaMemcpyHostToDevice, s));
+    st.add(xy, P.obs_xy.data(), nobs * 16);
     d.obs_xy = xy;
   }
   d.obs_h = A.alloc<float4>(2 * nobs);
   d.obs_e = A.alloc<float4>(nobs);
   d.obs_p = A.alloc<float4>(2 * nobs);
-  d.cam_off = A.upload(P.cam_off, s);
-  d.cam_obs = A.upload(P.cam_obs, s);
+  d.cam_off = st.up(A, P.cam_off);
+  d.cam_obs = st.up(A, P.cam_obs);
   d.pt_h = A.alloc<float>(9 * npt);
   d.pt_s = A.alloc<float4>(4 * npt);
   d.cam_hpp = nullptr;
   const size_t tile_floats = (size_t)P.tb * P.tb * kBlock;
   d.tiles = A.alloc<float>(P.tile_ij.size() * tile_floats);
   VLBA_CUDA(cudaMemsetAsync(d.tiles, 0, P.tile_ij.size() * tile_floats * 4, s));
-  d.tile_ij = A.upload(P.tile_ij, s);
-  d.blk_off = A.upload(P.blk_off, s);
-  d.pairs = reinterpret_cast<const uint2*>(A.upload(P.pairs, s));
-  d.blk_dst = reinterpret_cast<const uint2*>(A.upload(P.blk_dst, s));
-  d.diag_dst = A.upload(P.diag_dst, s);
-  d.dup_off = A.upload(P.dup_off, s);
-  d.dup_pairs = reinterpret_cast<const uint2*>(A.upload(P.dup_pairs, s));
+  d.tile_ij = st.up(A, P.tile_ij);
+  d.blk_off = st.up(A, P.blk_off);
+  d.pairs = reinterpret_cast<const uint2*>(st.up(A, P.pairs));
+  d.blk_dst = reinterpret_cast<const uint2*>(st.up(A, P.blk_dst));
+  d.diag_dst = st.up(A, P.diag_dst);
+  d.dup_off = st.up(A, P.dup_off);
+  d.dup_pairs = reinterpret_cast<const uint2*>(st.up(A, P.dup_pairs));
   const size_t nvec = (size_t)P.num_var_cams * 6;
   d.minv = A.alloc<float>(36 * (size_t)P.num_var_cams);
   d.rhs = A.alloc<float>(nvec);
@@ -327,11 +448,11 @@ void upload_plan_once(Context* c, uint32_t max_records) {
   d.q = A.alloc<float>(nvec);
   VLBA_CUDA(cudaMemsetAsync(d.x, 0, nvec * 4, s));
   d.partial = A.alloc<float>(P.tr_list.size() * (size_t)P.tb * 6);
-  d.tile_slot = reinterpret_cast<const uint2*>(A.upload(P.tile_slot, s));
-  d.tile_meta = reinterpret_cast<const uint4*>(A.upload(P.tile_meta, s));
-  d.tr_list_off = A.upload(P.tr_list_off, s);
-  d.tr_list = A.upload(P.tr_list, s);
-  d.tr_prob = A.upload(P.tr_prob, s);
+  d.tile_slot = reinterpret_cast<const uint2*>(st.up(A, P.tile_slot));
+  d.tile_meta = reinterpret_cast<const uint4*>(st.up(A, P.tile_meta));
+  d.tr_list_off = st.up(A, P.tr_list_off);
+  d.tr_list = st.up(A, P.tr_list);
+  d.tr_prob = st.up(A, P.tr_prob);
   d.dots = A.alloc<double>(9 * (size_t)(P.num_tile_rows ? P.num_tile_rows : 1));
   d.l2_resident_tiles = l2_tiles(c, c->l2_fraction);
   d.trace = nullptr;
@@ -342,11 +463,12 @@ void upload_plan_once(Context* c, uint32_t max_records) {
   d.error = A.alloc<unsigned int>(1);
   VLBA_CUDA(cudaMemsetAsync(d.barrier, 0, 4 * kBarrierWords, s));
   VLBA_CUDA(cudaMemsetAsync(d.error, 0, 4, s));
-  d.chunk_point_begin = A.upload(P.chunk_point_begin, s);
+  d.chunk_point_begin = st.up(A, P.chunk_point_begin);
   const size_t nch = P.chunk_point_begin.size() - 1;
   d.chunk_cost = A.alloc<double>(nch);
   d.chunk_bad = A.alloc<unsigned long long>(nch);
   d.chunk_step = A.alloc<double>(nch);
+  st.flush(s);
   c->dev = d;
   // Co-resident grid, but no more blocks than tiles or tile rows to work on
   // (fewer blocks make the grid barriers cheaper on small systems).
@@ -793,15 +915,34 @@ int guarded(Context* c, F&& f) {
   }
 }
 
+// Validation of n problems, on host threads when they hold many observations.
+std::vector<Validation> validate_all(const vlba_problem* const* probs,
+                                     const vlba_config* const* cfgs, uint32_t n) {
+  std::vector<Validation> v(n);
+  uint64_t obs = 0;
+  for (uint32_t i = 0; i < n; ++i) obs += probs[i] ? probs[i]->num_observations : 0;
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const unsigned T = (unsigned)std::min<uint64_t>({hw, n, obs / 500000 + 1});
+  std::atomic<uint32_t> next{0};
+  auto work = [&] {
+    for (uint32_t i; (i = next.fetch_add(1)) < n;) v[i] = validate_problem(probs[i], cfgs[i]);
+  };
+  std::vector<std::thread> pool;
+  for (unsigned t = 1; t < T; ++t) pool.emplace_back(work);
+  work();
+  for (auto& th : pool) th.join();
+  return v;
+}
+
 void do_upload(Context* c, const vlba_problem* const* probs, const vlba_config* const* cfgs,
                uint32_t n, uint32_t max_records, double* upload_ms) {
   const auto t0 = std::chrono::steady_clock::now();
   c->batch_slot.clear();
-  for (uint32_t i = 0; i < n; ++i) {
-    const Validation v = validate_problem(probs[i], cfgs[i]);
-    if (v.status != VLBA_OK)
-      throw Status(v.status, "problem " + std::to_string(i) + " failed validation", v.error_index);
-  }
+  const std::vector<Validation> vs = validate_all(probs, cfgs, n);
+  for (uint32_t i = 0; i < n; ++i)
+    if (vs[i].status != VLBA_OK)
+      throw Status(vs[i].status, "problem " + std::to_string(i) + " failed validation",
+                   vs[i].error_index);
   set_device(c);
   build_plan(probs, cfgs, n, (uint32_t)pick_tb(probs, n), &c->plan);
   const std::string bad = check_plan(c->plan);
@@ -823,23 +964,63 @@ void download_all(Context* c, const std::vector<int>& slot, vlba_problem* const*
   const Dev& d = c->dev;
   const Plan& P = c->plan;
   check_launch(launch_state_to_front(d, c->stream), "state gather");
-  std::vector<double> q(P.pose_q.size()), t(P.pose_t.size()), x(P.points.size());
-  VLBA_CUDA(cudaMemcpyAsync(q.data(), d.pose_q[0], q.size() * 8, cudaMemcpyDeviceToHost, c->stream));
-  VLBA_CUDA(cudaMemcpyAsync(t.data(), d.pose_t[0], t.size() * 8, cudaMemcpyDeviceToHost, c->stream));
-  VLBA_CUDA(cudaMemcpyAsync(x.data(), d.points[0], x.size() * 8, cudaMemcpyDeviceToHost, c->stream));
-  VLBA_CUDA(cudaStreamSynchronize(c->stream));
   for (size_t i = 0; i < slot.size(); ++i) {
     const int k = slot[i];
     if (k < 0 || !problems[i]) continue;
+    if (P.prob_pose_begin[k + 1] - P.prob_pose_begin[k] != problems[i]->num_poses ||
+        P.prob_point_begin[k + 1] - P.prob_point_begin[k] != problems[i]->num_landmarks)
+      throw Status(VLBA_ERR_INVALID_ARGUMENT, "download: problem sizes differ from the upload");
+  }
+  // The state lands in the pinned staging buffer when it fits (else in
+  // pageable vectors); then each problem's part is copied out.
+  const size_t nq = P.pose_q.size(), nt = P.pose_t.size(), nx = P.points.size();
+  const size_t bytes = 8 * (nq + nt + nx);
+  std::vector<double> host;
+  double* q = nullptr;
+  if (c->stage[0] && bytes <= c->stage_cap) {
+    VLBA_CUDA(cudaEventSynchronize(c->stage_ev[0]));
+    q = reinterpret_cast<double*>(c->stage[0]);
+  } else {
+    host.resize(nq + nt + nx);
+    q = host.data();
+  }
+  double* t = q + nq;
+  double* x = t + nt;
+  VLBA_CUDA(cudaMemcpyAsync(q, d.pose_q[0], nq * 8, cudaMemcpyDeviceToHost, c->stream));
+  VLBA_CUDA(cudaMemcpyAsync(t, d.pose_t[0], nt * 8, cudaMemcpyDeviceToHost, c->stream));
+  VLBA_CUDA(cudaMemcpyAsync(x, d.points[0], nx * 8, cudaMemcpyDeviceToHost, c->stream));
+  VLBA_CUDA(cudaStreamSynchronize(c->stream));
+  auto out = [&](size_t i) {
+    const int k = slot[i];
+    if (k < 0 || !problems[i]) return;
     vlba_problem* p = problems[i];
     const uint32_t pose0 = P.prob_pose_begin[k], pt0 = P.prob_point_begin[k];
     const size_t np = P.prob_pose_begin[k + 1] - pose0, nl = P.prob_point_begin[k + 1] - pt0;
-    if (np != p->num_poses || nl != p->num_landmarks)
-      throw Status(VLBA_ERR_INVALID_ARGUMENT, "download: problem sizes differ from the upload");
-    std::memcpy(p->pose_q, q.data() + 4 * (size_t)pose0, np * 32);
-    std::memcpy(p->pose_t, t.data() + 3 * (size_t)pose0, np * 24);
-    std::memcpy(p->landmarks, x.data() + 3 * (size_t)pt0, nl * 24);
+    std::memcpy(p->pose_q, q + 4 * (size_t)pose0, np * 32);
+    std::memcpy(p->pose_t, t + 3 * (size_t)pose0, np * 24);
+    std::memcpy(p->landmarks, x + 3 * (size_t)pt0, nl * 24);
+  };
+  if (slot.size() == 1) {
+    const int k = slot[0];
+    if (k >= 0 && problems[0]) {
+      vlba_problem* p = problems[0];
+      const uint32_t pose0 = P.prob_pose_begin[k], pt0 = P.prob_point_begin[k];
+      par_memcpy(p->pose_q, q + 4 * (size_t)pose0, (size_t)p->num_poses * 32);
+      par_memcpy(p->pose_t, t + 3 * (size_t)pose0, (size_t)p->num_poses * 24);
+      par_memcpy(p->landmarks, x + 3 * (size_t)pt0, (size_t)p->num_landmarks * 24);
+    }
+    return;
   }
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const unsigned T = (unsigned)std::min<size_t>({std::min(hw, 16u), slot.size(), bytes / (2u << 20) + 1});
+  std::atomic<size_t> next{0};
+  auto work = [&] {
+    for (size_t i; (i = next.fetch_add(1)) < slot.size();) out(i);
+  };
+  std::vector<std::thread> pool;
+  for (unsigned w = 1; w < T; ++w) pool.emplace_back(work);
+  work();
+  for (auto& th : pool) th.join();
 }
 
 }  // namespace
@@ -870,6 +1051,10 @@ void free_context(Context* c) {
   c->arena.release();
   for (auto& e : c->ev)
     if (e) cudaEventDestroy(e);
+  for (int i = 0; i < 2; ++i) {
+    if (c->stage_ev[i]) cudaEventDestroy(c->stage_ev[i]);
+    if (c->stage[i]) cudaFreeHost(c->stage[i]);
+  }
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }
@@ -1012,8 +1197,9 @@ int visloc_ba_cuda_batch_upload(void* ctx, uint32_t n, const vlba_problem* const
     std::vector<int> slot(n, -1);
     uint32_t max_rec = 0, flags = 0;
     int first_bad = VLBA_ERR_INVALID_ARGUMENT;
+    const std::vector<vlba::Validation> vs = vlba::validate_all(problems, configs, n);
     for (uint32_t i = 0; i < n; ++i) {
-      const vlba::Validation v = vlba::validate_problem(problems[i], configs[i]);
+      const vlba::Validation& v = vs[i];
       if (statuses) statuses[i] = v.status;
       if (v.status != VLBA_OK) {
         if (ps.empty() && first_bad == VLBA_ERR_INVALID_ARGUMENT) first_bad = v.status;
