@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define VLBA_ABI_VERSION 1u
+#define VLBA_ABI_VERSION 2u
 
 /* ------------------------------------------------------------------ status */
 /* Return codes.  The Rust shim maps VLBA_DECLINED to `None` (the caller then
@@ -54,7 +54,8 @@ enum vlba_status {
   VLBA_ERR_CUDA = 11,                  /* a CUDA call failed */
   VLBA_ERR_OUT_OF_MEMORY = 12,         /* device memory exhausted */
   VLBA_ERR_TIMEOUT = 13,               /* a bounded device wait gave up */
-  VLBA_ERR_BUSY = 14                   /* server queue full / ticket pending */
+  VLBA_ERR_BUSY = 14,                  /* server queue full / ticket pending */
+  VLBA_ERR_INVALID_OBSERVATION_WEIGHT = 15 /* BaError::InvalidObservationWeight(index) */
 };
 
 /* ------------------------------------------------------------------ camera */
@@ -114,6 +115,15 @@ typedef struct vlba_problem {
   const uint32_t* obs_camera;
   uint32_t num_cameras;
   const vlba_camera* cameras;
+  /* External confidence weight per observation (ABI version 2), the
+   * `observation_weights` of BundleAdjustment::optimize_with_observation_weights
+   * (bundle/optimize.rs:43-53): it multiplies the robust-kernel IRLS weight in
+   * the normal equations (normal_equations.rs:238,458) and each observation's
+   * robust cost (problem.rs:497-560); 1 keeps the plain contribution, 0 drops
+   * the residual.  Each must be finite and >= 0 (optimize.rs:628-650), else
+   * VLBA_ERR_INVALID_OBSERVATION_WEIGHT with the observation's index.  NULL:
+   * every weight is 1 (BundleAdjustment::optimize). */
+  const double* obs_weight;
 } vlba_problem;
 
 /* ------------------------------------------------------------------ config */
@@ -191,7 +201,7 @@ typedef struct vlba_result {
   uint64_t initial_nonprojectable;
   uint64_t final_nonprojectable;
   uint64_t total_pcg_iterations;
-  uint64_t error_index;            /* id for MISSING_POSE / MISSING_LANDMARK */
+  uint64_t error_index;            /* id for MISSING_POSE / MISSING_LANDMARK; observation index for INVALID_OBSERVATION_WEIGHT */
   double device_ms;                /* device time of the LM iterations */
   double upload_ms;                /* host+device time of the upload */
   uint64_t kernel_launches;        /* kernels launched by the LM iterations */
@@ -430,11 +440,12 @@ int visloc_ba_cuda_reduced_system(void* ctx, const vlba_problem* problem,
  *
  * The same robust cost and non-projectable count as visloc_ba_cuda_cost, for
  * a problem whose arrays are already in DEVICE memory: pose_q, pose_t,
- * landmarks, obs_pose, obs_landmark, obs_xy and obs_camera are device
- * pointers; `cameras` (at most VLBA_NOALLOC_MAX_CAMERAS) is read on the host
- * during the call; pose_fixed and landmark_fixed are ignored.  `cost` (one
- * double) and `counts` (two words: non-projectable observations, and
- * observations skipped for a pose, landmark or camera index out of range)
+ * landmarks, obs_pose, obs_landmark, obs_xy, obs_camera and obs_weight are
+ * device pointers; `cameras` (at most VLBA_NOALLOC_MAX_CAMERAS) is read on
+ * the host during the call; pose_fixed and landmark_fixed are ignored.
+ * `cost` (one double) and `counts` (two words: non-projectable observations,
+ * and observations skipped for a pose, landmark or camera index out of range
+ * or a weight that is negative or not finite)
  * are device pointers, written by a kernel enqueued on `stream` (a
  * cudaStream_t of the current device; NULL = default stream); the call
  * returns without waiting for it.

@@ -437,7 +437,9 @@ void cost_and_nonprojectable(const Problem& P, int threads, double* cost, uint64
       }
       const double rx = pred[0] - P.p->obs_xy[2 * o];
       const double ry = pred[1] - P.p->obs_xy[2 * o + 1];
-      s += P.kernel.cost(rx * rx + ry * ry);
+      // w * kernel.cost(s), the external weight 1 when absent (problem.rs:547-548).
+      const double rc = P.kernel.cost(rx * rx + ry * ry);
+      s += P.p->obs_weight ? P.p->obs_weight[o] * rc : rc;
     }
     part[ci] = s;
     partbad[ci] = b;
@@ -613,7 +615,11 @@ void build_normal(const Problem& P, const Slots& S, int threads, Normal* N) {
   for (long long oo = 0; oo < (long long)no; ++oo) {
     Contrib& k = c[oo];
     k.ok = residual_jacobians(P, (size_t)oo, k.r, k.jp, k.jl);
-    if (k.ok) k.w = P.kernel.weight(k.r[0] * k.r[0] + k.r[1] * k.r[1]);
+    // kernel.weight(s) * the external weight (normal_equations.rs:458).
+    if (k.ok) {
+      k.w = P.kernel.weight(k.r[0] * k.r[0] + k.r[1] * k.r[1]);
+      if (P.p->obs_weight) k.w *= P.p->obs_weight[oo];
+    }
   }
   // Pose blocks: each thread owns poses p with p % nt == tid.
 #pragma omp parallel num_threads(threads)
@@ -793,6 +799,16 @@ bool load_problem(const vlba_problem* p, const vlba_config* cfg, Problem* P, int
                   uint64_t* err_index) {
   *status = VLBA_OK;
   if (!p || !cfg) { *status = VLBA_ERR_INVALID_ARGUMENT; return false; }
+  // validate_observation_weights (optimize.rs:628-650) runs before the
+  // solve's own checks (optimize.rs:48); the count is num_observations by
+  // construction here.
+  if (p->obs_weight)
+    for (uint64_t o = 0; o < p->num_observations; ++o)
+      if (!std::isfinite(p->obs_weight[o]) || p->obs_weight[o] < 0.0) {
+        *status = VLBA_ERR_INVALID_OBSERVATION_WEIGHT;
+        if (err_index) *err_index = o;
+        return false;
+      }
   if (p->num_cameras == 0 || !p->cameras) { *status = VLBA_ERR_UNSUPPORTED_CAMERA_MODEL; return false; }
   P->p = p;
   P->per_obs_camera = p->obs_camera != nullptr;

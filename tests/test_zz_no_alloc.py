@@ -54,6 +54,8 @@ class DeviceProblem:
         p.obs_xy = dev(packed.obs_xy, C.c_double)
         if packed.obs_camera is not None:
             p.obs_camera = dev(packed.obs_camera, C.c_uint32)
+        if packed.obs_weight is not None:
+            p.obs_weight = dev(packed.obs_weight, C.c_double)
         self.abi = p
         self.cost = torch.empty(1, dtype=torch.float64, device="cuda")
         self.counts = torch.empty(2, dtype=torch.int64, device="cuda")
@@ -128,6 +130,33 @@ def test_out_of_range_indices_are_counted_and_skipped(solver):
         got, bad, invalid = noalloc_cost(lib, dp, cfg)
         assert invalid == 2 and bad == want_bad
         assert got == pytest.approx(want, rel=COST_RTOL)
+
+
+@pytest.mark.gpu
+def test_external_weights_match_the_allocating_cost(solver):
+    """Per-observation weights (device array): the same weighted cost as
+    visloc_ba_cuda_cost; a negative weight is counted and its observation
+    skipped."""
+    lib = solver.lib
+    p = synth.stereo_window(20, 1500, seed=6)
+    rng = np.random.default_rng(11)
+    p.obs_weight = rng.uniform(0.0, 2.0, p.num_observations)
+    cfg = BaConfig(robust_kernel=RobustKernel.huber(1.0))
+    want, want_bad = solver.cost(p, cfg)
+    dp = DeviceProblem(p)
+    for _ in range(2):
+        got, bad, invalid = noalloc_cost(lib, dp, cfg)
+        assert invalid == 0 and bad == want_bad
+        assert got == pytest.approx(want, rel=COST_RTOL)
+    w = p.obs_weight.copy()
+    w[9] = -1.0
+    skipped = p.copy()
+    skipped.obs_weight = np.where(np.arange(p.num_observations) == 9, 0.0, w)
+    want, _ = solver.cost(skipped, cfg)
+    broken = p.copy()
+    broken.obs_weight = w
+    got, bad, invalid = noalloc_cost(lib, DeviceProblem(broken), cfg)
+    assert invalid == 1 and got == pytest.approx(want, rel=COST_RTOL)
 
 
 def test_rejects_more_observations_than_the_scratch_holds():

@@ -155,6 +155,7 @@ struct Dev {
   const uint32_t* obs_cam;     // [K] camera index
   const uint32_t* obs_slot;    // [K] variable slot of the pose or kNone
   const double2* obs_xy;       // [K]
+  const double* obs_w;         // [K] external observation weights, or null (all 1)
   float4* obs_h;               // [2 K]: {h00,h01,h02,h11} {h12,h22,point,X.z}
   float4* obs_e;               // [K]:   {e0,e1,e2,w}
   float4* obs_p;               // [2 K]: the observation's point, per trial:

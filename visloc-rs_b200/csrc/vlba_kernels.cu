@@ -196,7 +196,10 @@ __global__ void __launch_bounds__(256) k_linearize(Dev d) {
       if (project_jacobian(cam, xs, pred, jpi)) {
         const double2 xy = d.obs_xy[k];
         const double rx = pred[0] - xy.x, ry = pred[1] - xy.y;
-        const double w = robust_weight(lp.robust_kernel, lp.robust_parameter, rx * rx + ry * ry);
+        // The robust IRLS weight times the external weight
+        // (normal_equations.rs:458).
+        double w = robust_weight(lp.robust_kernel, lp.robust_parameter, rx * rx + ry * ry);
+        if (d.obs_w) w *= d.obs_w[k];
         // Effective rotation world -> sensor.
         double Re[9];
         if (cam.rig) {
@@ -317,6 +320,35 @@ __global__ void __launch_bounds__(256) k_point_prep(Dev d) {
     ps[2] = make_float4(X2, (float)v[0], (float)v[1], (float)v[2]);
     ps[3] = make_float4((float)g[0], (float)g[1], (float)g[2], ok);
   }
+}
+
+// The damped inverse of point l's H_ll and v = H^-1 g in FP64, from the
+// FP64 sums k_point_prep stores as FP32 (the same formulas; k_point_prep
+// rounds the inverse to FP32 for the other kernels).  The camera diagonal
+// needs this precision: when a point has one contributing observation (its
+// others weighted 0, or observed twice by one camera), H_ll is H_o of rank 2
+// and H_o - H_o (H_ll + lambda I)^-1 H_o cancels down to O(lambda), far
+// below what an FP32 inverse with entries near 1/lambda resolves.
+__device__ __forceinline__ void point_inverse64(const Dev& d, uint32_t l, double lambda,
+                                                double* M, double* v) {
+  const float* ph = d.pt_h + 9 * (size_t)l;
+  double a = ph[0], b = ph[1], cc = ph[2], dd = ph[3], e = ph[4], f = ph[5];
+  if (lambda > 0.0) {
+    a += lambda;
+    dd += lambda;
+    f += lambda;
+  }
+  const double m22 = dd * f - e * e, m12 = b * f - e * cc, m11 = b * e - dd * cc;
+  const double det = a * m22 - b * m12 + cc * m11;
+  const double i0 = m22 / det, i1 = (cc * e - f * b) / det, i2 = (b * e - dd * cc) / det,
+               i3 = (a * f - cc * cc) / det, i4 = (cc * b - e * a) / det, i5 = (a * dd - b * b) / det;
+  M[0] = i0; M[1] = i1; M[2] = i2;
+  M[3] = i1; M[4] = i3; M[5] = i4;
+  M[6] = i2; M[7] = i4; M[8] = i5;
+  const double g0 = ph[6], g1 = ph[7], g2 = ph[8];
+  v[0] = i0 * g0 + i1 * g1 + i2 * g2;
+  v[1] = i1 * g0 + i3 * g1 + i4 * g2;
+  v[2] = i2 * g0 + i4 * g1 + i5 * g2;
 }
 
 // ------------------------------------------------- off-diagonal Schur blocks
@@ -449,6 +481,7 @@ __device__ __forceinline__ double quad3(const double* H, double a, double b, dou
 // then the FP64 Cholesky inverse of S_ii as the block-Jacobi preconditioner
 // (ba.wgsl:263-387; fallback to the inverse damped diagonal, ba.wgsl:375-383).
 constexpr int kDiagThreads = 128;
+
 constexpr int kDiagAcc = 33;  // 21 upper S, 6 rhs, 6 diag(H_pp)
 
 __global__ void __launch_bounds__(kDiagThreads) k_cam_diag(Dev d) {
@@ -467,14 +500,15 @@ __global__ void __launch_bounds__(kDiagThreads) k_cam_diag(Dev d) {
       const float4 h0 = d.obs_h[2 * (size_t)k], h1 = d.obs_h[2 * (size_t)k + 1];
       const float4 ev = d.obs_e[k];
       const uint32_t l = __float_as_uint(h1.z);
-      const float4 s0 = d.pt_s[4 * (size_t)l], s1 = d.pt_s[4 * (size_t)l + 1],
-                   s2 = d.pt_s[4 * (size_t)l + 2], s3 = d.pt_s[4 * (size_t)l + 3];
+      const float4 s1 = d.pt_s[4 * (size_t)l + 1], s2 = d.pt_s[4 * (size_t)l + 2],
+                   s3 = d.pt_s[4 * (size_t)l + 3];
       const double H[9] = {h0.x, h0.y, h0.z, h0.y, h0.w, h1.x, h0.z, h1.x, h1.y};
       const double X = s1.z, Y = s1.w, Z = s2.x;
       double K[9], u[3];
       const bool ok = s3.w != 0.0f;
       if (ok) {
-        const double Mi[9] = {s0.x, s0.y, s0.z, s0.y, s0.w, s1.x, s0.z, s1.x, s1.y};
+        double Mi[9], vv[3];
+        point_inverse64(d, l, lambda, Mi, vv);
         double M[9];
         for (int r = 0; r < 3; ++r)
           for (int cc = 0; cc < 3; ++cc)
@@ -483,7 +517,7 @@ __global__ void __launch_bounds__(kDiagThreads) k_cam_diag(Dev d) {
           for (int cc = 0; cc < 3; ++cc)
             K[r * 3 + cc] = H[r * 3 + cc] - (H[r * 3] * M[cc] + H[r * 3 + 1] * M[3 + cc] +
                                              H[r * 3 + 2] * M[6 + cc]);
-        const double v0 = s2.y, v1 = s2.z, v2 = s2.w;
+        const double v0 = vv[0], v1 = vv[1], v2 = vv[2];
         u[0] = H[0] * v0 + H[1] * v1 + H[2] * v2 - ev.x;
         u[1] = H[3] * v0 + H[4] * v1 + H[5] * v2 - ev.y;
         u[2] = H[6] * v0 + H[7] * v1 + H[8] * v2 - ev.z;
@@ -517,11 +551,12 @@ __global__ void __launch_bounds__(kDiagThreads) k_cam_diag(Dev d) {
       const float4 a0 = d.obs_h[2 * (size_t)pr.x], a1 = d.obs_h[2 * (size_t)pr.x + 1];
       const float4 b0 = d.obs_h[2 * (size_t)pr.y], b1 = d.obs_h[2 * (size_t)pr.y + 1];
       const uint32_t l = __float_as_uint(a1.z);
-      const float4 s0 = d.pt_s[4 * (size_t)l], s1 = d.pt_s[4 * (size_t)l + 1],
-                   s2 = d.pt_s[4 * (size_t)l + 2];
+      const float4 s1 = d.pt_s[4 * (size_t)l + 1], s2 = d.pt_s[4 * (size_t)l + 2];
+      if (d.pt_s[4 * (size_t)l + 3].w == 0.0f) continue;  // no inverse: no Schur term
       const double Hi[9] = {a0.x, a0.y, a0.z, a0.y, a0.w, a1.x, a0.z, a1.x, a1.y};
       const double Hj[9] = {b0.x, b0.y, b0.z, b0.y, b0.w, b1.x, b0.z, b1.x, b1.y};
-      const double Mi[9] = {s0.x, s0.y, s0.z, s0.y, s0.w, s1.x, s0.z, s1.x, s1.y};
+      double Mi[9], vv[3];
+      point_inverse64(d, l, lambda, Mi, vv);
       double M[9], K[9];
       for (int r = 0; r < 3; ++r)
         for (int cc = 0; cc < 3; ++cc)
@@ -689,28 +724,34 @@ __global__ void __launch_bounds__(256) k_cost(Dev d) {
       for (int a = 0; a < 3; ++a) X[a] = d.points[cur][3 * (size_t)l + a];
       const uint32_t k0 = d.pt_off[l], k1 = d.pt_off[l + 1];
       if (TRIAL) {
-        const float4 s0 = d.pt_s[4 * (size_t)l], s1 = d.pt_s[4 * (size_t)l + 1],
-                     s2 = d.pt_s[4 * (size_t)l + 2], s3 = d.pt_s[4 * (size_t)l + 3];
+        const float4 s1 = d.pt_s[4 * (size_t)l + 1], s2 = d.pt_s[4 * (size_t)l + 2],
+                     s3 = d.pt_s[4 * (size_t)l + 3];
         if (d.point_var[l] && s3.w != 0.0f) {
-          const float x = s1.z, y = s1.w, z = s2.x;
-          float u0 = s3.x, u1 = s3.y, u2 = s3.z;
+          // In FP64 with the point's FP64 damped inverse: a point whose depth
+          // one observation alone constrains has an inverse with entries near
+          // 1/lambda along its ray, which FP32 would turn into a large
+          // spurious step along the ray.
+          double Mi[9], vv[3];
+          point_inverse64(d, l, c.lambda, Mi, vv);
+          const double x = s1.z, y = s1.w, z = s2.x;
+          const float* ph = d.pt_h + 9 * (size_t)l;
+          double u0 = ph[6], u1 = ph[7], u2 = ph[8];
           for (uint32_t k = k0; k < k1; ++k) {
             const uint32_t slot = d.obs_slot[k];
             if (slot == kNone) continue;
             const float* dc = d.x + 6 * (size_t)slot;
-            const float w0 = dc[3], w1 = dc[4], w2 = dc[5];
-            const float b0 = dc[0] + (w1 * z - w2 * y);
-            const float b1 = dc[1] + (w2 * x - w0 * z);
-            const float b2 = dc[2] + (w0 * y - w1 * x);
+            const double w0 = dc[3], w1 = dc[4], w2 = dc[5];
+            const double b0 = dc[0] + (w1 * z - w2 * y);
+            const double b1 = dc[1] + (w2 * x - w0 * z);
+            const double b2 = dc[2] + (w0 * y - w1 * x);
             const float4 h0 = d.obs_h[2 * (size_t)k], h1 = d.obs_h[2 * (size_t)k + 1];
             u0 += h0.x * b0 + h0.y * b1 + h0.z * b2;
             u1 += h0.y * b0 + h0.w * b1 + h1.x * b2;
             u2 += h0.z * b0 + h1.x * b1 + h1.y * b2;
           }
-          const float dl0 = -(s0.x * u0 + s0.y * u1 + s0.z * u2);
-          const float dl1 = -(s0.y * u0 + s0.w * u1 + s1.x * u2);
-          const float dl2 = -(s0.z * u0 + s1.x * u1 + s1.y * u2);
-          const double e0 = dl0, e1 = dl1, e2 = dl2;
+          const double e0 = -(Mi[0] * u0 + Mi[1] * u1 + Mi[2] * u2);
+          const double e1 = -(Mi[3] * u0 + Mi[4] * u1 + Mi[5] * u2);
+          const double e2 = -(Mi[6] * u0 + Mi[7] * u1 + Mi[8] * u2);
           step = fmax(step, sqrt(e0 * e0 + e1 * e1 + e2 * e2));
           X[0] += e0;
           X[1] += e1;
@@ -738,7 +779,8 @@ __global__ void __launch_bounds__(256) k_cost(Dev d) {
       }
       const double2 xy = d.obs_xy[k];
       const double rx = pred[0] - xy.x, ry = pred[1] - xy.y;
-      cost += robust_cost(lp.robust_kernel, lp.robust_parameter, rx * rx + ry * ry);
+      const double rc = robust_cost(lp.robust_kernel, lp.robust_parameter, rx * rx + ry * ry);
+      cost += d.obs_w ? d.obs_w[k] * rc : rc;  // w * rho(s) (problem.rs:497-560)
     }
     const double tc = block_sum<double, 256>(cost, red);
     const unsigned long long tb = block_sum<unsigned long long, 256>(bad, redu);

@@ -69,6 +69,7 @@ struct NoallocArgs {
   const uint32_t* obs_landmark;
   const double2* obs_xy;
   const uint32_t* obs_camera;  // null: cameras[0] for every observation
+  const double* obs_weight;    // null: every weight 1
   uint32_t num_cameras;
   uint32_t robust_kernel;
   double robust_parameter;
@@ -110,7 +111,9 @@ __global__ void __launch_bounds__(256) k_cost_noalloc(const NoallocArgs a, unsig
     if (o < a.num_obs) {
       const uint32_t ip = a.obs_pose[o], il = a.obs_landmark[o];
       const uint32_t ic = a.obs_camera ? a.obs_camera[o] : 0u;
-      if (ip >= a.num_poses || il >= a.num_landmarks || ic >= a.num_cameras) {
+      const double w = a.obs_weight ? a.obs_weight[o] : 1.0;
+      if (ip >= a.num_poses || il >= a.num_landmarks || ic >= a.num_cameras || !isfinite(w) ||
+          w < 0.0) {
         invalid = 1;
       } else {
         double q[4], rt[12], X[3], xs[3], pred[2];
@@ -130,6 +133,7 @@ __global__ void __launch_bounds__(256) k_cost_noalloc(const NoallocArgs a, unsig
           const double2 xy = a.obs_xy[o];
           const double rx = pred[0] - xy.x, ry = pred[1] - xy.y;
           cost = robust_cost(a.robust_kernel, a.robust_parameter, rx * rx + ry * ry);
+          if (a.obs_weight) cost *= w;
         }
       }
     }
@@ -254,6 +258,7 @@ int visloc_ba_cuda_cost_noalloc(const vlba_problem* problem, const vlba_config* 
   a.obs_landmark = p.obs_landmark;
   a.obs_xy = reinterpret_cast<const double2*>(p.obs_xy);
   a.obs_camera = p.obs_camera;
+  a.obs_weight = p.obs_weight;
   a.num_cameras = p.num_cameras;
   a.robust_kernel = config->robust_kernel;
   a.robust_parameter = config->robust_parameter;

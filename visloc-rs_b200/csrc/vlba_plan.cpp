@@ -109,6 +109,15 @@ Validation validate_problem(const vlba_problem* p, const vlba_config* cfg) {
     v.status = VLBA_ERR_INVALID_ARGUMENT;
     return v;
   }
+  // External observation weights before anything else, as
+  // optimize_with_observation_weights checks them (optimize.rs:48, 628-650).
+  if (p->obs_weight)
+    for (uint64_t o = 0; o < p->num_observations; ++o)
+      if (!std::isfinite(p->obs_weight[o]) || p->obs_weight[o] < 0.0) {
+        v.status = VLBA_ERR_INVALID_OBSERVATION_WEIGHT;
+        v.error_index = o;
+        return v;
+      }
   // Camera model first (lm.rs:168 `intrinsics()?`); a model outside the
   // radial pinhole family is declined, so the caller runs its CPU solver.
   if (p->num_cameras == 0 || !p->cameras) { v.status = VLBA_ERR_UNSUPPORTED_CAMERA_MODEL; return v; }
@@ -243,6 +252,7 @@ void build_plan_serial(const vlba_problem* const* problems, const vlba_config* c
     keep(P.obs_cam, old.obs_cam);
     keep(P.obs_slot, old.obs_slot);
     keep(P.obs_xy, old.obs_xy);
+    keep(P.obs_w, old.obs_w);
     keep(P.cam_obs, old.cam_obs);
   }
   P.tb = tb;
@@ -269,6 +279,9 @@ void build_plan_serial(const vlba_problem* const* problems, const vlba_config* c
   P.obs_slot.resize(tot_obs);
   P.obs_xy.resize(2 * tot_obs);
   P.obs_point.resize(tot_obs);
+  bool weighted = false;
+  for (uint32_t i = 0; i < n; ++i) weighted = weighted || problems[i]->obs_weight != nullptr;
+  if (weighted) P.obs_w.resize(tot_obs);
   P.cameras.reserve(tot_cams);
   P.prob_pose_begin.push_back(0);
   P.prob_point_begin.push_back(0);
@@ -341,6 +354,7 @@ void build_plan_serial(const vlba_problem* const* problems, const vlba_config* c
         P.obs_slot[g] = P.pose_slot[pose];
         P.obs_xy[2 * (size_t)g] = p->obs_xy[2 * (size_t)o];
         P.obs_xy[2 * (size_t)g + 1] = p->obs_xy[2 * (size_t)o + 1];
+        if (weighted) P.obs_w[g] = p->obs_weight ? p->obs_weight[o] : 1.0;
       }
     });
     // Per-slot observation lists (ascending point-major index).
@@ -679,6 +693,7 @@ void merge_plans(const std::vector<const Plan*>& parts, Plan* out) {
     keep(P.obs_cam, old.obs_cam);
     keep(P.obs_slot, old.obs_slot);
     keep(P.obs_xy, old.obs_xy);
+    keep(P.obs_w, old.obs_w);
     keep(P.cam_obs, old.cam_obs);
   }
   if (parts.empty()) throw std::runtime_error("merge of no plans");
@@ -747,6 +762,9 @@ void merge_plans(const std::vector<const Plan*>& parts, Plan* out) {
   P.obs_cam.resize(T.obs);
   P.obs_slot.resize(T.obs);
   P.obs_xy.resize(2 * T.obs);
+  bool weighted = false;
+  for (const Plan* q : parts) weighted = weighted || !q->obs_w.empty();
+  if (weighted) P.obs_w.resize(T.obs);
   P.cam_off.assign(T.slot + 1, 0u);
   P.cam_obs.resize(T.camobs);
   P.tile_ij.resize(T.tile);
@@ -806,6 +824,10 @@ void merge_plans(const std::vector<const Plan*>& parts, Plan* out) {
     shift(P.obs_cam, obs_b, Q.obs_cam, cam_b);
     shift_none(P.obs_slot, obs_b, Q.obs_slot, slot_b);
     copy(P.obs_xy, 2 * (size_t)obs_b, Q.obs_xy);
+    if (weighted) {
+      if (Q.obs_w.empty()) std::fill_n(P.obs_w.begin() + obs_b, Q.obs_pose.size(), 1.0);
+      else copy(P.obs_w, obs_b, Q.obs_w);
+    }
     shift_off(P.cam_off, slot_b, Q.cam_off, camobs_b);
     shift(P.cam_obs, camobs_b, Q.cam_obs, obs_b);
     for (size_t k = 0; k < Q.tile_ij.size(); ++k) {
@@ -898,7 +920,7 @@ std::string check_plan(const Plan& P) {
   if (!all_of_range(npts, [&](uint64_t j) { return P.pt_off[j] <= P.pt_off[j + 1]; }))
     return bad("pt_off order");
   if (P.obs_cam.size() != nobs || P.obs_slot.size() != nobs || P.obs_xy.size() != 2 * nobs ||
-      P.obs_point.size() != nobs)
+      P.obs_point.size() != nobs || (!P.obs_w.empty() && P.obs_w.size() != nobs))
     return bad("obs sizes");
   if (!all_of_range(nobs, [&](uint64_t k) {
         const uint32_t l = P.obs_point[k];
@@ -966,6 +988,7 @@ size_t Plan::device_bytes() const {
   b += npose * (8 * (4 + 3 + 12) * 2 + 8 + 4 + 4);  // state x2, step, slot, prob
   b += npt * (8 * 3 * 2 + 4 + 1 + 4 + 36 + 64);     // points x2, off, var, prob, pt_h, pt_s
   b += nobs * (4 * 4 + 16 + 32 + 16 + 32);           // point, pose, cam, slot, xy, obs_h, obs_e, obs_p
+  b += obs_w.size() * 8;
   b += cam_obs.size() * 4 + pairs.size() * 8 + dup_pairs.size() * 8;
   b += blk_dst.size() * (8 + 4);
   b += tile_ij.size() * ((size_t)tb * tb * kBlock * 4 + 4 + 2 * (size_t)tb * 6 * 4);
@@ -981,7 +1004,7 @@ size_t Plan::upload_bytes() const {
   return b(prob_pose_begin) + b(prob_point_begin) + b(prob_tr_begin) + b(prob_chunk_begin) +
          b(pose_prob) + b(point_prob) + b(slot_prob) + b(params) + b(pose_q) + b(pose_t) +
          b(points) + b(pose_slot) + b(point_var) + b(cameras) + b(pt_off) + b(obs_point) + b(obs_pose) +
-         b(obs_cam) + b(obs_slot) + b(obs_xy) + b(cam_off) + b(cam_obs) + b(tile_ij) +
+         b(obs_cam) + b(obs_slot) + b(obs_xy) + b(obs_w) + b(cam_off) + b(cam_obs) + b(tile_ij) +
          b(blk_off) + b(pairs) + b(blk_dst) + b(diag_dst) + b(dup_off) + b(dup_pairs) +
          b(tr_list_off) + b(tr_list) + b(tr_prob) + b(chunk_point_begin) + b(tile_slot) + b(tile_meta);
 }

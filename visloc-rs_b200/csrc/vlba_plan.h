@@ -64,6 +64,9 @@ struct Plan {
   std::vector<uint32_t> pt_off;
   ObsArray<uint32_t> obs_point, obs_pose, obs_cam, obs_slot;
   ObsArray<double> obs_xy;  // 2 per obs
+  // External weight per observation; empty when no problem of the plan has
+  // weights (a problem without them gets 1 in a plan that has them).
+  ObsArray<double> obs_w;
   std::vector<uint32_t> cam_off;
   ObsArray<uint32_t> cam_obs;
 

@@ -420,6 +420,7 @@ void upload_plan_once(Context* c, uint32_t max_records) {
     st.add(xy, P.obs_xy.data(), nobs * 16);
     d.obs_xy = xy;
   }
+  d.obs_w = P.obs_w.empty() ? nullptr : st.up(A, P.obs_w);
   d.obs_h = A.alloc<float4>(2 * nobs);
   d.obs_e = A.alloc<float4>(nobs);
   d.obs_p = A.alloc<float4>(2 * nobs);
@@ -1173,9 +1174,9 @@ int visloc_ba_cuda_optimize(void* ctx, vlba_problem* problem, const vlba_config*
     c->flags = config ? config->flags : 0;
   });
   if (st != VLBA_OK) {
-    if (result && (st == VLBA_ERR_MISSING_POSE || st == VLBA_ERR_MISSING_LANDMARK)) {
+    if (result && (st == VLBA_ERR_MISSING_POSE || st == VLBA_ERR_MISSING_LANDMARK ||
+                   st == VLBA_ERR_INVALID_OBSERVATION_WEIGHT)) {
       uint64_t idx = 0;
-      vlba::validate_problem(problem, config);
       visloc_ba_cuda_check(problem, config, &idx);
       result->error_index = idx;
     }

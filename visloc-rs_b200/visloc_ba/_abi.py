@@ -10,7 +10,7 @@ from __future__ import annotations
 import ctypes as C
 import os
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 # enum vlba_status
 OK = 0
@@ -28,6 +28,7 @@ ERR_CUDA = 11
 ERR_OUT_OF_MEMORY = 12
 ERR_TIMEOUT = 13
 ERR_BUSY = 14
+ERR_INVALID_OBSERVATION_WEIGHT = 15
 
 STATUS_NAMES = {
     OK: "OK",
@@ -45,6 +46,7 @@ STATUS_NAMES = {
     ERR_OUT_OF_MEMORY: "OutOfMemory",
     ERR_TIMEOUT: "Timeout",
     ERR_BUSY: "Busy",
+    ERR_INVALID_OBSERVATION_WEIGHT: "InvalidObservationWeight",
 }
 
 # enum vlba_camera_model
@@ -91,6 +93,7 @@ class Problem(C.Structure):
         ("obs_camera", C.POINTER(C.c_uint32)),
         ("num_cameras", C.c_uint32),
         ("cameras", C.POINTER(Camera)),
+        ("obs_weight", C.POINTER(C.c_double)),
     ]
 
 

@@ -369,10 +369,11 @@ class PackedProblem:
     pose_q (N,4) f64 (w,i,j,k), pose_t (N,3), pose_fixed (N,) u8,
     landmarks (M,3), landmark_fixed (M,) u8, obs_pose / obs_landmark (K,) u32,
     obs_xy (K,2) f64, obs_camera (K,) u32 or None, cameras: list of
-    (Camera, SE3 sensor_from_rig)."""
+    (Camera, SE3 sensor_from_rig), obs_weight (K,) f64 external weights or
+    None (all 1; optimize_with_observation_weights, optimize.rs:43-53)."""
 
     def __init__(self, pose_q, pose_t, landmarks, obs_pose, obs_landmark, obs_xy, cameras,
-                 pose_fixed=None, landmark_fixed=None, obs_camera=None):
+                 pose_fixed=None, landmark_fixed=None, obs_camera=None, obs_weight=None):
         self.pose_q = np.ascontiguousarray(pose_q, dtype=np.float64).reshape(-1, 4)
         self.pose_t = np.ascontiguousarray(pose_t, dtype=np.float64).reshape(-1, 3)
         self.landmarks = np.ascontiguousarray(landmarks, dtype=np.float64).reshape(-1, 3)
@@ -391,6 +392,9 @@ class PackedProblem:
             None if obs_camera is None else np.ascontiguousarray(obs_camera, dtype=np.uint32)
         )
         self.cameras = [c if isinstance(c, tuple) else (c, SE3()) for c in cameras]
+        self.obs_weight = (
+            None if obs_weight is None else np.ascontiguousarray(obs_weight, dtype=np.float64)
+        )
         self._abi = None
 
     @property
@@ -409,7 +413,7 @@ class PackedProblem:
         return PackedProblem(
             self.pose_q.copy(), self.pose_t.copy(), self.landmarks.copy(), self.obs_pose,
             self.obs_landmark, self.obs_xy, list(self.cameras), self.pose_fixed,
-            self.landmark_fixed, self.obs_camera,
+            self.landmark_fixed, self.obs_camera, self.obs_weight,
         )
 
     def abi(self) -> _abi.Problem:
@@ -427,6 +431,7 @@ class PackedProblem:
         p.obs_landmark = _ptr(self.obs_landmark, C.c_uint32)
         p.obs_xy = _ptr(self.obs_xy, C.c_double)
         p.obs_camera = _ptr(self.obs_camera, C.c_uint32)
+        p.obs_weight = _ptr(self.obs_weight, C.c_double)
         cams = (_abi.Camera * len(self.cameras))(
             *[cam.to_abi(ext) for cam, ext in self.cameras]
         )

@@ -6,14 +6,15 @@ counterpart of the reference's crates/ba-gpu/examples/ba_gpu_replay.rs
 
     python visloc-rs_b200/visloc_ba/replay.py problem.txt [--iterations 20]
         [--local N] [--robust huber:1.0] [--pcg-tol 1e-4] [--pcg-max 100]
-        [--repeat 3]
+        [--repeat 3] [--weights]
 
 --local N keeps only the last N poses variable (fixing the rest), only the
 landmarks they observe and every pose observing those: the shape of the
-SfM's local BA window.  Per-observation weights in the file are not used by
-the accelerator path (the reference offers only unweighted problems to it,
-pipelines/slam/src/ba_accel.rs:1-7); the replay reports that they were
-present.  Prints one JSON object.
+SfM's local BA window.  Per-observation weights in the file are used only with
+--weights (the semantics of optimize_with_observation_weights; the reference
+offers only unweighted problems to its accelerator, pipelines/slam/src/
+ba_accel.rs:1-7); the replay reports whether they were present.  Prints one
+JSON object.
 """
 
 from __future__ import annotations
@@ -52,7 +53,8 @@ def local_window(packed: PackedProblem, n: int) -> PackedProblem:
     return PackedProblem(packed.pose_q[used], packed.pose_t[used], packed.landmarks[keep_lm],
                          pose_map[packed.obs_pose[sel]], lm_map[packed.obs_landmark[sel]],
                          packed.obs_xy[sel], packed.cameras, fixed,
-                         np.zeros(int(keep_lm.sum()), np.uint8), None)
+                         np.zeros(int(keep_lm.sum()), np.uint8), None,
+                         None if packed.obs_weight is None else packed.obs_weight[sel])
 
 
 def robust(spec: str) -> RobustKernel:
@@ -68,8 +70,10 @@ def robust(spec: str) -> RobustKernel:
 
 def rms_reprojection(solver: CudaSolver, packed: PackedProblem) -> float:
     """sqrt(mean squared reprojection error), from the device cost with no
-    robust kernel (ba_gpu_replay.rs:18-28)."""
-    cost, _ = solver.cost(packed, BaConfig(robust_kernel=RobustKernel.none()))
+    robust kernel and no weights (ba_gpu_replay.rs:18-28)."""
+    plain = packed.copy()
+    plain.obs_weight = None
+    cost, _ = solver.cost(plain, BaConfig(robust_kernel=RobustKernel.none()))
     return math.sqrt(cost / max(1, packed.num_observations))
 
 
@@ -83,9 +87,13 @@ def main(argv=None) -> int:
     ap.add_argument("--pcg-max", type=int, default=100)
     ap.add_argument("--repeat", type=int, default=1)
     ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--weights", action="store_true",
+                    help="solve with the file's per-observation weights")
     a = ap.parse_args(argv)
     t0 = time.perf_counter()
     packed, pose_ids, lm_ids, weights = read_packed_problem(a.problem)
+    if a.weights and weights is not None:
+        packed.obs_weight = np.ascontiguousarray(weights, dtype=np.float64)
     if a.local:
         packed = local_window(packed, a.local)
     load_s = time.perf_counter() - t0
@@ -94,6 +102,7 @@ def main(argv=None) -> int:
     out = {"problem": a.problem, "poses": packed.num_poses,
            "fixed_poses": int(packed.pose_fixed.sum()), "landmarks": packed.num_landmarks,
            "observations": packed.num_observations, "weights_in_file": weights is not None,
+           "weights_used": packed.obs_weight is not None,
            "local_window": a.local or None, "load_s": load_s}
     runs = []
     with CudaSolver(a.device) as solver:

@@ -330,12 +330,26 @@ class GpuBundleAdjuster:
         cfg.pcg_relative_tolerance = self.settings.pcg_relative_tolerance
         return cfg
 
-    def solve(self, ba: BundleAdjustment, config: BaConfig) -> BaResult:
+    def solve(self, ba: BundleAdjustment, config: BaConfig, observation_weights=None) -> BaResult:
         """BundleAdjustment::optimize semantics: mutate `ba`, return BaResult,
-        raise BaError.  Raises SolverError when the library declines."""
+        raise BaError.  Raises SolverError when the library declines.  With
+        `observation_weights` (one per observation, in the problem's
+        observation order), the semantics of
+        optimize_with_observation_weights (optimize.rs:43-53, 628-650)."""
         packed, pose_ids, lm_ids, missing = ba.pack()
+        if observation_weights is not None:
+            import numpy as np
+
+            w = np.ascontiguousarray(observation_weights, dtype=np.float64).reshape(-1)
+            expected = len(ba.observations) + len(ba.rig_observations)
+            if w.shape[0] != expected:
+                raise BaError("ObservationWeightCount",
+                              message=f"expected {expected}, got {w.shape[0]}")
+            packed.obs_weight = w
         cfg = self._config(config)
         st, res = self.solver.optimize(packed, cfg)
+        if st == _abi.ERR_INVALID_OBSERVATION_WEIGHT:
+            raise BaError("InvalidObservationWeight", int(res.error_index))
         if st in (_abi.ERR_MISSING_POSE, _abi.ERR_MISSING_LANDMARK) and missing is not None:
             raise missing
         if st in _ERROR_KIND:
@@ -344,6 +358,13 @@ class GpuBundleAdjuster:
             raise SolverError(st, self.solver.last_error())
         ba.unpack(packed, pose_ids, lm_ids)
         return res
+
+    def optimize_with_observation_weights(self, ba: BundleAdjustment, config: BaConfig,
+                                          observation_weights) -> BaResult:
+        """BundleAdjustment::optimize_with_observation_weights (optimize.rs:43-53)
+        on the device: each weight multiplies its observation's robust IRLS
+        weight and robust cost."""
+        return self.solve(ba, config, observation_weights)
 
     def optimize(self, ba: BundleAdjustment, config: BaConfig, scope: BaScope = BaScope.GLOBAL):
         """BaAccelerator::optimize: None = declined (run the CPU solver)."""
