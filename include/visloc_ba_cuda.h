@@ -432,6 +432,58 @@ int visloc_ba_cuda_reduced_system(void* ctx, const vlba_problem* problem,
                                   const vlba_config* config, double lambda,
                                   double* s_dense, double* rhs);
 
+/* --------------------------------------------------------------------- GNC */
+/* GncKernel (pipelines/slam/src/gnc.rs:38-48). */
+enum vlba_gnc_kernel {
+  VLBA_GNC_GEMAN_MCCLURE = 0,          /* GncKernel::GemanMcClure (default) */
+  VLBA_GNC_TRUNCATED_LEAST_SQUARES = 1 /* GncKernel::TruncatedLeastSquares */
+};
+
+/* GncConfig (gnc.rs:50-110); visloc_ba_cuda_default_gnc_config fills
+ * GncConfig::default() (gnc.rs:100-110). */
+typedef struct vlba_gnc_config {
+  uint32_t kernel;             /* vlba_gnc_kernel */
+  uint32_t max_outer;          /* cap on mu levels */
+  uint32_t inner_iterations;   /* LM iterations per level */
+  uint32_t has_auto_scale;     /* auto_scale: 0 = None */
+  double c;                    /* inlier scale in pixels (a floor under auto_scale) */
+  double anneal_factor;        /* geometric mu step, > 1 */
+  double auto_scale;           /* k of median + k 1.4826 MAD when has_auto_scale */
+  uint32_t auto_scale_readapt; /* re-estimate the scale at every level */
+  uint32_t reserved;
+} vlba_gnc_config;
+
+/* BaGncResult (bundle/mod.rs:975-1000); the weight vector is returned
+ * through `observation_weights`. */
+typedef struct vlba_gnc_result {
+  double initial_cost;         /* non-robust cost at the input estimate */
+  double final_cost;           /* sum of w s at the recovered estimate */
+  double inlier_cost;          /* sum of s over observations with w >= 0.5 */
+  double inlier_scale;         /* the c the solve used */
+  uint64_t observation_count;
+  uint32_t outer_iterations;
+  uint32_t converged;          /* the mu schedule reached its terminal level */
+  uint64_t lm_iterations;      /* inner LM iterations, all levels */
+  double device_ms;            /* device time of the inner solves */
+} vlba_gnc_result;
+
+void visloc_ba_cuda_default_gnc_config(vlba_gnc_config* gnc);
+
+/* BundleAdjustment::optimize_gnc (bundle/lm.rs:28-142): anneal the GNC
+ * surrogate from least squares to the robust cost, each level a short
+ * weighted LM solve (config's lambda schedule and tolerances, no robust
+ * kernel, gnc->inner_iterations iterations) from the previous level's state,
+ * with the per-observation Black-Rangarajan weights of the level.  The
+ * problem is uploaded once; residuals and weights move between host and
+ * device per level.  problem->obs_weight must be NULL (GNC sets the weights).
+ * On success the state is written back in place and, when
+ * `observation_weights` is not NULL, it receives the final weight of every
+ * observation in the problem's order (NaN where the observation cannot be
+ * evaluated at the final estimate). */
+int visloc_ba_cuda_optimize_gnc(void* ctx, vlba_problem* problem, const vlba_config* config,
+                                const vlba_gnc_config* gnc, vlba_gnc_result* result,
+                                double* observation_weights);
+
 /* ----------------------------------------------------- allocation-free cost */
 /* No counterpart in the reference: an addition for callers that cannot
  * allocate device memory when they need a cost -- a tracking thread with a

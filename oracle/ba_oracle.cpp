@@ -892,6 +892,29 @@ int vlba_oracle_cost(const vlba_problem* p, const vlba_config* cfg, int threads,
   return VLBA_OK;
 }
 
+// reprojection_squared_residuals (problem.rs:756-830): per observation, in
+// its order, the squared reprojection residual, NaN when the observation is
+// behind its sensor or does not project.
+int vlba_oracle_squared_residuals(const vlba_problem* p, const vlba_config* cfg, double* out) {
+  Problem P;
+  int status;
+  if (!load_problem(p, cfg, &P, &status, nullptr)) return status;
+  for (uint64_t o = 0; o < p->num_observations; ++o) {
+    const Se3& T = P.poses[p->obs_pose[o]];
+    const Cam& c = P.cam_of(o);
+    V3 xc = se3_transform(T, P.points[p->obs_landmark[o]]);
+    if (P.per_obs_camera) xc = se3_transform(c.sensor_from_rig, xc);
+    double pred[2];
+    if (xc.z <= 0.0 || !camera_project(c, xc, pred)) {
+      out[o] = std::numeric_limits<double>::quiet_NaN();
+      continue;
+    }
+    const double rx = pred[0] - p->obs_xy[2 * o], ry = pred[1] - p->obs_xy[2 * o + 1];
+    out[o] = rx * rx + ry * ry;
+  }
+  return VLBA_OK;
+}
+
 // Camera::project of one camera-frame point; returns 0 when it does not project.
 int vlba_oracle_camera_project(const vlba_camera* cam, const double xc[3], double out[2]) {
   Cam c;

@@ -31,6 +31,7 @@ EXPORTS = {
         C.c_int,
         [P(_abi.Problem), P(_abi.Config), C.c_int, P(C.c_double), P(C.c_uint64)],
     ),
+    "vlba_oracle_squared_residuals": (C.c_int, [P(_abi.Problem), P(_abi.Config), P(C.c_double)]),
     "vlba_oracle_camera_project": (C.c_int, [P(_abi.Camera), P(C.c_double), P(C.c_double)]),
     "vlba_oracle_mono_project": (
         C.c_int,
@@ -100,6 +101,142 @@ def cost(packed: PackedProblem, config: BaConfig | None = None, threads: int = 0
     if st != 0:
         raise RuntimeError(f"oracle cost failed: {_abi.STATUS_NAMES.get(st, st)}")
     return c.value, n.value
+
+
+def squared_residuals(packed: PackedProblem, config: BaConfig | None = None):
+    """Per-observation squared reprojection residual (NaN: not evaluable)."""
+    import numpy as np
+
+    config = config or BaConfig()
+    out = np.empty(packed.num_observations)
+    st = lib().vlba_oracle_squared_residuals(C.byref(packed.abi()), C.byref(config.to_abi()),
+                                             _dp(out))
+    if st != 0:
+        raise RuntimeError(f"oracle residuals failed: {_abi.STATUS_NAMES.get(st, st)}")
+    return out
+
+
+# ------------------------------------------------------------------- GNC
+# BundleAdjustment::optimize_gnc (bundle/lm.rs:28-142) over the oracle's
+# weighted LM, with the surrogate math of the reference's crate gnc
+# (pipelines/slam/src/gnc.rs:150-270) restated here in Python, apart from the
+# library's C++ restatement it checks.
+TLS_TERMINAL_MU = 200.0
+
+
+class GncSurrogate:
+    def __init__(self, kernel: int, c: float, factor: float, max_residual_sq: float):
+        self.kernel, self.c2, self.factor = kernel, c * c, factor
+        s_max = max(max_residual_sq, 0.0)
+        if kernel == _abi.GNC_TRUNCATED_LEAST_SQUARES:
+            denom = 2.0 * s_max - self.c2
+            self.mu = TLS_TERMINAL_MU if denom <= 0.0 else min(max(self.c2 / denom, 2.2250738585072014e-308),
+                                                                  TLS_TERMINAL_MU)
+        else:
+            self.mu = max(2.0 * s_max / self.c2, 1.0)
+
+    def weight(self, s: float) -> float:
+        s = max(s, 0.0)
+        if self.kernel == _abi.GNC_TRUNCATED_LEAST_SQUARES:
+            mu = self.mu
+            lo, hi = mu / (mu + 1.0) * self.c2, (mu + 1.0) / mu * self.c2
+            if s <= lo:
+                return 1.0
+            if s >= hi:
+                return 0.0
+            return (self.c2 * mu * (mu + 1.0) / s) ** 0.5 - mu
+        m = self.mu * self.c2
+        r = m / (s + m)
+        return r * r
+
+    def terminal(self) -> bool:
+        if self.kernel == _abi.GNC_TRUNCATED_LEAST_SQUARES:
+            return self.mu >= TLS_TERMINAL_MU
+        return self.mu <= 1.0
+
+    def anneal(self) -> bool:
+        if self.kernel == _abi.GNC_TRUNCATED_LEAST_SQUARES:
+            self.mu = min(self.mu * self.factor, TLS_TERMINAL_MU)
+        else:
+            self.mu = max(self.mu / self.factor, 1.0)
+        return self.terminal()
+
+
+def _median(v):
+    v = sorted(v)
+    n = len(v)
+    return v[n // 2] if n % 2 else 0.5 * (v[n // 2 - 1] + v[n // 2])
+
+
+def estimate_scale_mad(squared, k: float):
+    import math
+
+    rho = [math.sqrt(s) for s in squared if math.isfinite(s) and s >= 0.0]
+    if len(rho) < 2:
+        return None
+    med = _median(rho)
+    mad = _median([abs(r - med) for r in rho])
+    return med + k * 1.4826 * mad
+
+
+def optimize_gnc(packed: PackedProblem, config: BaConfig, gnc, threads: int = 0):
+    """In place on `packed`: (BaGncResult fields as a dict, final weights)."""
+    import copy
+    import math
+
+    import numpy as np
+
+    none = BaConfig(robust_kernel=_abi_none_kernel())
+    sq = squared_residuals(packed, none)
+    finite = np.isfinite(sq)
+    initial_cost = float(sq[finite].sum())
+    s_max = float(sq[finite].max()) if finite.any() else 0.0
+    c = gnc.c
+    if gnc.auto_scale is not None:
+        est = estimate_scale_mad(sq, gnc.auto_scale)
+        if est is not None:
+            c = max(est, gnc.c)
+    inlier_scale = c
+    state = GncSurrogate(gnc.kernel, c, gnc.anneal_factor, s_max)
+    inner = copy.copy(config)
+    inner.robust_kernel = _abi_none_kernel()
+    inner.max_iterations = max(1, gnc.inner_iterations)
+    w = np.ones(packed.num_observations)
+    outer, converged = 0, False
+    for _ in range(max(1, gnc.max_outer)):
+        outer += 1
+        terminal = state.terminal()
+        sq = squared_residuals(packed, none)
+        if gnc.auto_scale_readapt and gnc.auto_scale is not None:
+            est = estimate_scale_mad(sq, gnc.auto_scale)
+            if est is not None:
+                cc = max(est, gnc.c)
+                state.c2 = cc * cc
+                inlier_scale = cc
+        w = np.array([state.weight(s) if math.isfinite(s) else 1.0 for s in sq])
+        packed.obs_weight = w
+        st, _ = optimize(packed, inner, threads=threads)
+        packed.obs_weight = None
+        if st != 0:
+            raise RuntimeError(f"oracle GNC inner solve failed: {_abi.STATUS_NAMES.get(st, st)}")
+        if terminal:
+            converged = True
+            break
+        state.anneal()
+    sq = squared_residuals(packed, none)
+    w = np.array([state.weight(s) if math.isfinite(s) else math.nan for s in sq])
+    ok = np.isfinite(sq)
+    final_cost = float((w[ok] * sq[ok]).sum())
+    inlier_cost = float(sq[ok & (w >= 0.5)].sum())
+    return {"initial_cost": initial_cost, "final_cost": final_cost, "inlier_cost": inlier_cost,
+            "inlier_scale": inlier_scale, "observation_count": packed.num_observations,
+            "outer_iterations": outer, "converged": converged}, w
+
+
+def _abi_none_kernel():
+    from visloc_ba.problem import RobustKernel
+
+    return RobustKernel.none()
 
 
 def check(packed: PackedProblem, config: BaConfig | None = None):

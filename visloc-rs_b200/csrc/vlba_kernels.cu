@@ -323,8 +323,9 @@ __global__ void __launch_bounds__(256) k_point_prep(Dev d) {
 }
 
 // The damped inverse of point l's H_ll and v = H^-1 g in FP64, from the
-// FP64 sums k_point_prep stores as FP32 (the same formulas; k_point_prep
-// rounds the inverse to FP32 for the other kernels).  The camera diagonal
+// FP64 sums k_point_prep stores as FP32 (its cofactor formulas, with one
+// reciprocal of the determinant; k_point_prep rounds its inverse to FP32 for
+// the other kernels).  Called only for points whose determinant is nonzero.  The camera diagonal
 // needs this precision: when a point has one contributing observation (its
 // others weighted 0, or observed twice by one camera), H_ll is H_o of rank 2
 // and H_o - H_o (H_ll + lambda I)^-1 H_o cancels down to O(lambda), far
@@ -339,9 +340,10 @@ __device__ __forceinline__ void point_inverse64(const Dev& d, uint32_t l, double
     f += lambda;
   }
   const double m22 = dd * f - e * e, m12 = b * f - e * cc, m11 = b * e - dd * cc;
-  const double det = a * m22 - b * m12 + cc * m11;
-  const double i0 = m22 / det, i1 = (cc * e - f * b) / det, i2 = (b * e - dd * cc) / det,
-               i3 = (a * f - cc * cc) / det, i4 = (cc * b - e * a) / det, i5 = (a * dd - b * b) / det;
+  const double rdet = 1.0 / (a * m22 - b * m12 + cc * m11);
+  const double i0 = m22 * rdet, i1 = (cc * e - f * b) * rdet, i2 = (b * e - dd * cc) * rdet,
+               i3 = (a * f - cc * cc) * rdet, i4 = (cc * b - e * a) * rdet,
+               i5 = (a * dd - b * b) * rdet;
   M[0] = i0; M[1] = i1; M[2] = i2;
   M[3] = i1; M[4] = i3; M[5] = i4;
   M[6] = i2; M[7] = i4; M[8] = i5;
@@ -1968,6 +1970,41 @@ cudaError_t launch_reduced_fill(const Dev& d, uint32_t n, uint64_t ne, const dou
 cudaError_t launch_wait_probe(const unsigned int* flag, unsigned long long limit_ns,
                               unsigned int* err, unsigned long long* waited, cudaStream_t s) {
   k_wait_probe<<<1, 32, 0, s>>>(flag, limit_ns, err, waited);
+  return cudaGetLastError();
+}
+
+// Squared reprojection residual of every observation at the state in
+// buffer 0 (after k_state_to_front), in plan order; NaN where the
+// observation cannot be evaluated (behind the sensor or outside the
+// projection's domain): reprojection_squared_residuals (bundle/problem.rs:
+// 756-830), the input of the GNC weights.
+__global__ void __launch_bounds__(256) k_sq_residuals(Dev d, double* out) {
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < d.num_obs;
+       k += gridDim.x * blockDim.x) {
+    const uint32_t p = d.obs_pose[k], l = d.obs_point[k];
+    double q[4], rt[12], X[3], xs[3], pred[2];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) q[a] = d.pose_q[0][4 * (size_t)p + a];
+    quat_to_matrix(q, rt);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      rt[9 + a] = d.pose_t[0][3 * (size_t)p + a];
+      X[a] = d.points[0][3 * (size_t)l + a];
+    }
+    const DevCamera& cam = d.cameras[d.obs_cam[k]];
+    to_sensor(rt, cam, X, xs);
+    double s = __longlong_as_double(0x7ff8000000000000ll);  // NaN
+    if (xs[2] > 0.0 && camera_project(cam, xs, pred)) {
+      const double2 xy = d.obs_xy[k];
+      const double rx = pred[0] - xy.x, ry = pred[1] - xy.y;
+      s = rx * rx + ry * ry;
+    }
+    out[k] = s;
+  }
+}
+
+cudaError_t launch_sq_residuals(const Dev& d, double* out, cudaStream_t s) {
+  k_sq_residuals<<<grid1d(d.num_obs, 256), 256, 0, s>>>(d, out);
   return cudaGetLastError();
 }
 

@@ -28,6 +28,9 @@ cudaError_t launch_wait_probe(const unsigned int* flag, unsigned long long limit
                               unsigned int* err, unsigned long long* waited, cudaStream_t s);
 // Copy each problem's current state into state buffer 0 (for a bulk download).
 cudaError_t launch_state_to_front(const Dev& d, cudaStream_t s);
+// Squared reprojection residual per observation (plan order) at the state in
+// buffer 0; NaN where it cannot be evaluated.
+cudaError_t launch_sq_residuals(const Dev& d, double* out, cudaStream_t s);
 
 // Occupancy-derived grid of the persistent PCG kernel (0 if it cannot run).
 int pcg_grid_size(int tb, int sm_count);

@@ -253,6 +253,7 @@ void build_plan_serial(const vlba_problem* const* problems, const vlba_config* c
     keep(P.obs_slot, old.obs_slot);
     keep(P.obs_xy, old.obs_xy);
     keep(P.obs_w, old.obs_w);
+    keep(P.obs_src, old.obs_src);
     keep(P.cam_obs, old.cam_obs);
   }
   P.tb = tb;
@@ -279,6 +280,7 @@ void build_plan_serial(const vlba_problem* const* problems, const vlba_config* c
   P.obs_slot.resize(tot_obs);
   P.obs_xy.resize(2 * tot_obs);
   P.obs_point.resize(tot_obs);
+  P.obs_src.resize(tot_obs);
   bool weighted = false;
   for (uint32_t i = 0; i < n; ++i) weighted = weighted || problems[i]->obs_weight != nullptr;
   if (weighted) P.obs_w.resize(tot_obs);
@@ -355,6 +357,7 @@ void build_plan_serial(const vlba_problem* const* problems, const vlba_config* c
         P.obs_xy[2 * (size_t)g] = p->obs_xy[2 * (size_t)o];
         P.obs_xy[2 * (size_t)g + 1] = p->obs_xy[2 * (size_t)o + 1];
         if (weighted) P.obs_w[g] = p->obs_weight ? p->obs_weight[o] : 1.0;
+        P.obs_src[g] = o;
       }
     });
     // Per-slot observation lists (ascending point-major index).
@@ -694,6 +697,7 @@ void merge_plans(const std::vector<const Plan*>& parts, Plan* out) {
     keep(P.obs_slot, old.obs_slot);
     keep(P.obs_xy, old.obs_xy);
     keep(P.obs_w, old.obs_w);
+    keep(P.obs_src, old.obs_src);
     keep(P.cam_obs, old.cam_obs);
   }
   if (parts.empty()) throw std::runtime_error("merge of no plans");
@@ -762,6 +766,7 @@ void merge_plans(const std::vector<const Plan*>& parts, Plan* out) {
   P.obs_cam.resize(T.obs);
   P.obs_slot.resize(T.obs);
   P.obs_xy.resize(2 * T.obs);
+  P.obs_src.resize(T.obs);
   bool weighted = false;
   for (const Plan* q : parts) weighted = weighted || !q->obs_w.empty();
   if (weighted) P.obs_w.resize(T.obs);
@@ -824,6 +829,7 @@ void merge_plans(const std::vector<const Plan*>& parts, Plan* out) {
     shift(P.obs_cam, obs_b, Q.obs_cam, cam_b);
     shift_none(P.obs_slot, obs_b, Q.obs_slot, slot_b);
     copy(P.obs_xy, 2 * (size_t)obs_b, Q.obs_xy);
+    copy(P.obs_src, obs_b, Q.obs_src);
     if (weighted) {
       if (Q.obs_w.empty()) std::fill_n(P.obs_w.begin() + obs_b, Q.obs_pose.size(), 1.0);
       else copy(P.obs_w, obs_b, Q.obs_w);

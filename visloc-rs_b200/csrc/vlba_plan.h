@@ -67,6 +67,9 @@ struct Plan {
   // External weight per observation; empty when no problem of the plan has
   // weights (a problem without them gets 1 in a plan that has them).
   ObsArray<double> obs_w;
+  // Each observation's index in its problem's own order (host only: results
+  // per observation go back to the caller in that order).
+  ObsArray<uint32_t> obs_src;
   std::vector<uint32_t> cam_off;
   ObsArray<uint32_t> cam_obs;
 

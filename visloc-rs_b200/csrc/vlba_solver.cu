@@ -28,6 +28,7 @@
 #include <vector>
 
 #include "vlba_kernels.cuh"
+#include "vlba_gnc.h"
 #include "vlba_plan.h"
 
 namespace vlba {
@@ -169,6 +170,9 @@ struct Context {
   char* stage[2] = {nullptr, nullptr};
   size_t stage_cap = 0;
   cudaEvent_t stage_ev[2] = {};
+  // Per-observation squared residuals of a GNC solve (grown on demand).
+  double* gnc_sq = nullptr;
+  size_t gnc_cap = 0;
 };
 
 namespace {
@@ -1056,6 +1060,7 @@ void free_context(Context* c) {
     if (c->stage_ev[i]) cudaEventDestroy(c->stage_ev[i]);
     if (c->stage[i]) cudaFreeHost(c->stage[i]);
   }
+  if (c->gnc_sq) cudaFree(c->gnc_sq);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }
@@ -1286,6 +1291,149 @@ int visloc_ba_cuda_plan(const vlba_problem* problem, const vlba_config* config,
       double b_pcg = 0.0;
       info->bytes_per_iteration = vlba::algorithmic_bytes(plan, pcg_iterations, &b_pcg);
       info->bytes_per_pcg_iteration = b_pcg;
+    }
+  });
+}
+
+void visloc_ba_cuda_default_gnc_config(vlba_gnc_config* gnc) {
+  if (!gnc) return;
+  std::memset(gnc, 0, sizeof *gnc);  // GncConfig::default() (gnc.rs:100-110)
+  gnc->kernel = VLBA_GNC_GEMAN_MCCLURE;
+  gnc->c = 1.0;
+  gnc->anneal_factor = 1.4;
+  gnc->max_outer = 100;
+  gnc->inner_iterations = 5;
+}
+
+int visloc_ba_cuda_optimize_gnc(void* ctx, vlba_problem* problem, const vlba_config* config,
+                                const vlba_gnc_config* gnc, vlba_gnc_result* result,
+                                double* observation_weights) {
+  auto* c = static_cast<Context*>(ctx);
+  if (!c || !problem || !config || !gnc) return VLBA_ERR_INVALID_ARGUMENT;
+  if (result) std::memset(result, 0, sizeof *result);
+  return vlba::guarded(c, [&] {
+    using vlba::Status;
+    if (problem->obs_weight)
+      throw Status(VLBA_ERR_INVALID_ARGUMENT, "GNC sets the observation weights: obs_weight must be NULL");
+    if (gnc->kernel > VLBA_GNC_TRUNCATED_LEAST_SQUARES)
+      throw Status(VLBA_ERR_INVALID_ARGUMENT, "unknown GNC kernel");
+    const uint64_t n = problem->num_observations;
+    // The inner solve: the config's LM with no M-estimator (the GNC weights
+    // are the only robustification) and inner_iterations iterations
+    // (lm.rs:64-68).
+    vlba_config inner = *config;
+    inner.robust_kernel = VLBA_KERNEL_NONE;
+    inner.robust_parameter = 0.0;
+    inner.max_iterations = std::max(1u, gnc->inner_iterations);
+    inner.flags &= ~VLBA_FLAG_PROFILE;
+    std::vector<double> weights(n, 1.0);
+    vlba_problem up = *problem;
+    up.obs_weight = weights.data();  // a weight array on the device, rewritten per level
+    const vlba_problem* probs[1] = {&up};
+    const vlba_config* cfgs[1] = {&inner};
+    vlba::do_upload(c, probs, cfgs, 1, inner.max_iterations, nullptr);
+    c->flags = inner.flags;
+    vlba::Dev& d = c->dev;
+    const vlba::Plan& P = c->plan;
+    cudaStream_t s = c->stream;
+    if (c->gnc_cap < n) {
+      if (c->gnc_sq) cudaFree(c->gnc_sq);
+      c->gnc_sq = nullptr;
+      c->gnc_cap = 0;
+      VLBA_CUDA(cudaMalloc(&c->gnc_sq, std::max<uint64_t>(n, 1) * sizeof(double)));
+      c->gnc_cap = n;
+    }
+    // Squared residuals in plan order at the current state (also left in
+    // state buffer 0).
+    vlba::reset_state(c);  // the uploaded state into buffer 0, control words cleared
+    std::vector<double> sq(n), w(n, 1.0);
+    auto residuals = [&] {
+      vlba::check_launch(vlba::launch_state_to_front(d, s), "state gather");
+      vlba::check_launch(vlba::launch_sq_residuals(d, c->gnc_sq, s), "residuals");
+      VLBA_CUDA(cudaMemcpyAsync(sq.data(), c->gnc_sq, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+      VLBA_CUDA(cudaStreamSynchronize(s));
+    };
+    residuals();
+    double initial_cost = 0.0, s_max = 0.0;
+    for (double v : sq)
+      if (std::isfinite(v)) {
+        initial_cost += v;
+        s_max = std::max(s_max, v);
+      }
+    // Inlier scale: the configured c, or the MAD estimate floored at it
+    // (lm.rs:46-56).
+    double scale = gnc->c;
+    if (gnc->has_auto_scale) {
+      double est = 0.0;
+      if (vlba::estimate_scale_mad(sq, gnc->auto_scale, &est)) scale = std::max(est, gnc->c);
+    }
+    double inlier_scale = scale;
+    vlba::GncState state = vlba::GncState::start(gnc->kernel, scale, gnc->anneal_factor, s_max);
+    uint32_t outer = 0;
+    bool converged = false;
+    uint64_t lm_iterations = 0;
+    double device_ms = 0.0;
+    for (uint32_t level = 0; level < std::max(1u, gnc->max_outer); ++level) {
+      ++outer;
+      const bool terminal = state.terminal();
+      residuals();
+      if (gnc->auto_scale_readapt && gnc->has_auto_scale) {
+        double est = 0.0;
+        if (vlba::estimate_scale_mad(sq, gnc->auto_scale, &est)) {
+          const double cc = std::max(est, gnc->c);
+          state.set_inlier_scale(cc);
+          inlier_scale = cc;
+        }
+      }
+      for (uint64_t k = 0; k < n; ++k) w[k] = std::isfinite(sq[k]) ? state.weight(sq[k]) : 1.0;
+      VLBA_CUDA(cudaMemcpyAsync(const_cast<double*>(d.obs_w), w.data(), n * sizeof(double),
+                                cudaMemcpyHostToDevice, s));
+      // The level starts from the previous level's state.
+      VLBA_CUDA(cudaMemcpyAsync(const_cast<double*>(d.init_pose_q), d.pose_q[0], P.pose_q.size() * 8,
+                                cudaMemcpyDeviceToDevice, s));
+      VLBA_CUDA(cudaMemcpyAsync(const_cast<double*>(d.init_pose_t), d.pose_t[0], P.pose_t.size() * 8,
+                                cudaMemcpyDeviceToDevice, s));
+      VLBA_CUDA(cudaMemcpyAsync(const_cast<double*>(d.init_points), d.points[0], P.points.size() * 8,
+                                cudaMemcpyDeviceToDevice, s));
+      vlba::reset_state(c);
+      const vlba::RunStats rs = vlba::run_lm(c, false, nullptr);
+      device_ms += rs.device_ms;
+      vlba::Ctrl ctrl;
+      VLBA_CUDA(cudaMemcpy(&ctrl, d.ctrl, sizeof ctrl, cudaMemcpyDeviceToHost));
+      lm_iterations += ctrl.iteration;
+      if (terminal) {
+        converged = true;
+        break;
+      }
+      state.anneal();
+    }
+    // Final weights at the recovered estimate, NaN where an observation
+    // cannot be evaluated; the weighted and the inlier-only (w >= 0.5) costs
+    // (lm.rs:99-130).
+    residuals();
+    double final_cost = 0.0, inlier_cost = 0.0;
+    for (uint64_t k = 0; k < n; ++k) {
+      if (!std::isfinite(sq[k])) {
+        w[k] = std::nan("");
+        continue;
+      }
+      w[k] = state.weight(sq[k]);
+      final_cost += w[k] * sq[k];
+      if (w[k] >= 0.5) inlier_cost += sq[k];
+    }
+    vlba::download_problem(c, 0, problem);
+    if (observation_weights)
+      for (uint64_t k = 0; k < n; ++k) observation_weights[P.obs_src[k]] = w[k];
+    if (result) {
+      result->initial_cost = initial_cost;
+      result->final_cost = final_cost;
+      result->inlier_cost = inlier_cost;
+      result->inlier_scale = inlier_scale;
+      result->observation_count = n;
+      result->outer_iterations = outer;
+      result->converged = converged ? 1u : 0u;
+      result->lm_iterations = lm_iterations;
+      result->device_ms = device_ms;
     }
   });
 }

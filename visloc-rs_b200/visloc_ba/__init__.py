@@ -6,9 +6,11 @@ the library's C ABI (_abi.py, solver.py).
 """
 
 from .problem import (  # noqa: F401
+    AUTO_SCALE_K,
     SE3,
     BaConfig,
     BaError,
+    BaGncResult,
     BaIterationStats,
     BaObservation,
     BaResult,
@@ -17,6 +19,7 @@ from .problem import (  # noqa: F401
     BundleAdjustment,
     Camera,
     CameraModel,
+    GncConfig,
     PackedProblem,
     Pose,
     RobustKernel,

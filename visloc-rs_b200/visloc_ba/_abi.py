@@ -66,6 +66,10 @@ FLAG_PROFILE = 1
 FLAG_GRAPH = 2
 FLAG_AUTOTUNE = 4
 
+# enum vlba_gnc_kernel
+GNC_GEMAN_MCCLURE = 0
+GNC_TRUNCATED_LEAST_SQUARES = 1
+
 
 class Camera(C.Structure):
     _fields_ = [
@@ -207,6 +211,34 @@ class TicketInfo(C.Structure):
     ]
 
 
+class GncConfig(C.Structure):
+    _fields_ = [
+        ("kernel", C.c_uint32),
+        ("max_outer", C.c_uint32),
+        ("inner_iterations", C.c_uint32),
+        ("has_auto_scale", C.c_uint32),
+        ("c", C.c_double),
+        ("anneal_factor", C.c_double),
+        ("auto_scale", C.c_double),
+        ("auto_scale_readapt", C.c_uint32),
+        ("reserved", C.c_uint32),
+    ]
+
+
+class GncResult(C.Structure):
+    _fields_ = [
+        ("initial_cost", C.c_double),
+        ("final_cost", C.c_double),
+        ("inlier_cost", C.c_double),
+        ("inlier_scale", C.c_double),
+        ("observation_count", C.c_uint64),
+        ("outer_iterations", C.c_uint32),
+        ("converged", C.c_uint32),
+        ("lm_iterations", C.c_uint64),
+        ("device_ms", C.c_double),
+    ]
+
+
 SOLVER_EXPORTS = {
     "visloc_ba_cuda_abi_version": (C.c_uint32, []),
     "visloc_ba_cuda_default_config": (None, [P(Config)]),
@@ -271,6 +303,11 @@ SOLVER_EXPORTS = {
     "visloc_ba_cuda_cost_noalloc": (
         C.c_int,
         [P(Problem), P(Config), C.c_void_p, C.c_void_p, C.c_void_p, C.c_char_p, C.c_size_t],
+    ),
+    "visloc_ba_cuda_default_gnc_config": (None, [P(GncConfig)]),
+    "visloc_ba_cuda_optimize_gnc": (
+        C.c_int,
+        [C.c_void_p, P(Problem), P(Config), P(GncConfig), P(GncResult), P(C.c_double)],
     ),
 }
 

@@ -270,6 +270,51 @@ class BaConfig:
 
 
 @dataclass
+class GncConfig:
+    """GncConfig (pipelines/slam/src/gnc.rs:50-110) with its defaults."""
+
+    kernel: int = _abi.GNC_GEMAN_MCCLURE
+    c: float = 1.0
+    anneal_factor: float = 1.4
+    max_outer: int = 100
+    inner_iterations: int = 5
+    auto_scale: Optional[float] = None
+    auto_scale_readapt: bool = False
+
+    def to_abi(self) -> _abi.GncConfig:
+        g = _abi.GncConfig()
+        g.kernel = int(self.kernel)
+        g.max_outer = int(self.max_outer)
+        g.inner_iterations = int(self.inner_iterations)
+        g.has_auto_scale = 0 if self.auto_scale is None else 1
+        g.c = float(self.c)
+        g.anneal_factor = float(self.anneal_factor)
+        g.auto_scale = 0.0 if self.auto_scale is None else float(self.auto_scale)
+        g.auto_scale_readapt = 1 if self.auto_scale_readapt else 0
+        return g
+
+
+# GncConfig::auto_scale's recommended k (gnc.rs:92-96).
+AUTO_SCALE_K = 3.5
+
+
+@dataclass
+class BaGncResult:
+    """BaGncResult (bundle/mod.rs:975-1000)."""
+
+    initial_cost: float
+    final_cost: float
+    inlier_cost: float
+    inlier_scale: float
+    observation_count: int
+    outer_iterations: int
+    converged: bool
+    observation_weights: "np.ndarray"
+    lm_iterations: int = 0
+    device_ms: float = 0.0
+
+
+@dataclass
 class BaIterationStats:
     iteration: int
     cost_before: float

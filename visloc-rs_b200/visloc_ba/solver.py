@@ -17,9 +17,11 @@ from . import _abi
 from .problem import (
     BaConfig,
     BaError,
+    BaGncResult,
     BaResult,
     BaScope,
     BundleAdjustment,
+    GncConfig,
     PackedProblem,
     result_from_abi,
 )
@@ -90,6 +92,25 @@ class CudaSolver:
         if st != _abi.OK:
             return st, res
         return st, result_from_abi(res, iters, res.num_iterations)
+
+    def optimize_gnc(self, packed: PackedProblem, config: BaConfig, gnc: GncConfig | None = None):
+        """BundleAdjustment::optimize_gnc (bundle/lm.rs:28-142) in place on
+        `packed` (which must carry no weights of its own).  Returns (status,
+        BaGncResult | None); the weights are in the problem's observation
+        order, NaN where an observation cannot be evaluated."""
+        import numpy as np
+
+        gnc = gnc or GncConfig()
+        res = _abi.GncResult()
+        w = np.empty(packed.num_observations)
+        st = self.lib.visloc_ba_cuda_optimize_gnc(
+            self.ctx, C.byref(packed.abi()), C.byref(config.to_abi()), C.byref(gnc.to_abi()),
+            C.byref(res), w.ctypes.data_as(C.POINTER(C.c_double)))
+        if st != _abi.OK:
+            return st, None
+        return st, BaGncResult(res.initial_cost, res.final_cost, res.inlier_cost, res.inlier_scale,
+                               int(res.observation_count), int(res.outer_iterations),
+                               bool(res.converged), w, int(res.lm_iterations), res.device_ms)
 
     def upload(self, packed: PackedProblem, config: BaConfig) -> int:
         return self.lib.visloc_ba_cuda_upload(self.ctx, C.byref(packed.abi()),
@@ -365,6 +386,21 @@ class GpuBundleAdjuster:
         on the device: each weight multiplies its observation's robust IRLS
         weight and robust cost."""
         return self.solve(ba, config, observation_weights)
+
+    def optimize_gnc(self, ba: BundleAdjustment, config: BaConfig,
+                     gnc: GncConfig | None = None) -> BaGncResult:
+        """BundleAdjustment::optimize_gnc (bundle/lm.rs:28-142) on the device:
+        mutates `ba`; the weights follow the problem's observation order."""
+        packed, pose_ids, lm_ids, missing = ba.pack()
+        st, res = self.solver.optimize_gnc(packed, self._config(config), gnc)
+        if st in (_abi.ERR_MISSING_POSE, _abi.ERR_MISSING_LANDMARK) and missing is not None:
+            raise missing
+        if st in _ERROR_KIND:
+            raise BaError(_ERROR_KIND[st])
+        if st != _abi.OK:
+            raise SolverError(st, self.solver.last_error())
+        ba.unpack(packed, pose_ids, lm_ids)
+        return res
 
     def optimize(self, ba: BundleAdjustment, config: BaConfig, scope: BaScope = BaScope.GLOBAL):
         """BaAccelerator::optimize: None = declined (run the CPU solver)."""
