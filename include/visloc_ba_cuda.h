@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define VLBA_ABI_VERSION 2u
+#define VLBA_ABI_VERSION 3u
 
 /* ------------------------------------------------------------------ status */
 /* Return codes.  The Rust shim maps VLBA_DECLINED to `None` (the caller then
@@ -55,7 +55,8 @@ enum vlba_status {
   VLBA_ERR_OUT_OF_MEMORY = 12,         /* device memory exhausted */
   VLBA_ERR_TIMEOUT = 13,               /* a bounded device wait gave up */
   VLBA_ERR_BUSY = 14,                  /* server queue full / ticket pending */
-  VLBA_ERR_INVALID_OBSERVATION_WEIGHT = 15 /* BaError::InvalidObservationWeight(index) */
+  VLBA_ERR_INVALID_OBSERVATION_WEIGHT = 15, /* BaError::InvalidObservationWeight(index) */
+  VLBA_ERR_MISSING_STEREO_BASELINE = 16  /* BaError::MissingStereoBaseline */
 };
 
 /* ------------------------------------------------------------------ camera */
@@ -124,6 +125,27 @@ typedef struct vlba_problem {
    * VLBA_ERR_INVALID_OBSERVATION_WEIGHT with the observation's index.  NULL:
    * every weight is 1 (BundleAdjustment::optimize). */
   const double* obs_weight;
+  /* Stereo observations (ABI version 3).  obs_kind[o] (NULL: every
+   * observation is of kind 0):
+   *   0  a monocular or rig observation as described above;
+   *   1  BaStereoObservation (bundle/mod.rs:213-221), rectified stereo: left
+   *      pixel obs_xy, observed right column u_r = obs_stereo[2o]; residual
+   *      (u_l, v_l, u_r) with u_r predicted as u_l - fx stereo_baseline / z
+   *      (normal_equations.rs:496-570);
+   *   2  BaGeneralStereoObservation (mod.rs:223-237), calibrated stereo: left
+   *      pixel obs_xy, right pixel (obs_stereo[2o], obs_stereo[2o+1]) through
+   *      cameras[obs_right_camera[o]], whose sensor_from_rig is the rig
+   *      transform T_right<-left (sqrt_qr.rs:465-518).
+   * Kinds 1 and 2 project through cameras[0] (BundleAdjustment::camera) and
+   * the right camera with their pinhole intrinsics, without distortion, as
+   * the reference does; cameras[0] must then be PINHOLE or SIMPLE_PINHOLE
+   * (check_stereo_camera_model, problem.rs:733-745). */
+  const uint8_t* obs_kind;
+  const double* obs_stereo;          /* [2 * num_observations] (kinds 1 and 2) */
+  const uint32_t* obs_right_camera;  /* [num_observations] (kind 2) */
+  double stereo_baseline;            /* BundleAdjustment::stereo_baseline; finite and > 0
+                                        when an observation is of kind 1, else
+                                        VLBA_ERR_MISSING_STEREO_BASELINE */
 } vlba_problem;
 
 /* ------------------------------------------------------------------ config */
@@ -492,12 +514,14 @@ int visloc_ba_cuda_optimize_gnc(void* ctx, vlba_problem* problem, const vlba_con
  *
  * The same robust cost and non-projectable count as visloc_ba_cuda_cost, for
  * a problem whose arrays are already in DEVICE memory: pose_q, pose_t,
- * landmarks, obs_pose, obs_landmark, obs_xy, obs_camera and obs_weight are
- * device pointers; `cameras` (at most VLBA_NOALLOC_MAX_CAMERAS) is read on
- * the host during the call; pose_fixed and landmark_fixed are ignored.
- * `cost` (one double) and `counts` (two words: non-projectable observations,
- * and observations skipped for a pose, landmark or camera index out of range
- * or a weight that is negative or not finite)
+ * landmarks, obs_pose, obs_landmark, obs_xy, obs_camera, obs_weight,
+ * obs_kind, obs_stereo and obs_right_camera are device pointers; `cameras`
+ * (at most VLBA_NOALLOC_MAX_CAMERAS) is read on the host during the call;
+ * pose_fixed and landmark_fixed are ignored.  `cost` (one double) and
+ * `counts` (two words: non-projectable observations, and observations
+ * skipped for a pose, landmark or camera index out of range, a weight that
+ * is negative or not finite, or a stereo observation without a usable
+ * baseline, right camera or pinhole cameras[0])
  * are device pointers, written by a kernel enqueued on `stream` (a
  * cudaStream_t of the current device; NULL = default stream); the call
  * returns without waiting for it.

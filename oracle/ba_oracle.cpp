@@ -411,6 +411,93 @@ bool residual_jacobians(const Problem& P, size_t o, double r[2], double jp[12], 
   return true;
 }
 
+// Stereo observations (vlba_problem.obs_kind 1 and 2): rectified,
+// normal_equations.rs:496-570 -- r = (u_l, v_l, u_r) with u_r predicted as
+// u_l - fx b / z -- and calibrated general stereo, general_stereo_residual_
+// jacobians (sqrt_qr.rs:465-518) -- r = (u_l, v_l, u_r, v_r) with the right
+// point T_right<-left x_left.  Both through the pinhole intrinsics of
+// BundleAdjustment::camera (cams[0]) and the right camera, no distortion.
+// Returns the number of residual rows, 0 when a camera sees the point at
+// z <= 0; jp is m x 6, jl m x 3, row-major.
+int stereo_residual_jacobians(const Problem& P, size_t o, uint32_t kind, double* r, double* jp,
+                              double* jl) {
+  const Se3& T = P.poses[P.p->obs_pose[o]];
+  const V3& X = P.points[P.p->obs_landmark[o]];
+  const Cam& cl = P.cams[0];
+  double R[9], xsk[9], rxs[9];
+  quat_to_matrix(T.q, R);
+  skew(X, xsk);
+  mat3_mul(R, xsk, rxs);
+  double D[18];  // d x_left / d xi = [R | -R [X]x]
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) {
+      D[a * 6 + b] = R[a * 3 + b];
+      D[a * 6 + 3 + b] = -rxs[a * 3 + b];
+    }
+  const V3 xl = se3_transform(T, X);
+  if (xl.z <= 0.0) return 0;
+  const double* xy = P.p->obs_xy + 2 * o;
+  const double* st = P.p->obs_stereo + 2 * o;
+  // Rows (u, v) of a pinhole camera at point p: pixel and d/d p.
+  auto rows = [](const Cam& c, const V3& p, double* pix, double* j) {
+    const double z_inv = 1.0 / p.z, z_inv2 = z_inv * z_inv;
+    pix[0] = c.fx * p.x / p.z + c.cx;
+    pix[1] = c.fy * p.y / p.z + c.cy;
+    j[0] = c.fx * z_inv; j[1] = 0.0; j[2] = -c.fx * p.x * z_inv2;
+    j[3] = 0.0; j[4] = c.fy * z_inv; j[5] = -c.fy * p.y * z_inv2;
+  };
+  double pix[2], jpi[12];  // up to 4 rows of d pixel / d x_left
+  rows(cl, xl, pix, jpi);
+  r[0] = pix[0] - xy[0];
+  r[1] = pix[1] - xy[1];
+  int m;
+  if (kind == 1) {
+    const double b = P.p->stereo_baseline;
+    const double z_inv = 1.0 / xl.z;
+    r[2] = (pix[0] - cl.fx * b / xl.z) - st[0];
+    jpi[6] = cl.fx * z_inv;
+    jpi[7] = 0.0;
+    jpi[8] = -cl.fx * (xl.x - b) * z_inv * z_inv;
+    m = 3;
+  } else {
+    const Cam& cr = P.cams[P.p->obs_right_camera[o]];
+    const V3 xr = se3_transform(cr.sensor_from_rig, xl);
+    if (xr.z <= 0.0) return 0;
+    double pr[2], jr[6], Rr[9];
+    rows(cr, xr, pr, jr);
+    r[2] = pr[0] - st[0];
+    r[3] = pr[1] - st[1];
+    quat_to_matrix(cr.sensor_from_rig.q, Rr);
+    for (int a = 0; a < 2; ++a)  // d right pixel / d x_left = j_right Rr
+      for (int b = 0; b < 3; ++b) {
+        double s = 0.0;
+        for (int k = 0; k < 3; ++k) s += jr[a * 3 + k] * Rr[k * 3 + b];
+        jpi[6 + a * 3 + b] = s;
+      }
+    m = 4;
+  }
+  for (int a = 0; a < m; ++a) {
+    for (int b = 0; b < 6; ++b) {
+      double s = 0.0;
+      for (int k = 0; k < 3; ++k) s += jpi[a * 3 + k] * D[k * 6 + b];
+      jp[a * 6 + b] = s;
+    }
+    for (int b = 0; b < 3; ++b) {
+      double s = 0.0;
+      for (int k = 0; k < 3; ++k) s += jpi[a * 3 + k] * R[k * 3 + b];
+      jl[a * 3 + b] = s;
+    }
+  }
+  return m;
+}
+
+// Any observation: its residual rows (2, 3 or 4; 0 = not evaluable).
+int obs_residual_jacobians(const Problem& P, size_t o, double* r, double* jp, double* jl) {
+  const uint32_t kind = P.p->obs_kind ? P.p->obs_kind[o] : 0u;
+  if (kind == 0) return residual_jacobians(P, o, r, jp, jl) ? 2 : 0;
+  return stereo_residual_jacobians(P, o, kind, r, jp, jl);
+}
+
 // robust_cost_weighted + nonprojectable_observation_count (problem.rs:252-304,
 // 497-560): cost over projectable observations, count of the others.
 void cost_and_nonprojectable(const Problem& P, int threads, double* cost, uint64_t* bad) {
@@ -425,6 +512,20 @@ void cost_and_nonprojectable(const Problem& P, int threads, double* cost, uint64
     uint64_t b = 0;
     const size_t lo = (size_t)ci * chunk, hi = std::min(n, lo + chunk);
     for (size_t o = lo; o < hi; ++o) {
+      if (P.p->obs_kind && P.p->obs_kind[o] != 0) {
+        // Stereo: robust cost of the squared norm of its residual rows.
+        double r[4], jp[24], jl[12];
+        const int m = obs_residual_jacobians(P, o, r, jp, jl);
+        if (!m) {
+          ++b;
+          continue;
+        }
+        double ss = 0.0;
+        for (int i = 0; i < m; ++i) ss += r[i] * r[i];
+        const double rc = P.kernel.cost(ss);
+        s += P.p->obs_weight ? P.p->obs_weight[o] * rc : rc;
+        continue;
+      }
       const Se3& T = P.poses[P.p->obs_pose[o]];
       const V3& X = P.points[P.p->obs_landmark[o]];
       const Cam& c = P.cam_of(o);
@@ -609,15 +710,18 @@ void build_normal(const Problem& P, const Slots& S, int threads, Normal* N) {
   N->h_ll.assign(nl * 9, 0.0);
   N->b_l.assign(nl * 3, 0.0);
   N->cross.assign(nl, {});
-  struct Contrib { double r[2], jp[12], jl[6], w; bool ok; };
+  struct Contrib { double r[4], jp[24], jl[12], w; int m; bool ok; };
   std::vector<Contrib> c(no);
 #pragma omp parallel for schedule(static) num_threads(threads)
   for (long long oo = 0; oo < (long long)no; ++oo) {
     Contrib& k = c[oo];
-    k.ok = residual_jacobians(P, (size_t)oo, k.r, k.jp, k.jl);
+    k.m = obs_residual_jacobians(P, (size_t)oo, k.r, k.jp, k.jl);
+    k.ok = k.m > 0;
     // kernel.weight(s) * the external weight (normal_equations.rs:458).
     if (k.ok) {
-      k.w = P.kernel.weight(k.r[0] * k.r[0] + k.r[1] * k.r[1]);
+      double s = 0.0;
+      for (int i = 0; i < k.m; ++i) s += k.r[i] * k.r[i];
+      k.w = P.kernel.weight(s);
       if (P.p->obs_weight) k.w *= P.p->obs_weight[oo];
     }
   }
@@ -638,10 +742,13 @@ void build_normal(const Problem& P, const Slots& S, int threads, Normal* N) {
         double* b = &N->b_p[ps * 6];
         for (int rr = 0; rr < 6; ++rr) {
           for (int cc = 0; cc < 6; ++cc) {
-            const double v = k.jp[rr] * k.jp[cc] + k.jp[6 + rr] * k.jp[6 + cc];
+            double v = 0.0;
+            for (int i = 0; i < k.m; ++i) v += k.jp[6 * i + rr] * k.jp[6 * i + cc];
             h[rr * 6 + cc] += k.w * v;
           }
-          b[rr] += k.w * (k.jp[rr] * k.r[0] + k.jp[6 + rr] * k.r[1]);
+          double g = 0.0;
+          for (int i = 0; i < k.m; ++i) g += k.jp[6 * i + rr] * k.r[i];
+          b[rr] += k.w * g;
         }
       }
       const int64_t ls = S.lm_slot[P.p->obs_landmark[o]];
@@ -650,17 +757,23 @@ void build_normal(const Problem& P, const Slots& S, int threads, Normal* N) {
         double* b = &N->b_l[ls * 3];
         for (int rr = 0; rr < 3; ++rr) {
           for (int cc = 0; cc < 3; ++cc) {
-            const double v = k.jl[rr] * k.jl[cc] + k.jl[3 + rr] * k.jl[3 + cc];
+            double v = 0.0;
+            for (int i = 0; i < k.m; ++i) v += k.jl[3 * i + rr] * k.jl[3 * i + cc];
             h[rr * 3 + cc] += k.w * v;
           }
-          b[rr] += k.w * (k.jl[rr] * k.r[0] + k.jl[3 + rr] * k.r[1]);
+          double g = 0.0;
+          for (int i = 0; i < k.m; ++i) g += k.jl[3 * i + rr] * k.r[i];
+          b[rr] += k.w * g;
         }
         if (ps >= 0) {
           Cross x;
           x.pose = (uint32_t)ps;
           for (int rr = 0; rr < 6; ++rr)
-            for (int cc = 0; cc < 3; ++cc)
-              x.a[rr * 3 + cc] = k.w * (k.jp[rr] * k.jl[cc] + k.jp[6 + rr] * k.jl[3 + cc]);
+            for (int cc = 0; cc < 3; ++cc) {
+              double v = 0.0;
+              for (int i = 0; i < k.m; ++i) v += k.jp[6 * i + rr] * k.jl[3 * i + cc];
+              x.a[rr * 3 + cc] = k.w * v;
+            }
           N->cross[ls].push_back(x);
         }
       }
@@ -818,25 +931,56 @@ bool load_problem(const vlba_problem* p, const vlba_config* cfg, Problem* P, int
       *status = VLBA_ERR_UNSUPPORTED_CAMERA_MODEL;
       return false;
     }
-  // Order of the checks of lm.rs:168-229.
+  // Order of the checks of lm.rs:168-229: the stereo camera model
+  // (check_stereo_camera_model, problem.rs:733-745), then counts, then each
+  // observation list in turn -- monocular, rectified stereo (its baseline
+  // first), general stereo, rig.
+  bool rectified = false, general = false;
+  if (p->obs_kind)
+    for (uint64_t o = 0; o < p->num_observations; ++o) {
+      if (p->obs_kind[o] > 2) { *status = VLBA_ERR_INVALID_ARGUMENT; return false; }
+      rectified = rectified || p->obs_kind[o] == 1;
+      general = general || p->obs_kind[o] == 2;
+    }
+  if (((rectified || general) && !p->obs_stereo) || (general && !p->obs_right_camera)) {
+    *status = VLBA_ERR_INVALID_ARGUMENT;
+    return false;
+  }
+  if ((rectified || general) && p->cameras[0].model != VLBA_CAMERA_PINHOLE &&
+      p->cameras[0].model != VLBA_CAMERA_SIMPLE_PINHOLE) {
+    *status = VLBA_ERR_UNSUPPORTED_CAMERA_MODEL;
+    return false;
+  }
   if (p->num_poses == 0) { *status = VLBA_ERR_NO_POSES; return false; }
   if (p->num_observations == 0) { *status = VLBA_ERR_NO_OBSERVATIONS; return false; }
   if (p->num_landmarks == 0) { *status = VLBA_ERR_NO_LANDMARKS; return false; }
-  for (uint64_t o = 0; o < p->num_observations; ++o) {
-    if (p->obs_pose[o] >= p->num_poses) {
-      *status = VLBA_ERR_MISSING_POSE;
-      if (err_index) *err_index = p->obs_pose[o];
+  const int order[4] = {P->per_obs_camera ? -1 : 0, 1, 2, P->per_obs_camera ? 0 : -1};
+  for (int li = 0; li < 4; ++li) {
+    const int kind = order[li];
+    if (kind < 0) continue;
+    if (kind == 1 && rectified &&
+        !(std::isfinite(p->stereo_baseline) && p->stereo_baseline > 0.0)) {
+      *status = VLBA_ERR_MISSING_STEREO_BASELINE;
       return false;
     }
-    if (p->obs_landmark[o] >= p->num_landmarks) {
-      *status = VLBA_ERR_MISSING_LANDMARK;
-      if (err_index) *err_index = p->obs_landmark[o];
-      return false;
-    }
-    if (P->per_obs_camera && p->obs_camera[o] >= p->num_cameras) {
-      *status = VLBA_ERR_INVALID_ARGUMENT;
-      if (err_index) *err_index = o;
-      return false;
+    for (uint64_t o = 0; o < p->num_observations; ++o) {
+      if ((p->obs_kind ? (int)p->obs_kind[o] : 0) != kind) continue;
+      if (p->obs_pose[o] >= p->num_poses) {
+        *status = VLBA_ERR_MISSING_POSE;
+        if (err_index) *err_index = p->obs_pose[o];
+        return false;
+      }
+      if (p->obs_landmark[o] >= p->num_landmarks) {
+        *status = VLBA_ERR_MISSING_LANDMARK;
+        if (err_index) *err_index = p->obs_landmark[o];
+        return false;
+      }
+      if ((kind == 0 && P->per_obs_camera && p->obs_camera[o] >= p->num_cameras) ||
+          (kind == 2 && p->obs_right_camera[o] >= p->num_cameras)) {
+        *status = VLBA_ERR_INVALID_ARGUMENT;
+        if (err_index) *err_index = o;
+        return false;
+      }
     }
   }
   P->poses.resize(p->num_poses);
@@ -900,6 +1044,14 @@ int vlba_oracle_squared_residuals(const vlba_problem* p, const vlba_config* cfg,
   int status;
   if (!load_problem(p, cfg, &P, &status, nullptr)) return status;
   for (uint64_t o = 0; o < p->num_observations; ++o) {
+    if (p->obs_kind && p->obs_kind[o] != 0) {
+      double r[4], jp[24], jl[12];
+      const int m = obs_residual_jacobians(P, o, r, jp, jl);
+      double ss = 0.0;
+      for (int i = 0; i < m; ++i) ss += r[i] * r[i];
+      out[o] = m ? ss : std::numeric_limits<double>::quiet_NaN();
+      continue;
+    }
     const Se3& T = P.poses[p->obs_pose[o]];
     const Cam& c = P.cam_of(o);
     V3 xc = se3_transform(T, P.points[p->obs_landmark[o]]);

@@ -40,7 +40,8 @@ def test_library_exports_every_declared_symbol():
 
 def test_struct_sizes_match_the_header_layout():
     assert C.sizeof(_abi.Camera) == 8 + 8 * 8 + 4 * 8 + 3 * 8
-    assert C.sizeof(_abi.Problem) == 3 * 8 + 9 * 8 + 8 + 8 + 8  # ... cameras, obs_weight
+    # ... cameras, obs_weight, then obs_kind, obs_stereo, obs_right_camera, stereo_baseline
+    assert C.sizeof(_abi.Problem) == 3 * 8 + 9 * 8 + 8 + 8 + 8 + 4 * 8
     assert C.sizeof(_abi.Iteration) == 8 + 5 * 8 + 8 + 8 + 4 * 8
 
 

@@ -30,6 +30,11 @@
 namespace vlba {
 
 constexpr uint32_t kNone = 0xFFFFFFFFu;
+
+// Observation kinds (vlba_problem.obs_kind).
+constexpr uint32_t kObsMono = 0;           // BaObservation / BaRigObservation
+constexpr uint32_t kObsStereo = 1;         // BaStereoObservation (rectified)
+constexpr uint32_t kObsGeneralStereo = 2;  // BaGeneralStereoObservation
 constexpr int kBlock = 36;             // floats in a 6x6 block
 // Every device wait (on an mbarrier, a counter or a flag that another block
 // writes) gives up after this long, sets an error bit and lets its kernel
@@ -156,6 +161,12 @@ struct Dev {
   const uint32_t* obs_slot;    // [K] variable slot of the pose or kNone
   const double2* obs_xy;       // [K]
   const double* obs_w;         // [K] external observation weights, or null (all 1)
+  // Stereo observations (null when the plan has none): kind per observation
+  // (kObsMono / kObsStereo / kObsGeneralStereo), its stereo data ((u_r,
+  // baseline) rectified, the right pixel general) and right camera.
+  const uint8_t* obs_kind;     // [K]
+  const double2* obs_st;       // [K]
+  const uint32_t* obs_rcam;    // [K]
   float4* obs_h;               // [2 K]: {h00,h01,h02,h11} {h12,h22,point,X.z}
   float4* obs_e;               // [K]:   {e0,e1,e2,w}
   float4* obs_p;               // [2 K]: the observation's point, per trial:

@@ -128,5 +128,79 @@ __device__ __forceinline__ bool project_jacobian(const DevCamera& c, const doubl
   return ok;
 }
 
+// d(pinhole pixel)/d(sensor point) rows of camera c at p (z > 0), appended
+// as two rows of j (row-major, 3 wide), and the pixel (project_pinhole,
+// jacobians.rs:115-124, and pinhole_projection_jacobian, sqrt_qr.rs:445-463:
+// no distortion).
+__device__ __forceinline__ void pinhole_rows(const DevCamera& c, const double* p, double* pix,
+                                             double* j) {
+  const double z_inv = 1.0 / p[2];
+  pix[0] = c.fx * p[0] * z_inv + c.cx;
+  pix[1] = c.fy * p[1] * z_inv + c.cy;
+  if (j) {
+    j[0] = c.fx * z_inv;
+    j[1] = 0.0;
+    j[2] = -c.fx * p[0] * z_inv * z_inv;
+    j[3] = 0.0;
+    j[4] = c.fy * z_inv;
+    j[5] = -c.fy * p[1] * z_inv * z_inv;
+  }
+}
+
+// Residual rows of a stereo observation at its left-sensor point xs and,
+// when jl is not null, d r / d X (m x 3, row-major) for the world -> left
+// sensor rotation Re.  Returns m (3 or 4), or 0 when a camera sees the point
+// at z <= 0 (the observation does not count).
+//   kind 1, rectified (normal_equations.rs:496-570): r = (u_l, v_l, u_r)
+//     predicted minus observed with u_r = u_l - fx b / z; st = (u_r observed,
+//     baseline b).
+//   kind 2, general (sqrt_qr.rs:465-518): r = (u_l, v_l, u_r, v_r) with the
+//     right point camR.R xs + camR.t (T_right<-left) through camR's pinhole
+//     intrinsics; st = the right pixel.
+__device__ __forceinline__ int stereo_rows(uint32_t kind, const DevCamera& camL,
+                                           const DevCamera& camR, double2 xy, double2 st,
+                                           const double* xs, const double* Re, double* r,
+                                           double* jl) {
+  if (!(xs[2] > 0.0)) return 0;
+  double pix[2], jp[6];
+  pinhole_rows(camL, xs, pix, jl ? jp : nullptr);
+  r[0] = pix[0] - xy.x;
+  r[1] = pix[1] - xy.y;
+  if (kind == kObsStereo) {
+    const double z_inv = 1.0 / xs[2];
+    r[2] = (pix[0] - camL.fx * st.y * z_inv) - st.x;
+    if (jl) {
+      const double j3[3] = {camL.fx * z_inv, 0.0, -camL.fx * (xs[0] - st.y) * z_inv * z_inv};
+      for (int b = 0; b < 3; ++b) {
+        jl[b] = jp[0] * Re[b] + jp[1] * Re[3 + b] + jp[2] * Re[6 + b];
+        jl[3 + b] = jp[3] * Re[b] + jp[4] * Re[3 + b] + jp[5] * Re[6 + b];
+        jl[6 + b] = j3[0] * Re[b] + j3[1] * Re[3 + b] + j3[2] * Re[6 + b];
+      }
+    }
+    return 3;
+  }
+  double xr[3];
+  for (int a = 0; a < 3; ++a)
+    xr[a] = camR.R[a * 3] * xs[0] + camR.R[a * 3 + 1] * xs[1] + camR.R[a * 3 + 2] * xs[2] + camR.t[a];
+  if (!(xr[2] > 0.0)) return 0;
+  double pr[2], jr[6];
+  pinhole_rows(camR, xr, pr, jl ? jr : nullptr);
+  r[2] = pr[0] - st.x;
+  r[3] = pr[1] - st.y;
+  if (jl) {
+    double RR[9];  // world -> right sensor rotation: camR.R Re
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b)
+        RR[a * 3 + b] = camR.R[a * 3] * Re[b] + camR.R[a * 3 + 1] * Re[3 + b] + camR.R[a * 3 + 2] * Re[6 + b];
+    for (int b = 0; b < 3; ++b) {
+      jl[b] = jp[0] * Re[b] + jp[1] * Re[3 + b] + jp[2] * Re[6 + b];
+      jl[3 + b] = jp[3] * Re[b] + jp[4] * Re[3 + b] + jp[5] * Re[6 + b];
+      jl[6 + b] = jr[0] * RR[b] + jr[1] * RR[3 + b] + jr[2] * RR[6 + b];
+      jl[9 + b] = jr[3] * RR[b] + jr[4] * RR[3 + b] + jr[5] * RR[6 + b];
+    }
+  }
+  return 4;
+}
+
 }  // namespace
 }  // namespace vlba

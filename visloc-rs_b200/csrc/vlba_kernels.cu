@@ -193,7 +193,44 @@ __global__ void __launch_bounds__(256) k_linearize(Dev d) {
       to_sensor(rt, cam, X, xs);
       float h[6] = {0, 0, 0, 0, 0, 0}, e[3] = {0, 0, 0};
       float wf = 0.0f;
-      if (project_jacobian(cam, xs, pred, jpi)) {
+      const uint32_t kind = d.obs_kind ? d.obs_kind[k] : kObsMono;
+      if (kind != kObsMono) {
+        // Stereo: 3 or 4 residual rows through the same J_l factor.
+        double Re[9];
+        if (cam.rig) {
+          for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b)
+              Re[a * 3 + b] = cam.R[a * 3] * rt[b] + cam.R[a * 3 + 1] * rt[3 + b] +
+                              cam.R[a * 3 + 2] * rt[6 + b];
+        } else {
+#pragma unroll
+          for (int a = 0; a < 9; ++a) Re[a] = rt[a];
+        }
+        double r[4], jl[12];
+        const int m = stereo_rows(kind, cam, d.cameras[d.obs_rcam[k]], d.obs_xy[k], d.obs_st[k], xs,
+                                  Re, r, jl);
+        if (m) {
+          double ss = 0.0;
+          for (int i = 0; i < m; ++i) ss += r[i] * r[i];
+          double w = robust_weight(lp.robust_kernel, lp.robust_parameter, ss);
+          if (d.obs_w) w *= d.obs_w[k];
+          wf = (float)w;
+          float jf[12], rf[4];
+          for (int i = 0; i < 3 * m; ++i) jf[i] = (float)jl[i];
+          for (int i = 0; i < m; ++i) rf[i] = (float)r[i];
+          const int ab[6][2] = {{0, 0}, {0, 1}, {0, 2}, {1, 1}, {1, 2}, {2, 2}};
+          for (int q = 0; q < 6; ++q) {
+            float acc = 0.0f;
+            for (int i = 0; i < m; ++i) acc += jf[3 * i + ab[q][0]] * jf[3 * i + ab[q][1]];
+            h[q] = wf * acc;
+          }
+          for (int a = 0; a < 3; ++a) {
+            float acc = 0.0f;
+            for (int i = 0; i < m; ++i) acc += jf[3 * i + a] * rf[i];
+            e[a] = wf * acc;
+          }
+        }
+      } else if (project_jacobian(cam, xs, pred, jpi)) {
         const double2 xy = d.obs_xy[k];
         const double rx = pred[0] - xy.x, ry = pred[1] - xy.y;
         // The robust IRLS weight times the external weight
@@ -775,13 +812,28 @@ __global__ void __launch_bounds__(256) k_cost(Dev d) {
       const double* rt = d.pose_rt[pose_buf] + 12 * (size_t)d.obs_pose[k];
       double xs[3], pred[2];
       to_sensor(rt, cam, Xk, xs);
-      if (!(xs[2] > 0.0) || !camera_project(cam, xs, pred)) {
-        ++bad;
-        continue;
+      double ss;
+      const uint32_t kind = d.obs_kind ? d.obs_kind[k] : kObsMono;
+      if (kind != kObsMono) {
+        double r[4];
+        const int m = stereo_rows(kind, cam, d.cameras[d.obs_rcam[k]], d.obs_xy[k], d.obs_st[k], xs,
+                                  nullptr, r, nullptr);
+        if (!m) {
+          ++bad;
+          continue;
+        }
+        ss = 0.0;
+        for (int i = 0; i < m; ++i) ss += r[i] * r[i];
+      } else {
+        if (!(xs[2] > 0.0) || !camera_project(cam, xs, pred)) {
+          ++bad;
+          continue;
+        }
+        const double2 xy = d.obs_xy[k];
+        const double rx = pred[0] - xy.x, ry = pred[1] - xy.y;
+        ss = rx * rx + ry * ry;
       }
-      const double2 xy = d.obs_xy[k];
-      const double rx = pred[0] - xy.x, ry = pred[1] - xy.y;
-      const double rc = robust_cost(lp.robust_kernel, lp.robust_parameter, rx * rx + ry * ry);
+      const double rc = robust_cost(lp.robust_kernel, lp.robust_parameter, ss);
       cost += d.obs_w ? d.obs_w[k] * rc : rc;  // w * rho(s) (problem.rs:497-560)
     }
     const double tc = block_sum<double, 256>(cost, red);
@@ -1994,7 +2046,16 @@ __global__ void __launch_bounds__(256) k_sq_residuals(Dev d, double* out) {
     const DevCamera& cam = d.cameras[d.obs_cam[k]];
     to_sensor(rt, cam, X, xs);
     double s = __longlong_as_double(0x7ff8000000000000ll);  // NaN
-    if (xs[2] > 0.0 && camera_project(cam, xs, pred)) {
+    const uint32_t kind = d.obs_kind ? d.obs_kind[k] : kObsMono;
+    if (kind != kObsMono) {
+      double r[4];
+      const int m = stereo_rows(kind, cam, d.cameras[d.obs_rcam[k]], d.obs_xy[k], d.obs_st[k], xs,
+                                nullptr, r, nullptr);
+      if (m) {
+        s = 0.0;
+        for (int i = 0; i < m; ++i) s += r[i] * r[i];
+      }
+    } else if (xs[2] > 0.0 && camera_project(cam, xs, pred)) {
       const double2 xy = d.obs_xy[k];
       const double rx = pred[0] - xy.x, ry = pred[1] - xy.y;
       s = rx * rx + ry * ry;

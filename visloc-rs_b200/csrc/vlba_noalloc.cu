@@ -70,6 +70,11 @@ struct NoallocArgs {
   const double2* obs_xy;
   const uint32_t* obs_camera;  // null: cameras[0] for every observation
   const double* obs_weight;    // null: every weight 1
+  const uint8_t* obs_kind;     // null: every observation monocular or rig
+  const double* obs_stereo;
+  const uint32_t* obs_right_camera;
+  double stereo_baseline;
+  uint32_t stereo_camera_ok;   // cameras[0] is PINHOLE or SIMPLE_PINHOLE
   uint32_t num_cameras;
   uint32_t robust_kernel;
   double robust_parameter;
@@ -110,10 +115,17 @@ __global__ void __launch_bounds__(256) k_cost_noalloc(const NoallocArgs a, unsig
     unsigned long long bad = 0, invalid = 0;
     if (o < a.num_obs) {
       const uint32_t ip = a.obs_pose[o], il = a.obs_landmark[o];
-      const uint32_t ic = a.obs_camera ? a.obs_camera[o] : 0u;
+      const uint32_t kind = a.obs_kind ? a.obs_kind[o] : kObsMono;
+      const uint32_t ic = (kind == kObsMono && a.obs_camera) ? a.obs_camera[o] : 0u;
+      const uint32_t rc = (kind == kObsGeneralStereo && a.obs_right_camera) ? a.obs_right_camera[o] : 0u;
       const double w = a.obs_weight ? a.obs_weight[o] : 1.0;
+      const bool stereo_ok =
+          kind == kObsMono ||
+          (kind <= kObsGeneralStereo && a.stereo_camera_ok && rc < a.num_cameras &&
+           (kind != kObsGeneralStereo || a.obs_right_camera) &&
+           (kind != kObsStereo || (isfinite(a.stereo_baseline) && a.stereo_baseline > 0.0)));
       if (ip >= a.num_poses || il >= a.num_landmarks || ic >= a.num_cameras || !isfinite(w) ||
-          w < 0.0) {
+          w < 0.0 || !stereo_ok) {
         invalid = 1;
       } else {
         double q[4], rt[12], X[3], xs[3], pred[2];
@@ -127,7 +139,22 @@ __global__ void __launch_bounds__(256) k_cost_noalloc(const NoallocArgs a, unsig
         }
         const DevCamera& cam = a.cameras[ic];
         to_sensor(rt, cam, X, xs);
-        if (!(xs[2] > 0.0) || !camera_project(cam, xs, pred)) {
+        if (kind != kObsMono) {
+          const double2 st = kind == kObsStereo
+                                 ? make_double2(a.obs_stereo[2 * o], a.stereo_baseline)
+                                 : make_double2(a.obs_stereo[2 * o], a.obs_stereo[2 * o + 1]);
+          double r[4];
+          const int m = stereo_rows(kind, cam, a.cameras[rc], a.obs_xy[o], st, xs, nullptr, r,
+                                    nullptr);
+          if (!m) {
+            bad = 1;
+          } else {
+            double ss = 0.0;
+            for (int i = 0; i < m; ++i) ss += r[i] * r[i];
+            cost = robust_cost(a.robust_kernel, a.robust_parameter, ss);
+            if (a.obs_weight) cost *= w;
+          }
+        } else if (!(xs[2] > 0.0) || !camera_project(cam, xs, pred)) {
           bad = 1;
         } else {
           const double2 xy = a.obs_xy[o];
@@ -225,6 +252,8 @@ int visloc_ba_cuda_cost_noalloc(const vlba_problem* problem, const vlba_config* 
                 p.num_observations, kMaxObservations);
   if (!p.pose_q || !p.pose_t || !p.landmarks || !p.obs_pose || !p.obs_landmark || !p.obs_xy)
     return fail(error, error_capacity, VLBA_ERR_INVALID_ARGUMENT, "null problem array");
+  if (p.obs_kind && !p.obs_stereo)
+    return fail(error, error_capacity, VLBA_ERR_INVALID_ARGUMENT, "obs_kind without obs_stereo");
   NoallocArgs a;
   std::memset(&a, 0, sizeof a);
   for (uint32_t c = 0; c < p.num_cameras; ++c) {
@@ -259,6 +288,12 @@ int visloc_ba_cuda_cost_noalloc(const vlba_problem* problem, const vlba_config* 
   a.obs_xy = reinterpret_cast<const double2*>(p.obs_xy);
   a.obs_camera = p.obs_camera;
   a.obs_weight = p.obs_weight;
+  a.obs_kind = p.obs_kind;
+  a.obs_stereo = p.obs_stereo;
+  a.obs_right_camera = p.obs_right_camera;
+  a.stereo_baseline = p.stereo_baseline;
+  a.stereo_camera_ok = (p.cameras[0].model == VLBA_CAMERA_PINHOLE ||
+                        p.cameras[0].model == VLBA_CAMERA_SIMPLE_PINHOLE) ? 1u : 0u;
   a.num_cameras = p.num_cameras;
   a.robust_kernel = config->robust_kernel;
   a.robust_parameter = config->robust_parameter;

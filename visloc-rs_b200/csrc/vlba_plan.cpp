@@ -131,24 +131,72 @@ Validation validate_problem(const vlba_problem* p, const vlba_config* cfg) {
       return v;
     }
   }
+  // Stereo observations: known kinds with their arrays, and a pinhole
+  // BundleAdjustment::camera (check_stereo_camera_model, problem.rs:733-745).
+  bool has_stereo = false, has_rectified = false, has_general = false;
+  if (p->obs_kind)
+    for (uint64_t o = 0; o < p->num_observations; ++o) {
+      const uint32_t k = p->obs_kind[o];
+      if (k > kObsGeneralStereo) {
+        v.status = VLBA_ERR_INVALID_ARGUMENT;
+        v.error_index = o;
+        return v;
+      }
+      has_rectified = has_rectified || k == kObsStereo;
+      has_general = has_general || k == kObsGeneralStereo;
+    }
+  has_stereo = has_rectified || has_general;
+  if ((has_stereo && !p->obs_stereo) || (has_general && !p->obs_right_camera)) {
+    v.status = VLBA_ERR_INVALID_ARGUMENT;
+    return v;
+  }
+  if (has_stereo && p->cameras[0].model != VLBA_CAMERA_PINHOLE &&
+      p->cameras[0].model != VLBA_CAMERA_SIMPLE_PINHOLE) {
+    v.status = VLBA_ERR_UNSUPPORTED_CAMERA_MODEL;
+    return v;
+  }
   if (p->num_poses == 0) { v.status = VLBA_ERR_NO_POSES; return v; }
   if (p->num_observations == 0) { v.status = VLBA_ERR_NO_OBSERVATIONS; return v; }
   if (p->num_landmarks == 0) { v.status = VLBA_ERR_NO_LANDMARKS; return v; }
-  for (uint64_t o = 0; o < p->num_observations; ++o) {
+  // Pose and landmark references list by list, in the reference's order
+  // (lm.rs:185-228): monocular, rectified stereo (after its baseline),
+  // general stereo (with its right camera), rig.
+  auto kind_of = [&](uint64_t o) -> uint32_t { return p->obs_kind ? p->obs_kind[o] : kObsMono; };
+  auto refs_ok = [&](uint64_t o) {
     if (p->obs_pose[o] >= p->num_poses) {
       v.status = VLBA_ERR_MISSING_POSE;
       v.error_index = p->obs_pose[o];
-      return v;
+      return false;
     }
     if (p->obs_landmark[o] >= p->num_landmarks) {
       v.status = VLBA_ERR_MISSING_LANDMARK;
       v.error_index = p->obs_landmark[o];
+      return false;
+    }
+    return true;
+  };
+  const int lists[4] = {p->obs_camera ? -1 : (int)kObsMono, (int)kObsStereo, (int)kObsGeneralStereo,
+                        p->obs_camera ? (int)kObsMono : -1};
+  for (int li = 0; li < 4; ++li) {
+    if (lists[li] < 0 || (lists[li] != (int)kObsMono && !has_stereo)) continue;
+    if (lists[li] == (int)kObsStereo && has_rectified &&
+        !(std::isfinite(p->stereo_baseline) && p->stereo_baseline > 0.0)) {
+      v.status = VLBA_ERR_MISSING_STEREO_BASELINE;
       return v;
     }
-    if (p->obs_camera && p->obs_camera[o] >= p->num_cameras) {
-      v.status = VLBA_ERR_INVALID_ARGUMENT;
-      v.error_index = o;
-      return v;
+    for (uint64_t o = 0; o < p->num_observations; ++o) {
+      if (kind_of(o) != (uint32_t)lists[li]) continue;
+      if (!refs_ok(o)) return v;
+      if (lists[li] == (int)kObsGeneralStereo && p->obs_right_camera[o] >= p->num_cameras) {
+        v.status = VLBA_ERR_INVALID_ARGUMENT;
+        v.error_index = o;
+        return v;
+      }
+      if (lists[li] == (int)kObsMono && p->obs_camera && p->obs_camera[o] >= p->num_cameras) {
+        v.status = VLBA_ERR_INVALID_ARGUMENT;
+        v.error_index = o;
+        return v;
+      }
     }
   }
   bool any_var = false;
@@ -254,6 +302,9 @@ void build_plan_serial(const vlba_problem* const* problems, const vlba_config* c
     keep(P.obs_xy, old.obs_xy);
     keep(P.obs_w, old.obs_w);
     keep(P.obs_src, old.obs_src);
+    keep(P.obs_kind, old.obs_kind);
+    keep(P.obs_st, old.obs_st);
+    keep(P.obs_rcam, old.obs_rcam);
     keep(P.cam_obs, old.cam_obs);
   }
   P.tb = tb;
@@ -284,6 +335,13 @@ void build_plan_serial(const vlba_problem* const* problems, const vlba_config* c
   bool weighted = false;
   for (uint32_t i = 0; i < n; ++i) weighted = weighted || problems[i]->obs_weight != nullptr;
   if (weighted) P.obs_w.resize(tot_obs);
+  bool stereo = false;
+  for (uint32_t i = 0; i < n; ++i) stereo = stereo || problems[i]->obs_kind != nullptr;
+  if (stereo) {
+    P.obs_kind.resize(tot_obs);
+    P.obs_st.resize(2 * tot_obs);
+    P.obs_rcam.resize(tot_obs);
+  }
   P.cameras.reserve(tot_cams);
   P.prob_pose_begin.push_back(0);
   P.prob_point_begin.push_back(0);
@@ -352,7 +410,23 @@ void build_plan_serial(const vlba_problem* const* problems, const vlba_config* c
         const uint32_t g = obs_base + k;
         const uint32_t pose = pose_base + p->obs_pose[o];
         P.obs_pose[g] = pose;
-        P.obs_cam[g] = cam_base + (p->obs_camera ? p->obs_camera[o] : 0u);
+        const uint32_t kind = p->obs_kind ? p->obs_kind[o] : kObsMono;
+        // Stereo observations project through BundleAdjustment::camera.
+        P.obs_cam[g] = cam_base + (kind == kObsMono && p->obs_camera ? p->obs_camera[o] : 0u);
+        if (stereo) {
+          P.obs_kind[g] = (uint8_t)kind;
+          double s0 = 0.0, s1 = 0.0;
+          if (kind == kObsStereo) {
+            s0 = p->obs_stereo[2 * (size_t)o];
+            s1 = p->stereo_baseline;
+          } else if (kind == kObsGeneralStereo) {
+            s0 = p->obs_stereo[2 * (size_t)o];
+            s1 = p->obs_stereo[2 * (size_t)o + 1];
+          }
+          P.obs_st[2 * (size_t)g] = s0;
+          P.obs_st[2 * (size_t)g + 1] = s1;
+          P.obs_rcam[g] = cam_base + (kind == kObsGeneralStereo ? p->obs_right_camera[o] : 0u);
+        }
         P.obs_slot[g] = P.pose_slot[pose];
         P.obs_xy[2 * (size_t)g] = p->obs_xy[2 * (size_t)o];
         P.obs_xy[2 * (size_t)g + 1] = p->obs_xy[2 * (size_t)o + 1];
@@ -698,6 +772,9 @@ void merge_plans(const std::vector<const Plan*>& parts, Plan* out) {
     keep(P.obs_xy, old.obs_xy);
     keep(P.obs_w, old.obs_w);
     keep(P.obs_src, old.obs_src);
+    keep(P.obs_kind, old.obs_kind);
+    keep(P.obs_st, old.obs_st);
+    keep(P.obs_rcam, old.obs_rcam);
     keep(P.cam_obs, old.cam_obs);
   }
   if (parts.empty()) throw std::runtime_error("merge of no plans");
@@ -770,6 +847,13 @@ void merge_plans(const std::vector<const Plan*>& parts, Plan* out) {
   bool weighted = false;
   for (const Plan* q : parts) weighted = weighted || !q->obs_w.empty();
   if (weighted) P.obs_w.resize(T.obs);
+  bool stereo = false;
+  for (const Plan* q : parts) stereo = stereo || !q->obs_kind.empty();
+  if (stereo) {
+    P.obs_kind.resize(T.obs);
+    P.obs_st.resize(2 * T.obs);
+    P.obs_rcam.resize(T.obs);
+  }
   P.cam_off.assign(T.slot + 1, 0u);
   P.cam_obs.resize(T.camobs);
   P.tile_ij.resize(T.tile);
@@ -830,6 +914,18 @@ void merge_plans(const std::vector<const Plan*>& parts, Plan* out) {
     shift_none(P.obs_slot, obs_b, Q.obs_slot, slot_b);
     copy(P.obs_xy, 2 * (size_t)obs_b, Q.obs_xy);
     copy(P.obs_src, obs_b, Q.obs_src);
+    if (stereo) {
+      const size_t no = Q.obs_pose.size();
+      if (Q.obs_kind.empty()) {
+        std::fill_n(P.obs_kind.begin() + obs_b, no, (uint8_t)kObsMono);
+        std::fill_n(P.obs_st.begin() + 2 * (size_t)obs_b, 2 * no, 0.0);
+        std::fill_n(P.obs_rcam.begin() + obs_b, no, cam_b);
+      } else {
+        copy(P.obs_kind, obs_b, Q.obs_kind);
+        copy(P.obs_st, 2 * (size_t)obs_b, Q.obs_st);
+        shift(P.obs_rcam, obs_b, Q.obs_rcam, cam_b);
+      }
+    }
     if (weighted) {
       if (Q.obs_w.empty()) std::fill_n(P.obs_w.begin() + obs_b, Q.obs_pose.size(), 1.0);
       else copy(P.obs_w, obs_b, Q.obs_w);
@@ -928,6 +1024,14 @@ std::string check_plan(const Plan& P) {
   if (P.obs_cam.size() != nobs || P.obs_slot.size() != nobs || P.obs_xy.size() != 2 * nobs ||
       P.obs_point.size() != nobs || (!P.obs_w.empty() && P.obs_w.size() != nobs))
     return bad("obs sizes");
+  if (!P.obs_kind.empty()) {
+    if (P.obs_kind.size() != nobs || P.obs_st.size() != 2 * nobs || P.obs_rcam.size() != nobs)
+      return bad("stereo sizes");
+    if (!all_of_range(nobs, [&](uint64_t k) {
+          return P.obs_kind[k] <= kObsGeneralStereo && P.obs_rcam[k] < ncam;
+        }))
+      return bad("stereo observations");
+  }
   if (!all_of_range(nobs, [&](uint64_t k) {
         const uint32_t l = P.obs_point[k];
         return l < npts && P.pt_off[l] <= k && P.pt_off[l + 1] > k && P.obs_pose[k] < nposes &&
@@ -994,7 +1098,7 @@ size_t Plan::device_bytes() const {
   b += npose * (8 * (4 + 3 + 12) * 2 + 8 + 4 + 4);  // state x2, step, slot, prob
   b += npt * (8 * 3 * 2 + 4 + 1 + 4 + 36 + 64);     // points x2, off, var, prob, pt_h, pt_s
   b += nobs * (4 * 4 + 16 + 32 + 16 + 32);           // point, pose, cam, slot, xy, obs_h, obs_e, obs_p
-  b += obs_w.size() * 8;
+  b += obs_w.size() * 8 + obs_kind.size() * (1 + 16 + 4);
   b += cam_obs.size() * 4 + pairs.size() * 8 + dup_pairs.size() * 8;
   b += blk_dst.size() * (8 + 4);
   b += tile_ij.size() * ((size_t)tb * tb * kBlock * 4 + 4 + 2 * (size_t)tb * 6 * 4);
@@ -1010,7 +1114,8 @@ size_t Plan::upload_bytes() const {
   return b(prob_pose_begin) + b(prob_point_begin) + b(prob_tr_begin) + b(prob_chunk_begin) +
          b(pose_prob) + b(point_prob) + b(slot_prob) + b(params) + b(pose_q) + b(pose_t) +
          b(points) + b(pose_slot) + b(point_var) + b(cameras) + b(pt_off) + b(obs_point) + b(obs_pose) +
-         b(obs_cam) + b(obs_slot) + b(obs_xy) + b(obs_w) + b(cam_off) + b(cam_obs) + b(tile_ij) +
+         b(obs_cam) + b(obs_slot) + b(obs_xy) + b(obs_w) + b(obs_kind) + b(obs_st) + b(obs_rcam) +
+         b(cam_off) + b(cam_obs) + b(tile_ij) +
          b(blk_off) + b(pairs) + b(blk_dst) + b(diag_dst) + b(dup_off) + b(dup_pairs) +
          b(tr_list_off) + b(tr_list) + b(tr_prob) + b(chunk_point_begin) + b(tile_slot) + b(tile_meta);
 }

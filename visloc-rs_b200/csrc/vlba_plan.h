@@ -70,6 +70,13 @@ struct Plan {
   // Each observation's index in its problem's own order (host only: results
   // per observation go back to the caller in that order).
   ObsArray<uint32_t> obs_src;
+  // Stereo observations, present when some problem has them (empty
+  // otherwise): kind, stereo data (2 per observation: u_r and the baseline
+  // for rectified stereo, the right pixel for general stereo) and the right
+  // camera (general stereo).
+  ObsArray<uint8_t> obs_kind;
+  ObsArray<double> obs_st;
+  ObsArray<uint32_t> obs_rcam;
   std::vector<uint32_t> cam_off;
   ObsArray<uint32_t> cam_obs;
 

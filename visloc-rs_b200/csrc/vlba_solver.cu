@@ -425,6 +425,9 @@ void upload_plan_once(Context* c, uint32_t max_records) {
     d.obs_xy = xy;
   }
   d.obs_w = P.obs_w.empty() ? nullptr : st.up(A, P.obs_w);
+  d.obs_kind = P.obs_kind.empty() ? nullptr : st.up(A, P.obs_kind);
+  d.obs_st = P.obs_kind.empty() ? nullptr : reinterpret_cast<const double2*>(st.up(A, P.obs_st));
+  d.obs_rcam = P.obs_kind.empty() ? nullptr : st.up(A, P.obs_rcam);
   d.obs_h = A.alloc<float4>(2 * nobs);
   d.obs_e = A.alloc<float4>(nobs);
   d.obs_p = A.alloc<float4>(2 * nobs);

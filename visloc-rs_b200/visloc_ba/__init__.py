@@ -14,7 +14,9 @@ from .problem import (  # noqa: F401
     BaIterationStats,
     BaObservation,
     BaResult,
+    BaGeneralStereoObservation,
     BaRigObservation,
+    BaStereoObservation,
     BaScope,
     BundleAdjustment,
     Camera,

@@ -10,7 +10,7 @@ from __future__ import annotations
 import ctypes as C
 import os
 
-ABI_VERSION = 2
+ABI_VERSION = 3
 
 # enum vlba_status
 OK = 0
@@ -29,6 +29,7 @@ ERR_OUT_OF_MEMORY = 12
 ERR_TIMEOUT = 13
 ERR_BUSY = 14
 ERR_INVALID_OBSERVATION_WEIGHT = 15
+ERR_MISSING_STEREO_BASELINE = 16
 
 STATUS_NAMES = {
     OK: "OK",
@@ -47,7 +48,13 @@ STATUS_NAMES = {
     ERR_TIMEOUT: "Timeout",
     ERR_BUSY: "Busy",
     ERR_INVALID_OBSERVATION_WEIGHT: "InvalidObservationWeight",
+    ERR_MISSING_STEREO_BASELINE: "MissingStereoBaseline",
 }
+
+# vlba_problem.obs_kind
+OBS_MONO = 0
+OBS_STEREO = 1
+OBS_GENERAL_STEREO = 2
 
 # enum vlba_camera_model
 CAMERA_PINHOLE = 0
@@ -98,6 +105,10 @@ class Problem(C.Structure):
         ("num_cameras", C.c_uint32),
         ("cameras", C.POINTER(Camera)),
         ("obs_weight", C.POINTER(C.c_double)),
+        ("obs_kind", C.POINTER(C.c_uint8)),
+        ("obs_stereo", C.POINTER(C.c_double)),
+        ("obs_right_camera", C.POINTER(C.c_uint32)),
+        ("stereo_baseline", C.c_double),
     ]
 
 

@@ -184,6 +184,30 @@ class BaRigObservation:
     sensor_from_rig: SE3 = field(default_factory=SE3)
 
 
+@dataclass
+class BaStereoObservation:
+    """BaStereoObservation (mod.rs:213-221): rectified stereo, the right
+    row taken equal to the left one."""
+
+    keyframe_id: int
+    landmark_id: int
+    xy: tuple
+    u_right: float
+
+
+@dataclass
+class BaGeneralStereoObservation:
+    """BaGeneralStereoObservation (mod.rs:223-237): calibrated stereo with
+    T_right<-left = left_to_right."""
+
+    keyframe_id: int
+    landmark_id: int
+    xy_left: tuple
+    xy_right: tuple
+    right_camera: Camera
+    left_to_right: SE3 = field(default_factory=SE3)
+
+
 @dataclass(frozen=True)
 class RobustKernel:
     """RobustKernel::{None, Huber{delta}, Cauchy{c}} (pose_graph.rs:87-101)."""
@@ -415,10 +439,14 @@ class PackedProblem:
     landmarks (M,3), landmark_fixed (M,) u8, obs_pose / obs_landmark (K,) u32,
     obs_xy (K,2) f64, obs_camera (K,) u32 or None, cameras: list of
     (Camera, SE3 sensor_from_rig), obs_weight (K,) f64 external weights or
-    None (all 1; optimize_with_observation_weights, optimize.rs:43-53)."""
+    None (all 1; optimize_with_observation_weights, optimize.rs:43-53);
+    stereo observations: obs_kind (K,) u8 (0 monocular/rig, 1 rectified,
+    2 general stereo) or None, obs_stereo (K,2) f64 (u_r; the right pixel),
+    obs_right_camera (K,) u32 into `cameras`, stereo_baseline."""
 
     def __init__(self, pose_q, pose_t, landmarks, obs_pose, obs_landmark, obs_xy, cameras,
-                 pose_fixed=None, landmark_fixed=None, obs_camera=None, obs_weight=None):
+                 pose_fixed=None, landmark_fixed=None, obs_camera=None, obs_weight=None,
+                 obs_kind=None, obs_stereo=None, obs_right_camera=None, stereo_baseline=0.0):
         self.pose_q = np.ascontiguousarray(pose_q, dtype=np.float64).reshape(-1, 4)
         self.pose_t = np.ascontiguousarray(pose_t, dtype=np.float64).reshape(-1, 3)
         self.landmarks = np.ascontiguousarray(landmarks, dtype=np.float64).reshape(-1, 3)
@@ -440,6 +468,16 @@ class PackedProblem:
         self.obs_weight = (
             None if obs_weight is None else np.ascontiguousarray(obs_weight, dtype=np.float64)
         )
+        self.obs_kind = None if obs_kind is None else np.ascontiguousarray(obs_kind, dtype=np.uint8)
+        self.obs_stereo = (
+            None if obs_stereo is None
+            else np.ascontiguousarray(obs_stereo, dtype=np.float64).reshape(-1, 2)
+        )
+        self.obs_right_camera = (
+            None if obs_right_camera is None
+            else np.ascontiguousarray(obs_right_camera, dtype=np.uint32)
+        )
+        self.stereo_baseline = float(stereo_baseline)
         self._abi = None
 
     @property
@@ -458,7 +496,8 @@ class PackedProblem:
         return PackedProblem(
             self.pose_q.copy(), self.pose_t.copy(), self.landmarks.copy(), self.obs_pose,
             self.obs_landmark, self.obs_xy, list(self.cameras), self.pose_fixed,
-            self.landmark_fixed, self.obs_camera, self.obs_weight,
+            self.landmark_fixed, self.obs_camera, self.obs_weight, self.obs_kind, self.obs_stereo,
+            self.obs_right_camera, self.stereo_baseline,
         )
 
     def abi(self) -> _abi.Problem:
@@ -477,6 +516,10 @@ class PackedProblem:
         p.obs_xy = _ptr(self.obs_xy, C.c_double)
         p.obs_camera = _ptr(self.obs_camera, C.c_uint32)
         p.obs_weight = _ptr(self.obs_weight, C.c_double)
+        p.obs_kind = _ptr(self.obs_kind, C.c_uint8)
+        p.obs_stereo = _ptr(self.obs_stereo, C.c_double)
+        p.obs_right_camera = _ptr(self.obs_right_camera, C.c_uint32)
+        p.stereo_baseline = self.stereo_baseline
         cams = (_abi.Camera * len(self.cameras))(
             *[cam.to_abi(ext) for cam, ext in self.cameras]
         )
@@ -503,7 +546,10 @@ class BundleAdjustment:
         self.poses: dict[int, Pose] = {}
         self.landmarks: dict[int, tuple] = {}
         self.observations: list[BaObservation] = []
+        self.stereo_observations: list[BaStereoObservation] = []
+        self.general_stereo_observations: list[BaGeneralStereoObservation] = []
         self.rig_observations: list[BaRigObservation] = []
+        self.stereo_baseline: Optional[float] = None
         self.camera = camera
         self.fixed_poses: set[int] = set()
         self.fixed_landmarks: set[int] = set()
@@ -527,49 +573,75 @@ class BundleAdjustment:
     def add_rig_observation(self, obs: BaRigObservation):
         self.rig_observations.append(obs)
 
+    def add_stereo_observation(self, obs: BaStereoObservation):
+        self.stereo_observations.append(obs)
+
+    def add_general_stereo_observation(self, obs: BaGeneralStereoObservation):
+        self.general_stereo_observations.append(obs)
+
+    def set_stereo_baseline(self, baseline: float):
+        self.stereo_baseline = float(baseline)
+
     def pack(self):
         """Dense arrays in ascending id order, plus the id lists and a
-        validation error (BaError) for ids that do not resolve."""
+        validation error (BaError) for ids that do not resolve.  The
+        observations are flattened in the reference's order -- monocular,
+        rectified stereo, general stereo, rig (optimize.rs:30-35) -- which is
+        also the order of external weights."""
         pose_ids = sorted(self.poses)
         lm_ids = sorted(self.landmarks)
         pose_at = {pid: i for i, pid in enumerate(pose_ids)}
         lm_at = {lid: i for i, lid in enumerate(lm_ids)}
-        if self.observations and self.rig_observations:
-            raise BaError("Unsupported", message="mixed monocular and rig observations")
-        rig = bool(self.rig_observations)
-        obs = self.rig_observations if rig else self.observations
-        k = len(obs)
+        mono, rect, gen, rig = (self.observations, self.stereo_observations,
+                                self.general_stereo_observations, self.rig_observations)
+        k = len(mono) + len(rect) + len(gen) + len(rig)
         obs_pose = np.empty(k, np.uint32)
         obs_lm = np.empty(k, np.uint32)
         obs_xy = np.empty((k, 2))
+        kinds = np.zeros(k, np.uint8)
+        stereo = np.zeros((k, 2))
+        right = np.zeros(k, np.uint32)
+        obs_camera = np.zeros(k, np.uint32)
+        # cameras[0] is BundleAdjustment::camera; rig sensors and right
+        # cameras follow, each (camera, extrinsic) once.
+        cams: list = [(self.camera, SE3())]
+        keys: dict = {}
+
+        def camera_index(camera, ext):
+            key = (int(camera.model), tuple(camera.params), ext.rotation, ext.translation)
+            if key not in keys:
+                keys[key] = len(cams)
+                cams.append((camera, ext))
+            return keys[key]
+
         missing = None
-        for n, o in enumerate(obs):
-            if o.keyframe_id not in pose_at:
-                missing = missing or BaError("MissingPose", o.keyframe_id)
-                obs_pose[n] = 0xFFFFFFFF
-            else:
-                obs_pose[n] = pose_at[o.keyframe_id]
-            if o.landmark_id not in lm_at:
-                if missing is None and o.keyframe_id in pose_at:
-                    missing = BaError("MissingLandmark", o.landmark_id)
-                obs_lm[n] = 0xFFFFFFFF
-            else:
-                obs_lm[n] = lm_at[o.landmark_id]
-            obs_xy[n] = o.xy
-        cameras = [(self.camera, SE3())]
-        obs_camera = None
-        if rig:
-            cams: list = []
-            keys: dict = {}
-            obs_camera = np.empty(k, np.uint32)
-            for n, o in enumerate(obs):
-                key = (int(o.camera.model), tuple(o.camera.params), o.sensor_from_rig.rotation,
-                       o.sensor_from_rig.translation)
-                if key not in keys:
-                    keys[key] = len(cams)
-                    cams.append((o.camera, o.sensor_from_rig))
-                obs_camera[n] = keys[key]
-            cameras = cams or cameras
+        n = 0
+        for group, kind in ((mono, _abi.OBS_MONO), (rect, _abi.OBS_STEREO),
+                            (gen, _abi.OBS_GENERAL_STEREO), (rig, _abi.OBS_MONO)):
+            for o in group:
+                if o.keyframe_id not in pose_at:
+                    missing = missing or BaError("MissingPose", o.keyframe_id)
+                    obs_pose[n] = 0xFFFFFFFF
+                else:
+                    obs_pose[n] = pose_at[o.keyframe_id]
+                if o.landmark_id not in lm_at:
+                    if missing is None and o.keyframe_id in pose_at:
+                        missing = BaError("MissingLandmark", o.landmark_id)
+                    obs_lm[n] = 0xFFFFFFFF
+                else:
+                    obs_lm[n] = lm_at[o.landmark_id]
+                kinds[n] = kind
+                if group is gen:
+                    obs_xy[n] = o.xy_left
+                    stereo[n] = o.xy_right
+                    right[n] = camera_index(o.right_camera, o.left_to_right)
+                else:
+                    obs_xy[n] = o.xy
+                if group is rect:
+                    stereo[n, 0] = o.u_right
+                if group is rig:
+                    obs_camera[n] = camera_index(o.camera, o.sensor_from_rig)
+                n += 1
         pose_q = np.array([self.poses[i].world_to_camera.rotation for i in pose_ids],
                           dtype=np.float64).reshape(-1, 4)
         pose_t = np.array([self.poses[i].world_to_camera.translation for i in pose_ids],
@@ -577,8 +649,14 @@ class BundleAdjustment:
         lms = np.array([self.landmarks[i] for i in lm_ids], dtype=np.float64).reshape(-1, 3)
         pf = np.array([1 if i in self.fixed_poses else 0 for i in pose_ids], np.uint8)
         lf = np.array([1 if i in self.fixed_landmarks else 0 for i in lm_ids], np.uint8)
-        packed = PackedProblem(pose_q, pose_t, lms, obs_pose, obs_lm, obs_xy, cameras, pf, lf,
-                               obs_camera)
+        has_stereo = bool(rect) or bool(gen)
+        packed = PackedProblem(
+            pose_q, pose_t, lms, obs_pose, obs_lm, obs_xy, cams, pf, lf,
+            obs_camera if rig else None, None,
+            kinds if has_stereo else None, stereo if has_stereo else None,
+            right if gen else None,
+            self.stereo_baseline if self.stereo_baseline is not None else float("nan"),
+        )
         return packed, pose_ids, lm_ids, missing
 
     def unpack(self, packed: PackedProblem, pose_ids, lm_ids):

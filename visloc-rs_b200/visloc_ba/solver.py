@@ -35,6 +35,7 @@ _ERROR_KIND = {
     _abi.ERR_MISSING_LANDMARK: "MissingLandmark",
     _abi.ERR_UNSUPPORTED_CAMERA_MODEL: "UnsupportedCameraModel",
     _abi.ERR_SINGULAR_SYSTEM: "SingularSystem",
+    _abi.ERR_MISSING_STEREO_BASELINE: "MissingStereoBaseline",
 }
 
 
