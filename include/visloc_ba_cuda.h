@@ -349,10 +349,10 @@ int visloc_ba_cuda_batch_download(void* ctx, uint32_t n, vlba_problem* const* pr
  * sorted edges (a, b), a < b, and for each edge the (row b, column a)
  * block (f32, column-major), the right-hand side, and the stopping rule
  * |r| <= tol |rhs| within max_iterations.  The step (6 per node) and the
- * iteration count are returned.  Cluster and coarse-level preconditioners
- * and the accelerator-side elimination are not implemented: a shim returns
- * None for systems that carry them (empty offdiag, clusters or coarse), and
- * the caller runs its CPU solver. */
+ * iteration count are returned.  Systems that carry cluster inverses or a
+ * coarse level go to visloc_ba_cuda_reduced_solve_preconditioned below; the
+ * accelerator-side elimination (empty offdiag) is not implemented, and a
+ * shim returns None for it, so the caller eliminates on its CPU. */
 typedef struct vlba_reduced_system {
   uint32_t num_nodes;
   uint32_t reserved;
@@ -368,6 +368,50 @@ typedef struct vlba_reduced_system {
 
 int visloc_ba_cuda_reduced_solve(void* ctx, const vlba_reduced_system* system, double* x,
                                  uint32_t* iterations, double* relative_residual);
+
+/* The preconditioners of ReducedCameraSystem::clusters and ::coarse
+ * (pipelines/slam/src/ba_accel.rs:64-69; built by cluster_inverses and
+ * coarse_correction, pipelines/slam/src/colmap_incremental/rig_ba_solver.rs:
+ * 1101-1140 and 1235-1266; applied as in pcg_core, :1406-1480):
+ *
+ *   z = M r:  over each run c of cluster_size[c] consecutive nodes from
+ *             cluster_first[c], z_run = cluster inverse c times r_run; the
+ *             6x6 block-Jacobi inverse of the diagonal for nodes in no run;
+ *             then, with a coarse level, z += P (P^T S P)^-1 P^T r, where P
+ *             sums aggregates of coarse_group consecutive nodes over the
+ *             leading coarse_nodes.
+ *
+ * Runs are ascending and disjoint, at most 1024 nodes each; each inverse is
+ * (6 size)^2 doubles, column-major (nalgebra DMatrix), concatenated in run
+ * order.  coarse_inverse is (6 m)^2 doubles, column-major, m =
+ * ceil(coarse_nodes / coarse_group) <= 2048; coarse_nodes = 0 means no
+ * coarse level.  The reference hands over its runs as (first node, inverse)
+ * with all runs of one length k but the last: cluster_first[c] = c k. */
+typedef struct vlba_reduced_preconditioner {
+  uint32_t num_clusters;
+  uint32_t reserved;
+  const uint32_t* cluster_first;   /* [num_clusters] */
+  const uint32_t* cluster_size;    /* [num_clusters] nodes */
+  const double* cluster_inverse;   /* sum over runs of (6 size)^2 */
+  uint32_t coarse_group;
+  uint32_t coarse_nodes;
+  const double* coarse_inverse;    /* [(6 m)^2] or null without a level */
+} vlba_reduced_preconditioner;
+
+/* visloc_ba_cuda_reduced_solve with the preconditioner above (null: block-
+ * Jacobi, the same iteration as visloc_ba_cuda_reduced_solve up to the
+ * order of its sums).  The iteration follows pcg_core: x = 0, r = b, z = M r,
+ * p = z; per iteration q = S p, alpha = r.z / p.q, x += alpha p, r -= alpha
+ * q, stop once |r| <= tol |b| or max_iterations have run, else z = M r and
+ * p = z + beta p.  Vectors and S are f32, dots and scalars f64; every sum
+ * runs in a fixed order, so repeated solves give identical steps.  A p.q
+ * that is not positive and finite fails the solve as in pcg_core (which
+ * returns None): VLBA_DECLINED, and the caller runs its CPU solver.  A zero
+ * right-hand side gives x = 0 after 0 iterations. */
+int visloc_ba_cuda_reduced_solve_preconditioned(void* ctx, const vlba_reduced_system* system,
+                                                const vlba_reduced_preconditioner* pre,
+                                                double* x, uint32_t* iterations,
+                                                double* relative_residual);
 
 /* --------------------------------------------------------------- autotuner */
 /* Launch shape of the uploaded system: the blocks of the persistent PCG

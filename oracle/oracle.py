@@ -300,3 +300,149 @@ def reduced_system(packed: PackedProblem, lam: float, config: BaConfig | None = 
         C.byref(packed.abi()), C.byref(config.to_abi()), lam, threads, _dp(s), _dp(rhs),
         _dp(dp) if step else P(C.c_double)(), _dp(dl) if step else P(C.c_double)())
     return st, s, rhs, dp, dl
+
+
+# ------------------------------------------- reduced solve preconditioners
+# numpy restatement of the CPU iteration that ReducedSolveAccelerator::solve
+# replaces, with its two preconditioners.  Blocks are numpy 6x6 matrices:
+# diag[i] node i's damped diagonal block, offdiag[e] the (row b, column a)
+# block of edge edges[e] = (a, b), a < b.
+
+COARSE_MAX_AGGREGATES = 256  # PCG_COARSE_MAX_AGGREGATES, rig_ba_solver.rs:1158
+
+
+def cluster_inverses(diag, edges, offdiag, k: int):
+    """(first node, inverse) of S restricted to each run of k consecutive
+    nodes, the last run shorter (cluster_inverses, pipelines/slam/src/
+    colmap_incremental/rig_ba_solver.rs:1112-1140); None when a run is not
+    positive definite."""
+    n = len(diag)
+    starts = list(range(0, n, k))
+    mats = []
+    for s in starts:
+        m = min(k, n - s)
+        a = np.zeros((6 * m, 6 * m))
+        for i in range(m):
+            a[6 * i:6 * i + 6, 6 * i:6 * i + 6] = diag[s + i]
+        mats.append(a)
+    for (ea, eb), blk in zip(np.asarray(edges).reshape(-1, 2), offdiag):
+        ea, eb = int(ea), int(eb)
+        if ea // k != eb // k:
+            continue
+        c, ia, ib = ea // k, ea % k, eb % k
+        mats[c][6 * ib:6 * ib + 6, 6 * ia:6 * ia + 6] = blk
+        mats[c][6 * ia:6 * ia + 6, 6 * ib:6 * ib + 6] = np.asarray(blk).T
+    out = []
+    for s, a in zip(starts, mats):
+        try:
+            L = np.linalg.cholesky(a)
+        except np.linalg.LinAlgError:
+            return None
+        Li = np.linalg.inv(L)
+        out.append((s, Li.T @ Li))
+    return out
+
+
+def coarse_correction(diag, edges, offdiag, n_frames: int, group: int):
+    """(group, n_frames, (P^T S P)^-1) of the additive coarse level over the
+    leading n_frames nodes, group raised so that there are at most 256
+    aggregates (coarse_correction, rig_ba_solver.rs:1235-1266, and
+    CoarseCorrection::inverse, :1218-1229); None for fewer than two
+    aggregates or a coarse matrix that is not positive definite."""
+    group = max(group, -(-n_frames // COARSE_MAX_AGGREGATES))
+    m = -(-n_frames // group)
+    if m < 2:
+        return None
+    a = np.zeros((6 * m, 6 * m))
+    for i in range(n_frames):
+        g = i // group * 6
+        a[g:g + 6, g:g + 6] += diag[i]
+    for (ea, eb), blk in zip(np.asarray(edges).reshape(-1, 2), offdiag):
+        ea, eb = int(ea), int(eb)
+        if ea >= n_frames or eb >= n_frames:
+            continue
+        ga, gb = ea // group * 6, eb // group * 6
+        a[gb:gb + 6, ga:ga + 6] += blk
+        a[ga:ga + 6, gb:gb + 6] += np.asarray(blk).T
+    try:
+        np.linalg.cholesky(a)
+    except np.linalg.LinAlgError:
+        return None
+    return group, n_frames, np.linalg.inv(a)
+
+
+def reduced_matvec(diag, edges, offdiag):
+    """p -> S p over the block layout (edge_product, rig_ba_solver.rs:
+    1314-1331: each edge adds B p_a to row b and B^T p_b to row a)."""
+    diag = np.asarray(diag, np.float64)
+    e = np.asarray(edges, np.int64).reshape(-1, 2)
+    off = np.asarray(offdiag, np.float64).reshape(-1, 6, 6)
+
+    def mv(p):
+        p = p.reshape(-1, 6)
+        q = np.einsum("nij,nj->ni", diag, p)
+        if len(e):
+            np.add.at(q, e[:, 1], np.einsum("eij,ej->ei", off, p[e[:, 0]]))
+            np.add.at(q, e[:, 0], np.einsum("eji,ej->ei", off, p[e[:, 1]]))
+        return q.reshape(-1)
+
+    return mv
+
+
+def reduced_pcg(diag, edges, offdiag, rhs, tol: float, max_iterations: int,
+                clusters=None, coarse=None):
+    """pcg_core (rig_ba_solver.rs:1406-1480) in FP64: z = M r by the run
+    inverses (block-Jacobi without runs, and for nodes in no run) plus the
+    coarse level z += P (P^T S P)^-1 P^T r (CoarseCorrection::add_to,
+    :1198-1213); x = 0, r = b, p = z; stop once |r| <= tol |b| or after
+    max_iterations.  Returns (x (n, 6), iterations), or None on a p.q that
+    is not positive and finite."""
+    n = len(diag)
+    mv = reduced_matvec(diag, edges, offdiag)
+    jac = [np.linalg.inv(np.asarray(d, np.float64)) for d in diag]
+    runs = [(int(s), np.asarray(inv, np.float64)) for s, inv in (clusters or [])]
+
+    def apply(r):
+        rb = r.reshape(n, 6)
+        z = np.stack([jac[i] @ rb[i] for i in range(n)]).reshape(-1)
+        for s, inv in runs:
+            m = inv.shape[0]
+            z[6 * s:6 * s + m] = inv @ r[6 * s:6 * s + m]
+        if coarse is not None:
+            group, nodes, cinv = coarse
+            m = cinv.shape[0] // 6
+            rc = np.zeros(6 * m)
+            for i in range(nodes):
+                rc[i // group * 6:i // group * 6 + 6] += rb[i]
+            yc = np.asarray(cinv) @ rc
+            for i in range(nodes):
+                z[6 * i:6 * i + 6] += yc[i // group * 6:i // group * 6 + 6]
+        return z
+
+    b = np.asarray(rhs, np.float64).reshape(-1)
+    bn = np.sqrt(b @ b)
+    x = np.zeros_like(b)
+    if bn == 0.0:
+        return x.reshape(n, 6), 0
+    r = b.copy()
+    z = apply(r)
+    p = z.copy()
+    rz = r @ z
+    it = 0
+    for _ in range(max_iterations):
+        it += 1
+        q = mv(p)
+        pq = p @ q
+        if not np.isfinite(pq) or pq <= 0.0:
+            return None
+        alpha = rz / pq
+        x += alpha * p
+        r -= alpha * q
+        if np.sqrt(r @ r) <= tol * bn:
+            break
+        z = apply(r)
+        rz_next = r @ z
+        beta = rz_next / rz
+        rz = rz_next
+        p = z + beta * p
+    return x.reshape(n, 6), it

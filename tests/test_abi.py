@@ -43,6 +43,8 @@ def test_struct_sizes_match_the_header_layout():
     # ... cameras, obs_weight, then obs_kind, obs_stereo, obs_right_camera, stereo_baseline
     assert C.sizeof(_abi.Problem) == 3 * 8 + 9 * 8 + 8 + 8 + 8 + 4 * 8
     assert C.sizeof(_abi.Iteration) == 8 + 5 * 8 + 8 + 8 + 4 * 8
+    assert C.sizeof(_abi.ReducedSystem) == 8 + 8 + 4 * 8 + 8 + 8
+    assert C.sizeof(_abi.ReducedPreconditioner) == 8 + 3 * 8 + 8 + 8
 
 
 def test_default_config_is_the_reference_default():

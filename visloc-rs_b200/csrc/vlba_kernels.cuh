@@ -32,6 +32,40 @@ cudaError_t launch_state_to_front(const Dev& d, cudaStream_t s);
 // buffer 0; NaN where it cannot be evaluated.
 cudaError_t launch_sq_residuals(const Dev& d, double* out, cudaStream_t s);
 
+// Scalars of a preconditioned reduced solve (vlba_reduced.cu), on the device.
+struct RpScalars {
+  double alpha, beta, rz, bnorm, rnorm;
+  uint32_t iters;
+  uint32_t done;    // the loop is over: every kernel returns at once
+  uint32_t failed;  // p.q not positive and finite
+  uint32_t pad;
+};
+
+// The preconditioner and work arrays of a preconditioned reduced solve.
+struct RpData {
+  RpScalars* sc;
+  double* dots;                // [3 num_tile_rows]: per tile row p.q, r.z, r.r
+  uint32_t num_clusters;
+  uint32_t max_cluster_rows;   // 6 x the longest run
+  const uint32_t* cl_first;    // [num_clusters] first node
+  const uint32_t* cl_size;     // [num_clusters] nodes
+  const uint64_t* cl_off;      // [num_clusters] float offset of the inverse
+  const float* cl_mat;         // column-major run inverses
+  uint32_t coarse_m;           // aggregates (0: no coarse level)
+  uint32_t coarse_group;
+  uint32_t coarse_nodes;
+  uint32_t max_iterations;
+  const float* coarse_inv;     // [(6 m)^2] row-major
+  float* rc;                   // [6 m] P^T r
+  float* yc;                   // [6 m]
+  double tol;
+};
+
+// x = 0, r = b, z = M r, p = z and the initial scalars (sc zeroed first).
+cudaError_t launch_rp_init(const Dev& d, const RpData& rp, cudaStream_t s);
+// One iteration; a no-op once sc->done is set.
+cudaError_t launch_rp_iteration(const Dev& d, const RpData& rp, cudaStream_t s);
+
 // Occupancy-derived grid of the persistent PCG kernel (0 if it cannot run).
 int pcg_grid_size(int tb, int sm_count);
 size_t pcg_smem_bytes(int tb);

@@ -1,0 +1,347 @@
+// vlba_reduced.cu -- preconditioned CG on an uploaded reduced camera system
+// with the reference's run inverses and additive coarse level
+// (ReducedCameraSystem::clusters / coarse, pipelines/slam/src/ba_accel.rs:
+// 50-72; the iteration of crates/ba-gpu/src/shaders/reduced_pcg.wgsl):
+//
+//   z = M r:  z_run = inverse of the run's block of S times r_run over each
+//             run of consecutive nodes, the 6x6 block-Jacobi inverse for
+//             nodes in no run, plus (coarse level) P (P^T S P)^-1 P^T r with
+//             P summing each aggregate of `coarse_group` leading nodes.
+//
+// The system is the uploaded plan's tiles (the same S the persistent PCG
+// kernel streams); the loop is a sequence of small kernels with every scalar
+// on the device (no host round trip inside an iteration), each returning at
+// once when the solve is over.  Vectors are FP32 as in the persistent PCG,
+// dots FP64; every sum runs in a fixed order, so a solve is deterministic.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "vlba_kernels.cuh"
+
+namespace vlba {
+namespace {
+
+constexpr int kRow = 48;  // floats of a tile row (8 nodes x 6)
+
+__device__ __forceinline__ bool rp_done(const RpData& r) {
+  return *(volatile const uint32_t*)&r.sc->done != 0u;
+}
+
+__device__ __forceinline__ double warp_sum_d(double v) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  return v;
+}
+
+// Per tile row R, one warp: entries e = lane and lane + 32 (< 48).
+#define RP_ROW_LOOP(d)                                                              \
+  const uint32_t lane = threadIdx.x & 31u;                                          \
+  const uint32_t R = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;                  \
+  if (R >= (d).num_tile_rows) return;                                               \
+  const size_t base = (size_t)R * kRow;                                             \
+  const bool e1 = lane + 32u < (uint32_t)kRow;
+
+// x = 0, r = b; the rows' |b|^2.
+__global__ void k_rp_init_xr(Dev d, RpData rp) {
+  RP_ROW_LOOP(d)
+  double bb = 0.0;
+  for (uint32_t e = lane; e < (uint32_t)kRow; e += 32) {
+    const float b = d.rhs[base + e];
+    d.x[base + e] = 0.0f;
+    d.r[base + e] = b;
+    bb += (double)b * (double)b;
+  }
+  (void)e1;
+  bb = warp_sum_d(bb);
+  if (lane == 0) rp.dots[2 * (size_t)d.num_tile_rows + R] = bb;
+}
+
+// One warp per tile: the row-side partial S_IJ p_J and, off the diagonal,
+// the column-side partial S_IJ^T p_I into the tile's partial slots (as the
+// persistent PCG kernel does, from global memory instead of a TMA ring).
+__global__ void k_rp_matvec(Dev d, RpData rp) {
+  if (rp_done(rp)) return;
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t nw = gridDim.x * blockDim.x / 32u;
+  const int li = (int)(lane >> 3), lj = (int)(lane & 7);
+  for (uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) / 32u; t < d.num_tiles; t += nw) {
+    const uint4 meta = reinterpret_cast<const uint4*>(d.tile_meta)[t];
+    const uint32_t I = meta.x >> 16, J = meta.x & 0xFFFFu;
+    const float* tile = d.tiles + (size_t)t * 64 * kBlock;
+    float pj[6];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) pj[c] = d.p[(size_t)J * kRow + lj * 6 + c];
+    float row[2][6], col[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const float* blk = tile + (size_t)(lane + 32 * h) * kBlock;
+      float pi[6];
+#pragma unroll
+      for (int a = 0; a < 6; ++a) pi[a] = d.p[(size_t)I * kRow + (li + 4 * h) * 6 + a];
+#pragma unroll
+      for (int a = 0; a < 6; ++a) {
+        float acc = 0.0f;
+#pragma unroll
+        for (int c = 0; c < 6; ++c) acc += blk[a * 6 + c] * pj[c];
+        row[h][a] = acc;
+      }
+#pragma unroll
+      for (int c = 0; c < 6; ++c) {
+        float acc = 0.0f;
+#pragma unroll
+        for (int a = 0; a < 6; ++a) acc += blk[a * 6 + c] * pi[a];
+        col[c] += acc;
+      }
+    }
+#pragma unroll
+    for (int off = 4; off > 0; off >>= 1)
+#pragma unroll
+      for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int a = 0; a < 6; ++a) row[h][a] += __shfl_xor_sync(0xffffffffu, row[h][a], off);
+    if (lj == 0) {
+      float* part = d.partial + (size_t)meta.y * kRow;
+#pragma unroll
+      for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int a = 0; a < 6; ++a) part[(li + 4 * h) * 6 + a] = row[h][a];
+    }
+    if (I != J) {
+#pragma unroll
+      for (int off = 8; off < 32; off <<= 1)
+#pragma unroll
+        for (int c = 0; c < 6; ++c) col[c] += __shfl_xor_sync(0xffffffffu, col[c], off);
+      if (li == 0) {
+        float* part = d.partial + (size_t)meta.z * kRow;
+#pragma unroll
+        for (int c = 0; c < 6; ++c) part[lj * 6 + c] = col[c];
+      }
+    }
+  }
+}
+
+// q_R = the row's partial slots in order; the row's p.q.
+__global__ void k_rp_rowsum(Dev d, RpData rp) {
+  if (rp_done(rp)) return;
+  RP_ROW_LOOP(d)
+  const uint32_t m0 = d.tr_list_off[R], m1 = d.tr_list_off[R + 1];
+  float q0 = 0.0f, q1 = 0.0f;
+  for (uint32_t m = m0; m < m1; ++m) {
+    q0 += d.partial[(size_t)m * kRow + lane];
+    if (e1) q1 += d.partial[(size_t)m * kRow + 32 + lane];
+  }
+  d.q[base + lane] = q0;
+  double pq = (double)d.p[base + lane] * (double)q0;
+  if (e1) {
+    d.q[base + 32 + lane] = q1;
+    pq += (double)d.p[base + 32 + lane] * (double)q1;
+  }
+  pq = warp_sum_d(pq);
+  if (lane == 0) rp.dots[R] = pq;
+}
+
+// x += alpha p, r -= alpha q; the rows' |r|^2.
+__global__ void k_rp_update_xr(Dev d, RpData rp) {
+  if (rp_done(rp)) return;
+  RP_ROW_LOOP(d)
+  (void)e1;
+  const float af = (float)rp.sc->alpha;
+  double rr = 0.0;
+  for (uint32_t e = lane; e < (uint32_t)kRow; e += 32) {
+    d.x[base + e] += af * d.p[base + e];
+    const float rv = d.r[base + e] - af * d.q[base + e];
+    d.r[base + e] = rv;
+    rr += (double)rv * (double)rv;
+  }
+  rr = warp_sum_d(rr);
+  if (lane == 0) rp.dots[2 * (size_t)d.num_tile_rows + R] = rr;
+}
+
+// z = the 6x6 block-Jacobi inverse times r, every node (runs overwrite theirs).
+__global__ void k_rp_jacobi(Dev d, RpData rp) {
+  if (rp_done(rp)) return;
+  const size_t n = (size_t)d.num_var_cams * 6;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const size_t node = i / 6, a = i % 6;
+    const float* m = d.minv + 36 * node + a * 6;
+    float z = 0.0f;
+#pragma unroll
+    for (int b = 0; b < 6; ++b) z += m[b] * d.r[6 * node + b];
+    d.z[i] = z;
+  }
+}
+
+// One block per run: z_run = inverse (column-major, FP32) times r_run, the
+// run's residual staged in shared memory.
+__global__ void k_rp_cluster(Dev d, RpData rp) {
+  if (rp_done(rp)) return;
+  extern __shared__ float seg[];
+  for (uint32_t c = blockIdx.x; c < rp.num_clusters; c += gridDim.x) {
+    const uint32_t rows = 6u * rp.cl_size[c];
+    const size_t base = 6 * (size_t)rp.cl_first[c];
+    const float* mat = rp.cl_mat + rp.cl_off[c];
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < rows; i += blockDim.x) seg[i] = d.r[base + i];
+    __syncthreads();
+    for (uint32_t row = threadIdx.x; row < rows; row += blockDim.x) {
+      float acc = 0.0f;
+      for (uint32_t k = 0; k < rows; ++k) acc += mat[(size_t)k * rows + row] * seg[k];
+      d.z[base + row] = acc;
+    }
+  }
+}
+
+// rc = P^T r: per aggregate and component, the sum over its nodes in order.
+__global__ void k_rp_restrict(Dev d, RpData rp) {
+  if (rp_done(rp)) return;
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= 6u * rp.coarse_m) return;
+  const uint32_t g = j / 6u, k = j % 6u;
+  const uint32_t end = min((g + 1u) * rp.coarse_group, rp.coarse_nodes);
+  float acc = 0.0f;
+  for (uint32_t i = g * rp.coarse_group; i < end; ++i) acc += d.r[6 * (size_t)i + k];
+  rp.rc[j] = acc;
+}
+
+// yc = (P^T S P)^-1 rc (row-major), one block per row in a fixed-order
+// block sum.
+__global__ void __launch_bounds__(256) k_rp_coarse_apply(Dev d, RpData rp) {
+  if (rp_done(rp)) return;
+  __shared__ float red[256];
+  const uint32_t m = 6u * rp.coarse_m;
+  for (uint32_t t = blockIdx.x; t < m; t += gridDim.x) {
+    float acc = 0.0f;
+    for (uint32_t c = threadIdx.x; c < m; c += blockDim.x)
+      acc += rp.coarse_inv[(size_t)t * m + c] * rp.rc[c];
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = 128; s > 0; s >>= 1) {
+      if ((int)threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) rp.yc[t] = red[0];
+    __syncthreads();
+  }
+}
+
+// z += P yc over the aggregated nodes; the rows' r.z.
+__global__ void k_rp_prolong_rz(Dev d, RpData rp) {
+  if (rp_done(rp)) return;
+  RP_ROW_LOOP(d)
+  (void)e1;
+  double rz = 0.0;
+  for (uint32_t e = lane; e < (uint32_t)kRow; e += 32) {
+    const size_t i = base + e;
+    float z = d.z[i];
+    const size_t node = i / 6;
+    if (rp.coarse_m && node < rp.coarse_nodes) {
+      z += rp.yc[6 * (node / rp.coarse_group) + i % 6];
+      d.z[i] = z;
+    }
+    rz += (double)d.r[i] * (double)z;
+  }
+  rz = warp_sum_d(rz);
+  if (lane == 0) rp.dots[(size_t)d.num_tile_rows + R] = rz;
+}
+
+// p = z (first) or z + beta p.
+__global__ void k_rp_update_p(Dev d, RpData rp, int first) {
+  if (rp_done(rp)) return;
+  const size_t n = (size_t)d.num_var_cams * 6;
+  const float bf = first ? 0.0f : (float)rp.sc->beta;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    d.p[i] = first ? d.z[i] : d.z[i] + bf * d.p[i];
+}
+
+// Scalar steps, one warp: the rows' dots summed lane-strided, then a
+// butterfly (a fixed order).
+enum RpStep { kRpInit = 0, kRpAlpha = 1, kRpCheck = 2, kRpBeta = 3 };
+__global__ void k_rp_scalars(Dev d, RpData rp, int step) {
+  const uint32_t lane = threadIdx.x & 31u;
+  if (threadIdx.x >= 32 || rp_done(rp)) return;
+  const uint32_t rows = d.num_tile_rows;
+  const double* v = rp.dots + (size_t)(step == kRpAlpha ? 0 : step == kRpBeta ? 1 : 2) * rows;
+  double s = 0.0;
+  for (uint32_t r = lane; r < rows; r += 32) s += v[r];
+  s = warp_sum_d(s);
+  double rz = 0.0;
+  if (step == kRpInit) {  // |b|^2 and the initial r.z
+    for (uint32_t r = lane; r < rows; r += 32) rz += rp.dots[rows + r];
+    rz = warp_sum_d(rz);
+  }
+  if (lane != 0) return;
+  RpScalars& sc = *rp.sc;
+  switch (step) {
+    case kRpInit:
+      sc.bnorm = sqrt(s);
+      sc.rnorm = sc.bnorm;
+      sc.rz = rz;
+      sc.iters = 0u;
+      if (!(sc.bnorm > 0.0) || rp.max_iterations == 0u) sc.done = 1u;
+      break;
+    case kRpAlpha:  // a non-positive or non-finite curvature fails the solve
+      if (s > 0.0 && isfinite(s)) {
+        sc.alpha = sc.rz / s;
+      } else {
+        sc.failed = 1u;
+        sc.done = 1u;
+      }
+      break;
+    case kRpCheck:
+      sc.iters += 1u;
+      sc.rnorm = sqrt(s);
+      if (sc.rnorm <= rp.tol * sc.bnorm || sc.iters >= rp.max_iterations) sc.done = 1u;
+      break;
+    default:  // beta = r.z (new) / r.z (old)
+      sc.beta = s / sc.rz;
+      sc.rz = s;
+      break;
+  }
+}
+
+int rows_grid(const Dev& d) { return (int)((d.num_tile_rows + 7) / 8); }
+int flat_grid(size_t n) { return (int)std::min<size_t>((n + 255) / 256, 148 * 8); }
+
+void precondition(const Dev& d, const RpData& rp, cudaStream_t s) {
+  k_rp_jacobi<<<flat_grid((size_t)d.num_var_cams * 6), 256, 0, s>>>(d, rp);
+  if (rp.num_clusters)
+    k_rp_cluster<<<std::min<uint32_t>(rp.num_clusters, 148 * 4), 256, rp.max_cluster_rows * 4, s>>>(d, rp);
+  if (rp.coarse_m) {
+    k_rp_restrict<<<(6 * rp.coarse_m + 255) / 256, 256, 0, s>>>(d, rp);
+    k_rp_coarse_apply<<<std::min<uint32_t>(6 * rp.coarse_m, 148 * 8), 256, 0, s>>>(d, rp);
+  }
+  k_rp_prolong_rz<<<rows_grid(d), 256, 0, s>>>(d, rp);
+}
+
+}  // namespace
+
+cudaError_t launch_rp_init(const Dev& d, const RpData& rp, cudaStream_t s) {
+  if (rp.max_cluster_rows * 4 > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(k_rp_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)(rp.max_cluster_rows * 4));
+    if (e != cudaSuccess) return e;
+  }
+  k_rp_init_xr<<<rows_grid(d), 256, 0, s>>>(d, rp);
+  precondition(d, rp, s);
+  k_rp_scalars<<<1, 32, 0, s>>>(d, rp, kRpInit);
+  k_rp_update_p<<<flat_grid((size_t)d.num_var_cams * 6), 256, 0, s>>>(d, rp, 1);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rp_iteration(const Dev& d, const RpData& rp, cudaStream_t s) {
+  const int tiles_grid = (int)std::min<uint32_t>((d.num_tiles + 7) / 8, 148 * 16);
+  k_rp_matvec<<<std::max(1, tiles_grid), 256, 0, s>>>(d, rp);
+  k_rp_rowsum<<<rows_grid(d), 256, 0, s>>>(d, rp);
+  k_rp_scalars<<<1, 32, 0, s>>>(d, rp, kRpAlpha);
+  k_rp_update_xr<<<rows_grid(d), 256, 0, s>>>(d, rp);
+  k_rp_scalars<<<1, 32, 0, s>>>(d, rp, kRpCheck);
+  precondition(d, rp, s);
+  k_rp_scalars<<<1, 32, 0, s>>>(d, rp, kRpBeta);
+  k_rp_update_p<<<flat_grid((size_t)d.num_var_cams * 6), 256, 0, s>>>(d, rp, 0);
+  return cudaGetLastError();
+}
+
+}  // namespace vlba

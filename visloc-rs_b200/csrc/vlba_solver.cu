@@ -1920,56 +1920,248 @@ int visloc_ba_cuda_server_wait(void* server, uint64_t ticket, double timeout_ms,
   return st;
 }
 
+}  // extern "C"
+
+namespace vlba {
+
+// A device allocation freed with its holder (cudaFree waits for the work
+// that uses it).
+struct DeviceArray {
+  void* p = nullptr;
+  DeviceArray() = default;
+  DeviceArray(const DeviceArray&) = delete;
+  DeviceArray& operator=(const DeviceArray&) = delete;
+  ~DeviceArray() {
+    if (p) cudaFree(p);
+  }
+  void alloc(size_t bytes) { VLBA_CUDA(cudaMalloc(&p, std::max<size_t>(bytes, 16))); }
+  template <class T>
+  T* as() const {
+    return static_cast<T*>(p);
+  }
+};
+
+bool reduced_system_ok(const vlba_reduced_system* sys) {
+  return sys && sys->diag && sys->rhs && sys->num_nodes != 0 &&
+         (!sys->num_edges || (sys->edges && sys->offdiag)) && sys->tol >= 0.0;
+}
+
+// Plans and uploads a reduced system given in the reference's layout and
+// fills S's tiles, the block-Jacobi inverses and the rhs on the device.
+void reduced_setup(Context* c, const vlba_reduced_system* sys) {
+  vlba_config cfg;
+  visloc_ba_cuda_default_config(&cfg);
+  cfg.max_pcg_iterations = sys->max_iterations;
+  cfg.pcg_relative_tolerance = sys->tol;
+  const LmParams lp = make_params(&cfg);
+  build_reduced_plan(sys->num_nodes, sys->edges, sys->num_edges, 8, lp, &c->plan);
+  const std::string bad = check_plan(c->plan);
+  if (!bad.empty()) throw Status(VLBA_ERR_INVALID_ARGUMENT, bad);
+  upload_plan(c, 1);
+  cudaStream_t s = c->stream;
+  const size_t n = sys->num_nodes, ne = sys->num_edges;
+  DeviceArray diag, off, rhs;  // the caller's arrays, staged for the fill kernel
+  diag.alloc(36 * n * 8);
+  rhs.alloc(6 * n * 8);
+  if (ne) off.alloc(36 * ne * 4);
+  VLBA_CUDA(cudaMemcpyAsync(diag.p, sys->diag, 36 * n * 8, cudaMemcpyHostToDevice, s));
+  VLBA_CUDA(cudaMemcpyAsync(rhs.p, sys->rhs, 6 * n * 8, cudaMemcpyHostToDevice, s));
+  if (ne) VLBA_CUDA(cudaMemcpyAsync(off.p, sys->offdiag, 36 * ne * 4, cudaMemcpyHostToDevice, s));
+  reset_state(c);
+  check_launch(launch_reduced_fill(c->dev, (uint32_t)n, ne, diag.as<const double>(),
+                                   ne ? off.as<const float>() : nullptr, rhs.as<const double>(), s),
+               "reduced fill");
+  VLBA_CUDA(cudaStreamSynchronize(s));
+}
+
+void download_step(Context* c, size_t n, double* x) {
+  std::vector<float> xf(6 * n);
+  VLBA_CUDA(cudaMemcpyAsync(xf.data(), c->dev.x, xf.size() * 4, cudaMemcpyDeviceToHost, c->stream));
+  VLBA_CUDA(cudaStreamSynchronize(c->stream));
+  for (size_t i = 0; i < xf.size(); ++i) x[i] = xf[i];
+}
+
+constexpr uint32_t kMaxRunNodes = 1024;
+constexpr uint32_t kMaxAggregates = 2048;
+
+// The preconditioner's shape against the system's node count.
+std::string check_preconditioner(const vlba_reduced_preconditioner* pre, uint32_t n) {
+  if (!pre) return "";
+  if (pre->num_clusters) {
+    if (!pre->cluster_first || !pre->cluster_size || !pre->cluster_inverse)
+      return "cluster arrays missing";
+    uint64_t next = 0;
+    for (uint32_t k = 0; k < pre->num_clusters; ++k) {
+      const uint64_t f = pre->cluster_first[k], m = pre->cluster_size[k];
+      if (m == 0 || m > kMaxRunNodes)
+        return "run " + std::to_string(k) + " has " + std::to_string(m) + " nodes (1 to 1024)";
+      if (f < next || f + m > n)
+        return "run " + std::to_string(k) + " overlaps another or leaves the system";
+      next = f + m;
+    }
+  }
+  if (pre->coarse_nodes) {
+    if (pre->coarse_group == 0 || pre->coarse_nodes > n || !pre->coarse_inverse)
+      return "coarse level: group 0, too many nodes or no inverse";
+    if ((pre->coarse_nodes + (uint64_t)pre->coarse_group - 1) / pre->coarse_group > kMaxAggregates)
+      return "coarse level: more than 2048 aggregates";
+  }
+  return "";
+}
+
+// Iterations per CUDA graph launch of the preconditioned loop (the host
+// checks the done flag between launches).
+constexpr int kRpChunk = 8;
+
+void reduced_solve_preconditioned(Context* c, const vlba_reduced_system* sys,
+                                  const vlba_reduced_preconditioner* pre, double* x,
+                                  uint32_t* iterations, double* relative_residual) {
+  const size_t n = sys->num_nodes;
+  cudaStream_t s = c->stream;
+  Dev& d = c->dev;
+  RpData rp{};
+  // One device block: the scalars, the run tables and inverses, the coarse
+  // inverse (row-major) and its two vectors.
+  const uint32_t nc = pre ? pre->num_clusters : 0;
+  std::vector<uint64_t> cl_off(nc);
+  uint64_t cl_floats = 0;
+  uint32_t max_rows = 0;
+  for (uint32_t k = 0; k < nc; ++k) {
+    const uint64_t rows = 6ull * pre->cluster_size[k];
+    cl_off[k] = cl_floats;
+    cl_floats += rows * rows;
+    max_rows = std::max<uint32_t>(max_rows, (uint32_t)rows);
+  }
+  const uint32_t m = (pre && pre->coarse_nodes)
+                         ? (pre->coarse_nodes + pre->coarse_group - 1) / pre->coarse_group
+                         : 0;
+  const uint64_t cm = 6ull * m;
+  auto up16 = [](uint64_t b) { return (b + 15) & ~uint64_t(15); };
+  const uint64_t o_first = up16(sizeof(RpScalars)), o_size = o_first + up16(4ull * nc),
+                 o_off = o_size + up16(4ull * nc), o_mat = o_off + up16(8ull * nc),
+                 o_cinv = o_mat + up16(4 * cl_floats), o_rc = o_cinv + up16(4 * cm * cm),
+                 o_yc = o_rc + up16(4 * cm), total = o_yc + up16(4 * cm);
+  DeviceArray buf;
+  buf.alloc(total);
+  char* base = buf.as<char>();
+  {
+    std::vector<float> mat(cl_floats), cinv(cm * cm);
+    if (nc) {
+      std::atomic<uint32_t> next{0};
+      auto work = [&] {
+        for (uint32_t k; (k = next.fetch_add(1)) < nc;) {
+          const uint64_t cnt = 36ull * pre->cluster_size[k] * pre->cluster_size[k];
+          const double* src = pre->cluster_inverse + cl_off[k];
+          for (uint64_t e = 0; e < cnt; ++e) mat[cl_off[k] + e] = (float)src[e];
+        }
+      };
+      const unsigned nt = std::max(1u, std::min<unsigned>(std::thread::hardware_concurrency(), 32u));
+      std::vector<std::thread> pool;
+      for (unsigned t = 1; t < std::min<unsigned>(nt, nc); ++t) pool.emplace_back(work);
+      work();
+      for (auto& t : pool) t.join();
+      VLBA_CUDA(cudaMemcpyAsync(base + o_first, pre->cluster_first, 4ull * nc, cudaMemcpyHostToDevice, s));
+      VLBA_CUDA(cudaMemcpyAsync(base + o_size, pre->cluster_size, 4ull * nc, cudaMemcpyHostToDevice, s));
+      VLBA_CUDA(cudaMemcpyAsync(base + o_off, cl_off.data(), 8ull * nc, cudaMemcpyHostToDevice, s));
+      VLBA_CUDA(cudaMemcpyAsync(base + o_mat, mat.data(), 4 * cl_floats, cudaMemcpyHostToDevice, s));
+    }
+    if (m) {
+      for (uint64_t r = 0; r < cm; ++r)
+        for (uint64_t col = 0; col < cm; ++col)
+          cinv[r * cm + col] = (float)pre->coarse_inverse[col * cm + r];
+      VLBA_CUDA(cudaMemcpyAsync(base + o_cinv, cinv.data(), 4 * cm * cm, cudaMemcpyHostToDevice, s));
+    }
+    VLBA_CUDA(cudaMemsetAsync(base, 0, sizeof(RpScalars), s));
+    VLBA_CUDA(cudaStreamSynchronize(s));  // the host copies above are freed next
+  }
+  rp.sc = reinterpret_cast<RpScalars*>(base);
+  rp.dots = d.dots;
+  rp.num_clusters = nc;
+  rp.max_cluster_rows = max_rows;
+  rp.cl_first = reinterpret_cast<const uint32_t*>(base + o_first);
+  rp.cl_size = reinterpret_cast<const uint32_t*>(base + o_size);
+  rp.cl_off = reinterpret_cast<const uint64_t*>(base + o_off);
+  rp.cl_mat = reinterpret_cast<const float*>(base + o_mat);
+  rp.coarse_m = m;
+  rp.coarse_group = m ? pre->coarse_group : 1;
+  rp.coarse_nodes = m ? pre->coarse_nodes : 0;
+  rp.coarse_inv = reinterpret_cast<const float*>(base + o_cinv);
+  rp.rc = reinterpret_cast<float*>(base + o_rc);
+  rp.yc = reinterpret_cast<float*>(base + o_yc);
+  rp.max_iterations = sys->max_iterations;
+  rp.tol = sys->tol;
+
+  check_launch(launch_rp_init(d, rp, s), "preconditioned solve init");
+  // kRpChunk iterations as one graph, launched until the device says done.
+  struct Graph {
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t e = nullptr;
+    ~Graph() {
+      if (e) cudaGraphExecDestroy(e);
+      if (g) cudaGraphDestroy(g);
+    }
+  } gr;
+  VLBA_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  cudaError_t le = cudaSuccess;
+  for (int k = 0; k < kRpChunk && le == cudaSuccess; ++k) le = launch_rp_iteration(d, rp, s);
+  const cudaError_t ce = cudaStreamEndCapture(s, &gr.g);
+  check_launch(le, "preconditioned solve iteration");
+  VLBA_CUDA(ce);
+  VLBA_CUDA(cudaGraphInstantiate(&gr.e, gr.g, 0));
+  RpScalars sc{};
+  for (uint64_t launched = 0;; launched += kRpChunk) {
+    VLBA_CUDA(cudaMemcpyAsync(&sc, rp.sc, sizeof sc, cudaMemcpyDeviceToHost, s));
+    VLBA_CUDA(cudaStreamSynchronize(s));
+    if (sc.done || launched >= sys->max_iterations) break;
+    VLBA_CUDA(cudaGraphLaunch(gr.e, s));
+  }
+  if (sc.failed)
+    throw Status(VLBA_DECLINED, "p.q not positive and finite at iteration " +
+                                    std::to_string(sc.iters + 1) + ": the CPU solver takes the system");
+  download_step(c, n, x);
+  if (iterations) *iterations = sc.iters;
+  if (relative_residual) *relative_residual = sc.bnorm > 0 ? sc.rnorm / sc.bnorm : 0.0;
+}
+
+}  // namespace vlba
+
+extern "C" {
+
 int visloc_ba_cuda_reduced_solve(void* ctx, const vlba_reduced_system* sys, double* x,
                                  uint32_t* iterations, double* relative_residual) {
   auto* c = static_cast<Context*>(ctx);
-  if (!c || !sys || !x || !sys->diag || !sys->rhs || sys->num_nodes == 0 ||
-      (sys->num_edges && (!sys->edges || !sys->offdiag)) || !(sys->tol >= 0.0))
-    return VLBA_ERR_INVALID_ARGUMENT;
+  if (!c || !x || !vlba::reduced_system_ok(sys)) return VLBA_ERR_INVALID_ARGUMENT;
   return vlba::guarded(c, [&] {
     vlba::set_device(c);
-    vlba_config cfg;
-    visloc_ba_cuda_default_config(&cfg);
-    cfg.max_pcg_iterations = sys->max_iterations;
-    cfg.pcg_relative_tolerance = sys->tol;
-    const vlba::LmParams lp = vlba::make_params(&cfg);
-    vlba::build_reduced_plan(sys->num_nodes, sys->edges, sys->num_edges, 8, lp, &c->plan);
-    const std::string bad = vlba::check_plan(c->plan);
-    if (!bad.empty()) throw vlba::Status(VLBA_ERR_INVALID_ARGUMENT, bad);
-    vlba::upload_plan(c, 1);
+    vlba::reduced_setup(c, sys);
     cudaStream_t s = c->stream;
-    const size_t n = sys->num_nodes, ne = sys->num_edges;
-    // The caller's arrays, staged for the fill kernel.
-    struct Staged {
-      void* p = nullptr;
-      ~Staged() {
-        if (p) cudaFree(p);
-      }
-    } diag, off, rhs;
-    VLBA_CUDA(cudaMalloc(&diag.p, 36 * n * 8));
-    VLBA_CUDA(cudaMalloc(&rhs.p, 6 * n * 8));
-    if (ne) VLBA_CUDA(cudaMalloc(&off.p, 36 * ne * 4));
-    VLBA_CUDA(cudaMemcpyAsync(diag.p, sys->diag, 36 * n * 8, cudaMemcpyHostToDevice, s));
-    VLBA_CUDA(cudaMemcpyAsync(rhs.p, sys->rhs, 6 * n * 8, cudaMemcpyHostToDevice, s));
-    if (ne) VLBA_CUDA(cudaMemcpyAsync(off.p, sys->offdiag, 36 * ne * 4, cudaMemcpyHostToDevice, s));
     vlba::Dev& d = c->dev;
-    vlba::reset_state(c);
-    vlba::check_launch(vlba::launch_reduced_fill(d, (uint32_t)n, ne, (const double*)diag.p,
-                                                 (const float*)off.p, (const double*)rhs.p, s),
-                       "reduced fill");
     vlba::check_launch(vlba::launch_pcg_setup(d, s), "pcg setup");
     vlba::check_launch(vlba::launch_pcg(d, c->pcg_grid, s), "pcg");
-    std::vector<float> xf(6 * n);
-    VLBA_CUDA(cudaMemcpyAsync(xf.data(), d.x, xf.size() * 4, cudaMemcpyDeviceToHost, s));
     vlba::PcgState pg;
     VLBA_CUDA(cudaMemcpyAsync(&pg, d.pcg, sizeof pg, cudaMemcpyDeviceToHost, s));
     unsigned int err = 0;
     VLBA_CUDA(cudaMemcpyAsync(&err, d.error, 4, cudaMemcpyDeviceToHost, s));
     VLBA_CUDA(cudaStreamSynchronize(s));
     if (err) throw vlba::Status(VLBA_ERR_TIMEOUT, "a bounded device wait gave up");
-    for (size_t i = 0; i < xf.size(); ++i) x[i] = xf[i];
+    vlba::download_step(c, sys->num_nodes, x);
     if (iterations) *iterations = pg.iters;
     if (relative_residual) *relative_residual = pg.bnorm > 0 ? pg.rnorm / pg.bnorm : 0.0;
+  });
+}
+
+int visloc_ba_cuda_reduced_solve_preconditioned(void* ctx, const vlba_reduced_system* sys,
+                                                const vlba_reduced_preconditioner* pre,
+                                                double* x, uint32_t* iterations,
+                                                double* relative_residual) {
+  auto* c = static_cast<Context*>(ctx);
+  if (!c || !x || !vlba::reduced_system_ok(sys)) return VLBA_ERR_INVALID_ARGUMENT;
+  return vlba::guarded(c, [&] {
+    const std::string bad = vlba::check_preconditioner(pre, sys->num_nodes);
+    if (!bad.empty()) throw vlba::Status(VLBA_ERR_INVALID_ARGUMENT, bad);
+    vlba::set_device(c);
+    vlba::reduced_setup(c, sys);
+    vlba::reduced_solve_preconditioned(c, sys, pre, x, iterations, relative_residual);
   });
 }
 

@@ -203,6 +203,19 @@ class ReducedSystem(C.Structure):
     ]
 
 
+class ReducedPreconditioner(C.Structure):
+    _fields_ = [
+        ("num_clusters", C.c_uint32),
+        ("reserved", C.c_uint32),
+        ("cluster_first", C.POINTER(C.c_uint32)),
+        ("cluster_size", C.POINTER(C.c_uint32)),
+        ("cluster_inverse", C.POINTER(C.c_double)),
+        ("coarse_group", C.c_uint32),
+        ("coarse_nodes", C.c_uint32),
+        ("coarse_inverse", C.POINTER(C.c_double)),
+    ]
+
+
 class LaunchShape(C.Structure):
     _fields_ = [
         ("pcg_blocks", C.c_int32),
@@ -295,6 +308,10 @@ SOLVER_EXPORTS = {
     "visloc_ba_cuda_batch_download": (C.c_int, [C.c_void_p, C.c_uint32, P(P(Problem))]),
     "visloc_ba_cuda_reduced_solve": (
         C.c_int, [C.c_void_p, P(ReducedSystem), P(C.c_double), P(C.c_uint32), P(C.c_double)],
+    ),
+    "visloc_ba_cuda_reduced_solve_preconditioned": (
+        C.c_int, [C.c_void_p, P(ReducedSystem), P(ReducedPreconditioner), P(C.c_double),
+                  P(C.c_uint32), P(C.c_double)],
     ),
     "visloc_ba_cuda_autotune": (C.c_int, [C.c_void_p, P(LaunchShape)]),
     "visloc_ba_cuda_wait_probe": (C.c_int, [C.c_void_p, C.c_double, P(C.c_double)]),

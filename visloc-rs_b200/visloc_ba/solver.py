@@ -131,11 +131,17 @@ class CudaSolver:
         return self.lib.visloc_ba_cuda_download(self.ctx, C.byref(packed.abi()))
 
     # ------------------------------------------------------ reduced solve
-    def reduced_solve(self, diag, edges, offdiag, rhs, tol: float, max_iterations: int):
-        """ReducedSolveAccelerator::solve on a reduced camera system:
-        diag (n,6,6) damped diagonal blocks, edges (e,2) sorted (a, b) with
-        a < b, offdiag (e,6,6) the (row b, column a) blocks, rhs (n,6).
-        Returns (x (n,6), iterations, relative residual)."""
+    def reduced_solve(self, diag, edges, offdiag, rhs, tol: float, max_iterations: int,
+                      clusters=None, coarse=None):
+        """ReducedSolveAccelerator::solve on a reduced camera system
+        (ReducedCameraSystem, pipelines/slam/src/ba_accel.rs:50-72): diag
+        (n,6,6) damped diagonal blocks, edges (e,2) sorted (a, b) with a < b,
+        offdiag (e,6,6) the (row b, column a) blocks, rhs (n,6); clusters a
+        list of (first node, inverse (6m,6m)) over runs of consecutive nodes,
+        coarse (nodes per aggregate, leading nodes covered, inverse (6m,6m)).
+        Without either: block-Jacobi through the persistent PCG kernel.
+        Returns (x (n,6), iterations, relative residual); a breakdown raises
+        SolverError with status DECLINED, as pcg_core returns None."""
         import numpy as np
 
         diag = np.ascontiguousarray(np.asarray(diag, np.float64).transpose(0, 2, 1))  # column-major
@@ -156,9 +162,42 @@ class CudaSolver:
         x = np.zeros((n, 6))
         it = C.c_uint32()
         rr = C.c_double()
-        st = self.lib.visloc_ba_cuda_reduced_solve(self.ctx, C.byref(sysm),
-                                                   x.ctypes.data_as(C.POINTER(C.c_double)),
-                                                   C.byref(it), C.byref(rr))
+        xp = x.ctypes.data_as(C.POINTER(C.c_double))
+        if clusters is None and coarse is None:
+            st = self.lib.visloc_ba_cuda_reduced_solve(self.ctx, C.byref(sysm), xp,
+                                                       C.byref(it), C.byref(rr))
+        else:
+            pre = _abi.ReducedPreconditioner()
+            keep = []
+            if clusters:
+                for _, inv in clusters:
+                    sh = np.shape(inv)
+                    if len(sh) != 2 or sh[0] != sh[1] or sh[0] % 6:
+                        raise ValueError(f"cluster inverse of shape {sh}")
+                first = np.ascontiguousarray([c[0] for c in clusters], np.uint32)
+                size = np.ascontiguousarray([np.asarray(c[1]).shape[0] // 6 for c in clusters],
+                                            np.uint32)
+                # nalgebra's DMatrix is column-major.
+                inv = np.ascontiguousarray(np.concatenate(
+                    [np.asarray(c[1], np.float64).T.reshape(-1) for c in clusters]))
+                keep += [first, size, inv]
+                pre.num_clusters = len(clusters)
+                pre.cluster_first = first.ctypes.data_as(C.POINTER(C.c_uint32))
+                pre.cluster_size = size.ctypes.data_as(C.POINTER(C.c_uint32))
+                pre.cluster_inverse = inv.ctypes.data_as(C.POINTER(C.c_double))
+            if coarse is not None:
+                group, nodes, cinv = coarse
+                m = -(-int(nodes) // int(group)) if int(group) > 0 else 0
+                if np.shape(cinv) != (6 * m, 6 * m):
+                    raise ValueError(f"coarse inverse of shape {np.shape(cinv)} for "
+                                     f"{nodes} nodes in groups of {group}")
+                cinv = np.ascontiguousarray(np.asarray(cinv, np.float64).T)
+                keep.append(cinv)
+                pre.coarse_group = int(group)
+                pre.coarse_nodes = int(nodes)
+                pre.coarse_inverse = cinv.ctypes.data_as(C.POINTER(C.c_double))
+            st = self.lib.visloc_ba_cuda_reduced_solve_preconditioned(
+                self.ctx, C.byref(sysm), C.byref(pre), xp, C.byref(it), C.byref(rr))
         if st != _abi.OK:
             raise SolverError(st, self.last_error())
         return x, it.value, rr.value
