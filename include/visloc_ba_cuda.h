@@ -407,11 +407,70 @@ typedef struct vlba_reduced_preconditioner {
  * runs in a fixed order, so repeated solves give identical steps.  A p.q
  * that is not positive and finite fails the solve as in pcg_core (which
  * returns None): VLBA_DECLINED, and the caller runs its CPU solver.  A zero
- * right-hand side gives x = 0 after 0 iterations. */
+ * right-hand side gives x = 0 after 0 iterations.
+ *
+ * Both reduced-solve entry points accept offdiag = NULL with num_edges > 0:
+ * the blocks the context's last visloc_ba_cuda_reduced_eliminate formed, as
+ * ReducedCameraSystem::offdiag empty means (ba_accel.rs:58-60).  The edges
+ * must equal that elimination's, else VLBA_DECLINED (the reference's solve
+ * returns None without resident blocks). */
 int visloc_ba_cuda_reduced_solve_preconditioned(void* ctx, const vlba_reduced_system* system,
                                                 const vlba_reduced_preconditioner* pre,
                                                 double* x, uint32_t* iterations,
                                                 double* relative_residual);
+
+/* ReducedSolveAccelerator::eliminate (ba_accel.rs:136-144) on a
+ * PointElimination (ba_accel.rs:74-120): the off-diagonal blocks of the
+ * reduced camera system,
+ *
+ *   block(e) = extra(e) - sum over points p whose k-th and j-th nodes (k < j)
+ *              are s and t of  hcp[p, j] V_p^-1 hcp[p, k]^T,
+ *
+ * for each edge e = (s, t), s < t, the (row t, column s) block, formed on the
+ * device and kept there for the next solve with offdiag = NULL.  What
+ * returns to the caller: the blocks of run_edges (the edges inside its
+ * preconditioner runs, in that order) and, with coarse_group > 0, for each
+ * aggregate pair g <= h of the coarse level the sum of the blocks of edges
+ * from aggregate g to h within the leading coarse_nodes (coarse_sums[g m +
+ * h], m = ceil(coarse_nodes / coarse_group); entries g > h are zero).
+ *
+ * Each term is a 6x6 product of FP32 copies of hcp and of hcp V^-1 (formed
+ * in FP64), summed in FP64 in ascending point order, so the blocks do not
+ * depend on scheduling and repeated eliminations give identical blocks.
+ * The reference's per-node Cauchy-Schwarz bounds (`scale`) only scale its
+ * fixed-point sums; FP64 sums in a fixed order need none, and there is no
+ * field for them.  Its per-node slot lists (`slot_off`, `slots`) and edge
+ * row offsets (`row_off`) are derived here from the edges and point_nodes.
+ *
+ * The structure (edges, point_off, point_nodes) is indexed once per
+ * structure_id (nonzero) and kept while the id and the sizes stay the same;
+ * hcp is uploaded again whenever linearization_id changes.  Every pair of
+ * nodes of a point must be an edge.  VLBA_DECLINED when a returned block is
+ * not finite (the reference's None). */
+typedef struct vlba_point_elimination {
+  uint64_t structure_id;
+  uint64_t linearization_id;
+  uint32_t num_nodes;
+  uint32_t num_points;
+  uint64_t num_edges;
+  const uint32_t* edges;          /* [2 num_edges] (s, t), s < t, ascending */
+  const uint64_t* point_off;      /* [num_points + 1] into point_nodes / hcp */
+  const uint32_t* point_nodes;    /* ascending within each point */
+  const double* hcp;              /* [18 point_off[num_points]] 6x3 column-major J_node^T J_point */
+  const double* point_inverse;    /* [9 num_points] damped V_p^-1, 3x3 column-major */
+  const uint8_t* point_used;      /* [num_points] 0: left out (None); NULL: all used */
+  uint64_t num_extra;
+  const uint32_t* extra_edge;     /* [num_extra] edge of each direct coupling */
+  const double* extra_block;      /* [36 num_extra] column-major, added to its edge's block */
+  uint64_t num_run_edges;
+  const uint32_t* run_edges;      /* [num_run_edges] */
+  uint32_t coarse_group;          /* nodes per aggregate; 0: no coarse sums */
+  uint32_t coarse_nodes;          /* leading nodes the aggregates cover */
+} vlba_point_elimination;
+
+int visloc_ba_cuda_reduced_eliminate(void* ctx, const vlba_point_elimination* elimination,
+                                     double* run_blocks /* [36 num_run_edges] */,
+                                     double* coarse_sums /* [36 m m] or NULL without coarse */);
 
 /* --------------------------------------------------------------- autotuner */
 /* Launch shape of the uploaded system: the blocks of the persistent PCG

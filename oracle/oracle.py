@@ -446,3 +446,67 @@ def reduced_pcg(diag, edges, offdiag, rhs, tol: float, max_iterations: int,
         rz = rz_next
         p = z + beta * p
     return x.reshape(n, 6), it
+
+
+def eliminate_blocks(num_edges_or_edges, point_off, point_nodes, hcp, point_inverse, extra=()):
+    """The off-diagonal blocks of a point elimination in FP64 (the CPU's
+    eliminate_by_output, pipelines/slam/src/colmap_incremental/
+    rig_ba_solver.rs:2551-2648, as PointElimination documents it,
+    pipelines/slam/src/ba_accel.rs:74-80): for each point and each pair of
+    its nodes k < j, block(s, t) -= hcp[j] V^-1 hcp[k]^T, then the direct
+    couplings are added.  Blocks are (row t, column s) numpy 6x6."""
+    edges = np.asarray(num_edges_or_edges).reshape(-1, 2)
+    index = {(int(a), int(b)): e for e, (a, b) in enumerate(edges)}
+    blocks = np.zeros((len(edges), 6, 6))
+    for p in range(len(point_off) - 1):
+        v = point_inverse[p]
+        if v is None:
+            continue
+        lo, hi = int(point_off[p]), int(point_off[p + 1])
+        nodes = [int(x) for x in point_nodes[lo:hi]]
+        h = np.asarray(hcp[lo:hi], np.float64)
+        for k in range(len(nodes)):
+            scaled = h[k] @ v
+            for j in range(k + 1, len(nodes)):
+                blocks[index[(nodes[k], nodes[j])]] -= h[j] @ scaled.T
+    for e, m in extra:
+        blocks[int(e)] += m
+    return blocks
+
+
+def coarse_block_sums(edges, blocks, group: int, nodes: int):
+    """sums[g m + h] (g <= h): the sum of the blocks of edges (a, b) with a
+    in aggregate g and b in aggregate h, both below `nodes`
+    (EliminatedBlocks::coarse_sums, ba_accel.rs:119-125); zero for g > h."""
+    m = -(-nodes // group)
+    sums = np.zeros((m * m, 6, 6))
+    for (a, b), blk in zip(np.asarray(edges).reshape(-1, 2), blocks):
+        a, b = int(a), int(b)
+        if a < nodes and b < nodes:
+            sums[(a // group) * m + b // group] += blk
+    return sums
+
+
+def coarse_from_sums(diag, sums, n_frames: int, group: int):
+    """(group, n_frames, inverse) of the coarse level from aggregate-pair
+    block sums (coarse_from_sums, rig_ba_solver.rs:1276-1308): the diagonal
+    blocks summed per aggregate, each sum added to the (h, g) block and its
+    transpose to (g, h); None for fewer than two aggregates or a matrix that
+    is not positive definite."""
+    m = -(-n_frames // group)
+    if m < 2 or len(sums) != m * m:
+        return None
+    a = np.zeros((6 * m, 6 * m))
+    for i in range(n_frames):
+        g = i // group * 6
+        a[g:g + 6, g:g + 6] += diag[i]
+    for g in range(m):
+        for h in range(g, m):
+            s = sums[g * m + h]
+            a[6 * h:6 * h + 6, 6 * g:6 * g + 6] += s
+            a[6 * g:6 * g + 6, 6 * h:6 * h + 6] += s.T
+    try:
+        np.linalg.cholesky(a)
+    except np.linalg.LinAlgError:
+        return None
+    return group, n_frames, np.linalg.inv(a)

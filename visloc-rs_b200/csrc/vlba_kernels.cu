@@ -1836,24 +1836,26 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
 
 // A reduced camera system given by the caller (ReducedCameraSystem,
 // pipelines/slam/src/ba_accel.rs:50-72) into the tiles: edge e's (row b,
-// column a) block, column-major, to its row-major slot (and the mirrored
-// slot in a diagonal tile); node i's damped diagonal block, column-major
+// column a) block, column-major (f32, or the f64 blocks of a device
+// elimination), to its row-major slot (and the mirrored slot in a diagonal
+// tile); node i's damped diagonal block, column-major
 // f64, to its diagonal slot, its FP64 Cholesky inverse (the block-Jacobi
 // preconditioner; the diagonal's inverse if not positive definite) and its
 // rhs.  Padding slots keep zero blocks, preconditioner and rhs.
 __global__ void __launch_bounds__(256) k_reduced_fill(Dev d, uint32_t n, uint64_t ne,
                                                       const double* diag, const float* offdiag,
+                                                      const double* offdiag64,
                                                       const double* rhs) {
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < ne; e += stride) {
     const uint2 dst = d.blk_dst[e];
-    const float* src = offdiag + 36 * e;
 #pragma unroll
     for (int r = 0; r < 6; ++r)
 #pragma unroll
       for (int c = 0; c < 6; ++c) {
-        d.tiles[dst.x + r * 6 + c] = src[c * 6 + r];
-        if (dst.y != kNone) d.tiles[dst.y + c * 6 + r] = src[c * 6 + r];
+        const float v = offdiag ? offdiag[36 * e + c * 6 + r] : (float)offdiag64[36 * e + c * 6 + r];
+        d.tiles[dst.x + r * 6 + c] = v;
+        if (dst.y != kNone) d.tiles[dst.y + c * 6 + r] = v;
       }
   }
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < d.num_var_cams;
@@ -2013,9 +2015,10 @@ size_t pcg_smem_bytes(int) { return Pcg::kSmem; }
 int pcg_rows_per_block() { return Pcg::kOwnMax; }
 
 cudaError_t launch_reduced_fill(const Dev& d, uint32_t n, uint64_t ne, const double* diag,
-                                const float* offdiag, const double* rhs, cudaStream_t s) {
+                                const float* offdiag, const double* offdiag64, const double* rhs,
+                                cudaStream_t s) {
   const size_t work = std::max<size_t>((size_t)ne, d.num_var_cams);
-  k_reduced_fill<<<grid1d(work, 256), 256, 0, s>>>(d, n, ne, diag, offdiag, rhs);
+  k_reduced_fill<<<grid1d(work, 256), 256, 0, s>>>(d, n, ne, diag, offdiag, offdiag64, rhs);
   return cudaGetLastError();
 }
 

@@ -20,9 +20,11 @@ cudaError_t launch_pcg(const Dev& d, int sm_count, cudaStream_t s);
 cudaError_t launch_pose_update(const Dev& d, cudaStream_t s);
 cudaError_t launch_pcg_setup(const Dev& d, cudaStream_t s);
 // Fill the tiles, preconditioner and rhs of a reduced system given directly
-// (device arrays in the reference's layout).
+// (device arrays in the reference's layout; the off-diagonal blocks f32, or
+// f64 when offdiag is null).
 cudaError_t launch_reduced_fill(const Dev& d, uint32_t n, uint64_t ne, const double* diag,
-                                const float* offdiag, const double* rhs, cudaStream_t s);
+                                const float* offdiag, const double* offdiag64, const double* rhs,
+                                cudaStream_t s);
 // Bounded-wait self-test: waits on `flag` (which nothing sets) for limit_ns.
 cudaError_t launch_wait_probe(const unsigned int* flag, unsigned long long limit_ns,
                               unsigned int* err, unsigned long long* waited, cudaStream_t s);
@@ -65,6 +67,40 @@ struct RpData {
 cudaError_t launch_rp_init(const Dev& d, const RpData& rp, cudaStream_t s);
 // One iteration; a no-op once sc->done is set.
 cudaError_t launch_rp_iteration(const Dev& d, const RpData& rp, cudaStream_t s);
+
+// A point elimination on the device (vlba_reduced.cu): the pair index of the
+// structure, this call's camera-point blocks and point inverses, the blocks.
+struct ElimDev {
+  uint32_t n;
+  uint32_t num_points;
+  uint64_t num_edges;
+  uint64_t num_obs;
+  uint64_t num_run;
+  uint32_t coarse_m;           // aggregates (0: no coarse sums)
+  uint32_t coarse_group;
+  uint32_t coarse_nodes;
+  uint32_t pad;
+  const uint32_t* row_off;     // [n + 1]
+  const uint32_t* edge_t;      // [num_edges]
+  const uint32_t* pair_off;    // [num_edges + 1]
+  const uint2* pairs;          // (o_s, o_t), ascending point within an edge
+  const uint32_t* obs_point;   // [num_obs]
+  const double* hcp64;         // [18 num_obs] 6x3 column-major
+  const double* vinv64;        // [9 num_points] 3x3 column-major
+  const uint8_t* used;         // [num_points] or null (all used)
+  float* hcp32;                // [18 num_obs]
+  float* sk32;                 // [18 num_obs] hcp V^-1 (zero for a point left out)
+  const int32_t* extra_of;     // [num_edges] row of extra64 or -1; null: none
+  const double* extra64;       // [36 rows]
+  double* blocks;              // [36 num_edges] column-major (row t, column s)
+  const uint32_t* run_edges;   // [num_run]
+  double* run_out;             // [36 num_run]
+  double* coarse_out;          // [36 m m]
+};
+
+cudaError_t launch_el_prepare(const ElimDev& e, cudaStream_t s);
+cudaError_t launch_el_blocks(const ElimDev& e, cudaStream_t s);
+cudaError_t launch_el_outputs(const ElimDev& e, cudaStream_t s);
 
 // Occupancy-derived grid of the persistent PCG kernel (0 if it cannot run).
 int pcg_grid_size(int tb, int sm_count);

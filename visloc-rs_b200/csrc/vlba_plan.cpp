@@ -1134,4 +1134,101 @@ double algorithmic_bytes(const Plan& P, double k, double* b_pcg_out) {
   return b_lin + b_asm + k * b_pcg + b_bs + b_cost;
 }
 
+std::string build_elimination_index(uint32_t n, const uint32_t* edges, uint64_t ne,
+                                    uint32_t num_points, const uint64_t* point_off,
+                                    const uint32_t* point_nodes, ElimIndex* out) {
+  ElimIndex& X = *out;
+  X = ElimIndex();
+  X.n = n;
+  X.num_points = num_points;
+  X.num_edges = ne;
+  if (ne >= (1ull << 31)) return "too many edges";
+  if (point_off[0] != 0) return "point_off[0] is not 0";
+  const uint64_t nobs = point_off[num_points];
+  if (nobs >= (1ull << 32)) return "too many camera-point blocks";
+  X.num_obs = nobs;
+  // Edges: ascending, s < t < n; each node's range.
+  X.row_off.assign((size_t)n + 1, 0);
+  X.edge_t.resize(ne);
+  for (uint64_t e = 0; e < ne; ++e) {
+    const uint32_t s = edges[2 * e], t = edges[2 * e + 1];
+    if (!(s < t && t < n)) return "edge " + std::to_string(e) + " is not (s, t) with s < t < n";
+    if (e && (s < edges[2 * e - 2] || (s == edges[2 * e - 2] && t <= edges[2 * e - 1])))
+      return "edges are not sorted at " + std::to_string(e);
+    X.edge_t[e] = t;
+    ++X.row_off[s + 1];
+  }
+  for (uint32_t s = 0; s < n; ++s) X.row_off[s + 1] += X.row_off[s];
+  const uint32_t T = std::max(1u, std::min<uint32_t>(std::thread::hardware_concurrency(), 64u));
+  auto plo = [&](uint32_t t) { return (uint32_t)((uint64_t)num_points * t / T); };
+  // Pairs per point, each point's nodes checked.
+  std::vector<uint64_t> base((size_t)num_points + 1, 0);
+  std::vector<std::string> err(T);
+  run_threads(T, [&](uint32_t t) {
+    for (uint32_t p = plo(t); p < plo(t + 1) && err[t].empty(); ++p) {
+      const uint64_t a = point_off[p], b = point_off[p + 1];
+      if (b < a || b > nobs) {
+        err[t] = "point_off is not ascending at point " + std::to_string(p);
+        break;
+      }
+      for (uint64_t i = a; i < b; ++i)
+        if (point_nodes[i] >= n || (i > a && point_nodes[i] <= point_nodes[i - 1])) {
+          err[t] = "nodes of point " + std::to_string(p) + " are not ascending below n";
+          break;
+        }
+      base[p + 1] = (b - a) * (b - a - (b > a ? 1 : 0)) / 2;
+    }
+  });
+  for (auto& e : err)
+    if (!e.empty()) return e;
+  for (uint32_t p = 0; p < num_points; ++p) base[p + 1] += base[p];
+  const uint64_t npairs = base[num_points];
+  if (npairs >= (1ull << 32)) return "too many point pairs";
+  // Each pair's edge (binary search in row s) and observations, point-major.
+  std::vector<uint32_t, NoInit<uint32_t>> key(npairs), rec(2 * npairs);
+  run_threads(T, [&](uint32_t t) {
+    for (uint32_t p = plo(t); p < plo(t + 1) && err[t].empty(); ++p) {
+      const uint64_t a = point_off[p], b = point_off[p + 1];
+      uint64_t w = base[p];
+      for (uint64_t k = a; k < b; ++k) {
+        const uint32_t s = point_nodes[k];
+        const uint32_t* lo = X.edge_t.data() + X.row_off[s];
+        const uint32_t* hi = X.edge_t.data() + X.row_off[s + 1];
+        for (uint64_t j = k + 1; j < b; ++j) {
+          const uint32_t tn = point_nodes[j];
+          lo = std::lower_bound(lo, hi, tn);  // partners ascend: search on from the last
+          if (lo == hi || *lo != tn) {
+            err[t] = "nodes " + std::to_string(s) + " and " + std::to_string(tn) + " of point " +
+                     std::to_string(p) + " have no edge";
+            return;
+          }
+          key[w] = (uint32_t)(lo - X.edge_t.data());
+          rec[2 * w] = (uint32_t)k;
+          rec[2 * w + 1] = (uint32_t)j;
+          ++w;
+        }
+      }
+    }
+  });
+  for (auto& e : err)
+    if (!e.empty()) return e;
+  // Stable by edge: within an edge the pairs keep ascending point order.
+  std::vector<uint32_t, NoInit<uint32_t>> order(npairs);
+  X.pair_off.resize(ne + 1);
+  counting_sort((uint32_t)npairs, (uint32_t)ne, T, [&](uint32_t i) { return key[i]; }, 0u,
+                order.data(), X.pair_off.data());
+  X.pairs.resize(2 * npairs);
+  X.obs_point.resize(nobs);
+  run_threads(T, [&](uint32_t t) {
+    const uint64_t i0 = npairs * t / T, i1 = npairs * (t + 1) / T;
+    for (uint64_t i = i0; i < i1; ++i) {
+      X.pairs[2 * i] = rec[2 * (size_t)order[i]];
+      X.pairs[2 * i + 1] = rec[2 * (size_t)order[i] + 1];
+    }
+    for (uint32_t p = plo(t); p < plo(t + 1); ++p)
+      for (uint64_t o = point_off[p]; o < point_off[p + 1]; ++o) X.obs_point[o] = p;
+  });
+  return "";
+}
+
 }  // namespace vlba

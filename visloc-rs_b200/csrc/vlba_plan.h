@@ -138,6 +138,30 @@ void build_plan(const vlba_problem* const* problems, const vlba_config* const* c
 void build_reduced_plan(uint32_t n, const uint32_t* edges, uint64_t ne, uint32_t tb,
                         const LmParams& params, Plan* plan);
 
+// The pair index of a point elimination (ReducedSolveAccelerator::eliminate):
+// per edge (s, t) of the sorted edge list, the observation pairs (o_s, o_t) of
+// the points whose nodes include both s and t, in ascending point order.
+struct ElimIndex {
+  uint32_t n = 0;
+  uint32_t num_points = 0;
+  uint64_t num_edges = 0;
+  uint64_t num_obs = 0;
+  std::vector<uint32_t> row_off;                 // [n + 1] edges (s, _)
+  std::vector<uint32_t> edge_t;                  // [num_edges] second node
+  std::vector<uint32_t> pair_off;                // [num_edges + 1]
+  std::vector<uint32_t, NoInit<uint32_t>> pairs; // [2 pairs] (o_s, o_t)
+  std::vector<uint32_t, NoInit<uint32_t>> obs_point;  // [num_obs]
+};
+
+// Builds the index of n nodes, ne sorted edges and num_points points (their
+// nodes point_nodes[point_off[p] .. point_off[p + 1]], ascending) on the
+// host's threads.  Returns an empty string, or the first inconsistency found
+// (unsorted edges, a node out of range, a pair of nodes with no edge, a size
+// past the 32-bit indices).
+std::string build_elimination_index(uint32_t n, const uint32_t* edges, uint64_t ne,
+                                    uint32_t num_points, const uint64_t* point_off,
+                                    const uint32_t* point_nodes, ElimIndex* out);
+
 // Concatenate plans (built by build_plan) into one batch plan: indices are
 // offset, each problem's layout and order are kept, so a problem solves the
 // same in the merged plan as in its own.

@@ -302,6 +302,128 @@ __global__ void k_rp_scalars(Dev d, RpData rp, int step) {
   }
 }
 
+// ---------------------------------------------------------------- elimination
+// Per camera-point block o of point p: an FP32 copy of hcp and sk = hcp V_p^-1
+// (formed in FP64; zero for a point left out, whose pairs then add zero).
+__global__ void k_el_prepare(ElimDev E) {
+  for (uint64_t o = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; o < E.num_obs;
+       o += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t p = E.obs_point[o];
+    const double* h = E.hcp64 + 18 * o;
+    const double* v = E.vinv64 + 9 * (size_t)p;
+    const bool used = !E.used || E.used[p];
+    double hv[18];
+#pragma unroll
+    for (int q = 0; q < 18; ++q) hv[q] = h[q];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int r = 0; r < 6; ++r) {
+        const double sk = hv[r] * v[3 * i] + hv[6 + r] * v[3 * i + 1] + hv[12 + r] * v[3 * i + 2];
+        E.sk32[18 * o + 6 * i + r] = used ? (float)sk : 0.0f;
+      }
+#pragma unroll
+    for (int q = 0; q < 18; ++q) E.hcp32[18 * o + q] = (float)hv[q];
+  }
+}
+
+// One warp per edge (s, t): lane l owns entry l of the column-major block
+// (row r = l % 6 of t, column c = l / 6 of s), lanes 0-3 also entry 32 + l,
+// and sums its pairs' terms sum_i hcp_t[r][i] sk_s[c][i] in FP64 in the pair
+// order (ascending point): no reduction, no atomics.
+__global__ void __launch_bounds__(256) k_el_blocks(ElimDev E) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint64_t nw = (uint64_t)gridDim.x * blockDim.x / 32u;
+  const int r0 = (int)lane % 6, c0 = (int)lane / 6;
+  const int r1 = (int)(lane + 32) % 6, c1 = (int)(lane + 32) / 6;
+  const bool two = lane < 4u;
+  for (uint64_t e = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / 32u; e < E.num_edges;
+       e += nw) {
+    const uint32_t a = E.pair_off[e], b = E.pair_off[e + 1];
+    double acc0 = 0.0, acc1 = 0.0;
+    uint32_t i = a;
+    // Four pairs' loads in flight, summed in pair order.
+    for (; i + 4 <= b; i += 4) {
+      float v0[4], v1[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const uint2 pr = __ldg(E.pairs + i + u);
+        const float* ht = E.hcp32 + 18 * (size_t)pr.y;
+        const float* ss = E.sk32 + 18 * (size_t)pr.x;
+        float v = __ldg(ht + r0) * __ldg(ss + c0);
+        v = fmaf(__ldg(ht + 6 + r0), __ldg(ss + 6 + c0), v);
+        v0[u] = fmaf(__ldg(ht + 12 + r0), __ldg(ss + 12 + c0), v);
+        float w = 0.0f;
+        if (two) {
+          w = __ldg(ht + r1) * __ldg(ss + c1);
+          w = fmaf(__ldg(ht + 6 + r1), __ldg(ss + 6 + c1), w);
+          w = fmaf(__ldg(ht + 12 + r1), __ldg(ss + 12 + c1), w);
+        }
+        v1[u] = w;
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        acc0 += (double)v0[u];
+        acc1 += (double)v1[u];
+      }
+    }
+    for (; i < b; ++i) {
+      const uint2 pr = __ldg(E.pairs + i);
+      const float* ht = E.hcp32 + 18 * (size_t)pr.y;
+      const float* ss = E.sk32 + 18 * (size_t)pr.x;
+      float v = __ldg(ht + r0) * __ldg(ss + c0);
+      v = fmaf(__ldg(ht + 6 + r0), __ldg(ss + 6 + c0), v);
+      acc0 += (double)fmaf(__ldg(ht + 12 + r0), __ldg(ss + 12 + c0), v);
+      if (two) {
+        float w = __ldg(ht + r1) * __ldg(ss + c1);
+        w = fmaf(__ldg(ht + 6 + r1), __ldg(ss + 6 + c1), w);
+        acc1 += (double)fmaf(__ldg(ht + 12 + r1), __ldg(ss + 12 + c1), w);
+      }
+    }
+    const int x = E.extra_of ? E.extra_of[e] : -1;
+    double* out = E.blocks + 36 * e;
+    out[lane] = (x >= 0 ? E.extra64[36 * (size_t)x + lane] : 0.0) - acc0;
+    if (two) out[32 + lane] = (x >= 0 ? E.extra64[36 * (size_t)x + 32 + lane] : 0.0) - acc1;
+  }
+}
+
+// The blocks of the run edges, copied out.
+__global__ void k_el_gather(ElimDev E) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < 36 * E.num_run;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    E.run_out[i] = E.blocks[36 * (size_t)E.run_edges[i / 36] + i % 36];
+}
+
+// coarse_out[g m + h] (g <= h): the sum of the blocks of edges (a, b), a in
+// aggregate g, b in aggregate h, both below coarse_nodes, in node then edge
+// order.  One block per g, one warp per h, lanes over the 36 entries.
+__global__ void __launch_bounds__(256) k_el_coarse(ElimDev E) {
+  const uint32_t g = blockIdx.x, m = E.coarse_m, grp = E.coarse_group;
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const bool two = lane < 4u;
+  const uint32_t a1 = min((g + 1) * grp, E.coarse_nodes);
+  for (uint32_t h = g + warp; h < m; h += blockDim.x / 32u) {
+    const uint32_t t0 = h * grp, t1 = min((h + 1) * grp, E.coarse_nodes);
+    double acc0 = 0.0, acc1 = 0.0;
+    for (uint32_t a = g * grp; a < a1; ++a) {
+      uint32_t lo = E.row_off[a], hi = E.row_off[a + 1];
+      const uint32_t end = hi;
+      while (lo < hi) {
+        const uint32_t mid = (lo + hi) / 2;
+        if (E.edge_t[mid] < t0) lo = mid + 1;
+        else hi = mid;
+      }
+      for (uint32_t e = lo; e < end && E.edge_t[e] < t1; ++e) {
+        acc0 += E.blocks[36 * (size_t)e + lane];
+        if (two) acc1 += E.blocks[36 * (size_t)e + 32 + lane];
+      }
+    }
+    double* out = E.coarse_out + 36 * ((size_t)g * m + h);
+    out[lane] = acc0;
+    if (two) out[32 + lane] = acc1;
+  }
+}
+
 int rows_grid(const Dev& d) { return (int)((d.num_tile_rows + 7) / 8); }
 int flat_grid(size_t n) { return (int)std::min<size_t>((n + 255) / 256, 148 * 8); }
 
@@ -341,6 +463,23 @@ cudaError_t launch_rp_iteration(const Dev& d, const RpData& rp, cudaStream_t s) 
   precondition(d, rp, s);
   k_rp_scalars<<<1, 32, 0, s>>>(d, rp, kRpBeta);
   k_rp_update_p<<<flat_grid((size_t)d.num_var_cams * 6), 256, 0, s>>>(d, rp, 0);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_el_prepare(const ElimDev& e, cudaStream_t s) {
+  if (e.num_obs) k_el_prepare<<<flat_grid(e.num_obs), 256, 0, s>>>(e);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_el_blocks(const ElimDev& e, cudaStream_t s) {
+  if (e.num_edges)
+    k_el_blocks<<<(int)std::min<uint64_t>((e.num_edges + 7) / 8, 148 * 64), 256, 0, s>>>(e);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_el_outputs(const ElimDev& e, cudaStream_t s) {
+  if (e.num_run) k_el_gather<<<flat_grid(36 * e.num_run), 256, 0, s>>>(e);
+  if (e.coarse_m) k_el_coarse<<<e.coarse_m, 256, 0, s>>>(e);
   return cudaGetLastError();
 }
 

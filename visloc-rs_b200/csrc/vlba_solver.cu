@@ -11,6 +11,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cmath>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -49,6 +50,52 @@ struct Status : std::runtime_error {
   int code;
   uint64_t index;
   Status(int c, const std::string& m, uint64_t i = 0) : std::runtime_error(m), code(c), index(i) {}
+};
+
+// A device allocation freed with its holder (cudaFree waits for the work
+// that uses it).
+struct DeviceArray {
+  void* p = nullptr;
+  size_t bytes = 0;
+  DeviceArray() = default;
+  DeviceArray(const DeviceArray&) = delete;
+  DeviceArray& operator=(const DeviceArray&) = delete;
+  ~DeviceArray() { reset(); }
+  void reset() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  void alloc(size_t n) {
+    reset();
+    VLBA_CUDA(cudaMalloc(&p, std::max<size_t>(n, 16)));
+    bytes = n;
+  }
+  // At least n bytes, keeping the allocation when it is large enough.
+  void ensure(size_t n) {
+    if (!p || bytes < n) alloc(n);
+  }
+  template <class T>
+  T* as() const {
+    return static_cast<T*>(p);
+  }
+};
+
+// The state of the context's last point elimination: the structure's pair
+// index on the device (kept while the structure id and sizes stay the same),
+// the camera-point blocks (kept while the linearization id does), and the
+// blocks it formed, which a reduced solve with no off-diagonal blocks uses.
+struct ElimState {
+  uint64_t structure_id = 0;
+  uint64_t linearization_id = 0;
+  bool hcp_valid = false;
+  bool blocks_valid = false;
+  uint32_t n = 0, num_points = 0;
+  uint64_t num_edges = 0, num_obs = 0, num_pairs = 0;
+  std::vector<uint32_t> edges;  // the structure's edges (2 per edge), for the solve's check
+  DeviceArray row_off, edge_t, pair_off, pairs, obs_point;
+  DeviceArray hcp64, hcp32, sk32, vinv64, used, extra_of, extra64, blocks, run_edges, run_out,
+      coarse_out;
 };
 
 // A slab allocation that does not fit (the upload is redone on a larger slab).
@@ -173,6 +220,8 @@ struct Context {
   // Per-observation squared residuals of a GNC solve (grown on demand).
   double* gnc_sq = nullptr;
   size_t gnc_cap = 0;
+  // The last point elimination (ReducedSolveAccelerator::eliminate).
+  std::unique_ptr<ElimState> elim;
 };
 
 namespace {
@@ -1064,6 +1113,7 @@ void free_context(Context* c) {
     if (c->stage[i]) cudaFreeHost(c->stage[i]);
   }
   if (c->gnc_sq) cudaFree(c->gnc_sq);
+  c->elim.reset();
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }
@@ -1924,31 +1974,23 @@ int visloc_ba_cuda_server_wait(void* server, uint64_t ticket, double timeout_ms,
 
 namespace vlba {
 
-// A device allocation freed with its holder (cudaFree waits for the work
-// that uses it).
-struct DeviceArray {
-  void* p = nullptr;
-  DeviceArray() = default;
-  DeviceArray(const DeviceArray&) = delete;
-  DeviceArray& operator=(const DeviceArray&) = delete;
-  ~DeviceArray() {
-    if (p) cudaFree(p);
-  }
-  void alloc(size_t bytes) { VLBA_CUDA(cudaMalloc(&p, std::max<size_t>(bytes, 16))); }
-  template <class T>
-  T* as() const {
-    return static_cast<T*>(p);
-  }
-};
-
 bool reduced_system_ok(const vlba_reduced_system* sys) {
   return sys && sys->diag && sys->rhs && sys->num_nodes != 0 &&
-         (!sys->num_edges || (sys->edges && sys->offdiag)) && sys->tol >= 0.0;
+         (!sys->num_edges || sys->edges) && sys->tol >= 0.0;
 }
 
 // Plans and uploads a reduced system given in the reference's layout and
-// fills S's tiles, the block-Jacobi inverses and the rhs on the device.
+// fills S's tiles, the block-Jacobi inverses and the rhs on the device; with
+// no off-diagonal blocks (offdiag null), from the blocks of the context's
+// last elimination of the same edges.
 void reduced_setup(Context* c, const vlba_reduced_system* sys) {
+  const bool resident = sys->num_edges && !sys->offdiag;
+  if (resident) {
+    const ElimState* E = c->elim.get();
+    if (!E || !E->blocks_valid || E->n != sys->num_nodes || E->num_edges != sys->num_edges ||
+        std::memcmp(E->edges.data(), sys->edges, 8 * sys->num_edges) != 0)
+      throw Status(VLBA_DECLINED, "no off-diagonal blocks given and none formed for these edges");
+  }
   vlba_config cfg;
   visloc_ba_cuda_default_config(&cfg);
   cfg.max_pcg_iterations = sys->max_iterations;
@@ -1963,13 +2005,16 @@ void reduced_setup(Context* c, const vlba_reduced_system* sys) {
   DeviceArray diag, off, rhs;  // the caller's arrays, staged for the fill kernel
   diag.alloc(36 * n * 8);
   rhs.alloc(6 * n * 8);
-  if (ne) off.alloc(36 * ne * 4);
+  if (ne && !resident) off.alloc(36 * ne * 4);
   VLBA_CUDA(cudaMemcpyAsync(diag.p, sys->diag, 36 * n * 8, cudaMemcpyHostToDevice, s));
   VLBA_CUDA(cudaMemcpyAsync(rhs.p, sys->rhs, 6 * n * 8, cudaMemcpyHostToDevice, s));
-  if (ne) VLBA_CUDA(cudaMemcpyAsync(off.p, sys->offdiag, 36 * ne * 4, cudaMemcpyHostToDevice, s));
+  if (ne && !resident)
+    VLBA_CUDA(cudaMemcpyAsync(off.p, sys->offdiag, 36 * ne * 4, cudaMemcpyHostToDevice, s));
   reset_state(c);
   check_launch(launch_reduced_fill(c->dev, (uint32_t)n, ne, diag.as<const double>(),
-                                   ne ? off.as<const float>() : nullptr, rhs.as<const double>(), s),
+                                   ne && !resident ? off.as<const float>() : nullptr,
+                                   resident ? c->elim->blocks.as<const double>() : nullptr,
+                                   rhs.as<const double>(), s),
                "reduced fill");
   VLBA_CUDA(cudaStreamSynchronize(s));
 }
@@ -2123,6 +2168,139 @@ void reduced_solve_preconditioned(Context* c, const vlba_reduced_system* sys,
   if (relative_residual) *relative_residual = sc.bnorm > 0 ? sc.rnorm / sc.bnorm : 0.0;
 }
 
+// ReducedSolveAccelerator::eliminate on the device.  Returns false (and
+// sets nothing) when a returned block is not finite.
+bool reduced_eliminate(Context* c, const vlba_point_elimination* el, double* run_blocks,
+                       double* coarse_sums) {
+  cudaStream_t s = c->stream;
+  const uint32_t n = el->num_nodes, P = el->num_points;
+  const uint64_t ne = el->num_edges, nobs = el->point_off[P];
+  if (!c->elim) c->elim = std::make_unique<ElimState>();
+  ElimState& E = *c->elim;
+  E.blocks_valid = false;
+  if (E.structure_id != el->structure_id || E.n != n || E.num_points != P ||
+      E.num_edges != ne || E.num_obs != nobs) {
+    E.structure_id = 0;
+    E.hcp_valid = false;
+    ElimIndex X;
+    const std::string bad =
+        build_elimination_index(n, el->edges, ne, P, el->point_off, el->point_nodes, &X);
+    if (!bad.empty()) throw Status(VLBA_ERR_INVALID_ARGUMENT, bad);
+    E.num_pairs = X.pairs.size() / 2;
+    E.row_off.ensure(4 * X.row_off.size());
+    E.edge_t.ensure(4 * ne);
+    E.pair_off.ensure(4 * X.pair_off.size());
+    E.pairs.ensure(4 * X.pairs.size());
+    E.obs_point.ensure(4 * nobs);
+    VLBA_CUDA(cudaMemcpyAsync(E.row_off.p, X.row_off.data(), 4 * X.row_off.size(),
+                              cudaMemcpyHostToDevice, s));
+    VLBA_CUDA(cudaMemcpyAsync(E.edge_t.p, X.edge_t.data(), 4 * ne, cudaMemcpyHostToDevice, s));
+    VLBA_CUDA(cudaMemcpyAsync(E.pair_off.p, X.pair_off.data(), 4 * X.pair_off.size(),
+                              cudaMemcpyHostToDevice, s));
+    VLBA_CUDA(cudaMemcpyAsync(E.pairs.p, X.pairs.data(), 4 * X.pairs.size(),
+                              cudaMemcpyHostToDevice, s));
+    VLBA_CUDA(cudaMemcpyAsync(E.obs_point.p, X.obs_point.data(), 4 * nobs,
+                              cudaMemcpyHostToDevice, s));
+    E.edges.assign(el->edges, el->edges + 2 * ne);
+    E.hcp64.ensure(144 * nobs);
+    E.hcp32.ensure(72 * nobs);
+    E.sk32.ensure(72 * nobs);
+    E.blocks.ensure(288 * ne);
+    VLBA_CUDA(cudaStreamSynchronize(s));  // X's host arrays go next
+    E.n = n;
+    E.num_points = P;
+    E.num_edges = ne;
+    E.num_obs = nobs;
+    E.structure_id = el->structure_id;
+  }
+  if (!E.hcp_valid || E.linearization_id != el->linearization_id) {
+    VLBA_CUDA(cudaMemcpyAsync(E.hcp64.p, el->hcp, 144 * nobs, cudaMemcpyHostToDevice, s));
+    E.hcp_valid = true;
+    E.linearization_id = el->linearization_id;
+  }
+  // Per call: the point inverses, the couplings (merged per edge in their
+  // order), the run edges and the outputs.
+  E.vinv64.ensure(72ull * P);
+  VLBA_CUDA(cudaMemcpyAsync(E.vinv64.p, el->point_inverse, 72ull * P, cudaMemcpyHostToDevice, s));
+  if (el->point_used) {
+    E.used.ensure(P);
+    VLBA_CUDA(cudaMemcpyAsync(E.used.p, el->point_used, P, cudaMemcpyHostToDevice, s));
+  }
+  std::vector<int32_t> extra_of;
+  std::vector<double> extra;
+  if (el->num_extra) {
+    extra_of.assign(ne, -1);
+    for (uint64_t i = 0; i < el->num_extra; ++i) {
+      int32_t& x = extra_of[el->extra_edge[i]];
+      if (x < 0) {
+        x = (int32_t)(extra.size() / 36);
+        extra.insert(extra.end(), el->extra_block + 36 * i, el->extra_block + 36 * i + 36);
+      } else {
+        for (int q = 0; q < 36; ++q) extra[36 * (size_t)x + q] += el->extra_block[36 * i + q];
+      }
+    }
+    E.extra_of.ensure(4 * ne);
+    E.extra64.ensure(8 * extra.size());
+    VLBA_CUDA(cudaMemcpyAsync(E.extra_of.p, extra_of.data(), 4 * ne, cudaMemcpyHostToDevice, s));
+    VLBA_CUDA(cudaMemcpyAsync(E.extra64.p, extra.data(), 8 * extra.size(), cudaMemcpyHostToDevice,
+                              s));
+  }
+  const uint64_t nrun = el->num_run_edges;
+  if (nrun) {
+    E.run_edges.ensure(4 * nrun);
+    E.run_out.ensure(288 * nrun);
+    VLBA_CUDA(cudaMemcpyAsync(E.run_edges.p, el->run_edges, 4 * nrun, cudaMemcpyHostToDevice, s));
+  }
+  const uint32_t m = el->coarse_group && el->coarse_nodes
+                         ? (el->coarse_nodes + el->coarse_group - 1) / el->coarse_group
+                         : 0;
+  const uint64_t nsum = 36ull * m * m;
+  if (m) {
+    E.coarse_out.ensure(8 * nsum);
+    VLBA_CUDA(cudaMemsetAsync(E.coarse_out.p, 0, 8 * nsum, s));
+  }
+  ElimDev d{};
+  d.n = n;
+  d.num_points = P;
+  d.num_edges = ne;
+  d.num_obs = nobs;
+  d.num_run = nrun;
+  d.coarse_m = m;
+  d.coarse_group = m ? el->coarse_group : 1;
+  d.coarse_nodes = m ? el->coarse_nodes : 0;
+  d.row_off = E.row_off.as<const uint32_t>();
+  d.edge_t = E.edge_t.as<const uint32_t>();
+  d.pair_off = E.pair_off.as<const uint32_t>();
+  d.pairs = E.pairs.as<const uint2>();
+  d.obs_point = E.obs_point.as<const uint32_t>();
+  d.hcp64 = E.hcp64.as<const double>();
+  d.vinv64 = E.vinv64.as<const double>();
+  d.used = el->point_used ? E.used.as<const uint8_t>() : nullptr;
+  d.hcp32 = E.hcp32.as<float>();
+  d.sk32 = E.sk32.as<float>();
+  d.extra_of = el->num_extra ? E.extra_of.as<const int32_t>() : nullptr;
+  d.extra64 = el->num_extra ? E.extra64.as<const double>() : nullptr;
+  d.blocks = E.blocks.as<double>();
+  d.run_edges = E.run_edges.as<const uint32_t>();
+  d.run_out = E.run_out.as<double>();
+  d.coarse_out = E.coarse_out.as<double>();
+  check_launch(launch_el_prepare(d, s), "elimination prepare");
+  check_launch(launch_el_blocks(d, s), "elimination blocks");
+  check_launch(launch_el_outputs(d, s), "elimination outputs");
+  if (nrun)
+    VLBA_CUDA(cudaMemcpyAsync(run_blocks, E.run_out.p, 288 * nrun, cudaMemcpyDeviceToHost, s));
+  if (m && coarse_sums)
+    VLBA_CUDA(cudaMemcpyAsync(coarse_sums, E.coarse_out.p, 8 * nsum, cudaMemcpyDeviceToHost, s));
+  VLBA_CUDA(cudaStreamSynchronize(s));
+  for (uint64_t i = 0; i < 36 * nrun; ++i)
+    if (!std::isfinite(run_blocks[i])) return false;
+  if (m && coarse_sums)
+    for (uint64_t i = 0; i < nsum; ++i)
+      if (!std::isfinite(coarse_sums[i])) return false;
+  E.blocks_valid = true;
+  return true;
+}
+
 }  // namespace vlba
 
 extern "C" {
@@ -2162,6 +2340,38 @@ int visloc_ba_cuda_reduced_solve_preconditioned(void* ctx, const vlba_reduced_sy
     vlba::set_device(c);
     vlba::reduced_setup(c, sys);
     vlba::reduced_solve_preconditioned(c, sys, pre, x, iterations, relative_residual);
+  });
+}
+
+int visloc_ba_cuda_reduced_eliminate(void* ctx, const vlba_point_elimination* el,
+                                     double* run_blocks, double* coarse_sums) {
+  auto* c = static_cast<Context*>(ctx);
+  if (!c || !el || el->structure_id == 0 || el->num_nodes == 0 || !el->point_off ||
+      (el->num_edges && !el->edges) || (el->num_points && !el->point_inverse) ||
+      (el->num_extra && (!el->extra_edge || !el->extra_block)) ||
+      (el->num_run_edges && (!el->run_edges || !run_blocks)))
+    return VLBA_ERR_INVALID_ARGUMENT;
+  return vlba::guarded(c, [&] {
+    const uint64_t nobs = el->point_off[el->num_points];
+    if (nobs && (!el->point_nodes || !el->hcp))
+      throw vlba::Status(VLBA_ERR_INVALID_ARGUMENT, "point_nodes or hcp missing");
+    for (uint64_t i = 0; i < el->num_extra; ++i)
+      if (el->extra_edge[i] >= el->num_edges)
+        throw vlba::Status(VLBA_ERR_INVALID_ARGUMENT, "extra coupling " + std::to_string(i) +
+                                                          " names no edge");
+    for (uint64_t i = 0; i < el->num_run_edges; ++i)
+      if (el->run_edges[i] >= el->num_edges)
+        throw vlba::Status(VLBA_ERR_INVALID_ARGUMENT, "run edge " + std::to_string(i) +
+                                                          " names no edge");
+    if (el->coarse_group &&
+        (el->coarse_nodes > el->num_nodes || !coarse_sums ||
+         (el->coarse_nodes + (uint64_t)el->coarse_group - 1) / el->coarse_group > 2048))
+      throw vlba::Status(VLBA_ERR_INVALID_ARGUMENT,
+                         "coarse level: more nodes than the system, no output or over 2048 "
+                         "aggregates");
+    vlba::set_device(c);
+    if (!vlba::reduced_eliminate(c, el, run_blocks, coarse_sums))
+      throw vlba::Status(VLBA_DECLINED, "an eliminated block is not finite");
   });
 }
 

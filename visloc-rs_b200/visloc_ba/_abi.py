@@ -203,6 +203,29 @@ class ReducedSystem(C.Structure):
     ]
 
 
+class PointElimination(C.Structure):
+    _fields_ = [
+        ("structure_id", C.c_uint64),
+        ("linearization_id", C.c_uint64),
+        ("num_nodes", C.c_uint32),
+        ("num_points", C.c_uint32),
+        ("num_edges", C.c_uint64),
+        ("edges", C.POINTER(C.c_uint32)),
+        ("point_off", C.POINTER(C.c_uint64)),
+        ("point_nodes", C.POINTER(C.c_uint32)),
+        ("hcp", C.POINTER(C.c_double)),
+        ("point_inverse", C.POINTER(C.c_double)),
+        ("point_used", C.POINTER(C.c_uint8)),
+        ("num_extra", C.c_uint64),
+        ("extra_edge", C.POINTER(C.c_uint32)),
+        ("extra_block", C.POINTER(C.c_double)),
+        ("num_run_edges", C.c_uint64),
+        ("run_edges", C.POINTER(C.c_uint32)),
+        ("coarse_group", C.c_uint32),
+        ("coarse_nodes", C.c_uint32),
+    ]
+
+
 class ReducedPreconditioner(C.Structure):
     _fields_ = [
         ("num_clusters", C.c_uint32),
@@ -308,6 +331,9 @@ SOLVER_EXPORTS = {
     "visloc_ba_cuda_batch_download": (C.c_int, [C.c_void_p, C.c_uint32, P(P(Problem))]),
     "visloc_ba_cuda_reduced_solve": (
         C.c_int, [C.c_void_p, P(ReducedSystem), P(C.c_double), P(C.c_uint32), P(C.c_double)],
+    ),
+    "visloc_ba_cuda_reduced_eliminate": (
+        C.c_int, [C.c_void_p, P(PointElimination), P(C.c_double), P(C.c_double)],
     ),
     "visloc_ba_cuda_reduced_solve_preconditioned": (
         C.c_int, [C.c_void_p, P(ReducedSystem), P(ReducedPreconditioner), P(C.c_double),

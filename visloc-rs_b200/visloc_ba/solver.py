@@ -145,8 +145,9 @@ class CudaSolver:
         import numpy as np
 
         diag = np.ascontiguousarray(np.asarray(diag, np.float64).transpose(0, 2, 1))  # column-major
-        off = np.ascontiguousarray(np.asarray(offdiag, np.float32).reshape(-1, 6, 6)
-                                   .transpose(0, 2, 1))
+        # offdiag None: the blocks of the last reduced_eliminate of these edges.
+        off = None if offdiag is None else np.ascontiguousarray(
+            np.asarray(offdiag, np.float32).reshape(-1, 6, 6).transpose(0, 2, 1))
         edges = np.ascontiguousarray(np.asarray(edges, np.uint32).reshape(-1, 2))
         rhs = np.ascontiguousarray(np.asarray(rhs, np.float64).reshape(-1, 6))
         n = diag.shape[0]
@@ -155,7 +156,8 @@ class CudaSolver:
         sysm.num_edges = edges.shape[0]
         sysm.diag = diag.ctypes.data_as(C.POINTER(C.c_double))
         sysm.edges = edges.ctypes.data_as(C.POINTER(C.c_uint32))
-        sysm.offdiag = off.ctypes.data_as(C.POINTER(C.c_float))
+        sysm.offdiag = (C.POINTER(C.c_float)() if off is None
+                        else off.ctypes.data_as(C.POINTER(C.c_float)))
         sysm.rhs = rhs.ctypes.data_as(C.POINTER(C.c_double))
         sysm.tol = float(tol)
         sysm.max_iterations = int(max_iterations)
@@ -201,6 +203,67 @@ class CudaSolver:
         if st != _abi.OK:
             raise SolverError(st, self.last_error())
         return x, it.value, rr.value
+
+    def reduced_eliminate(self, structure_id: int, linearization_id: int, num_nodes: int,
+                          edges, point_off, point_nodes, hcp, point_inverse, extra=(),
+                          run_edges=(), coarse=None):
+        """ReducedSolveAccelerator::eliminate (PointElimination,
+        pipelines/slam/src/ba_accel.rs:74-130): edges (e,2) sorted (s, t),
+        point_off (P+1), point_nodes, hcp (K,6,3) per (point, node),
+        point_inverse a list of (3,3) damped point inverses or None (point
+        left out), extra a list of (edge, (6,6) block), run_edges, coarse
+        (nodes per aggregate, leading nodes covered) or None.  The blocks stay
+        on the device for reduced_solve(..., offdiag=None).  Returns
+        (run_blocks (len(run_edges),6,6), coarse_sums (m*m,6,6) or None);
+        a non-finite block raises SolverError with status DECLINED."""
+        import numpy as np
+
+        edges = np.ascontiguousarray(np.asarray(edges, np.uint32).reshape(-1, 2))
+        point_off = np.ascontiguousarray(np.asarray(point_off, np.uint64))
+        point_nodes = np.ascontiguousarray(np.asarray(point_nodes, np.uint32))
+        hcp = np.ascontiguousarray(np.asarray(hcp, np.float64).reshape(-1, 6, 3).transpose(0, 2, 1))
+        npts = len(point_off) - 1
+        used = np.ascontiguousarray([v is not None for v in point_inverse], np.uint8)
+        vinv = np.zeros((npts, 3, 3))
+        for p, v in enumerate(point_inverse):
+            if v is not None:
+                vinv[p] = np.asarray(v, np.float64).T  # column-major
+        vinv = np.ascontiguousarray(vinv)
+        ex_edge = np.ascontiguousarray([int(e) for e, _ in extra], np.uint32)
+        ex_blk = np.ascontiguousarray(
+            np.array([np.asarray(b, np.float64).T for _, b in extra]).reshape(-1, 36))
+        run_edges = np.ascontiguousarray(np.asarray(run_edges, np.uint32).reshape(-1))
+        el = _abi.PointElimination()
+        el.structure_id = int(structure_id)
+        el.linearization_id = int(linearization_id)
+        el.num_nodes = int(num_nodes)
+        el.num_points = npts
+        el.num_edges = edges.shape[0]
+        el.edges = edges.ctypes.data_as(C.POINTER(C.c_uint32))
+        el.point_off = point_off.ctypes.data_as(C.POINTER(C.c_uint64))
+        el.point_nodes = point_nodes.ctypes.data_as(C.POINTER(C.c_uint32))
+        el.hcp = hcp.ctypes.data_as(C.POINTER(C.c_double))
+        el.point_inverse = vinv.ctypes.data_as(C.POINTER(C.c_double))
+        el.point_used = used.ctypes.data_as(C.POINTER(C.c_uint8))
+        el.num_extra = len(ex_edge)
+        el.extra_edge = ex_edge.ctypes.data_as(C.POINTER(C.c_uint32))
+        el.extra_block = ex_blk.ctypes.data_as(C.POINTER(C.c_double))
+        el.num_run_edges = len(run_edges)
+        el.run_edges = run_edges.ctypes.data_as(C.POINTER(C.c_uint32))
+        m = 0
+        if coarse is not None:
+            el.coarse_group, el.coarse_nodes = int(coarse[0]), int(coarse[1])
+            m = -(-int(coarse[1]) // int(coarse[0])) if int(coarse[0]) > 0 else 0
+        run_out = np.zeros((len(run_edges), 36))
+        sums = np.zeros((m * m, 36)) if m else None
+        st = self.lib.visloc_ba_cuda_reduced_eliminate(
+            self.ctx, C.byref(el), run_out.ctypes.data_as(C.POINTER(C.c_double)),
+            sums.ctypes.data_as(C.POINTER(C.c_double)) if sums is not None
+            else C.POINTER(C.c_double)())
+        if st != _abi.OK:
+            raise SolverError(st, self.last_error())
+        unpack = lambda a: a.reshape(-1, 6, 6).transpose(0, 2, 1).copy()  # noqa: E731
+        return unpack(run_out), (unpack(sums) if sums is not None else None)
 
     def wait_probe(self, limit_ms: float):
         """(status, waited ms) of the bounded-wait self-test."""
