@@ -63,7 +63,8 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="ring-4m",
-                    choices=["ring-4m", "ring-50", "street-20m", "windows-512", "served"])
+                    choices=["ring-4m", "ring-50", "street-20m", "windows-512", "served",
+                             "reduced-5822"])
     ap.add_argument("--requests", type=int, default=300, help="served: stream length")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -710,11 +711,168 @@ def run_served(args, dist: Dist):
         print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------ reduced camera system path
+REDUCED_NODES = 5822  # SmallCity's photos
+
+
+def reduced_tiles(edges, n, tb=8):
+    """Tiles of S in the device layout: the tile pairs (I <= J) that hold an
+    edge, plus the diagonal tiles."""
+    import numpy as np
+
+    ti = edges[:, 0].astype(np.int64) // tb
+    tj = edges[:, 1].astype(np.int64) // tb
+    rows = -(-n // tb)
+    return int(np.unique(np.concatenate([ti * rows + tj, np.arange(rows) * (rows + 1)])).size)
+
+
+def reduced_cpu_iteration_ms(diag, edges, off, rhs, runs, coarse, iters=3):
+    """The oracle's FP64 numpy iteration (pcg_core's restatement) with the same
+    preconditioner: ms per PCG iteration over `iters` iterations, one core."""
+    from oracle import oracle
+
+    t0 = time.perf_counter()
+    oracle.reduced_pcg(diag, edges, off, rhs, 0.0, iters, clusters=runs, coarse=coarse)
+    return 1e3 * (time.perf_counter() - t0) / iters
+
+
+def run_reduced(args, dist: Dist):
+    """ReducedSolveAccelerator at SmallCity size (5,822 nodes): the
+    preconditioned PCG (runs of 32, coarse level of 32-node aggregates) and
+    block-Jacobi on a 3.4M-edge covisibility system given with its blocks:
+    ms per PCG iteration from the device times of the PCG loop (CUDA events
+    on the library's stream) of a 1e-6 solve and of a one-iteration solve, the
+    C call's fixed cost beside it; and the point elimination of
+    a street capture of 14.5M observations (first call with the structure's
+    index, then per trial), followed by the preconditioned solve on the
+    resident blocks.  Replicas at N > 1."""
+    import numpy as np
+
+    from visloc_ba import reduced, synth
+    from visloc_ba.solver import CudaSolver
+
+    if args.impl == "reference" and dist.rank != 0:
+        return
+    n = REDUCED_NODES
+    diag, edges, off = synth.covisibility_system(n, 450, 150)
+    rhs = np.random.default_rng(7 + dist.rank).standard_normal((n, 6))
+    runs = reduced.cluster_inverses(diag, edges, off, 32)
+    coarse = reduced.coarse_correction(diag, edges, off, n, 32)
+    desc = {"workload": "reduced-5822", "nodes": n, "edges": int(len(edges)),
+            "system": "covisibility: +-450 capture-order neighbours, 150 cross-pass",
+            "runs": 32, "coarse_group": int(coarse[0]), "coarse_aggregates": -(-n // coarse[0]),
+            "tiles": reduced_tiles(edges, n)}
+    if args.impl == "reference":
+        ms = reduced_cpu_iteration_ms(diag, edges, off, rhs, runs, coarse)
+        line = {"impl": "reference", "metric": "reduced_pcg_iteration_ms", "value": ms,
+                "unit": "ms", "n_gpus": args.gpus, "steps": 1, "warmup": 0, "ms_per_step": ms,
+                "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64", "data": "synthetic", "config": desc,
+                "cpu_baseline": {"value": ms, "unit": "ms", "cores": 1, "kind": "port",
+                                 "sample": "3 iterations of the FP64 numpy restatement"},
+                "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+    import torch
+
+    torch.cuda.set_device(dist.local)
+    solver = CudaSolver(dist.local)
+    clocks = Clocks(dist.local)
+
+    def solve(**kw):
+        """(iterations, device ms per PCG iteration, C-call ms) of a 1e-6
+        solve: the device time of its PCG loop less that of a one-iteration
+        solve (the loop's setup, the preconditioner's first application and
+        the graph's instantiation), over the iterations past the first."""
+        solver.reduced_solve(diag, edges, off, rhs, 1e-6, 1, **kw)
+        one = solver.reduced_timing()["pcg_ms"]
+        _, it, _ = solver.reduced_solve(diag, edges, off, rhs, 1e-6, 2000, **kw)
+        per = (solver.reduced_timing()["pcg_ms"] - one) / max(1, it - 1)
+        return it, per, solver.last_call_ms
+
+    for _ in range(args.warmup):
+        solve(clusters=runs, coarse=coarse)
+        solve()
+    dist.barrier()
+    clocks.start()
+    pre = [solve(clusters=runs, coarse=coarse) for _ in range(max(1, args.steps))]
+    bj = [solve() for _ in range(max(1, args.steps))]
+    clk = clocks.stop()
+    conv_pre, conv_bj = pre[0][0], bj[0][0]
+    it_pre = dist.max(float(np.median([p[1] for p in pre])))
+    it_bj = dist.max(float(np.median([b[1] for b in bj])))
+    call_pre = float(np.median([p[2] for p in pre]))
+    fixed = dist.max(call_pre - conv_pre * it_pre)
+    # Algorithmic bytes per preconditioned iteration: S's tiles once, the run
+    # inverses and the coarse inverse (FP32), about 40 vector passes.
+    m = -(-n // coarse[0])
+    b_iter = (desc["tiles"] * 64 * 144 + sum(4 * r.shape[0] ** 2 for _, r in runs)
+              + 4 * (6 * m) ** 2 + 40 * 24 * n)
+    peak, kind = hbm_peak()
+    achieved = b_iter / (it_pre * 1e-3) / 1e9
+    # Elimination of a street capture.
+    el = synth.street_elimination(n, 2500, seed=11 + dist.rank)
+    pl = el["point_off"][1:] - el["point_off"][:-1]
+    pairs = int((pl * (pl - 1) // 2).sum())
+    e2 = el["edges"]
+    in_run = np.flatnonzero(e2[:, 0] // 32 == e2[:, 1] // 32).astype(np.uint32)
+    group = reduced.coarse_group_size(n, 32)
+    args_el = (n, e2, el["point_off"], el["point_nodes"], el["hcp"])
+    solver.reduced_eliminate(1, 1, *args_el, el["point_inverse"], (), in_run, (group, n))
+    first_ms = solver.last_call_ms
+    trial, trial_dev = [], []
+    for k in range(max(2, args.steps)):
+        rb, sums = solver.reduced_eliminate(1, 1, *args_el, el["point_inverse"] * (1.0 - 0.01 * k),
+                                            (), in_run, (group, n))
+        trial.append(solver.last_call_ms)
+        trial_dev.append(solver.reduced_timing()["eliminate_ms"])
+    el_runs = reduced.cluster_inverses(el["diag"], e2[in_run], rb, 32)
+    el_coarse = reduced.coarse_from_sums(el["diag"], sums, n, group)
+    _, el_iters, el_rr = solver.reduced_solve(el["diag"], e2, None, el["rhs"], 1e-6, 500,
+                                              clusters=el_runs, coarse=el_coarse)
+    el_solve_ms = solver.last_call_ms
+    el_pcg_ms = solver.reduced_timing()["pcg_ms"]
+    if dist.rank != 0:
+        return
+    line = {
+        "metric": "reduced_pcg_iteration_ms", "value": it_pre, "unit": "ms",
+        "n_gpus": dist.world, "steps": max(1, args.steps), "warmup": args.warmup,
+        "ms_per_step": it_pre, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": 3.4 / it_pre, "dtype": "f32 vectors and S, f64 dots",
+        "data": "synthetic", "config": desc, "clocks": clk,
+        "block_jacobi_iteration_ms": it_bj, "fixed_cost_ms": fixed,
+        "solve_to_1e-6": {"preconditioned": {"iterations": conv_pre, "call_ms": call_pre},
+                          "block_jacobi": {"iterations": conv_bj,
+                                           "call_ms": float(np.median([b[2] for b in bj]))}},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None, "peak_kind": kind,
+                     "algorithmic_bytes_per_iteration": b_iter},
+        "elimination": {"observations": int(len(el["point_nodes"])), "points": int(len(pl)),
+                        "edges": int(len(e2)), "pairs": pairs, "first_call_ms": first_ms,
+                        "per_trial_ms": float(np.median(trial)),
+                        "per_trial_device_ms": float(np.median(trial_dev)),
+                        "solve_on_resident_blocks": {"iterations": el_iters,
+                                                     "relative_residual": el_rr,
+                                                     "call_ms": el_solve_ms,
+                                                     "pcg_device_ms": el_pcg_ms}},
+        "reference_l4": {"pcg_iteration_ms_3.4M_edges": 3.4, "per_solve_fixed_cost_ms": 590,
+                         "elimination_per_trial_ms": 1440},
+    }
+    if not args.no_cpu_baseline:
+        cpu = reduced_cpu_iteration_ms(diag, edges, off, rhs, runs, coarse)
+        line["cpu_baseline"] = {"value": cpu, "unit": "ms", "cores": 1, "kind": "port",
+                                "sample": "3 iterations of the FP64 numpy restatement"}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse_args()
     dist = Dist()
     try:
-        if args.impl == "reference":
+        if args.workload == "reduced-5822":
+            run_reduced(args, dist)
+        elif args.impl == "reference":
             run_reference(args, dist)
         elif args.workload == "windows-512":
             run_batch(args, dist)

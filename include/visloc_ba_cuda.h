@@ -472,6 +472,21 @@ int visloc_ba_cuda_reduced_eliminate(void* ctx, const vlba_point_elimination* el
                                      double* run_blocks /* [36 num_run_edges] */,
                                      double* coarse_sums /* [36 m m] or NULL without coarse */);
 
+/* Device times of the context's last reduced solve and elimination, from
+ * CUDA events on its stream: fill_ms the system's host-to-device copies and
+ * the fill of S's tiles, pcg_ms the PCG loop (with the host's checks between
+ * launches of the preconditioned loop), eliminate_ms the elimination's
+ * uploads of this call and its kernels.  Diagnostics for measurement; no
+ * counterpart in the reference. */
+typedef struct vlba_reduced_timing {
+  double fill_ms;
+  double pcg_ms;
+  double eliminate_ms;
+  double reserved;
+} vlba_reduced_timing;
+
+int visloc_ba_cuda_reduced_timing(void* ctx, vlba_reduced_timing* out);
+
 /* --------------------------------------------------------------- autotuner */
 /* Launch shape of the uploaded system: the blocks of the persistent PCG
  * kernel and the share of the L2 that keeps tiles of S resident across PCG

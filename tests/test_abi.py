@@ -45,6 +45,7 @@ def test_struct_sizes_match_the_header_layout():
     assert C.sizeof(_abi.Iteration) == 8 + 5 * 8 + 8 + 8 + 4 * 8
     assert C.sizeof(_abi.ReducedSystem) == 8 + 8 + 4 * 8 + 8 + 8
     assert C.sizeof(_abi.ReducedPreconditioner) == 8 + 3 * 8 + 8 + 8
+    assert C.sizeof(_abi.ReducedTiming) == 4 * 8
     assert C.sizeof(_abi.PointElimination) == 8 + 8 + 8 + 8 + 6 * 8 + 8 + 2 * 8 + 8 + 8 + 8
 
 

@@ -57,25 +57,76 @@ __global__ void k_rp_init_xr(Dev d, RpData rp) {
   if (lane == 0) rp.dots[2 * (size_t)d.num_tile_rows + R] = bb;
 }
 
+// 16-byte asynchronous global -> shared copies (LDGSTS), committed as groups.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned a = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(a), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+constexpr int kTileFloats = 64 * kBlock;   // 8 x 8 blocks of 36 floats
+constexpr int kMatvecWarps = 4;            // warps per block, each with a 2-tile ring
+constexpr size_t kMatvecSmem = (size_t)kMatvecWarps * 2 * kTileFloats * sizeof(float);
+
 // One warp per tile: the row-side partial S_IJ p_J and, off the diagonal,
 // the column-side partial S_IJ^T p_I into the tile's partial slots (as the
-// persistent PCG kernel does, from global memory instead of a TMA ring).
-__global__ void k_rp_matvec(Dev d, RpData rp) {
+// persistent PCG kernel does).  Each warp streams its tiles through a
+// two-stage shared-memory ring: coalesced 16-byte copies of the next tile
+// in flight while it multiplies the current one; lane l reads blocks l and
+// l + 32 as float4 at a 144-byte stride, free of bank conflicts within each
+// quarter warp.
+__global__ void __launch_bounds__(kMatvecWarps * 32) k_rp_matvec(Dev d, RpData rp) {
   if (rp_done(rp)) return;
-  const uint32_t lane = threadIdx.x & 31u;
-  const uint32_t nw = gridDim.x * blockDim.x / 32u;
+  extern __shared__ __align__(16) float rp_smem[];
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  float* ring = rp_smem + (size_t)warp * 2 * kTileFloats;
+  const uint32_t nw = gridDim.x * kMatvecWarps;
   const int li = (int)(lane >> 3), lj = (int)(lane & 7);
-  for (uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) / 32u; t < d.num_tiles; t += nw) {
+  auto issue = [&](uint32_t tile, int stage) {
+    const float4* src = reinterpret_cast<const float4*>(d.tiles + (size_t)tile * kTileFloats);
+    float* dst = ring + stage * kTileFloats;
+#pragma unroll
+    for (int k = 0; k < kTileFloats / 4 / 32; ++k)
+      cp_async16(dst + 4 * (k * 32 + lane), src + k * 32 + lane);
+    cp_async_commit();
+  };
+  uint32_t t = blockIdx.x * kMatvecWarps + warp;
+  int st = 0;
+  if (t < d.num_tiles) issue(t, 0);
+  for (; t < d.num_tiles; t += nw) {
+    const uint32_t tn = t + nw;
+    if (tn < d.num_tiles) {
+      issue(tn, st ^ 1);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncwarp();  // every lane's copies of this tile have landed
     const uint4 meta = reinterpret_cast<const uint4*>(d.tile_meta)[t];
     const uint32_t I = meta.x >> 16, J = meta.x & 0xFFFFu;
-    const float* tile = d.tiles + (size_t)t * 64 * kBlock;
+    const float* tile = ring + st * kTileFloats;
     float pj[6];
 #pragma unroll
     for (int c = 0; c < 6; ++c) pj[c] = d.p[(size_t)J * kRow + lj * 6 + c];
     float row[2][6], col[6] = {0, 0, 0, 0, 0, 0};
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
-      const float* blk = tile + (size_t)(lane + 32 * h) * kBlock;
+      const float4* blk = reinterpret_cast<const float4*>(tile + (size_t)(lane + 32 * h) * kBlock);
+      float sv[36];
+#pragma unroll
+      for (int q = 0; q < 9; ++q) {
+        const float4 v = blk[q];
+        sv[4 * q] = v.x;
+        sv[4 * q + 1] = v.y;
+        sv[4 * q + 2] = v.z;
+        sv[4 * q + 3] = v.w;
+      }
       float pi[6];
 #pragma unroll
       for (int a = 0; a < 6; ++a) pi[a] = d.p[(size_t)I * kRow + (li + 4 * h) * 6 + a];
@@ -83,17 +134,18 @@ __global__ void k_rp_matvec(Dev d, RpData rp) {
       for (int a = 0; a < 6; ++a) {
         float acc = 0.0f;
 #pragma unroll
-        for (int c = 0; c < 6; ++c) acc += blk[a * 6 + c] * pj[c];
+        for (int c = 0; c < 6; ++c) acc += sv[a * 6 + c] * pj[c];
         row[h][a] = acc;
       }
 #pragma unroll
       for (int c = 0; c < 6; ++c) {
         float acc = 0.0f;
 #pragma unroll
-        for (int a = 0; a < 6; ++a) acc += blk[a * 6 + c] * pi[a];
+        for (int a = 0; a < 6; ++a) acc += sv[a * 6 + c] * pi[a];
         col[c] += acc;
       }
     }
+    __syncwarp();  // the stage is read: the next issue may overwrite it
 #pragma unroll
     for (int off = 4; off > 0; off >>= 1)
 #pragma unroll
@@ -118,6 +170,7 @@ __global__ void k_rp_matvec(Dev d, RpData rp) {
         for (int c = 0; c < 6; ++c) part[lj * 6 + c] = col[c];
       }
     }
+    st ^= 1;
   }
 }
 
@@ -441,11 +494,9 @@ void precondition(const Dev& d, const RpData& rp, cudaStream_t s) {
 }  // namespace
 
 cudaError_t launch_rp_init(const Dev& d, const RpData& rp, cudaStream_t s) {
-  if (rp.max_cluster_rows * 4 > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(k_rp_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)(rp.max_cluster_rows * 4));
-    if (e != cudaSuccess) return e;
-  }
+  cudaError_t e = cudaFuncSetAttribute(k_rp_matvec, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)kMatvecSmem);
+  if (e != cudaSuccess) return e;
   k_rp_init_xr<<<rows_grid(d), 256, 0, s>>>(d, rp);
   precondition(d, rp, s);
   k_rp_scalars<<<1, 32, 0, s>>>(d, rp, kRpInit);
@@ -454,8 +505,10 @@ cudaError_t launch_rp_init(const Dev& d, const RpData& rp, cudaStream_t s) {
 }
 
 cudaError_t launch_rp_iteration(const Dev& d, const RpData& rp, cudaStream_t s) {
-  const int tiles_grid = (int)std::min<uint32_t>((d.num_tiles + 7) / 8, 148 * 16);
-  k_rp_matvec<<<std::max(1, tiles_grid), 256, 0, s>>>(d, rp);
+  // Three blocks per SM (their rings take 3 x 72 KB of shared memory).
+  const int tiles_grid =
+      (int)std::min<uint32_t>((d.num_tiles + kMatvecWarps - 1) / kMatvecWarps, 148 * 3);
+  k_rp_matvec<<<std::max(1, tiles_grid), kMatvecWarps * 32, kMatvecSmem, s>>>(d, rp);
   k_rp_rowsum<<<rows_grid(d), 256, 0, s>>>(d, rp);
   k_rp_scalars<<<1, 32, 0, s>>>(d, rp, kRpAlpha);
   k_rp_update_xr<<<rows_grid(d), 256, 0, s>>>(d, rp);

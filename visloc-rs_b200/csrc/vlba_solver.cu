@@ -222,6 +222,17 @@ struct Context {
   size_t gnc_cap = 0;
   // The last point elimination (ReducedSolveAccelerator::eliminate).
   std::unique_ptr<ElimState> elim;
+  // Device times of the last reduced solve and elimination.
+  vlba_reduced_timing reduced_ms{};
+  // Uploads of a plan (any entry point); the reduced system's layout is
+  // reused while no other plan replaced it and its edges stay the same.
+  uint64_t plan_generation = 0;
+  uint64_t reduced_generation = ~0ull;
+  std::vector<uint32_t> reduced_edges;
+  uint32_t reduced_nodes = 0;
+  // The reduced system's diagonal, rhs and blocks as copied from the caller,
+  // and the preconditioner of a preconditioned solve.
+  DeviceArray reduced_in, reduced_pre;
 };
 
 namespace {
@@ -554,6 +565,7 @@ void upload_plan_once(Context* c, uint32_t max_records) {
 }
 
 void upload_plan(Context* c, uint32_t max_records) {
+  ++c->plan_generation;
   const size_t est = c->plan.device_bytes() + (size_t)max_records * sizeof(vlba_iteration) *
                                                    c->plan.num_problems + (4u << 20);
   if (c->arena.growable()) c->arena.reserve(std::max(est, c->arena.capacity()));
@@ -1001,6 +1013,7 @@ void do_upload(Context* c, const vlba_problem* const* probs, const vlba_config* 
       throw Status(vs[i].status, "problem " + std::to_string(i) + " failed validation",
                    vs[i].error_index);
   set_device(c);
+  c->reduced_generation = ~0ull;  // the host plan no longer matches the reduced layout
   build_plan(probs, cfgs, n, (uint32_t)pick_tb(probs, n), &c->plan);
   const std::string bad = check_plan(c->plan);
   if (!bad.empty()) throw Status(VLBA_ERR_INVALID_ARGUMENT, bad);
@@ -1617,6 +1630,7 @@ int visloc_ba_cuda_cost(void* ctx, const vlba_problem* problem, const vlba_confi
     if (v.status != VLBA_OK && v.status != VLBA_ERR_ALL_POSES_FIXED)
       throw vlba::Status(v.status, "validation", v.error_index);
     vlba::set_device(c);
+    c->reduced_generation = ~0ull;
     vlba::build_plan(probs, cfgs, 1, 8, &c->plan);
     const std::string bad = vlba::check_plan(c->plan);
     if (!bad.empty()) throw vlba::Status(VLBA_ERR_INVALID_ARGUMENT, bad);
@@ -1791,6 +1805,7 @@ void run_batch(Server* S, uint32_t k, const std::vector<Ticket*>& batch) {
       records = std::max(records, t->config.max_iterations);
       flags |= t->config.flags;
     }
+    c->reduced_generation = ~0ull;
     if (parts.size() == 1) c->plan = std::move(batch[0]->plan);
     else merge_plans(parts, &c->plan);
     upload_plan(c, records);
@@ -1996,27 +2011,60 @@ void reduced_setup(Context* c, const vlba_reduced_system* sys) {
   cfg.max_pcg_iterations = sys->max_iterations;
   cfg.pcg_relative_tolerance = sys->tol;
   const LmParams lp = make_params(&cfg);
-  build_reduced_plan(sys->num_nodes, sys->edges, sys->num_edges, 8, lp, &c->plan);
-  const std::string bad = check_plan(c->plan);
-  if (!bad.empty()) throw Status(VLBA_ERR_INVALID_ARGUMENT, bad);
-  upload_plan(c, 1);
-  cudaStream_t s = c->stream;
   const size_t n = sys->num_nodes, ne = sys->num_edges;
-  DeviceArray diag, off, rhs;  // the caller's arrays, staged for the fill kernel
-  diag.alloc(36 * n * 8);
-  rhs.alloc(6 * n * 8);
-  if (ne && !resident) off.alloc(36 * ne * 4);
-  VLBA_CUDA(cudaMemcpyAsync(diag.p, sys->diag, 36 * n * 8, cudaMemcpyHostToDevice, s));
-  VLBA_CUDA(cudaMemcpyAsync(rhs.p, sys->rhs, 6 * n * 8, cudaMemcpyHostToDevice, s));
-  if (ne && !resident)
-    VLBA_CUDA(cudaMemcpyAsync(off.p, sys->offdiag, 36 * ne * 4, cudaMemcpyHostToDevice, s));
+  cudaStream_t s = c->stream;
+  // The layout (tiles, block destinations, PCG lists) depends on the edges
+  // only: rebuilt when they change or another upload replaced it.
+  const bool same = c->reduced_generation == c->plan_generation && c->reduced_nodes == n &&
+                    c->reduced_edges.size() == 2 * ne &&
+                    (ne == 0 || std::memcmp(c->reduced_edges.data(), sys->edges, 8 * ne) == 0);
+  if (!same) {
+    c->reduced_generation = ~0ull;
+    build_reduced_plan(sys->num_nodes, sys->edges, sys->num_edges, 8, lp, &c->plan);
+    const std::string bad = check_plan(c->plan);
+    if (!bad.empty()) throw Status(VLBA_ERR_INVALID_ARGUMENT, bad);
+    upload_plan(c, 1);
+    c->reduced_edges.assign(sys->edges, sys->edges + 2 * ne);
+    c->reduced_nodes = (uint32_t)n;
+    c->reduced_generation = c->plan_generation;
+  } else {
+    c->plan.params[0] = lp;  // this call's tolerance and iteration cap
+    VLBA_CUDA(cudaMemcpyAsync(const_cast<LmParams*>(c->dev.params), &c->plan.params[0],
+                              sizeof(LmParams), cudaMemcpyHostToDevice, s));
+  }
+  // The caller's arrays, staged for the fill kernel through pinned memory.
+  const size_t b_diag = 288 * n, b_rhs = 48 * n, b_off = resident ? 0 : 144 * ne;
+  c->reduced_in.ensure(b_diag + b_rhs + b_off);
+  char* in = c->reduced_in.as<char>();
+  VLBA_CUDA(cudaEventRecord(c->ev[0], s));
+  {
+    Stager st(c);
+    st.add(in, sys->diag, b_diag);
+    st.add(in + b_diag, sys->rhs, b_rhs);
+    if (b_off) st.add(in + b_diag + b_rhs, sys->offdiag, b_off);
+    st.flush(s);
+  }
   reset_state(c);
-  check_launch(launch_reduced_fill(c->dev, (uint32_t)n, ne, diag.as<const double>(),
-                                   ne && !resident ? off.as<const float>() : nullptr,
+  check_launch(launch_reduced_fill(c->dev, (uint32_t)n, ne, reinterpret_cast<const double*>(in),
+                                   b_off ? reinterpret_cast<const float*>(in + b_diag + b_rhs)
+                                         : nullptr,
                                    resident ? c->elim->blocks.as<const double>() : nullptr,
-                                   rhs.as<const double>(), s),
+                                   reinterpret_cast<const double*>(in + b_diag), s),
                "reduced fill");
+  VLBA_CUDA(cudaEventRecord(c->ev[1], s));
   VLBA_CUDA(cudaStreamSynchronize(s));
+  float ms = 0.0f;
+  VLBA_CUDA(cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]));
+  c->reduced_ms.fill_ms = ms;
+}
+
+// Device time from ev[2] (recorded at the PCG loop's start) to now.
+void record_pcg_ms(Context* c) {
+  VLBA_CUDA(cudaEventRecord(c->ev[3], c->stream));
+  VLBA_CUDA(cudaEventSynchronize(c->ev[3]));
+  float ms = 0.0f;
+  VLBA_CUDA(cudaEventElapsedTime(&ms, c->ev[2], c->ev[3]));
+  c->reduced_ms.pcg_ms = ms;
 }
 
 void download_step(Context* c, size_t n, double* x) {
@@ -2086,9 +2134,8 @@ void reduced_solve_preconditioned(Context* c, const vlba_reduced_system* sys,
                  o_off = o_size + up16(4ull * nc), o_mat = o_off + up16(8ull * nc),
                  o_cinv = o_mat + up16(4 * cl_floats), o_rc = o_cinv + up16(4 * cm * cm),
                  o_yc = o_rc + up16(4 * cm), total = o_yc + up16(4 * cm);
-  DeviceArray buf;
-  buf.alloc(total);
-  char* base = buf.as<char>();
+  c->reduced_pre.ensure(total);
+  char* base = c->reduced_pre.as<char>();
   {
     std::vector<float> mat(cl_floats), cinv(cm * cm);
     if (nc) {
@@ -2136,6 +2183,7 @@ void reduced_solve_preconditioned(Context* c, const vlba_reduced_system* sys,
   rp.max_iterations = sys->max_iterations;
   rp.tol = sys->tol;
 
+  VLBA_CUDA(cudaEventRecord(c->ev[2], s));
   check_launch(launch_rp_init(d, rp, s), "preconditioned solve init");
   // kRpChunk iterations as one graph, launched until the device says done.
   struct Graph {
@@ -2160,6 +2208,7 @@ void reduced_solve_preconditioned(Context* c, const vlba_reduced_system* sys,
     if (sc.done || launched >= sys->max_iterations) break;
     VLBA_CUDA(cudaGraphLaunch(gr.e, s));
   }
+  record_pcg_ms(c);
   if (sc.failed)
     throw Status(VLBA_DECLINED, "p.q not positive and finite at iteration " +
                                     std::to_string(sc.iters + 1) + ": the CPU solver takes the system");
@@ -2221,6 +2270,7 @@ bool reduced_eliminate(Context* c, const vlba_point_elimination* el, double* run
   // Per call: the point inverses, the couplings (merged per edge in their
   // order), the run edges and the outputs.
   E.vinv64.ensure(72ull * P);
+  VLBA_CUDA(cudaEventRecord(c->ev[4], s));
   VLBA_CUDA(cudaMemcpyAsync(E.vinv64.p, el->point_inverse, 72ull * P, cudaMemcpyHostToDevice, s));
   if (el->point_used) {
     E.used.ensure(P);
@@ -2287,11 +2337,17 @@ bool reduced_eliminate(Context* c, const vlba_point_elimination* el, double* run
   check_launch(launch_el_prepare(d, s), "elimination prepare");
   check_launch(launch_el_blocks(d, s), "elimination blocks");
   check_launch(launch_el_outputs(d, s), "elimination outputs");
+  VLBA_CUDA(cudaEventRecord(c->ev[5], s));
   if (nrun)
     VLBA_CUDA(cudaMemcpyAsync(run_blocks, E.run_out.p, 288 * nrun, cudaMemcpyDeviceToHost, s));
   if (m && coarse_sums)
     VLBA_CUDA(cudaMemcpyAsync(coarse_sums, E.coarse_out.p, 8 * nsum, cudaMemcpyDeviceToHost, s));
   VLBA_CUDA(cudaStreamSynchronize(s));
+  {
+    float ms = 0.0f;
+    VLBA_CUDA(cudaEventElapsedTime(&ms, c->ev[4], c->ev[5]));
+    c->reduced_ms.eliminate_ms = ms;
+  }
   for (uint64_t i = 0; i < 36 * nrun; ++i)
     if (!std::isfinite(run_blocks[i])) return false;
   if (m && coarse_sums)
@@ -2314,8 +2370,10 @@ int visloc_ba_cuda_reduced_solve(void* ctx, const vlba_reduced_system* sys, doub
     vlba::reduced_setup(c, sys);
     cudaStream_t s = c->stream;
     vlba::Dev& d = c->dev;
+    VLBA_CUDA(cudaEventRecord(c->ev[2], s));
     vlba::check_launch(vlba::launch_pcg_setup(d, s), "pcg setup");
     vlba::check_launch(vlba::launch_pcg(d, c->pcg_grid, s), "pcg");
+    vlba::record_pcg_ms(c);
     vlba::PcgState pg;
     VLBA_CUDA(cudaMemcpyAsync(&pg, d.pcg, sizeof pg, cudaMemcpyDeviceToHost, s));
     unsigned int err = 0;
@@ -2373,6 +2431,13 @@ int visloc_ba_cuda_reduced_eliminate(void* ctx, const vlba_point_elimination* el
     if (!vlba::reduced_eliminate(c, el, run_blocks, coarse_sums))
       throw vlba::Status(VLBA_DECLINED, "an eliminated block is not finite");
   });
+}
+
+int visloc_ba_cuda_reduced_timing(void* ctx, vlba_reduced_timing* out) {
+  auto* c = static_cast<Context*>(ctx);
+  if (!c || !out) return VLBA_ERR_INVALID_ARGUMENT;
+  *out = c->reduced_ms;
+  return VLBA_OK;
 }
 
 int visloc_ba_cuda_wait_probe(void* ctx, double limit_ms, double* waited_ms) {

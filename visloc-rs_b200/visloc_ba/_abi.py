@@ -226,6 +226,15 @@ class PointElimination(C.Structure):
     ]
 
 
+class ReducedTiming(C.Structure):
+    _fields_ = [
+        ("fill_ms", C.c_double),
+        ("pcg_ms", C.c_double),
+        ("eliminate_ms", C.c_double),
+        ("reserved", C.c_double),
+    ]
+
+
 class ReducedPreconditioner(C.Structure):
     _fields_ = [
         ("num_clusters", C.c_uint32),
@@ -332,6 +341,7 @@ SOLVER_EXPORTS = {
     "visloc_ba_cuda_reduced_solve": (
         C.c_int, [C.c_void_p, P(ReducedSystem), P(C.c_double), P(C.c_uint32), P(C.c_double)],
     ),
+    "visloc_ba_cuda_reduced_timing": (C.c_int, [C.c_void_p, P(ReducedTiming)]),
     "visloc_ba_cuda_reduced_eliminate": (
         C.c_int, [C.c_void_p, P(PointElimination), P(C.c_double), P(C.c_double)],
     ),

@@ -11,6 +11,7 @@ from __future__ import annotations
 import copy
 import ctypes as C
 import os
+import time
 from dataclasses import dataclass
 
 from . import _abi
@@ -165,6 +166,7 @@ class CudaSolver:
         it = C.c_uint32()
         rr = C.c_double()
         xp = x.ctypes.data_as(C.POINTER(C.c_double))
+        t0 = time.perf_counter()
         if clusters is None and coarse is None:
             st = self.lib.visloc_ba_cuda_reduced_solve(self.ctx, C.byref(sysm), xp,
                                                        C.byref(it), C.byref(rr))
@@ -198,8 +200,11 @@ class CudaSolver:
                 pre.coarse_group = int(group)
                 pre.coarse_nodes = int(nodes)
                 pre.coarse_inverse = cinv.ctypes.data_as(C.POINTER(C.c_double))
+            t0 = time.perf_counter()
             st = self.lib.visloc_ba_cuda_reduced_solve_preconditioned(
                 self.ctx, C.byref(sysm), C.byref(pre), xp, C.byref(it), C.byref(rr))
+        # Wall time of the C call alone (the conversions above excluded).
+        self.last_call_ms = (time.perf_counter() - t0) * 1e3
         if st != _abi.OK:
             raise SolverError(st, self.last_error())
         return x, it.value, rr.value
@@ -223,12 +228,16 @@ class CudaSolver:
         point_nodes = np.ascontiguousarray(np.asarray(point_nodes, np.uint32))
         hcp = np.ascontiguousarray(np.asarray(hcp, np.float64).reshape(-1, 6, 3).transpose(0, 2, 1))
         npts = len(point_off) - 1
-        used = np.ascontiguousarray([v is not None for v in point_inverse], np.uint8)
-        vinv = np.zeros((npts, 3, 3))
-        for p, v in enumerate(point_inverse):
-            if v is not None:
-                vinv[p] = np.asarray(v, np.float64).T  # column-major
-        vinv = np.ascontiguousarray(vinv)
+        if isinstance(point_inverse, np.ndarray):  # (P,3,3), every point used
+            used = np.ones(npts, np.uint8)
+            vinv = np.ascontiguousarray(np.asarray(point_inverse, np.float64).transpose(0, 2, 1))
+        else:
+            used = np.ascontiguousarray([v is not None for v in point_inverse], np.uint8)
+            vinv = np.zeros((npts, 3, 3))
+            for p, v in enumerate(point_inverse):
+                if v is not None:
+                    vinv[p] = np.asarray(v, np.float64).T  # column-major
+            vinv = np.ascontiguousarray(vinv)
         ex_edge = np.ascontiguousarray([int(e) for e, _ in extra], np.uint32)
         ex_blk = np.ascontiguousarray(
             np.array([np.asarray(b, np.float64).T for _, b in extra]).reshape(-1, 36))
@@ -256,14 +265,25 @@ class CudaSolver:
             m = -(-int(coarse[1]) // int(coarse[0])) if int(coarse[0]) > 0 else 0
         run_out = np.zeros((len(run_edges), 36))
         sums = np.zeros((m * m, 36)) if m else None
+        t0 = time.perf_counter()
         st = self.lib.visloc_ba_cuda_reduced_eliminate(
             self.ctx, C.byref(el), run_out.ctypes.data_as(C.POINTER(C.c_double)),
             sums.ctypes.data_as(C.POINTER(C.c_double)) if sums is not None
             else C.POINTER(C.c_double)())
+        self.last_call_ms = (time.perf_counter() - t0) * 1e3
         if st != _abi.OK:
             raise SolverError(st, self.last_error())
         unpack = lambda a: a.reshape(-1, 6, 6).transpose(0, 2, 1).copy()  # noqa: E731
         return unpack(run_out), (unpack(sums) if sums is not None else None)
+
+    def reduced_timing(self) -> dict:
+        """Device times (ms) of the last reduced solve and elimination:
+        fill_ms, pcg_ms, eliminate_ms."""
+        t = _abi.ReducedTiming()
+        st = self.lib.visloc_ba_cuda_reduced_timing(self.ctx, C.byref(t))
+        if st != _abi.OK:
+            raise SolverError(st, self.last_error())
+        return {"fill_ms": t.fill_ms, "pcg_ms": t.pcg_ms, "eliminate_ms": t.eliminate_ms}
 
     def wait_probe(self, limit_ms: float):
         """(status, waited ms) of the bounded-wait self-test."""

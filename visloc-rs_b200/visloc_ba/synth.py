@@ -434,3 +434,120 @@ def scene_extent(packed: PackedProblem) -> float:
     """Diagonal of the bounding box of the camera centres and points."""
     pts = np.concatenate([packed.camera_centers(), packed.landmarks], 0)
     return float(np.linalg.norm(pts.max(0) - pts.min(0)))
+
+
+# ------------------------------------------------------ reduced camera systems
+def covisibility_system(n=5822, band=450, cross=150, laplacian=False):
+    """A reduced camera system shaped like a city block revisited in four
+    passes (the shape of the reference's dense_covisibility_system test
+    fixture, rig_ba_solver.rs:5158-5196, widened to a SmallCity-sized
+    system): every node couples to its `band` capture-order neighbours on
+    each side (weight 1) and to `cross` nodes of the other passes at the same
+    place (weight 0.5); block entries ((7 r + 3 c + lo + hi) mod 11) 1e-3 w.
+    The diagonal is 10 + (i mod 5) plus node i's off-diagonal absolute row
+    sums times the identity, so the system is diagonally dominant SPD.
+    With laplacian=True the same graph carries the reference's chain_system
+    values instead (rig_ba_solver.rs:5244-5272): blocks -w I, w = 1 +
+    ((7 a + 3 b) mod 5) / 10, and the diagonal the weights' sum plus damping
+    1e-4 (1 + (i + r) mod 3), an ill-conditioned system whose solves run
+    hundreds of iterations.
+    Returns (diag (n,6,6), edges (e,2) sorted, offdiag (e,6,6) float32);
+    n=5822, band 450, cross 150 gives about 3.4M edges."""
+    q = n // 4
+    i = np.arange(n, dtype=np.int64)
+    a = np.repeat(i, band)
+    b = a + np.tile(np.arange(1, band + 1, dtype=np.int64), n)
+    keep = b < n
+    band_keys = a[keep] * n + b[keep]
+    ii = np.repeat(i, cross)
+    kk = np.tile(np.arange(cross, dtype=np.int64), n)
+    other = ((ii // q + 1 + kk % 3) % 4) * q + (ii % q + kk // 3) % q
+    lo, hi = np.minimum(ii, other), np.maximum(ii, other)
+    cross_keys = np.unique((lo * n + hi)[lo != hi])
+    keys = np.union1d(band_keys, cross_keys)
+    w = np.where(np.isin(keys, cross_keys, assume_unique=True), 0.5, 1.0).astype(np.float32)
+    lo, hi = keys // n, keys % n
+    if laplacian:
+        wl = 1.0 + ((lo * 7 + hi * 3) % 5) * 0.1
+        off = np.zeros((len(keys), 6, 6), np.float32)
+        for rr in range(6):
+            off[:, rr, rr] = -wl
+        wsum = np.bincount(lo, wl, minlength=n) + np.bincount(hi, wl, minlength=n)
+        damp = 1e-4 * (1 + (i[:, None] + np.arange(6)[None, :]) % 3)
+        diag = np.zeros((n, 6, 6))
+        diag[:, np.arange(6), np.arange(6)] = wsum[:, None] + damp
+        return diag, np.stack([lo, hi], 1).astype(np.uint32), off
+    r = np.arange(6)[:, None]
+    c = np.arange(6)[None, :]
+    off = np.empty((len(keys), 6, 6), np.float32)
+    s = (lo + hi).astype(np.int64)
+    for rr in range(6):
+        for cc in range(6):
+            off[:, rr, cc] = ((rr * 7 + cc * 3 + s) % 11) * 1e-3 * w
+    rowsum = np.abs(off).sum(axis=2).max(axis=1).astype(np.float64)
+    dom = np.bincount(lo, rowsum, minlength=n) + np.bincount(hi, rowsum, minlength=n)
+    diag = (10.0 + (i % 5) + dom)[:, None, None] * np.eye(6)
+    del r, c
+    return diag, np.stack([lo, hi], 1).astype(np.uint32), off
+
+
+def street_elimination(n=5822, obs_per_frame=2500, seed=0, chunk=1 << 20):
+    """A point elimination shaped like a long street capture (the reference's
+    street_scene benchmark, rig_ba_solver.rs:5322-5340): n frames along a
+    line, each point seen by consecutive frames with heavy-tailed track
+    lengths (95% 3-15 frames, 5% 40-120), about `obs_per_frame` observations
+    per frame.  Each observation has a random Jacobian [A (3x6) | B (3x3)];
+    hcp = A^T B, V_p = I + sum B^T B over its observations, and the damped
+    diagonal of the reduced system U - sum hcp V^-1 hcp^T, U = I + sum A^T A
+    (a Schur complement of an SPD matrix, so SPD).  Returns a dict with
+    edges, point_off, point_nodes, hcp (K,6,3), point_inverse (P,3,3), diag
+    (n,6,6) and rhs (n,6)."""
+    rng = np.random.default_rng(seed)
+    mean_len = 0.95 * 9.0 + 0.05 * 80.0
+    npts = int(n * obs_per_frame / mean_len)
+    long = rng.random(npts) < 0.05
+    length = np.where(long, rng.integers(40, 121, npts), rng.integers(3, 16, npts))
+    length = np.minimum(length, n)
+    start = rng.integers(0, n - length + 1)
+    point_off = np.zeros(npts + 1, np.uint64)
+    np.cumsum(length, out=point_off[1:])
+    nobs = int(point_off[-1])
+    pidx = np.repeat(np.arange(npts), length)
+    point_nodes = (start[pidx] + np.arange(nobs) - point_off[:-1][pidx].astype(np.int64)
+                   ).astype(np.uint32)
+    hcp = np.empty((nobs, 6, 3))
+    btb = np.empty((nobs, 3, 3))
+    ata = np.zeros((n, 6, 6))
+    for o0 in range(0, nobs, chunk):
+        o1 = min(nobs, o0 + chunk)
+        A = rng.standard_normal((o1 - o0, 3, 6))
+        B = rng.standard_normal((o1 - o0, 3, 3))
+        hcp[o0:o1] = np.einsum("oji,ojk->oik", A, B)
+        btb[o0:o1] = np.einsum("oji,ojk->oik", B, B)
+        g = np.einsum("oji,ojk->oik", A, A).reshape(-1, 36)
+        nodes = point_nodes[o0:o1]
+        for q in range(36):
+            ata.reshape(n, 36)[:, q] += np.bincount(nodes, g[:, q], minlength=n)
+    V = np.add.reduceat(btb, point_off[:-1].astype(np.int64), axis=0) + np.eye(3)
+    del btb
+    vinv = np.linalg.inv(V)
+    wvw = np.zeros((n, 36))
+    for o0 in range(0, nobs, chunk):
+        o1 = min(nobs, o0 + chunk)
+        h = hcp[o0:o1]
+        t = np.einsum("oij,ojk,olk->oil", h, vinv[pidx[o0:o1]], h).reshape(-1, 36)
+        nodes = point_nodes[o0:o1]
+        for q in range(36):
+            wvw[:, q] += np.bincount(nodes, t[:, q], minlength=n)
+    diag = ata + np.eye(6) - wvw.reshape(n, 6, 6)
+    ends = start + length - 1
+    reach = np.full(n, -1, np.int64)
+    np.maximum.at(reach, start, ends)
+    reach = np.maximum.accumulate(reach)
+    cnt = np.maximum(reach - np.arange(n), 0)
+    s = np.repeat(np.arange(n), cnt)
+    t = s + 1 + (np.arange(int(cnt.sum())) - np.repeat(np.cumsum(cnt) - cnt, cnt))
+    edges = np.stack([s, t], 1).astype(np.uint32)
+    rhs = rng.standard_normal((n, 6))
+    return {"edges": edges, "point_off": point_off, "point_nodes": point_nodes, "hcp": hcp,
+            "point_inverse": vinv, "diag": diag, "rhs": rhs}
