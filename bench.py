@@ -66,6 +66,11 @@ def parse_args():
                     choices=["ring-4m", "ring-50", "street-20m", "windows-512", "served",
                              "reduced-5822"])
     ap.add_argument("--requests", type=int, default=300, help="served: stream length")
+    ap.add_argument("--reduced-nodes", type=int, default=5822,
+                    help="reduced-5822: nodes (smaller for profiling captures)")
+    ap.add_argument("--obs-per-frame", type=int, default=2500,
+                    help="reduced-5822: observations per frame of the elimination scene")
+    ap.add_argument("--reduced-part", default="all", choices=["all", "solve", "eliminate"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
@@ -753,13 +758,15 @@ def run_reduced(args, dist: Dist):
 
     if args.impl == "reference" and dist.rank != 0:
         return
-    n = REDUCED_NODES
-    diag, edges, off = synth.covisibility_system(n, 450, 150)
+    n = args.reduced_nodes
+    band, cross = min(450, n // 8), min(150, n // 16)
+    diag, edges, off = synth.covisibility_system(n, band, cross)
     rhs = np.random.default_rng(7 + dist.rank).standard_normal((n, 6))
     runs = reduced.cluster_inverses(diag, edges, off, 32)
     coarse = reduced.coarse_correction(diag, edges, off, n, 32)
-    desc = {"workload": "reduced-5822", "nodes": n, "edges": int(len(edges)),
-            "system": "covisibility: +-450 capture-order neighbours, 150 cross-pass",
+    desc = {"workload": "reduced-5822" if n == REDUCED_NODES else f"reduced-{n}",
+            "nodes": n, "edges": int(len(edges)),
+            "system": f"covisibility: +-{band} capture-order neighbours, {cross} cross-pass",
             "runs": 32, "coarse_group": int(coarse[0]), "coarse_aggregates": -(-n // coarse[0]),
             "tiles": reduced_tiles(edges, n)}
     if args.impl == "reference":
@@ -791,13 +798,15 @@ def run_reduced(args, dist: Dist):
         per = (solver.reduced_timing()["pcg_ms"] - one) / max(1, it - 1)
         return it, per, solver.last_call_ms
 
-    for _ in range(args.warmup):
+    do_solve = args.reduced_part in ("all", "solve")
+    steps = max(1, args.steps) if do_solve else 0
+    for _ in range(args.warmup if do_solve else 0):
         solve(clusters=runs, coarse=coarse)
         solve()
     dist.barrier()
     clocks.start()
-    pre = [solve(clusters=runs, coarse=coarse) for _ in range(max(1, args.steps))]
-    bj = [solve() for _ in range(max(1, args.steps))]
+    pre = [solve(clusters=runs, coarse=coarse) for _ in range(steps)] or [(0, 0.0, 0.0)]
+    bj = [solve() for _ in range(steps)] or [(0, 0.0, 0.0)]
     clk = clocks.stop()
     conv_pre, conv_bj = pre[0][0], bj[0][0]
     it_pre = dist.max(float(np.median([p[1] for p in pre])))
@@ -810,9 +819,48 @@ def run_reduced(args, dist: Dist):
     b_iter = (desc["tiles"] * 64 * 144 + sum(4 * r.shape[0] ** 2 for _, r in runs)
               + 4 * (6 * m) ** 2 + 40 * 24 * n)
     peak, kind = hbm_peak()
-    achieved = b_iter / (it_pre * 1e-3) / 1e9
-    # Elimination of a street capture.
-    el = synth.street_elimination(n, 2500, seed=11 + dist.rank)
+    achieved = b_iter / (it_pre * 1e-3) / 1e9 if it_pre > 0 else 0.0
+    el_out = None
+    if args.reduced_part != "solve":  # elimination of a street capture
+        el = synth.street_elimination(n, args.obs_per_frame, seed=11 + dist.rank)
+        el_out = reduced_elimination(solver, el, n, args.steps)
+    if dist.rank != 0:
+        return
+    line = {
+        "metric": "reduced_pcg_iteration_ms", "value": it_pre, "unit": "ms",
+        "n_gpus": dist.world, "steps": max(1, args.steps), "warmup": args.warmup,
+        "ms_per_step": it_pre, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": 3.4 / it_pre if it_pre > 0 else None,
+        "dtype": "f32 vectors and S, f64 dots",
+        "data": "synthetic", "config": desc, "clocks": clk,
+        "block_jacobi_iteration_ms": it_bj, "fixed_cost_ms": fixed,
+        "solve_to_1e-6": {"preconditioned": {"iterations": conv_pre, "call_ms": call_pre},
+                          "block_jacobi": {"iterations": conv_bj,
+                                           "call_ms": float(np.median([b[2] for b in bj]))}},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None, "peak_kind": kind,
+                     "algorithmic_bytes_per_iteration": b_iter},
+        "elimination": el_out,
+        "reference_l4": {"pcg_iteration_ms_3.4M_edges": 3.4, "per_solve_fixed_cost_ms": 590,
+                         "elimination_per_trial_ms": 1440},
+    }
+    if not args.no_cpu_baseline and do_solve:
+        cpu = reduced_cpu_iteration_ms(diag, edges, off, rhs, runs, coarse)
+        line["cpu_baseline"] = {"value": cpu, "unit": "ms", "cores": 1, "kind": "port",
+                                "sample": "3 iterations of the FP64 numpy restatement"}
+    print(json.dumps(line), flush=True)
+
+
+def reduced_elimination(solver, el, n, steps):
+    """The elimination part of the reduced workload: the first call (the
+    structure's index and the blocks' upload), per-trial calls with new point
+    inverses (device time and C-call time), and a preconditioned solve on the
+    resident blocks with runs and a coarse level built from what the
+    elimination returned."""
+    import numpy as np
+
+    from visloc_ba import reduced
+
     pl = el["point_off"][1:] - el["point_off"][:-1]
     pairs = int((pl * (pl - 1) // 2).sum())
     e2 = el["edges"]
@@ -822,7 +870,7 @@ def run_reduced(args, dist: Dist):
     solver.reduced_eliminate(1, 1, *args_el, el["point_inverse"], (), in_run, (group, n))
     first_ms = solver.last_call_ms
     trial, trial_dev = [], []
-    for k in range(max(2, args.steps)):
+    for k in range(max(2, steps)):
         rb, sums = solver.reduced_eliminate(1, 1, *args_el, el["point_inverse"] * (1.0 - 0.01 * k),
                                             (), in_run, (group, n))
         trial.append(solver.last_call_ms)
@@ -831,39 +879,13 @@ def run_reduced(args, dist: Dist):
     el_coarse = reduced.coarse_from_sums(el["diag"], sums, n, group)
     _, el_iters, el_rr = solver.reduced_solve(el["diag"], e2, None, el["rhs"], 1e-6, 500,
                                               clusters=el_runs, coarse=el_coarse)
-    el_solve_ms = solver.last_call_ms
-    el_pcg_ms = solver.reduced_timing()["pcg_ms"]
-    if dist.rank != 0:
-        return
-    line = {
-        "metric": "reduced_pcg_iteration_ms", "value": it_pre, "unit": "ms",
-        "n_gpus": dist.world, "steps": max(1, args.steps), "warmup": args.warmup,
-        "ms_per_step": it_pre, "higher_is_better": False, "scaling": "weak",
-        "vs_baseline": 3.4 / it_pre, "dtype": "f32 vectors and S, f64 dots",
-        "data": "synthetic", "config": desc, "clocks": clk,
-        "block_jacobi_iteration_ms": it_bj, "fixed_cost_ms": fixed,
-        "solve_to_1e-6": {"preconditioned": {"iterations": conv_pre, "call_ms": call_pre},
-                          "block_jacobi": {"iterations": conv_bj,
-                                           "call_ms": float(np.median([b[2] for b in bj]))}},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None, "peak_kind": kind,
-                     "algorithmic_bytes_per_iteration": b_iter},
-        "elimination": {"observations": int(len(el["point_nodes"])), "points": int(len(pl)),
-                        "edges": int(len(e2)), "pairs": pairs, "first_call_ms": first_ms,
-                        "per_trial_ms": float(np.median(trial)),
-                        "per_trial_device_ms": float(np.median(trial_dev)),
-                        "solve_on_resident_blocks": {"iterations": el_iters,
-                                                     "relative_residual": el_rr,
-                                                     "call_ms": el_solve_ms,
-                                                     "pcg_device_ms": el_pcg_ms}},
-        "reference_l4": {"pcg_iteration_ms_3.4M_edges": 3.4, "per_solve_fixed_cost_ms": 590,
-                         "elimination_per_trial_ms": 1440},
-    }
-    if not args.no_cpu_baseline:
-        cpu = reduced_cpu_iteration_ms(diag, edges, off, rhs, runs, coarse)
-        line["cpu_baseline"] = {"value": cpu, "unit": "ms", "cores": 1, "kind": "port",
-                                "sample": "3 iterations of the FP64 numpy restatement"}
-    print(json.dumps(line), flush=True)
+    return {"observations": int(len(el["point_nodes"])), "points": int(len(pl)),
+            "edges": int(len(e2)), "pairs": pairs, "first_call_ms": first_ms,
+            "per_trial_ms": float(np.median(trial)),
+            "per_trial_device_ms": float(np.median(trial_dev)),
+            "solve_on_resident_blocks": {"iterations": el_iters, "relative_residual": el_rr,
+                                         "call_ms": solver.last_call_ms,
+                                         "pcg_device_ms": solver.reduced_timing()["pcg_ms"]}}
 
 
 def main():

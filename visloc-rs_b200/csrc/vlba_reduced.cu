@@ -358,85 +358,82 @@ __global__ void k_rp_scalars(Dev d, RpData rp, int step) {
 // ---------------------------------------------------------------- elimination
 // Per camera-point block o of point p: an FP32 copy of hcp and sk = hcp V_p^-1
 // (formed in FP64; zero for a point left out, whose pairs then add zero).
+// One thread per entry q = 6 i + r of the 6x3 outputs, so that consecutive
+// threads read and write consecutive addresses (the three hcp entries an
+// output needs come from the same 144-byte block, through L1).
 __global__ void k_el_prepare(ElimDev E) {
-  for (uint64_t o = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; o < E.num_obs;
-       o += (uint64_t)gridDim.x * blockDim.x) {
+  const uint64_t n = 18 * E.num_obs;
+  for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n;
+       j += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t o = j / 18;
+    const int q = (int)(j - 18 * o), i = q / 6, r = q - 6 * i;
     const uint32_t p = E.obs_point[o];
     const double* h = E.hcp64 + 18 * o;
     const double* v = E.vinv64 + 9 * (size_t)p;
     const bool used = !E.used || E.used[p];
-    double hv[18];
-#pragma unroll
-    for (int q = 0; q < 18; ++q) hv[q] = h[q];
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-      for (int r = 0; r < 6; ++r) {
-        const double sk = hv[r] * v[3 * i] + hv[6 + r] * v[3 * i + 1] + hv[12 + r] * v[3 * i + 2];
-        E.sk32[18 * o + 6 * i + r] = used ? (float)sk : 0.0f;
-      }
-#pragma unroll
-    for (int q = 0; q < 18; ++q) E.hcp32[18 * o + q] = (float)hv[q];
+    const double sk = h[r] * v[3 * i] + h[6 + r] * v[3 * i + 1] + h[12 + r] * v[3 * i + 2];
+    E.sk32[j] = used ? (float)sk : 0.0f;
+    E.hcp32[j] = (float)h[q];
   }
 }
 
-// One warp per edge (s, t): lane l owns entry l of the column-major block
-// (row r = l % 6 of t, column c = l / 6 of s), lanes 0-3 also entry 32 + l,
-// and sums its pairs' terms sum_i hcp_t[r][i] sk_s[c][i] in FP64 in the pair
-// order (ascending point): no reduction, no atomics.
-__global__ void __launch_bounds__(256) k_el_blocks(ElimDev E) {
+// One warp per edge (s, t), lane l taking the edge's pairs l, l + 32, ...
+// (ascending point order): each pair's 6x3 blocks hcp_t and sk_s arrive as
+// nine 8-byte loads each, their product hcp_t sk_s^T in FP32 is added to the
+// lane's FP64 6x6 accumulator, and the lanes' accumulators are summed by a
+// butterfly (a fixed order: the blocks do not depend on scheduling); then
+// block = extra - sum, column-major (row r of t, column c of s).
+__global__ void __launch_bounds__(128) k_el_blocks(ElimDev E) {
   const uint32_t lane = threadIdx.x & 31u;
   const uint64_t nw = (uint64_t)gridDim.x * blockDim.x / 32u;
-  const int r0 = (int)lane % 6, c0 = (int)lane / 6;
-  const int r1 = (int)(lane + 32) % 6, c1 = (int)(lane + 32) / 6;
-  const bool two = lane < 4u;
   for (uint64_t e = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / 32u; e < E.num_edges;
        e += nw) {
     const uint32_t a = E.pair_off[e], b = E.pair_off[e + 1];
-    double acc0 = 0.0, acc1 = 0.0;
-    uint32_t i = a;
-    // Four pairs' loads in flight, summed in pair order.
-    for (; i + 4 <= b; i += 4) {
-      float v0[4], v1[4];
+    double acc[36];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const uint2 pr = __ldg(E.pairs + i + u);
-        const float* ht = E.hcp32 + 18 * (size_t)pr.y;
-        const float* ss = E.sk32 + 18 * (size_t)pr.x;
-        float v = __ldg(ht + r0) * __ldg(ss + c0);
-        v = fmaf(__ldg(ht + 6 + r0), __ldg(ss + 6 + c0), v);
-        v0[u] = fmaf(__ldg(ht + 12 + r0), __ldg(ss + 12 + c0), v);
-        float w = 0.0f;
-        if (two) {
-          w = __ldg(ht + r1) * __ldg(ss + c1);
-          w = fmaf(__ldg(ht + 6 + r1), __ldg(ss + 6 + c1), w);
-          w = fmaf(__ldg(ht + 12 + r1), __ldg(ss + 12 + c1), w);
-        }
-        v1[u] = w;
-      }
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        acc0 += (double)v0[u];
-        acc1 += (double)v1[u];
-      }
-    }
-    for (; i < b; ++i) {
+    for (int q = 0; q < 36; ++q) acc[q] = 0.0;
+#pragma unroll 2
+    for (uint32_t i = a + lane; i < b; i += 32) {
       const uint2 pr = __ldg(E.pairs + i);
-      const float* ht = E.hcp32 + 18 * (size_t)pr.y;
-      const float* ss = E.sk32 + 18 * (size_t)pr.x;
-      float v = __ldg(ht + r0) * __ldg(ss + c0);
-      v = fmaf(__ldg(ht + 6 + r0), __ldg(ss + 6 + c0), v);
-      acc0 += (double)fmaf(__ldg(ht + 12 + r0), __ldg(ss + 12 + c0), v);
-      if (two) {
-        float w = __ldg(ht + r1) * __ldg(ss + c1);
-        w = fmaf(__ldg(ht + 6 + r1), __ldg(ss + 6 + c1), w);
-        acc1 += (double)fmaf(__ldg(ht + 12 + r1), __ldg(ss + 12 + c1), w);
+      const float2* ht2 = reinterpret_cast<const float2*>(E.hcp32 + 18 * (size_t)pr.y);
+      const float2* ss2 = reinterpret_cast<const float2*>(E.sk32 + 18 * (size_t)pr.x);
+      float h[18], g[18];
+#pragma unroll
+      for (int k = 0; k < 9; ++k) {
+        const float2 u = __ldg(ht2 + k), v = __ldg(ss2 + k);
+        h[2 * k] = u.x;
+        h[2 * k + 1] = u.y;
+        g[2 * k] = v.x;
+        g[2 * k + 1] = v.y;
       }
+      // h[6 i + r] = hcp_t[r][i], g[6 i + c] = sk_s[c][i].
+#pragma unroll
+      for (int c = 0; c < 6; ++c)
+#pragma unroll
+        for (int r = 0; r < 6; ++r) {
+          float v = h[r] * g[c];
+          v = fmaf(h[6 + r], g[6 + c], v);
+          v = fmaf(h[12 + r], g[12 + c], v);
+          acc[6 * c + r] += (double)v;
+        }
     }
+    // Butterfly over the lanes: every lane ends with the same 36 sums.
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+#pragma unroll
+      for (int q = 0; q < 36; ++q) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], off);
     const int x = E.extra_of ? E.extra_of[e] : -1;
     double* out = E.blocks + 36 * e;
-    out[lane] = (x >= 0 ? E.extra64[36 * (size_t)x + lane] : 0.0) - acc0;
-    if (two) out[32 + lane] = (x >= 0 ? E.extra64[36 * (size_t)x + 32 + lane] : 0.0) - acc1;
+    // Lane l writes entry l and (lanes 0-3) entry 32 + l.
+    double mine = acc[0], mine2 = acc[32];
+#pragma unroll
+    for (int q = 1; q < 32; ++q)
+      if ((int)lane == q) mine = acc[q];
+#pragma unroll
+    for (int q = 33; q < 36; ++q)
+      if ((int)lane == q - 32) mine2 = acc[q];
+    out[lane] = (x >= 0 ? E.extra64[36 * (size_t)x + lane] : 0.0) - mine;
+    if (lane < 4u) out[32 + lane] = (x >= 0 ? E.extra64[36 * (size_t)x + 32 + lane] : 0.0) - mine2;
   }
 }
 
@@ -520,13 +517,13 @@ cudaError_t launch_rp_iteration(const Dev& d, const RpData& rp, cudaStream_t s) 
 }
 
 cudaError_t launch_el_prepare(const ElimDev& e, cudaStream_t s) {
-  if (e.num_obs) k_el_prepare<<<flat_grid(e.num_obs), 256, 0, s>>>(e);
+  if (e.num_obs) k_el_prepare<<<flat_grid(18 * e.num_obs), 256, 0, s>>>(e);
   return cudaGetLastError();
 }
 
 cudaError_t launch_el_blocks(const ElimDev& e, cudaStream_t s) {
-  if (e.num_edges)
-    k_el_blocks<<<(int)std::min<uint64_t>((e.num_edges + 7) / 8, 148 * 64), 256, 0, s>>>(e);
+  if (e.num_edges)  // four warps a block: three blocks per SM at the kernel's registers
+    k_el_blocks<<<(int)std::min<uint64_t>((e.num_edges + 3) / 4, 148 * 96), 128, 0, s>>>(e);
   return cudaGetLastError();
 }
 

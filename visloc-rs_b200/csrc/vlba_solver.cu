@@ -2263,7 +2263,9 @@ bool reduced_eliminate(Context* c, const vlba_point_elimination* el, double* run
     E.structure_id = el->structure_id;
   }
   if (!E.hcp_valid || E.linearization_id != el->linearization_id) {
-    VLBA_CUDA(cudaMemcpyAsync(E.hcp64.p, el->hcp, 144 * nobs, cudaMemcpyHostToDevice, s));
+    Stager st(c);
+    st.add(E.hcp64.p, el->hcp, 144 * nobs);
+    st.flush(s);
     E.hcp_valid = true;
     E.linearization_id = el->linearization_id;
   }
@@ -2271,10 +2273,11 @@ bool reduced_eliminate(Context* c, const vlba_point_elimination* el, double* run
   // order), the run edges and the outputs.
   E.vinv64.ensure(72ull * P);
   VLBA_CUDA(cudaEventRecord(c->ev[4], s));
-  VLBA_CUDA(cudaMemcpyAsync(E.vinv64.p, el->point_inverse, 72ull * P, cudaMemcpyHostToDevice, s));
+  Stager st(c);  // this call's uploads, through pinned memory
+  st.add(E.vinv64.p, el->point_inverse, 72ull * P);
   if (el->point_used) {
     E.used.ensure(P);
-    VLBA_CUDA(cudaMemcpyAsync(E.used.p, el->point_used, P, cudaMemcpyHostToDevice, s));
+    st.add(E.used.p, el->point_used, P);
   }
   std::vector<int32_t> extra_of;
   std::vector<double> extra;
@@ -2291,16 +2294,16 @@ bool reduced_eliminate(Context* c, const vlba_point_elimination* el, double* run
     }
     E.extra_of.ensure(4 * ne);
     E.extra64.ensure(8 * extra.size());
-    VLBA_CUDA(cudaMemcpyAsync(E.extra_of.p, extra_of.data(), 4 * ne, cudaMemcpyHostToDevice, s));
-    VLBA_CUDA(cudaMemcpyAsync(E.extra64.p, extra.data(), 8 * extra.size(), cudaMemcpyHostToDevice,
-                              s));
+    st.add(E.extra_of.p, extra_of.data(), 4 * ne);
+    st.add(E.extra64.p, extra.data(), 8 * extra.size());
   }
   const uint64_t nrun = el->num_run_edges;
   if (nrun) {
     E.run_edges.ensure(4 * nrun);
     E.run_out.ensure(288 * nrun);
-    VLBA_CUDA(cudaMemcpyAsync(E.run_edges.p, el->run_edges, 4 * nrun, cudaMemcpyHostToDevice, s));
+    st.add(E.run_edges.p, el->run_edges, 4 * nrun);
   }
+  st.flush(s);
   const uint32_t m = el->coarse_group && el->coarse_nodes
                          ? (el->coarse_nodes + el->coarse_group - 1) / el->coarse_group
                          : 0;
