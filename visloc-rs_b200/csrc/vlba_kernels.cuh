@@ -40,7 +40,7 @@ struct RpScalars {
   uint32_t iters;
   uint32_t done;    // the loop is over: every kernel returns at once
   uint32_t failed;  // p.q not positive and finite
-  uint32_t pad;
+  uint32_t arrive;  // blocks of the running row kernel that have finished (reset by the last)
 };
 
 // The preconditioner and work arrays of a preconditioned reduced solve.
@@ -68,6 +68,10 @@ cudaError_t launch_rp_init(const Dev& d, const RpData& rp, cudaStream_t s);
 // One iteration; a no-op once sc->done is set.
 cudaError_t launch_rp_iteration(const Dev& d, const RpData& rp, cudaStream_t s);
 
+// Floats between consecutive FP32 camera-point blocks of an elimination: the
+// 18 entries of a 6x3 block padded to 80 bytes (16-byte aligned loads).
+constexpr int kElRec = 20;
+
 // A point elimination on the device (vlba_reduced.cu): the pair index of the
 // structure, this call's camera-point blocks and point inverses, the blocks.
 struct ElimDev {
@@ -88,8 +92,8 @@ struct ElimDev {
   const double* hcp64;         // [18 num_obs] 6x3 column-major
   const double* vinv64;        // [9 num_points] 3x3 column-major
   const uint8_t* used;         // [num_points] or null (all used)
-  float* hcp32;                // [18 num_obs]
-  float* sk32;                 // [18 num_obs] hcp V^-1 (zero for a point left out)
+  float* hcp32;                // [kElRec num_obs]
+  float* sk32;                 // [kElRec num_obs] hcp V^-1 (zero for a point left out)
   const int32_t* extra_of;     // [num_edges] row of extra64 or -1; null: none
   const double* extra64;       // [36 rows]
   double* blocks;              // [36 num_edges] column-major (row t, column s)

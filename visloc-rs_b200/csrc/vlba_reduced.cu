@@ -174,44 +174,141 @@ __global__ void __launch_bounds__(kMatvecWarps * 32) k_rp_matvec(Dev d, RpData r
   }
 }
 
-// q_R = the row's partial slots in order; the row's p.q.
+// ---- scalar steps
+// The rows' dots of a step summed lane-strided by one warp, then by a
+// butterfly (a fixed order), and the step's scalars; run by warp 0 of the
+// last block of a row kernel to finish (rp_arrive).
+enum RpStep { kRpInit = 0, kRpAlpha = 1, kRpCheck = 2, kRpBeta = 3 };
+__device__ void rp_scalar_step(const Dev& d, const RpData& rp, int step) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t rows = d.num_tile_rows;
+  const double* v = rp.dots + (size_t)(step == kRpAlpha ? 0 : step == kRpBeta ? 1 : 2) * rows;
+  double s = 0.0;
+  for (uint32_t r = lane; r < rows; r += 32) s += __ldcg(v + r);
+  s = warp_sum_d(s);
+  double rz = 0.0;
+  if (step == kRpInit) {  // |b|^2 and the initial r.z
+    for (uint32_t r = lane; r < rows; r += 32) rz += __ldcg(rp.dots + rows + r);
+    rz = warp_sum_d(rz);
+  }
+  if (lane != 0) return;
+  RpScalars& sc = *rp.sc;
+  switch (step) {
+    case kRpInit:
+      sc.bnorm = sqrt(s);
+      sc.rnorm = sc.bnorm;
+      sc.rz = rz;
+      sc.iters = 0u;
+      if (!(sc.bnorm > 0.0) || rp.max_iterations == 0u) sc.done = 1u;
+      break;
+    case kRpAlpha:  // a non-positive or non-finite curvature fails the solve
+      if (s > 0.0 && isfinite(s)) {
+        sc.alpha = sc.rz / s;
+      } else {
+        sc.failed = 1u;
+        sc.done = 1u;
+      }
+      break;
+    case kRpCheck:
+      sc.iters += 1u;
+      sc.rnorm = sqrt(s);
+      if (sc.rnorm <= rp.tol * sc.bnorm || sc.iters >= rp.max_iterations) sc.done = 1u;
+      break;
+    default:  // beta = r.z (new) / r.z (old)
+      sc.beta = s / sc.rz;
+      sc.rz = s;
+      break;
+  }
+}
+
+// Every block of a row kernel arrives once its rows' dots are written and
+// fenced; the last block to arrive (the one that sees the count reach the
+// grid size) resets the count and runs the scalar step.  No block waits for
+// another.  Every thread of the block must call it.
+__device__ void rp_arrive(const Dev& d, const RpData& rp, int step) {
+  __shared__ unsigned int last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const unsigned int prev = atomicAdd(&rp.sc->arrive, 1u);
+    last = prev == gridDim.x - 1 ? 1u : 0u;
+    if (last) rp.sc->arrive = 0u;  // every block has arrived
+  }
+  __syncthreads();
+  if (last && threadIdx.x < 32) {
+    __threadfence();
+    rp_scalar_step(d, rp, step);
+  }
+}
+
+// Tile row R of the calling warp (rows past the end take no part but arrive).
+__device__ __forceinline__ uint32_t rp_row() {
+  return (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+}
+
+// q_R = the row's partial slots in order; the row's p.q; then alpha.
 __global__ void k_rp_rowsum(Dev d, RpData rp) {
   if (rp_done(rp)) return;
-  RP_ROW_LOOP(d)
-  const uint32_t m0 = d.tr_list_off[R], m1 = d.tr_list_off[R + 1];
-  float q0 = 0.0f, q1 = 0.0f;
-  for (uint32_t m = m0; m < m1; ++m) {
-    q0 += d.partial[(size_t)m * kRow + lane];
-    if (e1) q1 += d.partial[(size_t)m * kRow + 32 + lane];
+  const uint32_t lane = threadIdx.x & 31u, R = rp_row();
+  if (R < d.num_tile_rows) {
+    const size_t base = (size_t)R * kRow;
+    const bool e1 = lane + 32u < (uint32_t)kRow;
+    const uint32_t m0 = d.tr_list_off[R], m1 = d.tr_list_off[R + 1];
+    float q0 = 0.0f, q1 = 0.0f;
+    for (uint32_t m = m0; m < m1; ++m) {
+      q0 += d.partial[(size_t)m * kRow + lane];
+      if (e1) q1 += d.partial[(size_t)m * kRow + 32 + lane];
+    }
+    d.q[base + lane] = q0;
+    double pq = (double)d.p[base + lane] * (double)q0;
+    if (e1) {
+      d.q[base + 32 + lane] = q1;
+      pq += (double)d.p[base + 32 + lane] * (double)q1;
+    }
+    pq = warp_sum_d(pq);
+    if (lane == 0) {
+      rp.dots[R] = pq;
+      __threadfence();
+    }
   }
-  d.q[base + lane] = q0;
-  double pq = (double)d.p[base + lane] * (double)q0;
-  if (e1) {
-    d.q[base + 32 + lane] = q1;
-    pq += (double)d.p[base + 32 + lane] * (double)q1;
-  }
-  pq = warp_sum_d(pq);
-  if (lane == 0) rp.dots[R] = pq;
+  rp_arrive(d, rp, kRpAlpha);
 }
 
-// x += alpha p, r -= alpha q; the rows' |r|^2.
+// x += alpha p, r -= alpha q; z = the 6x6 block-Jacobi inverse times r for
+// the row's nodes (runs overwrite theirs next); the rows' |r|^2; then the
+// stopping rule.
 __global__ void k_rp_update_xr(Dev d, RpData rp) {
   if (rp_done(rp)) return;
-  RP_ROW_LOOP(d)
-  (void)e1;
-  const float af = (float)rp.sc->alpha;
-  double rr = 0.0;
-  for (uint32_t e = lane; e < (uint32_t)kRow; e += 32) {
-    d.x[base + e] += af * d.p[base + e];
-    const float rv = d.r[base + e] - af * d.q[base + e];
-    d.r[base + e] = rv;
-    rr += (double)rv * (double)rv;
+  const uint32_t lane = threadIdx.x & 31u, R = rp_row();
+  if (R < d.num_tile_rows) {
+    const size_t base = (size_t)R * kRow;
+    const float af = (float)rp.sc->alpha;
+    double rr = 0.0;
+    for (uint32_t e = lane; e < (uint32_t)kRow; e += 32) {
+      d.x[base + e] += af * d.p[base + e];
+      const float rv = d.r[base + e] - af * d.q[base + e];
+      d.r[base + e] = rv;
+      rr += (double)rv * (double)rv;
+    }
+    __syncwarp();  // the row's new r is visible to the whole warp
+    for (uint32_t e = lane; e < (uint32_t)kRow; e += 32) {
+      const size_t node = (base + e) / 6, a = (base + e) % 6;
+      const float* m = d.minv + 36 * node + a * 6;
+      float z = 0.0f;
+#pragma unroll
+      for (int b = 0; b < 6; ++b) z += m[b] * d.r[6 * node + b];
+      d.z[base + e] = z;
+    }
+    rr = warp_sum_d(rr);
+    if (lane == 0) {
+      rp.dots[2 * (size_t)d.num_tile_rows + R] = rr;
+      __threadfence();
+    }
   }
-  rr = warp_sum_d(rr);
-  if (lane == 0) rp.dots[2 * (size_t)d.num_tile_rows + R] = rr;
+  rp_arrive(d, rp, kRpCheck);
 }
 
-// z = the 6x6 block-Jacobi inverse times r, every node (runs overwrite theirs).
+// z = the 6x6 block-Jacobi inverse times r, every node (the initial z).
 __global__ void k_rp_jacobi(Dev d, RpData rp) {
   if (rp_done(rp)) return;
   const size_t n = (size_t)d.num_var_cams * 6;
@@ -226,22 +323,44 @@ __global__ void k_rp_jacobi(Dev d, RpData rp) {
   }
 }
 
+constexpr int kClusterThreads = 1024;
+
 // One block per run: z_run = inverse (column-major, FP32) times r_run, the
-// run's residual staged in shared memory.
-__global__ void k_rp_cluster(Dev d, RpData rp) {
+// run's residual staged in shared memory.  A run of at most 512 rows splits
+// each row's sum over `parts` threads (contiguous column ranges, so reads
+// stay coalesced across the rows) and adds the parts in order.
+__global__ void __launch_bounds__(kClusterThreads) k_rp_cluster(Dev d, RpData rp) {
   if (rp_done(rp)) return;
-  extern __shared__ float seg[];
+  extern __shared__ float seg[];  // [rows] r, then [parts x rows] partial sums
   for (uint32_t c = blockIdx.x; c < rp.num_clusters; c += gridDim.x) {
     const uint32_t rows = 6u * rp.cl_size[c];
+    const uint32_t parts = rows <= 512u ? min(8u, blockDim.x / rows) : 1u;
     const size_t base = 6 * (size_t)rp.cl_first[c];
     const float* mat = rp.cl_mat + rp.cl_off[c];
     __syncthreads();
     for (uint32_t i = threadIdx.x; i < rows; i += blockDim.x) seg[i] = d.r[base + i];
     __syncthreads();
-    for (uint32_t row = threadIdx.x; row < rows; row += blockDim.x) {
-      float acc = 0.0f;
-      for (uint32_t k = 0; k < rows; ++k) acc += mat[(size_t)k * rows + row] * seg[k];
-      d.z[base + row] = acc;
+    if (parts > 1) {
+      float* part = seg + rows;
+      if (threadIdx.x < parts * rows) {
+        const uint32_t row = threadIdx.x % rows, pi = threadIdx.x / rows;
+        const uint32_t k0 = rows * pi / parts, k1 = rows * (pi + 1) / parts;
+        float acc = 0.0f;
+        for (uint32_t k = k0; k < k1; ++k) acc += mat[(size_t)k * rows + row] * seg[k];
+        part[pi * rows + row] = acc;
+      }
+      __syncthreads();
+      for (uint32_t row = threadIdx.x; row < rows; row += blockDim.x) {
+        float z = 0.0f;
+        for (uint32_t pi = 0; pi < parts; ++pi) z += part[pi * rows + row];
+        d.z[base + row] = z;
+      }
+    } else {
+      for (uint32_t row = threadIdx.x; row < rows; row += blockDim.x) {
+        float acc = 0.0f;
+        for (uint32_t k = 0; k < rows; ++k) acc += mat[(size_t)k * rows + row] * seg[k];
+        d.z[base + row] = acc;
+      }
     }
   }
 }
@@ -279,24 +398,31 @@ __global__ void __launch_bounds__(256) k_rp_coarse_apply(Dev d, RpData rp) {
   }
 }
 
-// z += P yc over the aggregated nodes; the rows' r.z.
-__global__ void k_rp_prolong_rz(Dev d, RpData rp) {
+// z += P yc over the aggregated nodes; the rows' r.z; then beta (or, for
+// the initial z, |b| and the first r.z).
+__global__ void k_rp_prolong_rz(Dev d, RpData rp, int step) {
   if (rp_done(rp)) return;
-  RP_ROW_LOOP(d)
-  (void)e1;
-  double rz = 0.0;
-  for (uint32_t e = lane; e < (uint32_t)kRow; e += 32) {
-    const size_t i = base + e;
-    float z = d.z[i];
-    const size_t node = i / 6;
-    if (rp.coarse_m && node < rp.coarse_nodes) {
-      z += rp.yc[6 * (node / rp.coarse_group) + i % 6];
-      d.z[i] = z;
+  const uint32_t lane = threadIdx.x & 31u, R = rp_row();
+  if (R < d.num_tile_rows) {
+    const size_t base = (size_t)R * kRow;
+    double rz = 0.0;
+    for (uint32_t e = lane; e < (uint32_t)kRow; e += 32) {
+      const size_t i = base + e;
+      float z = d.z[i];
+      const size_t node = i / 6;
+      if (rp.coarse_m && node < rp.coarse_nodes) {
+        z += rp.yc[6 * (node / rp.coarse_group) + i % 6];
+        d.z[i] = z;
+      }
+      rz += (double)d.r[i] * (double)z;
     }
-    rz += (double)d.r[i] * (double)z;
+    rz = warp_sum_d(rz);
+    if (lane == 0) {
+      rp.dots[(size_t)d.num_tile_rows + R] = rz;
+      __threadfence();
+    }
   }
-  rz = warp_sum_d(rz);
-  if (lane == 0) rp.dots[(size_t)d.num_tile_rows + R] = rz;
+  rp_arrive(d, rp, step);
 }
 
 // p = z (first) or z + beta p.
@@ -309,58 +435,13 @@ __global__ void k_rp_update_p(Dev d, RpData rp, int first) {
     d.p[i] = first ? d.z[i] : d.z[i] + bf * d.p[i];
 }
 
-// Scalar steps, one warp: the rows' dots summed lane-strided, then a
-// butterfly (a fixed order).
-enum RpStep { kRpInit = 0, kRpAlpha = 1, kRpCheck = 2, kRpBeta = 3 };
-__global__ void k_rp_scalars(Dev d, RpData rp, int step) {
-  const uint32_t lane = threadIdx.x & 31u;
-  if (threadIdx.x >= 32 || rp_done(rp)) return;
-  const uint32_t rows = d.num_tile_rows;
-  const double* v = rp.dots + (size_t)(step == kRpAlpha ? 0 : step == kRpBeta ? 1 : 2) * rows;
-  double s = 0.0;
-  for (uint32_t r = lane; r < rows; r += 32) s += v[r];
-  s = warp_sum_d(s);
-  double rz = 0.0;
-  if (step == kRpInit) {  // |b|^2 and the initial r.z
-    for (uint32_t r = lane; r < rows; r += 32) rz += rp.dots[rows + r];
-    rz = warp_sum_d(rz);
-  }
-  if (lane != 0) return;
-  RpScalars& sc = *rp.sc;
-  switch (step) {
-    case kRpInit:
-      sc.bnorm = sqrt(s);
-      sc.rnorm = sc.bnorm;
-      sc.rz = rz;
-      sc.iters = 0u;
-      if (!(sc.bnorm > 0.0) || rp.max_iterations == 0u) sc.done = 1u;
-      break;
-    case kRpAlpha:  // a non-positive or non-finite curvature fails the solve
-      if (s > 0.0 && isfinite(s)) {
-        sc.alpha = sc.rz / s;
-      } else {
-        sc.failed = 1u;
-        sc.done = 1u;
-      }
-      break;
-    case kRpCheck:
-      sc.iters += 1u;
-      sc.rnorm = sqrt(s);
-      if (sc.rnorm <= rp.tol * sc.bnorm || sc.iters >= rp.max_iterations) sc.done = 1u;
-      break;
-    default:  // beta = r.z (new) / r.z (old)
-      sc.beta = s / sc.rz;
-      sc.rz = s;
-      break;
-  }
-}
-
 // ---------------------------------------------------------------- elimination
 // Per camera-point block o of point p: an FP32 copy of hcp and sk = hcp V_p^-1
 // (formed in FP64; zero for a point left out, whose pairs then add zero).
 // One thread per entry q = 6 i + r of the 6x3 outputs, so that consecutive
 // threads read and write consecutive addresses (the three hcp entries an
-// output needs come from the same 144-byte block, through L1).
+// output needs come from the same 144-byte block, through L1).  The FP32
+// copies are kElRec floats apart (80 bytes: five 16-byte loads a block).
 __global__ void k_el_prepare(ElimDev E) {
   const uint64_t n = 18 * E.num_obs;
   for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n;
@@ -372,14 +453,14 @@ __global__ void k_el_prepare(ElimDev E) {
     const double* v = E.vinv64 + 9 * (size_t)p;
     const bool used = !E.used || E.used[p];
     const double sk = h[r] * v[3 * i] + h[6 + r] * v[3 * i + 1] + h[12 + r] * v[3 * i + 2];
-    E.sk32[j] = used ? (float)sk : 0.0f;
-    E.hcp32[j] = (float)h[q];
+    E.sk32[kElRec * o + q] = used ? (float)sk : 0.0f;
+    E.hcp32[kElRec * o + q] = (float)h[q];
   }
 }
 
 // One warp per edge (s, t), lane l taking the edge's pairs l, l + 32, ...
 // (ascending point order): each pair's 6x3 blocks hcp_t and sk_s arrive as
-// nine 8-byte loads each, their product hcp_t sk_s^T in FP32 is added to the
+// five 16-byte loads each, their product hcp_t sk_s^T in FP32 is added to the
 // lane's FP64 6x6 accumulator, and the lanes' accumulators are summed by a
 // butterfly (a fixed order: the blocks do not depend on scheduling); then
 // block = extra - sum, column-major (row r of t, column c of s).
@@ -395,16 +476,20 @@ __global__ void __launch_bounds__(128) k_el_blocks(ElimDev E) {
 #pragma unroll 2
     for (uint32_t i = a + lane; i < b; i += 32) {
       const uint2 pr = __ldg(E.pairs + i);
-      const float2* ht2 = reinterpret_cast<const float2*>(E.hcp32 + 18 * (size_t)pr.y);
-      const float2* ss2 = reinterpret_cast<const float2*>(E.sk32 + 18 * (size_t)pr.x);
-      float h[18], g[18];
+      const float4* ht4 = reinterpret_cast<const float4*>(E.hcp32 + kElRec * (size_t)pr.y);
+      const float4* ss4 = reinterpret_cast<const float4*>(E.sk32 + kElRec * (size_t)pr.x);
+      float h[kElRec], g[kElRec];  // entries 18 and 19 are padding
 #pragma unroll
-      for (int k = 0; k < 9; ++k) {
-        const float2 u = __ldg(ht2 + k), v = __ldg(ss2 + k);
-        h[2 * k] = u.x;
-        h[2 * k + 1] = u.y;
-        g[2 * k] = v.x;
-        g[2 * k + 1] = v.y;
+      for (int k = 0; k < kElRec / 4; ++k) {
+        const float4 u = __ldg(ht4 + k), v = __ldg(ss4 + k);
+        h[4 * k] = u.x;
+        h[4 * k + 1] = u.y;
+        h[4 * k + 2] = u.z;
+        h[4 * k + 3] = u.w;
+        g[4 * k] = v.x;
+        g[4 * k + 1] = v.y;
+        g[4 * k + 2] = v.z;
+        g[4 * k + 3] = v.w;
       }
       // h[6 i + r] = hcp_t[r][i], g[6 i + c] = sk_s[c][i].
 #pragma unroll
@@ -477,15 +562,16 @@ __global__ void __launch_bounds__(256) k_el_coarse(ElimDev E) {
 int rows_grid(const Dev& d) { return (int)((d.num_tile_rows + 7) / 8); }
 int flat_grid(size_t n) { return (int)std::min<size_t>((n + 255) / 256, 148 * 8); }
 
-void precondition(const Dev& d, const RpData& rp, cudaStream_t s) {
-  k_rp_jacobi<<<flat_grid((size_t)d.num_var_cams * 6), 256, 0, s>>>(d, rp);
+// z = M r beyond block-Jacobi: the runs, then the coarse level (restrict and
+// apply; its prolongation is in k_rp_prolong_rz).
+void precondition_rest(const Dev& d, const RpData& rp, cudaStream_t s) {
   if (rp.num_clusters)
-    k_rp_cluster<<<std::min<uint32_t>(rp.num_clusters, 148 * 4), 256, rp.max_cluster_rows * 4, s>>>(d, rp);
+    k_rp_cluster<<<std::min<uint32_t>(rp.num_clusters, 148 * 2), kClusterThreads,
+                   (rp.max_cluster_rows + kClusterThreads) * sizeof(float), s>>>(d, rp);
   if (rp.coarse_m) {
     k_rp_restrict<<<(6 * rp.coarse_m + 255) / 256, 256, 0, s>>>(d, rp);
     k_rp_coarse_apply<<<std::min<uint32_t>(6 * rp.coarse_m, 148 * 8), 256, 0, s>>>(d, rp);
   }
-  k_rp_prolong_rz<<<rows_grid(d), 256, 0, s>>>(d, rp);
 }
 
 }  // namespace
@@ -495,23 +581,25 @@ cudaError_t launch_rp_init(const Dev& d, const RpData& rp, cudaStream_t s) {
                                        (int)kMatvecSmem);
   if (e != cudaSuccess) return e;
   k_rp_init_xr<<<rows_grid(d), 256, 0, s>>>(d, rp);
-  precondition(d, rp, s);
-  k_rp_scalars<<<1, 32, 0, s>>>(d, rp, kRpInit);
+  k_rp_jacobi<<<flat_grid((size_t)d.num_var_cams * 6), 256, 0, s>>>(d, rp);
+  precondition_rest(d, rp, s);
+  k_rp_prolong_rz<<<rows_grid(d), 256, 0, s>>>(d, rp, kRpInit);
   k_rp_update_p<<<flat_grid((size_t)d.num_var_cams * 6), 256, 0, s>>>(d, rp, 1);
   return cudaGetLastError();
 }
 
+// One iteration: the product, q and alpha, the x and r update with the
+// block-Jacobi z and the stopping rule, the runs and the coarse level, r.z
+// and beta, the p update -- six to eight launches.
 cudaError_t launch_rp_iteration(const Dev& d, const RpData& rp, cudaStream_t s) {
   // Three blocks per SM (their rings take 3 x 72 KB of shared memory).
   const int tiles_grid =
       (int)std::min<uint32_t>((d.num_tiles + kMatvecWarps - 1) / kMatvecWarps, 148 * 3);
   k_rp_matvec<<<std::max(1, tiles_grid), kMatvecWarps * 32, kMatvecSmem, s>>>(d, rp);
   k_rp_rowsum<<<rows_grid(d), 256, 0, s>>>(d, rp);
-  k_rp_scalars<<<1, 32, 0, s>>>(d, rp, kRpAlpha);
   k_rp_update_xr<<<rows_grid(d), 256, 0, s>>>(d, rp);
-  k_rp_scalars<<<1, 32, 0, s>>>(d, rp, kRpCheck);
-  precondition(d, rp, s);
-  k_rp_scalars<<<1, 32, 0, s>>>(d, rp, kRpBeta);
+  precondition_rest(d, rp, s);
+  k_rp_prolong_rz<<<rows_grid(d), 256, 0, s>>>(d, rp, kRpBeta);
   k_rp_update_p<<<flat_grid((size_t)d.num_var_cams * 6), 256, 0, s>>>(d, rp, 0);
   return cudaGetLastError();
 }

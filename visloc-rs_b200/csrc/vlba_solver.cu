@@ -327,11 +327,16 @@ void par_memcpy(void* dst, const void* src, size_t n) {
 }
 
 // The context's two pinned staging buffers with at least `want` bytes each
-// (at most 64 MB); false when no pinned memory can be had.
+// (at most 64 MB); false when no pinned memory can be had.  They grow to at
+// least 16 MB and at least double, so that uploads of growing sizes (a
+// serving slot's batches) reallocate them a few times at most: freeing
+// pinned memory waits for the device.
+constexpr size_t kStageMax = 64u << 20;
 bool reserve_stage(Context* c, size_t want) {
-  constexpr size_t kMax = 64u << 20, kGrain = 1u << 20;
-  want = std::min(kMax, (want + kGrain - 1) / kGrain * kGrain);
+  constexpr size_t kMin = 16u << 20, kGrain = 1u << 20;
+  want = std::min(kStageMax, (want + kGrain - 1) / kGrain * kGrain);
   if (c->stage_cap >= want) return true;
+  want = std::min(kStageMax, std::max({want, kMin, 2 * c->stage_cap}));
   for (int i = 0; i < 2; ++i) {
     if (c->stage_ev[i]) VLBA_CUDA(cudaEventSynchronize(c->stage_ev[i]));
     else VLBA_CUDA(cudaEventCreateWithFlags(&c->stage_ev[i], cudaEventDisableTiming));
@@ -1911,6 +1916,7 @@ void* visloc_ba_cuda_server_create(int device, uint32_t slots, uint64_t memory_b
       S->slots.push_back(c);
       c->arena.use_slab(S->slot_bytes);
       c->gate = &S->gate;
+      vlba::reserve_stage(c, vlba::kStageMax);  // at full size before the first request
     }
     const uint32_t planners =
         std::max(1u, std::min(8u, std::thread::hardware_concurrency() / 2));
@@ -2252,8 +2258,8 @@ bool reduced_eliminate(Context* c, const vlba_point_elimination* el, double* run
                               cudaMemcpyHostToDevice, s));
     E.edges.assign(el->edges, el->edges + 2 * ne);
     E.hcp64.ensure(144 * nobs);
-    E.hcp32.ensure(72 * nobs);
-    E.sk32.ensure(72 * nobs);
+    E.hcp32.ensure(4 * kElRec * nobs);
+    E.sk32.ensure(4 * kElRec * nobs);
     E.blocks.ensure(288 * ne);
     VLBA_CUDA(cudaStreamSynchronize(s));  // X's host arrays go next
     E.n = n;
