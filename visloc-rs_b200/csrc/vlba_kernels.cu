@@ -1172,13 +1172,37 @@ __device__ ProbScal prob_scalars_warp(const Dev& d, uint32_t P, int k) {
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t t0 = d.prob_tr_begin[P], t1 = d.prob_tr_begin[P + 1];
   double v[5] = {0, 0, 0, 0, 0};  // rz(k-1), rz(k-2), rr(k-1), pq(k-1), b2
-  const int s1 = mod3(k - 1), s2 = mod3(k - 2), sp = (k - 1) & 1;
-  for (uint32_t tr = t0 + lane; tr < t1; tr += 32) {
-    v[0] += __ldcg(dot_at(d, kDotRz + s1, tr));
-    v[1] += __ldcg(dot_at(d, kDotRz + s2, tr));
-    v[2] += __ldcg(dot_at(d, kDotRr + s1, tr));
-    v[3] += __ldcg(dot_at(d, kDotPq + sp, tr));
-    v[4] += __ldcg(dot_at(d, kDotB2, tr));
+  const double* q0 = dot_at(d, kDotRz + mod3(k - 1), 0);
+  const double* q1 = dot_at(d, kDotRz + mod3(k - 2), 0);
+  const double* q2 = dot_at(d, kDotRr + mod3(k - 1), 0);
+  const double* q3 = dot_at(d, kDotPq + ((k - 1) & 1), 0);
+  const double* q4 = dot_at(d, kDotB2, 0);
+  // Lane l adds rows t0 + l, t0 + l + 32, ... in ascending order, two rows'
+  // loads issued before their adds (a problem of many tile rows otherwise
+  // makes the sums a chain of L2 round trips).
+  uint32_t tr = t0 + lane;
+  for (; tr + 32 < t1; tr += 64) {
+    const double a0 = __ldcg(q0 + tr), a1 = __ldcg(q1 + tr), a2 = __ldcg(q2 + tr),
+                 a3 = __ldcg(q3 + tr), a4 = __ldcg(q4 + tr);
+    const double b0 = __ldcg(q0 + tr + 32), b1 = __ldcg(q1 + tr + 32), b2 = __ldcg(q2 + tr + 32),
+                 b3 = __ldcg(q3 + tr + 32), b4 = __ldcg(q4 + tr + 32);
+    v[0] += a0;
+    v[1] += a1;
+    v[2] += a2;
+    v[3] += a3;
+    v[4] += a4;
+    v[0] += b0;
+    v[1] += b1;
+    v[2] += b2;
+    v[3] += b3;
+    v[4] += b4;
+  }
+  if (tr < t1) {
+    v[0] += __ldcg(q0 + tr);
+    v[1] += __ldcg(q1 + tr);
+    v[2] += __ldcg(q2 + tr);
+    v[3] += __ldcg(q3 + tr);
+    v[4] += __ldcg(q4 + tr);
   }
 #pragma unroll
   for (int e = 0; e < 5; ++e) v[e] = warp_sum(v[e]);
@@ -1771,9 +1795,20 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
         // The block's scalars of this iteration when they are this problem's
         // (the single-problem case), else this warp's own.
         const ProbScal ps = (sc_prob == P && sc_k == k) ? sc : prob_scalars_warp(d, P, k);
+        // Rows in the plain loop's order, four rows' loads ahead of their adds.
+        const double* pqd = dot_at(d, kDotPq + (k & 1), 0);
+        const uint32_t pt1 = d.prob_tr_begin[P + 1];
         double pq = 0.0;
-        for (uint32_t t2 = d.prob_tr_begin[P] + lane; t2 < d.prob_tr_begin[P + 1]; t2 += 32)
-          pq += __ldcg(dot_at(d, kDotPq + (k & 1), t2));
+        uint32_t t2 = d.prob_tr_begin[P] + lane;
+        for (; t2 + 96 < pt1; t2 += 128) {
+          const double a0 = __ldcg(pqd + t2), a1 = __ldcg(pqd + t2 + 32),
+                       a2 = __ldcg(pqd + t2 + 64), a3 = __ldcg(pqd + t2 + 96);
+          pq += a0;
+          pq += a1;
+          pq += a2;
+          pq += a3;
+        }
+        for (; t2 < pt1; t2 += 32) pq += __ldcg(pqd + t2);
         pq = warp_sum(pq);
         alpha = (ps.active && pq > 0.0 && isfinite(pq)) ? ps.rz / pq : 0.0;
         cprob = P;
