@@ -1177,27 +1177,41 @@ __device__ ProbScal prob_scalars_warp(const Dev& d, uint32_t P, int k) {
   const double* q2 = dot_at(d, kDotRr + mod3(k - 1), 0);
   const double* q3 = dot_at(d, kDotPq + ((k - 1) & 1), 0);
   const double* q4 = dot_at(d, kDotB2, 0);
-  // Lane l adds rows t0 + l, t0 + l + 32, ... in ascending order, two rows'
+  // Lane l adds rows t0 + l, t0 + l + 32, ... in ascending order, four rows'
   // loads issued before their adds (a problem of many tile rows otherwise
   // makes the sums a chain of L2 round trips).
   uint32_t tr = t0 + lane;
-  for (; tr + 32 < t1; tr += 64) {
-    const double a0 = __ldcg(q0 + tr), a1 = __ldcg(q1 + tr), a2 = __ldcg(q2 + tr),
-                 a3 = __ldcg(q3 + tr), a4 = __ldcg(q4 + tr);
-    const double b0 = __ldcg(q0 + tr + 32), b1 = __ldcg(q1 + tr + 32), b2 = __ldcg(q2 + tr + 32),
-                 b3 = __ldcg(q3 + tr + 32), b4 = __ldcg(q4 + tr + 32);
-    v[0] += a0;
-    v[1] += a1;
-    v[2] += a2;
-    v[3] += a3;
-    v[4] += a4;
-    v[0] += b0;
-    v[1] += b1;
-    v[2] += b2;
-    v[3] += b3;
-    v[4] += b4;
+  for (; tr + 96 < t1; tr += 128) {
+    const double a00 = __ldcg(q0 + tr), a01 = __ldcg(q1 + tr), a02 = __ldcg(q2 + tr),
+                 a03 = __ldcg(q3 + tr), a04 = __ldcg(q4 + tr);
+    const double a10 = __ldcg(q0 + tr + 32), a11 = __ldcg(q1 + tr + 32), a12 = __ldcg(q2 + tr + 32),
+                 a13 = __ldcg(q3 + tr + 32), a14 = __ldcg(q4 + tr + 32);
+    const double a20 = __ldcg(q0 + tr + 64), a21 = __ldcg(q1 + tr + 64), a22 = __ldcg(q2 + tr + 64),
+                 a23 = __ldcg(q3 + tr + 64), a24 = __ldcg(q4 + tr + 64);
+    const double a30 = __ldcg(q0 + tr + 96), a31 = __ldcg(q1 + tr + 96), a32 = __ldcg(q2 + tr + 96),
+                 a33 = __ldcg(q3 + tr + 96), a34 = __ldcg(q4 + tr + 96);
+    v[0] += a00;
+    v[1] += a01;
+    v[2] += a02;
+    v[3] += a03;
+    v[4] += a04;
+    v[0] += a10;
+    v[1] += a11;
+    v[2] += a12;
+    v[3] += a13;
+    v[4] += a14;
+    v[0] += a20;
+    v[1] += a21;
+    v[2] += a22;
+    v[3] += a23;
+    v[4] += a24;
+    v[0] += a30;
+    v[1] += a31;
+    v[2] += a32;
+    v[3] += a33;
+    v[4] += a34;
   }
-  if (tr < t1) {
+  for (; tr < t1; tr += 32) {
     v[0] += __ldcg(q0 + tr);
     v[1] += __ldcg(q1 + tr);
     v[2] += __ldcg(q2 + tr);
