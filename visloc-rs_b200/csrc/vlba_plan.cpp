@@ -1,6 +1,8 @@
 // vlba_plan.cpp -- see vlba_plan.h.
 #include "vlba_plan.h"
 
+#include <sys/mman.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -10,6 +12,13 @@
 #include <thread>
 
 namespace vlba {
+
+void advise_huge_pages(void* p, size_t bytes) {
+  constexpr uintptr_t kHuge = 2u << 20;
+  const uintptr_t a = ((uintptr_t)p + kHuge - 1) & ~(kHuge - 1);
+  const uintptr_t e = ((uintptr_t)p + bytes) & ~(kHuge - 1);
+  if (e > a) madvise(reinterpret_cast<void*>(a), e - a, MADV_HUGEPAGE);
+}
 
 namespace {
 
@@ -474,20 +483,27 @@ void build_plan_serial(const vlba_problem* const* problems, const vlba_config* c
     }
     // f(la, lb, a, b) for every pair a > b of variable-slot observations of a
     // variable point in range t (local slots, local observation indices).
+    // The arrays are read through local pointers (the compiler cannot keep a
+    // vector's data pointer in a register across the callers' stores).
+    const uint8_t* const pvar = P.point_var.data() + point_base;
+    const uint32_t* const oslot = P.obs_slot.data() + obs_base;
+    const uint32_t* const pcnt = cnt.data();
     auto each_pair = [&](uint32_t t, auto&& f, uint64_t* var) {
-      for (uint32_t j = range[t]; j < range[t + 1]; ++j) {
-        if (!P.point_var[point_base + j]) continue;
-        const uint32_t k0 = cnt[j], k1 = cnt[j + 1];
+      uint64_t nv = 0;
+      for (uint32_t j = range[t], je = range[t + 1]; j < je; ++j) {
+        if (!pvar[j]) continue;
+        const uint32_t k0 = pcnt[j], k1 = pcnt[j + 1];
         for (uint32_t a = k0; a < k1; ++a) {
-          const uint32_t sa = P.obs_slot[obs_base + a];
+          const uint32_t sa = oslot[a];
           if (sa == kNone) continue;
-          if (var) ++*var;
+          ++nv;
           for (uint32_t b = k0; b < a; ++b) {
-            const uint32_t sb = P.obs_slot[obs_base + b];
+            const uint32_t sb = oslot[b];
             if (sb != kNone) f(sa - slot_base, sb - slot_base, a, b);
           }
         }
       }
+      if (var) *var += nv;
     };
     // (A) per range: terms of each row, same-camera terms of each slot.
     std::vector<std::vector<uint64_t>> tcnt(T, std::vector<uint64_t>(2 * (size_t)nvar, 0));
@@ -528,17 +544,22 @@ void build_plan_serial(const vlba_problem* const* problems, const vlba_config* c
     run_threads(T, [&](uint32_t t) {
       uint64_t* pos = tcnt[t].data();
       uint64_t* dpos = pos + nvar;
-      each_pair(t, [&](uint32_t la, uint32_t lb, uint32_t a, uint32_t b) {
+      PairIdx* const pairs = P.pairs.data();
+      PairIdx* const dups = P.dup_pairs.data();
+      uint32_t* const tcol = term_col.data();
+      each_pair(t, [=](uint32_t la, uint32_t lb, uint32_t a, uint32_t b) {
         const uint32_t ga = obs_base + a, gb = obs_base + b;
         if (la > lb) {
-          term_col[pos[la] - pair_base] = lb;
-          P.pairs[pos[la]++] = PairIdx{ga, gb};
+          const uint64_t w = pos[la]++;
+          tcol[w - pair_base] = lb;
+          pairs[w] = PairIdx{ga, gb};
         } else if (lb > la) {
-          term_col[pos[lb] - pair_base] = la;
-          P.pairs[pos[lb]++] = PairIdx{gb, ga};
+          const uint64_t w = pos[lb]++;
+          tcol[w - pair_base] = la;
+          pairs[w] = PairIdx{gb, ga};
         } else {
-          P.dup_pairs[dpos[la]++] = PairIdx{ga, gb};
-          P.dup_pairs[dpos[la]++] = PairIdx{gb, ga};
+          dups[dpos[la]++] = PairIdx{ga, gb};
+          dups[dpos[la]++] = PairIdx{gb, ga};
         }
       }, nullptr);
     });
@@ -551,11 +572,14 @@ void build_plan_serial(const vlba_problem* const* problems, const vlba_config* c
         std::vector<uint32_t> mark(nvar, 0), touched;
         std::vector<uint64_t> at(nvar, 0);
         std::vector<PairIdx> buf;
+        const uint32_t* const tcol = term_col.data();
+        PairIdx* const pairs = P.pairs.data();
+        uint32_t* const mk = mark.data();
         for (uint32_t i; (i = next.fetch_add(1)) < nvar;) {
           const uint64_t lo = row_at[i], hi = row_at[i + 1];
           touched.clear();
           for (uint64_t k = lo; k < hi; ++k)
-            if (mark[term_col[k - pair_base]]++ == 0) touched.push_back(term_col[k - pair_base]);
+            if (mk[tcol[k - pair_base]]++ == 0) touched.push_back(tcol[k - pair_base]);
           std::sort(touched.begin(), touched.end());
           row_col[i] = touched;
           row_count[i].resize(touched.size());
@@ -567,8 +591,9 @@ void build_plan_serial(const vlba_problem* const* problems, const vlba_config* c
             mark[touched[b]] = 0;
           }
           if (touched.size() > 1) {
-            buf.assign(P.pairs.begin() + lo, P.pairs.begin() + hi);
-            for (uint64_t k = lo; k < hi; ++k) P.pairs[at[term_col[k - pair_base]]++] = buf[k - lo];
+            buf.assign(pairs + lo, pairs + hi);
+            uint64_t* const at_ = at.data();
+            for (uint64_t k = lo; k < hi; ++k) pairs[at_[tcol[k - pair_base]]++] = buf[k - lo];
           }
         }
       });

@@ -19,9 +19,16 @@ struct PairIdx {
   uint32_t a, b;
 };
 
+// Asks the kernel to back [p, p + bytes) with transparent huge pages (where
+// it only does so on request): the builder's scatters write into many
+// streams across arrays of hundreds of MB, which 4 KB pages make
+// TLB-bound.  A hint only.
+void advise_huge_pages(void* p, size_t bytes);
+
 // Allocator whose resize() leaves new elements uninitialised, for the large
 // pair arrays that the builder sizes first and then writes in full (from
-// several threads, which then also take the page faults).
+// several threads, which then also take the page faults).  Allocations of 8 MB
+// or more are advised huge pages before their first touch.
 template <typename T>
 struct NoInit : std::allocator<T> {
   template <typename U>
@@ -31,6 +38,11 @@ struct NoInit : std::allocator<T> {
   NoInit() noexcept = default;
   template <typename U>
   NoInit(const NoInit<U>&) noexcept {}
+  T* allocate(size_t n) {
+    T* p = std::allocator<T>::allocate(n);
+    if (n * sizeof(T) >= (8u << 20)) advise_huge_pages(p, n * sizeof(T));
+    return p;
+  }
   template <typename U>
   void construct(U* p) noexcept {
     ::new (static_cast<void*>(p)) U;
