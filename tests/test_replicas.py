@@ -59,3 +59,34 @@ def test_two_replicas_aggregate_over_gloo():
     assert st0 == 0 and st1 == 0
     assert tmax0 == tmax1 == pytest.approx(max(dt0, dt1))
     assert rate0 == rate1 == pytest.approx((it0 + it1) / max(dt0, dt1))
+
+
+def test_reduced_reference_arm_runs_on_the_cpu():
+    """bench.py's reduced-camera workload, reference arm (the oracle's FP64
+    iteration, no GPU), at a small size: one JSON line with the contract's
+    keys, and the tile count of the device layout for its edges."""
+    import json
+    import subprocess
+
+    out = subprocess.run(
+        [sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--workload",
+         "reduced-5822", "--reduced-nodes", "160"],
+        capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert out.returncode == 0, out.stderr[-2000:]
+    line = json.loads(out.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["metric"] == "reduced_pcg_iteration_ms"
+    assert line["value"] > 0 and line["higher_is_better"] is False
+    assert line["config"]["nodes"] == 160 and line["config"]["workload"] == "reduced-160"
+    assert line["cpu_baseline"]["kind"] == "port" and line["e2e"]["h2d_bytes_per_step"] == 0
+
+
+def test_reduced_tiles_counts_the_device_layout():
+    sys.path[:0] = [ROOT]
+    import numpy as np
+
+    import bench
+
+    edges = np.array([(0, 1), (0, 9), (3, 20), (8, 9), (16, 17)], np.uint32)
+    # Tile rows of 8 nodes: 3 rows for 21 nodes; diagonal tiles (0,0), (1,1), (2,2) plus the
+    # off-diagonal tiles (0,1) and (0,2).
+    assert bench.reduced_tiles(edges, 21) == 5
