@@ -406,7 +406,9 @@ typedef struct vlba_reduced_preconditioner {
  * p = z + beta p.  Vectors and S are f32, dots and scalars f64; every sum
  * runs in a fixed order, so repeated solves give identical steps.  A p.q
  * that is not positive and finite fails the solve as in pcg_core (which
- * returns None): VLBA_DECLINED, and the caller runs its CPU solver.  A zero
+ * returns None): VLBA_DECLINED, and the caller runs its CPU solver.  Edges
+ * out of order or repeated are declined too, as the reference's solver does
+ * (VLBA_ERR_INVALID_ARGUMENT for an edge that is not a < b < nodes).  A zero
  * right-hand side gives x = 0 after 0 iterations.
  *
  * Both reduced-solve entry points accept offdiag = NULL with num_edges > 0:

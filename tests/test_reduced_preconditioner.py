@@ -260,3 +260,29 @@ def test_gpu_rejects_malformed_preconditioners(solver):
                dict(clusters=[(0, np.eye(10))])):
         with pytest.raises(ValueError):
             solver.reduced_solve(diag, edges, off, b, 1e-6, 100, **kw)
+
+
+@pytest.mark.gpu
+def test_gpu_unsorted_edges_decline(solver):
+    """As the reference's solver (reduced.rs, solves_are_deterministic_and_
+    unsorted_edges_decline): edges out of order are declined, for either
+    preconditioner; malformed edges are an invalid argument."""
+    diag, edges, off = chain_system(60)
+    b = pattern_rhs(60).reshape(-1, 6)
+    runs = oracle.cluster_inverses(diag, edges, off, 16)
+    swapped = edges.copy()
+    swapped[[0, -1]] = swapped[[-1, 0]]
+    off_sw = off.copy()
+    off_sw[[0, -1]] = off_sw[[-1, 0]]
+    for kw in ({}, dict(clusters=runs)):
+        with pytest.raises(SolverError) as e:
+            solver.reduced_solve(diag, swapped, off_sw, b, 1e-6, 100, **kw)
+        assert e.value.status == _abi.DECLINED, kw
+    bad = edges.copy()
+    bad[3] = (bad[3][1], bad[3][0])  # a > b
+    with pytest.raises(SolverError) as e:
+        solver.reduced_solve(diag, bad, off, b, 1e-6, 100)
+    assert e.value.status == _abi.ERR_INVALID_ARGUMENT
+    # The sorted system still solves afterwards.
+    _, it, rr = solver.reduced_solve(diag, edges, off, b, 1e-6, 500, clusters=runs)
+    assert rr <= 1e-6 and it > 0

@@ -2025,6 +2025,17 @@ void reduced_setup(Context* c, const vlba_reduced_system* sys) {
                     c->reduced_edges.size() == 2 * ne &&
                     (ne == 0 || std::memcmp(c->reduced_edges.data(), sys->edges, 8 * ne) == 0);
   if (!same) {
+    // Edges out of order or repeated: the reference's solver declines them
+    // (its product needs each node's edges contiguous), and so does this one.
+    for (uint64_t e = 0; e < ne; ++e) {
+      const uint32_t a = sys->edges[2 * e], b = sys->edges[2 * e + 1];
+      if (!(a < b && b < n))
+        throw Status(VLBA_ERR_INVALID_ARGUMENT, "edge " + std::to_string(e) +
+                                                    " is not (a, b) with a < b < nodes");
+      if (e && ((uint64_t)sys->edges[2 * e - 2] << 32 | sys->edges[2 * e - 1]) >=
+                   ((uint64_t)a << 32 | b))
+        throw Status(VLBA_DECLINED, "edges are not sorted and distinct at " + std::to_string(e));
+    }
     c->reduced_generation = ~0ull;
     build_reduced_plan(sys->num_nodes, sys->edges, sys->num_edges, 8, lp, &c->plan);
     const std::string bad = check_plan(c->plan);
