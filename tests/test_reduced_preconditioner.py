@@ -286,3 +286,65 @@ def test_gpu_unsorted_edges_decline(solver):
     # The sorted system still solves afterwards.
     _, it, rr = solver.reduced_solve(diag, edges, off, b, 1e-6, 500, clusters=runs)
     assert rr <= 1e-6 and it > 0
+
+
+def relative_constraint_system(n, seed):
+    """J^T J of random relative constraints M (x_b - x_a) in scaled variables
+    along a capture-ordered chain (four neighbours each, n / 4 long-range
+    edges), node scales 10^(1 + U(-1, 1)), a weak prior 1e-3 s^2 I: SPD and
+    Laplacian-like (the shape of the reference's random_system,
+    crates/ba-gpu/src/reduced.rs:1050-1098).  Blocks are rounded to f32 as the
+    system hands them over."""
+    rng = np.random.default_rng(seed)
+    edges = {(b - d, b) for b in range(1, n) for d in range(1, min(4, b) + 1)}
+    for _ in range(n // 4):
+        a, b = (int(v) for v in rng.integers(0, n, 2))
+        if a + 4 < b:
+            edges.add((a, b))
+    edges = sorted(edges)
+    scale = 10.0 ** (rng.uniform(-1.0, 1.0, n) + 1.0)
+    diag = [np.eye(6) * 1e-3 * s * s for s in scale]
+    off = []
+    for a, b in edges:
+        m = rng.uniform(-1.0, 1.0, (6, 6)) + 2.0 * np.eye(6)
+        fa, fb = -m * scale[a], m * scale[b]
+        diag[a] = diag[a] + fa.T @ fa
+        diag[b] = diag[b] + fb.T @ fb
+        off.append((fb.T @ fa).astype(np.float32).astype(np.float64))
+    rhs = (rng.uniform(-1.0, 1.0, (n, 6)) * scale[:, None] * 1e3).reshape(-1)
+    return diag, np.array(edges, np.uint32), np.array(off), rhs
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n,k,group", [(300, 32, 16), (150, 1, None), (77, 32, None),
+                                       (61, 8, 7)])
+def test_gpu_matches_the_fp64_iteration_on_relative_constraints(solver, n, k, group):
+    """The reference's gpu_pcg_matches_the_cpu_iteration cases (reduced.rs:
+    1197-1250): runs of k nodes (k = 1: block-Jacobi), an optional coarse
+    level over every node, tolerance 1e-2; the device within 1 + 10% of the
+    FP64 iteration count, its true residual within 1.2 tol and its step
+    within 1e-3 of the FP64 one."""
+    diag, edges, off, b = relative_constraint_system(n, 7 + n)
+    S = dense(diag, edges, off)
+    runs = oracle.cluster_inverses(diag, edges, off, k) if k > 1 else None
+    coarse = None
+    if group:
+        m = -(-n // group)
+        P = np.zeros((6 * n, 6 * m))
+        for i in range(n):
+            P[6 * i:6 * i + 6, 6 * (i // group):6 * (i // group) + 6] = np.eye(6)
+        coarse = (group, n, np.linalg.inv(P.T @ S @ P))
+    tol = 1e-2
+    x_ref, it_ref = oracle.reduced_pcg(diag, edges, off, b, tol, 500, clusters=runs,
+                                       coarse=coarse)
+    assert it_ref > 3
+    variants = [dict(clusters=runs or [], coarse=coarse)]
+    if runs is None and coarse is None:
+        variants.append({})  # block-Jacobi through the persistent kernel too
+    for kw in variants:
+        x, it, _ = solver.reduced_solve(diag, edges, off, b.reshape(-1, 6), tol, 500, **kw)
+        x = x.reshape(-1)
+        assert abs(it - it_ref) <= 1 + it_ref // 10, (kw.keys(), it, it_ref)
+        assert np.linalg.norm(b - S @ x) <= 1.2 * tol * np.linalg.norm(b)
+        xr = x_ref.reshape(-1)
+        assert np.linalg.norm(x - xr) <= 1e-3 * np.linalg.norm(xr)
