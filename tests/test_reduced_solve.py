@@ -84,3 +84,22 @@ def test_reduced_solve_stops_at_the_iteration_cap(solver):
     diag, edges, off, b = reference_layout(S, rhs)
     x, iters, rr = solver.reduced_solve(diag, edges, off, b, 1e-12, 7)
     assert iters == 7 and rr > 1e-12
+
+
+def test_layout_reuse_takes_each_calls_values(solver):
+    """Solves of the same edges reuse the device layout: each call's blocks,
+    right-hand side, tolerance and iteration cap must still be the ones
+    used (twice the matrix gives half the step; a cap of 4, then a full
+    solve, on the persistent kernel and on the preconditioned loop)."""
+    p = synth.street_loop(120, 5000, seed=87)
+    st, S, rhs, _, _ = oracle.reduced_system(p, 1e-1, BaConfig(), step=False)
+    diag, edges, off, b = reference_layout(S, rhs)
+    for kw in ({}, dict(clusters=[])):
+        x1, it1, rr1 = solver.reduced_solve(diag, edges, off, b, 1e-6, 500, **kw)
+        x2, it2, _ = solver.reduced_solve(2 * diag, edges, 2 * off, b, 1e-6, 500, **kw)
+        assert rr1 <= 1e-6
+        assert np.abs(2 * x2 - x1).max() <= 1e-4 * np.abs(x1).max()
+        _, it3, rr3 = solver.reduced_solve(diag, edges, off, b, 1e-6, 4, **kw)
+        assert it3 == 4 and rr3 > 1e-6
+        _, it4, rr4 = solver.reduced_solve(diag, edges, off, b, 1e-6, 500, **kw)
+        assert it4 == it1 and rr4 <= 1e-6

@@ -246,30 +246,37 @@ __device__ __forceinline__ uint32_t rp_row() {
   return (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 }
 
-// q_R = the row's partial slots in order; the row's p.q; then alpha.
-__global__ void k_rp_rowsum(Dev d, RpData rp) {
+// q_R = the sum of the row's partial slots; the row's p.q; then alpha.  One
+// block per tile row: kRowGroups groups of the row's 48 entries, group g
+// adding slots g, g + kRowGroups, ... in order (coalesced across the entries),
+// then the groups in order -- a fixed order, with enough threads in flight for
+// rows of many slots.
+constexpr int kRowGroups = 5;
+__global__ void __launch_bounds__(kRow * kRowGroups) k_rp_rowsum(Dev d, RpData rp) {
   if (rp_done(rp)) return;
-  const uint32_t lane = threadIdx.x & 31u, R = rp_row();
-  if (R < d.num_tile_rows) {
+  __shared__ float part[kRowGroups][kRow];
+  __shared__ double pqs[kRow];
+  const uint32_t R = blockIdx.x;
+  const uint32_t c = threadIdx.x % kRow, g = threadIdx.x / kRow;
+  const uint32_t m0 = d.tr_list_off[R], m1 = d.tr_list_off[R + 1];
+  float acc = 0.0f;
+  for (uint32_t m = m0 + g; m < m1; m += kRowGroups) acc += d.partial[(size_t)m * kRow + c];
+  part[g][c] = acc;
+  __syncthreads();
+  if (threadIdx.x < (uint32_t)kRow) {
+    float q = 0.0f;
+#pragma unroll
+    for (int k = 0; k < kRowGroups; ++k) q += part[k][c];
     const size_t base = (size_t)R * kRow;
-    const bool e1 = lane + 32u < (uint32_t)kRow;
-    const uint32_t m0 = d.tr_list_off[R], m1 = d.tr_list_off[R + 1];
-    float q0 = 0.0f, q1 = 0.0f;
-    for (uint32_t m = m0; m < m1; ++m) {
-      q0 += d.partial[(size_t)m * kRow + lane];
-      if (e1) q1 += d.partial[(size_t)m * kRow + 32 + lane];
-    }
-    d.q[base + lane] = q0;
-    double pq = (double)d.p[base + lane] * (double)q0;
-    if (e1) {
-      d.q[base + 32 + lane] = q1;
-      pq += (double)d.p[base + 32 + lane] * (double)q1;
-    }
-    pq = warp_sum_d(pq);
-    if (lane == 0) {
-      rp.dots[R] = pq;
-      __threadfence();
-    }
+    d.q[base + c] = q;
+    pqs[c] = (double)d.p[base + c] * (double)q;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double pq = 0.0;
+    for (int e = 0; e < kRow; ++e) pq += pqs[e];
+    rp.dots[R] = pq;
+    __threadfence();
   }
   rp_arrive(d, rp, kRpAlpha);
 }
@@ -596,7 +603,7 @@ cudaError_t launch_rp_iteration(const Dev& d, const RpData& rp, cudaStream_t s) 
   const int tiles_grid =
       (int)std::min<uint32_t>((d.num_tiles + kMatvecWarps - 1) / kMatvecWarps, 148 * 3);
   k_rp_matvec<<<std::max(1, tiles_grid), kMatvecWarps * 32, kMatvecSmem, s>>>(d, rp);
-  k_rp_rowsum<<<rows_grid(d), 256, 0, s>>>(d, rp);
+  k_rp_rowsum<<<d.num_tile_rows, kRow * kRowGroups, 0, s>>>(d, rp);
   k_rp_update_xr<<<rows_grid(d), 256, 0, s>>>(d, rp);
   precondition_rest(d, rp, s);
   k_rp_prolong_rz<<<rows_grid(d), 256, 0, s>>>(d, rp, kRpBeta);
