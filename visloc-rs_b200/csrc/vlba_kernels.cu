@@ -1165,61 +1165,58 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
-// Per-problem scalars computed by one warp (every lane returns the same
-// values): the sums over the problem's tile rows in lane-strided order and a
-// butterfly; the sticky flag is read once and broadcast.
-__device__ ProbScal prob_scalars_warp(const Dev& d, uint32_t P, int k) {
+// Sums of a problem's tile-row dots (rz(k-1), rz(k-2), rr(k-1), pq(k-1), b2)
+// in one fixed order: the rows are dealt to kSumSlots slots -- row
+// t0 + 32 (w + kSumSlots i) + l to lane l of slot w -- each lane adds its rows
+// in ascending order (two rows' loads ahead of their adds), a butterfly sums
+// the slot, and the slots are added in order.  A block computes the slots on
+// its warps at once (the block's scalars), one warp computes them in turn:
+// the same sums, so every block takes the same decisions.
+constexpr int kSumSlots = 8;
+__device__ __forceinline__ void dot_sums_slot(const Dev& d, int k, uint32_t t0, uint32_t t1,
+                                              uint32_t w, double (&v)[5]) {
   const uint32_t lane = threadIdx.x & 31u;
-  const uint32_t t0 = d.prob_tr_begin[P], t1 = d.prob_tr_begin[P + 1];
-  double v[5] = {0, 0, 0, 0, 0};  // rz(k-1), rz(k-2), rr(k-1), pq(k-1), b2
   const double* q0 = dot_at(d, kDotRz + mod3(k - 1), 0);
   const double* q1 = dot_at(d, kDotRz + mod3(k - 2), 0);
   const double* q2 = dot_at(d, kDotRr + mod3(k - 1), 0);
   const double* q3 = dot_at(d, kDotPq + ((k - 1) & 1), 0);
   const double* q4 = dot_at(d, kDotB2, 0);
-  // Lane l adds rows t0 + l, t0 + l + 32, ... in ascending order, four rows'
-  // loads issued before their adds (a problem of many tile rows otherwise
-  // makes the sums a chain of L2 round trips).
-  uint32_t tr = t0 + lane;
-  for (; tr + 96 < t1; tr += 128) {
-    const double a00 = __ldcg(q0 + tr), a01 = __ldcg(q1 + tr), a02 = __ldcg(q2 + tr),
-                 a03 = __ldcg(q3 + tr), a04 = __ldcg(q4 + tr);
-    const double a10 = __ldcg(q0 + tr + 32), a11 = __ldcg(q1 + tr + 32), a12 = __ldcg(q2 + tr + 32),
-                 a13 = __ldcg(q3 + tr + 32), a14 = __ldcg(q4 + tr + 32);
-    const double a20 = __ldcg(q0 + tr + 64), a21 = __ldcg(q1 + tr + 64), a22 = __ldcg(q2 + tr + 64),
-                 a23 = __ldcg(q3 + tr + 64), a24 = __ldcg(q4 + tr + 64);
-    const double a30 = __ldcg(q0 + tr + 96), a31 = __ldcg(q1 + tr + 96), a32 = __ldcg(q2 + tr + 96),
-                 a33 = __ldcg(q3 + tr + 96), a34 = __ldcg(q4 + tr + 96);
-    v[0] += a00;
-    v[1] += a01;
-    v[2] += a02;
-    v[3] += a03;
-    v[4] += a04;
-    v[0] += a10;
-    v[1] += a11;
-    v[2] += a12;
-    v[3] += a13;
-    v[4] += a14;
-    v[0] += a20;
-    v[1] += a21;
-    v[2] += a22;
-    v[3] += a23;
-    v[4] += a24;
-    v[0] += a30;
-    v[1] += a31;
-    v[2] += a32;
-    v[3] += a33;
-    v[4] += a34;
+  constexpr uint32_t kStep = 32 * kSumSlots;
+  double a[5] = {0, 0, 0, 0, 0};
+  uint32_t tr = t0 + 32 * w + lane;
+  for (; tr + kStep < t1; tr += 2 * kStep) {
+    const double x0 = __ldcg(q0 + tr), x1 = __ldcg(q1 + tr), x2 = __ldcg(q2 + tr),
+                 x3 = __ldcg(q3 + tr), x4 = __ldcg(q4 + tr);
+    const double y0 = __ldcg(q0 + tr + kStep), y1 = __ldcg(q1 + tr + kStep),
+                 y2 = __ldcg(q2 + tr + kStep), y3 = __ldcg(q3 + tr + kStep),
+                 y4 = __ldcg(q4 + tr + kStep);
+    a[0] += x0;
+    a[1] += x1;
+    a[2] += x2;
+    a[3] += x3;
+    a[4] += x4;
+    a[0] += y0;
+    a[1] += y1;
+    a[2] += y2;
+    a[3] += y3;
+    a[4] += y4;
   }
-  for (; tr < t1; tr += 32) {
-    v[0] += __ldcg(q0 + tr);
-    v[1] += __ldcg(q1 + tr);
-    v[2] += __ldcg(q2 + tr);
-    v[3] += __ldcg(q3 + tr);
-    v[4] += __ldcg(q4 + tr);
+  if (tr < t1) {
+    a[0] += __ldcg(q0 + tr);
+    a[1] += __ldcg(q1 + tr);
+    a[2] += __ldcg(q2 + tr);
+    a[3] += __ldcg(q3 + tr);
+    a[4] += __ldcg(q4 + tr);
   }
 #pragma unroll
-  for (int e = 0; e < 5; ++e) v[e] = warp_sum(v[e]);
+  for (int e = 0; e < 5; ++e) v[e] = warp_sum(a[e]);
+}
+
+// Per-problem scalars from the sums of dot_sums_slot (every lane of the
+// calling warp returns the same values); the sticky flag is read once and
+// broadcast.
+__device__ ProbScal prob_scalars_from(const Dev& d, uint32_t P, int k, const double (&v)[5]) {
+  const uint32_t lane = threadIdx.x & 31u;
   int sticky = 0;
   if (lane == 0) sticky = (int)*(volatile uint32_t*)&d.pcg[P].active;
   sticky = __shfl_sync(0xffffffffu, sticky, 0);
@@ -1251,6 +1248,19 @@ __device__ ProbScal prob_scalars_warp(const Dev& d, uint32_t P, int k) {
     }
   }
   return s;
+}
+
+// The same scalars computed by one warp alone, the slots in turn.
+__device__ ProbScal prob_scalars_warp(const Dev& d, uint32_t P, int k) {
+  const uint32_t t0 = d.prob_tr_begin[P], t1 = d.prob_tr_begin[P + 1];
+  double tot[5] = {0, 0, 0, 0, 0};
+  for (uint32_t w = 0; w < (uint32_t)kSumSlots; ++w) {
+    double v[5];
+    dot_sums_slot(d, k, t0, t1, w, v);
+#pragma unroll
+    for (int e = 0; e < 5; ++e) tot[e] += v[e];
+  }
+  return prob_scalars_from(d, P, k, tot);
 }
 
 // Fixed-order sum of a double over the block: butterfly per warp, then the
@@ -1366,11 +1376,26 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
   bool ok = true;
 
   // Block-level per-problem scalars (cached per problem and iteration).
+  // The block's scalars of problem P: each warp sums one slot of the rows'
+  // dots, warp 0 adds the slots in order (the sums of prob_scalars_warp).
+  static_assert(NW >= kSumSlots, "a warp per slot of the scalar sums");
+  __shared__ double s_slot[kSumSlots][5];
   auto scal = [&](uint32_t P, int k) {
     if (sc_prob == P && sc_k == k) return;  // uniform: shared values
     __syncthreads();
+    if (warp < (uint32_t)kSumSlots) {
+      double v[5];
+      dot_sums_slot(d, k, d.prob_tr_begin[P], d.prob_tr_begin[P + 1], warp, v);
+      if (lane == 0)
+        for (int e = 0; e < 5; ++e) s_slot[warp][e] = v[e];
+    }
+    __syncthreads();
     if (warp == 0) {
-      const ProbScal s = prob_scalars_warp(d, P, k);
+      double tot[5] = {0, 0, 0, 0, 0};
+      for (int w = 0; w < kSumSlots; ++w)
+#pragma unroll
+        for (int e = 0; e < 5; ++e) tot[e] += s_slot[w][e];
+      const ProbScal s = prob_scalars_from(d, P, k, tot);
       if (lane == 0) {
         sc = s;
         sc_prob = P;
@@ -1525,12 +1550,17 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
     trace_mark(d, k, 0);
     // ---- A: status of the problems whose first tile row this block owns
     // (by that row's warp), then the warps' tiles.
+    // The block's scalars of its first tile's problem first: the owner of
+    // that problem (the single-problem case) reads them from there.
+    if (NW > 0) {
+      if (gw0 < ntiles) scal(d.tile_meta[gw0].w, k);
+    }
     for (uint32_t j = warp; j < nown; j += NW) {
       const uint32_t tr = blockIdx.x + j * G;
       const uint32_t P = own_prob[j];
       if (d.prob_tr_begin[P] != tr) continue;  // owner = first tile row
       if (!*(volatile uint32_t*)&d.pcg[P].active) continue;
-      const ProbScal ps = prob_scalars_warp(d, P, k);
+      const ProbScal ps = (sc_prob == P && sc_k == k) ? sc : prob_scalars_warp(d, P, k);
       if (!ps.active && lane == 0) {
         PcgState& st = d.pcg[P];
         st.iters = ps.iters;
@@ -1543,11 +1573,6 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
         atomicSub(d.barrier + 2, 1u);
       }
       __syncwarp();
-    }
-    // The block computes the scalars of its first tile's problem once; warps
-    // whose tile is of that problem read them from shared memory.
-    if (NW > 0) {
-      if (gw0 < ntiles) scal(d.tile_meta[gw0].w, k);
     }
     trace_mark(d, k, 1);
     {
