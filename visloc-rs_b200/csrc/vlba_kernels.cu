@@ -1263,6 +1263,31 @@ __device__ ProbScal prob_scalars_warp(const Dev& d, uint32_t P, int k) {
   return prob_scalars_from(d, P, k, tot);
 }
 
+// p.q(k) of a problem in the same slot order as dot_sums_slot: slot w's
+// lane-strided sum (two rows' loads ahead of their adds) and butterfly.
+__device__ __forceinline__ double pq_slot(const Dev& d, int k, uint32_t t0, uint32_t t1,
+                                          uint32_t w) {
+  const double* q = dot_at(d, kDotPq + (k & 1), 0);
+  constexpr uint32_t kStep = 32 * kSumSlots;
+  double a = 0.0;
+  uint32_t tr = t0 + 32 * w + (threadIdx.x & 31u);
+  for (; tr + kStep < t1; tr += 2 * kStep) {
+    const double x = __ldcg(q + tr), y = __ldcg(q + tr + kStep);
+    a += x;
+    a += y;
+  }
+  if (tr < t1) a += __ldcg(q + tr);
+  return warp_sum(a);
+}
+
+// The same p.q computed by one warp alone, the slots in turn.
+__device__ double pq_warp(const Dev& d, uint32_t P, int k) {
+  const uint32_t t0 = d.prob_tr_begin[P], t1 = d.prob_tr_begin[P + 1];
+  double pq = 0.0;
+  for (uint32_t w = 0; w < (uint32_t)kSumSlots; ++w) pq += pq_slot(d, k, t0, t1, w);
+  return pq;
+}
+
 // Fixed-order sum of a double over the block: butterfly per warp, then the
 // warps in order (result valid in every thread).
 template <int NW>
@@ -1824,7 +1849,19 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
     if (*(volatile unsigned int*)(d.barrier + 2) == 0u) break;  // every problem done
 
     // ---- C, one warp per owned row: alpha = rz / p.q of the row's
-    // problem; x, r, z updates; the row's r.z and r.r.
+    // problem; x, r, z updates; the row's r.z and r.r.  The p.q of the
+    // block's own problem is summed by the block's warps, one slot each
+    // (the sums of pq_warp, which the warps use for other problems).
+    const bool own_sc = sc_k == k && sc_prob != kNone;
+    if (own_sc) {
+      __syncthreads();
+      if (warp < (uint32_t)kSumSlots) {
+        const double v = pq_slot(d, k, d.prob_tr_begin[sc_prob], d.prob_tr_begin[sc_prob + 1],
+                                 warp);
+        if (lane == 0) s_slot[warp][0] = v;
+      }
+      __syncthreads();
+    }
     uint32_t cprob = kNone;
     double alpha = 0.0;
     for (uint32_t j = warp; j < nown; j += NW) {
@@ -1833,22 +1870,14 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
       if (P != cprob) {
         // The block's scalars of this iteration when they are this problem's
         // (the single-problem case), else this warp's own.
-        const ProbScal ps = (sc_prob == P && sc_k == k) ? sc : prob_scalars_warp(d, P, k);
-        // Rows in the plain loop's order, four rows' loads ahead of their adds.
-        const double* pqd = dot_at(d, kDotPq + (k & 1), 0);
-        const uint32_t pt1 = d.prob_tr_begin[P + 1];
+        const bool mine = own_sc && sc_prob == P;
+        const ProbScal ps = mine ? sc : prob_scalars_warp(d, P, k);
         double pq = 0.0;
-        uint32_t t2 = d.prob_tr_begin[P] + lane;
-        for (; t2 + 96 < pt1; t2 += 128) {
-          const double a0 = __ldcg(pqd + t2), a1 = __ldcg(pqd + t2 + 32),
-                       a2 = __ldcg(pqd + t2 + 64), a3 = __ldcg(pqd + t2 + 96);
-          pq += a0;
-          pq += a1;
-          pq += a2;
-          pq += a3;
+        if (mine) {
+          for (int w = 0; w < kSumSlots; ++w) pq += s_slot[w][0];
+        } else {
+          pq = pq_warp(d, P, k);
         }
-        for (; t2 < pt1; t2 += 32) pq += __ldcg(pqd + t2);
-        pq = warp_sum(pq);
         alpha = (ps.active && pq > 0.0 && isfinite(pq)) ? ps.rz / pq : 0.0;
         cprob = P;
       }
