@@ -1254,7 +1254,9 @@ __device__ ProbScal prob_scalars_from(const Dev& d, uint32_t P, int k, const dou
 __device__ ProbScal prob_scalars_warp(const Dev& d, uint32_t P, int k) {
   const uint32_t t0 = d.prob_tr_begin[P], t1 = d.prob_tr_begin[P + 1];
   double tot[5] = {0, 0, 0, 0, 0};
-  for (uint32_t w = 0; w < (uint32_t)kSumSlots; ++w) {
+  // Slots past the problem's last row hold no rows: left out (as the block
+  // form leaves them out), so a problem of few rows costs one slot.
+  for (uint32_t w = 0; w < (uint32_t)kSumSlots && t0 + 32 * w < t1; ++w) {
     double v[5];
     dot_sums_slot(d, k, t0, t1, w, v);
 #pragma unroll
@@ -1284,7 +1286,8 @@ __device__ __forceinline__ double pq_slot(const Dev& d, int k, uint32_t t0, uint
 __device__ double pq_warp(const Dev& d, uint32_t P, int k) {
   const uint32_t t0 = d.prob_tr_begin[P], t1 = d.prob_tr_begin[P + 1];
   double pq = 0.0;
-  for (uint32_t w = 0; w < (uint32_t)kSumSlots; ++w) pq += pq_slot(d, k, t0, t1, w);
+  for (uint32_t w = 0; w < (uint32_t)kSumSlots && t0 + 32 * w < t1; ++w)
+    pq += pq_slot(d, k, t0, t1, w);
   return pq;
 }
 
@@ -1417,7 +1420,8 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
     __syncthreads();
     if (warp == 0) {
       double tot[5] = {0, 0, 0, 0, 0};
-      for (int w = 0; w < kSumSlots; ++w)
+      const uint32_t t0 = d.prob_tr_begin[P], t1 = d.prob_tr_begin[P + 1];
+      for (uint32_t w = 0; w < (uint32_t)kSumSlots && t0 + 32 * w < t1; ++w)
 #pragma unroll
         for (int e = 0; e < 5; ++e) tot[e] += s_slot[w][e];
       const ProbScal s = prob_scalars_from(d, P, k, tot);
@@ -1874,7 +1878,9 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
         const ProbScal ps = mine ? sc : prob_scalars_warp(d, P, k);
         double pq = 0.0;
         if (mine) {
-          for (int w = 0; w < kSumSlots; ++w) pq += s_slot[w][0];
+          const uint32_t t0 = d.prob_tr_begin[P], t1 = d.prob_tr_begin[P + 1];
+          for (uint32_t w = 0; w < (uint32_t)kSumSlots && t0 + 32 * w < t1; ++w)
+            pq += s_slot[w][0];
         } else {
           pq = pq_warp(d, P, k);
         }
