@@ -100,8 +100,21 @@ struct ElimDev {
   const uint32_t* run_edges;   // [num_run]
   double* run_out;             // [36 num_run]
   double* coarse_out;          // [36 m m]
+  // The structure's pair index, built on the device: per node its blocks in
+  // point order, each block's point and the points' block ranges; per edge
+  // a count (then a write cursor); the pairs written; an error flag.
+  const uint32_t* slot_off;    // [n + 1]
+  const uint32_t* slot_obs;    // [num_obs]
+  const uint32_t* point_off;   // [num_points + 1]
+  const uint32_t* point_nodes; // [num_obs]
+  uint32_t* cursor;            // [num_edges]
+  uint2* pairs_out;            // [pairs]
+  unsigned int* err;           // bit 0: a pair of a point's nodes has no edge
 };
 
+// The pair index: write = false counts each edge's pairs into cursor (zeroed
+// first); write = true writes them at cursor (set to the edges' offsets).
+cudaError_t launch_el_index(const ElimDev& e, bool write, cudaStream_t s);
 cudaError_t launch_el_prepare(const ElimDev& e, cudaStream_t s);
 cudaError_t launch_el_blocks(const ElimDev& e, cudaStream_t s);
 cudaError_t launch_el_outputs(const ElimDev& e, cudaStream_t s);

@@ -1186,8 +1186,9 @@ std::string build_elimination_index(uint32_t n, const uint32_t* edges, uint64_t 
   for (uint32_t s = 0; s < n; ++s) X.row_off[s + 1] += X.row_off[s];
   const uint32_t T = std::max(1u, std::min<uint32_t>(std::thread::hardware_concurrency(), 64u));
   auto plo = [&](uint32_t t) { return (uint32_t)((uint64_t)num_points * t / T); };
-  // Pairs per point, each point's nodes checked.
-  std::vector<uint64_t> base((size_t)num_points + 1, 0);
+  // Each point's nodes checked; its blocks' point.
+  X.obs_point.resize(nobs);
+  X.point_off.resize((size_t)num_points + 1);
   std::vector<std::string> err(T);
   run_threads(T, [&](uint32_t t) {
     for (uint32_t p = plo(t); p < plo(t + 1) && err[t].empty(); ++p) {
@@ -1196,63 +1197,24 @@ std::string build_elimination_index(uint32_t n, const uint32_t* edges, uint64_t 
         err[t] = "point_off is not ascending at point " + std::to_string(p);
         break;
       }
-      for (uint64_t i = a; i < b; ++i)
+      X.point_off[p] = (uint32_t)a;
+      for (uint64_t i = a; i < b; ++i) {
         if (point_nodes[i] >= n || (i > a && point_nodes[i] <= point_nodes[i - 1])) {
           err[t] = "nodes of point " + std::to_string(p) + " are not ascending below n";
           break;
         }
-      base[p + 1] = (b - a) * (b - a - (b > a ? 1 : 0)) / 2;
-    }
-  });
-  for (auto& e : err)
-    if (!e.empty()) return e;
-  for (uint32_t p = 0; p < num_points; ++p) base[p + 1] += base[p];
-  const uint64_t npairs = base[num_points];
-  if (npairs >= (1ull << 32)) return "too many point pairs";
-  // Each pair's edge (binary search in row s) and observations, point-major.
-  std::vector<uint32_t, NoInit<uint32_t>> key(npairs), rec(2 * npairs);
-  run_threads(T, [&](uint32_t t) {
-    for (uint32_t p = plo(t); p < plo(t + 1) && err[t].empty(); ++p) {
-      const uint64_t a = point_off[p], b = point_off[p + 1];
-      uint64_t w = base[p];
-      for (uint64_t k = a; k < b; ++k) {
-        const uint32_t s = point_nodes[k];
-        const uint32_t* lo = X.edge_t.data() + X.row_off[s];
-        const uint32_t* hi = X.edge_t.data() + X.row_off[s + 1];
-        for (uint64_t j = k + 1; j < b; ++j) {
-          const uint32_t tn = point_nodes[j];
-          lo = std::lower_bound(lo, hi, tn);  // partners ascend: search on from the last
-          if (lo == hi || *lo != tn) {
-            err[t] = "nodes " + std::to_string(s) + " and " + std::to_string(tn) + " of point " +
-                     std::to_string(p) + " have no edge";
-            return;
-          }
-          key[w] = (uint32_t)(lo - X.edge_t.data());
-          rec[2 * w] = (uint32_t)k;
-          rec[2 * w + 1] = (uint32_t)j;
-          ++w;
-        }
+        X.obs_point[i] = p;
       }
     }
   });
   for (auto& e : err)
     if (!e.empty()) return e;
-  // Stable by edge: within an edge the pairs keep ascending point order.
-  std::vector<uint32_t, NoInit<uint32_t>> order(npairs);
-  X.pair_off.resize(ne + 1);
-  counting_sort((uint32_t)npairs, (uint32_t)ne, T, [&](uint32_t i) { return key[i]; }, 0u,
-                order.data(), X.pair_off.data());
-  X.pairs.resize(2 * npairs);
-  X.obs_point.resize(nobs);
-  run_threads(T, [&](uint32_t t) {
-    const uint64_t i0 = npairs * t / T, i1 = npairs * (t + 1) / T;
-    for (uint64_t i = i0; i < i1; ++i) {
-      X.pairs[2 * i] = rec[2 * (size_t)order[i]];
-      X.pairs[2 * i + 1] = rec[2 * (size_t)order[i] + 1];
-    }
-    for (uint32_t p = plo(t); p < plo(t + 1); ++p)
-      for (uint64_t o = point_off[p]; o < point_off[p + 1]; ++o) X.obs_point[o] = p;
-  });
+  X.point_off[num_points] = (uint32_t)nobs;
+  // Per node, its blocks in index (= point) order: a stable counting sort.
+  X.slot_obs.resize(nobs);
+  X.slot_off.resize((size_t)n + 1);
+  counting_sort((uint32_t)nobs, n, T, [&](uint32_t i) { return point_nodes[i]; }, 0u,
+                X.slot_obs.data(), X.slot_off.data());
   return "";
 }
 

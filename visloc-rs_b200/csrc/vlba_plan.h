@@ -150,26 +150,27 @@ void build_plan(const vlba_problem* const* problems, const vlba_config* const* c
 void build_reduced_plan(uint32_t n, const uint32_t* edges, uint64_t ne, uint32_t tb,
                         const LmParams& params, Plan* plan);
 
-// The pair index of a point elimination (ReducedSolveAccelerator::eliminate):
-// per edge (s, t) of the sorted edge list, the observation pairs (o_s, o_t) of
-// the points whose nodes include both s and t, in ascending point order.
+// The structure of a point elimination (ReducedSolveAccelerator::eliminate)
+// from which the device builds its pair index: the sorted edges by first
+// node, and per node its camera-point blocks in ascending point order.
 struct ElimIndex {
   uint32_t n = 0;
   uint32_t num_points = 0;
   uint64_t num_edges = 0;
   uint64_t num_obs = 0;
-  std::vector<uint32_t> row_off;                 // [n + 1] edges (s, _)
-  std::vector<uint32_t> edge_t;                  // [num_edges] second node
-  std::vector<uint32_t> pair_off;                // [num_edges + 1]
-  std::vector<uint32_t, NoInit<uint32_t>> pairs; // [2 pairs] (o_s, o_t)
+  std::vector<uint32_t> row_off;                      // [n + 1] edges (s, _)
+  std::vector<uint32_t> edge_t;                       // [num_edges] second node
+  std::vector<uint32_t> slot_off;                     // [n + 1]
+  std::vector<uint32_t, NoInit<uint32_t>> slot_obs;   // [num_obs] blocks by node, then point
   std::vector<uint32_t, NoInit<uint32_t>> obs_point;  // [num_obs]
+  std::vector<uint32_t> point_off;                    // [num_points + 1] (32-bit)
 };
 
-// Builds the index of n nodes, ne sorted edges and num_points points (their
-// nodes point_nodes[point_off[p] .. point_off[p + 1]], ascending) on the
-// host's threads.  Returns an empty string, or the first inconsistency found
-// (unsorted edges, a node out of range, a pair of nodes with no edge, a size
-// past the 32-bit indices).
+// Builds it for n nodes, ne sorted edges and num_points points (their nodes
+// point_nodes[point_off[p] .. point_off[p + 1]], ascending) on the host's
+// threads.  Returns an empty string, or the first inconsistency found
+// (unsorted edges, a node out of range or out of order, a size past the
+// 32-bit indices); a pair of nodes with no edge is found on the device.
 std::string build_elimination_index(uint32_t n, const uint32_t* edges, uint64_t ne,
                                     uint32_t num_points, const uint64_t* point_off,
                                     const uint32_t* point_nodes, ElimIndex* out);

@@ -443,6 +443,47 @@ __global__ void k_rp_update_p(Dev d, RpData rp, int first) {
 }
 
 // ---------------------------------------------------------------- elimination
+// The pair index of a structure: one warp per node s walks the node's blocks
+// x in point order, the lanes over the later blocks y of x's point (nodes
+// ascend within a point, so these are its partners t > s); each pair (x, y)
+// belongs to edge (s, t), found by binary search in s's edges.  Counting
+// (atomics: the totals do not depend on order), then writing at the edge's
+// cursor: the partners of one x are distinct edges, and only s's warp
+// touches s's edges, so each edge's pairs land in point order with no race.
+template <bool WRITE>
+__global__ void __launch_bounds__(256) k_el_index(ElimDev E) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t nw = gridDim.x * blockDim.x / 32u;
+  for (uint32_t s = (blockIdx.x * blockDim.x + threadIdx.x) / 32u; s < E.n; s += nw) {
+    const uint32_t e0 = E.row_off[s], e1 = E.row_off[s + 1];
+    for (uint32_t q = E.slot_off[s]; q < E.slot_off[s + 1]; ++q) {
+      const uint32_t x = E.slot_obs[q];
+      const uint32_t y1 = E.point_off[E.obs_point[x] + 1];
+      for (uint32_t y = x + 1 + lane; y < y1; y += 32) {
+        const uint32_t t = E.point_nodes[y];
+        uint32_t lo = e0, hi = e1;
+        while (lo < hi) {
+          const uint32_t mid = (lo + hi) / 2;
+          if (E.edge_t[mid] < t) lo = mid + 1;
+          else hi = mid;
+        }
+        if (lo == e1 || E.edge_t[lo] != t) {
+          atomicOr(E.err, 1u);
+          continue;
+        }
+        if (WRITE) {
+          const uint32_t pos = E.cursor[lo];
+          E.cursor[lo] = pos + 1;
+          E.pairs_out[pos] = make_uint2(x, y);
+        } else {
+          atomicAdd(E.cursor + lo, 1u);
+        }
+      }
+      __syncwarp();  // this x's cursor updates before the next x's reads
+    }
+  }
+}
+
 // Per camera-point block o of point p: an FP32 copy of hcp and sk = hcp V_p^-1
 // (formed in FP64; zero for a point left out, whose pairs then add zero).
 // One thread per entry q = 6 i + r of the 6x3 outputs, so that consecutive
@@ -608,6 +649,13 @@ cudaError_t launch_rp_iteration(const Dev& d, const RpData& rp, cudaStream_t s) 
   precondition_rest(d, rp, s);
   k_rp_prolong_rz<<<rows_grid(d), 256, 0, s>>>(d, rp, kRpBeta);
   k_rp_update_p<<<flat_grid((size_t)d.num_var_cams * 6), 256, 0, s>>>(d, rp, 0);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_el_index(const ElimDev& e, bool write, cudaStream_t s) {
+  const int g = (int)std::min<uint32_t>((e.n + 7) / 8, 148 * 16);
+  if (write) k_el_index<true><<<std::max(1, g), 256, 0, s>>>(e);
+  else k_el_index<false><<<std::max(1, g), 256, 0, s>>>(e);
   return cudaGetLastError();
 }
 

@@ -93,7 +93,8 @@ struct ElimState {
   uint32_t n = 0, num_points = 0;
   uint64_t num_edges = 0, num_obs = 0, num_pairs = 0;
   std::vector<uint32_t> edges;  // the structure's edges (2 per edge), for the solve's check
-  DeviceArray row_off, edge_t, pair_off, pairs, obs_point;
+  DeviceArray row_off, edge_t, pair_off, pairs, obs_point, slot_off, slot_obs, point_off32,
+      point_nodes, cursor, flag;
   DeviceArray hcp64, hcp32, sk32, vinv64, used, extra_of, extra64, blocks, run_edges, run_out,
       coarse_out;
 };
@@ -2252,21 +2253,66 @@ bool reduced_eliminate(Context* c, const vlba_point_elimination* el, double* run
     const std::string bad =
         build_elimination_index(n, el->edges, ne, P, el->point_off, el->point_nodes, &X);
     if (!bad.empty()) throw Status(VLBA_ERR_INVALID_ARGUMENT, bad);
-    E.num_pairs = X.pairs.size() / 2;
+    // The structure on the device; its pair index built there: counts per
+    // edge, their prefix here, then the pairs at each edge's cursor.
     E.row_off.ensure(4 * X.row_off.size());
     E.edge_t.ensure(4 * ne);
-    E.pair_off.ensure(4 * X.pair_off.size());
-    E.pairs.ensure(4 * X.pairs.size());
+    E.slot_off.ensure(4 * X.slot_off.size());
+    E.slot_obs.ensure(4 * nobs);
     E.obs_point.ensure(4 * nobs);
-    VLBA_CUDA(cudaMemcpyAsync(E.row_off.p, X.row_off.data(), 4 * X.row_off.size(),
-                              cudaMemcpyHostToDevice, s));
-    VLBA_CUDA(cudaMemcpyAsync(E.edge_t.p, X.edge_t.data(), 4 * ne, cudaMemcpyHostToDevice, s));
-    VLBA_CUDA(cudaMemcpyAsync(E.pair_off.p, X.pair_off.data(), 4 * X.pair_off.size(),
-                              cudaMemcpyHostToDevice, s));
-    VLBA_CUDA(cudaMemcpyAsync(E.pairs.p, X.pairs.data(), 4 * X.pairs.size(),
-                              cudaMemcpyHostToDevice, s));
-    VLBA_CUDA(cudaMemcpyAsync(E.obs_point.p, X.obs_point.data(), 4 * nobs,
-                              cudaMemcpyHostToDevice, s));
+    E.point_off32.ensure(4 * X.point_off.size());
+    E.point_nodes.ensure(4 * nobs);
+    E.pair_off.ensure(4 * (ne + 1));
+    E.cursor.ensure(4 * ne);
+    E.flag.ensure(4);
+    {
+      Stager st(c);
+      st.add(E.row_off.p, X.row_off.data(), 4 * X.row_off.size());
+      st.add(E.edge_t.p, X.edge_t.data(), 4 * ne);
+      st.add(E.slot_off.p, X.slot_off.data(), 4 * X.slot_off.size());
+      st.add(E.slot_obs.p, X.slot_obs.data(), 4 * nobs);
+      st.add(E.obs_point.p, X.obs_point.data(), 4 * nobs);
+      st.add(E.point_off32.p, X.point_off.data(), 4 * X.point_off.size());
+      st.add(E.point_nodes.p, el->point_nodes, 4 * nobs);
+      st.flush(s);
+    }
+    VLBA_CUDA(cudaMemsetAsync(E.cursor.p, 0, 4 * ne, s));
+    VLBA_CUDA(cudaMemsetAsync(E.flag.p, 0, 4, s));
+    ElimDev ix{};
+    ix.n = n;
+    ix.num_points = P;
+    ix.num_edges = ne;
+    ix.num_obs = nobs;
+    ix.row_off = E.row_off.as<const uint32_t>();
+    ix.edge_t = E.edge_t.as<const uint32_t>();
+    ix.slot_off = E.slot_off.as<const uint32_t>();
+    ix.slot_obs = E.slot_obs.as<const uint32_t>();
+    ix.obs_point = E.obs_point.as<const uint32_t>();
+    ix.point_off = E.point_off32.as<const uint32_t>();
+    ix.point_nodes = E.point_nodes.as<const uint32_t>();
+    ix.cursor = E.cursor.as<uint32_t>();
+    ix.err = E.flag.as<unsigned int>();
+    check_launch(launch_el_index(ix, false, s), "elimination index count");
+    std::vector<uint32_t> cnt(ne + 1, 0);
+    unsigned int ierr = 0;
+    VLBA_CUDA(cudaMemcpyAsync(cnt.data(), E.cursor.p, 4 * ne, cudaMemcpyDeviceToHost, s));
+    VLBA_CUDA(cudaMemcpyAsync(&ierr, E.flag.p, 4, cudaMemcpyDeviceToHost, s));
+    VLBA_CUDA(cudaStreamSynchronize(s));
+    if (ierr) throw Status(VLBA_ERR_INVALID_ARGUMENT, "two nodes of a point have no edge");
+    uint64_t total = 0;
+    for (uint64_t e = 0; e < ne; ++e) {
+      const uint32_t k = cnt[e];
+      cnt[e] = (uint32_t)total;
+      total += k;
+    }
+    if (total >= (1ull << 32)) throw Status(VLBA_ERR_INVALID_ARGUMENT, "too many point pairs");
+    cnt[ne] = (uint32_t)total;
+    E.num_pairs = total;
+    E.pairs.ensure(8 * total);
+    VLBA_CUDA(cudaMemcpyAsync(E.pair_off.p, cnt.data(), 4 * (ne + 1), cudaMemcpyHostToDevice, s));
+    VLBA_CUDA(cudaMemcpyAsync(E.cursor.p, cnt.data(), 4 * ne, cudaMemcpyHostToDevice, s));
+    ix.pairs_out = E.pairs.as<uint2>();
+    check_launch(launch_el_index(ix, true, s), "elimination index write");
     E.edges.assign(el->edges, el->edges + 2 * ne);
     E.hcp64.ensure(144 * nobs);
     E.hcp32.ensure(4 * kElRec * nobs);
