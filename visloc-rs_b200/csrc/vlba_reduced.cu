@@ -13,6 +13,12 @@
 // on the device (no host round trip inside an iteration), each returning at
 // once when the solve is over.  Vectors are FP32 as in the persistent PCG,
 // dots FP64; every sum runs in a fixed order, so a solve is deterministic.
+//
+// Also here: the point elimination of ReducedSolveAccelerator::eliminate
+// (ba_accel.rs:74-144) -- the structure's pair index (k_el_index), the
+// FP32 camera-point blocks and their products with the point inverses
+// (k_el_prepare), the per-edge FP64 block sums (k_el_blocks), and the run
+// blocks and coarse aggregate-pair sums returned to the caller.
 #include <cuda_runtime.h>
 
 #include <algorithm>
