@@ -348,3 +348,30 @@ def test_gpu_matches_the_fp64_iteration_on_relative_constraints(solver, n, k, gr
         assert np.linalg.norm(b - S @ x) <= 1.2 * tol * np.linalg.norm(b)
         xr = x_ref.reshape(-1)
         assert np.linalg.norm(x - xr) <= 1e-3 * np.linalg.norm(xr)
+
+
+@pytest.mark.parametrize("k", [7, 8, 16, 32])
+def test_caller_side_helpers_match_the_oracle(k):
+    """visloc_ba.reduced (the caller's preparation of the preconditioners,
+    vectorised) against the oracle's restatements of cluster_inverses,
+    coarse_correction and coarse_from_sums, on the chain and covisibility
+    systems (ragged last runs and aggregates included)."""
+    from visloc_ba import reduced
+
+    for diag, edges, off in (chain_system(100), covisibility_system(64)):
+        want = oracle.cluster_inverses(diag, edges, off, k)
+        got = reduced.cluster_inverses(diag, edges, off, k)
+        assert [s for s, _ in got] == [s for s, _ in want]
+        for (_, a), (_, b) in zip(got, want):
+            np.testing.assert_allclose(a, b, rtol=1e-9, atol=1e-12 * np.abs(b).max())
+        n = len(diag)
+        for nodes, group in ((n, k), (n - 5, k - 1)):
+            want_c = oracle.coarse_correction(diag, edges, off, nodes, group)
+            got_c = reduced.coarse_correction(diag, edges, off, nodes, group)
+            assert got_c[:2] == want_c[:2]
+            np.testing.assert_allclose(got_c[2], want_c[2], rtol=1e-8,
+                                       atol=1e-10 * np.abs(want_c[2]).max())
+            sums = oracle.coarse_block_sums(edges, off, want_c[0], nodes)
+            from_sums = reduced.coarse_from_sums(diag, sums, nodes, want_c[0])
+            np.testing.assert_allclose(from_sums[2], want_c[2], rtol=1e-8,
+                                       atol=1e-10 * np.abs(want_c[2]).max())
