@@ -585,13 +585,19 @@ __global__ void k_el_gather(ElimDev E) {
 
 // coarse_out[g m + h] (g <= h): the sum of the blocks of edges (a, b), a in
 // aggregate g, b in aggregate h, both below coarse_nodes, in node then edge
-// order.  One block per g, one warp per h, lanes over the 36 entries.
+// order.  One warp per aggregate pair (g, h), g <= h, lanes over the 36
+// entries.
 __global__ void __launch_bounds__(256) k_el_coarse(ElimDev E) {
-  const uint32_t g = blockIdx.x, m = E.coarse_m, grp = E.coarse_group;
-  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const uint32_t m = E.coarse_m, grp = E.coarse_group;
+  const uint32_t lane = threadIdx.x & 31u;
   const bool two = lane < 4u;
-  const uint32_t a1 = min((g + 1) * grp, E.coarse_nodes);
-  for (uint32_t h = g + warp; h < m; h += blockDim.x / 32u) {
+  const uint64_t npairs = (uint64_t)m * m;
+  const uint64_t nw = (uint64_t)gridDim.x * blockDim.x / 32u;
+  for (uint64_t gh = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / 32u; gh < npairs;
+       gh += nw) {
+    const uint32_t g = (uint32_t)(gh / m), h = (uint32_t)(gh % m);
+    if (h < g) continue;
+    const uint32_t a1 = min((g + 1) * grp, E.coarse_nodes);
     const uint32_t t0 = h * grp, t1 = min((h + 1) * grp, E.coarse_nodes);
     double acc0 = 0.0, acc1 = 0.0;
     for (uint32_t a = g * grp; a < a1; ++a) {
@@ -607,7 +613,7 @@ __global__ void __launch_bounds__(256) k_el_coarse(ElimDev E) {
         if (two) acc1 += E.blocks[36 * (size_t)e + 32 + lane];
       }
     }
-    double* out = E.coarse_out + 36 * ((size_t)g * m + h);
+    double* out = E.coarse_out + 36 * gh;
     out[lane] = acc0;
     if (two) out[32 + lane] = acc1;
   }
@@ -678,7 +684,9 @@ cudaError_t launch_el_blocks(const ElimDev& e, cudaStream_t s) {
 
 cudaError_t launch_el_outputs(const ElimDev& e, cudaStream_t s) {
   if (e.num_run) k_el_gather<<<flat_grid(36 * e.num_run), 256, 0, s>>>(e);
-  if (e.coarse_m) k_el_coarse<<<e.coarse_m, 256, 0, s>>>(e);
+  if (e.coarse_m)
+    k_el_coarse<<<(int)std::min<uint64_t>(((uint64_t)e.coarse_m * e.coarse_m + 7) / 8, 148 * 16),
+                  256, 0, s>>>(e);
   return cudaGetLastError();
 }
 
