@@ -1261,4 +1261,181 @@ int vlba_oracle_optimize(vlba_problem* p, const vlba_config* cfg, int solver, in
   return VLBA_OK;
 }
 
+// ---------------------------------------------------------------------------
+// pcg_core (pipelines/slam/src/colmap_incremental/rig_ba_solver.rs:1406-1480)
+// on a reduced camera system as ReducedCameraSystem hands it over
+// (ba_accel.rs:50-72): damped diagonal blocks (column-major f64), sorted
+// edges (a, b) with their (row b, column a) blocks (column-major f32, read in
+// f64 with fused multiply-adds as edge_product does, :1314-1331), the run
+// inverses (z over each run, block-Jacobi Cholesky inverses elsewhere) and
+// the additive coarse level (CoarseCorrection::add_to, :1198-1213).  On
+// `threads` OpenMP threads (0: all): each node's product sums its own
+// diagonal, then its edges in edge order; dots add fixed chunks of nodes,
+// then the chunks in order -- the result does not depend on the thread
+// count.  Returns 0 (x and *iterations set), 1 (a non-positive or non-finite
+// p.q: pcg_core's None) or 2 (a diagonal block that is not positive definite:
+// pcg_core's None too).
+int vlba_oracle_reduced_pcg(uint32_t n, uint64_t ne, const uint32_t* edges, const double* diag,
+                            const float* offdiag, const double* rhs, double tol,
+                            uint32_t max_iterations, uint32_t num_clusters,
+                            const uint32_t* cluster_first, const uint32_t* cluster_size,
+                            const double* cluster_inverse, uint32_t coarse_group,
+                            uint32_t coarse_nodes, const double* coarse_inverse, int threads,
+                            double* x, uint32_t* iterations) {
+  if (threads > 0) omp_set_num_threads(threads);
+  const size_t N = 6 * (size_t)n;
+  // Incident edges per node, in edge order (CSR).
+  std::vector<uint64_t> off(n + 1, 0);
+  for (uint64_t e = 0; e < ne; ++e) {
+    ++off[edges[2 * e] + 1];
+    ++off[edges[2 * e + 1] + 1];
+  }
+  for (uint32_t i = 0; i < n; ++i) off[i + 1] += off[i];
+  std::vector<uint64_t> inc(2 * ne), fill(off.begin(), off.end() - 1);
+  for (uint64_t e = 0; e < ne; ++e) {
+    inc[fill[edges[2 * e]]++] = e;
+    inc[fill[edges[2 * e + 1]]++] = e;
+  }
+  // Block-Jacobi inverses (pcg_core factors every diagonal block).
+  std::vector<double> jac(36 * (size_t)n);
+  int bad = 0;
+#pragma omp parallel for schedule(static) reduction(| : bad)
+  for (int64_t i = 0; i < (int64_t)n; ++i) {
+    // d.cholesky().map(|c| c.inverse()): factor, then solve for each column.
+    std::vector<double> a(36);
+    for (int r = 0; r < 6; ++r)
+      for (int c = 0; c < 6; ++c) a[r * 6 + c] = diag[36 * i + c * 6 + r];
+    if (!cholesky(a, 6, 1)) {
+      bad |= 1;
+      continue;
+    }
+    for (int c = 0; c < 6; ++c) {
+      std::vector<double> col(6, 0.0);
+      col[c] = 1.0;
+      cholesky_solve(a, 6, col);
+      for (int r = 0; r < 6; ++r) jac[36 * i + r * 6 + c] = col[r];
+    }
+  }
+  if (bad) return 2;
+  std::vector<uint64_t> cl_off(num_clusters + 1, 0);
+  for (uint32_t c = 0; c < num_clusters; ++c)
+    cl_off[c + 1] = cl_off[c] + 36ull * cluster_size[c] * cluster_size[c];
+  std::vector<uint8_t> in_run(n, 0);
+  for (uint32_t c = 0; c < num_clusters; ++c)
+    for (uint32_t k = 0; k < cluster_size[c]; ++k) in_run[cluster_first[c] + k] = 1;
+  const uint32_t m = coarse_group && coarse_nodes ? (coarse_nodes + coarse_group - 1) / coarse_group
+                                                   : 0;
+  auto matvec = [&](const std::vector<double>& p, std::vector<double>& q) {
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int64_t i = 0; i < (int64_t)n; ++i) {
+      double y[6];
+      for (int r = 0; r < 6; ++r) {
+        double acc = 0.0;
+        for (int c = 0; c < 6; ++c) acc = std::fma(diag[36 * i + c * 6 + r], p[6 * i + c], acc);
+        y[r] = acc;
+      }
+      for (uint64_t k = off[i]; k < off[i + 1]; ++k) {
+        const uint64_t e = inc[k];
+        const float* B = offdiag + 36 * e;  // (row b, column a), column-major
+        if (edges[2 * e + 1] == (uint32_t)i) {  // row b: B p_a
+          const double* pa = &p[6 * (size_t)edges[2 * e]];
+          for (int c = 0; c < 6; ++c)
+            for (int r = 0; r < 6; ++r) y[r] = std::fma((double)B[c * 6 + r], pa[c], y[r]);
+        } else {  // row a: B^T p_b
+          const double* pb = &p[6 * (size_t)edges[2 * e + 1]];
+          for (int c = 0; c < 6; ++c) {
+            double d0 = 0.0;
+            for (int r = 0; r < 6; ++r) d0 = std::fma((double)B[c * 6 + r], pb[r], d0);
+            y[c] += d0;
+          }
+        }
+      }
+      for (int r = 0; r < 6; ++r) q[6 * i + r] = y[r];
+    }
+  };
+  constexpr size_t kChunk = 6 * 256;
+  const size_t nchunks = (N + kChunk - 1) / kChunk;
+  std::vector<double> part(nchunks);
+  auto dot = [&](const std::vector<double>& a, const std::vector<double>& b) {
+#pragma omp parallel for schedule(static)
+    for (int64_t c = 0; c < (int64_t)nchunks; ++c) {
+      double s = 0.0;
+      for (size_t k = c * kChunk; k < std::min(N, (c + 1) * kChunk); ++k) s += a[k] * b[k];
+      part[c] = s;
+    }
+    double s = 0.0;
+    for (size_t c = 0; c < nchunks; ++c) s += part[c];
+    return s;
+  };
+  std::vector<double> rc(6 * (size_t)m), yc(6 * (size_t)m);
+  auto apply = [&](const std::vector<double>& r, std::vector<double>& z) {
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < (int64_t)n; ++i) {
+      if (in_run[i]) continue;
+      for (int a = 0; a < 6; ++a) {
+        double s = 0.0;
+        for (int b = 0; b < 6; ++b) s += jac[36 * i + a * 6 + b] * r[6 * i + b];
+        z[6 * i + a] = s;
+      }
+    }
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t c = 0; c < (int64_t)num_clusters; ++c) {
+      const size_t rows = 6 * (size_t)cluster_size[c], base = 6 * (size_t)cluster_first[c];
+      const double* M = cluster_inverse + cl_off[c];
+      for (size_t row = 0; row < rows; ++row) {
+        double s = 0.0;
+        for (size_t k = 0; k < rows; ++k) s += M[k * rows + row] * r[base + k];
+        z[base + row] = s;
+      }
+    }
+    if (m) {
+      std::fill(rc.begin(), rc.end(), 0.0);
+      for (uint32_t i = 0; i < coarse_nodes; ++i)
+        for (int k = 0; k < 6; ++k) rc[6 * (i / coarse_group) + k] += r[6 * (size_t)i + k];
+      const size_t M6 = 6 * (size_t)m;
+#pragma omp parallel for schedule(static)
+      for (int64_t row = 0; row < (int64_t)M6; ++row) {
+        double s = 0.0;
+        for (size_t k = 0; k < M6; ++k) s += coarse_inverse[k * M6 + row] * rc[k];
+        yc[row] = s;
+      }
+      for (uint32_t i = 0; i < coarse_nodes; ++i)
+        for (int k = 0; k < 6; ++k) z[6 * (size_t)i + k] += yc[6 * (i / coarse_group) + k];
+    }
+  };
+  std::vector<double> b(rhs, rhs + N), r(b), z(N), p(N), q(N), xs(N, 0.0);
+  const double bnorm = std::sqrt(dot(b, b));
+  uint32_t it = 0;
+  if (bnorm == 0.0) {
+    std::memset(x, 0, N * sizeof(double));
+    *iterations = 0;
+    return 0;
+  }
+  apply(r, z);
+  p = z;
+  double rz = dot(r, z);
+  for (uint32_t k = 0; k < max_iterations; ++k) {
+    ++it;
+    matvec(p, q);
+    const double pq = dot(p, q);
+    if (!std::isfinite(pq) || pq <= 0.0) return 1;
+    const double alpha = rz / pq;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < (int64_t)N; ++i) {
+      xs[i] += alpha * p[i];
+      r[i] -= alpha * q[i];
+    }
+    if (std::sqrt(dot(r, r)) <= tol * bnorm) break;
+    apply(r, z);
+    const double rz_next = dot(r, z);
+    const double beta = rz_next / rz;
+    rz = rz_next;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < (int64_t)N; ++i) p[i] = z[i] + beta * p[i];
+  }
+  std::memcpy(x, xs.data(), N * sizeof(double));
+  *iterations = it;
+  return 0;
+}
+
 }  // extern "C"

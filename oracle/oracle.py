@@ -32,6 +32,12 @@ EXPORTS = {
         [P(_abi.Problem), P(_abi.Config), C.c_int, P(C.c_double), P(C.c_uint64)],
     ),
     "vlba_oracle_squared_residuals": (C.c_int, [P(_abi.Problem), P(_abi.Config), P(C.c_double)]),
+    "vlba_oracle_reduced_pcg": (
+        C.c_int,
+        [C.c_uint32, C.c_uint64, P(C.c_uint32), P(C.c_double), P(C.c_float), P(C.c_double),
+         C.c_double, C.c_uint32, C.c_uint32, P(C.c_uint32), P(C.c_uint32), P(C.c_double),
+         C.c_uint32, C.c_uint32, P(C.c_double), C.c_int, P(C.c_double), P(C.c_uint32)],
+    ),
     "vlba_oracle_camera_project": (C.c_int, [P(_abi.Camera), P(C.c_double), P(C.c_double)]),
     "vlba_oracle_mono_project": (
         C.c_int,
@@ -510,3 +516,33 @@ def coarse_from_sums(diag, sums, n_frames: int, group: int):
     except np.linalg.LinAlgError:
         return None
     return group, n_frames, np.linalg.inv(a)
+
+
+def reduced_pcg_threaded(diag, edges, offdiag, rhs, tol: float, max_iterations: int,
+                         clusters=None, coarse=None, threads: int = 0):
+    """pcg_core on the host's threads (the C++ restatement in ba_oracle.cpp):
+    the same iteration as reduced_pcg with the off-diagonal blocks read as
+    f32, as the plug-in receives them.  Returns (x (n, 6), iterations), or
+    None where pcg_core returns None."""
+    diag = np.ascontiguousarray(np.asarray(diag, np.float64).transpose(0, 2, 1))  # column-major
+    off = np.ascontiguousarray(np.asarray(offdiag, np.float32).reshape(-1, 6, 6).transpose(0, 2, 1))
+    e = np.ascontiguousarray(np.asarray(edges, np.uint32).reshape(-1, 2))
+    b = np.ascontiguousarray(np.asarray(rhs, np.float64).reshape(-1))
+    n = diag.shape[0]
+    runs = clusters or []
+    first = np.ascontiguousarray([r[0] for r in runs], np.uint32)
+    size = np.ascontiguousarray([np.shape(r[1])[0] // 6 for r in runs], np.uint32)
+    inv = np.ascontiguousarray(np.concatenate(
+        [np.asarray(r[1], np.float64).T.reshape(-1) for r in runs]) if runs else np.zeros(1))
+    group, nodes, cinv = coarse if coarse is not None else (0, 0, np.zeros((1, 1)))
+    cinv = np.ascontiguousarray(np.asarray(cinv, np.float64).T)
+    x = np.zeros(6 * n)
+    it = C.c_uint32()
+    st = lib().vlba_oracle_reduced_pcg(
+        n, e.shape[0], e.ctypes.data_as(P(C.c_uint32)), _dp(diag), off.ctypes.data_as(P(C.c_float)),
+        _dp(b), float(tol), int(max_iterations), len(runs), first.ctypes.data_as(P(C.c_uint32)),
+        size.ctypes.data_as(P(C.c_uint32)), _dp(inv), int(group), int(nodes), _dp(cinv),
+        int(threads), _dp(x), C.byref(it))
+    if st != 0:
+        return None
+    return x.reshape(n, 6), it.value

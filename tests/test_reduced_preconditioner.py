@@ -375,3 +375,30 @@ def test_caller_side_helpers_match_the_oracle(k):
             from_sums = reduced.coarse_from_sums(diag, sums, nodes, want_c[0])
             np.testing.assert_allclose(from_sums[2], want_c[2], rtol=1e-8,
                                        atol=1e-10 * np.abs(want_c[2]).max())
+
+
+@pytest.mark.parametrize("threads", [1, 4])
+def test_threaded_oracle_iteration_matches_the_numpy_one(threads):
+    """The oracle's threaded C++ pcg_core (the reduced workload's CPU
+    baseline) against its numpy restatement, pinned above to the reference's
+    recorded counts: the chain system with runs of 32 and the coarse level,
+    block-Jacobi on the covisibility system, and the breakdown case."""
+    diag, edges, off = chain_system(600)
+    off32 = off.astype(np.float32).astype(np.float64)
+    b = pattern_rhs(600)
+    runs = oracle.cluster_inverses(diag, edges, off32, 32)
+    coarse = oracle.coarse_correction(diag, edges, off32, 600, 32)
+    for kw in (dict(clusters=runs), dict(clusters=runs, coarse=coarse)):
+        x_np, it_np = oracle.reduced_pcg(diag, edges, off32, b, 1e-8, 500, **kw)
+        x_c, it_c = oracle.reduced_pcg_threaded(diag, edges, off, b, 1e-8, 500, threads=threads,
+                                                **kw)
+        assert abs(it_c - it_np) <= 1, (it_c, it_np)
+        assert np.abs(x_c - x_np).max() <= 1e-6 * np.abs(x_np).max()
+    d2, e2, o2 = covisibility_system(64)
+    b2 = pattern_rhs(64)
+    x_np, it_np = oracle.reduced_pcg(d2, e2, o2.astype(np.float32).astype(np.float64), b2, 1e-10, 500)
+    x_c, it_c = oracle.reduced_pcg_threaded(d2, e2, o2, b2, 1e-10, 500, threads=threads)
+    assert it_c == it_np and np.abs(x_c - x_np).max() <= 1e-9 * np.abs(x_np).max()
+    bad = [np.eye(6), np.eye(6)]
+    assert oracle.reduced_pcg_threaded(bad, np.array([(0, 1)]), np.array([2.0 * np.eye(6)]),
+                                       np.concatenate([np.ones(6), -np.ones(6)]), 1e-8, 50) is None
