@@ -1284,18 +1284,20 @@ int vlba_oracle_reduced_pcg(uint32_t n, uint64_t ne, const uint32_t* edges, cons
                             double* x, uint32_t* iterations) {
   if (threads > 0) omp_set_num_threads(threads);
   const size_t N = 6 * (size_t)n;
-  // Incident edges per node, in edge order (CSR).
-  std::vector<uint64_t> off(n + 1, 0);
+  // Per node its out-edges (a = i, contiguous: edges are sorted) and its
+  // in-edges (b = i), each list in edge order.
+  std::vector<uint64_t> out_off(n + 1, 0), in_off(n + 1, 0);
   for (uint64_t e = 0; e < ne; ++e) {
-    ++off[edges[2 * e] + 1];
-    ++off[edges[2 * e + 1] + 1];
+    ++out_off[edges[2 * e] + 1];
+    ++in_off[edges[2 * e + 1] + 1];
   }
-  for (uint32_t i = 0; i < n; ++i) off[i + 1] += off[i];
-  std::vector<uint64_t> inc(2 * ne), fill(off.begin(), off.end() - 1);
-  for (uint64_t e = 0; e < ne; ++e) {
-    inc[fill[edges[2 * e]]++] = e;
-    inc[fill[edges[2 * e + 1]]++] = e;
+  for (uint32_t i = 0; i < n; ++i) {
+    out_off[i + 1] += out_off[i];
+    in_off[i + 1] += in_off[i];
   }
+  std::vector<uint64_t> in_edge(ne), fill(in_off.begin(), in_off.end() - 1);
+  for (uint64_t e = 0; e < ne; ++e) in_edge[fill[edges[2 * e + 1]]++] = e;
+  std::vector<double> u(6 * ne);  // B p_a per edge, gathered by row b
   // Block-Jacobi inverses (pcg_core factors every diagonal block).
   std::vector<double> jac(36 * (size_t)n);
   int bad = 0;
@@ -1325,6 +1327,9 @@ int vlba_oracle_reduced_pcg(uint32_t n, uint64_t ne, const uint32_t* edges, cons
     for (uint32_t k = 0; k < cluster_size[c]; ++k) in_run[cluster_first[c] + k] = 1;
   const uint32_t m = coarse_group && coarse_nodes ? (coarse_nodes + coarse_group - 1) / coarse_group
                                                    : 0;
+  // Each block read once per product, as edge_product does: row a adds its
+  // out-edges' B^T p_b and leaves B p_a per edge; row b then adds its
+  // in-edges' in edge order.
   auto matvec = [&](const std::vector<double>& p, std::vector<double>& q) {
 #pragma omp parallel for schedule(dynamic, 64)
     for (int64_t i = 0; i < (int64_t)n; ++i) {
@@ -1334,24 +1339,28 @@ int vlba_oracle_reduced_pcg(uint32_t n, uint64_t ne, const uint32_t* edges, cons
         for (int c = 0; c < 6; ++c) acc = std::fma(diag[36 * i + c * 6 + r], p[6 * i + c], acc);
         y[r] = acc;
       }
-      for (uint64_t k = off[i]; k < off[i + 1]; ++k) {
-        const uint64_t e = inc[k];
+      const double* pa = &p[6 * (size_t)i];
+      for (uint64_t e = out_off[i]; e < out_off[i + 1]; ++e) {
         const float* B = offdiag + 36 * e;  // (row b, column a), column-major
-        if (edges[2 * e + 1] == (uint32_t)i) {  // row b: B p_a
-          const double* pa = &p[6 * (size_t)edges[2 * e]];
-          for (int c = 0; c < 6; ++c)
-            for (int r = 0; r < 6; ++r) y[r] = std::fma((double)B[c * 6 + r], pa[c], y[r]);
-        } else {  // row a: B^T p_b
-          const double* pb = &p[6 * (size_t)edges[2 * e + 1]];
-          for (int c = 0; c < 6; ++c) {
-            double d0 = 0.0;
-            for (int r = 0; r < 6; ++r) d0 = std::fma((double)B[c * 6 + r], pb[r], d0);
-            y[c] += d0;
+        const double* pb = &p[6 * (size_t)edges[2 * e + 1]];
+        double tb[6] = {0, 0, 0, 0, 0, 0};
+        for (int c = 0; c < 6; ++c) {
+          double d0 = 0.0;
+          for (int r = 0; r < 6; ++r) {
+            const double v = B[c * 6 + r];
+            tb[r] = std::fma(v, pa[c], tb[r]);
+            d0 = std::fma(v, pb[r], d0);
           }
+          y[c] += d0;
         }
+        for (int r = 0; r < 6; ++r) u[6 * e + r] = tb[r];
       }
       for (int r = 0; r < 6; ++r) q[6 * i + r] = y[r];
     }
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int64_t i = 0; i < (int64_t)n; ++i)
+      for (uint64_t k = in_off[i]; k < in_off[i + 1]; ++k)
+        for (int r = 0; r < 6; ++r) q[6 * i + r] += u[6 * in_edge[k] + r];
   };
   constexpr size_t kChunk = 6 * 256;
   const size_t nchunks = (N + kChunk - 1) / kChunk;
