@@ -24,11 +24,15 @@
 //   Camera::project ............. crates/core/src/types/camera.rs:351-432
 //   quaternion arithmetic ....... nalgebra 0.33.3 (UnitQuaternion *, transform,
 //                                 from_scaled_axis, to_rotation_matrix)
+//   reduced-camera PCG .......... colmap_incremental/rig_ba_solver.rs:1406-1480
+//                                 (pcg_core, with edge_product :1314-1331 and
+//                                 the run and coarse preconditioners)
 //
 // Parallel loops (OpenMP) never change a result: every accumulator is owned by
 // one thread and visited in the serial order, as the reference's rayon paths
 // guarantee (bundle/mod.rs:22-70).  Compiled with -ffp-contract=off so no
-// multiply-add is fused, matching Rust's arithmetic.
+// multiply-add is fused, matching Rust's arithmetic, except where the
+// reference itself fuses (edge_product's mul_add, restated with std::fma).
 
 #include <algorithm>
 #include <cmath>
