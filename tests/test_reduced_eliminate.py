@@ -211,3 +211,38 @@ def test_gpu_rejects_malformed_eliminations(solver):
         with pytest.raises(SolverError) as e:
             solver.reduced_eliminate(**args)
         assert e.value.status == _abi.ERR_INVALID_ARGUMENT, kw
+
+
+def test_synthetic_reduced_workload_generators():
+    """The bench's reduced-camera inputs (visloc_ba.synth): the covisibility
+    system has sorted distinct edges and a diagonally dominant SPD matrix; the
+    street elimination's edges are exactly the node pairs its points share,
+    and its damped diagonal with the eliminated blocks is SPD."""
+    from visloc_ba import synth
+
+    diag, edges, off = synth.covisibility_system(200, 20, 8)
+    keys = edges[:, 0].astype(np.int64) * 200 + edges[:, 1]
+    assert np.all(np.diff(keys) > 0) and np.all(edges[:, 0] < edges[:, 1])
+    S = np.zeros((1200, 1200))
+    for i, d in enumerate(diag):
+        S[6 * i:6 * i + 6, 6 * i:6 * i + 6] = d
+    for (a, b), B in zip(edges, off.astype(np.float64)):
+        S[6 * b:6 * b + 6, 6 * a:6 * a + 6] = B
+        S[6 * a:6 * a + 6, 6 * b:6 * b + 6] = B.T
+    assert np.all(np.diag(S) > np.abs(S).sum(axis=1) - np.diag(S))
+    el = synth.street_elimination(150, 60, seed=3)
+    po, pn = el["point_off"], el["point_nodes"]
+    want = sorted({(int(pn[k]), int(pn[j])) for p in range(len(po) - 1)
+                   for k in range(int(po[p]), int(po[p + 1]))
+                   for j in range(k + 1, int(po[p + 1]))})
+    assert [tuple(e) for e in el["edges"].tolist()] == want
+    blocks = oracle.eliminate_blocks(el["edges"], po, pn, el["hcp"], list(el["point_inverse"]))
+    S = np.zeros((900, 900))
+    for i, d in enumerate(el["diag"]):
+        S[6 * i:6 * i + 6, 6 * i:6 * i + 6] = d
+    for (a, b), B in zip(el["edges"], blocks):
+        S[6 * b:6 * b + 6, 6 * a:6 * a + 6] = B
+        S[6 * a:6 * a + 6, 6 * b:6 * b + 6] = B.T
+    assert np.linalg.eigvalsh(S).min() > 0.0
+    # The full-size system the bench measures: the published edge count.
+    assert abs(len(synth.covisibility_system()[1]) - 3.4e6) < 0.05e6
