@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define VLBA_ABI_VERSION 3u
+#define VLBA_ABI_VERSION 4u
 
 /* ------------------------------------------------------------------ status */
 /* Return codes.  The Rust shim maps VLBA_DECLINED to `None` (the caller then
@@ -175,7 +175,21 @@ typedef struct vlba_config {
   uint32_t max_pcg_iterations;     /* per LM linear solve */
   uint32_t flags;                  /* VLBA_FLAG_* */
   double pcg_relative_tolerance;   /* stop once |r| <= tol |b| */
-  uint32_t reserved[8];
+  /* Joint self-calibration switches of BaConfig (ABI version 4;
+   * bundle/mod.rs:669-700).  This solver keeps the intrinsics fixed, so a
+   * nonzero value in any of them makes every solving entry point return
+   * VLBA_DECLINED before it looks at the problem, and the caller runs its
+   * CPU solver -- the decline of GpuBundleAdjuster::check for
+   * refine_intrinsics || refine_distortion (crates/ba-gpu/src/solver.rs:
+   * 214-216).  refine_tangential_distortion and shared_focal only take
+   * effect with refine_intrinsics in the reference (mod.rs:682-700) and are
+   * declined here as well, so no config that could change the answer is
+   * solved with the intrinsics held. */
+  uint32_t refine_intrinsics;
+  uint32_t refine_distortion;
+  uint32_t refine_tangential_distortion;
+  uint32_t shared_focal;
+  uint32_t reserved[4];
 } vlba_config;
 
 /* Record per-iteration device phase times in vlba_iteration (costs a device

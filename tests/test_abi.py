@@ -149,3 +149,59 @@ def test_plan_handles_duplicate_observations():
                         np.concatenate([p.obs_camera, p.obs_camera[:5]]))
     st, info = plan(dup, BaConfig(robust_kernel=RobustKernel.huber(1.0)))
     assert st == _abi.OK
+
+
+REFINEMENT_FLAGS = ["refine_intrinsics", "refine_distortion", "refine_tangential_distortion",
+                    "shared_focal"]
+
+
+@pytest.mark.parametrize("flag", REFINEMENT_FLAGS)
+def test_intrinsics_refinement_is_declined(flag):
+    """GpuBundleAdjuster::check declines refine_intrinsics || refine_distortion
+    before looking at the problem (crates/ba-gpu/src/solver.rs:214-216); this
+    library keeps the intrinsics fixed, so it declines every self-calibration
+    switch of BaConfig (bundle/mod.rs:669-700), first of all checks."""
+    cfg = BaConfig(**{flag: True})
+    assert getattr(cfg.to_abi(), flag) == 1
+    packed, _, _, _ = drifted_bundle().pack()
+    assert check(packed, BaConfig())[0] == _abi.OK
+    assert check(packed, cfg)[0] == _abi.DECLINED
+    assert plan(packed, cfg)[0] == _abi.DECLINED
+    # Declined before validation: a problem with a missing pose is not an error here.
+    bad = PackedProblem([[1, 0, 0, 0]], [[0, 0, 0]], [[0, 0, 5]], [4], [0], [[1, 2]], [pinhole()])
+    assert check(bad, cfg)[0] == _abi.DECLINED
+
+
+@pytest.mark.parametrize("term,value", [
+    ("gravity_prior", object()),
+    ("per_pose_gravity_prior", object()),
+    ("position_prior", object()),
+    ("pairwise_pose_factors", [object()]),
+    ("velocities", {1: (0.0, 0.0, 0.0)}),
+    ("imu_factors", [object()]),
+    ("biases", {1: object()}),
+    ("bias_random_walk_factors", [object()]),
+    ("navigation_state_prior", object()),
+    ("fixed_pose_rotations", {1}),
+])
+def test_unmodelled_terms_are_declined_by_the_accelerator(term, value):
+    """Priors, the inertial state and rotation-fixed poses make
+    GpuBundleAdjuster::check return Unsupported (solver.rs:230-246), so the
+    plug-in returns None and the CPU solver runs.  The accelerator here is
+    built without a device: a solve attempt would fail on its missing solver,
+    so None proves that the decline came first and left `ba` untouched."""
+    from visloc_ba.solver import GpuBaSettings, GpuBundleAdjuster
+
+    ba = drifted_bundle()
+    before = {k: (tuple(p.world_to_camera.rotation), tuple(p.world_to_camera.translation))
+              for k, p in ba.poses.items()}
+    acc = object.__new__(GpuBundleAdjuster)
+    acc.solver = None
+    acc.settings = GpuBaSettings()
+    assert ba.unsupported_terms() is None
+    setattr(ba, term, value)
+    assert ba.unsupported_terms() is not None
+    assert acc.optimize(ba, BaConfig()) is None
+    after = {k: (tuple(p.world_to_camera.rotation), tuple(p.world_to_camera.translation))
+             for k, p in ba.poses.items()}
+    assert after == before

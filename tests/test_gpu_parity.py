@@ -256,3 +256,19 @@ def test_linear_step_matches_the_exact_solve(solver, ncams):
     assert rr <= 1e-7 and iters < 500
     assert np.abs(dp - dp_ref).max() <= 1e-3 * np.abs(dp_ref).max()
     assert np.abs(dl - dl_ref).max() <= 1e-3 * np.abs(dl_ref).max()
+
+
+@pytest.mark.parametrize("flag", ["refine_intrinsics", "refine_distortion",
+                                  "refine_tangential_distortion", "shared_focal"])
+def test_accelerator_declines_intrinsics_refinement(flag):
+    """BaConfig{refine_intrinsics: true} must not be solved with the
+    intrinsics held: the plug-in returns None, as GpuBundleAdjuster::check
+    makes it do (crates/ba-gpu/src/solver.rs:214-216), and `ba` is untouched;
+    the same problem without the flag is solved."""
+    ba = drifted_bundle()
+    before = {k: p.world_to_camera for k, p in ba.poses.items()}
+    acc = GpuBundleAdjuster(0, GpuBaSettings(100, 1e-6, True))
+    assert acc.optimize(ba, BaConfig(**{flag: True})) is None
+    assert {k: p.world_to_camera for k, p in ba.poses.items()} == before
+    res = acc.optimize(ba, BaConfig())
+    assert res is not None and res.final_cost < 1e-12

@@ -108,6 +108,14 @@ LmParams make_params(const vlba_config* cfg) {
 Validation validate_problem(const vlba_problem* p, const vlba_config* cfg) {
   Validation v;
   if (!p || !cfg) { v.status = VLBA_ERR_INVALID_ARGUMENT; return v; }
+  // Joint intrinsics refinement is the CPU solver's (optimize.rs:9-27):
+  // declined before anything else, as GpuBundleAdjuster::check does first
+  // (crates/ba-gpu/src/solver.rs:214-216).
+  if (cfg->refine_intrinsics || cfg->refine_distortion || cfg->refine_tangential_distortion ||
+      cfg->shared_focal) {
+    v.status = VLBA_DECLINED;
+    return v;
+  }
   if (cfg->robust_kernel > VLBA_KERNEL_CAUCHY) { v.status = VLBA_ERR_INVALID_ARGUMENT; return v; }
   if (p->num_poses >= kNone || p->num_landmarks >= kNone || p->num_observations >= kNone) {
     v.status = VLBA_ERR_INVALID_ARGUMENT;

@@ -1630,6 +1630,9 @@ int visloc_ba_cuda_cost(void* ctx, const vlba_problem* problem, const vlba_confi
   return vlba::guarded(c, [&] {
     vlba_config cfg = *config;
     cfg.max_iterations = 0;
+    // The cost does not depend on what a solve would refine.
+    cfg.refine_intrinsics = cfg.refine_distortion = 0;
+    cfg.refine_tangential_distortion = cfg.shared_focal = 0;
     const vlba_problem* probs[1] = {problem};
     const vlba_config* cfgs[1] = {&cfg};
     const vlba::Validation v = vlba::validate_problem(problem, &cfg);

@@ -10,7 +10,7 @@ from __future__ import annotations
 import ctypes as C
 import os
 
-ABI_VERSION = 3
+ABI_VERSION = 4
 
 # enum vlba_status
 OK = 0
@@ -130,7 +130,11 @@ class Config(C.Structure):
         ("max_pcg_iterations", C.c_uint32),
         ("flags", C.c_uint32),
         ("pcg_relative_tolerance", C.c_double),
-        ("reserved", C.c_uint32 * 8),
+        ("refine_intrinsics", C.c_uint32),
+        ("refine_distortion", C.c_uint32),
+        ("refine_tangential_distortion", C.c_uint32),
+        ("shared_focal", C.c_uint32),
+        ("reserved", C.c_uint32 * 4),
     ]
 
 

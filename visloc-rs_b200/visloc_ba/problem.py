@@ -268,6 +268,14 @@ class BaConfig:
     graph: bool = False
     # Choose the launch shape before the first solve of an upload.
     autotune: bool = False
+    # Joint self-calibration (mod.rs:669-700).  The device solver holds the
+    # intrinsics fixed, so any of these makes it decline (the caller's CPU
+    # solver runs instead), as GpuBundleAdjuster::check does for
+    # refine_intrinsics / refine_distortion (crates/ba-gpu/src/solver.rs:214-216).
+    refine_intrinsics: bool = False
+    refine_distortion: bool = False
+    refine_tangential_distortion: bool = False
+    shared_focal: bool = False
 
     def to_abi(self) -> _abi.Config:
         c = _abi.Config()
@@ -290,6 +298,10 @@ class BaConfig:
         c.pcg_relative_tolerance = float(self.pcg_relative_tolerance)
         c.flags = ((_abi.FLAG_PROFILE if self.profile else 0) | (_abi.FLAG_GRAPH if self.graph else 0)
                    | (_abi.FLAG_AUTOTUNE if self.autotune else 0))
+        c.refine_intrinsics = int(bool(self.refine_intrinsics))
+        c.refine_distortion = int(bool(self.refine_distortion))
+        c.refine_tangential_distortion = int(bool(self.refine_tangential_distortion))
+        c.shared_focal = int(bool(self.shared_focal))
         return c
 
 
@@ -553,6 +565,34 @@ class BundleAdjustment:
         self.camera = camera
         self.fixed_poses: set[int] = set()
         self.fixed_landmarks: set[int] = set()
+        # Terms of the reference problem that this solver does not model
+        # (mod.rs:530-622): rotation-fixed poses, priors and the inertial
+        # state.  They are carried so that the accelerator can decline a
+        # problem that holds any of them, as GpuBundleAdjuster::check does
+        # (crates/ba-gpu/src/solver.rs:230-246); the device never sees them.
+        self.fixed_pose_rotations: set[int] = set()
+        self.gravity_prior = None
+        self.per_pose_gravity_prior = None
+        self.position_prior = None
+        self.pairwise_pose_factors: list = []
+        self.velocities: dict = {}
+        self.imu_factors: list = []
+        self.biases: dict = {}
+        self.bias_random_walk_factors: list = []
+        self.navigation_state_prior = None
+
+    def unsupported_terms(self) -> Optional[str]:
+        """The first term of the problem this solver does not model, in the
+        order GpuBundleAdjuster::check tests them (solver.rs:230-246), or
+        None."""
+        if (self.gravity_prior is not None or self.per_pose_gravity_prior is not None
+                or self.position_prior is not None or self.pairwise_pose_factors
+                or self.velocities or self.imu_factors or self.biases
+                or self.bias_random_walk_factors or self.navigation_state_prior is not None):
+            return "prior/inertial terms"
+        if self.fixed_pose_rotations:
+            return "rotation-fixed poses"
+        return None
 
     # problem.rs:186-233
     def add_pose(self, id: int, pose: Pose):

@@ -526,8 +526,14 @@ class GpuBundleAdjuster:
         return res
 
     def optimize(self, ba: BundleAdjustment, config: BaConfig, scope: BaScope = BaScope.GLOBAL):
-        """BaAccelerator::optimize: None = declined (run the CPU solver)."""
+        """BaAccelerator::optimize: None = declined (run the CPU solver).
+        Declined: local windows unless enabled (solver.rs:29-33); priors, the
+        inertial state and rotation-fixed poses, which the device solver does
+        not model (solver.rs:230-246); and, in the library, joint intrinsics
+        refinement (solver.rs:214-216)."""
         if scope == BaScope.LOCAL and not self.settings.local_windows:
+            return None
+        if ba.unsupported_terms() is not None:
             return None
         try:
             return self.solve(ba, config)
