@@ -233,9 +233,11 @@ def hbm_peak():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def traffic_per_pcg_iteration():
-    """DRAM bytes per PCG iteration of k_pcg from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "k_pcg_ring4m_traffic.txt")
+def traffic_per_pcg_iteration(workload: str):
+    """DRAM bytes per PCG iteration of k_pcg from the committed ncu summary
+    of this workload (profiles/k_pcg_<workload>_traffic.txt); None for a
+    workload that has no capture of its own."""
+    path = os.path.join(ROOT, "profiles", f"k_pcg_{workload.replace('-', '')}_traffic.txt")
     try:
         with open(path) as f:
             for line in f:
@@ -379,6 +381,17 @@ def run_ours(args, dist: Dist):
     dist.barrier()
     clk = clocks.stop()
 
+    # Error of the timed solve's result against the FP64 oracle's solve of the
+    # same seeded input (committed fixture), where one exists.
+    parity_line = None
+    if args.workload == "ring-4m":
+        from oracle import parity
+
+        final = problem.copy()
+        if solver.download(final) == 0:
+            parity_line = parity.ring4m_parity(problem, results[-1].final_cost,
+                                               final.camera_centers())
+
     dev_ms = sum(r.device_ms for r in results)
     lm_iters = sum(len(r.iterations) for r in results)
     pcg_iters = sum(it.pcg_iterations for r in results for it in r.iterations)
@@ -392,7 +405,7 @@ def run_ours(args, dist: Dist):
     b_pcg = info.bytes_per_pcg_iteration
     peak, peak_kind = hbm_peak()
     achieved = (pcg_iters * b_pcg) / (pcg_ms / 1e3) / 1e9 if pcg_ms > 0 else 0.0
-    traffic = traffic_per_pcg_iteration()
+    traffic = traffic_per_pcg_iteration(args.workload)
     n_pcg_launches = sum(1 for r in results for it in r.iterations)
     mean_k = pcg_iters / max(1, n_pcg_launches)
     # Whole LM step: algorithmic bytes of linearisation + trial at the mean k.
@@ -464,6 +477,7 @@ def run_ours(args, dist: Dist):
                              ("pcg", "pcg_ms"), ("update_cost_decide", "update_ms")]},
             "final_cost": results[-1].final_cost,
             "initial_cost": results[-1].initial_cost,
+            "parity": parity_line,
             "wall_s": wall,
             "clocks": clk,
             "gpu_launches": int(launches),

@@ -660,13 +660,17 @@ int visloc_ba_cuda_optimize_gnc(void* ctx, vlba_problem* problem, const vlba_con
  * cudaStream_t of the current device; NULL = default stream); the call
  * returns without waiting for it.
  *
- * Nothing is allocated: the kernel's scratch is a fixed 1 MiB array in the
- * library's device code, held by every GPU that loads the library, which
- * limits a call to VLBA_NOALLOC_MAX_OBSERVATIONS observations (larger
- * problems return VLBA_ERR_INVALID_ARGUMENT).  All calls on a device share
- * that array: calls whose kernels may overlap on the GPU race and must be
- * serialised by the caller.  The first call on each device looks the
- * array's address up (set-up); make it before any stream capture.
+ * Nothing is allocated: the kernel's scratch is a fixed array of 1 MiB +
+ * 256 B (a 256-byte header and 65,536 partials of 16 B) in the library's
+ * device code, held by every GPU that loads the library until the process
+ * exits, which limits a call to VLBA_NOALLOC_MAX_OBSERVATIONS observations
+ * (larger problems return VLBA_ERR_INVALID_ARGUMENT).  All calls on a device
+ * share that array: calls whose kernels may overlap on the GPU race and must
+ * be serialised by the caller.  The first call on each device looks the
+ * array's address up (set-up), and so does the first call after the
+ * device's current context has changed (a cudaDeviceReset, after which the
+ * array may sit elsewhere, or another context of the device made current);
+ * make those calls before any stream capture.
  * `error` (capacity `error_capacity`, may be NULL) receives a message when
  * the status is not VLBA_OK. */
 #define VLBA_NOALLOC_MAX_OBSERVATIONS 16777216ull

@@ -7,14 +7,20 @@ from __future__ import annotations
 
 import math
 
+import numpy as np
+
 from visloc_ba import (
+    SE3,
     BaObservation,
     BundleAdjustment,
     Camera,
     CameraModel,
+    PackedProblem,
     Pose,
     quat_from_axis_angle,
+    synth,
 )
+from visloc_ba import _abi
 
 
 def pinhole() -> Camera:
@@ -102,3 +108,72 @@ def drifted_bundle(camera: Camera | None = None) -> BundleAdjustment:
 def center_error(ba: BundleAdjustment, pid: int, truth) -> float:
     c = ba.poses[pid].camera_center_world()
     return math.sqrt(sum((a - b) ** 2 for a, b in zip(c, truth)))
+
+
+# ------------------------------------------------ synthetic stereo windows
+def _left_and_rectified(seed, cams, points):
+    """The synthetic rig window, its left-camera observation rows, and for
+    each left observation with a right partner (same pose and point) its row
+    and the right column u_r."""
+    p = synth.stereo_window(cams, points, seed=seed)
+    left = np.nonzero(p.obs_camera == 0)[0]
+    keys = {}
+    for k in np.nonzero(p.obs_camera != 0)[0]:
+        keys[(int(p.obs_pose[k]), int(p.obs_landmark[k]))] = k
+    rows, ur = [], []
+    for k in left:
+        r = keys.get((int(p.obs_pose[k]), int(p.obs_landmark[k])))
+        if r is not None:
+            rows.append(k)
+            ur.append(p.obs_xy[r, 0])
+    return p, left, np.array(rows), np.array(ur)
+
+
+def stereo_window_packed(seed=3, cams=12, points=700):
+    """A synthetic rectified-stereo window: every rig observation pair of the
+    synthetic stereo window becomes one rectified observation (the right
+    camera of that window is translated by the baseline along x)."""
+    p, _, rows, ur = _left_and_rectified(seed, cams, points)
+    cam_left, ext_right = p.cameras[0][0], p.cameras[1][1]
+    baseline = -ext_right.translation[0]
+    stereo = np.zeros((rows.size, 2))
+    stereo[:, 0] = ur
+    return PackedProblem(p.pose_q, p.pose_t, p.landmarks, p.obs_pose[rows], p.obs_landmark[rows],
+                         p.obs_xy[rows], [cam_left], p.pose_fixed, p.landmark_fixed, None, None,
+                         np.full(rows.size, _abi.OBS_STEREO, np.uint8), stereo, None, baseline)
+
+
+def general_stereo_window_packed(seed=3, cams=12, points=700):
+    """The same window as calibrated stereo: right pixel (u_r, v), right
+    camera = the left one shifted by the baseline."""
+    p = stereo_window_packed(seed, cams, points)
+    st = p.obs_stereo.copy()
+    st[:, 1] = p.obs_xy[:, 1]
+    right = (p.cameras[0][0], SE3((1.0, 0.0, 0.0, 0.0), (-p.stereo_baseline, 0.0, 0.0)))
+    return PackedProblem(p.pose_q, p.pose_t, p.landmarks, p.obs_pose, p.obs_landmark, p.obs_xy,
+                         [p.cameras[0], right], p.pose_fixed, p.landmark_fixed, None, None,
+                         np.full(p.num_observations, _abi.OBS_GENERAL_STEREO, np.uint8), st,
+                         np.ones(p.num_observations, np.uint32), 0.0)
+
+
+def mixed_stereo_window_packed(seed=3, cams=12, points=700, camera=None):
+    """Monocular and rectified stereo observations in one problem, in the
+    reference's flattened order (monocular first): every left-camera
+    observation of the window as a monocular one, then the rectified ones.
+    Returns the problem and its monocular part alone.  `camera` replaces
+    BundleAdjustment::camera (cameras[0])."""
+    p, left, rows, ur = _left_and_rectified(seed, cams, points)
+    cam_left, ext_right = p.cameras[0][0], p.cameras[1][1]
+    cam = camera or cam_left
+    baseline = -ext_right.translation[0]
+    idx = np.concatenate([left, rows])
+    kind = np.concatenate([np.zeros(left.size, np.uint8),
+                           np.full(rows.size, _abi.OBS_STEREO, np.uint8)])
+    stereo = np.zeros((idx.size, 2))
+    stereo[left.size:, 0] = ur
+    mixed = PackedProblem(p.pose_q, p.pose_t, p.landmarks, p.obs_pose[idx], p.obs_landmark[idx],
+                          p.obs_xy[idx], [cam], p.pose_fixed, p.landmark_fixed, None, None, kind,
+                          stereo, None, baseline)
+    mono = PackedProblem(p.pose_q, p.pose_t, p.landmarks, p.obs_pose[left], p.obs_landmark[left],
+                         p.obs_xy[left], [cam], p.pose_fixed, p.landmark_fixed)
+    return mixed, mono

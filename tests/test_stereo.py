@@ -16,7 +16,8 @@ import math
 import numpy as np
 import pytest
 
-from _scenes import pinhole, pose_at, pose_with_yaw, project, world_grid
+from _scenes import (general_stereo_window_packed, pinhole, pose_at, pose_with_yaw, project,
+                     stereo_window_packed, world_grid)
 from oracle import oracle
 from visloc_ba import (
     SE3,
@@ -204,33 +205,6 @@ def test_weights_follow_the_flattened_observation_order():
 
 
 # ------------------------------------------------------------------ GPU side
-def stereo_window_packed(seed=3, cams=12, points=700):
-    """A synthetic rectified-stereo window: every rig observation pair of the
-    synthetic stereo window becomes one rectified observation (the right
-    camera of that window is translated by the baseline along x)."""
-    p = synth.stereo_window(cams, points, seed=seed)
-    left = p.obs_camera == 0
-    # The left camera of the window: its monocular observations, plus the
-    # right column of the same point in the same pose where there is one.
-    keys = {}
-    for k in np.nonzero(~left)[0]:
-        keys[(int(p.obs_pose[k]), int(p.obs_landmark[k]))] = k
-    rows, ur = [], []
-    for k in np.nonzero(left)[0]:
-        r = keys.get((int(p.obs_pose[k]), int(p.obs_landmark[k])))
-        if r is not None:
-            rows.append(k)
-            ur.append(p.obs_xy[r, 0])
-    rows = np.array(rows)
-    cam_left, ext_right = p.cameras[0][0], p.cameras[1][1]
-    baseline = -ext_right.translation[0]
-    stereo = np.zeros((rows.size, 2))
-    stereo[:, 0] = ur
-    return PackedProblem(p.pose_q, p.pose_t, p.landmarks, p.obs_pose[rows], p.obs_landmark[rows],
-                         p.obs_xy[rows], [cam_left], p.pose_fixed, p.landmark_fixed, None, None,
-                         np.full(rows.size, _abi.OBS_STEREO, np.uint8), stereo, None, baseline)
-
-
 @pytest.mark.gpu
 def test_device_stereo_scenes_recover_truth(solver):
     acc = GpuBundleAdjuster(0, GpuBaSettings(100, 1e-8, True))
@@ -260,17 +234,7 @@ def test_device_stereo_scenes_recover_truth(solver):
 @pytest.mark.gpu
 @pytest.mark.parametrize("general", [False, True])
 def test_stereo_window_matches_the_oracle(solver, general):
-    p = stereo_window_packed()
-    if general:
-        # The same window as calibrated stereo: right pixel (u_r, v), right
-        # camera = the left one shifted by the baseline.
-        st = p.obs_stereo.copy()
-        st[:, 1] = p.obs_xy[:, 1]
-        right = (p.cameras[0][0], SE3((1.0, 0.0, 0.0, 0.0), (-p.stereo_baseline, 0.0, 0.0)))
-        p = PackedProblem(p.pose_q, p.pose_t, p.landmarks, p.obs_pose, p.obs_landmark, p.obs_xy,
-                          [p.cameras[0], right], p.pose_fixed, p.landmark_fixed, None, None,
-                          np.full(p.num_observations, _abi.OBS_GENERAL_STEREO, np.uint8), st,
-                          np.ones(p.num_observations, np.uint32), 0.0)
+    p = general_stereo_window_packed() if general else stereo_window_packed()
     from visloc_ba import RobustKernel
 
     cfg = BaConfig(max_iterations=20, robust_kernel=RobustKernel.huber(1.0),

@@ -21,7 +21,8 @@ import ctypes as C
 import numpy as np
 import pytest
 
-from visloc_ba import BaConfig, PackedProblem, RobustKernel, synth
+from _scenes import general_stereo_window_packed, mixed_stereo_window_packed, stereo_window_packed
+from visloc_ba import BaConfig, Camera, CameraModel, PackedProblem, RobustKernel, synth
 from visloc_ba import _abi
 
 COST_RTOL = 1e-12  # the cost tolerance of the GPU-vs-oracle cost test
@@ -30,32 +31,37 @@ MAX_OBS = 16777216  # VLBA_NOALLOC_MAX_OBSERVATIONS
 
 class DeviceProblem:
     """A PackedProblem's arrays copied into device memory (by torch, on the
-    test's side: the entry point under test allocates nothing itself)."""
+    test's side: the entry point under test allocates nothing itself).  Every
+    array field of the problem is copied; one left on the host would hand the
+    kernel a host pointer, so an array field this helper does not know fails
+    here instead."""
+
+    ARRAYS = {
+        "pose_q": C.c_double, "pose_t": C.c_double, "landmarks": C.c_double,
+        "obs_pose": C.c_uint32, "obs_landmark": C.c_uint32, "obs_xy": C.c_double,
+        "obs_camera": C.c_uint32, "obs_weight": C.c_double, "obs_kind": C.c_uint8,
+        "obs_stereo": C.c_double, "obs_right_camera": C.c_uint32,
+    }
+    # Read on the host (cameras) or ignored by the entry point (fixed flags).
+    HOST = {"cameras", "pose_fixed", "landmark_fixed"}
 
     def __init__(self, packed: PackedProblem):
         import torch
 
         self.packed = packed
         self.keep = []
-
-        def dev(a, ctype):
+        p = packed.abi()  # host cameras; array fields replaced below
+        pointer_fields = {name for name, t in _abi.Problem._fields_
+                          if issubclass(t, C._Pointer)}
+        assert pointer_fields == set(self.ARRAYS) | self.HOST, pointer_fields
+        for name, ctype in self.ARRAYS.items():
+            a = getattr(packed, name)
             if a is None:
-                return None
+                assert not getattr(p, name), name
+                continue
             t = torch.from_numpy(np.ascontiguousarray(a)).cuda()
             self.keep.append(t)
-            return C.cast(C.c_void_p(t.data_ptr()), C.POINTER(ctype))
-
-        p = packed.abi()  # host cameras; array fields replaced below
-        p.pose_q = dev(packed.pose_q, C.c_double)
-        p.pose_t = dev(packed.pose_t, C.c_double)
-        p.landmarks = dev(packed.landmarks, C.c_double)
-        p.obs_pose = dev(packed.obs_pose, C.c_uint32)
-        p.obs_landmark = dev(packed.obs_landmark, C.c_uint32)
-        p.obs_xy = dev(packed.obs_xy, C.c_double)
-        if packed.obs_camera is not None:
-            p.obs_camera = dev(packed.obs_camera, C.c_uint32)
-        if packed.obs_weight is not None:
-            p.obs_weight = dev(packed.obs_weight, C.c_double)
+            setattr(p, name, C.cast(C.c_void_p(t.data_ptr()), C.POINTER(ctype)))
         self.abi = p
         self.cost = torch.empty(1, dtype=torch.float64, device="cuda")
         self.counts = torch.empty(2, dtype=torch.int64, device="cuda")
@@ -84,7 +90,10 @@ def problems():
     return [
         ("ring-12-per-camera-radial", synth.ring_problem(12, 1500, seed=71)),
         ("ring-40-shared-pinhole", shared),
-        ("stereo-window", synth.stereo_window(20, 1500, seed=6)),
+        ("stereo-rig-window", synth.stereo_window(20, 1500, seed=6)),
+        ("rectified-stereo-window", stereo_window_packed(seed=7, cams=16, points=1200)),
+        ("general-stereo-window", general_stereo_window_packed(seed=8, cams=16, points=1200)),
+        ("mono-and-rectified-window", mixed_stereo_window_packed(seed=9, cams=16, points=1200)[0]),
         ("pose-only", synth.pose_only(800, seed=4)),
     ]
 
@@ -111,24 +120,65 @@ def test_matches_the_allocating_cost_on_calls_in_a_row(solver):
 
 @pytest.mark.gpu
 def test_out_of_range_indices_are_counted_and_skipped(solver):
+    """Where visloc_ba_cuda_cost rejects the whole problem, this entry point
+    counts the offending observation as invalid and skips it: a pose,
+    landmark or camera index out of range, a NaN or infinite weight."""
     lib = solver.lib
     p = synth.ring_problem(12, 800, seed=72)
     cfg = BaConfig(robust_kernel=RobustKernel.huber(1.0))
+    rng = np.random.default_rng(5)
+    w = rng.uniform(0.5, 1.5, p.num_observations)
     broken = PackedProblem(p.pose_q, p.pose_t, p.landmarks, p.obs_pose.copy(),
                            p.obs_landmark.copy(), p.obs_xy, p.cameras, p.pose_fixed,
-                           p.landmark_fixed, p.obs_camera)
+                           p.landmark_fixed, p.obs_camera.copy(), w.copy())
     broken.obs_pose[5] = p.num_poses
     broken.obs_landmark[17] = p.num_landmarks + 3
+    broken.obs_camera[31] = len(p.cameras)
+    broken.obs_weight[23] = np.nan
+    broken.obs_weight[40] = np.inf
+    bad_rows = [5, 17, 23, 31, 40]
     keep = np.ones(p.num_observations, bool)
-    keep[[5, 17]] = False
+    keep[bad_rows] = False
     trimmed = PackedProblem(p.pose_q, p.pose_t, p.landmarks, p.obs_pose[keep],
                             p.obs_landmark[keep], p.obs_xy[keep], p.cameras, p.pose_fixed,
-                            p.landmark_fixed, p.obs_camera[keep])
+                            p.landmark_fixed, p.obs_camera[keep], w[keep])
     want, want_bad = solver.cost(trimmed, cfg)
     dp = DeviceProblem(broken)
     for _ in range(2):
         got, bad, invalid = noalloc_cost(lib, dp, cfg)
-        assert invalid == 2 and bad == want_bad
+        assert invalid == len(bad_rows) and bad == want_bad
+        assert got == pytest.approx(want, rel=COST_RTOL)
+
+
+@pytest.mark.gpu
+def test_unusable_stereo_observations_are_counted_and_skipped(solver):
+    """Rectified stereo observations without a usable baseline (0, negative,
+    NaN), or with a cameras[0] outside the pinhole models, are counted as
+    invalid and skipped; the monocular observations of the same problem are
+    still summed, to the cost visloc_ba_cuda_cost gives for them alone."""
+    lib = solver.lib
+    cfg = BaConfig(robust_kernel=RobustKernel.cauchy(2.0))
+    mixed, mono = mixed_stereo_window_packed(seed=10, cams=16, points=1200)
+    n_stereo = int((mixed.obs_kind == _abi.OBS_STEREO).sum())
+    assert 0 < n_stereo < mixed.num_observations
+    want, want_bad = solver.cost(mono, cfg)
+    for baseline in (0.0, -0.11, float("nan")):
+        q = mixed.copy()
+        q.stereo_baseline = baseline
+        dp = DeviceProblem(q)
+        for _ in range(2):
+            got, bad, invalid = noalloc_cost(lib, dp, cfg)
+            assert invalid == n_stereo and bad == want_bad
+            assert got == pytest.approx(want, rel=COST_RTOL)
+    left = mixed.cameras[0][0]
+    radial = Camera(CameraModel.SIMPLE_RADIAL, left.width, left.height,
+                    [left.params[0], left.params[2], left.params[3], 0.02])
+    mixed_r, mono_r = mixed_stereo_window_packed(seed=10, cams=16, points=1200, camera=radial)
+    want, want_bad = solver.cost(mono_r, cfg)
+    dp = DeviceProblem(mixed_r)
+    for _ in range(2):
+        got, bad, invalid = noalloc_cost(lib, dp, cfg)
+        assert invalid == n_stereo and bad == want_bad
         assert got == pytest.approx(want, rel=COST_RTOL)
 
 

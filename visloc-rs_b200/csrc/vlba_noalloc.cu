@@ -22,10 +22,13 @@
 //
 // Device pointers: host code never passes g_noalloc_scratch itself to a
 // kernel -- in host code the name is a host-side stand-in, not a device
-// address.  The device address is looked up once per device with
-// cudaGetSymbolAddress (scratch_address below) on the first call made with
-// that device current; make that first call before any stream capture.
+// address.  The device address is looked up with cudaGetSymbolAddress
+// (scratch_address below) on the first call made with that device current,
+// and looked up again when the device's current context is no longer the
+// one the address was taken in (after cudaDeviceReset the module is loaded
+// anew and the array may move); make such a call before any stream capture.
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -198,17 +201,53 @@ __global__ void __launch_bounds__(256) k_cost_noalloc(const NoallocArgs a, unsig
   }
 }
 
-// Device address of g_noalloc_scratch on the current device, looked up once
-// per device.  nullptr and `err` set on failure.
+// Process-unique id of the calling thread's current context (cuCtxGetId),
+// or 0 when there is none or the driver cannot tell.  The driver functions
+// come through the runtime's entry-point query, so the library needs no
+// link-time dependency on libcuda.
+unsigned long long current_context_id() {
+  using GetCurrent = CUresult (*)(CUcontext*);
+  using GetId = CUresult (*)(CUcontext, unsigned long long*);
+  static GetCurrent get_current = nullptr;
+  static GetId get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<GetCurrent>(f);
+    f = nullptr;
+    q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<GetId>(f);
+  });
+  if (!get_current || !get_id) return 0;
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  if (get_current(&ctx) != CUDA_SUCCESS || !ctx || get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
+
+// Device address of g_noalloc_scratch on the current device: looked up on
+// the first call with the device current and again whenever the current
+// context differs from the one it was taken in (a cudaDeviceReset in
+// between, or another context of the device made current).  nullptr and
+// `err` set on failure.
 unsigned char* scratch_address(int device, cudaError_t* err) {
   static std::mutex mu;
   static unsigned char* addr[kMaxDevices] = {};
+  static unsigned long long context_of[kMaxDevices] = {};
   std::lock_guard<std::mutex> lock(mu);
-  if (!addr[device]) {
+  const unsigned long long ctx = current_context_id();
+  if (!addr[device] || ctx == 0 || ctx != context_of[device]) {
     unsigned char* ptr = nullptr;
     *err = cudaGetSymbolAddress((void**)&ptr, g_noalloc_scratch);
     if (*err != cudaSuccess) return nullptr;
     addr[device] = ptr;
+    // The lookup makes the device's primary context current if none was.
+    context_of[device] = current_context_id();
   }
   *err = cudaSuccess;
   return addr[device];
