@@ -12,7 +12,6 @@ cost within 1e-5 relative and camera centres within 1e-5 of the scene extent.
 
 from __future__ import annotations
 
-import numpy as np
 import pytest
 
 from oracle import parity

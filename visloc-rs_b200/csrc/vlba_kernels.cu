@@ -173,7 +173,7 @@ __global__ void __launch_bounds__(256) k_pose_table(Dev d) {
 // One thread per observation (point-major order): the residual and analytic
 // Jacobian in FP64, the IRLS weight, and the observation's H_o and e_o.  The
 // point sums H_ll and g_l are formed by k_point_prep from these records.
-__global__ void __launch_bounds__(256) k_linearize(Dev d) {
+__global__ void __launch_bounds__(256, 3) k_linearize(Dev d) {
   for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < d.num_obs;
        k += gridDim.x * blockDim.x) {
     const uint32_t l = d.obs_point[k];
@@ -276,6 +276,9 @@ __global__ void __launch_bounds__(256) k_linearize(Dev d) {
 }
 
 // ------------------------------------------------------------ point prep
+// Observations a chunked kernel stages through shared memory per pass.
+constexpr uint32_t kObsStage = 1024;
+
 // Damped landmark inverse (FP64 cofactors, nalgebra Matrix3::try_inverse:
 // singular iff det == 0) and v = H^-1 g.  A singular or fixed point gets a
 // zero inverse, which drops it from the reduced system and back-substitution
@@ -737,16 +740,23 @@ __global__ void __launch_bounds__(256) k_pose_update(Dev d) {
 
 // ------------------------------------------------- back-substitution + cost
 // One block of 256 threads per chunk of (at most 256) points of one problem,
-// in two steps: one thread per point -- with TRIAL, the landmark step
-// dl = -H^-1 (g + sum_o H_o (rho + omega x X)) of every variable point
-// (W_o^T dc = H_o B dc) and the candidate point X + dl -- then one thread per
-// observation of the chunk for the cost at the candidate poses/points (the
-// current state without TRIAL).  Sums in a fixed order per chunk.
+// in two steps.  With TRIAL, first the landmark step
+//   dl = -H^-1 (g + sum_o H_o (rho + omega x X))
+// of every variable point (W_o^T dc = H_o B dc) and the candidate point
+// X + dl: the chunk's observations (contiguous) each form their term
+// H_o (rho + omega x X) on one thread, kObsStage per pass, into shared
+// memory, and each point's thread adds its own terms from there in
+// observation order.  Then one thread per observation of the chunk for the
+// cost at the candidate poses/points (the current state without TRIAL).
+// Sums in a fixed order per chunk.
 template <bool TRIAL>
 __global__ void __launch_bounds__(256) k_cost(Dev d) {
   __shared__ double red[256];
   __shared__ unsigned long long redu[256];
-  __shared__ double sX[3 * 256];  // the chunk's (candidate) points
+  __shared__ double sX[3 * 256];                      // the chunk's (candidate) points
+  __shared__ float sXf[TRIAL ? 3 * 256 : 1];          // the points as FP32 (pt_s)
+  __shared__ double sC[TRIAL ? 3 * kObsStage : 1];    // staged observation terms
+  __shared__ unsigned char sAct[TRIAL ? 256 : 1];     // point takes a step
   for (uint32_t ch = blockIdx.x; ch < d.num_point_chunks; ch += gridDim.x) {
     const uint32_t lo = d.chunk_point_begin[ch], hi = d.chunk_point_begin[ch + 1];
     const uint32_t P = d.point_prob[lo];
@@ -757,50 +767,92 @@ __global__ void __launch_bounds__(256) k_cost(Dev d) {
     const LmParams& lp = d.params[P];
     double cost = 0.0, step = 0.0;
     unsigned long long bad = 0;
-    for (uint32_t l = lo + threadIdx.x; l < hi; l += blockDim.x) {
-      double X[3];
+    const uint32_t l = lo + threadIdx.x;
+    const bool mine = l < hi;
+    double X[3] = {0.0, 0.0, 0.0};
+    if (mine) {
 #pragma unroll
       for (int a = 0; a < 3; ++a) X[a] = d.points[cur][3 * (size_t)l + a];
-      const uint32_t k0 = d.pt_off[l], k1 = d.pt_off[l + 1];
-      if (TRIAL) {
+    }
+    if (TRIAL) {
+      const uint32_t o0 = d.pt_off[lo], o1 = d.pt_off[hi];
+      bool act = false;
+      if (mine) {
         const float4 s1 = d.pt_s[4 * (size_t)l + 1], s2 = d.pt_s[4 * (size_t)l + 2],
                      s3 = d.pt_s[4 * (size_t)l + 3];
-        if (d.point_var[l] && s3.w != 0.0f) {
-          // In FP64 with the point's FP64 damped inverse: a point whose depth
-          // one observation alone constrains has an inverse with entries near
-          // 1/lambda along its ray, which FP32 would turn into a large
-          // spurious step along the ray.
-          double Mi[9], vv[3];
-          point_inverse64(d, l, c.lambda, Mi, vv);
-          const double x = s1.z, y = s1.w, z = s2.x;
-          const float* ph = d.pt_h + 9 * (size_t)l;
-          double u0 = ph[6], u1 = ph[7], u2 = ph[8];
-          for (uint32_t k = k0; k < k1; ++k) {
-            const uint32_t slot = d.obs_slot[k];
-            if (slot == kNone) continue;
+        act = d.point_var[l] && s3.w != 0.0f;
+        sXf[3 * threadIdx.x] = s1.z;
+        sXf[3 * threadIdx.x + 1] = s1.w;
+        sXf[3 * threadIdx.x + 2] = s2.x;
+        sAct[threadIdx.x] = act ? 1 : 0;
+      }
+      __syncthreads();
+      // In FP64 with the point's FP64 damped inverse: a point whose depth one
+      // observation alone constrains has an inverse with entries near
+      // 1/lambda along its ray, which FP32 would turn into a large spurious
+      // step along the ray.
+      double u0 = 0.0, u1 = 0.0, u2 = 0.0;
+      if (act) {
+        const float* ph = d.pt_h + 9 * (size_t)l;
+        u0 = ph[6];
+        u1 = ph[7];
+        u2 = ph[8];
+      }
+      const uint32_t k0 = mine ? d.pt_off[l] : 0u, k1 = mine ? d.pt_off[l + 1] : 0u;
+      for (uint32_t base = o0; base < o1; base += kObsStage) {
+        const uint32_t end = min(o1, base + kObsStage);
+        for (uint32_t k = base + threadIdx.x; k < end; k += blockDim.x) {
+          double t0 = 0.0, t1 = 0.0, t2 = 0.0;
+          const uint32_t pl = d.obs_point[k] - lo;
+          const uint32_t slot = d.obs_slot[k];
+          if (sAct[pl] && slot != kNone) {
+            const double x = sXf[3 * pl], y = sXf[3 * pl + 1], z = sXf[3 * pl + 2];
             const float* dc = d.x + 6 * (size_t)slot;
             const double w0 = dc[3], w1 = dc[4], w2 = dc[5];
             const double b0 = dc[0] + (w1 * z - w2 * y);
             const double b1 = dc[1] + (w2 * x - w0 * z);
             const double b2 = dc[2] + (w0 * y - w1 * x);
             const float4 h0 = d.obs_h[2 * (size_t)k], h1 = d.obs_h[2 * (size_t)k + 1];
-            u0 += h0.x * b0 + h0.y * b1 + h0.z * b2;
-            u1 += h0.y * b0 + h0.w * b1 + h1.x * b2;
-            u2 += h0.z * b0 + h1.x * b1 + h1.y * b2;
+            t0 = h0.x * b0 + h0.y * b1 + h0.z * b2;
+            t1 = h0.y * b0 + h0.w * b1 + h1.x * b2;
+            t2 = h0.z * b0 + h1.x * b1 + h1.y * b2;
           }
-          const double e0 = -(Mi[0] * u0 + Mi[1] * u1 + Mi[2] * u2);
-          const double e1 = -(Mi[3] * u0 + Mi[4] * u1 + Mi[5] * u2);
-          const double e2 = -(Mi[6] * u0 + Mi[7] * u1 + Mi[8] * u2);
-          step = fmax(step, sqrt(e0 * e0 + e1 * e1 + e2 * e2));
-          X[0] += e0;
-          X[1] += e1;
-          X[2] += e2;
+          double* q = sC + 3 * (k - base);
+          q[0] = t0;
+          q[1] = t1;
+          q[2] = t2;
         }
+        __syncthreads();
+        if (act) {
+          const uint32_t a = max(k0, base), b = min(k1, end);
+          for (uint32_t k = a; k < b; ++k) {
+            const double* q = sC + 3 * (k - base);
+            u0 += q[0];
+            u1 += q[1];
+            u2 += q[2];
+          }
+        }
+        __syncthreads();
+      }
+      if (act) {
+        double Mi[9], vv[3];
+        point_inverse64(d, l, c.lambda, Mi, vv);
+        const double e0 = -(Mi[0] * u0 + Mi[1] * u1 + Mi[2] * u2);
+        const double e1 = -(Mi[3] * u0 + Mi[4] * u1 + Mi[5] * u2);
+        const double e2 = -(Mi[6] * u0 + Mi[7] * u1 + Mi[8] * u2);
+        step = fmax(step, sqrt(e0 * e0 + e1 * e1 + e2 * e2));
+        X[0] += e0;
+        X[1] += e1;
+        X[2] += e2;
+      }
+      if (mine) {
 #pragma unroll
         for (int a = 0; a < 3; ++a) d.points[cur ^ 1u][3 * (size_t)l + a] = X[a];
       }
+    }
+    if (mine) {
 #pragma unroll
-      for (int a = 0; a < 3; ++a) sX[3 * (l - lo) + a] = X[a];
+      for (int a = 0; a < 3; ++a) sX[3 * threadIdx.x + a] = X[a];
     }
     __syncthreads();
     // The chunk's observations, one thread each (stride 256), at the points
