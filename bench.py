@@ -73,6 +73,8 @@ def parse_args():
     ap.add_argument("--reduced-part", default="all", choices=["all", "solve", "eliminate"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="ring-4m: skip the other workloads' sub-objects of the line")
     return ap.parse_args()
 
 
@@ -484,8 +486,8 @@ def run_ours(args, dist: Dist):
             "e2e": e2e,
             "cpu_baseline": cpu,
         }
-        print(json.dumps(line), flush=True)
     solver.close()
+    return line if dist.rank == 0 else None
 
 
 def run_batch(args, dist: Dist):
@@ -598,8 +600,8 @@ def run_batch(args, dist: Dist):
             "e2e": e2e,
             "cpu_baseline": cpu,
         }
-        print(json.dumps(line), flush=True)
     solver.close()
+    return line if dist.rank == 0 else None
 
 
 def served_requests(n, seed):
@@ -734,7 +736,8 @@ def run_served(args, dist: Dist):
                                                   for _, p in reqs))},
             "cpu_baseline": None,
         }
-        print(json.dumps(line), flush=True)
+        return line
+    return None
 
 
 # ------------------------------------------------ reduced camera system path
@@ -880,7 +883,7 @@ def run_reduced(args, dist: Dist):
         line["cpu_baseline"] = {"value": cpu, "unit": "ms", "cores": cores, "kind": "port",
                                 "sample": "a 1e-6 solve less a one-iteration solve of the "
                                           "FP64 C++ pcg_core restatement, all host threads"}
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def reduced_elimination(solver, el, n, steps):
@@ -920,20 +923,67 @@ def reduced_elimination(solver, el, n, steps):
                                          "pcg_device_ms": solver.reduced_timing()["pcg_ms"]}}
 
 
+def compact(line, keys):
+    """The named keys of a workload's line (for the default line's
+    other_workloads object)."""
+    if line is None:
+        return None
+    return {k: line.get(k) for k in keys if k in line}
+
+
+def other_workloads(args, dist: Dist):
+    """The other benchmarked workloads, each run and timed on its own after
+    the headline solve (short step counts; each with its own clock record),
+    so that one default bench run records them all.  Outside the headline
+    `value`."""
+    out = {}
+    common = ["metric", "value", "unit", "ms_per_step", "config", "clocks"]
+    sub = argparse.Namespace(**{**vars(args), "steps": min(args.steps, 3),
+                                "warmup": min(args.warmup, 2), "no_e2e": False,
+                                "no_cpu_baseline": False, "workload": "windows-512"})
+    t0 = time.perf_counter()
+    out["windows-512"] = compact(run_batch(sub, dist), common + [
+        "observations_per_s", "windows_per_s", "plain_per_problem_lm_iterations_per_s",
+        "roofline", "phase_ms_per_lm_iteration", "e2e", "cpu_baseline"])
+    sub = argparse.Namespace(**{**vars(sub), "workload": "served", "no_cpu_baseline": True})
+    out["served"] = compact(run_served(sub, dist), common + [
+        "latency_ms", "latency_by_kind", "offered_rate", "plain_per_problem_solves_per_s",
+        "saturated_solves_per_s", "saturated_latency_ms"])
+    if out["served"]:
+        s = out["served"]
+        s["speedup_over_plain"] = s["value"] / s["plain_per_problem_solves_per_s"]
+    sub = argparse.Namespace(**{**vars(sub), "workload": "reduced-5822", "no_cpu_baseline": False,
+                                "reduced_nodes": REDUCED_NODES, "reduced_part": "all"})
+    out["reduced-5822"] = compact(run_reduced(sub, dist), common + [
+        "block_jacobi_iteration_ms", "fixed_cost_ms", "solve_to_1e-6", "roofline",
+        "elimination", "reference_l4", "cpu_baseline", "vs_baseline"])
+    out["wall_s"] = time.perf_counter() - t0
+    return out
+
+
 def main():
     args = parse_args()
     dist = Dist()
     try:
+        line = None
         if args.workload == "reduced-5822":
-            run_reduced(args, dist)
+            line = run_reduced(args, dist)
         elif args.impl == "reference":
             run_reference(args, dist)
         elif args.workload == "windows-512":
-            run_batch(args, dist)
+            line = run_batch(args, dist)
         elif args.workload == "served":
-            run_served(args, dist)
+            line = run_served(args, dist)
         else:
-            run_ours(args, dist)
+            line = run_ours(args, dist)
+            # One process per GPU of the default run also measures the other
+            # workloads (N = 1 only: the scaling runs time the headline alone).
+            if dist.world == 1 and args.workload == "ring-4m" and not args.no_extras:
+                extra = other_workloads(args, dist)
+                if line is not None:
+                    line["other_workloads"] = extra
+        if line is not None and dist.rank == 0:
+            print(json.dumps(line), flush=True)
     finally:
         dist.close()
 

@@ -90,3 +90,14 @@ def test_reduced_tiles_counts_the_device_layout():
     # Tile rows of 8 nodes: 3 rows for 21 nodes; diagonal tiles (0,0), (1,1), (2,2) plus the
     # off-diagonal tiles (0,1) and (0,2).
     assert bench.reduced_tiles(edges, 21) == 5
+
+
+def test_compact_keeps_the_named_keys():
+    """The default line's other_workloads entries keep only the named keys of
+    each workload's own line."""
+    import bench
+
+    line = {"value": 1.0, "unit": "u", "clocks": {}, "noise": [1, 2]}
+    assert bench.compact(line, ["value", "unit", "clocks", "missing"]) == {
+        "value": 1.0, "unit": "u", "clocks": {}}
+    assert bench.compact(None, ["value"]) is None
