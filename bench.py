@@ -252,26 +252,20 @@ def traffic_per_pcg_iteration(workload: str):
 
 # -------------------------------------------------------------- CPU side
 def cpu_sample(problem, cfg, threads=0):
-    """One LM iteration of the FP64 oracle on all host cores: (seconds,
-    fraction of the workload's observations it covered).  A problem too large
-    for the oracle's dense reduced solve (more than 2,000 poses) is sampled
-    as the sub-problem of a contiguous stretch of 700 of its poses."""
+    """One LM iteration of the FP64 oracle on all host cores, on the whole
+    workload: (seconds, fraction of the workload's observations it covered,
+    always 1).  The oracle's sparse solve factors the reduced system in band
+    storage when it is banded (the street loop) and densely otherwise."""
     from oracle import oracle
-    from visloc_ba import synth
 
-    frac = 1.0
-    if problem.num_poses > 2000:
-        sub = synth.sub_problem(problem, range(700))
-        frac = sub.num_observations / problem.num_observations
-        problem = sub
     c = problem.copy()
     one = type(cfg)(**{**cfg.__dict__, "max_iterations": 1})
     t0 = time.perf_counter()
-    st, _ = oracle.optimize(c, one, solver=oracle.SPARSE, threads=threads)
+    st, _ = oracle.optimize(c, one, solver=oracle.SPARSE_BANDED, threads=threads)
     dt = time.perf_counter() - t0
     if st != 0:
         raise RuntimeError(f"oracle failed: {st}")
-    return dt, frac
+    return dt, 1.0
 
 
 def batch_cpu_sample(problems, cfg, windows=128):
@@ -386,13 +380,13 @@ def run_ours(args, dist: Dist):
     # Error of the timed solve's result against the FP64 oracle's solve of the
     # same seeded input (committed fixture), where one exists.
     parity_line = None
-    if args.workload == "ring-4m":
-        from oracle import parity
+    from oracle import parity
 
+    if args.workload in parity.FIXTURES:
         final = problem.copy()
         if solver.download(final) == 0:
-            parity_line = parity.ring4m_parity(problem, results[-1].final_cost,
-                                               final.camera_centers())
+            parity_line = parity.workload_parity(args.workload, problem,
+                                                 results[-1].final_cost, final.camera_centers())
 
     dev_ms = sum(r.device_ms for r in results)
     lm_iters = sum(len(r.iterations) for r in results)
@@ -451,8 +445,8 @@ def run_ours(args, dist: Dist):
                 "rate scaled by that share)")
         cpu = {"value": frac / dt, "unit": "LM iterations/s", "cores": os.cpu_count(),
                "kind": "port",
-               "sample": f"1 LM iteration (FP64 Schur + Cholesky) of {what}, "
-                         f"{os.cpu_count()} threads, {dt:.1f} s"}
+               "sample": f"1 LM iteration (FP64 Schur + Cholesky, banded when the reduced "
+                         f"system is) of {what}, {os.cpu_count()} threads, {dt:.1f} s"}
 
     if dist.rank == 0:
         line = {

@@ -27,6 +27,12 @@
 //   reduced-camera PCG .......... colmap_incremental/rig_ba_solver.rs:1406-1480
 //                                 (pcg_core, with edge_product :1314-1331 and
 //                                 the run and coarse preconditioners)
+//   matrix-free LM backend ...... bundle/implicit_schur.rs:108-300 (operator,
+//                                 block-Jacobi), :302-376 (cluster8), :390-473
+//                                 (apply, preconditioner), :522-736 (PCG),
+//                                 :789-828 (complete_delta); step dispatch
+//                                 bundle/matrix_free.rs:1106-1190, entry
+//                                 bundle/optimize.rs:105-139
 //
 // Parallel loops (OpenMP) never change a result: every accumulator is owned by
 // one thread and visited in the serial order, as the reference's rayon paths
@@ -35,9 +41,11 @@
 // reference itself fuses (edge_product's mul_add, restated with std::fma).
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <functional>
 #include <limits>
 #include <vector>
 
@@ -860,6 +868,162 @@ void reduce(const Normal& N, size_t np, size_t nl, double lambda, int threads,
     }
 }
 
+// ----------------------------------------------------- banded sparse solve
+// LinearSolver::Sparse on a reduced system whose blocks lie in a band (a
+// street loop: covisible cameras are near each other along the capture
+// order, and the loop closes back to the start).  The reference factors S
+// with a block Cholesky in a fill-reducing order (block_cholesky.rs:13-120,
+// 250-310, order from reordering.rs); any symmetric order gives the same
+// solution up to rounding, and here it is a bandwidth-reducing one: the
+// capture order, or the "fold" order 0, n-1, 1, n-2, ... that turns a closed
+// loop's cyclic band into a plain band of twice the width.  S's lower band
+// is stored row-major, W + 1 scalars per row (W = 6 w + 5 for a block
+// half-bandwidth w), and factored in place column by column.
+struct Band {
+  size_t n = 0, W = 0;
+  std::vector<uint32_t> pos;  // permuted position of each variable pose
+  std::vector<double> a;      // [n (W + 1)]: entry (i, j), i - W <= j <= i, at i (W+1) + j - i + W
+  double& at(size_t i, size_t j) { return a[i * (W + 1) + j + W - i]; }
+  double at(size_t i, size_t j) const { return a[i * (W + 1) + j + W - i]; }
+};
+
+// Block half-bandwidth of the reduced system under `pos`: the largest
+// |pos(i) - pos(j)| over camera pairs that share a landmark with an inverse.
+size_t band_width(const Normal& N, const std::vector<uint8_t>& ok, const std::vector<uint32_t>& pos) {
+  size_t w = 0;
+  for (size_t l = 0; l < N.cross.size(); ++l) {
+    if (!ok[l] || N.cross[l].empty()) continue;
+    uint32_t lo = ~0u, hi = 0;
+    for (const Cross& c : N.cross[l]) {
+      lo = std::min(lo, pos[c.pose]);
+      hi = std::max(hi, pos[c.pose]);
+    }
+    w = std::max(w, (size_t)(hi - lo));
+  }
+  return w;
+}
+
+// The damped reduced system in band storage and its rhs (original pose
+// order), with the block order of smaller bandwidth; false when even that
+// band is wider than a third of the system (then the dense path is cheaper).
+bool reduce_banded(const Normal& N, size_t np, size_t nl, double lambda, int threads, Band& B,
+                   std::vector<double>& rhs, std::vector<uint8_t>& inv_ok,
+                   std::vector<double>& hinv) {
+  inv_ok.assign(nl, 0);
+  hinv.assign(nl * 9, 0.0);
+  for (size_t l = 0; l < nl; ++l) {
+    double h[9];
+    std::memcpy(h, &N.h_ll[l * 9], sizeof h);
+    if (lambda > 0.0) { h[0] += lambda; h[4] += lambda; h[8] += lambda; }
+    inv_ok[l] = try_inverse3(h, &hinv[l * 9]) ? 1 : 0;
+  }
+  std::vector<uint32_t> ident(np), fold(np);
+  for (size_t i = 0; i < np; ++i) {
+    ident[i] = (uint32_t)i;
+    fold[i] = (uint32_t)(i < (np + 1) / 2 ? 2 * i : 2 * (np - 1 - i) + 1);
+  }
+  const size_t wi = band_width(N, inv_ok, ident), wf = band_width(N, inv_ok, fold);
+  B.pos = wf < wi ? fold : ident;
+  const size_t w = std::min(wi, wf);
+  if (3 * w > np) return false;
+  B.n = np * 6;
+  B.W = 6 * w + 5;
+  B.a.assign(B.n * (B.W + 1), 0.0);
+  rhs.assign(np * 6, 0.0);
+  for (size_t p = 0; p < np; ++p) {
+    const size_t P = B.pos[p];
+    for (int r = 0; r < 6; ++r) {
+      for (int c = 0; c <= r; ++c) {
+        double v = N.h_pp[p * 36 + r * 6 + c];
+        if (r == c && lambda > 0.0) v += lambda;
+        B.at(6 * P + r, 6 * P + c) = v;
+      }
+      rhs[p * 6 + r] = -N.b_p[p * 6 + r];
+    }
+  }
+  // Schur terms, each permuted block row owned by one thread (landmark order).
+#pragma omp parallel num_threads(threads)
+  {
+#ifdef _OPENMP
+    const int tid = omp_get_thread_num(), nt = omp_get_num_threads();
+#else
+    const int tid = 0, nt = 1;
+#endif
+    for (size_t l = 0; l < nl; ++l) {
+      if (!inv_ok[l]) continue;
+      const double* hi = &hinv[l * 9];
+      const std::vector<Cross>& cr = N.cross[l];
+      for (const Cross& a : cr) {
+        const size_t Pa = B.pos[a.pose];
+        if ((int)(Pa % nt) != tid) continue;
+        double ah[18];
+        for (int r = 0; r < 6; ++r)
+          for (int c = 0; c < 3; ++c) {
+            double t = 0.0;
+            for (int k = 0; k < 3; ++k) t += a.a[r * 3 + k] * hi[k * 3 + c];
+            ah[r * 3 + c] = t;
+          }
+        for (const Cross& b : cr) {
+          const size_t Pb = B.pos[b.pose];
+          if (Pb > Pa) continue;
+          for (int r = 0; r < 6; ++r)
+            for (int c = 0; c < 6; ++c) {
+              if (Pb == Pa && c > r) continue;
+              double t = 0.0;
+              for (int k = 0; k < 3; ++k) t += ah[r * 3 + k] * b.a[c * 3 + k];
+              B.at(6 * Pa + r, 6 * Pb + c) -= t;
+            }
+        }
+        const double* bl = &N.b_l[l * 3];
+        for (int k = 0; k < 6; ++k) {
+          double t = 0.0;
+          for (int q = 0; q < 3; ++q) t += ah[k * 3 + q] * bl[q];
+          rhs[a.pose * 6 + k] += t;
+        }
+      }
+    }
+  }
+  return true;
+}
+
+// In-place band Cholesky (left-looking, column by column; the rows of a
+// column in parallel).  False when not positive definite.
+bool band_cholesky(Band& B, int threads) {
+  const size_t n = B.n, W = B.W;
+  for (size_t j = 0; j < n; ++j) {
+    const size_t k0 = j > W ? j - W : 0;
+    double d = B.at(j, j);
+    for (size_t k = k0; k < j; ++k) d -= B.at(j, k) * B.at(j, k);
+    if (!(d > 0.0) || !std::isfinite(d)) return false;
+    const double ljj = std::sqrt(d);
+    B.at(j, j) = ljj;
+    const size_t i1 = std::min(n - 1, j + W);
+#pragma omp parallel for schedule(static) num_threads(threads) if (i1 - j > 64)
+    for (long long ii = (long long)j + 1; ii <= (long long)i1; ++ii) {
+      const size_t i = (size_t)ii;
+      const size_t q0 = std::max(k0, i > W ? i - W : 0);
+      double t = B.at(i, j);
+      for (size_t k = q0; k < j; ++k) t -= B.at(i, k) * B.at(j, k);
+      B.at(i, j) = t / ljj;
+    }
+  }
+  return true;
+}
+
+void band_solve(const Band& B, std::vector<double>& x) {
+  const size_t n = B.n, W = B.W;
+  for (size_t i = 0; i < n; ++i) {
+    double s = x[i];
+    for (size_t k = i > W ? i - W : 0; k < i; ++k) s -= B.at(i, k) * x[k];
+    x[i] = s / B.at(i, i);
+  }
+  for (size_t ii = n; ii-- > 0;) {
+    double s = x[ii];
+    for (size_t k = ii + 1; k <= std::min(n - 1, ii + W); ++k) s -= B.at(k, ii) * x[k];
+    x[ii] = s / B.at(ii, ii);
+  }
+}
+
 // solve_step (normal_equations.rs:1314-1733).  Returns false on
 // BaError::SingularSystem.
 bool solve_step(const Normal& N, size_t np, size_t nl, double lambda, int solver,
@@ -880,18 +1044,31 @@ bool solve_step(const Normal& N, size_t np, size_t nl, double lambda, int solver
   }
   std::vector<double> s, rhs, hinv;
   std::vector<uint8_t> ok;
-  reduce(N, np, nl, lambda, threads, s, rhs, ok, hinv);
-  const size_t dim = np * 6;
-  std::vector<double> x = rhs;
-  std::vector<double> a = s;
-  if (cholesky(a, dim, threads)) {
-    cholesky_solve(a, dim, x);
+  Band band;
+  if (solver == 2 && reduce_banded(N, np, nl, lambda, threads, band, rhs, ok, hinv)) {
+    // LinearSolver::Sparse, factored in band storage (Cholesky only).
+    if (!band_cholesky(band, threads)) return false;
+    std::vector<double> x(np * 6);
+    for (size_t p = 0; p < np; ++p)
+      for (int r = 0; r < 6; ++r) x[6 * band.pos[p] + r] = rhs[p * 6 + r];
+    band_solve(band, x);
+    dp.resize(np * 6);
+    for (size_t p = 0; p < np; ++p)
+      for (int r = 0; r < 6; ++r) dp[p * 6 + r] = x[6 * band.pos[p] + r];
   } else {
-    if (solver == 1) return false;  // LinearSolver::Sparse: block Cholesky only
-    x = rhs;
-    if (!lu_solve(s, dim, x)) return false;
+    reduce(N, np, nl, lambda, threads, s, rhs, ok, hinv);
+    const size_t dim = np * 6;
+    std::vector<double> x = rhs;
+    std::vector<double> a = s;
+    if (cholesky(a, dim, threads)) {
+      cholesky_solve(a, dim, x);
+    } else {
+      if (solver >= 1) return false;  // LinearSolver::Sparse: block Cholesky only
+      x = rhs;
+      if (!lu_solve(s, dim, x)) return false;
+    }
+    dp = x;
   }
-  dp = x;
   // Back-substitution (normal_equations.rs:1717-1733).
 #pragma omp parallel for schedule(static) num_threads(threads)
   for (long long ll = 0; ll < (long long)nl; ++ll) {
@@ -1016,6 +1193,390 @@ void store_problem(const Problem& P, vlba_problem* p) {
     p->landmarks[3 * i + 2] = P.points[i].z;
   }
 }
+
+// ------------------------------------------------ matrix-free implicit Schur
+// ImplicitSchurOperator (bundle/implicit_schur.rs:108-300): the reduced
+// camera system S = D + lambda I - sum_l sum_(a,b) A_a H_l^-1 A_b^T applied
+// without forming it.  Errors mirror ImplicitSchurError; the LM treats any of
+// them as BaError::SingularSystem (bundle/lm.rs:574-590: reject, lambda up).
+enum MfError {
+  kMfOk = 0,
+  kMfNonFinite = 1,
+  kMfNonSpdPreconditioner = 2,
+  kMfMaxIterations = 3,
+  kMfNonPositiveCurvature = 4,
+  kMfResidualCheckFailed = 5,
+  kMfEmptySystem = 6,
+  kMfInvalidTolerance = 7,
+};
+
+bool all_finite(const double* v, size_t n) {
+  for (size_t i = 0; i < n; ++i)
+    if (!std::isfinite(v[i])) return false;
+  return true;
+}
+
+// In-place inverse of the SPD n x n row-major matrix through its Cholesky
+// factor (nalgebra block.cholesky().inverse()); false when not positive
+// definite.
+bool spd_inverse(std::vector<double>& a, size_t n) {
+  std::vector<double> l = a;
+  if (!cholesky(l, n, 1)) return false;
+  std::vector<double> col(n);
+  for (size_t c = 0; c < n; ++c) {
+    std::fill(col.begin(), col.end(), 0.0);
+    col[c] = 1.0;
+    cholesky_solve(l, n, col);
+    for (size_t r = 0; r < n; ++r) a[r * n + c] = col[r];
+  }
+  return true;
+}
+
+struct MfOperator {
+  size_t np = 0, nl = 0;
+  const Normal* N = nullptr;
+  std::vector<double> diag;    // [36 np] damped pose blocks
+  std::vector<double> hinv;    // [9 nl] damped landmark inverses
+  std::vector<uint8_t> inv_ok; // try_inverse succeeded
+  std::vector<double> pinv;    // [36 np] block-Jacobi inverses
+  std::vector<std::vector<double>> cluster;  // cluster8 inverses (6k x 6k)
+  std::vector<double> rhs;     // [6 np]
+  // Per pose, its cross blocks (landmark, index) in landmark order, so the
+  // parallel apply subtracts them in the serial order of the reference.
+  std::vector<std::vector<std::pair<uint32_t, uint32_t>>> at_pose;
+};
+
+// ImplicitSchurOperator::new_with_debug (implicit_schur.rs:133-300).
+int mf_build(const Normal& N, size_t np, size_t nl, double lambda, int threads, MfOperator* op) {
+  if (!std::isfinite(lambda) || lambda < 0.0) return kMfNonFinite;
+  if (np == 0) return kMfEmptySystem;
+  op->np = np;
+  op->nl = nl;
+  op->N = &N;
+  if (!all_finite(N.b_p.data(), N.b_p.size()) || !all_finite(N.h_pp.data(), N.h_pp.size()))
+    return kMfNonFinite;
+  op->diag = N.h_pp;
+  if (lambda > 0.0)
+    for (size_t p = 0; p < np; ++p)
+      for (int c = 0; c < 6; ++c) op->diag[p * 36 + c * 7] += lambda;
+  op->hinv.assign(nl * 9, 0.0);
+  op->inv_ok.assign(nl, 0);
+  op->rhs.resize(np * 6);
+  for (size_t i = 0; i < np * 6; ++i) op->rhs[i] = -N.b_p[i];
+  for (size_t l = 0; l < nl; ++l) {
+    if (!all_finite(&N.h_ll[l * 9], 9) || !all_finite(&N.b_l[l * 3], 3)) return kMfNonFinite;
+    for (const Cross& c : N.cross[l])
+      if (!all_finite(c.a, 18)) return kMfNonFinite;
+    double h[9];
+    std::memcpy(h, &N.h_ll[l * 9], sizeof h);
+    if (lambda > 0.0) { h[0] += lambda; h[4] += lambda; h[8] += lambda; }
+    double* hi = &op->hinv[l * 9];
+    if (!try_inverse3(h, hi)) continue;  // skipped, as solve_step skips it
+    if (!all_finite(hi, 9)) return kMfNonFinite;
+    op->inv_ok[l] = 1;
+    // rhs += A H^-1 b_l per cross block.
+    const double* bl = &N.b_l[l * 3];
+    const double v[3] = {hi[0] * bl[0] + hi[1] * bl[1] + hi[2] * bl[2],
+                         hi[3] * bl[0] + hi[4] * bl[1] + hi[5] * bl[2],
+                         hi[6] * bl[0] + hi[7] * bl[1] + hi[8] * bl[2]};
+    for (const Cross& c : N.cross[l])
+      for (int r = 0; r < 6; ++r)
+        op->rhs[c.pose * 6 + r] += c.a[r * 3] * v[0] + c.a[r * 3 + 1] * v[1] + c.a[r * 3 + 2] * v[2];
+  }
+  if (!all_finite(op->rhs.data(), op->rhs.size())) return kMfNonFinite;
+  // Block-Jacobi: D + lambda - G H^-1 G^T with the cross blocks of one pose
+  // grouped first (two sensors of one rig frame share the pose block).
+  op->pinv = op->diag;
+  for (size_t l = 0; l < nl; ++l) {
+    if (!op->inv_ok[l]) continue;
+    const std::vector<Cross>& cr = N.cross[l];
+    std::vector<std::pair<uint32_t, std::array<double, 18>>> grouped;  // ascending pose
+    for (const Cross& c : cr) {
+      auto it = std::lower_bound(grouped.begin(), grouped.end(), c.pose,
+                                 [](const auto& e, uint32_t p) { return e.first < p; });
+      if (it == grouped.end() || it->first != c.pose) {
+        std::array<double, 18> z{};
+        it = grouped.insert(it, {c.pose, z});
+      }
+      for (int e = 0; e < 18; ++e) it->second[e] += c.a[e];
+    }
+    const double* hi = &op->hinv[l * 9];
+    for (const auto& g : grouped) {
+      double gh[18];
+      for (int r = 0; r < 6; ++r)
+        for (int c = 0; c < 3; ++c)
+          gh[r * 3 + c] = g.second[r * 3] * hi[c] + g.second[r * 3 + 1] * hi[3 + c] +
+                          g.second[r * 3 + 2] * hi[6 + c];
+      double* blk = &op->pinv[g.first * 36];
+      for (int r = 0; r < 6; ++r)
+        for (int c = 0; c < 6; ++c)
+          blk[r * 6 + c] -= gh[r * 3] * g.second[c * 3] + gh[r * 3 + 1] * g.second[c * 3 + 1] +
+                            gh[r * 3 + 2] * g.second[c * 3 + 2];
+    }
+  }
+  if (!all_finite(op->pinv.data(), op->pinv.size())) return kMfNonFinite;
+  for (size_t p = 0; p < np; ++p) {
+    std::vector<double> blk(op->pinv.begin() + p * 36, op->pinv.begin() + p * 36 + 36);
+    if (!spd_inverse(blk, 6)) return kMfNonSpdPreconditioner;
+    if (!all_finite(blk.data(), 36)) return kMfNonFinite;
+    std::copy(blk.begin(), blk.end(), op->pinv.begin() + p * 36);
+  }
+  op->at_pose.assign(np, {});
+  for (size_t l = 0; l < nl; ++l) {
+    if (!op->inv_ok[l]) continue;
+    for (uint32_t k = 0; k < (uint32_t)N.cross[l].size(); ++k)
+      op->at_pose[N.cross[l][k].pose].push_back({(uint32_t)l, k});
+  }
+  (void)threads;
+  return kMfOk;
+}
+
+// with_cluster8 (implicit_schur.rs:302-376): principal Schur blocks of
+// consecutive groups of eight poses, inverted by Cholesky; replaces the
+// block-Jacobi preconditioner.
+int mf_cluster8(MfOperator* op) {
+  constexpr size_t K = 8;
+  const size_t np = op->np;
+  const size_t nc = (np + K - 1) / K;
+  op->cluster.assign(nc, {});
+  for (size_t c = 0; c < nc; ++c) {
+    const size_t n = std::min(K, np - c * K) * 6;
+    std::vector<double>& b = op->cluster[c];
+    b.assign(n * n, 0.0);
+    for (size_t s = 0; s < n / 6; ++s)
+      for (int r = 0; r < 6; ++r)
+        for (int q = 0; q < 6; ++q) b[(s * 6 + r) * n + s * 6 + q] = op->diag[(c * K + s) * 36 + r * 6 + q];
+  }
+  const Normal& N = *op->N;
+  for (size_t l = 0; l < op->nl; ++l) {
+    if (!op->inv_ok[l]) continue;
+    // Cross sums per pose, members per cluster in first-seen order.
+    std::vector<std::pair<uint32_t, std::array<double, 18>>> sums;  // first-seen order
+    for (const Cross& x : N.cross[l]) {
+      auto it = std::find_if(sums.begin(), sums.end(), [&](const auto& e) { return e.first == x.pose; });
+      if (it == sums.end()) {
+        std::array<double, 18> z{};
+        sums.push_back({x.pose, z});
+        it = sums.end() - 1;
+      }
+      for (int e = 0; e < 18; ++e) it->second[e] += x.a[e];
+    }
+    const double* hi = &op->hinv[l * 9];
+    for (const auto& a : sums) {
+      double left[18];
+      for (int r = 0; r < 6; ++r)
+        for (int c = 0; c < 3; ++c)
+          left[r * 3 + c] = a.second[r * 3] * hi[c] + a.second[r * 3 + 1] * hi[3 + c] +
+                            a.second[r * 3 + 2] * hi[6 + c];
+      for (const auto& b : sums) {
+        if (a.first / K != b.first / K) continue;
+        std::vector<double>& blk = op->cluster[a.first / K];
+        const size_t n = (size_t)std::sqrt((double)blk.size());
+        for (int r = 0; r < 6; ++r)
+          for (int c = 0; c < 6; ++c)
+            blk[((a.first % K) * 6 + r) * n + (b.first % K) * 6 + c] -=
+                left[r * 3] * b.second[c * 3] + left[r * 3 + 1] * b.second[c * 3 + 1] +
+                left[r * 3 + 2] * b.second[c * 3 + 2];
+      }
+    }
+  }
+  for (size_t c = 0; c < nc; ++c) {
+    std::vector<double>& blk = op->cluster[c];
+    if (!all_finite(blk.data(), blk.size())) return kMfNonFinite;
+    const size_t n = (size_t)std::sqrt((double)blk.size());
+    if (!spd_inverse(blk, n)) return kMfNonSpdPreconditioner;
+    if (!all_finite(blk.data(), blk.size())) return kMfNonFinite;
+  }
+  return kMfOk;
+}
+
+// apply (implicit_schur.rs:390-431): D x - sum_l sum_a A_a H^-1 (sum_b A_b^T
+// x_b), every cross block kept (repeated pose slots are separate sensor
+// rows).  Per landmark in parallel, then per pose in landmark order.
+void mf_apply(const MfOperator& op, const double* x, double* out, int threads) {
+  const Normal& N = *op.N;
+  std::vector<double> red(op.nl * 3, 0.0);
+#pragma omp parallel for schedule(static) num_threads(threads)
+  for (long long ll = 0; ll < (long long)op.nl; ++ll) {
+    const size_t l = (size_t)ll;
+    if (!op.inv_ok[l]) continue;
+    double pr[3] = {0.0, 0.0, 0.0};
+    for (const Cross& c : N.cross[l]) {
+      const double* xp = x + c.pose * 6;
+      for (int k = 0; k < 3; ++k) {
+        double t = 0.0;
+        for (int r = 0; r < 6; ++r) t += c.a[r * 3 + k] * xp[r];
+        pr[k] += t;
+      }
+    }
+    const double* hi = &op.hinv[l * 9];
+    for (int k = 0; k < 3; ++k) red[l * 3 + k] = hi[k * 3] * pr[0] + hi[k * 3 + 1] * pr[1] + hi[k * 3 + 2] * pr[2];
+  }
+#pragma omp parallel for schedule(static) num_threads(threads)
+  for (long long pp = 0; pp < (long long)op.np; ++pp) {
+    const size_t p = (size_t)pp;
+    const double* blk = &op.diag[p * 36];
+    const double* xp = x + p * 6;
+    double o[6];
+    for (int r = 0; r < 6; ++r) {
+      double t = 0.0;
+      for (int c = 0; c < 6; ++c) t += blk[r * 6 + c] * xp[c];
+      o[r] = t;
+    }
+    for (const auto& lk : op.at_pose[p]) {
+      const Cross& c = N.cross[lk.first][lk.second];
+      const double* rl = &red[lk.first * 3];
+      for (int r = 0; r < 6; ++r) o[r] -= c.a[r * 3] * rl[0] + c.a[r * 3 + 1] * rl[1] + c.a[r * 3 + 2] * rl[2];
+    }
+    for (int r = 0; r < 6; ++r) out[p * 6 + r] = o[r];
+  }
+}
+
+// apply_preconditioner (implicit_schur.rs:433-473).
+void mf_precondition(const MfOperator& op, const double* r, double* z) {
+  if (!op.cluster.empty()) {
+    size_t off = 0;
+    for (const std::vector<double>& inv : op.cluster) {
+      const size_t n = (size_t)std::sqrt((double)inv.size());
+      for (size_t a = 0; a < n; ++a) {
+        double t = 0.0;
+        for (size_t b = 0; b < n; ++b) t += inv[a * n + b] * r[off + b];
+        z[off + a] = t;
+      }
+      off += n;
+    }
+    return;
+  }
+  for (size_t p = 0; p < op.np; ++p) {
+    const double* blk = &op.pinv[p * 36];
+    for (int a = 0; a < 6; ++a) {
+      double t = 0.0;
+      for (int b = 0; b < 6; ++b) t += blk[a * 6 + b] * r[p * 6 + b];
+      z[p * 6 + a] = t;
+    }
+  }
+}
+
+double dot(const std::vector<double>& a, const std::vector<double>& b) {
+  double s = 0.0;
+  for (size_t i = 0; i < a.size(); ++i) s += a[i] * b[i];
+  return s;
+}
+
+struct MfPcgOptions {
+  uint32_t max_iterations;
+  double relative_tolerance, absolute_tolerance;
+};
+
+// solve_pcg (implicit_schur.rs:475-736 with no restarts): x = 0, r = b;
+// stop once |r| <= max(abs, rel |b|) and the true residual |b - A x| agrees,
+// else fail: MaxIterations at the cap (unless the true residual meets the
+// target there), NonPositiveCurvature for p.Ap <= 0 or r.z <= 0,
+// ResidualCheckFailed when the recursive residual met the target but the
+// true one did not.
+int mf_solve_pcg(const MfOperator& op, const std::vector<double>& b, const MfPcgOptions& o,
+                 int threads, std::vector<double>& x, uint32_t* iterations, double* residual,
+                 double* target_out) {
+  const size_t n = op.np * 6;
+  *iterations = 0;
+  if (!all_finite(b.data(), n)) return kMfNonFinite;
+  if (!std::isfinite(o.relative_tolerance) || o.relative_tolerance < 0.0 ||
+      !std::isfinite(o.absolute_tolerance) || o.absolute_tolerance < 0.0)
+    return kMfInvalidTolerance;
+  const double bnorm = std::sqrt(dot(b, b));
+  const double target = std::max(o.absolute_tolerance, o.relative_tolerance * bnorm);
+  if (target_out) *target_out = target;
+  if (!std::isfinite(target)) return kMfNonFinite;
+  x.assign(n, 0.0);
+  std::vector<double> r = b, z(n), p(n), q(n);
+  double rn = std::sqrt(dot(r, r));
+  if (!std::isfinite(rn)) return kMfNonFinite;
+  auto true_norm = [&]() {
+    mf_apply(op, x.data(), q.data(), threads);
+    double s = 0.0;
+    for (size_t i = 0; i < n; ++i) s += (b[i] - q[i]) * (b[i] - q[i]);
+    return std::sqrt(s);
+  };
+  if (rn <= target) {
+    const double t = true_norm();
+    *residual = t;
+    return t <= target ? kMfOk : kMfResidualCheckFailed;
+  }
+  if (o.max_iterations == 0) {
+    *residual = rn;
+    return kMfMaxIterations;
+  }
+  mf_precondition(op, r.data(), z.data());
+  double rho = dot(r, z);
+  if (!std::isfinite(rho) || rho <= 0.0) return kMfNonPositiveCurvature;
+  p = z;
+  for (uint32_t it = 1; it <= o.max_iterations; ++it) {
+    mf_apply(op, p.data(), q.data(), threads);
+    const double curv = dot(p, q);
+    if (!std::isfinite(curv) || curv <= 0.0) return kMfNonPositiveCurvature;
+    const double alpha = rho / curv;
+    if (!std::isfinite(alpha)) return kMfNonFinite;
+    for (size_t i = 0; i < n; ++i) {
+      x[i] += alpha * p[i];
+      r[i] -= alpha * q[i];
+    }
+    rn = std::sqrt(dot(r, r));
+    *iterations = it;
+    if (!all_finite(x.data(), n) || !std::isfinite(rn)) return kMfNonFinite;
+    if (rn <= target) {
+      const double t = true_norm();
+      *residual = t;
+      return t <= target ? kMfOk : kMfResidualCheckFailed;
+    }
+    if (it == o.max_iterations) {
+      const double t = true_norm();
+      *residual = t;
+      return t <= target ? kMfOk : kMfMaxIterations;
+    }
+    mf_precondition(op, r.data(), z.data());
+    const double next = dot(r, z);
+    if (!std::isfinite(next) || next <= 0.0) return kMfNonPositiveCurvature;
+    const double beta = next / rho;
+    if (!std::isfinite(beta)) return kMfNonFinite;
+    for (size_t i = 0; i < n; ++i) p[i] = z[i] + beta * p[i];
+    rho = next;
+  }
+  return kMfMaxIterations;
+}
+
+// complete_delta (implicit_schur.rs:789-828): dl = H^-1 (-b_l - sum A^T dp).
+int mf_complete_delta(const MfOperator& op, const std::vector<double>& dp, int threads,
+                      std::vector<double>& dl) {
+  const Normal& N = *op.N;
+  if (!all_finite(dp.data(), dp.size())) return kMfNonFinite;
+  dl.assign(op.nl * 3, 0.0);
+  bool bad = false;
+#pragma omp parallel for schedule(static) num_threads(threads) reduction(|| : bad)
+  for (long long ll = 0; ll < (long long)op.nl; ++ll) {
+    const size_t l = (size_t)ll;
+    if (!op.inv_ok[l]) continue;
+    double acc[3] = {-N.b_l[l * 3], -N.b_l[l * 3 + 1], -N.b_l[l * 3 + 2]};
+    for (const Cross& c : N.cross[l])
+      for (int k = 0; k < 3; ++k) {
+        double t = 0.0;
+        for (int r = 0; r < 6; ++r) t += c.a[r * 3 + k] * dp[c.pose * 6 + r];
+        acc[k] -= t;
+      }
+    const double* hi = &op.hinv[l * 9];
+    for (int k = 0; k < 3; ++k) {
+      dl[l * 3 + k] = hi[k * 3] * acc[0] + hi[k * 3 + 1] * acc[1] + hi[k * 3 + 2] * acc[2];
+      if (!std::isfinite(dl[l * 3 + k])) bad = true;
+    }
+  }
+  return bad ? kMfNonFinite : kMfOk;
+}
+
+// The reference LM loop (lm.rs:356-1009, Legacy or matrix-free backend): the
+// linear solve is `step`, which returns false for BaError::SingularSystem.
+using StepFn = std::function<bool(const Normal&, size_t, size_t, double, std::vector<double>&,
+                                  std::vector<double>&)>;
+int run_lm(vlba_problem* p, const vlba_config* cfg, int threads, vlba_result* res,
+           vlba_iteration* its, uint32_t cap, const StepFn& step);
 
 }  // namespace
 
@@ -1142,11 +1703,12 @@ int vlba_oracle_reduced_system(const vlba_problem* p, const vlba_config* cfg, do
   return VLBA_OK;
 }
 
-// BundleAdjustment::optimize (lm.rs:162-1017, Legacy backend).
-// solver: 0 = LinearSolver::Dense (Cholesky, LU fallback), 1 = Sparse
-// (Cholesky only).  threads <= 0: all.
-int vlba_oracle_optimize(vlba_problem* p, const vlba_config* cfg, int solver, int threads,
-                         vlba_result* res, vlba_iteration* its, uint32_t cap) {
+}  // extern "C"
+
+namespace {
+
+int run_lm(vlba_problem* p, const vlba_config* cfg, int threads, vlba_result* res,
+           vlba_iteration* its, uint32_t cap, const StepFn& step) {
   Problem P;
   int status;
   uint64_t err_index = 0;
@@ -1192,7 +1754,7 @@ int vlba_oracle_optimize(vlba_problem* p, const vlba_config* cfg, int solver, in
     const std::vector<V3> saved_points = P.points;
     const double cost_before = current_cost;
     std::vector<double> dp, dl;
-    if (!solve_step(N, np, nl, lambda, solver, nt, dp, dl)) {
+    if (!step(N, np, nl, lambda, dp, dl)) {
       lambda = std::min(lambda * cfg->lambda_increase_factor, cfg->max_lambda);
       push(iteration, cost_before, cost_before, 0.0, 0.0, lambda, false);
       if (lambda >= cfg->max_lambda) break;
@@ -1263,6 +1825,136 @@ int vlba_oracle_optimize(vlba_problem* p, const vlba_config* cfg, int solver, in
     res->final_nonprojectable = final_nonproj;
   }
   return VLBA_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+// BundleAdjustment::optimize (lm.rs:162-1017, Legacy backend).
+// solver: 0 = LinearSolver::Dense (Cholesky, LU fallback), 1 = Sparse
+// (Cholesky only), 2 = Sparse factored in band storage when the reduced
+// system is banded in the capture or fold order (else as 1).  threads <= 0:
+// all.
+int vlba_oracle_optimize(vlba_problem* p, const vlba_config* cfg, int solver, int threads,
+                         vlba_result* res, vlba_iteration* its, uint32_t cap) {
+  const int nt = threads_or_default(threads);
+  return run_lm(p, cfg, threads, res, its, cap,
+                [&](const Normal& N, size_t np, size_t nl, double lambda, std::vector<double>& dp,
+                    std::vector<double>& dl) {
+                  return solve_step(N, np, nl, lambda, solver, nt, dp, dl);
+                });
+}
+
+// BundleAdjustment::optimize_matrix_free (bundle/optimize.rs:105-139): the
+// same LM loop with the landmark-eliminated system solved by bounded PCG on
+// the implicit Schur operator (MatrixFreeBaOptions: max_pcg_iterations,
+// pcg_relative_tolerance, pcg_absolute_tolerance; defaults 128, 1e-12,
+// 1e-12, bundle/mod.rs:781-798), block-Jacobi preconditioned or, with
+// cluster8, by the principal Schur blocks of groups of eight poses
+// (optimize_matrix_free_cluster8, optimize.rs:192-208).  A failed solve (any
+// ImplicitSchurError) rejects the step and raises lambda, as SingularSystem
+// does (lm.rs:574-600).  pcg_iterations (may be NULL) receives the total PCG
+// iterations, failures (may be NULL) the failed solves.  Requires at least
+// one variable pose (validate_matrix_free_entry, optimize.rs:386-431).
+int vlba_oracle_optimize_matrix_free(vlba_problem* p, const vlba_config* cfg,
+                                     uint32_t max_pcg_iterations, double pcg_relative_tolerance,
+                                     double pcg_absolute_tolerance, int cluster8, int threads,
+                                     vlba_result* res, vlba_iteration* its, uint32_t cap,
+                                     uint64_t* pcg_iterations, uint32_t* failures) {
+  if (!cfg || cfg->max_iterations == 0) return VLBA_ERR_INVALID_ARGUMENT;
+  if (cfg->has_initial_lambda && !(std::isfinite(cfg->initial_lambda) && cfg->initial_lambda > 0.0))
+    return VLBA_ERR_INVALID_ARGUMENT;
+  if (p) {
+    bool any_var = false;
+    for (uint64_t i = 0; i < p->num_poses && !any_var; ++i)
+      any_var = !(p->pose_fixed && p->pose_fixed[i]);
+    if (!any_var) return VLBA_DECLINED;  // MatrixFreeBaError::Ineligible
+  }
+  const int nt = threads_or_default(threads);
+  uint64_t total = 0;
+  uint32_t failed = 0;
+  const MfPcgOptions opt{max_pcg_iterations, pcg_relative_tolerance, pcg_absolute_tolerance};
+  const int st = run_lm(
+      p, cfg, threads, res, its, cap,
+      [&](const Normal& N, size_t np, size_t nl, double lambda, std::vector<double>& dp,
+          std::vector<double>& dl) {
+        MfOperator op;
+        int e = mf_build(N, np, nl, lambda, nt, &op);
+        if (e == kMfOk && cluster8) e = mf_cluster8(&op);
+        uint32_t iters = 0;
+        double resid = 0.0, target = 0.0;
+        if (e == kMfOk) e = mf_solve_pcg(op, op.rhs, opt, nt, dp, &iters, &resid, &target);
+        total += iters;
+        if (e == kMfOk) e = mf_complete_delta(op, dp, nt, dl);
+        if (e != kMfOk) ++failed;
+        return e == kMfOk;
+      });
+  if (pcg_iterations) *pcg_iterations = total;
+  if (failures) *failures = failed;
+  return st;
+}
+
+// The implicit Schur operator on a normal-equation system given directly
+// (NormalEquationsBa with a PoseDiagonal camera Hessian): np pose blocks
+// diag[36 np] (row-major), b_p[6 np], nl landmarks h_ll[9 nl], b_l[3 nl],
+// and per landmark cross_count[l] cross blocks (cross_pose, cross_block 6x3
+// row-major) in order.  Outputs (each may be NULL): rhs[6 np]; apply_out =
+// S x (x[6 np]); precond_out = M^-1 probe; with solve, the PCG solution
+// solution[6 np] of S x = rhs_in (rhs_in NULL: the operator's rhs) under
+// the options, its iterations, true residual and target, and the landmark
+// step delta_l[3 nl] of that solution.  Returns the ImplicitSchurError code
+// (0 = ok) of the first failing step.  Test hook for the reference's
+// operator tests (implicit_schur.rs:952-1619).
+int vlba_oracle_mf_system(uint32_t np, const double* diag, const double* b_p, uint32_t nl,
+                          const double* h_ll, const double* b_l, const uint32_t* cross_count,
+                          const uint32_t* cross_pose, const double* cross_block, double lambda,
+                          int cluster8, const double* x, double* apply_out, const double* probe,
+                          double* precond_out, double* rhs_out, int solve, const double* rhs_in,
+                          uint32_t max_iterations, double relative_tolerance,
+                          double absolute_tolerance, double* solution, uint32_t* iterations,
+                          double* residual, double* target, double* delta_l) {
+  Normal N;
+  N.h_pp.assign(diag, diag + 36 * (size_t)np);
+  N.b_p.assign(b_p, b_p + 6 * (size_t)np);
+  N.h_ll.assign(h_ll, h_ll + 9 * (size_t)nl);
+  N.b_l.assign(b_l, b_l + 3 * (size_t)nl);
+  N.cross.assign(nl, {});
+  size_t at = 0;
+  for (uint32_t l = 0; l < nl; ++l)
+    for (uint32_t k = 0; k < cross_count[l]; ++k, ++at) {
+      Cross c;
+      c.pose = cross_pose[at];
+      if (c.pose >= np) return kMfNonFinite;
+      std::memcpy(c.a, cross_block + 18 * at, sizeof c.a);
+      N.cross[l].push_back(c);
+    }
+  MfOperator op;
+  int e = mf_build(N, np, nl, lambda, 1, &op);
+  if (e == kMfOk && cluster8) e = mf_cluster8(&op);
+  if (e != kMfOk) return e;
+  const size_t n = 6 * (size_t)np;
+  if (rhs_out) std::copy(op.rhs.begin(), op.rhs.end(), rhs_out);
+  if (x && apply_out) mf_apply(op, x, apply_out, 1);
+  if (probe && precond_out) mf_precondition(op, probe, precond_out);
+  if (!solve) return kMfOk;
+  std::vector<double> b = rhs_in ? std::vector<double>(rhs_in, rhs_in + n) : op.rhs;
+  std::vector<double> sol;
+  uint32_t it = 0;
+  double r = 0.0, t = 0.0;
+  e = mf_solve_pcg(op, b, MfPcgOptions{max_iterations, relative_tolerance, absolute_tolerance}, 1,
+                   sol, &it, &r, &t);
+  if (iterations) *iterations = it;
+  if (residual) *residual = r;
+  if (target) *target = t;
+  if (solution && sol.size() == n) std::copy(sol.begin(), sol.end(), solution);
+  if (e != kMfOk) return e;
+  if (delta_l) {
+    std::vector<double> dl;
+    e = mf_complete_delta(op, sol, 1, dl);
+    std::copy(dl.begin(), dl.end(), delta_l);
+  }
+  return e;
 }
 
 // ---------------------------------------------------------------------------

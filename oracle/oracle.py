@@ -59,6 +59,19 @@ EXPORTS = {
         [P(_abi.Problem), P(_abi.Config), C.c_int, C.c_int, P(_abi.Result),
          P(_abi.Iteration), C.c_uint32],
     ),
+    "vlba_oracle_optimize_matrix_free": (
+        C.c_int,
+        [P(_abi.Problem), P(_abi.Config), C.c_uint32, C.c_double, C.c_double, C.c_int, C.c_int,
+         P(_abi.Result), P(_abi.Iteration), C.c_uint32, P(C.c_uint64), P(C.c_uint32)],
+    ),
+    "vlba_oracle_mf_system": (
+        C.c_int,
+        [C.c_uint32, P(C.c_double), P(C.c_double), C.c_uint32, P(C.c_double), P(C.c_double),
+         P(C.c_uint32), P(C.c_uint32), P(C.c_double), C.c_double, C.c_int, P(C.c_double),
+         P(C.c_double), P(C.c_double), P(C.c_double), P(C.c_double), C.c_int, P(C.c_double),
+         C.c_uint32, C.c_double, C.c_double, P(C.c_double), P(C.c_uint32), P(C.c_double),
+         P(C.c_double), P(C.c_double)],
+    ),
 }
 
 _LIB = None
@@ -84,6 +97,9 @@ def _dp(a):
 
 SPARSE = 1
 DENSE = 0
+# LinearSolver::Sparse factored in band storage (capture or fold order) when the
+# reduced system is banded; otherwise as SPARSE.
+SPARSE_BANDED = 2
 
 
 def optimize(packed: PackedProblem, config: BaConfig, solver: int = DENSE, threads: int = 0):
@@ -96,6 +112,85 @@ def optimize(packed: PackedProblem, config: BaConfig, solver: int = DENSE, threa
     st = lib().vlba_oracle_optimize(C.byref(prob), C.byref(cfg), solver, threads,
                                     C.byref(res), iters, cap)
     return st, result_from_abi(res, iters, res.num_iterations)
+
+
+# ImplicitSchurError of the matrix-free restatement (implicit_schur.rs).
+MF_OK, MF_NON_FINITE, MF_NON_SPD_PRECONDITIONER, MF_MAX_ITERATIONS = 0, 1, 2, 3
+MF_NON_POSITIVE_CURVATURE, MF_RESIDUAL_CHECK_FAILED, MF_EMPTY_SYSTEM = 4, 5, 6
+MF_INVALID_TOLERANCE = 7
+
+
+def optimize_matrix_free(packed: PackedProblem, config: BaConfig, max_pcg_iterations: int = 128,
+                         pcg_relative_tolerance: float = 1e-12,
+                         pcg_absolute_tolerance: float = 1e-12, cluster8: bool = False,
+                         threads: int = 0):
+    """BundleAdjustment::optimize_matrix_free (bundle/optimize.rs:105-139)
+    in place on `packed`, the MatrixFreeBaOptions defaults as defaults:
+    (status, BaResult, total PCG iterations, failed linear solves)."""
+    prob = packed.abi()
+    cfg = config.to_abi()
+    res = _abi.Result()
+    cap = max(1, int(config.max_iterations))
+    iters = (_abi.Iteration * cap)()
+    total = C.c_uint64()
+    failed = C.c_uint32()
+    st = lib().vlba_oracle_optimize_matrix_free(
+        C.byref(prob), C.byref(cfg), int(max_pcg_iterations), float(pcg_relative_tolerance),
+        float(pcg_absolute_tolerance), int(bool(cluster8)), threads, C.byref(res), iters, cap,
+        C.byref(total), C.byref(failed))
+    return st, result_from_abi(res, iters, res.num_iterations), total.value, failed.value
+
+
+def mf_system(diag, b_p, h_ll, b_l, cross, lam, *, cluster8=False, x=None, probe=None,
+              solve=False, rhs=None, max_iterations=128, relative_tolerance=1e-12,
+              absolute_tolerance=1e-12):
+    """The matrix-free operator on a normal-equation system given directly
+    (NormalEquationsBa with pose blocks): diag (np,6,6), b_p (6 np), h_ll
+    (nl,3,3), b_l (nl,3), cross: per landmark a list of (pose, 6x3 block).
+    Returns a dict with the status and the requested outputs: rhs, apply
+    (S x), precond (M^-1 probe), and with solve the PCG solution,
+    iterations, residual, target and the landmark step delta_l."""
+    diag = np.ascontiguousarray(diag, np.float64).reshape(-1, 36)
+    npose = diag.shape[0]
+    b_p = np.ascontiguousarray(b_p, np.float64).reshape(-1)
+    h_ll = np.ascontiguousarray(h_ll, np.float64).reshape(-1, 9)
+    nl = h_ll.shape[0]
+    b_l = np.ascontiguousarray(b_l, np.float64).reshape(-1)
+    counts = np.array([len(c) for c in cross], np.uint32)
+    poses = np.array([p for c in cross for p, _ in c], np.uint32)
+    blocks = np.ascontiguousarray(
+        np.array([np.asarray(b, np.float64).reshape(6, 3) for c in cross for _, b in c]).reshape(-1))
+    n = 6 * npose
+    out = {"rhs": np.empty(n)}
+    none = P(C.c_double)()
+    args_x = none
+    if x is not None:
+        x = np.ascontiguousarray(x, np.float64)
+        out["apply"] = np.empty(n)
+        args_x = _dp(x)
+    args_probe = none
+    if probe is not None:
+        probe = np.ascontiguousarray(probe, np.float64)
+        out["precond"] = np.empty(n)
+        args_probe = _dp(probe)
+    sol = np.zeros(n)
+    dl = np.zeros(3 * nl)
+    it = C.c_uint32()
+    resid = C.c_double()
+    tgt = C.c_double()
+    rhs_arr = None if rhs is None else np.ascontiguousarray(rhs, np.float64)
+    st = lib().vlba_oracle_mf_system(
+        npose, _dp(diag), _dp(b_p), nl, _dp(h_ll), _dp(b_l), counts.ctypes.data_as(P(C.c_uint32)),
+        poses.ctypes.data_as(P(C.c_uint32)), _dp(blocks), float(lam), int(bool(cluster8)),
+        args_x, _dp(out["apply"]) if x is not None else none, args_probe,
+        _dp(out["precond"]) if probe is not None else none, _dp(out["rhs"]), int(bool(solve)),
+        none if rhs_arr is None else _dp(rhs_arr), int(max_iterations), float(relative_tolerance),
+        float(absolute_tolerance), _dp(sol), C.byref(it), C.byref(resid), C.byref(tgt), _dp(dl))
+    out["status"] = st
+    if solve:
+        out.update(solution=sol, iterations=it.value, residual=resid.value, target=tgt.value,
+                   delta_l=dl)
+    return out
 
 
 def cost(packed: PackedProblem, config: BaConfig | None = None, threads: int = 0):

@@ -55,6 +55,15 @@ def ring4m_config():
                     max_pcg_iterations=200, pcg_relative_tolerance=1e-6)
 
 
+def street20m_config():
+    """The benchmarked street-20m solve: Huber 1 px, 15 LM iterations, PCG
+    tolerance 1e-6 with at most 200 iterations on the device."""
+    from visloc_ba import BaConfig, RobustKernel
+
+    return BaConfig(max_iterations=15, robust_kernel=RobustKernel.huber(1.0),
+                    max_pcg_iterations=200, pcg_relative_tolerance=1e-6)
+
+
 def windows_config():
     """The benchmarked windows-512 solve: Huber 1 px, 10 LM iterations, PCG
     tolerance 1e-6 with at most 200 iterations on the device."""
@@ -84,18 +93,32 @@ def compare_state(final_cost: float, centers: np.ndarray, oracle_cost: float,
     return {"final_cost_rel": rel, "centre_err_of_extent": dc}
 
 
-def ring4m_parity(problem, final_cost: float, centers: np.ndarray):
-    """Error of a ring-4m solve (its final cost and camera centres) against
-    the oracle fixture; None when the fixture is absent or was made from a
-    different input."""
-    fx = load("ring4m")
+FIXTURES = {
+    "ring-4m": ("ring4m", "FP64 sparse Schur + block Cholesky LM, 30 iterations "
+                          "(tests/golden/ring4m_oracle.npz)"),
+    "street-20m": ("street20m", "FP64 sparse Schur + banded block Cholesky LM, 15 iterations "
+                                "(tests/golden/street20m_oracle.npz)"),
+}
+
+
+def workload_parity(workload: str, problem, final_cost: float, centers: np.ndarray):
+    """Error of a benchmarked solve (its final cost and camera centres)
+    against the oracle fixture of `workload`; None when the fixture is absent
+    or was made from a different input."""
+    if workload not in FIXTURES:
+        return None
+    name, what = FIXTURES[workload]
+    fx = load(name)
     if fx is None or str(fx["digest"]) != input_digest(problem):
         return None
     out = compare_state(final_cost, centers, float(fx["final_cost"]), fx["centers"],
                         float(fx["extent"]))
-    out.update({"oracle": "FP64 sparse Schur + block Cholesky LM, 30 iterations "
-                          "(tests/golden/ring4m_oracle.npz)",
-                "oracle_final_cost": float(fx["final_cost"]), "tolerance": TOLERANCE,
+    out.update({"oracle": what, "oracle_final_cost": float(fx["final_cost"]),
+                "tolerance": TOLERANCE,
                 "within_tolerance": bool(out["final_cost_rel"] <= TOLERANCE
                                          and out["centre_err_of_extent"] <= TOLERANCE)})
     return out
+
+
+def ring4m_parity(problem, final_cost: float, centers: np.ndarray):
+    return workload_parity("ring-4m", problem, final_cost, centers)

@@ -8,12 +8,14 @@ generator is caught instead of compared against a stale answer), the initial
 and final cost, the per-iteration trace (cost after each trial, accepted,
 lambda) and the camera centres of the final state (f64).
 
-    python tests/golden/make_parity_fixtures.py [ring-4m] [windows-512-sample]
+    python tests/golden/make_parity_fixtures.py [ring-4m] [windows-512-sample] [street-20m]
 
 ring-4m: 1,200 cameras, 500k points, 4.06M observations, Huber 1 px, 30 LM
 iterations, the oracle's sparse Schur + block Cholesky solve (SPARSE) on all
-host threads (about 3 minutes on 8 threads).  windows-512-sample: 32 windows
+host threads (about 5 minutes on 8 threads).  windows-512-sample: 32 windows
 of the windows-512 batch (every 16th), 10 LM iterations each, dense solve.
+street-20m: 5,600 cameras, ~19.7M observations, 15 LM iterations, the sparse
+solve in band storage (about 3 minutes on 8 threads).
 The expected values come from the oracle (this repository's FP64
 restatement of the reference solver), not from the Rust reference, which
 cannot run here.
@@ -32,7 +34,7 @@ sys.path[:0] = [ROOT, os.path.join(ROOT, "visloc-rs_b200")]
 import numpy as np  # noqa: E402
 
 from oracle.parity import (WINDOW_SAMPLE, fixture_path, input_digest,  # noqa: E402
-                           ring4m_config, windows_config)
+                           ring4m_config, street20m_config, windows_config)
 from visloc_ba import synth  # noqa: E402
 
 
@@ -55,6 +57,27 @@ def make_ring4m():
     print(f"ring-4m: oracle {time.time() - t0:.0f} s, cost {res.initial_cost:.10e} -> "
           f"{res.final_cost:.10e}, {len(res.iterations)} iterations")
     np.savez_compressed(fixture_path("ring4m"), digest=digest,
+                        initial_cost=res.initial_cost, final_cost=res.final_cost,
+                        extent=synth.scene_extent(q), centers=q.camera_centers(),
+                        **trace_arrays(res))
+
+
+def make_street20m():
+    """street-20m: 5,600 cameras on a closed street loop, ~2.9M facade points,
+    ~19.7M observations, Huber 1 px, 15 LM iterations; the oracle's Sparse
+    solve in band storage (the loop's reduced system is a cyclic band), all
+    host threads (about 10 s per LM iteration on 8 threads)."""
+    from oracle import oracle
+
+    p = synth.street_loop(seed=3000)
+    digest = input_digest(p)
+    q = p.copy()
+    t0 = time.time()
+    st, res = oracle.optimize(q, street20m_config(), solver=oracle.SPARSE_BANDED)
+    assert st == 0, st
+    print(f"street-20m: oracle {time.time() - t0:.0f} s, cost {res.initial_cost:.10e} -> "
+          f"{res.final_cost:.10e}, {len(res.iterations)} iterations")
+    np.savez_compressed(fixture_path("street20m"), digest=digest,
                         initial_cost=res.initial_cost, final_cost=res.final_cost,
                         extent=synth.scene_extent(q), centers=q.camera_centers(),
                         **trace_arrays(res))
@@ -88,8 +111,10 @@ def make_windows_sample():
 
 
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["ring-4m", "windows-512-sample"]
+    which = sys.argv[1:] or ["ring-4m", "windows-512-sample", "street-20m"]
     if "windows-512-sample" in which:
         make_windows_sample()
     if "ring-4m" in which:
         make_ring4m()
+    if "street-20m" in which:
+        make_street20m()
