@@ -241,6 +241,7 @@ typedef struct vlba_result {
   double device_ms;                /* device time of the LM iterations */
   double upload_ms;                /* host+device time of the upload */
   uint64_t kernel_launches;        /* kernels launched by the LM iterations */
+  uint64_t upload_bytes;           /* host -> device bytes of the upload (ABI version 4) */
 } vlba_result;
 
 /* Device layout of a problem, computed on the host without touching the GPU

@@ -170,3 +170,29 @@ def test_launch_shapes_do_not_change_results(solver):
     res = solver.batch_solve_uploaded()
     for a, b in zip(r0, res):
         assert a.final_cost == b.final_cost
+
+
+def test_device_built_terms_equal_the_host_build(solver):
+    """A problem of at least 200,000 observations solved alone has its Schur
+    terms built on the device; in a batch, the host builds them.  Both lay
+    each block's terms out in ascending point order, so the two solves are
+    bit-identical -- on a ring (dense reduced system) and a street loop
+    (banded, closed)."""
+    big_ring = synth.ring_problem(120, 40000, seed=43, width=2000, height=1500,
+                                  focal=(1500, 1500), k1=(0.0, 0.0), per_camera_intrinsics=False,
+                                  track=("geometric", 8.0, 2, 40))
+    street = synth.street_loop(400, 60000, seed=44, fixed=(0, 1, 200))
+    small = synth.ring_problem(8, 300, seed=45)
+    c = cfg(max_iterations=6)
+    for big in (big_ring, street):
+        assert big.num_observations >= 200_000
+        q = big.copy()
+        st, alone = solver.optimize(q, c)
+        assert st == _abi.OK, solver.last_error()
+        batch = [big.copy(), small.copy()]
+        statuses, results = solver.batch_optimize(batch, c)
+        assert statuses == [_abi.OK, _abi.OK]
+        assert results[0].final_cost == alone.final_cost
+        assert [i.pcg_iterations for i in results[0].iterations] == \
+            [i.pcg_iterations for i in alone.iterations]
+        assert same_state(batch[0], q)

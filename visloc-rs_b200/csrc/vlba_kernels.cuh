@@ -119,6 +119,34 @@ cudaError_t launch_el_prepare(const ElimDev& e, cudaStream_t s);
 cudaError_t launch_el_blocks(const ElimDev& e, cudaStream_t s);
 cudaError_t launch_el_outputs(const ElimDev& e, cudaStream_t s);
 
+// The Schur terms of one problem built on the device (vlba_pairs.cu): the
+// arrays of its plan the builders read, their scratch and outputs.
+struct RowsDev {
+  uint32_t nvar;               // variable camera slots (rows)
+  const uint32_t* cam_off;     // [nvar + 1] into cam_obs
+  const uint32_t* cam_obs;     // per slot, its observations ascending
+  const uint32_t* obs_point;
+  const uint32_t* obs_slot;
+  const uint8_t* point_var;
+  const uint32_t* pt_off;
+  uint2* tri;                  // [nvar (nvar - 1) / 2] per-row (column, terms) scratch
+  uint32_t* row_nblk;          // [nvar]
+  uint32_t* row_blk;           // [nvar + 1]
+  uint32_t* col;               // [nvar (nvar - 1) / 2] packed columns
+  uint32_t* count;             // [nvar (nvar - 1) / 2] packed term counts
+  uint32_t* flags;             // bit 0: a point seen twice by one slot; bit 1: a term
+                               // outside its block or a block left short
+};
+
+// Count each row's terms per column and pack the rows' (column, count)
+// lists by the prefix of their lengths (row_blk).
+cudaError_t launch_rows_count(const RowsDev& r, cudaStream_t s);
+// Write every term at its place: per block in point order (the host order).
+cudaError_t launch_rows_place(const RowsDev& r, const uint32_t* blk_off, const uint32_t* row_blk,
+                              const uint32_t* blk_col, uint2* pairs, cudaStream_t s);
+size_t rows_count_smem(uint32_t nvar);
+size_t rows_place_smem(uint32_t nvar);
+
 // Occupancy-derived grid of the persistent PCG kernel (0 if it cannot run).
 int pcg_grid_size(int tb, int sm_count);
 size_t pcg_smem_bytes(int tb);

@@ -1,0 +1,236 @@
+// vlba_pairs.cu -- the Schur terms of one problem's reduced system built on
+// the device at upload (the largest part of the plan: one 8-byte term per
+// pair of a variable point's observations by two variable cameras).
+//
+// The host plan (vlba_plan.cpp) lists the terms per block (camera pair
+// (i, j), i > j, blocks row-major, columns ascending), each block's terms in
+// ascending point order; the off-diagonal assembly sums them in that order,
+// so the order fixes every block's rounding.  Here:
+//
+//   k_rows_count  one block per camera row i: walks the row camera's
+//                 observations (ascending point order) and, for each, the
+//                 other observations of its point; counts the terms of each
+//                 column j < i in shared memory, then writes the row's
+//                 nonzero columns and counts in ascending column order.
+//                 A point seen twice by one camera (same-camera terms) sets
+//                 a flag: those plans are built on the host.
+//   k_rows_pack   the rows' lists, packed by the prefix of their lengths.
+//   k_rows_place  one warp per camera row: the row's observations in groups
+//                 of 32 consecutive ones (32 distinct points, ascending);
+//                 for each column, the lanes that have a term there take
+//                 consecutive places in lane order (a shared bit mask per
+//                 column and the lane's rank in it), so each block receives
+//                 its terms in ascending point order -- the host's order.
+//                 Every place is checked against its block's range; a term
+//                 outside it, or a block left short, sets the error flag
+//                 and writes nothing outside the array.
+//
+// The host lays out the blocks, tiles and destinations from the counts
+// (exactly as for terms it builds itself) between the two passes.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "vlba_kernels.cuh"
+
+namespace vlba {
+namespace {
+
+__global__ void __launch_bounds__(256) k_rows_count(RowsDev r) {
+  extern __shared__ uint32_t cnt[];  // [nvar]
+  __shared__ uint32_t s_part[256];
+  for (uint32_t i = blockIdx.x; i < r.nvar; i += gridDim.x) {
+    for (uint32_t j = threadIdx.x; j < r.nvar; j += blockDim.x) cnt[j] = 0u;
+    __syncthreads();
+    for (uint32_t q = r.cam_off[i] + threadIdx.x; q < r.cam_off[i + 1]; q += blockDim.x) {
+      const uint32_t a = r.cam_obs[q];
+      const uint32_t p = r.obs_point[a];
+      if (!r.point_var[p]) continue;
+      for (uint32_t b = r.pt_off[p]; b < r.pt_off[p + 1]; ++b) {
+        if (b == a) continue;
+        const uint32_t sb = r.obs_slot[b];
+        if (sb == kNone) continue;
+        if (sb == i) {
+          atomicOr(r.flags, 1u);  // same-camera terms: the host builds this plan
+        } else if (sb < i) {
+          atomicAdd(&cnt[sb], 1u);
+        }
+      }
+    }
+    __syncthreads();
+    // Compaction in ascending column: thread t owns columns [t c, (t+1) c).
+    const uint32_t per = (i + blockDim.x - 1) / blockDim.x;
+    const uint32_t j0 = min(i, threadIdx.x * per), j1 = min(i, j0 + per);
+    uint32_t mine = 0;
+    for (uint32_t j = j0; j < j1; ++j) mine += cnt[j] != 0u;
+    s_part[threadIdx.x] = mine;
+    __syncthreads();
+    // Exclusive prefix over the 256 thread counts (serial in thread 0's
+    // order is enough: 256 adds).
+    if (threadIdx.x == 0) {
+      uint32_t run = 0;
+      for (uint32_t t = 0; t < blockDim.x; ++t) {
+        const uint32_t v = s_part[t];
+        s_part[t] = run;
+        run += v;
+      }
+      r.row_nblk[i] = run;
+    }
+    __syncthreads();
+    uint2* out = r.tri + (size_t)i * (i - (i > 0 ? 1u : 0u)) / 2;  // row i holds <= i entries
+    uint32_t k = s_part[threadIdx.x];
+    for (uint32_t j = j0; j < j1; ++j)
+      if (cnt[j] != 0u) out[k++] = make_uint2(j, cnt[j]);
+    __syncthreads();
+  }
+}
+
+// Exclusive prefix of the rows' block counts (one block): row_blk[i], and
+// row_blk[nvar] the total.
+__global__ void __launch_bounds__(1024) k_rows_scan(RowsDev r) {
+  __shared__ uint32_t s_part[1024];
+  const uint32_t per = (r.nvar + blockDim.x - 1) / blockDim.x;
+  const uint32_t i0 = min(r.nvar, threadIdx.x * per), i1 = min(r.nvar, i0 + per);
+  uint32_t sum = 0;
+  for (uint32_t i = i0; i < i1; ++i) sum += r.row_nblk[i];
+  s_part[threadIdx.x] = sum;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t run = 0;
+    for (uint32_t t = 0; t < blockDim.x; ++t) {
+      const uint32_t v = s_part[t];
+      s_part[t] = run;
+      run += v;
+    }
+    r.row_blk[r.nvar] = run;
+  }
+  __syncthreads();
+  uint32_t run = s_part[threadIdx.x];
+  for (uint32_t i = i0; i < i1; ++i) {
+    r.row_blk[i] = run;
+    run += r.row_nblk[i];
+  }
+}
+
+__global__ void __launch_bounds__(256) k_rows_pack(RowsDev r) {
+  for (uint32_t i = blockIdx.x; i < r.nvar; i += gridDim.x) {
+    const uint2* src = r.tri + (size_t)i * (i - (i > 0 ? 1u : 0u)) / 2;
+    const uint32_t base = r.row_blk[i], n = r.row_nblk[i];
+    for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) {
+      const uint2 v = src[k];
+      r.col[base + k] = v.x;
+      r.count[base + k] = v.y;
+    }
+  }
+}
+
+// One warp per row; shared memory per warp: the column cursors, the ends of
+// their blocks and the lane masks of the current group.
+__global__ void __launch_bounds__(32) k_rows_place(RowsDev r, const uint32_t* blk_off,
+                                                   const uint32_t* row_blk, const uint32_t* blk_col,
+                                                   uint2* pairs) {
+  extern __shared__ uint32_t sm[];
+  uint32_t* cursor = sm;              // [nvar]
+  uint32_t* end = sm + r.nvar;        // [nvar]
+  uint32_t* mask = sm + 2 * r.nvar;   // [nvar]
+  const uint32_t lane = threadIdx.x;
+  const uint32_t lt = (1u << lane) - 1u;
+  for (uint32_t i = blockIdx.x; i < r.nvar; i += gridDim.x) {
+    for (uint32_t j = lane; j < r.nvar; j += 32) {
+      cursor[j] = kNone;
+      end[j] = 0u;
+      mask[j] = 0u;
+    }
+    __syncwarp();
+    for (uint32_t b = row_blk[i] + lane; b < row_blk[i + 1]; b += 32) {
+      cursor[blk_col[b]] = blk_off[b];
+      end[blk_col[b]] = blk_off[b + 1];
+    }
+    __syncwarp();
+    bool bad = false;
+    const uint32_t q0 = r.cam_off[i], q1 = r.cam_off[i + 1];
+    for (uint32_t g = q0; g < q1; g += 32) {
+      const uint32_t q = g + lane;
+      uint32_t a = kNone, b0 = 0, b1 = 0;
+      if (q < q1) {
+        a = r.cam_obs[q];
+        const uint32_t p = r.obs_point[a];
+        if (r.point_var[p]) {
+          b0 = r.pt_off[p];
+          b1 = r.pt_off[p + 1];
+        }
+      }
+      // Mark: this lane has a term in each column of its point's other slots.
+      for (uint32_t b = b0; b < b1; ++b) {
+        const uint32_t sb = r.obs_slot[b];
+        if (b != a && sb != kNone && sb < i) atomicOr(&mask[sb], 1u << lane);
+      }
+      __syncwarp();
+      // Place: the lanes of a column in lane order from its cursor.
+      for (uint32_t b = b0; b < b1; ++b) {
+        const uint32_t sb = r.obs_slot[b];
+        if (b == a || sb == kNone || sb >= i) continue;
+        const uint32_t c = cursor[sb];
+        const uint32_t at = c + __popc(mask[sb] & lt);
+        if (c == kNone || at >= end[sb]) {
+          bad = true;
+        } else {
+          pairs[at] = make_uint2(a, b);
+        }
+      }
+      __syncwarp();
+      // Advance each column's cursor by its lanes (the lowest one writes).
+      for (uint32_t b = b0; b < b1; ++b) {
+        const uint32_t sb = r.obs_slot[b];
+        if (b == a || sb == kNone || sb >= i) continue;
+        const uint32_t m = mask[sb];
+        if ((uint32_t)(__ffs(m) - 1) == lane && cursor[sb] != kNone) cursor[sb] += __popc(m);
+      }
+      __syncwarp();
+      for (uint32_t b = b0; b < b1; ++b) {
+        const uint32_t sb = r.obs_slot[b];
+        if (b != a && sb != kNone && sb < i) mask[sb] = 0u;
+      }
+      __syncwarp();
+    }
+    // Every block of the row filled exactly.
+    for (uint32_t b = row_blk[i] + lane; b < row_blk[i + 1]; b += 32)
+      if (cursor[blk_col[b]] != blk_off[b + 1]) bad = true;
+    if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(r.flags, 2u);
+    __syncwarp();
+  }
+}
+
+}  // namespace
+
+size_t rows_count_smem(uint32_t nvar) { return (size_t)nvar * 4; }
+size_t rows_place_smem(uint32_t nvar) { return (size_t)nvar * 12; }
+
+cudaError_t launch_rows_count(const RowsDev& r, cudaStream_t s) {
+  const size_t sm = rows_count_smem(r.nvar);
+  cudaError_t e = cudaFuncSetAttribute(k_rows_count, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)sm);
+  if (e != cudaSuccess) return e;
+  const int g = (int)(r.nvar < 148u * 8u ? r.nvar : 148u * 8u);
+  k_rows_count<<<g, 256, sm, s>>>(r);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_rows_scan<<<1, 1024, 0, s>>>(r);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_rows_pack<<<g, 256, 0, s>>>(r);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rows_place(const RowsDev& r, const uint32_t* blk_off, const uint32_t* row_blk,
+                              const uint32_t* blk_col, uint2* pairs, cudaStream_t s) {
+  const size_t sm = rows_place_smem(r.nvar);
+  cudaError_t e = cudaFuncSetAttribute(k_rows_place, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)sm);
+  if (e != cudaSuccess) return e;
+  const int g = (int)(r.nvar < 148u * 64u ? r.nvar : 148u * 64u);
+  k_rows_place<<<g, 32, sm, s>>>(r, blk_off, row_blk, blk_col, pairs);
+  return cudaGetLastError();
+}
+
+}  // namespace vlba

@@ -297,7 +297,8 @@ void counting_sort(uint32_t n, uint32_t m, uint32_t T, Key key, uint32_t value_b
 }
 
 void build_plan_serial(const vlba_problem* const* problems, const vlba_config* const* configs,
-                       uint32_t n, uint32_t tb, Plan* plan, uint32_t max_threads) {
+                       uint32_t n, uint32_t tb, Plan* plan, uint32_t max_threads,
+                       const RowBlocksFn* device_rows) {
   Plan& P = *plan;
   {
     // A plan rebuilt in place keeps the memory of its largest arrays (their
@@ -461,152 +462,191 @@ void build_plan_serial(const vlba_problem* const* problems, const vlba_config* c
     }, obs_base, P.cam_obs.data() + list_base, c2.data());
     P.cam_obs.resize(list_base + (size_t)c2[nslots]);
     for (uint32_t s = 0; s < nslots; ++s) P.cam_off.push_back(list_base + c2[s + 1]);
-    // Camera pairs sharing a variable point: blocks (i, j), j < i (local
-    // slots), each holding its terms (x, y) -- x the observation in slot i,
-    // y the one in slot j -- in point order and, within a point, in the order
-    // of the loop "for a, for b < a" over the point's observations.  Points
-    // with enough work are split into T contiguous ranges, one per thread,
-    // in three passes that keep that order whatever T is: (A) count each
-    // row's terms per range; (B) scatter them row-major, ranges in order,
-    // with each term's column beside it; (C) per row, a stable counting sort
-    // by column.  A point's observations in one slot give that slot's
-    // same-camera terms, both orders.
-    uint32_t T = 1;
-    std::vector<uint32_t> range{0, nl};
-    if (max_threads > 1) {
-      std::vector<double> work(nl + 1, 0.0);
-      for (uint32_t j = 0; j < nl; ++j) {
-        const double t = (double)(cnt[j + 1] - cnt[j]);
-        work[j + 1] = work[j] + t * t;
-      }
-      if (work[nl] > 2e6)
-        T = std::max(1u, std::min<uint32_t>({max_threads, nvar, (uint32_t)(work[nl] / 2e5)}));
-      range.assign(T + 1, nl);
-      range[0] = 0;
-      for (uint32_t t = 1, j = 0; t < T; ++t) {
-        const double goal = work[nl] * t / T;
-        while (j < nl && work[j + 1] < goal) ++j;
-        range[t] = j;
-      }
-    }
-    // f(la, lb, a, b) for every pair a > b of variable-slot observations of a
-    // variable point in range t (local slots, local observation indices).
-    // The arrays are read through local pointers (the compiler cannot keep a
-    // vector's data pointer in a register across the callers' stores).
-    const uint8_t* const pvar = P.point_var.data() + point_base;
-    const uint32_t* const oslot = P.obs_slot.data() + obs_base;
-    const uint32_t* const pcnt = cnt.data();
-    auto each_pair = [&](uint32_t t, auto&& f, uint64_t* var) {
-      uint64_t nv = 0;
-      for (uint32_t j = range[t], je = range[t + 1]; j < je; ++j) {
-        if (!pvar[j]) continue;
-        const uint32_t k0 = pcnt[j], k1 = pcnt[j + 1];
-        for (uint32_t a = k0; a < k1; ++a) {
-          const uint32_t sa = oslot[a];
-          if (sa == kNone) continue;
-          ++nv;
-          for (uint32_t b = k0; b < a; ++b) {
-            const uint32_t sb = oslot[b];
-            if (sb != kNone) f(sa - slot_base, sb - slot_base, a, b);
-          }
-        }
-      }
-      if (var) *var += nv;
-    };
-    // (A) per range: terms of each row, same-camera terms of each slot.
-    std::vector<std::vector<uint64_t>> tcnt(T, std::vector<uint64_t>(2 * (size_t)nvar, 0));
-    std::vector<uint64_t> tvar(T, 0);
-    run_threads(T, [&](uint32_t t) {
-      uint64_t* c = tcnt[t].data();
-      each_pair(t, [c, nvar](uint32_t la, uint32_t lb, uint32_t, uint32_t) {
-        if (la != lb) ++c[std::max(la, lb)];
-        else c[nvar + la] += 2;
-      }, &tvar[t]);
-    });
-    for (uint32_t t = 0; t < T; ++t) P.var_obs += tvar[t];
-    // Row and slot ranges; per range, its start inside each (the counts
-    // become positions).
-    const uint64_t pair_base = P.pairs.size(), dup_base = P.dup_pairs.size();
-    std::vector<uint64_t> row_at(nvar + 1, pair_base), dup_at(nslots + 1, dup_base);
-    for (uint32_t i = 0; i < nvar; ++i) {
-      uint64_t at = row_at[i], d = dup_at[i];
-      for (uint32_t t = 0; t < T; ++t) {
-        const uint64_t c = tcnt[t][i], e = tcnt[t][nvar + i];
-        tcnt[t][i] = at;
-        tcnt[t][nvar + i] = d;
-        at += c;
-        d += e;
-      }
-      row_at[i + 1] = at;
-      dup_at[i + 1] = d;
-    }
-    for (uint32_t s = nvar; s < nslots; ++s) dup_at[s + 1] = dup_at[s];
-    if (row_at[nvar] >= kNone) throw std::runtime_error("more than 2^32 Schur terms");
-    if (dup_at[nslots] >= kNone) throw std::runtime_error("more than 2^32 same-camera terms");
-    P.pairs.resize(row_at[nvar]);
-    P.dup_pairs.resize(dup_at[nslots]);
-    for (uint32_t s = 0; s < nslots; ++s) P.dup_off.push_back((uint32_t)dup_at[s + 1]);
-    // (B) scatter, each term's column beside it.
-    auto& term_col = P.scratch;
-    term_col.resize(row_at[nvar] - pair_base);
-    run_threads(T, [&](uint32_t t) {
-      uint64_t* pos = tcnt[t].data();
-      uint64_t* dpos = pos + nvar;
-      PairIdx* const pairs = P.pairs.data();
-      PairIdx* const dups = P.dup_pairs.data();
-      uint32_t* const tcol = term_col.data();
-      each_pair(t, [=](uint32_t la, uint32_t lb, uint32_t a, uint32_t b) {
-        const uint32_t ga = obs_base + a, gb = obs_base + b;
-        if (la > lb) {
-          const uint64_t w = pos[la]++;
-          tcol[w - pair_base] = lb;
-          pairs[w] = PairIdx{ga, gb};
-        } else if (lb > la) {
-          const uint64_t w = pos[lb]++;
-          tcol[w - pair_base] = la;
-          pairs[w] = PairIdx{gb, ga};
-        } else {
-          dups[dpos[la]++] = PairIdx{ga, gb};
-          dups[dpos[la]++] = PairIdx{gb, ga};
-        }
-      }, nullptr);
-    });
-    // (C) per row, a stable counting sort of its terms by column; the row's
-    // blocks are its distinct columns, ascending.
     std::vector<std::vector<uint32_t>> row_col(nvar), row_count(nvar);
-    {
-      std::atomic<uint32_t> next{0};
-      run_threads(T, [&](uint32_t) {
-        std::vector<uint32_t> mark(nvar, 0), touched;
-        std::vector<uint64_t> at(nvar, 0);
-        std::vector<PairIdx> buf;
-        const uint32_t* const tcol = term_col.data();
-        PairIdx* const pairs = P.pairs.data();
-        uint32_t* const mk = mark.data();
-        for (uint32_t i; (i = next.fetch_add(1)) < nvar;) {
-          const uint64_t lo = row_at[i], hi = row_at[i + 1];
-          touched.clear();
-          for (uint64_t k = lo; k < hi; ++k)
-            if (mk[tcol[k - pair_base]]++ == 0) touched.push_back(tcol[k - pair_base]);
-          std::sort(touched.begin(), touched.end());
-          row_col[i] = touched;
-          row_count[i].resize(touched.size());
-          uint64_t run = lo;
-          for (size_t b = 0; b < touched.size(); ++b) {
-            row_count[i][b] = mark[touched[b]];
-            at[touched[b]] = run;
-            run += mark[touched[b]];
-            mark[touched[b]] = 0;
-          }
-          if (touched.size() > 1) {
-            buf.assign(pairs + lo, pairs + hi);
-            uint64_t* const at_ = at.data();
-            for (uint64_t k = lo; k < hi; ++k) pairs[at_[tcol[k - pair_base]]++] = buf[k - lo];
+    const uint64_t pair_base = P.pairs.size();
+    std::vector<uint64_t> row_at(nvar + 1, pair_base);
+    // The block structure from the device when it can take this problem
+    // (one problem, no point seen twice by one slot): the terms are then
+    // written there, in the order of the host build below.
+    RowBlocks rb;
+    const bool device_terms = n == 1 && device_rows && *device_rows &&
+                              (*device_rows)(P, nvar, &rb) && rb.row_off.size() == nvar + 1u;
+    if (device_terms) {
+      uint64_t nv = 0;
+      for (uint32_t j = 0; j < nl; ++j) {
+        if (!P.point_var[point_base + j]) continue;
+        for (uint32_t k = cnt[j]; k < cnt[j + 1]; ++k) nv += P.obs_slot[obs_base + k] != kNone;
+      }
+      P.var_obs += nv;
+      for (uint32_t i = 0; i < nvar; ++i) {
+        uint64_t at = row_at[i];
+        for (uint32_t q = rb.row_off[i]; q < rb.row_off[i + 1]; ++q) {
+          if (rb.col[q] >= i || rb.count[q] == 0 || (q > rb.row_off[i] && rb.col[q] <= rb.col[q - 1]))
+            throw std::runtime_error("device row blocks out of order");
+          row_col[i].push_back(rb.col[q]);
+          row_count[i].push_back(rb.count[q]);
+          at += rb.count[q];
+        }
+        row_at[i + 1] = at;
+      }
+      if (row_at[nvar] >= kNone) throw std::runtime_error("more than 2^32 Schur terms");
+      for (uint32_t s = 0; s < nslots; ++s) P.dup_off.push_back((uint32_t)P.dup_pairs.size());
+      P.pairs_on_device = true;
+      P.num_pairs = row_at[nvar];
+      P.row_blk.assign(1, 0u);
+      for (uint32_t i = 0; i < nvar; ++i) {
+        for (uint32_t c : row_col[i]) P.blk_col.push_back(c);
+        P.row_blk.push_back((uint32_t)P.blk_col.size());
+      }
+      for (uint32_t s = nvar; s < nslots; ++s) P.row_blk.push_back((uint32_t)P.blk_col.size());
+    } else {
+      // Camera pairs sharing a variable point: blocks (i, j), j < i (local
+      // slots), each holding its terms (x, y) -- x the observation in slot i,
+      // y the one in slot j -- in point order and, within a point, in the order
+      // of the loop "for a, for b < a" over the point's observations.  Points
+      // with enough work are split into T contiguous ranges, one per thread,
+      // in three passes that keep that order whatever T is: (A) count each
+      // row's terms per range; (B) scatter them row-major, ranges in order,
+      // with each term's column beside it; (C) per row, a stable counting sort
+      // by column.  A point's observations in one slot give that slot's
+      // same-camera terms, both orders.
+      uint32_t T = 1;
+      std::vector<uint32_t> range{0, nl};
+      if (max_threads > 1) {
+        std::vector<double> work(nl + 1, 0.0);
+        for (uint32_t j = 0; j < nl; ++j) {
+          const double t = (double)(cnt[j + 1] - cnt[j]);
+          work[j + 1] = work[j] + t * t;
+        }
+        if (work[nl] > 2e6)
+          T = std::max(1u, std::min<uint32_t>({max_threads, nvar, (uint32_t)(work[nl] / 2e5)}));
+        range.assign(T + 1, nl);
+        range[0] = 0;
+        for (uint32_t t = 1, j = 0; t < T; ++t) {
+          const double goal = work[nl] * t / T;
+          while (j < nl && work[j + 1] < goal) ++j;
+          range[t] = j;
+        }
+      }
+      // f(la, lb, a, b) for every pair a > b of variable-slot observations of a
+      // variable point in range t (local slots, local observation indices).
+      // The arrays are read through local pointers (the compiler cannot keep a
+      // vector's data pointer in a register across the callers' stores).
+      const uint8_t* const pvar = P.point_var.data() + point_base;
+      const uint32_t* const oslot = P.obs_slot.data() + obs_base;
+      const uint32_t* const pcnt = cnt.data();
+      auto each_pair = [&](uint32_t t, auto&& f, uint64_t* var) {
+        uint64_t nv = 0;
+        for (uint32_t j = range[t], je = range[t + 1]; j < je; ++j) {
+          if (!pvar[j]) continue;
+          const uint32_t k0 = pcnt[j], k1 = pcnt[j + 1];
+          for (uint32_t a = k0; a < k1; ++a) {
+            const uint32_t sa = oslot[a];
+            if (sa == kNone) continue;
+            ++nv;
+            for (uint32_t b = k0; b < a; ++b) {
+              const uint32_t sb = oslot[b];
+              if (sb != kNone) f(sa - slot_base, sb - slot_base, a, b);
+            }
           }
         }
+        if (var) *var += nv;
+      };
+      // (A) per range: terms of each row, same-camera terms of each slot.
+      std::vector<std::vector<uint64_t>> tcnt(T, std::vector<uint64_t>(2 * (size_t)nvar, 0));
+      std::vector<uint64_t> tvar(T, 0);
+      run_threads(T, [&](uint32_t t) {
+        uint64_t* c = tcnt[t].data();
+        each_pair(t, [c, nvar](uint32_t la, uint32_t lb, uint32_t, uint32_t) {
+          if (la != lb) ++c[std::max(la, lb)];
+          else c[nvar + la] += 2;
+        }, &tvar[t]);
       });
+      for (uint32_t t = 0; t < T; ++t) P.var_obs += tvar[t];
+      // Row and slot ranges; per range, its start inside each (the counts
+      // become positions).
+      const uint64_t dup_base = P.dup_pairs.size();
+      std::vector<uint64_t> dup_at(nslots + 1, dup_base);
+      for (uint32_t i = 0; i < nvar; ++i) {
+        uint64_t at = row_at[i], d = dup_at[i];
+        for (uint32_t t = 0; t < T; ++t) {
+          const uint64_t c = tcnt[t][i], e = tcnt[t][nvar + i];
+          tcnt[t][i] = at;
+          tcnt[t][nvar + i] = d;
+          at += c;
+          d += e;
+        }
+        row_at[i + 1] = at;
+        dup_at[i + 1] = d;
+      }
+      for (uint32_t s = nvar; s < nslots; ++s) dup_at[s + 1] = dup_at[s];
+      if (row_at[nvar] >= kNone) throw std::runtime_error("more than 2^32 Schur terms");
+      if (dup_at[nslots] >= kNone) throw std::runtime_error("more than 2^32 same-camera terms");
+      P.pairs.resize(row_at[nvar]);
+      P.dup_pairs.resize(dup_at[nslots]);
+      for (uint32_t s = 0; s < nslots; ++s) P.dup_off.push_back((uint32_t)dup_at[s + 1]);
+      // (B) scatter, each term's column beside it.
+      auto& term_col = P.scratch;
+      term_col.resize(row_at[nvar] - pair_base);
+      run_threads(T, [&](uint32_t t) {
+        uint64_t* pos = tcnt[t].data();
+        uint64_t* dpos = pos + nvar;
+        PairIdx* const pairs = P.pairs.data();
+        PairIdx* const dups = P.dup_pairs.data();
+        uint32_t* const tcol = term_col.data();
+        each_pair(t, [=](uint32_t la, uint32_t lb, uint32_t a, uint32_t b) {
+          const uint32_t ga = obs_base + a, gb = obs_base + b;
+          if (la > lb) {
+            const uint64_t w = pos[la]++;
+            tcol[w - pair_base] = lb;
+            pairs[w] = PairIdx{ga, gb};
+          } else if (lb > la) {
+            const uint64_t w = pos[lb]++;
+            tcol[w - pair_base] = la;
+            pairs[w] = PairIdx{gb, ga};
+          } else {
+            dups[dpos[la]++] = PairIdx{ga, gb};
+            dups[dpos[la]++] = PairIdx{gb, ga};
+          }
+        }, nullptr);
+      });
+      // (C) per row, a stable counting sort of its terms by column; the row's
+      // blocks are its distinct columns, ascending.
+      {
+        std::atomic<uint32_t> next{0};
+        run_threads(T, [&](uint32_t) {
+          std::vector<uint32_t> mark(nvar, 0), touched;
+          std::vector<uint64_t> at(nvar, 0);
+          std::vector<PairIdx> buf;
+          const uint32_t* const tcol = term_col.data();
+          PairIdx* const pairs = P.pairs.data();
+          uint32_t* const mk = mark.data();
+          for (uint32_t i; (i = next.fetch_add(1)) < nvar;) {
+            const uint64_t lo = row_at[i], hi = row_at[i + 1];
+            touched.clear();
+            for (uint64_t k = lo; k < hi; ++k)
+              if (mk[tcol[k - pair_base]]++ == 0) touched.push_back(tcol[k - pair_base]);
+            std::sort(touched.begin(), touched.end());
+            row_col[i] = touched;
+            row_count[i].resize(touched.size());
+            uint64_t run = lo;
+            for (size_t b = 0; b < touched.size(); ++b) {
+              row_count[i][b] = mark[touched[b]];
+              at[touched[b]] = run;
+              run += mark[touched[b]];
+              mark[touched[b]] = 0;
+            }
+            if (touched.size() > 1) {
+              buf.assign(pairs + lo, pairs + hi);
+              uint64_t* const at_ = at.data();
+              for (uint64_t k = lo; k < hi; ++k) pairs[at_[tcol[k - pair_base]]++] = buf[k - lo];
+            }
+          }
+        });
+      }
+      term_col.clear();
     }
-    term_col.clear();
+
     // Blocks in row-major order; per-tile existence.
     const uint32_t ntr = nslots / tb;
     std::vector<uint8_t> tile_has((size_t)ntr * ntr, 0);
@@ -683,7 +723,7 @@ void build_plan_serial(const vlba_problem* const* problems, const vlba_config* c
   // Partial slots: position of (tile, side) in the tile-row lists, so a row's
   // partials are contiguous.
   finish_tiles(P);
-  P.num_pairs = P.pairs.size();
+  if (!P.pairs_on_device) P.num_pairs = P.pairs.size();
   // Lanes per block in the off-diagonal assembly.  The lane count sets the
   // order of each block's sum, so it is the same for every problem and batch
   // (a result must not depend on what it is batched with).
@@ -996,10 +1036,11 @@ void merge_plans(const std::vector<const Plan*>& parts, Plan* out) {
 }
 
 void build_plan(const vlba_problem* const* problems, const vlba_config* const* configs,
-                uint32_t n, uint32_t tb, Plan* plan, uint32_t max_threads) {
+                uint32_t n, uint32_t tb, Plan* plan, uint32_t max_threads,
+                const RowBlocksFn* device_rows) {
   if (max_threads == 0) max_threads = std::max(1u, std::thread::hardware_concurrency());
   if (n <= 1) {
-    build_plan_serial(problems, configs, n, tb, plan, max_threads);
+    build_plan_serial(problems, configs, n, tb, plan, max_threads, device_rows);
     return;
   }
   // One plan per problem on the host's threads, then one merge: the same
@@ -1011,7 +1052,7 @@ void build_plan(const vlba_problem* const* problems, const vlba_config* const* c
   auto work = [&] {
     for (uint32_t i; (i = next.fetch_add(1)) < n && !failed.load();) {
       try {
-        build_plan_serial(problems + i, configs + i, 1, tb, &parts[i], 1);
+        build_plan_serial(problems + i, configs + i, 1, tb, &parts[i], 1, nullptr);
       } catch (...) {
         if (!failed.exchange(true)) err = std::current_exception();
       }
@@ -1080,10 +1121,24 @@ std::string check_plan(const Plan& P) {
     return bad("cam_obs");
   if (P.slot_prob.size() != nslots || nslots != (uint64_t)P.num_tile_rows * P.tb)
     return bad("slots");
-  if (P.blk_off.size() != P.blk_dst.size() + 1 || P.blk_off.back() != P.pairs.size())
+  const uint64_t npairs = P.pairs_on_device ? P.num_pairs : P.pairs.size();
+  if (P.blk_off.size() != P.blk_dst.size() + 1 || P.blk_off.back() != npairs)
     return bad("blk_off");
   for (size_t b = 0; b + 1 < P.blk_off.size(); ++b)
     if (P.blk_off[b] > P.blk_off[b + 1]) return bad("blk_off order");
+  // Terms built on the device are checked there, against the same ranges,
+  // before any kernel reads them.
+  if (P.pairs_on_device) {
+    if (!P.pairs.empty() || P.num_problems != 1 || P.blk_col.size() != P.blk_dst.size() ||
+        P.row_blk.size() != (size_t)P.num_var_cams + 1 || P.row_blk.back() != P.blk_col.size())
+      return bad("device terms");
+    for (size_t i = 0; i + 1 < P.row_blk.size(); ++i) {
+      if (P.row_blk[i] > P.row_blk[i + 1]) return bad("row_blk order");
+      for (uint32_t b = P.row_blk[i]; b < P.row_blk[i + 1]; ++b)
+        if (P.blk_col[b] >= i || (b > P.row_blk[i] && P.blk_col[b] <= P.blk_col[b - 1]))
+          return bad("blk_col");
+    }
+  }
   if (!all_of_range(P.pairs.size(), [&](uint64_t q) { return P.pairs[q].a < nobs && P.pairs[q].b < nobs; }))
     return bad("pairs");
   for (const PairIdx& d : P.blk_dst) {
@@ -1132,7 +1187,7 @@ size_t Plan::device_bytes() const {
   b += npt * (8 * 3 * 2 + 4 + 1 + 4 + 36 + 64);     // points x2, off, var, prob, pt_h, pt_s
   b += nobs * (4 * 4 + 16 + 32 + 16 + 32);           // point, pose, cam, slot, xy, obs_h, obs_e, obs_p
   b += obs_w.size() * 8 + obs_kind.size() * (1 + 16 + 4);
-  b += cam_obs.size() * 4 + pairs.size() * 8 + dup_pairs.size() * 8;
+  b += cam_obs.size() * 4 + (pairs_on_device ? num_pairs : pairs.size()) * 8 + dup_pairs.size() * 8;
   b += blk_dst.size() * (8 + 4);
   b += tile_ij.size() * ((size_t)tb * tb * kBlock * 4 + 4 + 2 * (size_t)tb * 6 * 4);
   b += (size_t)num_var_cams * (4 + 4 + 4 + 4 + 36 * 4 + 6 * 4 * 6);
@@ -1150,7 +1205,8 @@ size_t Plan::upload_bytes() const {
          b(obs_cam) + b(obs_slot) + b(obs_xy) + b(obs_w) + b(obs_kind) + b(obs_st) + b(obs_rcam) +
          b(cam_off) + b(cam_obs) + b(tile_ij) +
          b(blk_off) + b(pairs) + b(blk_dst) + b(diag_dst) + b(dup_off) + b(dup_pairs) +
-         b(tr_list_off) + b(tr_list) + b(tr_prob) + b(chunk_point_begin) + b(tile_slot) + b(tile_meta);
+         b(tr_list_off) + b(tr_list) + b(tr_prob) + b(chunk_point_begin) + b(tile_slot) + b(tile_meta) +
+         b(row_blk) + b(blk_col);
 }
 
 double algorithmic_bytes(const Plan& P, double k, double* b_pcg_out) {

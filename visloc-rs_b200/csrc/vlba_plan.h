@@ -9,6 +9,7 @@
 #include <new>
 #include <string>
 #include <utility>
+#include <functional>
 #include <vector>
 
 #include "vlba_common.cuh"
@@ -116,6 +117,13 @@ struct Plan {
   uint64_t var_obs = 0;          // observations with a variable point
   uint64_t camera_pairs = 0;     // nonzero off-diagonal blocks (N_e)
   uint64_t num_pairs = 0;        // point contributions to those blocks
+  // The terms (pairs) are not on the host: the device writes num_pairs of
+  // them at upload, per block in point order as the host build would; the
+  // block structure (blk_off, blk_dst, tiles) and blk_col, each block's
+  // column slot, are the host's.
+  bool pairs_on_device = false;
+  std::vector<uint32_t> blk_col;
+  std::vector<uint32_t> row_blk;   // [num_var_cams + 1] first block of each row
 
   size_t device_bytes() const;
   size_t upload_bytes() const;  // bytes copied host -> device by an upload
@@ -136,13 +144,32 @@ Validation validate_problem(const vlba_problem* p, const vlba_config* cfg);
 
 LmParams make_params(const vlba_config* cfg);
 
+// The off-diagonal block structure of one problem's reduced system, found
+// elsewhere (on the device) from the plan's point-major observations: per
+// variable slot i, its columns j < i that share a variable point with it,
+// ascending, and the number of terms (shared points) of each.  The builder
+// then lays out everything but the terms themselves, which the device
+// writes in the same order as the host build (Plan::pairs_on_device).
+struct RowBlocks {
+  std::vector<uint32_t> row_off;  // [nvar + 1] into col / count
+  std::vector<uint32_t> col;      // per row, ascending
+  std::vector<uint32_t> count;    // terms of each (row, col) block
+};
+// Returns false when some point has two observations in one slot (same-
+// camera terms), which the host build handles, or when the device cannot
+// take the problem; the builder then builds the terms on the host.
+using RowBlocksFn = std::function<bool(const Plan& P, uint32_t nvar, RowBlocks* out)>;
+
 // Build the plan for `n` problems (all must have validated OK); with n > 1
 // each problem is built on its own host thread and the parts are merged;
 // one large problem splits its pair counting over up to `max_threads` threads
-// (0: all the host's).  `tb` is the tile size in blocks.  Throws std::runtime_error on internal
-// inconsistency.
+// (0: all the host's).  `tb` is the tile size in blocks.  With n == 1 and
+// `device_rows`, the block structure comes from device_rows and the terms are
+// left to the device (Plan::pairs_on_device) when it succeeds.  Throws
+// std::runtime_error on internal inconsistency.
 void build_plan(const vlba_problem* const* problems, const vlba_config* const* configs,
-                uint32_t n, uint32_t tb, Plan* plan, uint32_t max_threads = 0);
+                uint32_t n, uint32_t tb, Plan* plan, uint32_t max_threads = 0,
+                const RowBlocksFn* device_rows = nullptr);
 
 // The layout of a reduced camera system given directly (n nodes, sorted
 // edges (a, b), a < b): its tiles, block destinations and PCG lists, with no

@@ -234,6 +234,10 @@ struct Context {
   // The reduced system's diagonal, rhs and blocks as copied from the caller,
   // and the preconditioner of a preconditioned solve.
   DeviceArray reduced_in, reduced_pre;
+  // Scratch of the device-built Schur terms (vlba_pairs.cu): the plan arrays
+  // the row counts read, the per-row lists and the flags.
+  DeviceArray rows_in, rows_out;
+  uint64_t last_upload_bytes = 0;
 };
 
 namespace {
@@ -432,6 +436,10 @@ class Stager {
 };
 
 // Upload a built plan: allocate and fill every device array of Dev.
+void check_launch(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) throw CudaError(e, what);
+}
+
 void upload_plan_once(Context* c, uint32_t max_records) {
   Plan& P = c->plan;
   cudaStream_t s = c->stream;
@@ -507,7 +515,17 @@ void upload_plan_once(Context* c, uint32_t max_records) {
   VLBA_CUDA(cudaMemsetAsync(d.tiles, 0, P.tile_ij.size() * tile_floats * 4, s));
   d.tile_ij = st.up(A, P.tile_ij);
   d.blk_off = st.up(A, P.blk_off);
-  d.pairs = reinterpret_cast<const uint2*>(st.up(A, P.pairs));
+  uint2* dev_pairs = nullptr;
+  const uint32_t* dev_row_blk = nullptr;
+  const uint32_t* dev_blk_col = nullptr;
+  if (P.pairs_on_device) {
+    dev_pairs = A.alloc<uint2>(P.num_pairs);
+    d.pairs = dev_pairs;
+    dev_row_blk = st.up(A, P.row_blk);
+    dev_blk_col = st.up(A, P.blk_col);
+  } else {
+    d.pairs = reinterpret_cast<const uint2*>(st.up(A, P.pairs));
+  }
   d.blk_dst = reinterpret_cast<const uint2*>(st.up(A, P.blk_dst));
   d.diag_dst = st.up(A, P.diag_dst);
   d.dup_off = st.up(A, P.dup_off);
@@ -544,6 +562,27 @@ void upload_plan_once(Context* c, uint32_t max_records) {
   d.chunk_step = A.alloc<double>(nch);
   st.flush(s);
   c->dev = d;
+  if (P.pairs_on_device) {
+    // The terms, from the uploaded point-major observations and per-slot
+    // lists, at the places the host laid out; checked as they are written.
+    RowsDev r{};
+    r.nvar = P.row_blk.size() > 0 ? (uint32_t)P.row_blk.size() - 1 : 0u;
+    r.cam_off = d.cam_off;
+    r.cam_obs = d.cam_obs;
+    r.obs_point = d.obs_point;
+    r.obs_slot = d.obs_slot;
+    r.point_var = d.point_var;
+    r.pt_off = d.pt_off;
+    c->rows_out.ensure(16);
+    r.flags = c->rows_out.as<uint32_t>();
+    VLBA_CUDA(cudaMemsetAsync(r.flags, 0, 4, s));
+    check_launch(launch_rows_place(r, d.blk_off, dev_row_blk, dev_blk_col, dev_pairs, s),
+                 "Schur terms");
+    uint32_t flags = 0;
+    VLBA_CUDA(cudaMemcpyAsync(&flags, r.flags, 4, cudaMemcpyDeviceToHost, s));
+    VLBA_CUDA(cudaStreamSynchronize(s));
+    if (flags) throw std::runtime_error("device Schur terms do not match the plan's blocks");
+  }
   // Co-resident grid, but no more blocks than tiles or tile rows to work on
   // (fewer blocks make the grid barriers cheaper on small systems).
   c->pcg_grid = P.num_tile_rows ? pcg_grid_size((int)P.tb, c->sm_count) : 0;
@@ -596,9 +635,6 @@ void reset_state(Context* c) {
   VLBA_CUDA(cudaMemsetAsync(d.error, 0, 4, s));
 }
 
-void check_launch(cudaError_t e, const char* what) {
-  if (e != cudaSuccess) throw CudaError(e, what);
-}
 
 struct RunStats {
   double device_ms = 0.0;
@@ -1009,6 +1045,71 @@ std::vector<Validation> validate_all(const vlba_problem* const* probs,
   return v;
 }
 
+// Problems of at least this many observations have their Schur terms built
+// on the device (below it the host build is quick and avoids the round trip).
+constexpr uint64_t kDeviceTermsMinObs = 200000;
+// Rows the device builders take (their shared memory holds 12 bytes per row).
+constexpr uint32_t kDeviceTermsMaxRows = 16384;
+
+// The block structure of the plan's single problem from the device: uploads
+// what the row counts read (point-major order, per-slot lists), counts and
+// packs each row's columns, and returns them; false (the host builds the
+// terms) for a point seen twice by one slot or a system the device builders
+// do not take.
+bool device_row_blocks(Context* c, const Plan& P, uint32_t nvar, RowBlocks* out) {
+  if (nvar < 2 || nvar > kDeviceTermsMaxRows) return false;
+  cudaStream_t s = c->stream;
+  const size_t ntri = (size_t)nvar * (nvar - 1) / 2;
+  auto up16 = [](size_t b) { return (b + 15) & ~size_t(15); };
+  const size_t b_coff = up16(4 * P.cam_off.size()), b_cobs = up16(4 * P.cam_obs.size()),
+               b_opt = up16(4 * P.obs_point.size()), b_oslot = up16(4 * P.obs_slot.size()),
+               b_pvar = up16(P.point_var.size()), b_poff = up16(4 * P.pt_off.size());
+  c->rows_in.ensure(b_coff + b_cobs + b_opt + b_oslot + b_pvar + b_poff);
+  char* in = c->rows_in.as<char>();
+  const size_t b_tri = up16(8 * ntri), b_nblk = up16(4 * (size_t)nvar),
+               b_rblk = up16(4 * ((size_t)nvar + 1)), b_list = up16(4 * ntri);
+  c->rows_out.ensure(16 + b_tri + b_nblk + b_rblk + 2 * b_list);
+  char* o = c->rows_out.as<char>();
+  RowsDev r{};
+  r.nvar = nvar;
+  size_t at = 0;
+  auto put = [&](const void* src, size_t bytes, size_t room) {
+    char* dst = in + at;
+    if (bytes) VLBA_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
+    at += room;
+    return dst;
+  };
+  r.cam_off = reinterpret_cast<const uint32_t*>(put(P.cam_off.data(), 4 * P.cam_off.size(), b_coff));
+  r.cam_obs = reinterpret_cast<const uint32_t*>(put(P.cam_obs.data(), 4 * P.cam_obs.size(), b_cobs));
+  r.obs_point = reinterpret_cast<const uint32_t*>(put(P.obs_point.data(), 4 * P.obs_point.size(), b_opt));
+  r.obs_slot = reinterpret_cast<const uint32_t*>(put(P.obs_slot.data(), 4 * P.obs_slot.size(), b_oslot));
+  r.point_var = reinterpret_cast<const uint8_t*>(put(P.point_var.data(), P.point_var.size(), b_pvar));
+  r.pt_off = reinterpret_cast<const uint32_t*>(put(P.pt_off.data(), 4 * P.pt_off.size(), b_poff));
+  r.flags = reinterpret_cast<uint32_t*>(o);
+  r.tri = reinterpret_cast<uint2*>(o + 16);
+  r.row_nblk = reinterpret_cast<uint32_t*>(o + 16 + b_tri);
+  r.row_blk = reinterpret_cast<uint32_t*>(o + 16 + b_tri + b_nblk);
+  r.col = reinterpret_cast<uint32_t*>(o + 16 + b_tri + b_nblk + b_rblk);
+  r.count = reinterpret_cast<uint32_t*>(o + 16 + b_tri + b_nblk + b_rblk + b_list);
+  VLBA_CUDA(cudaMemsetAsync(r.flags, 0, 4, s));
+  check_launch(launch_rows_count(r, s), "Schur term counts");
+  uint32_t flags = 0;
+  out->row_off.resize((size_t)nvar + 1);
+  VLBA_CUDA(cudaMemcpyAsync(&flags, r.flags, 4, cudaMemcpyDeviceToHost, s));
+  VLBA_CUDA(cudaMemcpyAsync(out->row_off.data(), r.row_blk, 4 * ((size_t)nvar + 1),
+                            cudaMemcpyDeviceToHost, s));
+  VLBA_CUDA(cudaStreamSynchronize(s));
+  if (flags & 1u) return false;
+  const size_t nb = out->row_off[nvar];
+  if (nb > ntri) throw std::runtime_error("device Schur term counts out of range");
+  out->col.resize(nb);
+  out->count.resize(nb);
+  VLBA_CUDA(cudaMemcpyAsync(out->col.data(), r.col, 4 * nb, cudaMemcpyDeviceToHost, s));
+  VLBA_CUDA(cudaMemcpyAsync(out->count.data(), r.count, 4 * nb, cudaMemcpyDeviceToHost, s));
+  VLBA_CUDA(cudaStreamSynchronize(s));
+  return true;
+}
+
 void do_upload(Context* c, const vlba_problem* const* probs, const vlba_config* const* cfgs,
                uint32_t n, uint32_t max_records, double* upload_ms) {
   const auto t0 = std::chrono::steady_clock::now();
@@ -1020,7 +1121,14 @@ void do_upload(Context* c, const vlba_problem* const* probs, const vlba_config* 
                    vs[i].error_index);
   set_device(c);
   c->reduced_generation = ~0ull;  // the host plan no longer matches the reduced layout
-  build_plan(probs, cfgs, n, (uint32_t)pick_tb(probs, n), &c->plan);
+  // One large problem: its Schur terms (the plan's largest part) are found
+  // and written on the device; the host lays out the rest.
+  const RowBlocksFn device_rows = [c](const Plan& P, uint32_t nvar, RowBlocks* out) {
+    return device_row_blocks(c, P, nvar, out);
+  };
+  const bool large = n == 1 && probs[0]->num_observations >= kDeviceTermsMinObs;
+  build_plan(probs, cfgs, n, (uint32_t)pick_tb(probs, n), &c->plan, 0,
+             large ? &device_rows : nullptr);
   const std::string bad = check_plan(c->plan);
   if (!bad.empty()) throw Status(VLBA_ERR_INVALID_ARGUMENT, bad);
   upload_plan(c, max_records);
@@ -1032,6 +1140,14 @@ void do_upload(Context* c, const vlba_problem* const* probs, const vlba_config* 
   }
   const auto t1 = std::chrono::steady_clock::now();
   if (upload_ms) *upload_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+  // Host -> device bytes of this upload: the plan's arrays, and with terms
+  // built on the device the arrays its row counts read (sent once more).
+  const Plan& P = c->plan;
+  c->last_upload_bytes = P.upload_bytes();
+  if (P.pairs_on_device)
+    c->last_upload_bytes += 4 * (P.cam_off.size() + P.cam_obs.size() + P.obs_point.size() +
+                                 P.obs_slot.size() + P.pt_off.size()) +
+                            P.point_var.size();
 }
 
 // Write the current state of every uploaded problem back into `problems`
@@ -1261,7 +1377,10 @@ int visloc_ba_cuda_optimize(void* ctx, vlba_problem* problem, const vlba_config*
   }
   st = visloc_ba_cuda_solve_uploaded(ctx, nullptr, result, iterations, iterations_capacity);
   if (st != VLBA_OK) return st;
-  if (result) result->upload_ms = upload_ms;
+  if (result) {
+    result->upload_ms = upload_ms;
+    result->upload_bytes = c->last_upload_bytes;
+  }
   return visloc_ba_cuda_download(ctx, problem);
 }
 

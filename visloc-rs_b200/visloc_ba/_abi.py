@@ -169,6 +169,7 @@ class Result(C.Structure):
         ("device_ms", C.c_double),
         ("upload_ms", C.c_double),
         ("kernel_launches", C.c_uint64),
+        ("upload_bytes", C.c_uint64),
     ]
 
 

@@ -379,6 +379,7 @@ class BaResult:
     device_ms: float = 0.0
     upload_ms: float = 0.0
     kernel_launches: int = 0
+    upload_bytes: int = 0
 
 
 class BaError(Exception):
@@ -434,6 +435,7 @@ def result_from_abi(res: _abi.Result, iters, count: int) -> BaResult:
         res.device_ms,
         res.upload_ms,
         int(res.kernel_launches),
+        int(res.upload_bytes),
     )
 
 
