@@ -472,12 +472,17 @@ void build_plan_serial(const vlba_problem* const* problems, const vlba_config* c
     const bool device_terms = n == 1 && device_rows && *device_rows &&
                               (*device_rows)(P, nvar, &rb) && rb.row_off.size() == nvar + 1u;
     if (device_terms) {
-      uint64_t nv = 0;
-      for (uint32_t j = 0; j < nl; ++j) {
-        if (!P.point_var[point_base + j]) continue;
-        for (uint32_t k = cnt[j]; k < cnt[j + 1]; ++k) nv += P.obs_slot[obs_base + k] != kNone;
-      }
-      P.var_obs += nv;
+      std::vector<uint64_t> part(To, 0);
+      run_threads(To, [&](uint32_t t) {
+        uint64_t nv = 0;
+        const uint32_t j0 = (uint32_t)((uint64_t)nl * t / To), j1 = (uint32_t)((uint64_t)nl * (t + 1) / To);
+        for (uint32_t j = j0; j < j1; ++j) {
+          if (!P.point_var[point_base + j]) continue;
+          for (uint32_t k = cnt[j]; k < cnt[j + 1]; ++k) nv += P.obs_slot[obs_base + k] != kNone;
+        }
+        part[t] = nv;
+      });
+      for (uint32_t t = 0; t < To; ++t) P.var_obs += part[t];
       for (uint32_t i = 0; i < nvar; ++i) {
         uint64_t at = row_at[i];
         for (uint32_t q = rb.row_off[i]; q < rb.row_off[i + 1]; ++q) {

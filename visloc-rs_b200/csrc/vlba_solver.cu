@@ -237,6 +237,11 @@ struct Context {
   // Scratch of the device-built Schur terms (vlba_pairs.cu): the plan arrays
   // the row counts read, the per-row lists and the flags.
   DeviceArray rows_in, rows_out;
+  // Where rows_in holds the plan arrays the row counts read (byte offsets of
+  // cam_off, cam_obs, obs_point, obs_slot, point_var, pt_off), valid for the
+  // plan built last with its terms on the device: its upload copies them from
+  // there instead of from the host again.
+  size_t rows_in_at[6] = {0, 0, 0, 0, 0, 0};
   uint64_t last_upload_bytes = 0;
 };
 
@@ -484,15 +489,26 @@ void upload_plan_once(Context* c, uint32_t max_records) {
   d.init_pose_q = st.up(A, P.pose_q);
   d.init_pose_t = st.up(A, P.pose_t);
   d.init_points = st.up(A, P.points);
+  // With the terms built on the device, the arrays its row counts read are
+  // on the device already: copied from there, not sent again.
+  auto from_rows = [&](const auto& v, int k) {
+    using T = typename std::decay_t<decltype(v)>::value_type;
+    T* p = A.alloc<T>(v.size());
+    if (!v.empty())
+      VLBA_CUDA(cudaMemcpyAsync(p, c->rows_in.as<char>() + c->rows_in_at[k], v.size() * sizeof(T),
+                                cudaMemcpyDeviceToDevice, s));
+    return p;
+  };
+  const bool reuse = P.pairs_on_device;
   d.pose_slot = st.up(A, P.pose_slot);
-  d.point_var = st.up(A, P.point_var);
+  d.point_var = reuse ? from_rows(P.point_var, 4) : st.up(A, P.point_var);
   d.pose_step = A.alloc<double>(npose);
   d.cameras = st.up(A, P.cameras);
-  d.pt_off = st.up(A, P.pt_off);
-  d.obs_point = st.up(A, P.obs_point);
+  d.pt_off = reuse ? from_rows(P.pt_off, 5) : st.up(A, P.pt_off);
+  d.obs_point = reuse ? from_rows(P.obs_point, 2) : st.up(A, P.obs_point);
   d.obs_pose = st.up(A, P.obs_pose);
   d.obs_cam = st.up(A, P.obs_cam);
-  d.obs_slot = st.up(A, P.obs_slot);
+  d.obs_slot = reuse ? from_rows(P.obs_slot, 3) : st.up(A, P.obs_slot);
   {
     double2* xy = A.alloc<double2>(nobs);
     st.add(xy, P.obs_xy.data(), nobs * 16);
@@ -505,8 +521,8 @@ void upload_plan_once(Context* c, uint32_t max_records) {
   d.obs_h = A.alloc<float4>(2 * nobs);
   d.obs_e = A.alloc<float4>(nobs);
   d.obs_p = A.alloc<float4>(2 * nobs);
-  d.cam_off = st.up(A, P.cam_off);
-  d.cam_obs = st.up(A, P.cam_obs);
+  d.cam_off = reuse ? from_rows(P.cam_off, 0) : st.up(A, P.cam_off);
+  d.cam_obs = reuse ? from_rows(P.cam_obs, 1) : st.up(A, P.cam_obs);
   d.pt_h = A.alloc<float>(9 * npt);
   d.pt_s = A.alloc<float4>(4 * npt);
   d.cam_hpp = nullptr;
@@ -1073,9 +1089,12 @@ bool device_row_blocks(Context* c, const Plan& P, uint32_t nvar, RowBlocks* out)
   RowsDev r{};
   r.nvar = nvar;
   size_t at = 0;
+  int slot = 0;
+  Stager st(c);  // through the pinned staging buffers
   auto put = [&](const void* src, size_t bytes, size_t room) {
     char* dst = in + at;
-    if (bytes) VLBA_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
+    c->rows_in_at[slot++] = at;
+    st.add(dst, src, bytes);
     at += room;
     return dst;
   };
@@ -1085,6 +1104,7 @@ bool device_row_blocks(Context* c, const Plan& P, uint32_t nvar, RowBlocks* out)
   r.obs_slot = reinterpret_cast<const uint32_t*>(put(P.obs_slot.data(), 4 * P.obs_slot.size(), b_oslot));
   r.point_var = reinterpret_cast<const uint8_t*>(put(P.point_var.data(), P.point_var.size(), b_pvar));
   r.pt_off = reinterpret_cast<const uint32_t*>(put(P.pt_off.data(), 4 * P.pt_off.size(), b_poff));
+  st.flush(s);
   r.flags = reinterpret_cast<uint32_t*>(o);
   r.tri = reinterpret_cast<uint2*>(o + 16);
   r.row_nblk = reinterpret_cast<uint32_t*>(o + 16 + b_tri);
@@ -1113,25 +1133,47 @@ bool device_row_blocks(Context* c, const Plan& P, uint32_t nvar, RowBlocks* out)
 void do_upload(Context* c, const vlba_problem* const* probs, const vlba_config* const* cfgs,
                uint32_t n, uint32_t max_records, double* upload_ms) {
   const auto t0 = std::chrono::steady_clock::now();
+  // VLBA_TRACE_UPLOAD: host time of the upload's phases, to stderr (the
+  // analogue of the reference's VISLOC_BA_TRACE_PHASE_TIMING, lm.rs:345).
+  const bool trace = std::getenv("VLBA_TRACE_UPLOAD") != nullptr;
+  auto ms_since = [](std::chrono::steady_clock::time_point a) {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - a).count();
+  };
   c->batch_slot.clear();
   const std::vector<Validation> vs = validate_all(probs, cfgs, n);
   for (uint32_t i = 0; i < n; ++i)
     if (vs[i].status != VLBA_OK)
       throw Status(vs[i].status, "problem " + std::to_string(i) + " failed validation",
                    vs[i].error_index);
+  const double t_validate = ms_since(t0);
   set_device(c);
   c->reduced_generation = ~0ull;  // the host plan no longer matches the reduced layout
   // One large problem: its Schur terms (the plan's largest part) are found
   // and written on the device; the host lays out the rest.
-  const RowBlocksFn device_rows = [c](const Plan& P, uint32_t nvar, RowBlocks* out) {
-    return device_row_blocks(c, P, nvar, out);
+  double t_rows = 0.0;
+  const RowBlocksFn device_rows = [c, &t_rows, &ms_since](const Plan& P, uint32_t nvar,
+                                                          RowBlocks* out) {
+    const auto r0 = std::chrono::steady_clock::now();
+    const bool ok = device_row_blocks(c, P, nvar, out);
+    t_rows = ms_since(r0);
+    return ok;
   };
   const bool large = n == 1 && probs[0]->num_observations >= kDeviceTermsMinObs;
+  const auto tb0 = std::chrono::steady_clock::now();
   build_plan(probs, cfgs, n, (uint32_t)pick_tb(probs, n), &c->plan, 0,
              large ? &device_rows : nullptr);
+  const double t_build = ms_since(tb0);
+  const auto tc0 = std::chrono::steady_clock::now();
   const std::string bad = check_plan(c->plan);
   if (!bad.empty()) throw Status(VLBA_ERR_INVALID_ARGUMENT, bad);
+  const double t_check = ms_since(tc0);
+  const auto tu0 = std::chrono::steady_clock::now();
   upload_plan(c, max_records);
+  if (trace)
+    std::fprintf(stderr,
+                 "vlba upload: validate %.2f ms, plan %.2f ms (device row counts %.2f ms), "
+                 "check %.2f ms, copy and device terms %.2f ms\n",
+                 t_validate, t_build, t_rows, t_check, ms_since(tu0));
   c->num_poses.clear();
   c->num_points.clear();
   for (uint32_t i = 0; i < n; ++i) {
@@ -1140,14 +1182,11 @@ void do_upload(Context* c, const vlba_problem* const* probs, const vlba_config* 
   }
   const auto t1 = std::chrono::steady_clock::now();
   if (upload_ms) *upload_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
-  // Host -> device bytes of this upload: the plan's arrays, and with terms
-  // built on the device the arrays its row counts read (sent once more).
+  // Host -> device bytes of this upload: the plan's arrays.
   const Plan& P = c->plan;
+  // (With terms built on the device, the arrays its row counts read went
+  // over once, before the plan's other arrays, and count among them.)
   c->last_upload_bytes = P.upload_bytes();
-  if (P.pairs_on_device)
-    c->last_upload_bytes += 4 * (P.cam_off.size() + P.cam_obs.size() + P.obs_point.size() +
-                                 P.obs_slot.size() + P.pt_off.size()) +
-                            P.point_var.size();
 }
 
 // Write the current state of every uploaded problem back into `problems`
