@@ -732,7 +732,7 @@ void build_plan_serial(const vlba_problem* const* problems, const vlba_config* c
   // Lanes per block in the off-diagonal assembly.  The lane count sets the
   // order of each block's sum, so it is the same for every problem and batch
   // (a result must not depend on what it is batched with).
-  P.group = 8;
+  P.group = 4;
 }
 
 // Partial slots (positions of each tile's row and column side in the
@@ -762,7 +762,7 @@ void build_reduced_plan(uint32_t n, const uint32_t* edges, uint64_t ne, uint32_t
   if (n == 0) throw std::runtime_error("a reduced system of no nodes");
   if (ne >= kNone) throw std::runtime_error("more than 2^32 edges");
   P.tb = tb;
-  P.group = 8;
+  P.group = 4;
   P.num_problems = 1;
   const uint32_t nslots = round_up(n, tb), ntr = nslots / tb;
   P.prob_pose_begin = {0, 0};
