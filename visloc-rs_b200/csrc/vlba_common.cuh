@@ -179,6 +179,8 @@ struct Dev {
   // per point, per linearisation / per trial
   float* pt_h;                 // [9 M] H_ll upper (6) + g_l (3)
   float4* pt_s;                // [4 M] {hinv00,01,02,11} {hinv12,22,X.x,X.y} {X.z,v0,v1,v2} {g0,g1,g2,ok}
+  double2* pt_inv;             // [5 M] per trial, a point with an inverse: its FP64 damped
+                               // inverse {i00,i01} {i02,i11} {i12,i22} and v = H^-1 g {v0,v1} {v2,-}
 
   // per camera
   double* cam_hpp;             // [27 C] H_pp upper 21 + g_p 6 (f64)

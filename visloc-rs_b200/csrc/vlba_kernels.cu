@@ -346,6 +346,19 @@ __global__ void __launch_bounds__(256) k_point_prep(Dev d) {
         v[1] = inv[1] * g[0] + inv[3] * g[1] + inv[4] * g[2];
         v[2] = inv[2] * g[0] + inv[4] * g[1] + inv[5] * g[2];
         ok = 1.0f;
+        // The FP64 copy the camera diagonal and the back-substitution read
+        // (point_inverse64): the same cofactors over one reciprocal of the
+        // determinant, formed once per point instead of per observation.
+        const double rdet = 1.0 / det;
+        const double i0 = m22 * rdet, i1 = (cc * e - f * b) * rdet, i2 = (b * e - dd * cc) * rdet,
+                     i3 = (a * f - cc * cc) * rdet, i4 = (cc * b - e * a) * rdet,
+                     i5 = (a * dd - b * b) * rdet;
+        double2* pi = d.pt_inv + 5 * (size_t)l;
+        pi[0] = make_double2(i0, i1);
+        pi[1] = make_double2(i2, i3);
+        pi[2] = make_double2(i4, i5);
+        pi[3] = make_double2(i0 * g[0] + i1 * g[1] + i2 * g[2], i1 * g[0] + i3 * g[1] + i4 * g[2]);
+        pi[4] = make_double2(i2 * g[0] + i4 * g[1] + i5 * g[2], 0.0);
       }
     }
     float4* ps = d.pt_s + 4 * (size_t)l;
@@ -362,35 +375,24 @@ __global__ void __launch_bounds__(256) k_point_prep(Dev d) {
   }
 }
 
-// The damped inverse of point l's H_ll and v = H^-1 g in FP64, from the
-// FP64 sums k_point_prep stores as FP32 (its cofactor formulas, with one
-// reciprocal of the determinant; k_point_prep rounds its inverse to FP32 for
-// the other kernels).  Called only for points whose determinant is nonzero.  The camera diagonal
-// needs this precision: when a point has one contributing observation (its
-// others weighted 0, or observed twice by one camera), H_ll is H_o of rank 2
-// and H_o - H_o (H_ll + lambda I)^-1 H_o cancels down to O(lambda), far
-// below what an FP32 inverse with entries near 1/lambda resolves.
-__device__ __forceinline__ void point_inverse64(const Dev& d, uint32_t l, double lambda,
-                                                double* M, double* v) {
-  const float* ph = d.pt_h + 9 * (size_t)l;
-  double a = ph[0], b = ph[1], cc = ph[2], dd = ph[3], e = ph[4], f = ph[5];
-  if (lambda > 0.0) {
-    a += lambda;
-    dd += lambda;
-    f += lambda;
-  }
-  const double m22 = dd * f - e * e, m12 = b * f - e * cc, m11 = b * e - dd * cc;
-  const double rdet = 1.0 / (a * m22 - b * m12 + cc * m11);
-  const double i0 = m22 * rdet, i1 = (cc * e - f * b) * rdet, i2 = (b * e - dd * cc) * rdet,
-               i3 = (a * f - cc * cc) * rdet, i4 = (cc * b - e * a) * rdet,
-               i5 = (a * dd - b * b) * rdet;
-  M[0] = i0; M[1] = i1; M[2] = i2;
-  M[3] = i1; M[4] = i3; M[5] = i4;
-  M[6] = i2; M[7] = i4; M[8] = i5;
-  const double g0 = ph[6], g1 = ph[7], g2 = ph[8];
-  v[0] = i0 * g0 + i1 * g1 + i2 * g2;
-  v[1] = i1 * g0 + i3 * g1 + i4 * g2;
-  v[2] = i2 * g0 + i4 * g1 + i5 * g2;
+// The damped inverse of point l's H_ll and v = H^-1 g in FP64, as
+// k_point_prep formed them this trial from the FP64 sums it stores as FP32
+// (its cofactor formulas over one reciprocal of the determinant; it rounds
+// its own inverse to FP32 for the other kernels).  Read only for points
+// whose determinant is nonzero.  The camera diagonal needs this precision:
+// when a point has one contributing observation (its others weighted 0, or
+// observed twice by one camera), H_ll is H_o of rank 2 and
+// H_o - H_o (H_ll + lambda I)^-1 H_o cancels down to O(lambda), far below
+// what an FP32 inverse with entries near 1/lambda resolves.
+__device__ __forceinline__ void point_inverse64(const Dev& d, uint32_t l, double* M, double* v) {
+  const double2* pi = d.pt_inv + 5 * (size_t)l;
+  const double2 a = pi[0], b = pi[1], c = pi[2], e = pi[3], f = pi[4];
+  M[0] = a.x; M[1] = a.y; M[2] = b.x;
+  M[3] = a.y; M[4] = b.y; M[5] = c.x;
+  M[6] = b.x; M[7] = c.x; M[8] = c.y;
+  v[0] = e.x;
+  v[1] = e.y;
+  v[2] = f.x;
 }
 
 // ------------------------------------------------- off-diagonal Schur blocks
@@ -550,7 +552,7 @@ __global__ void __launch_bounds__(kDiagThreads) k_cam_diag(Dev d) {
       const bool ok = s3.w != 0.0f;
       if (ok) {
         double Mi[9], vv[3];
-        point_inverse64(d, l, lambda, Mi, vv);
+        point_inverse64(d, l, Mi, vv);
         double M[9];
         for (int r = 0; r < 3; ++r)
           for (int cc = 0; cc < 3; ++cc)
@@ -598,7 +600,7 @@ __global__ void __launch_bounds__(kDiagThreads) k_cam_diag(Dev d) {
       const double Hi[9] = {a0.x, a0.y, a0.z, a0.y, a0.w, a1.x, a0.z, a1.x, a1.y};
       const double Hj[9] = {b0.x, b0.y, b0.z, b0.y, b0.w, b1.x, b0.z, b1.x, b1.y};
       double Mi[9], vv[3];
-      point_inverse64(d, l, lambda, Mi, vv);
+      point_inverse64(d, l, Mi, vv);
       double M[9], K[9];
       for (int r = 0; r < 3; ++r)
         for (int cc = 0; cc < 3; ++cc)
@@ -836,7 +838,7 @@ __global__ void __launch_bounds__(256) k_cost(Dev d) {
       }
       if (act) {
         double Mi[9], vv[3];
-        point_inverse64(d, l, c.lambda, Mi, vv);
+        point_inverse64(d, l, Mi, vv);
         const double e0 = -(Mi[0] * u0 + Mi[1] * u1 + Mi[2] * u2);
         const double e1 = -(Mi[3] * u0 + Mi[4] * u1 + Mi[5] * u2);
         const double e2 = -(Mi[6] * u0 + Mi[7] * u1 + Mi[8] * u2);

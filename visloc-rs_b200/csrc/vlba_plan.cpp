@@ -1189,7 +1189,8 @@ size_t Plan::device_bytes() const {
   const size_t npose = pose_prob.size(), npt = point_prob.size(), nobs = obs_pose.size();
   size_t b = 0;
   b += npose * (8 * (4 + 3 + 12) * 2 + 8 + 4 + 4);  // state x2, step, slot, prob
-  b += npt * (8 * 3 * 2 + 4 + 1 + 4 + 36 + 64);     // points x2, off, var, prob, pt_h, pt_s
+  b += npt * (8 * 3 * 2 + 4 + 1 + 4 + 36 + 64 + 80);  // points x2, off, var, prob, pt_h, pt_s,
+                                                      // pt_inv
   b += nobs * (4 * 4 + 16 + 32 + 16 + 32);           // point, pose, cam, slot, xy, obs_h, obs_e, obs_p
   b += obs_w.size() * 8 + obs_kind.size() * (1 + 16 + 4);
   b += cam_obs.size() * 4 + (pairs_on_device ? num_pairs : pairs.size()) * 8 + dup_pairs.size() * 8;

@@ -525,6 +525,7 @@ void upload_plan_once(Context* c, uint32_t max_records) {
   d.cam_obs = reuse ? from_rows(P.cam_obs, 1) : st.up(A, P.cam_obs);
   d.pt_h = A.alloc<float>(9 * npt);
   d.pt_s = A.alloc<float4>(4 * npt);
+  d.pt_inv = A.alloc<double2>(5 * npt);
   d.cam_hpp = nullptr;
   const size_t tile_floats = (size_t)P.tb * P.tb * kBlock;
   d.tiles = A.alloc<float>(P.tile_ij.size() * tile_floats);
