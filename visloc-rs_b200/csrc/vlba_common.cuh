@@ -175,6 +175,7 @@ struct Dev {
   // per-camera observation lists (indices into the point-major order)
   const uint32_t* cam_off;     // [num_var_cams + 1]
   const uint32_t* cam_obs;
+  uint32_t* cam_pt;            // [cam_obs] each listed observation's point (set at upload)
 
   // per point, per linearisation / per trial
   float* pt_h;                 // [9 M] H_ll upper (6) + g_l (3)

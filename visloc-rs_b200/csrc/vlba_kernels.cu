@@ -43,6 +43,18 @@ namespace {
 // Upper-triangle index of (r, c), r <= c, in a symmetric 6x6.
 __host__ __device__ constexpr int ut6(int r, int c) { return r * 6 - (r * (r + 1)) / 2 + c; }
 
+// A pose's 12 derived doubles (R row-major, t; 96 bytes at a 32-byte
+// aligned offset) as three 32-byte loads: a warp gathers the poses of 32
+// observations, so each load instruction costs one L1 wavefront per pose.
+// The table is read-only while the gathering kernels run.
+__device__ __forceinline__ void load_rt(const double* rt, double* out) {
+#pragma unroll
+  for (int q = 0; q < 3; ++q)
+    asm("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];"
+        : "=d"(out[4 * q]), "=d"(out[4 * q + 1]), "=d"(out[4 * q + 2]), "=d"(out[4 * q + 3])
+        : "l"(rt + 4 * q));
+}
+
 // S += sign * B^T K B for symmetric or general 3x3 K and B = [I | -[X]x]:
 // B^T K B = [[K, -K[X]x], [[X]x K, -[X]x K [X]x]]; full 6x6 row-major.
 template <typename T>
@@ -188,7 +200,8 @@ __global__ void __launch_bounds__(256, 3) k_linearize(Dev d) {
     {
       const uint32_t pose = d.obs_pose[k];
       const DevCamera& cam = d.cameras[d.obs_cam[k]];
-      const double* rt = d.pose_rt[cur] + 12 * (size_t)pose;
+      double rt[12];
+      load_rt(d.pose_rt[cur] + 12 * (size_t)pose, rt);
       double xs[3], pred[2], jpi[6];
       to_sensor(rt, cam, X, xs);
       float h[6] = {0, 0, 0, 0, 0, 0}, e[3] = {0, 0, 0};
@@ -524,83 +537,133 @@ __device__ __forceinline__ double quad3(const double* H, double a, double b, dou
 //   b_i  = sum_o B^T (H_o v - e_o)                        (-g_p + sum W v)
 // then the FP64 Cholesky inverse of S_ii as the block-Jacobi preconditioner
 // (ba.wgsl:263-387; fallback to the inverse damped diagonal, ba.wgsl:375-383).
+// Thread t adds the camera's observations t, t + 128, ... in list (= point)
+// order, so the blocks running at one time read the records of nearby
+// points.  An observation's record and its point's records are one gather
+// away (the point stored beside the list, cam_pt), nine loads of 16 and 32
+// bytes issued together; the next observation's indices are loaded while
+// this one is summed (measured on ring-4m: 270 -> 210 us against the record
+// read through the observation's own point index).
+// Warps sum by a butterfly, then in warp order: fixed order throughout.
 constexpr int kDiagThreads = 128;
+constexpr int kDiagAcc = 27;  // 21 upper S, 6 rhs
 
-constexpr int kDiagAcc = 33;  // 21 upper S, 6 rhs, 6 diag(H_pp)
+// Fixed-order block sum of n per-thread values: butterfly within each warp,
+// then the warps' sums in warp order; the totals land in tot[0, n).
+template <int N>
+__device__ __forceinline__ void diag_block_sum(double* acc, double* red, double* tot) {
+#pragma unroll
+  for (int e = 0; e < N; ++e) {
+    double v = acc[e];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+    acc[e] = v;
+  }
+  const int warp = threadIdx.x / 32;
+  if ((threadIdx.x % 32) == 0) {
+#pragma unroll
+    for (int e = 0; e < N; ++e) red[warp * N + e] = acc[e];
+  }
+  __syncthreads();
+  if (threadIdx.x < (unsigned)N) {
+    double t = 0.0;
+    for (int w = 0; w < kDiagThreads / 32; ++w) t += red[w * N + threadIdx.x];
+    tot[threadIdx.x] = t;
+  }
+  __syncthreads();
+}
+
+// Observation k (of point l)'s terms of S_ii and b_i.
+__device__ __forceinline__ void cam_diag_obs(const Dev& d, uint32_t k, uint32_t l, double* acc) {
+  float4 h0, h1, s2, s3;
+  ld8(d.obs_h + 2 * (size_t)k, h0, h1);
+  const float4 ev = __ldg(d.obs_e + k);
+  const float4 s1 = __ldg(d.pt_s + 4 * (size_t)l + 1);
+  ld8(d.pt_s + 4 * (size_t)l + 2, s2, s3);
+  // The point's FP64 damped inverse and v (formed by k_point_prep when the
+  // point has one; read unconditionally so the loads go out together).
+  const double2* pi = d.pt_inv + 5 * (size_t)l;
+  const double2 ia = __ldg(pi), ib = __ldg(pi + 1), ic = __ldg(pi + 2), ie = __ldg(pi + 3),
+                if_ = __ldg(pi + 4);
+  const double H[9] = {h0.x, h0.y, h0.z, h0.y, h0.w, h1.x, h0.z, h1.x, h1.y};
+  const double X = s1.z, Y = s1.w, Z = s2.x;
+  double K[9], w[3];
+  if (s3.w != 0.0f) {
+    const double Mi[9] = {ia.x, ia.y, ib.x, ia.y, ib.y, ic.x, ib.x, ic.x, ic.y};
+    double M[9];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc)
+        M[r * 3 + cc] = Mi[r * 3] * H[cc] + Mi[r * 3 + 1] * H[3 + cc] + Mi[r * 3 + 2] * H[6 + cc];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc)
+        K[r * 3 + cc] = H[r * 3 + cc] - (H[r * 3] * M[cc] + H[r * 3 + 1] * M[3 + cc] +
+                                         H[r * 3 + 2] * M[6 + cc]);
+    const double v0 = ie.x, v1 = ie.y, v2 = if_.x;
+    w[0] = H[0] * v0 + H[1] * v1 + H[2] * v2 - ev.x;
+    w[1] = H[3] * v0 + H[4] * v1 + H[5] * v2 - ev.y;
+    w[2] = H[6] * v0 + H[7] * v1 + H[8] * v2 - ev.z;
+  } else {
+#pragma unroll
+    for (int q = 0; q < 9; ++q) K[q] = H[q];
+    w[0] = -(double)ev.x;
+    w[1] = -(double)ev.y;
+    w[2] = -(double)ev.z;
+  }
+  add_btkb_upper(K, X, Y, Z, acc, 1.0);
+  acc[21] += w[0];
+  acc[22] += w[1];
+  acc[23] += w[2];
+  acc[24] += Y * w[2] - Z * w[1];
+  acc[25] += Z * w[0] - X * w[2];
+  acc[26] += X * w[1] - Y * w[0];
+}
 
 __global__ void __launch_bounds__(kDiagThreads) k_cam_diag(Dev d) {
   __shared__ double red[(kDiagThreads / 32) * kDiagAcc];
   __shared__ double tot[kDiagAcc];
+  __shared__ int s_fail;
+  const uint32_t t = threadIdx.x;
   for (uint32_t s = blockIdx.x; s < d.num_var_cams; s += gridDim.x) {
     const uint32_t P = d.slot_prob[s];
     if (d.ctrl[P].done) continue;
-    const double lambda = d.ctrl[P].lambda;
+    const uint32_t o0 = d.cam_off[s], o1 = d.cam_off[s + 1];
     double acc[kDiagAcc];
 #pragma unroll
     for (int e = 0; e < kDiagAcc; ++e) acc[e] = 0.0;
-    const uint32_t o0 = d.cam_off[s], o1 = d.cam_off[s + 1];
-    for (uint32_t idx = o0 + threadIdx.x; idx < o1; idx += kDiagThreads) {
-      const uint32_t k = d.cam_obs[idx];
-      const float4 h0 = d.obs_h[2 * (size_t)k], h1 = d.obs_h[2 * (size_t)k + 1];
-      const float4 ev = d.obs_e[k];
-      const uint32_t l = __float_as_uint(h1.z);
-      const float4 s1 = d.pt_s[4 * (size_t)l + 1], s2 = d.pt_s[4 * (size_t)l + 2],
-                   s3 = d.pt_s[4 * (size_t)l + 3];
-      const double H[9] = {h0.x, h0.y, h0.z, h0.y, h0.w, h1.x, h0.z, h1.x, h1.y};
-      const double X = s1.z, Y = s1.w, Z = s2.x;
-      double K[9], u[3];
-      const bool ok = s3.w != 0.0f;
-      if (ok) {
-        double Mi[9], vv[3];
-        point_inverse64(d, l, Mi, vv);
-        double M[9];
-        for (int r = 0; r < 3; ++r)
-          for (int cc = 0; cc < 3; ++cc)
-            M[r * 3 + cc] = Mi[r * 3] * H[cc] + Mi[r * 3 + 1] * H[3 + cc] + Mi[r * 3 + 2] * H[6 + cc];
-        for (int r = 0; r < 3; ++r)
-          for (int cc = 0; cc < 3; ++cc)
-            K[r * 3 + cc] = H[r * 3 + cc] - (H[r * 3] * M[cc] + H[r * 3 + 1] * M[3 + cc] +
-                                             H[r * 3 + 2] * M[6 + cc]);
-        const double v0 = vv[0], v1 = vv[1], v2 = vv[2];
-        u[0] = H[0] * v0 + H[1] * v1 + H[2] * v2 - ev.x;
-        u[1] = H[3] * v0 + H[4] * v1 + H[5] * v2 - ev.y;
-        u[2] = H[6] * v0 + H[7] * v1 + H[8] * v2 - ev.z;
-      } else {
-        for (int e = 0; e < 9; ++e) K[e] = H[e];
-        u[0] = -(double)ev.x;
-        u[1] = -(double)ev.y;
-        u[2] = -(double)ev.z;
+    uint32_t idx = o0 + t, k = kNone, l = 0u;
+    if (idx < o1) {
+      k = d.cam_obs[idx];
+      l = d.cam_pt[idx];
+    }
+    while (k != kNone) {
+      const uint32_t nidx = idx + kDiagThreads;
+      uint32_t nk = kNone, nl = 0u;
+      if (nidx < o1) {
+        nk = d.cam_obs[nidx];
+        nl = d.cam_pt[nidx];
       }
-      add_btkb_upper(K, X, Y, Z, acc, 1.0);
-      acc[21] += u[0];
-      acc[22] += u[1];
-      acc[23] += u[2];
-      acc[24] += Y * u[2] - Z * u[1];
-      acc[25] += Z * u[0] - X * u[2];
-      acc[26] += X * u[1] - Y * u[0];
-      // diag(B^T H B) for the fallback preconditioner: H_aa, then the
-      // quadratic forms (X x e_a)^T H (X x e_a).
-      acc[27] += H[0];
-      acc[28] += H[4];
-      acc[29] += H[8];
-      acc[30] += quad3(H, 0.0, Z, -Y);
-      acc[31] += quad3(H, -Z, 0.0, X);
-      acc[32] += quad3(H, Y, -X, 0.0);
+      cam_diag_obs(d, k, l, acc);
+      idx = nidx;
+      k = nk;
+      l = nl;
     }
     // Same-camera pairs k != k' of one point (a point observed twice by a
     // camera): -B^T H_k H^-1 H_k' B, both orders listed.
-    for (uint32_t idx = d.dup_off[s] + threadIdx.x; idx < d.dup_off[s + 1];
-         idx += kDiagThreads) {
-      const uint2 pr = d.dup_pairs[idx];
+    for (uint32_t i = d.dup_off[s] + t; i < d.dup_off[s + 1]; i += kDiagThreads) {
+      const uint2 pr = d.dup_pairs[i];
       const float4 a0 = d.obs_h[2 * (size_t)pr.x], a1 = d.obs_h[2 * (size_t)pr.x + 1];
       const float4 b0 = d.obs_h[2 * (size_t)pr.y], b1 = d.obs_h[2 * (size_t)pr.y + 1];
-      const uint32_t l = __float_as_uint(a1.z);
-      const float4 s1 = d.pt_s[4 * (size_t)l + 1], s2 = d.pt_s[4 * (size_t)l + 2];
-      if (d.pt_s[4 * (size_t)l + 3].w == 0.0f) continue;  // no inverse: no Schur term
+      const uint32_t pl = __float_as_uint(a1.z);
+      const float4 s1 = d.pt_s[4 * (size_t)pl + 1], s2 = d.pt_s[4 * (size_t)pl + 2];
+      if (d.pt_s[4 * (size_t)pl + 3].w == 0.0f) continue;  // no inverse: no Schur term
       const double Hi[9] = {a0.x, a0.y, a0.z, a0.y, a0.w, a1.x, a0.z, a1.x, a1.y};
       const double Hj[9] = {b0.x, b0.y, b0.z, b0.y, b0.w, b1.x, b0.z, b1.x, b1.y};
       double Mi[9], vv[3];
-      point_inverse64(d, l, Mi, vv);
+      point_inverse64(d, pl, Mi, vv);
       double M[9], K[9];
       for (int r = 0; r < 3; ++r)
         for (int cc = 0; cc < 3; ++cc)
@@ -610,28 +673,9 @@ __global__ void __launch_bounds__(kDiagThreads) k_cam_diag(Dev d) {
           K[r * 3 + cc] = Hi[r * 3] * M[cc] + Hi[r * 3 + 1] * M[3 + cc] + Hi[r * 3 + 2] * M[6 + cc];
       add_btkb_upper(K, (double)s1.z, (double)s1.w, (double)s2.x, acc, -1.0);
     }
-    // Fixed-order reduction: butterfly within each warp, then the warps'
-    // sums in warp order.
-#pragma unroll
-    for (int e = 0; e < kDiagAcc; ++e) {
-      double v = acc[e];
-#pragma unroll
-      for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-      acc[e] = v;
-    }
-    const int warp = threadIdx.x / 32;
-    if ((threadIdx.x % 32) == 0) {
-#pragma unroll
-      for (int e = 0; e < kDiagAcc; ++e) red[warp * kDiagAcc + e] = acc[e];
-    }
-    __syncthreads();
-    if (threadIdx.x < (unsigned)kDiagAcc) {
-      double t = 0.0;
-      for (int w = 0; w < kDiagThreads / 32; ++w) t += red[w * kDiagAcc + threadIdx.x];
-      tot[threadIdx.x] = t;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
+    diag_block_sum<kDiagAcc>(acc, red, tot);
+    const double lambda = d.ctrl[P].lambda;
+    if (t == 0) {
       double S[36], inv[36];
       for (int r = 0; r < 6; ++r)
         for (int cc = 0; cc < 6; ++cc) {
@@ -642,11 +686,36 @@ __global__ void __launch_bounds__(kDiagThreads) k_cam_diag(Dev d) {
       float* blk = d.tiles + d.diag_dst[s];
       for (int e = 0; e < 36; ++e) blk[e] = (float)S[e];
       for (int a = 0; a < 6; ++a) d.rhs[6 * (size_t)s + a] = (float)tot[21 + a];
-      if (!chol_inverse6(S, inv)) {
-        for (int e = 0; e < 36; ++e) inv[e] = 0.0;
-        for (int a = 0; a < 6; ++a) inv[a * 7] = 1.0 / fmax(tot[27 + a] + lambda, 1e-20);
+      const bool ok = chol_inverse6(S, inv);
+      if (ok)
+        for (int e = 0; e < 36; ++e) d.minv[36 * (size_t)s + e] = (float)inv[e];
+      s_fail = ok ? 0 : 1;
+    }
+    __syncthreads();
+    if (s_fail) {
+      // Not positive definite: the inverse damped diagonal of B^T H B over
+      // the camera's observations (H_aa, then the quadratic forms
+      // (X x e_a)^T H (X x e_a)), summed only for such a camera.
+      double g[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+      for (uint32_t i = o0 + t; i < o1; i += kDiagThreads) {
+        const uint32_t kk = d.cam_obs[i], pl = d.cam_pt[i];
+        const float4 h0 = d.obs_h[2 * (size_t)kk], h1 = d.obs_h[2 * (size_t)kk + 1];
+        const float4 s1 = d.pt_s[4 * (size_t)pl + 1], s2 = d.pt_s[4 * (size_t)pl + 2];
+        const double H[9] = {h0.x, h0.y, h0.z, h0.y, h0.w, h1.x, h0.z, h1.x, h1.y};
+        const double X = s1.z, Y = s1.w, Z = s2.x;
+        g[0] += H[0];
+        g[1] += H[4];
+        g[2] += H[8];
+        g[3] += quad3(H, 0.0, Z, -Y);
+        g[4] += quad3(H, -Z, 0.0, X);
+        g[5] += quad3(H, Y, -X, 0.0);
       }
-      for (int e = 0; e < 36; ++e) d.minv[36 * (size_t)s + e] = (float)inv[e];
+      diag_block_sum<6>(g, red, tot);
+      if (t == 0) {
+        for (int e = 0; e < 36; ++e) d.minv[36 * (size_t)s + e] = 0.0f;
+        for (int a = 0; a < 6; ++a)
+          d.minv[36 * (size_t)s + a * 7] = (float)(1.0 / fmax(tot[a] + lambda, 1e-20));
+      }
     }
     __syncthreads();
   }
@@ -809,11 +878,13 @@ __global__ void __launch_bounds__(256) k_cost(Dev d) {
           const uint32_t slot = d.obs_slot[k];
           if (sAct[pl] && slot != kNone) {
             const double x = sXf[3 * pl], y = sXf[3 * pl + 1], z = sXf[3 * pl + 2];
-            const float* dc = d.x + 6 * (size_t)slot;
-            const double w0 = dc[3], w1 = dc[4], w2 = dc[5];
-            const double b0 = dc[0] + (w1 * z - w2 * y);
-            const double b1 = dc[1] + (w2 * x - w0 * z);
-            const double b2 = dc[2] + (w0 * y - w1 * x);
+            // The slot's step as three 8-byte loads.
+            const float2* dc = reinterpret_cast<const float2*>(d.x + 6 * (size_t)slot);
+            const float2 c01 = dc[0], c23 = dc[1], c45 = dc[2];
+            const double w0 = c23.y, w1 = c45.x, w2 = c45.y;
+            const double b0 = c01.x + (w1 * z - w2 * y);
+            const double b1 = c01.y + (w2 * x - w0 * z);
+            const double b2 = c23.x + (w0 * y - w1 * x);
             const float4 h0 = d.obs_h[2 * (size_t)k], h1 = d.obs_h[2 * (size_t)k + 1];
             t0 = h0.x * b0 + h0.y * b1 + h0.z * b2;
             t1 = h0.y * b0 + h0.w * b1 + h1.x * b2;
@@ -863,7 +934,8 @@ __global__ void __launch_bounds__(256) k_cost(Dev d) {
     for (uint32_t k = o0 + threadIdx.x; k < o1; k += blockDim.x) {
       const double* Xk = sX + 3 * (d.obs_point[k] - lo);
       const DevCamera& cam = d.cameras[d.obs_cam[k]];
-      const double* rt = d.pose_rt[pose_buf] + 12 * (size_t)d.obs_pose[k];
+      double rt[12];
+      load_rt(d.pose_rt[pose_buf] + 12 * (size_t)d.obs_pose[k], rt);
       double xs[3], pred[2];
       to_sensor(rt, cam, Xk, xs);
       double ss;
@@ -2061,6 +2133,13 @@ __global__ void k_wait_probe(const unsigned int* flag, unsigned long long limit_
 }
 
 // Current state (buffer Ctrl::cur) of every problem into buffer 0.
+// The point of every listed observation, beside the per-slot lists (read
+// by the camera-diagonal sums with the observation index, both coalesced).
+__global__ void __launch_bounds__(256) k_cam_points(Dev d, uint32_t n) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    d.cam_pt[i] = d.obs_point[d.cam_obs[i]];
+}
+
 __global__ void __launch_bounds__(256) k_state_to_front(Dev d) {
   const uint32_t stride = gridDim.x * blockDim.x;
   for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < d.num_poses; p += stride) {
@@ -2232,6 +2311,12 @@ __global__ void __launch_bounds__(256) k_sq_residuals(Dev d, double* out) {
 
 cudaError_t launch_sq_residuals(const Dev& d, double* out, cudaStream_t s) {
   k_sq_residuals<<<grid1d(d.num_obs, 256), 256, 0, s>>>(d, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_cam_points(const Dev& d, uint32_t n, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  k_cam_points<<<grid1d(n, 256), 256, 0, s>>>(d, n);
   return cudaGetLastError();
 }
 

@@ -16,6 +16,8 @@ cudaError_t launch_linearize(const Dev& d, cudaStream_t s);
 cudaError_t launch_point_prep(const Dev& d, cudaStream_t s);
 cudaError_t launch_offdiag(const Dev& d, cudaStream_t s);
 cudaError_t launch_cam_diag(const Dev& d, cudaStream_t s);
+// cam_pt[i] = obs_point[cam_obs[i]] for the n listed observations.
+cudaError_t launch_cam_points(const Dev& d, uint32_t n, cudaStream_t s);
 cudaError_t launch_pcg(const Dev& d, int sm_count, cudaStream_t s);
 cudaError_t launch_pose_update(const Dev& d, cudaStream_t s);
 cudaError_t launch_pcg_setup(const Dev& d, cudaStream_t s);

@@ -105,6 +105,32 @@ LmParams make_params(const vlba_config* cfg) {
   return lp;
 }
 
+namespace {
+
+// Lowest index in [0, n) at which pred fails (n if none), on the host's
+// threads for large n: each thread scans its own range in order and stops at
+// its first failure, and the lowest of those is the serial scan's answer.
+template <typename F>
+uint64_t first_failing(uint64_t n, F&& pred) {
+  const uint64_t hw = std::max(1u, std::thread::hardware_concurrency());
+  const uint32_t T = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(hw, n >> 18));
+  std::vector<uint64_t> first(T, n);
+  auto body = [&](uint32_t t) {
+    for (uint64_t i = n * t / T, e = n * (t + 1) / T; i < e; ++i)
+      if (!pred(i)) {
+        first[t] = i;
+        return;
+      }
+  };
+  std::vector<std::thread> pool;
+  for (uint32_t t = 1; t < T; ++t) pool.emplace_back(body, t);
+  body(0);
+  for (auto& th : pool) th.join();
+  return *std::min_element(first.begin(), first.end());
+}
+
+}  // namespace
+
 Validation validate_problem(const vlba_problem* p, const vlba_config* cfg) {
   Validation v;
   if (!p || !cfg) { v.status = VLBA_ERR_INVALID_ARGUMENT; return v; }
@@ -128,13 +154,16 @@ Validation validate_problem(const vlba_problem* p, const vlba_config* cfg) {
   }
   // External observation weights before anything else, as
   // optimize_with_observation_weights checks them (optimize.rs:48, 628-650).
-  if (p->obs_weight)
-    for (uint64_t o = 0; o < p->num_observations; ++o)
-      if (!std::isfinite(p->obs_weight[o]) || p->obs_weight[o] < 0.0) {
-        v.status = VLBA_ERR_INVALID_OBSERVATION_WEIGHT;
-        v.error_index = o;
-        return v;
-      }
+  if (p->obs_weight) {
+    const uint64_t o = first_failing(p->num_observations, [&](uint64_t k) {
+      return std::isfinite(p->obs_weight[k]) && p->obs_weight[k] >= 0.0;
+    });
+    if (o < p->num_observations) {
+      v.status = VLBA_ERR_INVALID_OBSERVATION_WEIGHT;
+      v.error_index = o;
+      return v;
+    }
+  }
   // Camera model first (lm.rs:168 `intrinsics()?`); a model outside the
   // radial pinhole family is declined, so the caller runs its CPU solver.
   if (p->num_cameras == 0 || !p->cameras) { v.status = VLBA_ERR_UNSUPPORTED_CAMERA_MODEL; return v; }
@@ -201,19 +230,19 @@ Validation validate_problem(const vlba_problem* p, const vlba_config* cfg) {
       v.status = VLBA_ERR_MISSING_STEREO_BASELINE;
       return v;
     }
-    for (uint64_t o = 0; o < p->num_observations; ++o) {
-      if (kind_of(o) != (uint32_t)lists[li]) continue;
+    // The list's first observation with a bad reference, then its error as
+    // the serial checks below order them.
+    const uint64_t o = first_failing(p->num_observations, [&](uint64_t k) {
+      if (kind_of(k) != (uint32_t)lists[li]) return true;
+      return p->obs_pose[k] < p->num_poses && p->obs_landmark[k] < p->num_landmarks &&
+             !(lists[li] == (int)kObsGeneralStereo && p->obs_right_camera[k] >= p->num_cameras) &&
+             !(lists[li] == (int)kObsMono && p->obs_camera && p->obs_camera[k] >= p->num_cameras);
+    });
+    if (o < p->num_observations) {
       if (!refs_ok(o)) return v;
-      if (lists[li] == (int)kObsGeneralStereo && p->obs_right_camera[o] >= p->num_cameras) {
-        v.status = VLBA_ERR_INVALID_ARGUMENT;
-        v.error_index = o;
-        return v;
-      }
-      if (lists[li] == (int)kObsMono && p->obs_camera && p->obs_camera[o] >= p->num_cameras) {
-        v.status = VLBA_ERR_INVALID_ARGUMENT;
-        v.error_index = o;
-        return v;
-      }
+      v.status = VLBA_ERR_INVALID_ARGUMENT;
+      v.error_index = o;
+      return v;
     }
   }
   bool any_var = false;
@@ -462,7 +491,6 @@ void build_plan_serial(const vlba_problem* const* problems, const vlba_config* c
     }, obs_base, P.cam_obs.data() + list_base, c2.data());
     P.cam_obs.resize(list_base + (size_t)c2[nslots]);
     for (uint32_t s = 0; s < nslots; ++s) P.cam_off.push_back(list_base + c2[s + 1]);
-    std::vector<std::vector<uint32_t>> row_col(nvar), row_count(nvar);
     const uint64_t pair_base = P.pairs.size();
     std::vector<uint64_t> row_at(nvar + 1, pair_base);
     // The block structure from the device when it can take this problem
@@ -471,6 +499,9 @@ void build_plan_serial(const vlba_problem* const* problems, const vlba_config* c
     RowBlocks rb;
     const bool device_terms = n == 1 && device_rows && *device_rows &&
                               (*device_rows)(P, nvar, &rb) && rb.row_off.size() == nvar + 1u;
+    // Each row's blocks (columns ascending) and their term counts, flat:
+    // row i's are [blk_row[i], blk_row[i + 1]) of blk_cols / blk_cnts.
+    std::vector<uint32_t> blk_row, blk_cols, blk_cnts;
     if (device_terms) {
       std::vector<uint64_t> part(To, 0);
       run_threads(To, [&](uint32_t t) {
@@ -483,27 +514,33 @@ void build_plan_serial(const vlba_problem* const* problems, const vlba_config* c
         part[t] = nv;
       });
       for (uint32_t t = 0; t < To; ++t) P.var_obs += part[t];
-      for (uint32_t i = 0; i < nvar; ++i) {
-        uint64_t at = row_at[i];
-        for (uint32_t q = rb.row_off[i]; q < rb.row_off[i + 1]; ++q) {
-          if (rb.col[q] >= i || rb.count[q] == 0 || (q > rb.row_off[i] && rb.col[q] <= rb.col[q - 1]))
-            throw std::runtime_error("device row blocks out of order");
-          row_col[i].push_back(rb.col[q]);
-          row_count[i].push_back(rb.count[q]);
-          at += rb.count[q];
+      blk_row = std::move(rb.row_off);
+      blk_cols = std::move(rb.col);
+      blk_cnts = std::move(rb.count);
+      if (blk_row[0] != 0 || blk_cols.size() != blk_row[nvar] || blk_cnts.size() != blk_row[nvar])
+        throw std::runtime_error("device row blocks out of range");
+      // Each row's columns below it, ascending, with terms; its term total.
+      std::vector<uint64_t> row_terms(nvar, 0);
+      run_threads(To, [&](uint32_t t) {
+        for (uint32_t i = (uint32_t)((uint64_t)nvar * t / To); i < (uint32_t)((uint64_t)nvar * (t + 1) / To); ++i) {
+          if (blk_row[i] > blk_row[i + 1]) throw std::runtime_error("device row blocks out of order");
+          uint64_t sum = 0;
+          for (uint32_t q = blk_row[i]; q < blk_row[i + 1]; ++q) {
+            if (blk_cols[q] >= i || blk_cnts[q] == 0 || (q > blk_row[i] && blk_cols[q] <= blk_cols[q - 1]))
+              throw std::runtime_error("device row blocks out of order");
+            sum += blk_cnts[q];
+          }
+          row_terms[i] = sum;
         }
-        row_at[i + 1] = at;
-      }
+      });
+      for (uint32_t i = 0; i < nvar; ++i) row_at[i + 1] = row_at[i] + row_terms[i];
       if (row_at[nvar] >= kNone) throw std::runtime_error("more than 2^32 Schur terms");
       for (uint32_t s = 0; s < nslots; ++s) P.dup_off.push_back((uint32_t)P.dup_pairs.size());
       P.pairs_on_device = true;
       P.num_pairs = row_at[nvar];
-      P.row_blk.assign(1, 0u);
-      for (uint32_t i = 0; i < nvar; ++i) {
-        for (uint32_t c : row_col[i]) P.blk_col.push_back(c);
-        P.row_blk.push_back((uint32_t)P.blk_col.size());
-      }
-      for (uint32_t s = nvar; s < nslots; ++s) P.row_blk.push_back((uint32_t)P.blk_col.size());
+      P.row_blk.assign(blk_row.begin(), blk_row.end());
+      P.row_blk.resize((size_t)nslots + 1, blk_row[nvar]);
+      P.blk_col.assign(blk_cols.begin(), blk_cols.end());
     } else {
       // Camera pairs sharing a variable point: blocks (i, j), j < i (local
       // slots), each holding its terms (x, y) -- x the observation in slot i,
@@ -617,6 +654,7 @@ void build_plan_serial(const vlba_problem* const* problems, const vlba_config* c
       });
       // (C) per row, a stable counting sort of its terms by column; the row's
       // blocks are its distinct columns, ascending.
+      std::vector<std::vector<uint32_t>> row_col(nvar), row_count(nvar);
       {
         std::atomic<uint32_t> next{0};
         run_threads(T, [&](uint32_t) {
@@ -650,23 +688,39 @@ void build_plan_serial(const vlba_problem* const* problems, const vlba_config* c
         });
       }
       term_col.clear();
+      blk_row.assign(nvar + 1, 0u);
+      for (uint32_t i = 0; i < nvar; ++i) blk_row[i + 1] = blk_row[i] + (uint32_t)row_col[i].size();
+      blk_cols.reserve(blk_row[nvar]);
+      blk_cnts.reserve(blk_row[nvar]);
+      for (uint32_t i = 0; i < nvar; ++i) {
+        blk_cols.insert(blk_cols.end(), row_col[i].begin(), row_col[i].end());
+        blk_cnts.insert(blk_cnts.end(), row_count[i].begin(), row_count[i].end());
+      }
     }
 
-    // Blocks in row-major order; per-tile existence.
+    // Blocks in row-major order; per-tile existence.  Rows run on the host's
+    // threads in whole tile rows (a tile row's existence flags are its own).
     const uint32_t ntr = nslots / tb;
     std::vector<uint8_t> tile_has((size_t)ntr * ntr, 0);
     const uint32_t blk_base = (uint32_t)P.blk_dst.size();
-    std::vector<uint32_t> row_blk(nvar + 1, 0);  // first local block of each row
-    for (uint32_t i = 0; i < nvar; ++i) {
-      row_blk[i + 1] = row_blk[i] + (uint32_t)row_col[i].size();
-      uint64_t run = row_at[i];
-      for (size_t b = 0; b < row_col[i].size(); ++b) {
-        tile_has[(size_t)(i / tb) * ntr + row_col[i][b] / tb] = 1;
-        run += row_count[i][b];
-        P.blk_off.push_back((uint32_t)run);
-      }
-    }
-    const uint32_t nblk = row_blk[nvar];
+    const uint32_t nblk = blk_row[nvar];
+    const uint32_t Tr = std::max(1u, std::min<uint32_t>(To, ntr));
+    auto tile_rows = [&](uint32_t t, auto&& f) {
+      for (uint32_t I = (uint32_t)((uint64_t)ntr * t / Tr); I < (uint32_t)((uint64_t)ntr * (t + 1) / Tr); ++I)
+        for (uint32_t i = I * tb; i < std::min(nvar, (I + 1) * tb); ++i) f(I, i);
+    };
+    P.blk_off.resize((size_t)blk_base + 1 + nblk);
+    uint32_t* const boff = P.blk_off.data() + blk_base + 1;
+    run_threads(Tr, [&](uint32_t t) {
+      tile_rows(t, [&](uint32_t I, uint32_t i) {
+        uint64_t run = row_at[i];
+        for (uint32_t b = blk_row[i]; b < blk_row[i + 1]; ++b) {
+          tile_has[(size_t)I * ntr + blk_cols[b] / tb] = 1;
+          run += blk_cnts[b];
+          boff[b] = (uint32_t)run;
+        }
+      });
+    });
     P.camera_pairs += nblk;
     for (uint32_t t = 0; t < ntr; ++t) tile_has[(size_t)t * ntr + t] = 1;
     // Compact tile ids, row-major.
@@ -681,16 +735,19 @@ void build_plan_serial(const vlba_problem* const* problems, const vlba_config* c
         }
     // Block destinations.
     P.blk_dst.resize(blk_base + nblk);
-    for (uint32_t i = 0; i < nvar; ++i)
-      for (uint32_t b = row_blk[i]; b < row_blk[i + 1]; ++b) {
-        const uint32_t jj = row_col[i][b - row_blk[i]];
-        const uint32_t I = i / tb, J = jj / tb, li = i % tb, lj = jj % tb;
-        const uint32_t t = tile_id[(size_t)I * ntr + J];
-        PairIdx dst;
-        dst.a = t * tile_floats + (li * tb + lj) * kBlock;
-        dst.b = (I == J) ? t * tile_floats + (lj * tb + li) * kBlock : kNone;
-        P.blk_dst[blk_base + b] = dst;
-      }
+    run_threads(Tr, [&](uint32_t t) {
+      tile_rows(t, [&](uint32_t I, uint32_t i) {
+        for (uint32_t b = blk_row[i]; b < blk_row[i + 1]; ++b) {
+          const uint32_t jj = blk_cols[b];
+          const uint32_t J = jj / tb, li = i % tb, lj = jj % tb;
+          const uint32_t tt = tile_id[(size_t)I * ntr + J];
+          PairIdx dst;
+          dst.a = tt * tile_floats + (li * tb + lj) * kBlock;
+          dst.b = (I == J) ? tt * tile_floats + (lj * tb + li) * kBlock : kNone;
+          P.blk_dst[blk_base + b] = dst;
+        }
+      });
+    });
     for (uint32_t s = 0; s < nslots; ++s) {
       const uint32_t I = s / tb, li = s % tb;
       P.diag_dst.push_back(tile_id[(size_t)I * ntr + I] * tile_floats + (li * tb + li) * kBlock);
@@ -1193,7 +1250,7 @@ size_t Plan::device_bytes() const {
                                                       // pt_inv
   b += nobs * (4 * 4 + 16 + 32 + 16 + 32);           // point, pose, cam, slot, xy, obs_h, obs_e, obs_p
   b += obs_w.size() * 8 + obs_kind.size() * (1 + 16 + 4);
-  b += cam_obs.size() * 4 + (pairs_on_device ? num_pairs : pairs.size()) * 8 + dup_pairs.size() * 8;
+  b += cam_obs.size() * 8 + (pairs_on_device ? num_pairs : pairs.size()) * 8 + dup_pairs.size() * 8;
   b += blk_dst.size() * (8 + 4);
   b += tile_ij.size() * ((size_t)tb * tb * kBlock * 4 + 4 + 2 * (size_t)tb * 6 * 4);
   b += (size_t)num_var_cams * (4 + 4 + 4 + 4 + 36 * 4 + 6 * 4 * 6);

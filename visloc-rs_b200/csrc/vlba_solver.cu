@@ -445,7 +445,9 @@ void check_launch(cudaError_t e, const char* what) {
   if (e != cudaSuccess) throw CudaError(e, what);
 }
 
-void upload_plan_once(Context* c, uint32_t max_records) {
+// `before_kernels` (if set) runs before the first kernel that reads the
+// plan's arrays: the copies may start while the host still checks the plan.
+void upload_plan_once(Context* c, uint32_t max_records, const std::function<void()>& before_kernels) {
   Plan& P = c->plan;
   cudaStream_t s = c->stream;
   drop_graph(c);  // its kernels hold the old device pointers
@@ -523,6 +525,7 @@ void upload_plan_once(Context* c, uint32_t max_records) {
   d.obs_p = A.alloc<float4>(2 * nobs);
   d.cam_off = reuse ? from_rows(P.cam_off, 0) : st.up(A, P.cam_off);
   d.cam_obs = reuse ? from_rows(P.cam_obs, 1) : st.up(A, P.cam_obs);
+  d.cam_pt = A.alloc<uint32_t>(P.cam_obs.size());
   d.pt_h = A.alloc<float>(9 * npt);
   d.pt_s = A.alloc<float4>(4 * npt);
   d.pt_inv = A.alloc<double2>(5 * npt);
@@ -579,6 +582,8 @@ void upload_plan_once(Context* c, uint32_t max_records) {
   d.chunk_step = A.alloc<double>(nch);
   st.flush(s);
   c->dev = d;
+  if (before_kernels) before_kernels();
+  check_launch(launch_cam_points(d, (uint32_t)P.cam_obs.size(), s), "camera lists");
   if (P.pairs_on_device) {
     // The terms, from the uploaded point-major observations and per-slot
     // lists, at the places the host laid out; checked as they are written.
@@ -626,17 +631,18 @@ void upload_plan_once(Context* c, uint32_t max_records) {
   c->uploaded = true;
 }
 
-void upload_plan(Context* c, uint32_t max_records) {
+void upload_plan(Context* c, uint32_t max_records,
+                 const std::function<void()>& before_kernels = nullptr) {
   ++c->plan_generation;
   const size_t est = c->plan.device_bytes() + (size_t)max_records * sizeof(vlba_iteration) *
                                                    c->plan.num_problems + (4u << 20);
   if (c->arena.growable()) c->arena.reserve(std::max(est, c->arena.capacity()));
   try {
-    upload_plan_once(c, max_records);
+    upload_plan_once(c, max_records, before_kernels);
   } catch (const SlabFull& f) {
     // The estimate was short: one retry on a slab with room to spare.
     c->arena.reserve(std::max(2 * c->arena.capacity(), f.need + f.need / 2));
-    upload_plan_once(c, max_records);
+    upload_plan_once(c, max_records, before_kernels);
   }
 }
 
@@ -1164,17 +1170,38 @@ void do_upload(Context* c, const vlba_problem* const* probs, const vlba_config* 
   build_plan(probs, cfgs, n, (uint32_t)pick_tb(probs, n), &c->plan, 0,
              large ? &device_rows : nullptr);
   const double t_build = ms_since(tb0);
-  const auto tc0 = std::chrono::steady_clock::now();
-  const std::string bad = check_plan(c->plan);
-  if (!bad.empty()) throw Status(VLBA_ERR_INVALID_ARGUMENT, bad);
-  const double t_check = ms_since(tc0);
+  // The plan check runs on its own thread while the arrays are copied, and
+  // ends before the first kernel reads them.
   const auto tu0 = std::chrono::steady_clock::now();
-  upload_plan(c, max_records);
+  std::string bad;
+  double t_check = 0.0, t_wait = 0.0;
+  std::thread checker([&] {
+    const auto tc0 = std::chrono::steady_clock::now();
+    bad = check_plan(c->plan);
+    t_check = ms_since(tc0);
+  });
+  struct Join {
+    std::thread& t;
+    ~Join() {
+      if (t.joinable()) t.join();
+    }
+  } join{checker};
+  const std::function<void()> checked = [&] {
+    if (checker.joinable()) {
+      const auto w0 = std::chrono::steady_clock::now();
+      checker.join();
+      t_wait = ms_since(w0);
+    }
+    if (!bad.empty()) throw Status(VLBA_ERR_INVALID_ARGUMENT, bad);
+  };
+  upload_plan(c, max_records, checked);
+  checked();
   if (trace)
     std::fprintf(stderr,
                  "vlba upload: validate %.2f ms, plan %.2f ms (device row counts %.2f ms), "
-                 "check %.2f ms, copy and device terms %.2f ms\n",
-                 t_validate, t_build, t_rows, t_check, ms_since(tu0));
+                 "copy, check and device terms %.2f ms (check %.2f ms beside the copies, "
+                 "%.2f ms waited)\n",
+                 t_validate, t_build, t_rows, ms_since(tu0), t_check, t_wait);
   c->num_poses.clear();
   c->num_points.clear();
   for (uint32_t i = 0; i < n; ++i) {
