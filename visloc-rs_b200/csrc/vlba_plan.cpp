@@ -1242,6 +1242,24 @@ std::string check_plan(const Plan& P) {
   return std::string();
 }
 
+void block_order(const Plan& P, uint32_t window, std::vector<uint32_t>* order) {
+  const uint32_t nb = (uint32_t)P.blk_dst.size();
+  const uint32_t g = std::max(1u, P.group);
+  order->resize(nb);
+  uint32_t* const o = order->data();
+  const uint32_t nw = (nb + window - 1) / window;
+  const uint32_t hw = std::max(1u, std::thread::hardware_concurrency());
+  const uint32_t T = std::max(1u, std::min<uint32_t>(hw, nw / 64));
+  run_threads(T, [&](uint32_t t) {
+    for (uint32_t w = (uint32_t)((uint64_t)nw * t / T); w < (uint32_t)((uint64_t)nw * (t + 1) / T); ++w) {
+      const uint32_t b0 = w * window, b1 = std::min(nb, b0 + window);
+      for (uint32_t b = b0; b < b1; ++b) o[b] = b;
+      auto passes = [&](uint32_t b) { return (P.blk_off[b + 1] - P.blk_off[b] + g - 1) / g; };
+      std::stable_sort(o + b0, o + b1, [&](uint32_t a, uint32_t b) { return passes(a) > passes(b); });
+    }
+  });
+}
+
 size_t Plan::device_bytes() const {
   const size_t npose = pose_prob.size(), npt = point_prob.size(), nobs = obs_pose.size();
   size_t b = 0;
@@ -1251,7 +1269,7 @@ size_t Plan::device_bytes() const {
   b += nobs * (4 * 4 + 16 + 32 + 16 + 32);           // point, pose, cam, slot, xy, obs_h, obs_e, obs_p
   b += obs_w.size() * 8 + obs_kind.size() * (1 + 16 + 4);
   b += cam_obs.size() * 8 + (pairs_on_device ? num_pairs : pairs.size()) * 8 + dup_pairs.size() * 8;
-  b += blk_dst.size() * (8 + 4);
+  b += blk_dst.size() * (8 + 4 + 4);
   b += tile_ij.size() * ((size_t)tb * tb * kBlock * 4 + 4 + 2 * (size_t)tb * 6 * 4);
   b += (size_t)num_var_cams * (4 + 4 + 4 + 4 + 36 * 4 + 6 * 4 * 6);
   b += tr_list.size() * 4 + (size_t)num_tile_rows * (4 + 4 + 16 * 8);

@@ -547,6 +547,9 @@ void upload_plan_once(Context* c, uint32_t max_records, const std::function<void
     d.pairs = reinterpret_cast<const uint2*>(st.up(A, P.pairs));
   }
   d.blk_dst = reinterpret_cast<const uint2*>(st.up(A, P.blk_dst));
+  std::vector<uint32_t> blk_order;
+  block_order(P, 256, &blk_order);
+  d.blk_order = st.up(A, blk_order);
   d.diag_dst = st.up(A, P.diag_dst);
   d.dup_off = st.up(A, P.dup_off);
   d.dup_pairs = reinterpret_cast<const uint2*>(st.up(A, P.dup_pairs));
