@@ -20,7 +20,9 @@
 //                 for each column, the lanes that have a term there take
 //                 consecutive places in lane order (a shared bit mask per
 //                 column and the lane's rank in it), so each block receives
-//                 its terms in ascending point order -- the host's order.
+//                 its terms in ascending point order -- the host's order;
+//                 the column's lowest lane then advances its cursor and
+//                 clears its mask.
 //                 Every place is checked against its block's range; a term
 //                 outside it, or a block left short, sets the error flag
 //                 and writes nothing outside the array.
@@ -179,17 +181,17 @@ __global__ void __launch_bounds__(32) k_rows_place(RowsDev r, const uint32_t* bl
         }
       }
       __syncwarp();
-      // Advance each column's cursor by its lanes (the lowest one writes).
+      // Advance each column's cursor by its lanes and clear its mask: the
+      // lowest lane of the column does both (another lane of the column then
+      // reads the full mask or zero, and does nothing either way).
       for (uint32_t b = b0; b < b1; ++b) {
         const uint32_t sb = r.obs_slot[b];
         if (b == a || sb == kNone || sb >= i) continue;
-        const uint32_t m = mask[sb];
-        if ((uint32_t)(__ffs(m) - 1) == lane && cursor[sb] != kNone) cursor[sb] += __popc(m);
-      }
-      __syncwarp();
-      for (uint32_t b = b0; b < b1; ++b) {
-        const uint32_t sb = r.obs_slot[b];
-        if (b != a && sb != kNone && sb < i) mask[sb] = 0u;
+        const uint32_t m = static_cast<volatile uint32_t*>(mask)[sb];
+        if (m != 0u && (uint32_t)(__ffs(m) - 1) == lane) {
+          if (cursor[sb] != kNone) cursor[sb] += __popc(m);
+          atomicExch(&mask[sb], 0u);
+        }
       }
       __syncwarp();
     }

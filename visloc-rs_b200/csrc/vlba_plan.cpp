@@ -444,16 +444,42 @@ void build_plan_serial(const vlba_problem* const* problems, const vlba_config* c
     const uint32_t To = std::max(1u, std::min<uint32_t>(max_threads, no / 200000));
     const uint32_t Ts = std::max(1u, std::min<uint32_t>(To, (uint32_t)((32u << 20) / (nl + 1u))));
     std::vector<uint32_t> cnt(nl + 1, 0);
-    std::vector<uint32_t> order(no);
-    counting_sort(no, nl, Ts, [p](uint32_t o) { return p->obs_landmark[o]; }, 0u, order.data(),
-                  cnt.data());
+    std::vector<uint32_t, NoInit<uint32_t>> order;
+    // Observations listed by landmark already (point-major exports): the
+    // stable sort is the identity, and landmark j starts where the landmark
+    // index first reaches j.
+    std::vector<uint8_t> unsorted(To, 0);
+    const uint32_t* const ol = p->obs_landmark;
+    run_threads(To, [&](uint32_t t) {
+      const uint32_t a = std::max(1u, (uint32_t)((uint64_t)no * t / To)),
+                     e = (uint32_t)((uint64_t)no * (t + 1) / To);
+      for (uint32_t o = a; o < e; ++o)
+        if (ol[o - 1] > ol[o]) {
+          unsorted[t] = 1;
+          return;
+        }
+    });
+    const bool identity = std::find(unsorted.begin(), unsorted.end(), 1) == unsorted.end();
+    if (identity) {
+      run_threads(To, [&](uint32_t t) {
+        const uint32_t a = (uint32_t)((uint64_t)no * t / To), e = (uint32_t)((uint64_t)no * (t + 1) / To);
+        for (uint32_t o = a; o < e; ++o)
+          for (uint32_t j = o ? ol[o - 1] + 1 : 0u; j <= ol[o]; ++j) cnt[j] = o;
+        if (t == To - 1)
+          for (uint32_t j = no ? ol[no - 1] + 1 : 0u; j <= nl; ++j) cnt[j] = no;
+      });
+    } else {
+      order.resize(no);
+      counting_sort(no, nl, Ts, [p](uint32_t o) { return p->obs_landmark[o]; }, 0u, order.data(),
+                    cnt.data());
+    }
     run_threads(To, [&](uint32_t t) {
       for (uint32_t j = (uint32_t)((uint64_t)nl * t / To); j < (uint32_t)((uint64_t)nl * (t + 1) / To); ++j) {
         P.pt_off[point_base + j + 1] = obs_base + cnt[j + 1];
         for (uint32_t k = cnt[j]; k < cnt[j + 1]; ++k) P.obs_point[obs_base + k] = point_base + j;
       }
       for (uint32_t k = (uint32_t)((uint64_t)no * t / To); k < (uint32_t)((uint64_t)no * (t + 1) / To); ++k) {
-        const uint32_t o = order[k];
+        const uint32_t o = identity ? k : order[k];
         const uint32_t g = obs_base + k;
         const uint32_t pose = pose_base + p->obs_pose[o];
         P.obs_pose[g] = pose;
