@@ -193,6 +193,11 @@ struct Context {
   int device = 0;
   int sm_count = 148;
   cudaStream_t stream = nullptr;
+  // The camera-diagonal sums run on `side` beside the off-diagonal assembly
+  // (fork and join events on `stream`; both kernels are latency-bound and
+  // write disjoint blocks).
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
   cudaEvent_t ev[6] = {};
   std::string error;
   Arena arena;
@@ -732,8 +737,13 @@ uint64_t enqueue_iteration(Context* c, cudaEvent_t* ev) {
   check_launch(launch_linearize(d, s), "linearize");
   if (ev) VLBA_CUDA(cudaEventRecord(ev[1], s));
   check_launch(launch_point_prep(d, s), "point prep");
+  // Camera blocks on the side stream beside the off-diagonal blocks.
+  VLBA_CUDA(cudaEventRecord(c->fork, s));
+  VLBA_CUDA(cudaStreamWaitEvent(c->side, c->fork, 0));
+  check_launch(launch_cam_diag(d, c->side), "camera blocks");
+  VLBA_CUDA(cudaEventRecord(c->join, c->side));
   check_launch(launch_offdiag(d, s), "off-diagonal blocks");
-  check_launch(launch_cam_diag(d, s), "camera blocks");
+  VLBA_CUDA(cudaStreamWaitEvent(s, c->join, 0));
   check_launch(launch_pcg_setup(d, s), "pcg setup");
   if (ev) VLBA_CUDA(cudaEventRecord(ev[2], s));
   if (c->gate && d.num_tile_rows) {
@@ -1302,6 +1312,9 @@ Context* make_context(int device) {
   c->pcg_grid_hint = 4 * prop.multiProcessorCount;
   if (const char* f = std::getenv("VLBA_L2_RESIDENT_FRACTION")) c->l2_fraction = std::atof(f);
   VLBA_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  VLBA_CUDA(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
+  VLBA_CUDA(cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming));
+  VLBA_CUDA(cudaEventCreateWithFlags(&c->join, cudaEventDisableTiming));
   for (auto& e : c->ev) VLBA_CUDA(cudaEventCreate(&e));
   return c.release();
 }
@@ -1319,6 +1332,9 @@ void free_context(Context* c) {
   }
   if (c->gnc_sq) cudaFree(c->gnc_sq);
   c->elim.reset();
+  if (c->fork) cudaEventDestroy(c->fork);
+  if (c->join) cudaEventDestroy(c->join);
+  if (c->side) cudaStreamDestroy(c->side);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }
