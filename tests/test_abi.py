@@ -98,6 +98,37 @@ def test_validation_statuses():
     assert check(packed)[0] == _abi.OK
 
 
+def test_validation_of_a_large_problem_reports_the_first_bad_observation():
+    """Past a few hundred thousand observations validation scans them on the
+    host's threads; the error reported is still the serial scan's: the
+    lowest bad observation, its pose checked before its landmark."""
+    n, poses, points = 1_500_000, 50, 200_000
+    rng = np.random.default_rng(5)
+    q = np.tile([1.0, 0.0, 0.0, 0.0], (poses, 1))
+    t = np.zeros((poses, 3))
+    x = rng.normal(size=(points, 3)) + [0.0, 0.0, 10.0]
+    obs_pose = rng.integers(0, poses, n).astype(np.uint32)
+    obs_landmark = rng.integers(0, points, n).astype(np.uint32)
+    xy = rng.normal(size=(n, 2))
+
+    def run(pose, landmark, weight=None):
+        return check(PackedProblem(q, t, x, pose, landmark, xy, [pinhole()], obs_weight=weight))
+
+    assert run(obs_pose, obs_landmark)[0] == _abi.OK
+    op, ol = obs_pose.copy(), obs_landmark.copy()
+    op[1_400_000] = poses + 3
+    ol[900_000] = points + 9
+    assert run(op, ol) == (_abi.ERR_MISSING_LANDMARK, points + 9)
+    op[700_000] = poses + 1
+    assert run(op, ol) == (_abi.ERR_MISSING_POSE, poses + 1)
+    ol[700_000] = points + 2  # same observation: the pose is checked first
+    assert run(op, ol) == (_abi.ERR_MISSING_POSE, poses + 1)
+    w = np.ones(n)
+    w[1_200_000] = -1.0
+    w[300_001] = np.nan
+    assert run(obs_pose, obs_landmark, w) == (_abi.ERR_INVALID_OBSERVATION_WEIGHT, 300_001)
+
+
 @pytest.mark.parametrize("maker", [
     lambda: synth.ring_problem(12, 400, seed=7),
     lambda: synth.ring_problem(50, 5000, seed=1001),

@@ -172,6 +172,36 @@ def test_launch_shapes_do_not_change_results(solver):
         assert a.final_cost == b.final_cost
 
 
+def test_observation_order_does_not_change_the_solve(solver):
+    """Observations listed by landmark skip the plan's counting sort (its
+    stable result is then the identity); listed in another order they go
+    through it.  Both give the same point-major plan, so the solves agree
+    bit for bit."""
+    sorted_ring = synth.ring_problem(120, 40000, seed=46, width=2000, height=1500,
+                                     focal=(1500, 1500), k1=(0.0, 0.0),
+                                     per_camera_intrinsics=False,
+                                     track=("geometric", 8.0, 2, 40))
+    ol = np.asarray(sorted_ring.obs_landmark)
+    assert np.all(np.diff(ol.astype(np.int64)) >= 0)
+    assert sorted_ring.num_observations >= 200_000
+    starts = np.flatnonzero(np.r_[True, ol[1:] != ol[:-1]])
+    ends = np.r_[starts[1:], len(ol)]
+    perm = np.concatenate([np.arange(a, b) for a, b in zip(starts[::-1], ends[::-1])])
+    p = sorted_ring
+    shuffled = PackedProblem(p.pose_q, p.pose_t, p.landmarks, p.obs_pose[perm], p.obs_landmark[perm],
+                             p.obs_xy[perm], p.cameras, p.pose_fixed, p.landmark_fixed,
+                             None if p.obs_camera is None else p.obs_camera[perm])
+    c = cfg(max_iterations=5)
+    a, b = sorted_ring.copy(), shuffled.copy()
+    st, ra = solver.optimize(a, c)
+    assert st == _abi.OK, solver.last_error()
+    st, rb = solver.optimize(b, c)
+    assert st == _abi.OK, solver.last_error()
+    assert ra.final_cost == rb.final_cost
+    assert [i.pcg_iterations for i in ra.iterations] == [i.pcg_iterations for i in rb.iterations]
+    assert same_state(a, b)
+
+
 def test_device_built_terms_equal_the_host_build(solver):
     """A problem of at least 200,000 observations solved alone has its Schur
     terms built on the device; in a batch, the host builds them.  Both lay
