@@ -189,7 +189,7 @@ __global__ void __launch_bounds__(256, 3) k_linearize(Dev d) {
   for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < d.num_obs;
        k += gridDim.x * blockDim.x) {
     const uint32_t l = d.obs_point[k];
-    const uint32_t P = d.point_prob[l];
+    const uint32_t P = d.num_problems == 1 ? 0u : d.point_prob[l];
     const Ctrl& c = d.ctrl[P];
     if (c.done || !c.relinearize) continue;
     const uint32_t cur = c.cur;
@@ -299,7 +299,7 @@ constexpr uint32_t kObsStage = 1024;
 __global__ void __launch_bounds__(256) k_point_prep(Dev d) {
   for (uint32_t l = blockIdx.x * blockDim.x + threadIdx.x; l < d.num_points;
        l += gridDim.x * blockDim.x) {
-    const uint32_t P = d.point_prob[l];
+    const uint32_t P = d.num_problems == 1 ? 0u : d.point_prob[l];
     const Ctrl& c = d.ctrl[P];
     if (c.done) continue;
     const uint32_t cur = c.cur;
@@ -433,16 +433,20 @@ __global__ void __launch_bounds__(256, 2) k_offdiag(Dev d) {
   for (uint32_t wb = warp_global; wb < nwb; wb += warps_total) {
     const uint32_t q = wb * kPerWarp + (threadIdx.x % 32) / G;
     bool valid = q < d.num_offdiag_blocks;
-    uint2 dst = make_uint2(kNone, kNone);
+    uint2 dst = make_uint2(kNone, kNone), pr = make_uint2(0u, 0u);
     uint32_t c0 = 0, c1 = 0;
     if (valid) {
+      // The block's range and first pair go out beside its problem's status
+      // (a single problem's is the same for every block): the pair loads do
+      // not wait for the lookup of the problem.
       const uint32_t b = d.blk_order[q];
       dst = d.blk_dst[b];
-      const uint32_t tile = dst.x / tile_floats;
-      const uint32_t I = d.tile_ij[tile] >> 16;
-      valid = !d.ctrl[d.tr_prob[I]].done;
       c0 = d.blk_off[b];
       c1 = d.blk_off[b + 1];
+      if (c0 + lane < c1) pr = d.pairs[c0 + lane];
+      const uint32_t P =
+          d.num_problems == 1 ? 0u : d.tr_prob[d.tile_ij[dst.x / tile_floats] >> 16];
+      valid = !d.ctrl[P].done;
     }
     float acc[36], cmp[36];
 #pragma unroll
@@ -451,7 +455,6 @@ __global__ void __launch_bounds__(256, 2) k_offdiag(Dev d) {
       cmp[e] = 0.0f;
     }
     if (valid && c0 + lane < c1) {
-      uint2 pr = d.pairs[c0 + lane];
       for (uint32_t cidx = c0 + lane; cidx < c1; cidx += G) {
         float4 a0, a1, p0, p1, b0, b1;
         ld8(d.obs_h + 2 * (size_t)pr.x, a0, a1);
@@ -632,7 +635,7 @@ __global__ void __launch_bounds__(kDiagThreads) k_cam_diag(Dev d) {
   __shared__ int s_fail;
   const uint32_t t = threadIdx.x;
   for (uint32_t s = blockIdx.x; s < d.num_var_cams; s += gridDim.x) {
-    const uint32_t P = d.slot_prob[s];
+    const uint32_t P = d.num_problems == 1 ? 0u : d.slot_prob[s];
     if (d.ctrl[P].done) continue;
     const uint32_t o0 = d.cam_off[s], o1 = d.cam_off[s + 1];
     double acc[kDiagAcc];
@@ -834,7 +837,7 @@ __global__ void __launch_bounds__(256) k_cost(Dev d) {
   __shared__ unsigned char sAct[TRIAL ? 256 : 1];     // point takes a step
   for (uint32_t ch = blockIdx.x; ch < d.num_point_chunks; ch += gridDim.x) {
     const uint32_t lo = d.chunk_point_begin[ch], hi = d.chunk_point_begin[ch + 1];
-    const uint32_t P = d.point_prob[lo];
+    const uint32_t P = d.num_problems == 1 ? 0u : d.point_prob[lo];
     const Ctrl& c = d.ctrl[P];
     if (c.done) continue;  // uniform: a chunk lies inside one problem
     const uint32_t cur = c.cur;
