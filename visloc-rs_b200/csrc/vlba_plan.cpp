@@ -1,6 +1,8 @@
 // vlba_plan.cpp -- see vlba_plan.h.
 #include "vlba_plan.h"
 
+#include <cuda_runtime.h>
+
 #include <sys/mman.h>
 
 #include <algorithm>
@@ -9,9 +11,50 @@
 #include <atomic>
 #include <exception>
 #include <stdexcept>
+#include <map>
+#include <mutex>
 #include <thread>
 
 namespace vlba {
+
+namespace {
+thread_local int t_pin_depth = 0;
+std::mutex g_pin_mu;
+std::map<uintptr_t, size_t> g_pinned;  // base -> bytes of page-locked allocations
+}  // namespace
+
+PinScope::PinScope() { ++t_pin_depth; }
+PinScope::~PinScope() { --t_pin_depth; }
+bool pin_requested() { return t_pin_depth > 0; }
+
+void pin_allocation(void* p, size_t bytes) {
+  if (cudaHostRegister(p, bytes, cudaHostRegisterDefault) != cudaSuccess) {
+    (void)cudaGetLastError();  // stays pageable: the upload stages it
+    return;
+  }
+  std::lock_guard<std::mutex> lock(g_pin_mu);
+  g_pinned[(uintptr_t)p] = bytes;
+}
+
+void unpin_allocation(void* p) {
+  {
+    std::lock_guard<std::mutex> lock(g_pin_mu);
+    auto it = g_pinned.find((uintptr_t)p);
+    if (it == g_pinned.end()) return;
+    g_pinned.erase(it);
+  }
+  cudaHostUnregister(p);
+  (void)cudaGetLastError();
+}
+
+bool pinned_range(const void* p, size_t bytes) {
+  std::lock_guard<std::mutex> lock(g_pin_mu);
+  if (g_pinned.empty()) return false;
+  auto it = g_pinned.upper_bound((uintptr_t)p);
+  if (it == g_pinned.begin()) return false;
+  --it;
+  return (uintptr_t)p + bytes <= it->first + it->second;
+}
 
 void advise_huge_pages(void* p, size_t bytes) {
   constexpr uintptr_t kHuge = 2u << 20;

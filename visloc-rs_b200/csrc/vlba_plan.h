@@ -26,10 +26,26 @@ struct PairIdx {
 // TLB-bound.  A hint only.
 void advise_huge_pages(void* p, size_t bytes);
 
+// Page-locking of the large plan arrays an upload copies, so that the copies
+// go from them straight to the device instead of through staging buffers.
+// While a PinScope is alive on a thread, the arrays of 8 MB or more that it
+// allocates are page-locked (where the device allows it; else they stay
+// pageable) until they are freed; a plan rebuilt in place keeps them.
+struct PinScope {
+  PinScope();
+  ~PinScope();
+};
+bool pin_requested();
+void pin_allocation(void* p, size_t bytes);
+void unpin_allocation(void* p);
+// [p, p + bytes) lies inside one page-locked allocation.
+bool pinned_range(const void* p, size_t bytes);
+
 // Allocator whose resize() leaves new elements uninitialised, for the large
 // pair arrays that the builder sizes first and then writes in full (from
 // several threads, which then also take the page faults).  Allocations of 8 MB
-// or more are advised huge pages before their first touch.
+// or more are advised huge pages before their first touch, and page-locked
+// inside a PinScope.
 template <typename T>
 struct NoInit : std::allocator<T> {
   template <typename U>
@@ -41,8 +57,15 @@ struct NoInit : std::allocator<T> {
   NoInit(const NoInit<U>&) noexcept {}
   T* allocate(size_t n) {
     T* p = std::allocator<T>::allocate(n);
-    if (n * sizeof(T) >= (8u << 20)) advise_huge_pages(p, n * sizeof(T));
+    if (n * sizeof(T) >= (8u << 20)) {
+      advise_huge_pages(p, n * sizeof(T));
+      if (pin_requested()) pin_allocation(p, n * sizeof(T));
+    }
     return p;
+  }
+  void deallocate(T* p, size_t n) {
+    if (n * sizeof(T) >= (8u << 20)) unpin_allocation(p);
+    std::allocator<T>::deallocate(p, n);
   }
   template <typename U>
   void construct(U* p) noexcept {

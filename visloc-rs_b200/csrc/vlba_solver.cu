@@ -388,9 +388,16 @@ class Stager {
     return p;
   }
   void add(void* dst, const void* src, size_t bytes) {
-    if (bytes) items_.push_back(Item{static_cast<char*>(dst), static_cast<const char*>(src), bytes});
+    if (!bytes) return;
+    const Item it{static_cast<char*>(dst), static_cast<const char*>(src), bytes};
+    // Page-locked plan arrays go straight to the device.
+    if (pinned_range(src, bytes)) direct_.push_back(it);
+    else items_.push_back(it);
   }
   void flush(cudaStream_t s) {
+    for (const Item& it : direct_)
+      VLBA_CUDA(cudaMemcpyAsync(it.dst, it.src, it.bytes, cudaMemcpyHostToDevice, s));
+    direct_.clear();
     size_t total = 0;
     for (const Item& it : items_) total += it.bytes;
     if (total == 0) return;
@@ -442,7 +449,7 @@ class Stager {
     size_t bytes;
   };
   Context* c_;
-  std::vector<Item> items_;
+  std::vector<Item> items_, direct_;
 };
 
 // Upload a built plan: allocate and fill every device array of Dev.
@@ -1180,8 +1187,14 @@ void do_upload(Context* c, const vlba_problem* const* probs, const vlba_config* 
   };
   const bool large = n == 1 && probs[0]->num_observations >= kDeviceTermsMinObs;
   const auto tb0 = std::chrono::steady_clock::now();
-  build_plan(probs, cfgs, n, (uint32_t)pick_tb(probs, n), &c->plan, 0,
-             large ? &device_rows : nullptr);
+  {
+    // A large problem's plan arrays are page-locked when first allocated
+    // (a context's plan keeps them for the next upload), so they are copied
+    // to the device without staging.
+    std::unique_ptr<PinScope> pin(large ? new PinScope() : nullptr);
+    build_plan(probs, cfgs, n, (uint32_t)pick_tb(probs, n), &c->plan, 0,
+               large ? &device_rows : nullptr);
+  }
   const double t_build = ms_since(tb0);
   // The plan check runs on its own thread while the arrays are copied, and
   // ends before the first kernel reads them.
