@@ -385,6 +385,7 @@ void build_plan_serial(const vlba_problem* const* problems, const vlba_config* c
     keep(P.pairs, old.pairs);
     keep(P.dup_pairs, old.dup_pairs);
     keep(P.scratch, old.scratch);
+    keep(P.points, old.points);
     keep(P.obs_point, old.obs_point);
     keep(P.obs_pose, old.obs_pose);
     keep(P.obs_cam, old.obs_cam);
@@ -487,7 +488,7 @@ void build_plan_serial(const vlba_problem* const* problems, const vlba_config* c
     const uint32_t To = std::max(1u, std::min<uint32_t>(max_threads, no / 200000));
     const uint32_t Ts = std::max(1u, std::min<uint32_t>(To, (uint32_t)((32u << 20) / (nl + 1u))));
     std::vector<uint32_t> cnt(nl + 1, 0);
-    std::vector<uint32_t, NoInit<uint32_t>> order;
+    std::unique_ptr<uint32_t[]> order;  // uninitialised, never page-locked
     // Observations listed by landmark already (point-major exports): the
     // stable sort is the identity, and landmark j starts where the landmark
     // index first reaches j.
@@ -512,8 +513,8 @@ void build_plan_serial(const vlba_problem* const* problems, const vlba_config* c
           for (uint32_t j = no ? ol[no - 1] + 1 : 0u; j <= nl; ++j) cnt[j] = no;
       });
     } else {
-      order.resize(no);
-      counting_sort(no, nl, Ts, [p](uint32_t o) { return p->obs_landmark[o]; }, 0u, order.data(),
+      order.reset(new uint32_t[no]);
+      counting_sort(no, nl, Ts, [p](uint32_t o) { return p->obs_landmark[o]; }, 0u, order.get(),
                     cnt.data());
     }
     run_threads(To, [&](uint32_t t) {
@@ -1205,7 +1206,7 @@ void build_plan(const vlba_problem* const* problems, const vlba_config* const* c
 template <typename F>
 bool all_of_range(uint64_t n, F&& pred) {
   const uint64_t hw = std::max(1u, std::thread::hardware_concurrency());
-  const uint32_t T = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(hw, n >> 20));
+  const uint32_t T = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(hw, n >> 16));
   std::atomic<bool> ok{true};
   run_threads(T, [&](uint32_t t) {
     for (uint64_t i = n * t / T, e = n * (t + 1) / T; i < e; ++i)
@@ -1246,8 +1247,8 @@ std::string check_plan(const Plan& P) {
   for (uint64_t i = 0; i < nposes; ++i)
     if (P.pose_slot[i] != kNone && P.pose_slot[i] >= nslots) return bad("pose_slot");
   if (P.cam_off.size() != nslots + 1 || P.cam_off.back() != P.cam_obs.size()) return bad("cam_off");
-  for (uint64_t s = 0; s < nslots; ++s)
-    if (P.cam_off[s] > P.cam_off[s + 1]) return bad("cam_off order");
+  if (!all_of_range(nslots, [&](uint64_t s) { return P.cam_off[s] <= P.cam_off[s + 1]; }))
+    return bad("cam_off order");
   if (!all_of_range(P.cam_obs.size(), [&](uint64_t q) { return P.cam_obs[q] < nobs; }))
     return bad("cam_obs");
   if (P.slot_prob.size() != nslots || nslots != (uint64_t)P.num_tile_rows * P.tb)
@@ -1255,27 +1256,32 @@ std::string check_plan(const Plan& P) {
   const uint64_t npairs = P.pairs_on_device ? P.num_pairs : P.pairs.size();
   if (P.blk_off.size() != P.blk_dst.size() + 1 || P.blk_off.back() != npairs)
     return bad("blk_off");
-  for (size_t b = 0; b + 1 < P.blk_off.size(); ++b)
-    if (P.blk_off[b] > P.blk_off[b + 1]) return bad("blk_off order");
+  if (!all_of_range(P.blk_off.size() - 1, [&](uint64_t b) { return P.blk_off[b] <= P.blk_off[b + 1]; }))
+    return bad("blk_off order");
   // Terms built on the device are checked there, against the same ranges,
   // before any kernel reads them.
   if (P.pairs_on_device) {
     if (!P.pairs.empty() || P.num_problems != 1 || P.blk_col.size() != P.blk_dst.size() ||
         P.row_blk.size() != (size_t)P.num_var_cams + 1 || P.row_blk.back() != P.blk_col.size())
       return bad("device terms");
-    for (size_t i = 0; i + 1 < P.row_blk.size(); ++i) {
-      if (P.row_blk[i] > P.row_blk[i + 1]) return bad("row_blk order");
-      for (uint32_t b = P.row_blk[i]; b < P.row_blk[i + 1]; ++b)
-        if (P.blk_col[b] >= i || (b > P.row_blk[i] && P.blk_col[b] <= P.blk_col[b - 1]))
-          return bad("blk_col");
-    }
+    if (!all_of_range(P.row_blk.size() - 1, [&](uint64_t i) { return P.row_blk[i] <= P.row_blk[i + 1]; }))
+      return bad("row_blk order");
+    if (!all_of_range(P.row_blk.size() - 1, [&](uint64_t i) {
+          for (uint32_t b = P.row_blk[i]; b < P.row_blk[i + 1]; ++b)
+            if (P.blk_col[b] >= i || (b > P.row_blk[i] && P.blk_col[b] <= P.blk_col[b - 1]))
+              return false;
+          return true;
+        }))
+      return bad("blk_col");
   }
   if (!all_of_range(P.pairs.size(), [&](uint64_t q) { return P.pairs[q].a < nobs && P.pairs[q].b < nobs; }))
     return bad("pairs");
-  for (const PairIdx& d : P.blk_dst) {
-    if ((uint64_t)d.a + kBlock > ntiles * tile_floats) return bad("blk_dst");
-    if (d.b != kNone && (uint64_t)d.b + kBlock > ntiles * tile_floats) return bad("blk_dst mirror");
-  }
+  if (!all_of_range(P.blk_dst.size(), [&](uint64_t b) {
+        const PairIdx& d = P.blk_dst[b];
+        return (uint64_t)d.a + kBlock <= ntiles * tile_floats &&
+               (d.b == kNone || (uint64_t)d.b + kBlock <= ntiles * tile_floats);
+      }))
+    return bad("blk_dst");
   if (P.diag_dst.size() != nslots) return bad("diag_dst size");
   for (uint32_t d : P.diag_dst)
     if ((uint64_t)d + kBlock > ntiles * tile_floats) return bad("diag_dst");

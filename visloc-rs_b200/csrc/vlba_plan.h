@@ -88,7 +88,7 @@ struct Plan {
   std::vector<uint32_t> pose_prob, point_prob, slot_prob;
   std::vector<LmParams> params;
 
-  std::vector<double> pose_q, pose_t, points;
+  std::vector<double> pose_q, pose_t;
   std::vector<uint32_t> pose_slot;
   std::vector<uint8_t> point_var;
   std::vector<DevCamera> cameras;
@@ -98,6 +98,7 @@ struct Plan {
   template <typename T>
   using ObsArray = std::vector<T, NoInit<T>>;
   std::vector<uint32_t> pt_off;
+  ObsArray<double> points;  // 3 per landmark
   ObsArray<uint32_t> obs_point, obs_pose, obs_cam, obs_slot;
   ObsArray<double> obs_xy;  // 2 per obs
   // External weight per observation; empty when no problem of the plan has

@@ -248,6 +248,9 @@ struct Context {
   // there instead of from the host again.
   size_t rows_in_at[6] = {0, 0, 0, 0, 0, 0};
   uint64_t last_upload_bytes = 0;
+  // Host milliseconds of the last upload's device-side steps (for the
+  // VLBA_TRACE_UPLOAD line): array copies issued, then the device terms.
+  double up_copy_ms = 0.0, up_terms_ms = 0.0, up_flush_ms = 0.0;
 };
 
 namespace {
@@ -467,6 +470,7 @@ void upload_plan_once(Context* c, uint32_t max_records, const std::function<void
   c->uploaded = false;
   Dev d;
   std::memset(&d, 0, sizeof d);
+  const auto u0 = std::chrono::steady_clock::now();
   const size_t npose = P.pose_prob.size(), npt = P.point_prob.size(), nobs = P.obs_pose.size();
   d.num_problems = P.num_problems;
   d.num_poses = (uint32_t)npose;
@@ -595,8 +599,12 @@ void upload_plan_once(Context* c, uint32_t max_records, const std::function<void
   d.chunk_cost = A.alloc<double>(nch);
   d.chunk_bad = A.alloc<unsigned long long>(nch);
   d.chunk_step = A.alloc<double>(nch);
+  const auto uf = std::chrono::steady_clock::now();
   st.flush(s);
   c->dev = d;
+  const auto u1 = std::chrono::steady_clock::now();
+  c->up_flush_ms = std::chrono::duration<double, std::milli>(u1 - uf).count();
+  c->up_copy_ms = std::chrono::duration<double, std::milli>(u1 - u0).count();
   if (before_kernels) before_kernels();
   check_launch(launch_cam_points(d, (uint32_t)P.cam_obs.size(), s), "camera lists");
   if (P.pairs_on_device) {
@@ -620,6 +628,8 @@ void upload_plan_once(Context* c, uint32_t max_records, const std::function<void
     VLBA_CUDA(cudaStreamSynchronize(s));
     if (flags) throw std::runtime_error("device Schur terms do not match the plan's blocks");
   }
+  c->up_terms_ms =
+      std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - u1).count();
   // Co-resident grid, but no more blocks than tiles or tile rows to work on
   // (fewer blocks make the grid barriers cheaper on small systems).
   c->pcg_grid = P.num_tile_rows ? pcg_grid_size((int)P.tb, c->sm_count) : 0;
@@ -1225,9 +1235,10 @@ void do_upload(Context* c, const vlba_problem* const* probs, const vlba_config* 
   if (trace)
     std::fprintf(stderr,
                  "vlba upload: validate %.2f ms, plan %.2f ms (device row counts %.2f ms), "
-                 "copy, check and device terms %.2f ms (check %.2f ms beside the copies, "
-                 "%.2f ms waited)\n",
-                 t_validate, t_build, t_rows, ms_since(tu0), t_check, t_wait);
+                 "copy, check and device terms %.2f ms (arrays issued %.2f ms, of it staged copies "
+                 "%.2f ms; check %.2f ms beside them, %.2f ms waited; device terms %.2f ms)\n",
+                 t_validate, t_build, t_rows, ms_since(tu0), c->up_copy_ms, c->up_flush_ms, t_check,
+                 t_wait, c->up_terms_ms);
   c->num_poses.clear();
   c->num_points.clear();
   for (uint32_t i = 0; i < n; ++i) {
