@@ -144,10 +144,12 @@ struct RowsDev {
 // lists by the prefix of their lengths (row_blk).
 cudaError_t launch_rows_count(const RowsDev& r, cudaStream_t s);
 // Write every term at its place: per block in point order (the host order).
+// max_row_blocks: the most blocks of any row (sizes the per-row state).
 cudaError_t launch_rows_place(const RowsDev& r, const uint32_t* blk_off, const uint32_t* row_blk,
-                              const uint32_t* blk_col, uint2* pairs, cudaStream_t s);
+                              const uint32_t* blk_col, uint32_t max_row_blocks, uint2* pairs,
+                              cudaStream_t s);
 size_t rows_count_smem(uint32_t nvar);
-size_t rows_place_smem(uint32_t nvar);
+size_t rows_place_smem(uint32_t nvar, uint32_t max_row_blocks);
 
 // Occupancy-derived grid of the persistent PCG kernel (0 if it cannot run).
 int pcg_grid_size(int tb, int sm_count);

@@ -17,9 +17,10 @@
 //   k_rows_pack   the rows' lists, packed by the prefix of their lengths.
 //   k_rows_place  one warp per camera row: the row's observations in groups
 //                 of 32 consecutive ones (32 distinct points, ascending);
-//                 for each column, the lanes that have a term there take
+//                 for each of the row's blocks (found from the column by a
+//                 shared map), the lanes that have a term there take
 //                 consecutive places in lane order (a shared bit mask per
-//                 column and the lane's rank in it), so each block receives
+//                 block and the lane's rank in it), so each block receives
 //                 its terms in ascending point order -- the host's order;
 //                 the column's lowest lane then advances its cursor and
 //                 clears its mask.
@@ -126,30 +127,38 @@ __global__ void __launch_bounds__(256) k_rows_pack(RowsDev r) {
   }
 }
 
-// One warp per row; shared memory per warp: the column cursors, the ends of
-// their blocks and the lane masks of the current group.
+// One warp per row.  Shared memory per warp: a map from column slot to the
+// row's block (0xFFFF: no block of this row), then per block of the row its
+// cursor, its end and the lane mask of the current group -- sized by the
+// longest row's block count rather than by the slot count, so that many
+// warps fit on an SM when rows have few blocks.
+constexpr uint16_t kNoBlock = 0xFFFFu;
+
 __global__ void __launch_bounds__(32) k_rows_place(RowsDev r, const uint32_t* blk_off,
                                                    const uint32_t* row_blk, const uint32_t* blk_col,
-                                                   uint2* pairs) {
+                                                   uint32_t max_row_blocks, uint2* pairs) {
   extern __shared__ uint32_t sm[];
-  uint32_t* cursor = sm;              // [nvar]
-  uint32_t* end = sm + r.nvar;        // [nvar]
-  uint32_t* mask = sm + 2 * r.nvar;   // [nvar]
+  uint16_t* colmap = reinterpret_cast<uint16_t*>(sm);           // [nvar]
+  uint32_t* cursor = sm + (r.nvar + 1) / 2;                     // [max_row_blocks]
+  uint32_t* end = cursor + max_row_blocks;                      // [max_row_blocks]
+  uint32_t* mask = end + max_row_blocks;                        // [max_row_blocks]
   const uint32_t lane = threadIdx.x;
   const uint32_t lt = (1u << lane) - 1u;
+  for (uint32_t j = lane; j < r.nvar; j += 32) colmap[j] = kNoBlock;
+  __syncwarp();
   for (uint32_t i = blockIdx.x; i < r.nvar; i += gridDim.x) {
-    for (uint32_t j = lane; j < r.nvar; j += 32) {
-      cursor[j] = kNone;
-      end[j] = 0u;
-      mask[j] = 0u;
+    const uint32_t rb0 = row_blk[i], rb1 = row_blk[i + 1];
+    bool bad = rb1 - rb0 > max_row_blocks;
+    const uint32_t nb = bad ? 0u : rb1 - rb0;
+    for (uint32_t q = lane; q < nb; q += 32) {
+      const uint32_t col = blk_col[rb0 + q];
+      if (col < i) colmap[col] = (uint16_t)q;
+      else bad = true;
+      cursor[q] = blk_off[rb0 + q];
+      end[q] = blk_off[rb0 + q + 1];
+      mask[q] = 0u;
     }
     __syncwarp();
-    for (uint32_t b = row_blk[i] + lane; b < row_blk[i + 1]; b += 32) {
-      cursor[blk_col[b]] = blk_off[b];
-      end[blk_col[b]] = blk_off[b + 1];
-    }
-    __syncwarp();
-    bool bad = false;
     const uint32_t q0 = r.cam_off[i], q1 = r.cam_off[i + 1];
     for (uint32_t g = q0; g < q1; g += 32) {
       const uint32_t q = g + lane;
@@ -162,42 +171,49 @@ __global__ void __launch_bounds__(32) k_rows_place(RowsDev r, const uint32_t* bl
           b1 = r.pt_off[p + 1];
         }
       }
-      // Mark: this lane has a term in each column of its point's other slots.
-      for (uint32_t b = b0; b < b1; ++b) {
-        const uint32_t sb = r.obs_slot[b];
-        if (b != a && sb != kNone && sb < i) atomicOr(&mask[sb], 1u << lane);
-      }
-      __syncwarp();
-      // Place: the lanes of a column in lane order from its cursor.
+      // Mark: this lane has a term in the block of each of its point's other
+      // slots below this row.
       for (uint32_t b = b0; b < b1; ++b) {
         const uint32_t sb = r.obs_slot[b];
         if (b == a || sb == kNone || sb >= i) continue;
-        const uint32_t c = cursor[sb];
-        const uint32_t at = c + __popc(mask[sb] & lt);
-        if (c == kNone || at >= end[sb]) {
-          bad = true;
-        } else {
-          pairs[at] = make_uint2(a, b);
-        }
+        const uint32_t lb = colmap[sb];
+        if (lb == kNoBlock) bad = true;  // a term outside the row's blocks
+        else atomicOr(&mask[lb], 1u << lane);
       }
       __syncwarp();
-      // Advance each column's cursor by its lanes and clear its mask: the
-      // lowest lane of the column does both (another lane of the column then
+      // Place: the lanes of a block in lane order from its cursor.
+      for (uint32_t b = b0; b < b1; ++b) {
+        const uint32_t sb = r.obs_slot[b];
+        if (b == a || sb == kNone || sb >= i) continue;
+        const uint32_t lb = colmap[sb];
+        if (lb == kNoBlock) continue;
+        const uint32_t at = cursor[lb] + __popc(mask[lb] & lt);
+        if (at >= end[lb]) bad = true;
+        else pairs[at] = make_uint2(a, b);
+      }
+      __syncwarp();
+      // Advance each block's cursor by its lanes and clear its mask: the
+      // lowest lane of the block does both (another lane of the block then
       // reads the full mask or zero, and does nothing either way).
       for (uint32_t b = b0; b < b1; ++b) {
         const uint32_t sb = r.obs_slot[b];
         if (b == a || sb == kNone || sb >= i) continue;
-        const uint32_t m = static_cast<volatile uint32_t*>(mask)[sb];
+        const uint32_t lb = colmap[sb];
+        if (lb == kNoBlock) continue;
+        const uint32_t m = static_cast<volatile uint32_t*>(mask)[lb];
         if (m != 0u && (uint32_t)(__ffs(m) - 1) == lane) {
-          if (cursor[sb] != kNone) cursor[sb] += __popc(m);
-          atomicExch(&mask[sb], 0u);
+          cursor[lb] += __popc(m);
+          atomicExch(&mask[lb], 0u);
         }
       }
       __syncwarp();
     }
-    // Every block of the row filled exactly.
-    for (uint32_t b = row_blk[i] + lane; b < row_blk[i + 1]; b += 32)
-      if (cursor[blk_col[b]] != blk_off[b + 1]) bad = true;
+    // Every block of the row filled exactly; the map back to empty.
+    for (uint32_t q = lane; q < nb; q += 32) {
+      if (cursor[q] != end[q]) bad = true;
+      const uint32_t col = blk_col[rb0 + q];
+      if (col < i) colmap[col] = kNoBlock;
+    }
     if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(r.flags, 2u);
     __syncwarp();
   }
@@ -206,7 +222,9 @@ __global__ void __launch_bounds__(32) k_rows_place(RowsDev r, const uint32_t* bl
 }  // namespace
 
 size_t rows_count_smem(uint32_t nvar) { return (size_t)nvar * 4; }
-size_t rows_place_smem(uint32_t nvar) { return (size_t)nvar * 12; }
+size_t rows_place_smem(uint32_t nvar, uint32_t max_row_blocks) {
+  return (size_t)(nvar + 1) / 2 * 4 + (size_t)max_row_blocks * 12;
+}
 
 cudaError_t launch_rows_count(const RowsDev& r, cudaStream_t s) {
   const size_t sm = rows_count_smem(r.nvar);
@@ -225,13 +243,14 @@ cudaError_t launch_rows_count(const RowsDev& r, cudaStream_t s) {
 }
 
 cudaError_t launch_rows_place(const RowsDev& r, const uint32_t* blk_off, const uint32_t* row_blk,
-                              const uint32_t* blk_col, uint2* pairs, cudaStream_t s) {
-  const size_t sm = rows_place_smem(r.nvar);
+                              const uint32_t* blk_col, uint32_t max_row_blocks, uint2* pairs,
+                              cudaStream_t s) {
+  const size_t sm = rows_place_smem(r.nvar, max_row_blocks);
   cudaError_t e = cudaFuncSetAttribute(k_rows_place, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)sm);
   if (e != cudaSuccess) return e;
   const int g = (int)(r.nvar < 148u * 64u ? r.nvar : 148u * 64u);
-  k_rows_place<<<g, 32, sm, s>>>(r, blk_off, row_blk, blk_col, pairs);
+  k_rows_place<<<g, 32, sm, s>>>(r, blk_off, row_blk, blk_col, max_row_blocks, pairs);
   return cudaGetLastError();
 }
 

@@ -621,7 +621,10 @@ void upload_plan_once(Context* c, uint32_t max_records, const std::function<void
     c->rows_out.ensure(16);
     r.flags = c->rows_out.as<uint32_t>();
     VLBA_CUDA(cudaMemsetAsync(r.flags, 0, 4, s));
-    check_launch(launch_rows_place(r, d.blk_off, dev_row_blk, dev_blk_col, dev_pairs, s),
+    uint32_t max_row_blocks = 0;
+    for (uint32_t i = 0; i < r.nvar; ++i)
+      max_row_blocks = std::max(max_row_blocks, P.row_blk[i + 1] - P.row_blk[i]);
+    check_launch(launch_rows_place(r, d.blk_off, dev_row_blk, dev_blk_col, max_row_blocks, dev_pairs, s),
                  "Schur terms");
     uint32_t flags = 0;
     VLBA_CUDA(cudaMemcpyAsync(&flags, r.flags, 4, cudaMemcpyDeviceToHost, s));
@@ -1103,6 +1106,8 @@ std::vector<Validation> validate_all(const vlba_problem* const* probs,
 constexpr uint64_t kDeviceTermsMinObs = 200000;
 // Rows the device builders take (their shared memory holds 12 bytes per row).
 constexpr uint32_t kDeviceTermsMaxRows = 16384;
+// Dynamic shared memory one block may use on sm_100.
+constexpr size_t kMaxDynamicSmem = 227u * 1024u;
 
 // The block structure of the plan's single problem from the device: uploads
 // what the row counts read (point-major order, per-slot lists), counts and
@@ -1159,6 +1164,12 @@ bool device_row_blocks(Context* c, const Plan& P, uint32_t nvar, RowBlocks* out)
   if (flags & 1u) return false;
   const size_t nb = out->row_off[nvar];
   if (nb > ntri) throw std::runtime_error("device Schur term counts out of range");
+  // The placement keeps per-row state for the longest row's blocks in
+  // shared memory; a system whose rows do not fit is laid out on the host.
+  uint32_t max_row_blocks = 0;
+  for (uint32_t i = 0; i < nvar; ++i)
+    max_row_blocks = std::max(max_row_blocks, out->row_off[i + 1] - out->row_off[i]);
+  if (rows_place_smem(nvar, max_row_blocks) > kMaxDynamicSmem) return false;
   out->col.resize(nb);
   out->count.resize(nb);
   VLBA_CUDA(cudaMemcpyAsync(out->col.data(), r.col, 4 * nb, cudaMemcpyDeviceToHost, s));
