@@ -2140,6 +2140,29 @@ __global__ void k_wait_probe(const unsigned int* flag, unsigned long long limit_
 }
 
 // Current state (buffer Ctrl::cur) of every problem into buffer 0.
+// The off-diagonal assembly's block order: each window of 256 blocks in plan
+// order sorted by the loop passes its blocks take at g lanes, longest first,
+// ties in plan order (a block's rank is the count of blocks of its window
+// before it in that order).
+__global__ void __launch_bounds__(256) k_block_order(const uint32_t* blk_off, uint32_t nb,
+                                                     uint32_t g, uint32_t* order) {
+  __shared__ uint32_t key[256];
+  const uint32_t b0 = blockIdx.x * 256u, t = threadIdx.x;
+  const uint32_t n = min(256u, nb - b0);
+  uint32_t k = 0;
+  if (t < n) k = (blk_off[b0 + t + 1] - blk_off[b0 + t] + g - 1) / g;
+  key[t] = k;
+  __syncthreads();
+  if (t < n) {
+    uint32_t rank = 0;
+    for (uint32_t j = 0; j < n; ++j) {
+      const uint32_t kj = key[j];
+      rank += (kj > k || (kj == k && j < t)) ? 1u : 0u;
+    }
+    order[b0 + rank] = b0 + t;
+  }
+}
+
 // The point of every listed observation, beside the per-slot lists (read
 // by the camera-diagonal sums with the observation index, both coalesced).
 __global__ void __launch_bounds__(256) k_cam_points(Dev d, uint32_t n) {
@@ -2318,6 +2341,13 @@ __global__ void __launch_bounds__(256) k_sq_residuals(Dev d, double* out) {
 
 cudaError_t launch_sq_residuals(const Dev& d, double* out, cudaStream_t s) {
   k_sq_residuals<<<grid1d(d.num_obs, 256), 256, 0, s>>>(d, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_block_order(const Dev& d, cudaStream_t s) {
+  if (d.num_offdiag_blocks == 0) return cudaSuccess;
+  k_block_order<<<(d.num_offdiag_blocks + 255) / 256, 256, 0, s>>>(
+      d.blk_off, d.num_offdiag_blocks, d.group, const_cast<uint32_t*>(d.blk_order));
   return cudaGetLastError();
 }
 

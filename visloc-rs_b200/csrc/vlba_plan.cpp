@@ -474,13 +474,25 @@ void build_plan_serial(const vlba_problem* const* problems, const vlba_config* c
     P.real_var_cams += nvar;
     const uint32_t nslots = round_up(nvar, tb);
     for (uint32_t s = 0; s < nslots; ++s) P.slot_prob.push_back(pi);
-    for (uint32_t j = 0; j < nl; ++j) {
-      const uint32_t g = point_base + j;
-      for (int a = 0; a < 3; ++a) P.points[3 * (size_t)g + a] = p->landmarks[3 * (size_t)j + a];
-      P.point_prob[g] = pi;
-      const bool var = !(p->landmark_fixed && p->landmark_fixed[j]);
-      P.point_var[g] = var ? 1 : 0;
-      if (var) ++P.var_points;
+    {
+      const uint32_t Tp = std::max(1u, std::min<uint32_t>(max_threads, nl / 100000));
+      std::vector<uint64_t> nvp(Tp, 0);
+      run_threads(Tp, [&](uint32_t t) {
+        double* const pts = P.points.data();
+        uint32_t* const pprob = P.point_prob.data();
+        uint8_t* const pvar = P.point_var.data();
+        uint64_t nv = 0;
+        for (uint32_t j = (uint32_t)((uint64_t)nl * t / Tp); j < (uint32_t)((uint64_t)nl * (t + 1) / Tp); ++j) {
+          const uint32_t g = point_base + j;
+          for (int a = 0; a < 3; ++a) pts[3 * (size_t)g + a] = p->landmarks[3 * (size_t)j + a];
+          pprob[g] = pi;
+          const bool var = !(p->landmark_fixed && p->landmark_fixed[j]);
+          pvar[g] = var ? 1 : 0;
+          nv += var;
+        }
+        nvp[t] = nv;
+      });
+      for (uint32_t t = 0; t < Tp; ++t) P.var_points += nvp[t];
     }
     // Point-major observation order: stable counting sort by landmark.
     // Observation-level passes run on up to max_threads threads (the
@@ -517,19 +529,31 @@ void build_plan_serial(const vlba_problem* const* problems, const vlba_config* c
       counting_sort(no, nl, Ts, [p](uint32_t o) { return p->obs_landmark[o]; }, 0u, order.get(),
                     cnt.data());
     }
+    // Observations with a variable point and a variable pose, per thread.
+    std::vector<uint64_t> nvo(To, 0);
     run_threads(To, [&](uint32_t t) {
       for (uint32_t j = (uint32_t)((uint64_t)nl * t / To); j < (uint32_t)((uint64_t)nl * (t + 1) / To); ++j) {
         P.pt_off[point_base + j + 1] = obs_base + cnt[j + 1];
         for (uint32_t k = cnt[j]; k < cnt[j + 1]; ++k) P.obs_point[obs_base + k] = point_base + j;
       }
+      // The arrays through local pointers (the compiler cannot keep a
+      // vector's data pointer in a register across the stores).
+      uint32_t* const opose = P.obs_pose.data();
+      uint32_t* const ocam = P.obs_cam.data();
+      uint32_t* const oslot = P.obs_slot.data();
+      double* const oxy = P.obs_xy.data();
+      uint32_t* const osrc = P.obs_src.data();
+      const uint32_t* const pslot = P.pose_slot.data();
+      const uint8_t* const pvar = P.point_var.data();
+      uint64_t nv = 0;
       for (uint32_t k = (uint32_t)((uint64_t)no * t / To); k < (uint32_t)((uint64_t)no * (t + 1) / To); ++k) {
         const uint32_t o = identity ? k : order[k];
         const uint32_t g = obs_base + k;
         const uint32_t pose = pose_base + p->obs_pose[o];
-        P.obs_pose[g] = pose;
+        opose[g] = pose;
         const uint32_t kind = p->obs_kind ? p->obs_kind[o] : kObsMono;
         // Stereo observations project through BundleAdjustment::camera.
-        P.obs_cam[g] = cam_base + (kind == kObsMono && p->obs_camera ? p->obs_camera[o] : 0u);
+        ocam[g] = cam_base + (kind == kObsMono && p->obs_camera ? p->obs_camera[o] : 0u);
         if (stereo) {
           P.obs_kind[g] = (uint8_t)kind;
           double s0 = 0.0, s1 = 0.0;
@@ -544,12 +568,15 @@ void build_plan_serial(const vlba_problem* const* problems, const vlba_config* c
           P.obs_st[2 * (size_t)g + 1] = s1;
           P.obs_rcam[g] = cam_base + (kind == kObsGeneralStereo ? p->obs_right_camera[o] : 0u);
         }
-        P.obs_slot[g] = P.pose_slot[pose];
-        P.obs_xy[2 * (size_t)g] = p->obs_xy[2 * (size_t)o];
-        P.obs_xy[2 * (size_t)g + 1] = p->obs_xy[2 * (size_t)o + 1];
+        const uint32_t slot = pslot[pose];
+        oslot[g] = slot;
+        nv += slot != kNone && pvar[point_base + p->obs_landmark[o]];
+        oxy[2 * (size_t)g] = p->obs_xy[2 * (size_t)o];
+        oxy[2 * (size_t)g + 1] = p->obs_xy[2 * (size_t)o + 1];
         if (weighted) P.obs_w[g] = p->obs_weight ? p->obs_weight[o] : 1.0;
-        P.obs_src[g] = o;
+        osrc[g] = o;
       }
+      nvo[t] = nv;
     });
     // Per-slot observation lists (ascending point-major index).
     std::vector<uint32_t> c2(nslots + 1, 0);
@@ -573,17 +600,7 @@ void build_plan_serial(const vlba_problem* const* problems, const vlba_config* c
     // row i's are [blk_row[i], blk_row[i + 1]) of blk_cols / blk_cnts.
     std::vector<uint32_t> blk_row, blk_cols, blk_cnts;
     if (device_terms) {
-      std::vector<uint64_t> part(To, 0);
-      run_threads(To, [&](uint32_t t) {
-        uint64_t nv = 0;
-        const uint32_t j0 = (uint32_t)((uint64_t)nl * t / To), j1 = (uint32_t)((uint64_t)nl * (t + 1) / To);
-        for (uint32_t j = j0; j < j1; ++j) {
-          if (!P.point_var[point_base + j]) continue;
-          for (uint32_t k = cnt[j]; k < cnt[j + 1]; ++k) nv += P.obs_slot[obs_base + k] != kNone;
-        }
-        part[t] = nv;
-      });
-      for (uint32_t t = 0; t < To; ++t) P.var_obs += part[t];
+      for (uint32_t t = 0; t < To; ++t) P.var_obs += nvo[t];
       blk_row = std::move(rb.row_off);
       blk_cols = std::move(rb.col);
       blk_cnts = std::move(rb.count);
@@ -1315,24 +1332,6 @@ std::string check_plan(const Plan& P) {
       P.prob_tr_begin.size() != P.num_problems + 1u)
     return bad("problem ranges");
   return std::string();
-}
-
-void block_order(const Plan& P, uint32_t window, std::vector<uint32_t>* order) {
-  const uint32_t nb = (uint32_t)P.blk_dst.size();
-  const uint32_t g = std::max(1u, P.group);
-  order->resize(nb);
-  uint32_t* const o = order->data();
-  const uint32_t nw = (nb + window - 1) / window;
-  const uint32_t hw = std::max(1u, std::thread::hardware_concurrency());
-  const uint32_t T = std::max(1u, std::min<uint32_t>(hw, nw / 64));
-  run_threads(T, [&](uint32_t t) {
-    for (uint32_t w = (uint32_t)((uint64_t)nw * t / T); w < (uint32_t)((uint64_t)nw * (t + 1) / T); ++w) {
-      const uint32_t b0 = w * window, b1 = std::min(nb, b0 + window);
-      for (uint32_t b = b0; b < b1; ++b) o[b] = b;
-      auto passes = [&](uint32_t b) { return (P.blk_off[b + 1] - P.blk_off[b] + g - 1) / g; };
-      std::stable_sort(o + b0, o + b1, [&](uint32_t a, uint32_t b) { return passes(a) > passes(b); });
-    }
-  });
 }
 
 size_t Plan::device_bytes() const {

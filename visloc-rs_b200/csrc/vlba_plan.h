@@ -153,12 +153,6 @@ struct Plan {
   size_t upload_bytes() const;  // bytes copied host -> device by an upload
 };
 
-// The order in which the off-diagonal assembly takes the blocks: windows of
-// `window` consecutive blocks, each sorted (stably) by the loop passes its
-// blocks take at P.group lanes, so the blocks sharing a warp take about as
-// many passes (a block's sums do not depend on where it runs).
-void block_order(const Plan& P, uint32_t window, std::vector<uint32_t>* order);
-
 // Per-problem outcome of validation (BaError order of lm.rs:168-229).
 struct Validation {
   int status = VLBA_OK;

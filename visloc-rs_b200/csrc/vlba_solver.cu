@@ -563,9 +563,7 @@ void upload_plan_once(Context* c, uint32_t max_records, const std::function<void
     d.pairs = reinterpret_cast<const uint2*>(st.up(A, P.pairs));
   }
   d.blk_dst = reinterpret_cast<const uint2*>(st.up(A, P.blk_dst));
-  std::vector<uint32_t> blk_order;
-  block_order(P, 256, &blk_order);
-  d.blk_order = st.up(A, blk_order);
+  d.blk_order = A.alloc<uint32_t>(P.blk_dst.size());
   d.diag_dst = st.up(A, P.diag_dst);
   d.dup_off = st.up(A, P.dup_off);
   d.dup_pairs = reinterpret_cast<const uint2*>(st.up(A, P.dup_pairs));
@@ -607,6 +605,7 @@ void upload_plan_once(Context* c, uint32_t max_records, const std::function<void
   c->up_copy_ms = std::chrono::duration<double, std::milli>(u1 - u0).count();
   if (before_kernels) before_kernels();
   check_launch(launch_cam_points(d, (uint32_t)P.cam_obs.size(), s), "camera lists");
+  check_launch(launch_block_order(d, s), "block order");
   if (P.pairs_on_device) {
     // The terms, from the uploaded point-major observations and per-slot
     // lists, at the places the host laid out; checked as they are written.
