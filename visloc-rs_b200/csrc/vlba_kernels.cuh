@@ -152,7 +152,8 @@ cudaError_t launch_rows_place(const RowsDev& r, const uint32_t* blk_off, const u
                               const uint32_t* blk_col, uint32_t max_row_blocks, uint2* pairs,
                               cudaStream_t s);
 size_t rows_count_smem(uint32_t nvar);
-size_t rows_place_smem(uint32_t nvar, uint32_t max_row_blocks);
+// Shared memory of the placement with `warps` warps per row.
+size_t rows_place_smem(uint32_t nvar, uint32_t max_row_blocks, int warps);
 
 // Occupancy-derived grid of the persistent PCG kernel (0 if it cannot run).
 int pcg_grid_size(int tb, int sm_count);

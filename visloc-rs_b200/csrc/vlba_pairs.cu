@@ -127,103 +127,153 @@ __global__ void __launch_bounds__(256) k_rows_pack(RowsDev r) {
   }
 }
 
-// One warp per row.  Shared memory per warp: a map from column slot to the
-// row's block (0xFFFF: no block of this row), then per block of the row its
-// cursor, its end and the lane mask of the current group -- sized by the
-// longest row's block count rather than by the slot count, so that many
-// warps fit on an SM when rows have few blocks.
+// W warps per row, each taking a contiguous segment of the row's
+// observation list (whole groups of 32).  Shared memory per block: a map
+// from column slot to the row's block (0xFFFF: no block of this row), then
+// per warp and block of the row a cursor, a limit and the lane mask of the
+// current group -- sized by the longest row's block count.  A first pass
+// counts each warp's terms per block; the counts, added in warp order from
+// the block's start, give each warp's first place in the block, and the next
+// warp's first place is its limit.  The segments are consecutive in point
+// order, so each block still receives its terms in ascending point order.
 constexpr uint16_t kNoBlock = 0xFFFFu;
 
-__global__ void __launch_bounds__(32) k_rows_place(RowsDev r, const uint32_t* blk_off,
-                                                   const uint32_t* row_blk, const uint32_t* blk_col,
-                                                   uint32_t max_row_blocks, uint2* pairs) {
+template <int W>
+__global__ void __launch_bounds__(32 * W) k_rows_place(RowsDev r, const uint32_t* blk_off,
+                                                       const uint32_t* row_blk,
+                                                       const uint32_t* blk_col,
+                                                       uint32_t max_row_blocks, uint2* pairs) {
   extern __shared__ uint32_t sm[];
-  uint16_t* colmap = reinterpret_cast<uint16_t*>(sm);           // [nvar]
-  uint32_t* cursor = sm + (r.nvar + 1) / 2;                     // [max_row_blocks]
-  uint32_t* end = cursor + max_row_blocks;                      // [max_row_blocks]
-  uint32_t* mask = end + max_row_blocks;                        // [max_row_blocks]
-  const uint32_t lane = threadIdx.x;
+  __shared__ int s_bad;
+  uint16_t* colmap = reinterpret_cast<uint16_t*>(sm);       // [nvar]
+  uint32_t* cur = sm + (r.nvar + 1) / 2;                     // [W][max_row_blocks]
+  uint32_t* lim = cur + (size_t)W * max_row_blocks;          // [W][max_row_blocks]
+  uint32_t* msk = lim + (size_t)W * max_row_blocks;          // [W][max_row_blocks]
+  const uint32_t lane = threadIdx.x % 32, w = threadIdx.x / 32;
   const uint32_t lt = (1u << lane) - 1u;
-  for (uint32_t j = lane; j < r.nvar; j += 32) colmap[j] = kNoBlock;
-  __syncwarp();
+  uint32_t* const mcur = cur + (size_t)w * max_row_blocks;
+  uint32_t* const mlim = lim + (size_t)w * max_row_blocks;
+  uint32_t* const mmsk = msk + (size_t)w * max_row_blocks;
+  for (uint32_t j = threadIdx.x; j < r.nvar; j += 32 * W) colmap[j] = kNoBlock;
+  if (threadIdx.x == 0) s_bad = 0;
+  __syncthreads();
   for (uint32_t i = blockIdx.x; i < r.nvar; i += gridDim.x) {
     const uint32_t rb0 = row_blk[i], rb1 = row_blk[i + 1];
     bool bad = rb1 - rb0 > max_row_blocks;
     const uint32_t nb = bad ? 0u : rb1 - rb0;
-    for (uint32_t q = lane; q < nb; q += 32) {
+    for (uint32_t q = threadIdx.x; q < nb; q += 32 * W) {
       const uint32_t col = blk_col[rb0 + q];
       if (col < i) colmap[col] = (uint16_t)q;
       else bad = true;
-      cursor[q] = blk_off[rb0 + q];
-      end[q] = blk_off[rb0 + q + 1];
-      mask[q] = 0u;
     }
-    __syncwarp();
+    for (uint32_t q = threadIdx.x; q < (uint32_t)W * nb; q += 32 * W) {
+      const uint32_t ww = q / nb, qq = q % nb;
+      cur[(size_t)ww * max_row_blocks + qq] = 0u;
+      msk[(size_t)ww * max_row_blocks + qq] = 0u;
+    }
+    __syncthreads();
+    // This warp's segment: groups [g0, g1) of the row's list.
     const uint32_t q0 = r.cam_off[i], q1 = r.cam_off[i + 1];
-    for (uint32_t g = q0; g < q1; g += 32) {
-      const uint32_t q = g + lane;
-      uint32_t a = kNone, b0 = 0, b1 = 0;
+    const uint32_t ngroups = (q1 - q0 + 31) / 32;
+    const uint32_t g0 = ngroups * w / W, g1 = ngroups * (w + 1) / W;
+    // Each lane's observation and its point's range in a group.
+    auto lane_obs = [&](uint32_t g, uint32_t* a, uint32_t* b0, uint32_t* b1) {
+      const uint32_t q = q0 + 32 * g + lane;
+      *a = kNone;
+      *b0 = *b1 = 0u;
       if (q < q1) {
-        a = r.cam_obs[q];
-        const uint32_t p = r.obs_point[a];
+        *a = r.cam_obs[q];
+        const uint32_t p = r.obs_point[*a];
         if (r.point_var[p]) {
-          b0 = r.pt_off[p];
-          b1 = r.pt_off[p + 1];
+          *b0 = r.pt_off[p];
+          *b1 = r.pt_off[p + 1];
         }
       }
-      // Mark: this lane has a term in the block of each of its point's other
-      // slots below this row.
+    };
+    // Pass 1: this warp's terms per block.
+    for (uint32_t g = g0; g < g1; ++g) {
+      uint32_t a, b0, b1;
+      lane_obs(g, &a, &b0, &b1);
       for (uint32_t b = b0; b < b1; ++b) {
         const uint32_t sb = r.obs_slot[b];
         if (b == a || sb == kNone || sb >= i) continue;
         const uint32_t lb = colmap[sb];
         if (lb == kNoBlock) bad = true;  // a term outside the row's blocks
-        else atomicOr(&mask[lb], 1u << lane);
+        else atomicAdd(&mcur[lb], 1u);
+      }
+    }
+    __syncthreads();
+    // Each warp's first place and limit per block, warps in order.
+    for (uint32_t q = threadIdx.x; q < nb; q += 32 * W) {
+      uint32_t run = blk_off[rb0 + q];
+      for (int ww = 0; ww < W; ++ww) {
+        const uint32_t c = cur[(size_t)ww * max_row_blocks + q];
+        cur[(size_t)ww * max_row_blocks + q] = run;
+        run += c;
+        lim[(size_t)ww * max_row_blocks + q] = run;
+      }
+      if (run != blk_off[rb0 + q + 1]) bad = true;  // the block's size
+    }
+    __syncthreads();
+    // Pass 2: the lanes of a block in lane order from this warp's cursor.
+    for (uint32_t g = g0; g < g1; ++g) {
+      uint32_t a, b0, b1;
+      lane_obs(g, &a, &b0, &b1);
+      for (uint32_t b = b0; b < b1; ++b) {
+        const uint32_t sb = r.obs_slot[b];
+        if (b == a || sb == kNone || sb >= i) continue;
+        const uint32_t lb = colmap[sb];
+        if (lb != kNoBlock) atomicOr(&mmsk[lb], 1u << lane);
       }
       __syncwarp();
-      // Place: the lanes of a block in lane order from its cursor.
       for (uint32_t b = b0; b < b1; ++b) {
         const uint32_t sb = r.obs_slot[b];
         if (b == a || sb == kNone || sb >= i) continue;
         const uint32_t lb = colmap[sb];
         if (lb == kNoBlock) continue;
-        const uint32_t at = cursor[lb] + __popc(mask[lb] & lt);
-        if (at >= end[lb]) bad = true;
+        const uint32_t at = mcur[lb] + __popc(mmsk[lb] & lt);
+        if (at >= mlim[lb]) bad = true;
         else pairs[at] = make_uint2(a, b);
       }
       __syncwarp();
-      // Advance each block's cursor by its lanes and clear its mask: the
-      // lowest lane of the block does both (another lane of the block then
-      // reads the full mask or zero, and does nothing either way).
+      // The block's lowest lane advances its cursor and clears its mask
+      // (another lane of the block then reads the full mask or zero, and
+      // does nothing either way).
       for (uint32_t b = b0; b < b1; ++b) {
         const uint32_t sb = r.obs_slot[b];
         if (b == a || sb == kNone || sb >= i) continue;
         const uint32_t lb = colmap[sb];
         if (lb == kNoBlock) continue;
-        const uint32_t m = static_cast<volatile uint32_t*>(mask)[lb];
+        const uint32_t m = static_cast<volatile uint32_t*>(mmsk)[lb];
         if (m != 0u && (uint32_t)(__ffs(m) - 1) == lane) {
-          cursor[lb] += __popc(m);
-          atomicExch(&mask[lb], 0u);
+          mcur[lb] += __popc(m);
+          atomicExch(&mmsk[lb], 0u);
         }
       }
       __syncwarp();
     }
-    // Every block of the row filled exactly; the map back to empty.
-    for (uint32_t q = lane; q < nb; q += 32) {
-      if (cursor[q] != end[q]) bad = true;
+    __syncthreads();
+    // Every warp's share of every block filled exactly; the map back to
+    // empty.
+    for (uint32_t q = threadIdx.x; q < (uint32_t)W * nb; q += 32 * W) {
+      const uint32_t ww = q / nb, qq = q % nb;
+      if (cur[(size_t)ww * max_row_blocks + qq] != lim[(size_t)ww * max_row_blocks + qq]) bad = true;
+    }
+    for (uint32_t q = threadIdx.x; q < nb; q += 32 * W) {
       const uint32_t col = blk_col[rb0 + q];
       if (col < i) colmap[col] = kNoBlock;
     }
-    if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(r.flags, 2u);
-    __syncwarp();
+    if (bad) s_bad = 1;
+    __syncthreads();
   }
+  if (threadIdx.x == 0 && s_bad) atomicOr(r.flags, 2u);
 }
 
 }  // namespace
 
 size_t rows_count_smem(uint32_t nvar) { return (size_t)nvar * 4; }
-size_t rows_place_smem(uint32_t nvar, uint32_t max_row_blocks) {
-  return (size_t)(nvar + 1) / 2 * 4 + (size_t)max_row_blocks * 12;
+size_t rows_place_smem(uint32_t nvar, uint32_t max_row_blocks, int warps) {
+  return (size_t)(nvar + 1) / 2 * 4 + (size_t)max_row_blocks * 12 * warps;
 }
 
 cudaError_t launch_rows_count(const RowsDev& r, cudaStream_t s) {
@@ -245,12 +295,21 @@ cudaError_t launch_rows_count(const RowsDev& r, cudaStream_t s) {
 cudaError_t launch_rows_place(const RowsDev& r, const uint32_t* blk_off, const uint32_t* row_blk,
                               const uint32_t* blk_col, uint32_t max_row_blocks, uint2* pairs,
                               cudaStream_t s) {
-  const size_t sm = rows_place_smem(r.nvar, max_row_blocks);
-  cudaError_t e = cudaFuncSetAttribute(k_rows_place, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)sm);
+  // Four warps per row where their state fits in shared memory, else one.
+  constexpr size_t kMaxSmem = 227u * 1024u;
+  const int g = (int)(r.nvar < 148u * 16u ? r.nvar : 148u * 16u);
+  size_t sm = rows_place_smem(r.nvar, max_row_blocks, 4);
+  cudaError_t e;
+  if (sm <= kMaxSmem) {
+    e = cudaFuncSetAttribute(k_rows_place<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    k_rows_place<4><<<g, 128, sm, s>>>(r, blk_off, row_blk, blk_col, max_row_blocks, pairs);
+    return cudaGetLastError();
+  }
+  sm = rows_place_smem(r.nvar, max_row_blocks, 1);
+  e = cudaFuncSetAttribute(k_rows_place<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
-  const int g = (int)(r.nvar < 148u * 64u ? r.nvar : 148u * 64u);
-  k_rows_place<<<g, 32, sm, s>>>(r, blk_off, row_blk, blk_col, max_row_blocks, pairs);
+  k_rows_place<1><<<g, 32, sm, s>>>(r, blk_off, row_blk, blk_col, max_row_blocks, pairs);
   return cudaGetLastError();
 }
 

@@ -1168,7 +1168,7 @@ bool device_row_blocks(Context* c, const Plan& P, uint32_t nvar, RowBlocks* out)
   uint32_t max_row_blocks = 0;
   for (uint32_t i = 0; i < nvar; ++i)
     max_row_blocks = std::max(max_row_blocks, out->row_off[i + 1] - out->row_off[i]);
-  if (rows_place_smem(nvar, max_row_blocks) > kMaxDynamicSmem) return false;
+  if (rows_place_smem(nvar, max_row_blocks, 1) > kMaxDynamicSmem) return false;
   out->col.resize(nb);
   out->count.resize(nb);
   VLBA_CUDA(cudaMemcpyAsync(out->col.data(), r.col, 4 * nb, cudaMemcpyDeviceToHost, s));
