@@ -190,7 +190,10 @@ struct Dev {
   float* tiles;                // [num_tiles * tb*tb * 36]
   const uint32_t* tile_ij;     // [num_tiles] (I << 16) | J
   const uint32_t* blk_off;     // [num_offdiag_blocks + 1] pair ranges
-  const uint32_t* blk_order;   // [num_offdiag_blocks] the assembly's block order
+  // The assembly's blocks in the order it takes them: each one's term range
+  // (first, end) and destination, at its place in that order.
+  const uint2* ord_range;      // [num_offdiag_blocks]
+  const uint2* ord_dst;        // [num_offdiag_blocks]
   const uint2* pairs;          // (k_i, k_j), sorted by block then point
   const uint2* blk_dst;        // [num_offdiag_blocks] float offsets (block, mirror or kNone)
   const uint32_t* diag_dst;    // [num_var_cams] float offset of the diagonal block

@@ -418,8 +418,9 @@ __device__ __forceinline__ void point_inverse64(const Dev& d, uint32_t l, double
 // A term reads three 32-byte records with one request each -- H_i (with the
 // point's z), the point's damped inverse and x, y stored beside observation
 // i, and H_j -- all addressed by the pair entry, whose successor is fetched
-// while the current term is computed.  Warps take the blocks in blk_order
-// (plan order, sorted by length within windows of 256 blocks): the groups of
+// while the current term is computed.  Warps take the blocks in the order of
+// ord_range / ord_dst (plan order, sorted by length within windows of 256
+// blocks, each block's range and destination stored at its place): the groups of
 // a warp then loop about as many times (lane-pass efficiency 0.82 -> 0.99 on
 // ring-4m) while the blocks running at one time stay those of nearby rows.
 template <int G>
@@ -439,10 +440,10 @@ __global__ void __launch_bounds__(256, 2) k_offdiag(Dev d) {
       // The block's range and first pair go out beside its problem's status
       // (a single problem's is the same for every block): the pair loads do
       // not wait for the lookup of the problem.
-      const uint32_t b = d.blk_order[q];
-      dst = d.blk_dst[b];
-      c0 = d.blk_off[b];
-      c1 = d.blk_off[b + 1];
+      const uint2 range = d.ord_range[q];
+      dst = d.ord_dst[q];
+      c0 = range.x;
+      c1 = range.y;
       if (c0 + lane < c1) pr = d.pairs[c0 + lane];
       const uint32_t P =
           d.num_problems == 1 ? 0u : d.tr_prob[d.tile_ij[dst.x / tile_floats] >> 16];
@@ -2143,9 +2144,11 @@ __global__ void k_wait_probe(const unsigned int* flag, unsigned long long limit_
 // The off-diagonal assembly's block order: each window of 256 blocks in plan
 // order sorted by the loop passes its blocks take at g lanes, longest first,
 // ties in plan order (a block's rank is the count of blocks of its window
-// before it in that order).
-__global__ void __launch_bounds__(256) k_block_order(const uint32_t* blk_off, uint32_t nb,
-                                                     uint32_t g, uint32_t* order) {
+// before it in that order); each block's term range and destination are
+// written at its place in that order.
+__global__ void __launch_bounds__(256) k_block_order(const uint32_t* blk_off, const uint2* blk_dst,
+                                                     uint32_t nb, uint32_t g, uint2* ord_range,
+                                                     uint2* ord_dst) {
   __shared__ uint32_t key[256];
   const uint32_t b0 = blockIdx.x * 256u, t = threadIdx.x;
   const uint32_t n = min(256u, nb - b0);
@@ -2159,7 +2162,8 @@ __global__ void __launch_bounds__(256) k_block_order(const uint32_t* blk_off, ui
       const uint32_t kj = key[j];
       rank += (kj > k || (kj == k && j < t)) ? 1u : 0u;
     }
-    order[b0 + rank] = b0 + t;
+    ord_range[b0 + rank] = make_uint2(blk_off[b0 + t], blk_off[b0 + t + 1]);
+    ord_dst[b0 + rank] = blk_dst[b0 + t];
   }
 }
 
@@ -2347,7 +2351,8 @@ cudaError_t launch_sq_residuals(const Dev& d, double* out, cudaStream_t s) {
 cudaError_t launch_block_order(const Dev& d, cudaStream_t s) {
   if (d.num_offdiag_blocks == 0) return cudaSuccess;
   k_block_order<<<(d.num_offdiag_blocks + 255) / 256, 256, 0, s>>>(
-      d.blk_off, d.num_offdiag_blocks, d.group, const_cast<uint32_t*>(d.blk_order));
+      d.blk_off, d.blk_dst, d.num_offdiag_blocks, d.group, const_cast<uint2*>(d.ord_range),
+      const_cast<uint2*>(d.ord_dst));
   return cudaGetLastError();
 }
 

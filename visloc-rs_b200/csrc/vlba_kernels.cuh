@@ -16,8 +16,8 @@ cudaError_t launch_linearize(const Dev& d, cudaStream_t s);
 cudaError_t launch_point_prep(const Dev& d, cudaStream_t s);
 cudaError_t launch_offdiag(const Dev& d, cudaStream_t s);
 cudaError_t launch_cam_diag(const Dev& d, cudaStream_t s);
-// blk_order: each window of 256 blocks sorted by the loop passes its blocks
-// take at d.group lanes (longest first, ties in plan order).
+// ord_range / ord_dst: the blocks of each window of 256 sorted by the loop
+// passes they take at d.group lanes (longest first, ties in plan order).
 cudaError_t launch_block_order(const Dev& d, cudaStream_t s);
 // cam_pt[i] = obs_point[cam_obs[i]] for the n listed observations.
 cudaError_t launch_cam_points(const Dev& d, uint32_t n, cudaStream_t s);

@@ -563,7 +563,8 @@ void upload_plan_once(Context* c, uint32_t max_records, const std::function<void
     d.pairs = reinterpret_cast<const uint2*>(st.up(A, P.pairs));
   }
   d.blk_dst = reinterpret_cast<const uint2*>(st.up(A, P.blk_dst));
-  d.blk_order = A.alloc<uint32_t>(P.blk_dst.size());
+  d.ord_range = A.alloc<uint2>(P.blk_dst.size());
+  d.ord_dst = A.alloc<uint2>(P.blk_dst.size());
   d.diag_dst = st.up(A, P.diag_dst);
   d.dup_off = st.up(A, P.dup_off);
   d.dup_pairs = reinterpret_cast<const uint2*>(st.up(A, P.dup_pairs));
