@@ -169,7 +169,7 @@ struct Dev {
   const uint32_t* obs_rcam;    // [K]
   float4* obs_h;               // [2 K]: {h00,h01,h02,h11} {h12,h22,point,X.z}
   float4* obs_e;               // [K]:   {e0,e1,e2,w}
-  float4* obs_p;               // [2 K]: the observation's point, per trial:
+  float4* pt_p;                // [2 M]: each point's record, per trial:
                                //        {hinv00,01,02,11} {hinv12,22,X.x,X.y}
 
   // per-camera observation lists (indices into the point-major order)
@@ -195,6 +195,7 @@ struct Dev {
   const uint2* ord_range;      // [num_offdiag_blocks]
   const uint2* ord_dst;        // [num_offdiag_blocks]
   const uint2* pairs;          // (k_i, k_j), sorted by block then point
+  uint32_t* pair_pt;           // [pairs] each term's point (set at upload)
   const uint2* blk_dst;        // [num_offdiag_blocks] float offsets (block, mirror or kNone)
   const uint32_t* diag_dst;    // [num_var_cams] float offset of the diagonal block
   const uint32_t* dup_off;     // [num_var_cams + 1] same-camera pairs k != k'

@@ -379,10 +379,8 @@ __global__ void __launch_bounds__(256) k_point_prep(Dev d) {
     const float4 p1 = make_float4((float)inv[4], (float)inv[5], X0, X1);
     ps[0] = p0;
     ps[1] = p1;
-    // The same 32 bytes beside each observation of a variable point (read by
-    // the off-diagonal assembly next to the observation's own record).
-    if (d.point_var[l])
-      for (uint32_t k = d.pt_off[l]; k < d.pt_off[l + 1]; ++k) st8(d.obs_p + 2 * (size_t)k, p0, p1);
+    // The same 32 bytes as one record for the off-diagonal assembly.
+    st8(d.pt_p + 2 * (size_t)l, p0, p1);
     ps[2] = make_float4(X2, (float)v[0], (float)v[1], (float)v[2]);
     ps[3] = make_float4((float)g[0], (float)g[1], (float)g[2], ok);
   }
@@ -416,9 +414,9 @@ __device__ __forceinline__ void point_inverse64(const Dev& d, uint32_t l, double
 // mirrored slot inside a diagonal tile).
 //
 // A term reads three 32-byte records with one request each -- H_i (with the
-// point's z), the point's damped inverse and x, y stored beside observation
-// i, and H_j -- all addressed by the pair entry, whose successor is fetched
-// while the current term is computed.  Warps take the blocks in the order of
+// point's z), the point's record (damped inverse and x, y), and H_j --
+// addressed by the pair entry and the term's point stored beside it, whose
+// successors are fetched while the current term is computed.  Warps take the blocks in the order of
 // ord_range / ord_dst (plan order, sorted by length within windows of 256
 // blocks, each block's range and destination stored at its place): the groups of
 // a warp then loop about as many times (lane-pass efficiency 0.82 -> 0.99 on
@@ -435,7 +433,7 @@ __global__ void __launch_bounds__(256, 2) k_offdiag(Dev d) {
     const uint32_t q = wb * kPerWarp + (threadIdx.x % 32) / G;
     bool valid = q < d.num_offdiag_blocks;
     uint2 dst = make_uint2(kNone, kNone), pr = make_uint2(0u, 0u);
-    uint32_t c0 = 0, c1 = 0;
+    uint32_t c0 = 0, c1 = 0, pt = 0;
     if (valid) {
       // The block's range and first pair go out beside its problem's status
       // (a single problem's is the same for every block): the pair loads do
@@ -444,7 +442,10 @@ __global__ void __launch_bounds__(256, 2) k_offdiag(Dev d) {
       dst = d.ord_dst[q];
       c0 = range.x;
       c1 = range.y;
-      if (c0 + lane < c1) pr = d.pairs[c0 + lane];
+      if (c0 + lane < c1) {
+        pr = d.pairs[c0 + lane];
+        pt = d.pair_pt[c0 + lane];
+      }
       const uint32_t P =
           d.num_problems == 1 ? 0u : d.tr_prob[d.tile_ij[dst.x / tile_floats] >> 16];
       valid = !d.ctrl[P].done;
@@ -459,9 +460,12 @@ __global__ void __launch_bounds__(256, 2) k_offdiag(Dev d) {
       for (uint32_t cidx = c0 + lane; cidx < c1; cidx += G) {
         float4 a0, a1, p0, p1, b0, b1;
         ld8(d.obs_h + 2 * (size_t)pr.x, a0, a1);
-        ld8(d.obs_p + 2 * (size_t)pr.x, p0, p1);
+        ld8(d.pt_p + 2 * (size_t)pt, p0, p1);
         ld8(d.obs_h + 2 * (size_t)pr.y, b0, b1);
-        if (cidx + G < c1) pr = d.pairs[cidx + G];
+        if (cidx + G < c1) {
+          pr = d.pairs[cidx + G];
+          pt = d.pair_pt[cidx + G];
+        }
         const float Hi[9] = {a0.x, a0.y, a0.z, a0.y, a0.w, a1.x, a0.z, a1.x, a1.y};
         const float Hj[9] = {b0.x, b0.y, b0.z, b0.y, b0.w, b1.x, b0.z, b1.x, b1.y};
         const float Mi[9] = {p0.x, p0.y, p0.z, p0.y, p0.w, p1.x, p0.z, p1.x, p1.y};
@@ -2167,6 +2171,15 @@ __global__ void __launch_bounds__(256) k_block_order(const uint32_t* blk_off, co
   }
 }
 
+// The point of every Schur term, beside the term list (read by the
+// off-diagonal assembly with the term, both coalesced).
+__global__ void __launch_bounds__(256) k_pair_points(const uint2* pairs, const uint32_t* obs_point,
+                                                     uint64_t n, uint32_t* pair_pt) {
+  for (uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; q < n;
+       q += (uint64_t)gridDim.x * blockDim.x)
+    pair_pt[q] = obs_point[pairs[q].x];
+}
+
 // The point of every listed observation, beside the per-slot lists (read
 // by the camera-diagonal sums with the observation index, both coalesced).
 __global__ void __launch_bounds__(256) k_cam_points(Dev d, uint32_t n) {
@@ -2345,6 +2358,12 @@ __global__ void __launch_bounds__(256) k_sq_residuals(Dev d, double* out) {
 
 cudaError_t launch_sq_residuals(const Dev& d, double* out, cudaStream_t s) {
   k_sq_residuals<<<grid1d(d.num_obs, 256), 256, 0, s>>>(d, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pair_points(const Dev& d, uint64_t n, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  k_pair_points<<<grid1d(n, 256), 256, 0, s>>>(d.pairs, d.obs_point, n, d.pair_pt);
   return cudaGetLastError();
 }
 

@@ -19,6 +19,8 @@ cudaError_t launch_cam_diag(const Dev& d, cudaStream_t s);
 // ord_range / ord_dst: the blocks of each window of 256 sorted by the loop
 // passes they take at d.group lanes (longest first, ties in plan order).
 cudaError_t launch_block_order(const Dev& d, cudaStream_t s);
+// pair_pt[q] = obs_point[pairs[q].x] for the n Schur terms.
+cudaError_t launch_pair_points(const Dev& d, uint64_t n, cudaStream_t s);
 // cam_pt[i] = obs_point[cam_obs[i]] for the n listed observations.
 cudaError_t launch_cam_points(const Dev& d, uint32_t n, cudaStream_t s);
 cudaError_t launch_pcg(const Dev& d, int sm_count, cudaStream_t s);
@@ -150,7 +152,7 @@ cudaError_t launch_rows_count(const RowsDev& r, cudaStream_t s);
 // max_row_blocks: the most blocks of any row (sizes the per-row state).
 cudaError_t launch_rows_place(const RowsDev& r, const uint32_t* blk_off, const uint32_t* row_blk,
                               const uint32_t* blk_col, uint32_t max_row_blocks, uint2* pairs,
-                              cudaStream_t s);
+                              uint32_t* pair_pt, cudaStream_t s);
 size_t rows_count_smem(uint32_t nvar);
 // Shared memory of the placement with `warps` warps per row.
 size_t rows_place_smem(uint32_t nvar, uint32_t max_row_blocks, int warps);

@@ -21,7 +21,8 @@
 //                 shared map), the lanes that have a term there take
 //                 consecutive places in lane order (a shared bit mask per
 //                 block and the lane's rank in it), so each block receives
-//                 its terms in ascending point order -- the host's order;
+//                 its terms in ascending point order -- the host's order
+//                 (with each term's point beside it);
 //                 the column's lowest lane then advances its cursor and
 //                 clears its mask.
 //                 Every place is checked against its block's range; a term
@@ -142,7 +143,8 @@ template <int W>
 __global__ void __launch_bounds__(32 * W) k_rows_place(RowsDev r, const uint32_t* blk_off,
                                                        const uint32_t* row_blk,
                                                        const uint32_t* blk_col,
-                                                       uint32_t max_row_blocks, uint2* pairs) {
+                                                       uint32_t max_row_blocks, uint2* pairs,
+                                                       uint32_t* pair_pt) {
   extern __shared__ uint32_t sm[];
   __shared__ int s_bad;
   uint16_t* colmap = reinterpret_cast<uint16_t*>(sm);       // [nvar]
@@ -177,13 +179,15 @@ __global__ void __launch_bounds__(32 * W) k_rows_place(RowsDev r, const uint32_t
     const uint32_t ngroups = (q1 - q0 + 31) / 32;
     const uint32_t g0 = ngroups * w / W, g1 = ngroups * (w + 1) / W;
     // Each lane's observation and its point's range in a group.
-    auto lane_obs = [&](uint32_t g, uint32_t* a, uint32_t* b0, uint32_t* b1) {
+    auto lane_obs = [&](uint32_t g, uint32_t* a, uint32_t* b0, uint32_t* b1, uint32_t* pp) {
       const uint32_t q = q0 + 32 * g + lane;
       *a = kNone;
       *b0 = *b1 = 0u;
+      *pp = 0u;
       if (q < q1) {
         *a = r.cam_obs[q];
         const uint32_t p = r.obs_point[*a];
+        *pp = p;
         if (r.point_var[p]) {
           *b0 = r.pt_off[p];
           *b1 = r.pt_off[p + 1];
@@ -192,8 +196,8 @@ __global__ void __launch_bounds__(32 * W) k_rows_place(RowsDev r, const uint32_t
     };
     // Pass 1: this warp's terms per block.
     for (uint32_t g = g0; g < g1; ++g) {
-      uint32_t a, b0, b1;
-      lane_obs(g, &a, &b0, &b1);
+      uint32_t a, b0, b1, pp;
+      lane_obs(g, &a, &b0, &b1, &pp);
       for (uint32_t b = b0; b < b1; ++b) {
         const uint32_t sb = r.obs_slot[b];
         if (b == a || sb == kNone || sb >= i) continue;
@@ -217,8 +221,8 @@ __global__ void __launch_bounds__(32 * W) k_rows_place(RowsDev r, const uint32_t
     __syncthreads();
     // Pass 2: the lanes of a block in lane order from this warp's cursor.
     for (uint32_t g = g0; g < g1; ++g) {
-      uint32_t a, b0, b1;
-      lane_obs(g, &a, &b0, &b1);
+      uint32_t a, b0, b1, pp;
+      lane_obs(g, &a, &b0, &b1, &pp);
       for (uint32_t b = b0; b < b1; ++b) {
         const uint32_t sb = r.obs_slot[b];
         if (b == a || sb == kNone || sb >= i) continue;
@@ -232,8 +236,12 @@ __global__ void __launch_bounds__(32 * W) k_rows_place(RowsDev r, const uint32_t
         const uint32_t lb = colmap[sb];
         if (lb == kNoBlock) continue;
         const uint32_t at = mcur[lb] + __popc(mmsk[lb] & lt);
-        if (at >= mlim[lb]) bad = true;
-        else pairs[at] = make_uint2(a, b);
+        if (at >= mlim[lb]) {
+          bad = true;
+        } else {
+          pairs[at] = make_uint2(a, b);
+          pair_pt[at] = pp;
+        }
       }
       __syncwarp();
       // The block's lowest lane advances its cursor and clears its mask
@@ -294,7 +302,7 @@ cudaError_t launch_rows_count(const RowsDev& r, cudaStream_t s) {
 
 cudaError_t launch_rows_place(const RowsDev& r, const uint32_t* blk_off, const uint32_t* row_blk,
                               const uint32_t* blk_col, uint32_t max_row_blocks, uint2* pairs,
-                              cudaStream_t s) {
+                              uint32_t* pair_pt, cudaStream_t s) {
   // Four warps per row where their state fits in shared memory, else one.
   constexpr size_t kMaxSmem = 227u * 1024u;
   const int g = (int)(r.nvar < 148u * 16u ? r.nvar : 148u * 16u);
@@ -303,13 +311,13 @@ cudaError_t launch_rows_place(const RowsDev& r, const uint32_t* blk_off, const u
   if (sm <= kMaxSmem) {
     e = cudaFuncSetAttribute(k_rows_place<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
-    k_rows_place<4><<<g, 128, sm, s>>>(r, blk_off, row_blk, blk_col, max_row_blocks, pairs);
+    k_rows_place<4><<<g, 128, sm, s>>>(r, blk_off, row_blk, blk_col, max_row_blocks, pairs, pair_pt);
     return cudaGetLastError();
   }
   sm = rows_place_smem(r.nvar, max_row_blocks, 1);
   e = cudaFuncSetAttribute(k_rows_place<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
-  k_rows_place<1><<<g, 32, sm, s>>>(r, blk_off, row_blk, blk_col, max_row_blocks, pairs);
+  k_rows_place<1><<<g, 32, sm, s>>>(r, blk_off, row_blk, blk_col, max_row_blocks, pairs, pair_pt);
   return cudaGetLastError();
 }
 

@@ -538,7 +538,7 @@ void upload_plan_once(Context* c, uint32_t max_records, const std::function<void
   d.obs_rcam = P.obs_kind.empty() ? nullptr : st.up(A, P.obs_rcam);
   d.obs_h = A.alloc<float4>(2 * nobs);
   d.obs_e = A.alloc<float4>(nobs);
-  d.obs_p = A.alloc<float4>(2 * nobs);
+  d.pt_p = A.alloc<float4>(2 * npt);
   d.cam_off = reuse ? from_rows(P.cam_off, 0) : st.up(A, P.cam_off);
   d.cam_obs = reuse ? from_rows(P.cam_obs, 1) : st.up(A, P.cam_obs);
   d.cam_pt = A.alloc<uint32_t>(P.cam_obs.size());
@@ -562,6 +562,8 @@ void upload_plan_once(Context* c, uint32_t max_records, const std::function<void
   } else {
     d.pairs = reinterpret_cast<const uint2*>(st.up(A, P.pairs));
   }
+  const uint64_t npairs = P.pairs_on_device ? P.num_pairs : P.pairs.size();
+  d.pair_pt = A.alloc<uint32_t>(npairs);
   d.blk_dst = reinterpret_cast<const uint2*>(st.up(A, P.blk_dst));
   d.ord_range = A.alloc<uint2>(P.blk_dst.size());
   d.ord_dst = A.alloc<uint2>(P.blk_dst.size());
@@ -624,13 +626,15 @@ void upload_plan_once(Context* c, uint32_t max_records, const std::function<void
     uint32_t max_row_blocks = 0;
     for (uint32_t i = 0; i < r.nvar; ++i)
       max_row_blocks = std::max(max_row_blocks, P.row_blk[i + 1] - P.row_blk[i]);
-    check_launch(launch_rows_place(r, d.blk_off, dev_row_blk, dev_blk_col, max_row_blocks, dev_pairs, s),
+    check_launch(launch_rows_place(r, d.blk_off, dev_row_blk, dev_blk_col, max_row_blocks, dev_pairs,
+                                   d.pair_pt, s),
                  "Schur terms");
     uint32_t flags = 0;
     VLBA_CUDA(cudaMemcpyAsync(&flags, r.flags, 4, cudaMemcpyDeviceToHost, s));
     VLBA_CUDA(cudaStreamSynchronize(s));
     if (flags) throw std::runtime_error("device Schur terms do not match the plan's blocks");
   }
+  if (!P.pairs_on_device) check_launch(launch_pair_points(d, npairs, s), "term points");
   c->up_terms_ms =
       std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - u1).count();
   // Co-resident grid, but no more blocks than tiles or tile rows to work on
