@@ -180,8 +180,10 @@ struct Dev {
   // per point, per linearisation / per trial
   float* pt_h;                 // [9 M] H_ll upper (6) + g_l (3)
   float4* pt_s;                // [4 M] {hinv00,01,02,11} {hinv12,22,X.x,X.y} {X.z,v0,v1,v2} {g0,g1,g2,ok}
-  double2* pt_inv;             // [5 M] per trial, a point with an inverse: its FP64 damped
-                               // inverse {i00,i01} {i02,i11} {i12,i22} and v = H^-1 g {v0,v1} {v2,-}
+  double* pt_c;                // [12 M] per trial, 96 bytes per point: its FP64 damped inverse
+                               // {i00,i01,i02,i11,i12,i22}, v = H^-1 g {v0,v1,v2}, then
+                               // X.x, X.y | X.z, ok as f32 pairs, one spare (zero inverse
+                               // and v for a point without one)
 
   // per camera
   double* cam_hpp;             // [27 C] H_pp upper 21 + g_p 6 (f64)

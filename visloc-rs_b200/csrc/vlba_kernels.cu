@@ -181,6 +181,26 @@ __global__ void __launch_bounds__(256) k_pose_table(Dev d) {
   }
 }
 
+// 32-byte load and store of four doubles (the point records are 32-byte
+// aligned and read-only while the kernels that read them run).
+__device__ __forceinline__ void ld4d(const double* p, double* o) {
+  asm("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];"
+      : "=d"(o[0]), "=d"(o[1]), "=d"(o[2]), "=d"(o[3])
+      : "l"(p));
+}
+__device__ __forceinline__ void st4d(double* p, double a, double b, double c, double e) {
+  asm volatile("st.global.v4.f64 [%0], {%1,%2,%3,%4};" ::"l"(p), "d"(a), "d"(b), "d"(c), "d"(e)
+               : "memory");
+}
+// Two f32 values in one double's bits (low word first).
+__device__ __forceinline__ double pack2f(float lo, float hi) {
+  return __longlong_as_double(((long long)__float_as_uint(hi) << 32) | (long long)__float_as_uint(lo));
+}
+__device__ __forceinline__ float2 unpack2f(double v) {
+  const unsigned long long u = (unsigned long long)__double_as_longlong(v);
+  return make_float2(__uint_as_float((uint32_t)u), __uint_as_float((uint32_t)(u >> 32)));
+}
+
 // ------------------------------------------------------------- linearize
 // One thread per observation (point-major order): the residual and analytic
 // Jacobian in FP64, the IRLS weight, and the observation's H_o and e_o.  The
@@ -308,6 +328,7 @@ __global__ void __launch_bounds__(256) k_point_prep(Dev d) {
     const float X1 = (float)d.points[cur][3 * (size_t)l + 1];
     const float X2 = (float)d.points[cur][3 * (size_t)l + 2];
     double inv[6] = {0, 0, 0, 0, 0, 0}, v[3] = {0, 0, 0}, g[3] = {0, 0, 0};
+    double ci[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};  // the FP64 record's inverse and v
     float ok = 0.0f;
     if (d.point_var[l] && c.relinearize) {
       // H_ll and g_l of the new linearisation: the observations' records
@@ -366,13 +387,22 @@ __global__ void __launch_bounds__(256) k_point_prep(Dev d) {
         const double i0 = m22 * rdet, i1 = (cc * e - f * b) * rdet, i2 = (b * e - dd * cc) * rdet,
                      i3 = (a * f - cc * cc) * rdet, i4 = (cc * b - e * a) * rdet,
                      i5 = (a * dd - b * b) * rdet;
-        double2* pi = d.pt_inv + 5 * (size_t)l;
-        pi[0] = make_double2(i0, i1);
-        pi[1] = make_double2(i2, i3);
-        pi[2] = make_double2(i4, i5);
-        pi[3] = make_double2(i0 * g[0] + i1 * g[1] + i2 * g[2], i1 * g[0] + i3 * g[1] + i4 * g[2]);
-        pi[4] = make_double2(i2 * g[0] + i4 * g[1] + i5 * g[2], 0.0);
+        ci[0] = i0;
+        ci[1] = i1;
+        ci[2] = i2;
+        ci[3] = i3;
+        ci[4] = i4;
+        ci[5] = i5;
+        ci[6] = i0 * g[0] + i1 * g[1] + i2 * g[2];
+        ci[7] = i1 * g[0] + i3 * g[1] + i4 * g[2];
+        ci[8] = i2 * g[0] + i4 * g[1] + i5 * g[2];
       }
+    }
+    {
+      double* pc = d.pt_c + 12 * (size_t)l;
+      st4d(pc, ci[0], ci[1], ci[2], ci[3]);
+      st4d(pc + 4, ci[4], ci[5], ci[6], ci[7]);
+      st4d(pc + 8, ci[8], pack2f(X0, X1), pack2f(X2, ok), 0.0);
     }
     float4* ps = d.pt_s + 4 * (size_t)l;
     const float4 p0 = make_float4((float)inv[0], (float)inv[1], (float)inv[2], (float)inv[3]);
@@ -396,14 +426,17 @@ __global__ void __launch_bounds__(256) k_point_prep(Dev d) {
 // H_o - H_o (H_ll + lambda I)^-1 H_o cancels down to O(lambda), far below
 // what an FP32 inverse with entries near 1/lambda resolves.
 __device__ __forceinline__ void point_inverse64(const Dev& d, uint32_t l, double* M, double* v) {
-  const double2* pi = d.pt_inv + 5 * (size_t)l;
-  const double2 a = pi[0], b = pi[1], c = pi[2], e = pi[3], f = pi[4];
-  M[0] = a.x; M[1] = a.y; M[2] = b.x;
-  M[3] = a.y; M[4] = b.y; M[5] = c.x;
-  M[6] = b.x; M[7] = c.x; M[8] = c.y;
-  v[0] = e.x;
-  v[1] = e.y;
-  v[2] = f.x;
+  double c[12];
+  const double* pc = d.pt_c + 12 * (size_t)l;
+  ld4d(pc, c);
+  ld4d(pc + 4, c + 4);
+  ld4d(pc + 8, c + 8);
+  M[0] = c[0]; M[1] = c[1]; M[2] = c[2];
+  M[3] = c[1]; M[4] = c[3]; M[5] = c[4];
+  M[6] = c[2]; M[7] = c[4]; M[8] = c[5];
+  v[0] = c[6];
+  v[1] = c[7];
+  v[2] = c[8];
 }
 
 // ------------------------------------------------- off-diagonal Schur blocks
@@ -587,21 +620,21 @@ __device__ __forceinline__ void diag_block_sum(double* acc, double* red, double*
 
 // Observation k (of point l)'s terms of S_ii and b_i.
 __device__ __forceinline__ void cam_diag_obs(const Dev& d, uint32_t k, uint32_t l, double* acc) {
-  float4 h0, h1, s2, s3;
+  float4 h0, h1;
   ld8(d.obs_h + 2 * (size_t)k, h0, h1);
   const float4 ev = __ldg(d.obs_e + k);
-  const float4 s1 = __ldg(d.pt_s + 4 * (size_t)l + 1);
-  ld8(d.pt_s + 4 * (size_t)l + 2, s2, s3);
-  // The point's FP64 damped inverse and v (formed by k_point_prep when the
-  // point has one; read unconditionally so the loads go out together).
-  const double2* pi = d.pt_inv + 5 * (size_t)l;
-  const double2 ia = __ldg(pi), ib = __ldg(pi + 1), ic = __ldg(pi + 2), ie = __ldg(pi + 3),
-                if_ = __ldg(pi + 4);
+  // The point's 96-byte record: FP64 damped inverse and v, X and the ok flag.
+  double c[12];
+  const double* pc = d.pt_c + 12 * (size_t)l;
+  ld4d(pc, c);
+  ld4d(pc + 4, c + 4);
+  ld4d(pc + 8, c + 8);
+  const float2 xy = unpack2f(c[9]), zo = unpack2f(c[10]);
   const double H[9] = {h0.x, h0.y, h0.z, h0.y, h0.w, h1.x, h0.z, h1.x, h1.y};
-  const double X = s1.z, Y = s1.w, Z = s2.x;
+  const double X = xy.x, Y = xy.y, Z = zo.x;
   double K[9], w[3];
-  if (s3.w != 0.0f) {
-    const double Mi[9] = {ia.x, ia.y, ib.x, ia.y, ib.y, ic.x, ib.x, ic.x, ic.y};
+  if (zo.y != 0.0f) {
+    const double Mi[9] = {c[0], c[1], c[2], c[1], c[3], c[4], c[2], c[4], c[5]};
     double M[9];
 #pragma unroll
     for (int r = 0; r < 3; ++r)
@@ -614,7 +647,7 @@ __device__ __forceinline__ void cam_diag_obs(const Dev& d, uint32_t k, uint32_t 
       for (int cc = 0; cc < 3; ++cc)
         K[r * 3 + cc] = H[r * 3 + cc] - (H[r * 3] * M[cc] + H[r * 3 + 1] * M[3 + cc] +
                                          H[r * 3 + 2] * M[6 + cc]);
-    const double v0 = ie.x, v1 = ie.y, v2 = if_.x;
+    const double v0 = c[6], v1 = c[7], v2 = c[8];
     w[0] = H[0] * v0 + H[1] * v1 + H[2] * v2 - ev.x;
     w[1] = H[3] * v0 + H[4] * v1 + H[5] * v2 - ev.y;
     w[2] = H[6] * v0 + H[7] * v1 + H[8] * v2 - ev.z;

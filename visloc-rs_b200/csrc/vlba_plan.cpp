@@ -1338,8 +1338,8 @@ size_t Plan::device_bytes() const {
   const size_t npose = pose_prob.size(), npt = point_prob.size(), nobs = obs_pose.size();
   size_t b = 0;
   b += npose * (8 * (4 + 3 + 12) * 2 + 8 + 4 + 4);  // state x2, step, slot, prob
-  b += npt * (8 * 3 * 2 + 4 + 1 + 4 + 36 + 64 + 80 + 32);  // points x2, off, var, prob, pt_h,
-                                                           // pt_s, pt_inv, pt_p
+  b += npt * (8 * 3 * 2 + 4 + 1 + 4 + 36 + 64 + 96 + 32);  // points x2, off, var, prob, pt_h,
+                                                           // pt_s, pt_c, pt_p
   b += nobs * (4 * 4 + 16 + 32 + 16);                // point, pose, cam, slot, xy, obs_h, obs_e
   b += obs_w.size() * 8 + obs_kind.size() * (1 + 16 + 4);
   b += cam_obs.size() * 8 + (pairs_on_device ? num_pairs : pairs.size()) * 12 + dup_pairs.size() * 8;

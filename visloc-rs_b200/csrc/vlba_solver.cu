@@ -544,7 +544,7 @@ void upload_plan_once(Context* c, uint32_t max_records, const std::function<void
   d.cam_pt = A.alloc<uint32_t>(P.cam_obs.size());
   d.pt_h = A.alloc<float>(9 * npt);
   d.pt_s = A.alloc<float4>(4 * npt);
-  d.pt_inv = A.alloc<double2>(5 * npt);
+  d.pt_c = A.alloc<double>(12 * npt);
   d.cam_hpp = nullptr;
   const size_t tile_floats = (size_t)P.tb * P.tb * kBlock;
   d.tiles = A.alloc<float>(P.tile_ij.size() * tile_floats);
