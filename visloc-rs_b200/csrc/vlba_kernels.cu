@@ -584,11 +584,12 @@ __device__ __forceinline__ double quad3(const double* H, double a, double b, dou
 // (ba.wgsl:263-387; fallback to the inverse damped diagonal, ba.wgsl:375-383).
 // Thread t adds the camera's observations t, t + 128, ... in list (= point)
 // order, so the blocks running at one time read the records of nearby
-// points.  An observation's record and its point's records are one gather
-// away (the point stored beside the list, cam_pt), nine loads of 16 and 32
-// bytes issued together; the next observation's indices are loaded while
-// this one is summed (measured on ring-4m: 270 -> 210 us against the record
-// read through the observation's own point index).
+// points.  An observation's records and its point's 96-byte FP64 record are
+// one gather away (the point stored beside the list, cam_pt), five loads of
+// 16 and 32 bytes issued together; the next observation's indices are loaded
+// while this one is summed (measured on ring-4m: 270 -> 210 us against the
+// records read through the observation's own point index, and about 175 us
+// with the point's data in one record instead of three).
 // Warps sum by a butterfly, then in warp order: fixed order throughout.
 constexpr int kDiagThreads = 128;
 constexpr int kDiagAcc = 27;  // 21 upper S, 6 rhs
