@@ -588,8 +588,8 @@ __device__ __forceinline__ double quad3(const double* H, double a, double b, dou
 // one gather away (the point stored beside the list, cam_pt), five loads of
 // 16 and 32 bytes issued together; the next observation's indices are loaded
 // while this one is summed (measured on ring-4m: 270 -> 210 us against the
-// records read through the observation's own point index, and about 175 us
-// with the point's data in one record instead of three).
+// records read through the observation's own point index; the point's data
+// in one record instead of three took another 36 us off the assembly).
 // Warps sum by a butterfly, then in warp order: fixed order throughout.
 constexpr int kDiagThreads = 128;
 constexpr int kDiagAcc = 27;  // 21 upper S, 6 rhs
