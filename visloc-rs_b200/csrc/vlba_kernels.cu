@@ -4,11 +4,13 @@
 // lm.rs:356-1009, GPU twin crates/ba-gpu/src/solver.rs:552-690 with the
 // shaders of crates/ba-gpu/src/shaders/ba.wgsl) is the kernel sequence
 //
-//   k_linearize     per point, after an accepted step: residual, analytic
-//                   Jacobian, robust weight; per-obs H_o, e_o; per-point H_ll,
-//                   g_l                               (ba.wgsl:63-135, 185-204)
-//   k_point_prep    per point: damped 3x3 inverse in FP64, v = H^-1 g
-//                                                      (ba.wgsl:209-243)
+//   k_linearize     per observation, after an accepted step: residual,
+//                   analytic Jacobian, robust weight; H_o, e_o
+//                                                      (ba.wgsl:63-135)
+//   k_point_prep    per point: H_ll and g_l from its observations' records
+//                   (after an accepted step), damped 3x3 inverse in FP64,
+//                   v = H^-1 g; the point's records for the assembly
+//                                                      (ba.wgsl:185-243)
 //   k_offdiag       per camera pair: S_ij = -sum W_i H^-1 W_j^T, a segmented
 //                   reduction over the pair's points (no atomics)
 //   k_cam_diag      per camera: S_ii = H_pp + lambda I - sum W H^-1 W^T, the
