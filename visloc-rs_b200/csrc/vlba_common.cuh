@@ -107,6 +107,12 @@ struct PcgState {
   uint32_t pad;
 };
 
+// Off-diagonal blocks of at least this many terms are summed on kLongLanes
+// lanes instead of the plan's lane count (a block's summation order then
+// depends on its own length only, the same alone and in any batch).
+constexpr uint32_t kLongBlockTerms = 1024;
+constexpr int kLongLanes = 16;
+
 // Everything the kernels touch.  Passed by value.
 struct Dev {
   // sizes
@@ -196,6 +202,13 @@ struct Dev {
   // (first, end) and destination, at its place in that order.
   const uint2* ord_range;      // [num_offdiag_blocks]
   const uint2* ord_dst;        // [num_offdiag_blocks]
+  // Blocks of at least kLongBlockTerms terms, summed on kLongLanes lanes
+  // (the lane count of a block follows from its own length alone), listed
+  // in any order: their term ranges and destinations, and their count.
+  const uint2* long_range;     // [num_offdiag_blocks]
+  const uint2* long_dst;       // [num_offdiag_blocks]
+  uint32_t* num_long;          // [1] appended by the block order at upload
+  uint32_t num_long_blocks;    // the same count, read back at upload
   const uint2* pairs;          // (k_i, k_j), sorted by block then point
   uint32_t* pair_pt;           // [pairs] each term's point (set at upload)
   const uint2* blk_dst;        // [num_offdiag_blocks] float offsets (block, mirror or kNone)

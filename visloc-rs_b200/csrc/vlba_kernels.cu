@@ -456,34 +456,38 @@ __device__ __forceinline__ void point_inverse64(const Dev& d, uint32_t l, double
 // blocks, each block's range and destination stored at its place): the groups of
 // a warp then loop about as many times (lane-pass efficiency 0.82 -> 0.99 on
 // ring-4m) while the blocks running at one time stay those of nearby rows.
-template <int G>
+// LONG: the blocks of the long list (at least kLongBlockTerms terms) on G
+// lanes each; otherwise the other blocks in the length-sorted order.
+template <int G, bool LONG>
 __global__ void __launch_bounds__(256, 2) k_offdiag(Dev d) {
   constexpr int kPerWarp = 32 / G;
   const uint32_t lane = threadIdx.x % G;
   const uint32_t warp_global = (blockIdx.x * blockDim.x + threadIdx.x) / 32;
   const uint32_t warps_total = gridDim.x * blockDim.x / 32;
   const uint32_t tile_floats = d.tb * d.tb * kBlock;
-  const uint32_t nwb = (d.num_offdiag_blocks + kPerWarp - 1) / kPerWarp;
+  const uint32_t nblocks = LONG ? d.num_long_blocks : d.num_offdiag_blocks;
+  const uint32_t nwb = (nblocks + kPerWarp - 1) / kPerWarp;
   for (uint32_t wb = warp_global; wb < nwb; wb += warps_total) {
     const uint32_t q = wb * kPerWarp + (threadIdx.x % 32) / G;
-    bool valid = q < d.num_offdiag_blocks;
+    bool valid = q < nblocks;
     uint2 dst = make_uint2(kNone, kNone), pr = make_uint2(0u, 0u);
     uint32_t c0 = 0, c1 = 0, pt = 0;
     if (valid) {
       // The block's range and first pair go out beside its problem's status
       // (a single problem's is the same for every block): the pair loads do
       // not wait for the lookup of the problem.
-      const uint2 range = d.ord_range[q];
-      dst = d.ord_dst[q];
+      const uint2 range = LONG ? d.long_range[q] : d.ord_range[q];
+      dst = LONG ? d.long_dst[q] : d.ord_dst[q];
       c0 = range.x;
       c1 = range.y;
+      if (!LONG && c1 - c0 >= kLongBlockTerms) c1 = c0;  // the long kernel's block
       if (c0 + lane < c1) {
         pr = d.pairs[c0 + lane];
         pt = d.pair_pt[c0 + lane];
       }
       const uint32_t P =
           d.num_problems == 1 ? 0u : d.tr_prob[d.tile_ij[dst.x / tile_floats] >> 16];
-      valid = !d.ctrl[P].done;
+      valid = !d.ctrl[P].done && (LONG || range.y - range.x < kLongBlockTerms);
     }
     float acc[36], cmp[36];
 #pragma unroll
@@ -2188,7 +2192,8 @@ __global__ void k_wait_probe(const unsigned int* flag, unsigned long long limit_
 // written at its place in that order.
 __global__ void __launch_bounds__(256) k_block_order(const uint32_t* blk_off, const uint2* blk_dst,
                                                      uint32_t nb, uint32_t g, uint2* ord_range,
-                                                     uint2* ord_dst) {
+                                                     uint2* ord_dst, uint2* long_range,
+                                                     uint2* long_dst, uint32_t* num_long) {
   __shared__ uint32_t key[256];
   const uint32_t b0 = blockIdx.x * 256u, t = threadIdx.x;
   const uint32_t n = min(256u, nb - b0);
@@ -2202,8 +2207,14 @@ __global__ void __launch_bounds__(256) k_block_order(const uint32_t* blk_off, co
       const uint32_t kj = key[j];
       rank += (kj > k || (kj == k && j < t)) ? 1u : 0u;
     }
-    ord_range[b0 + rank] = make_uint2(blk_off[b0 + t], blk_off[b0 + t + 1]);
+    const uint2 range = make_uint2(blk_off[b0 + t], blk_off[b0 + t + 1]);
+    ord_range[b0 + rank] = range;
     ord_dst[b0 + rank] = blk_dst[b0 + t];
+    if (range.y - range.x >= kLongBlockTerms) {
+      const uint32_t at = atomicAdd(num_long, 1u);  // any order: a block's sums do not depend on it
+      long_range[at] = range;
+      long_dst[at] = blk_dst[b0 + t];
+    }
   }
 }
 
@@ -2309,13 +2320,18 @@ cudaError_t launch_offdiag(const Dev& d, cudaStream_t s) {
   const size_t threads_needed = (size_t)d.num_offdiag_blocks * d.group;
   const int g = grid1d(threads_needed, 256, 148 * 16);
   switch (d.group) {
-    case 1: k_offdiag<1><<<g, 256, 0, s>>>(d); break;
-    case 2: k_offdiag<2><<<g, 256, 0, s>>>(d); break;
-    case 4: k_offdiag<4><<<g, 256, 0, s>>>(d); break;
-    case 8: k_offdiag<8><<<g, 256, 0, s>>>(d); break;
-    case 16: k_offdiag<16><<<g, 256, 0, s>>>(d); break;
-    default: k_offdiag<32><<<g, 256, 0, s>>>(d); break;
+    case 1: k_offdiag<1, false><<<g, 256, 0, s>>>(d); break;
+    case 2: k_offdiag<2, false><<<g, 256, 0, s>>>(d); break;
+    case 4: k_offdiag<4, false><<<g, 256, 0, s>>>(d); break;
+    case 8: k_offdiag<8, false><<<g, 256, 0, s>>>(d); break;
+    case 16: k_offdiag<16, false><<<g, 256, 0, s>>>(d); break;
+    default: k_offdiag<32, false><<<g, 256, 0, s>>>(d); break;
   }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  if (d.num_long_blocks == 0) return cudaSuccess;
+  const int gl = grid1d((size_t)d.num_long_blocks * kLongLanes, 256, 148 * 16);
+  k_offdiag<kLongLanes, true><<<gl, 256, 0, s>>>(d);
   return cudaGetLastError();
 }
 
@@ -2405,9 +2421,12 @@ cudaError_t launch_pair_points(const Dev& d, uint64_t n, cudaStream_t s) {
 
 cudaError_t launch_block_order(const Dev& d, cudaStream_t s) {
   if (d.num_offdiag_blocks == 0) return cudaSuccess;
+  cudaError_t e = cudaMemsetAsync(d.num_long, 0, 4, s);
+  if (e != cudaSuccess) return e;
   k_block_order<<<(d.num_offdiag_blocks + 255) / 256, 256, 0, s>>>(
       d.blk_off, d.blk_dst, d.num_offdiag_blocks, d.group, const_cast<uint2*>(d.ord_range),
-      const_cast<uint2*>(d.ord_dst));
+      const_cast<uint2*>(d.ord_dst), const_cast<uint2*>(d.long_range),
+      const_cast<uint2*>(d.long_dst), d.num_long);
   return cudaGetLastError();
 }
 

@@ -1343,7 +1343,7 @@ size_t Plan::device_bytes() const {
   b += nobs * (4 * 4 + 16 + 32 + 16);                // point, pose, cam, slot, xy, obs_h, obs_e
   b += obs_w.size() * 8 + obs_kind.size() * (1 + 16 + 4);
   b += cam_obs.size() * 8 + (pairs_on_device ? num_pairs : pairs.size()) * 12 + dup_pairs.size() * 8;
-  b += blk_dst.size() * (8 + 4 + 16);
+  b += blk_dst.size() * (8 + 4 + 32);
   b += tile_ij.size() * ((size_t)tb * tb * kBlock * 4 + 4 + 2 * (size_t)tb * 6 * 4);
   b += (size_t)num_var_cams * (4 + 4 + 4 + 4 + 36 * 4 + 6 * 4 * 6);
   b += tr_list.size() * 4 + (size_t)num_tile_rows * (4 + 4 + 16 * 8);

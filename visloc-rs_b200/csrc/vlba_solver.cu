@@ -567,6 +567,9 @@ void upload_plan_once(Context* c, uint32_t max_records, const std::function<void
   d.blk_dst = reinterpret_cast<const uint2*>(st.up(A, P.blk_dst));
   d.ord_range = A.alloc<uint2>(P.blk_dst.size());
   d.ord_dst = A.alloc<uint2>(P.blk_dst.size());
+  d.long_range = A.alloc<uint2>(P.blk_dst.size());
+  d.long_dst = A.alloc<uint2>(P.blk_dst.size());
+  d.num_long = A.alloc<uint32_t>(1);
   d.diag_dst = st.up(A, P.diag_dst);
   d.dup_off = st.up(A, P.dup_off);
   d.dup_pairs = reinterpret_cast<const uint2*>(st.up(A, P.dup_pairs));
@@ -609,6 +612,9 @@ void upload_plan_once(Context* c, uint32_t max_records, const std::function<void
   if (before_kernels) before_kernels();
   check_launch(launch_cam_points(d, (uint32_t)P.cam_obs.size(), s), "camera lists");
   check_launch(launch_block_order(d, s), "block order");
+  uint32_t num_long = 0;
+  if (d.num_offdiag_blocks)
+    VLBA_CUDA(cudaMemcpyAsync(&num_long, d.num_long, 4, cudaMemcpyDeviceToHost, s));
   if (P.pairs_on_device) {
     // The terms, from the uploaded point-major observations and per-slot
     // lists, at the places the host laid out; checked as they are written.
@@ -660,6 +666,9 @@ void upload_plan_once(Context* c, uint32_t max_records, const std::function<void
   }
   if (c->dev.trace && c->pcg_grid > c->pcg_grid_hint) c->dev.trace = nullptr;  // sized for fewer blocks
   VLBA_CUDA(cudaStreamSynchronize(s));
+  if (num_long > c->dev.num_offdiag_blocks)
+    throw std::runtime_error("long off-diagonal block count out of range");
+  c->dev.num_long_blocks = num_long;
   c->uploaded = true;
 }
 
@@ -785,8 +794,10 @@ uint64_t enqueue_iteration(Context* c, cudaEvent_t* ev) {
   check_launch(launch_decide(d, false, s), "decide");
   if (ev) VLBA_CUDA(cudaEventRecord(ev[4], s));
   // linearize, point prep, pcg setup, pose update, cost, decide always;
-  // off-diagonal, camera-diagonal and PCG kernels when the system has them.
-  return 6 + (d.num_offdiag_blocks ? 1 : 0) + (d.num_var_cams ? 1 : 0) + (d.num_tile_rows ? 1 : 0);
+  // off-diagonal (short and long blocks), camera-diagonal and PCG kernels
+  // when the system has them.
+  return 6 + (d.num_offdiag_blocks ? 1 : 0) + (d.num_long_blocks ? 1 : 0) + (d.num_var_cams ? 1 : 0) +
+         (d.num_tile_rows ? 1 : 0);
 }
 
 uint64_t enqueue_initial(Context* c) {
