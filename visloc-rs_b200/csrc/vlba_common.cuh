@@ -111,7 +111,7 @@ struct PcgState {
 // lanes instead of the plan's lane count (a block's summation order then
 // depends on its own length only, the same alone and in any batch).
 constexpr uint32_t kLongBlockTerms = 1024;
-constexpr int kLongLanes = 16;
+constexpr int kLongLanes = 32;
 
 // Everything the kernels touch.  Passed by value.
 struct Dev {
