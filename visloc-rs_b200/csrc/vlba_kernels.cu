@@ -1152,7 +1152,7 @@ __global__ void __launch_bounds__(256) k_decide(Dev d) {
 // One cooperative launch runs every iteration; two grid barriers each.
 //   A  every warp streams its own tiles of S (8 x 8 blocks of 6x6, 9.2 KB)
 //      HBM/L2 -> shared memory with cp.async.bulk (TMA) through a private
-//      three-stage ring, and writes per tile (I,J) the row-side partial
+//      two-stage ring, and writes per tile (I,J) the row-side partial
 //      S_IJ p_J and the column-side partial S_IJ^T p_I, with p = z + beta p
 //      formed on the fly; no block-wide synchronisation per tile.  Partials
 //      of a tile row are contiguous; each tile posts a release increment on
@@ -1184,7 +1184,7 @@ struct Pcg {
   static constexpr int kOwnMax = 32;
   static constexpr int kOwnFloats = 5 * kRow + 6 * kRow;
   static constexpr size_t kSmem = kWarps * kWarpBytes + (size_t)kWarps * kRow * 4 +
-                                  (size_t)kThreads * 8 + (size_t)kOwnMax * kOwnFloats * 4 + 64;
+                                  (size_t)kWarps * 8 + (size_t)kOwnMax * kOwnFloats * 4 + 64;
 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
@@ -1527,7 +1527,7 @@ __device__ __forceinline__ void take_slots(float (&v)[U][2], Src src, Valid vali
       if (valid(u, e)) __stcg(src(u) + 32 * e, __uint_as_float(kSlotEmpty));
 }
 
-__global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
+__global__ void __launch_bounds__(Pcg::kThreads, 1) k_pcg(Dev d) {
   using C = Pcg;
   constexpr int NW = C::kWarps;
   extern __shared__ __align__(128) unsigned char smem[];
@@ -1538,8 +1538,8 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
   float* const wPI = reinterpret_cast<float*>(wbase + (size_t)C::kStages * C::kTileBytes);
   float* const wPJ = wPI + C::kRow;
   float* const colw = reinterpret_cast<float*>(smem + (size_t)NW * C::kWarpBytes);  // [NW kRow]
-  double* const red = reinterpret_cast<double*>(colw + NW * C::kRow);             // [N]
-  float* const own = reinterpret_cast<float*>(red + C::kThreads);  // [kOwnMax][kOwnFloats]
+  double* const red = reinterpret_cast<double*>(colw + NW * C::kRow);             // [NW]
+  float* const own = reinterpret_cast<float*>(red + NW);  // [kOwnMax][kOwnFloats]
   __shared__ uint64_t mbar[NW][C::kStages];
   __shared__ ProbScal sc;
   __shared__ uint32_t sc_prob;
@@ -1566,17 +1566,19 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
     sc_k = -2;
   }
   __syncthreads();
-  // Warp tile sequence s = k Mw + m: stage s % kStages, phase (s / kStages) & 1.
-  // `issued` (sequence number of the next copy) and `iss_m` (its tile index
-  // m, kept modulo Mw by increments) are tracked by lane 0 alone.
+  // Warp tile sequence s = k Mw + m: stage s % kStages, phase (s / kStages) & 1,
+  // both kept by increments: (cst, cph) for the next tile to consume, ist for
+  // the next copy.  `issued` (sequence number of the next copy), `iss_m` (its
+  // tile index m, kept modulo Mw) and ist are tracked by lane 0 alone.
   uint64_t issued = 0, consumed = 0;
-  uint32_t iss_m = 0;
+  uint32_t iss_m = 0, ist = 0, cst = 0, cph = 0;
   auto issue = [&]() {  // lane 0 only
     const uint32_t t = gw + iss_m * TW;
-    const int st = (int)(issued % C::kStages);
+    const int st = (int)ist;
     tma_load(ring + (size_t)st * C::kTileFloats, d.tiles + (size_t)t * C::kTileFloats,
              C::kTileBytes, &mbar[warp][st], t < d.l2_resident_tiles ? keep : stream);
     ++issued;
+    ist = ist + 1u == (uint32_t)C::kStages ? 0u : ist + 1u;
     iss_m = (iss_m + 1u == Mw) ? 0u : iss_m + 1u;
   };
   bool ok = true;
@@ -1745,9 +1747,10 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
     for (size_t i = (size_t)blockIdx.x * blockDim.x + tid; i < n; i += (size_t)G * blockDim.x)
       __stcg(d.partial + i, __uint_as_float(kSlotEmpty));
   }
-  // The metadata of the warp's first two tiles (the same every iteration).
+  // The metadata of the warp's first three tiles (the same every iteration).
   const uint4 meta0 = Mw > 0 ? d.tile_meta[gw] : make_uint4(0u, 0u, 0u, 0u);
   const uint4 meta1 = Mw > 1 ? d.tile_meta[gw + TW] : make_uint4(0u, 0u, 0u, 0u);
+  const uint4 meta2 = Mw > 2 ? d.tile_meta[gw + 2 * TW] : make_uint4(0u, 0u, 0u, 0u);
   // The first tiles of every warp go out before the barrier.
   if (lane == 0)
     while (issued < (uint64_t)C::kStages && issued < Mw) issue();
@@ -1783,20 +1786,22 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
     }
     trace_mark(d, k, 1);
     {
-      // Software pipeline per warp: tile metadata two tiles ahead, the p/z
+      // Software pipeline per warp: tile metadata three tiles ahead, the p/z
       // segments (entries e = lane + 32 j of [0, 2 kRow): row I's, then row
-      // J's) one tile ahead, the tile itself kStages ahead (TMA ring).
+      // J's) two tiles ahead in two register sets that alternate (the loop
+      // is unrolled by two, so neither set is indexed at run time), the tile
+      // itself kStages ahead (TMA ring).
       constexpr int kPre = (2 * C::kRow + 31) / 32;
-      float pre_p[kPre], pre_z[kPre];
-      auto prefetch_seg = [&](uint32_t ij) {
+      float pa_p[kPre], pa_z[kPre], pb_p[kPre], pb_z[kPre];
+      auto prefetch_seg = [&](float (&pp)[kPre], float (&pz)[kPre], uint32_t ij) {
 #pragma unroll
         for (int j = 0; j < kPre; ++j) {
           const uint32_t e = lane + 32u * j;
           if (e < 2u * C::kRow) {
             const uint32_t row = e < (uint32_t)C::kRow ? (ij >> 16) : (ij & 0xFFFFu);
             const size_t at = (size_t)row * C::kRow + (e % C::kRow);
-            pre_p[j] = __ldcg(d.p + at);
-            pre_z[j] = __ldcg(d.z + at);
+            pp[j] = __ldcg(d.p + at);
+            pz[j] = __ldcg(d.z + at);
           }
         }
       };
@@ -1804,15 +1809,20 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
       ProbScal ws;
       ws.active = 0;
       ws.beta = 0.0;
-      uint4 meta_cur = meta0, meta_nxt = meta1;
-      if (Mw > 0) prefetch_seg(meta_cur.x);
+      uint4 meta_cur = meta0, meta_n1 = meta1, meta_n2 = meta2;
+      if (Mw > 0) prefetch_seg(pa_p, pa_z, meta0.x);
+      if (Mw > 1) prefetch_seg(pb_p, pb_z, meta1.x);
       trace_warp(d, k, gw, TW, 0);
-      for (uint32_t m = 0; m < Mw; ++m) {
+      // Tile m with its segments in (pre_p, pre_z); they are refilled with
+      // tile m + 2's once copied out.  A tile's segments are read before its
+      // partials are stored, so before the owners of its rows can reduce
+      // them and write the next p.
+      auto step = [&](uint32_t m, float (&pre_p)[kPre], float (&pre_z)[kPre]) {
         const uint64_t s = (uint64_t)k * Mw + m;
         trace_tile(d, k, gw, TW, m, 0);
         const uint4 meta = meta_cur;
-        uint4 meta_nn = make_uint4(0u, 0u, 0u, 0u);
-        if (m + 2 < Mw) meta_nn = d.tile_meta[gw + (m + 2) * TW];
+        uint4 meta_n3 = make_uint4(0u, 0u, 0u, 0u);
+        if (m + 3 < Mw) meta_n3 = d.tile_meta[gw + (m + 3) * TW];
         const uint32_t I = meta.x >> 16, J = meta.x & 0xFFFFu;
         const uint32_t P = meta.w;
         if (P != wprob) {
@@ -1832,13 +1842,16 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
             }
           }
         }
-        if (m + 1 < Mw) prefetch_seg(meta_nxt.x);
-        const int st = (int)(s % C::kStages);
+        if (m + 2 < Mw) prefetch_seg(pre_p, pre_z, meta_n2.x);
+        const int st = (int)cst;
         trace_tile(d, k, gw, TW, m, 1);
         const bool arrived =
-            __all_sync(0xffffffffu, mbar_wait(&mbar[warp][st], (uint32_t)((s / C::kStages) & 1),
-                                              d.error));
+            __all_sync(0xffffffffu, mbar_wait(&mbar[warp][st], cph, d.error));
         consumed = s + 1;
+        if (++cst == (uint32_t)C::kStages) {
+          cst = 0u;
+          cph ^= 1u;
+        }
         __syncwarp();  // the segments are visible to the whole warp
         trace_tile(d, k, gw, TW, m, 2);
         if (!arrived) ok = false;
@@ -1952,8 +1965,13 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
         // Refill the stage with the tile kStages ahead (possibly the next
         // iteration's; S does not change during the solve).
         if (lane == 0 && issued < s + 1 + C::kStages) issue();
-        meta_cur = meta_nxt;
-        meta_nxt = meta_nn;
+        meta_cur = meta_n1;
+        meta_n1 = meta_n2;
+        meta_n2 = meta_n3;
+      };
+      for (uint32_t m = 0; m < Mw; m += 2) {
+        step(m, pa_p, pa_z);
+        if (m + 1 < Mw) step(m + 1, pb_p, pb_z);
       }
       trace_warp(d, k, gw, TW, 1);
     }
@@ -2106,8 +2124,11 @@ __global__ void __launch_bounds__(Pcg::kThreads) k_pcg(Dev d) {
   if (lane == 0) {
     for (uint64_t s = consumed; s < issued; ++s) {
       const unsigned long long t_end = now_ns() + kWaitLimitNs;
-      while (!mbar_try_wait(&mbar[warp][s % C::kStages], (uint32_t)((s / C::kStages) & 1)) &&
-             now_ns() <= t_end) {
+      while (!mbar_try_wait(&mbar[warp][cst], cph) && now_ns() <= t_end) {
+      }
+      if (++cst == (uint32_t)C::kStages) {
+        cst = 0u;
+        cph ^= 1u;
       }
     }
   }
