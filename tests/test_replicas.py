@@ -101,3 +101,15 @@ def test_compact_keeps_the_named_keys():
     assert bench.compact(line, ["value", "unit", "clocks", "missing"]) == {
         "value": 1.0, "unit": "u", "clocks": {}}
     assert bench.compact(None, ["value"]) is None
+
+
+def test_pcg_traffic_comes_only_from_the_workloads_own_capture():
+    """The roofline's DRAM traffic is read from the committed ncu summary of
+    the same workload; a workload without a capture of its own reports none."""
+    sys.path[:0] = [ROOT]
+    import bench
+
+    ring = bench.traffic_per_pcg_iteration("ring-4m")
+    assert ring is not None and 1e7 < ring < 1.1e8  # below B_pcg = 106.5 MB: S partly in L2
+    for name in ("street-20m", "windows-512", "ring-50"):
+        assert bench.traffic_per_pcg_iteration(name) is None
