@@ -1155,12 +1155,15 @@ __global__ void __launch_bounds__(256) k_decide(Dev d) {
 //      two-stage ring, and writes per tile (I,J) the row-side partial
 //      S_IJ p_J and the column-side partial S_IJ^T p_I, with p = z + beta p
 //      formed on the fly; no block-wide synchronisation per tile.  Partials
-//      of a tile row are contiguous; each tile posts a release increment on
-//      the row's arrival counter.  The owner block of a row (row mod grid)
-//      then waits (bounded) for the row's count and reduces it in a fixed
-//      order into q, the new p and the partial p.q.
+//      of a tile row are contiguous slots that hold an empty marker until
+//      their tile stores them; the owner block of a row (row mod grid) reads
+//      each slot as soon as it is filled (bounded), reduces the row in a
+//      fixed order into q, the new p and the partial p.q, and empties the
+//      slots again.
+//   -- grid barrier --
 //   C  the owner of a tile row: x += alpha p, r -= alpha q, z = M^-1 r and
 //      the partial dots r.z and r.r.
+//   -- grid barrier --
 // The first tiles of the next iteration are prefetched before the barriers.
 // The leading tiles (a byte budget set from the L2 size) are loaded with an
 // L2 evict_last policy and the rest with evict_first; at exit the resident
